@@ -1,0 +1,894 @@
+/*
+ * CPU oracle -- TEST INFRASTRUCTURE ONLY (see exa_oracle.h).
+ *
+ * Plain-C FP64 restatement of ExaHyPE's generic ADER-DG and FV kernels.
+ * Every function cites the reference file:line it follows.  Loop orders
+ * follow the reference so that rounding stays close to it; the DG tables
+ * come from the project's generated dg_tables.h (derived from the
+ * mathematics and pinned against the reference's tables by
+ * tests/test_dg_tables.py).
+ */
+#include "exa_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../exahype_b200/csrc/dg_tables.h"
+
+#define GAMMA 1.4
+#define W(N, i) (exa_gl_weights[(N)][(i)])
+
+/* ------------------------------------------------------------------ */
+/* PDE: GenericEulerKernelTest3D.cpp:26-82, GenericEulerKernelTest2D.cpp:28-79 */
+void orc_euler_flux(int dim, int planar, const double* Q, double* F) {
+  const double irho = 1.0 / Q[0];
+  const double j2 = planar ? (Q[1] * Q[1] + Q[2] * Q[2])
+                           : (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]);
+  const double p = (GAMMA - 1) * (Q[4] - 0.5 * j2 * irho);
+  for (int d = 0; d < dim; d++) {
+    double* f = F + 5 * d;
+    const double jn = Q[d + 1];
+    f[0] = jn;
+    f[1] = irho * jn * Q[1];
+    f[2] = irho * jn * Q[2];
+    f[3] = irho * jn * Q[3];
+    f[d + 1] += p;
+    f[4] = irho * jn * (Q[4] + p);
+  }
+}
+
+void orc_euler_eigenvalues(int planar, const double* Q, int d, double* lambda) {
+  const double irho = 1.0 / Q[0];
+  const double j2 = planar ? (Q[1] * Q[1] + Q[2] * Q[2])
+                           : (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]);
+  const double p = (GAMMA - 1) * (Q[4] - 0.5 * j2 * irho);
+  const double un = Q[d + 1] * irho;
+  const double c = sqrt(GAMMA * p * irho);
+  lambda[0] = un - c;
+  lambda[1] = un;
+  lambda[2] = un;
+  lambda[3] = un;
+  lambda[4] = un + c;
+}
+
+/* ------------------------------------------------------------------ */
+/* 3D space-time predictor:
+ * kernels/aderdg/generic/c/3d/spaceTimePredictorNonlinear.cpph
+ *   Picard loop :43-317, time averaging :325-397, extrapolation :399-519,
+ *   driver :523-577.  Flux only (the Euler PDE has no source / NCP). */
+static int stp3d(int N, int V, int P, int planar, double* lQhbnd, double* lFhbnd,
+                 double* lQi, double* lQi_old, double* rhs, double* lFi,
+                 double* lQhi, double* lFhi, const double* luh,
+                 const double* dx, double dt) {
+  const int B = N + 1, D = V + P, B2 = B * B, B3 = B2 * B, B4 = B3 * B;
+#define LUH(z, y, x, m) luh[(((z) * B + (y)) * B + (x)) * D + (m)]
+#define LQI(z, y, x, t, m) lQi[((((z) * B + (y)) * B + (x)) * B + (t)) * D + (m)]
+#define LFI(t, z, y, x, d, m) lFi[(((((t) * B + (z)) * B + (y)) * B + (x)) * 4 + (d)) * V + (m)]
+#define RHS(t, z, y, x, m) rhs[((((t) * B + (z)) * B + (y)) * B + (x)) * V + (m)]
+  /* trivial initial guess :65-79 */
+  for (int z = 0; z < B; z++)
+    for (int y = 0; y < B; y++)
+      for (int x = 0; x < B; x++)
+        for (int t = 0; t < B; t++)
+          for (int m = 0; m < D; m++) LQI(z, y, x, t, m) = LUH(z, y, x, m);
+
+  const int maxit = 2 * (N + 1); /* :82 */
+  int it;
+  for (it = 0; it < maxit; it++) {
+    memcpy(lQi_old, lQi, sizeof(double) * B4 * D);
+    for (int t = 0; t < B; t++) {
+      /* fluxes :93-115 */
+      for (int z = 0; z < B; z++)
+        for (int y = 0; y < B; y++)
+          for (int x = 0; x < B; x++) {
+            double F[15];
+            orc_euler_flux(3, planar, &LQI(z, y, x, t, 0), F);
+            for (int d = 0; d < 3; d++)
+              for (int m = 0; m < V; m++) LFI(t, z, y, x, d, m) = F[5 * d + m];
+            for (int m = 0; m < V; m++) LFI(t, z, y, x, 3, m) = 0.0;
+          }
+      /* rhs0 :117-133 */
+      for (int z = 0; z < B; z++)
+        for (int y = 0; y < B; y++)
+          for (int x = 0; x < B; x++) {
+            const double w = W(N, z) * W(N, y) * W(N, x);
+            for (int m = 0; m < V; m++)
+              RHS(t, z, y, x, m) = w * exa_f0[N][t] * LUH(z, y, x, m);
+          }
+      /* x derivative :141-169 */
+      for (int z = 0; z < B; z++)
+        for (int y = 0; y < B; y++) {
+          const double us = W(N, t) * W(N, z) * W(N, y) * dt / dx[0];
+          for (int l = 0; l < B; l++)
+            for (int m = 0; m < V; m++)
+              for (int n = 0; n < B; n++)
+                RHS(t, z, y, l, m) -= us * LFI(t, z, y, n, 0, m) * exa_kxi[N][n][l];
+        }
+      /* y derivative :171-197 */
+      for (int z = 0; z < B; z++)
+        for (int x = 0; x < B; x++) {
+          const double us = W(N, t) * W(N, z) * W(N, x) * dt / dx[1];
+          for (int l = 0; l < B; l++)
+            for (int m = 0; m < V; m++)
+              for (int n = 0; n < B; n++)
+                RHS(t, z, l, x, m) -= us * LFI(t, z, n, x, 1, m) * exa_kxi[N][n][l];
+        }
+      /* z derivative :199-225 */
+      for (int y = 0; y < B; y++)
+        for (int x = 0; x < B; x++) {
+          const double us = W(N, t) * W(N, y) * W(N, x) * dt / dx[2];
+          for (int l = 0; l < B; l++)
+            for (int m = 0; m < V; m++)
+              for (int n = 0; n < B; n++)
+                RHS(t, l, y, x, m) -= us * LFI(t, n, y, x, 2, m) * exa_kxi[N][n][l];
+        }
+    }
+    /* zero the variables (not the parameters) :255-268 */
+    for (int s = 0; s < B4; s++)
+      for (int m = 0; m < V; m++) lQi[s * D + m] = 0.0;
+    /* discrete time integral with iK1 :270-296 */
+    for (int z = 0; z < B; z++)
+      for (int y = 0; y < B; y++)
+        for (int x = 0; x < B; x++) {
+          const double iw = 1.0 / (W(N, z) * W(N, y) * W(N, x));
+          for (int l = 0; l < B; l++)
+            for (int m = 0; m < V; m++)
+              for (int n = 0; n < B; n++)
+                LQI(z, y, x, l, m) += iw * RHS(n, z, y, x, m) * exa_ik1[N][l][n];
+        }
+    /* exit condition :298-306 */
+    double sq = 0.0;
+    for (int i = 0; i < B4 * D; i++) sq += (lQi_old[i] - lQi[i]) * (lQi_old[i] - lQi[i]);
+    if (sq < 1e-7 * 1e-7) { it++; break; }
+  }
+  /* time averaging :325-397 */
+  double* fx = lFhi;
+  double* fy = lFhi + B3 * V;
+  double* fz = lFhi + 2 * B3 * V;
+  double* sh = lFhi + 3 * B3 * V;
+  memset(lQhi, 0, sizeof(double) * B3 * D);
+  memset(lFhi, 0, sizeof(double) * 4 * B3 * V);
+  for (int z = 0; z < B; z++)
+    for (int y = 0; y < B; y++)
+      for (int x = 0; x < B; x++) {
+        for (int m = 0; m < V; m++)
+          for (int t = 0; t < B; t++) {
+            fx[((z * B + y) * B + x) * V + m] += LFI(t, z, y, x, 0, m) * W(N, t);
+            fy[((z * B + x) * B + y) * V + m] += LFI(t, z, y, x, 1, m) * W(N, t);
+            fz[((y * B + x) * B + z) * V + m] += LFI(t, z, y, x, 2, m) * W(N, t);
+          }
+        for (int m = 0; m < D; m++)
+          for (int t = 0; t < B; t++)
+            lQhi[((z * B + y) * B + x) * D + m] += LQI(z, y, x, t, m) * W(N, t);
+      }
+  (void)sh;
+  /* extrapolation :399-519 */
+  memset(lQhbnd, 0, sizeof(double) * 6 * B2 * D);
+  memset(lFhbnd, 0, sizeof(double) * 6 * B2 * V);
+#define QB(f, i, j, m) lQhbnd[(((f) * B + (i)) * B + (j)) * D + (m)]
+#define FB(f, i, j, m) lFhbnd[(((f) * B + (i)) * B + (j)) * V + (m)]
+  for (int i = 0; i < B; i++)
+    for (int j = 0; j < B; j++) {
+      for (int k = 0; k < V; k++)
+        for (int l = 0; l < B; l++) {
+          FB(0, i, j, k) += fx[((i * B + j) * B + l) * V + k] * exa_flcoeff[N][l];
+          FB(1, i, j, k) += fx[((i * B + j) * B + l) * V + k] * exa_frcoeff[N][l];
+          FB(2, i, j, k) += fy[((i * B + j) * B + l) * V + k] * exa_flcoeff[N][l];
+          FB(3, i, j, k) += fy[((i * B + j) * B + l) * V + k] * exa_frcoeff[N][l];
+          FB(4, i, j, k) += fz[((i * B + j) * B + l) * V + k] * exa_flcoeff[N][l];
+          FB(5, i, j, k) += fz[((i * B + j) * B + l) * V + k] * exa_frcoeff[N][l];
+        }
+      for (int k = 0; k < D; k++)
+        for (int l = 0; l < B; l++) {
+          QB(0, i, j, k) += lQhi[((i * B + j) * B + l) * D + k] * exa_flcoeff[N][l];
+          QB(1, i, j, k) += lQhi[((i * B + j) * B + l) * D + k] * exa_frcoeff[N][l];
+          QB(2, i, j, k) += lQhi[((i * B + l) * B + j) * D + k] * exa_flcoeff[N][l];
+          QB(3, i, j, k) += lQhi[((i * B + l) * B + j) * D + k] * exa_frcoeff[N][l];
+          QB(4, i, j, k) += lQhi[((l * B + i) * B + j) * D + k] * exa_flcoeff[N][l];
+          QB(5, i, j, k) += lQhi[((l * B + i) * B + j) * D + k] * exa_frcoeff[N][l];
+        }
+    }
+#undef QB
+#undef FB
+#undef LUH
+#undef LQI
+#undef LFI
+#undef RHS
+  return it;
+}
+
+/* 2D space-time predictor:
+ * kernels/aderdg/generic/c/2d/spaceTimePredictorNonlinear.cpph
+ *   Picard :43-266, averaging :274-330, extrapolation :332-409,
+ *   driver :586-634. */
+static int stp2d(int N, int V, int P, int planar, double* lQhbnd, double* lFhbnd,
+                 double* lQi, double* lQi_old, double* rhs, double* lFi,
+                 double* lQhi, double* lFhi, const double* luh,
+                 const double* dx, double dt) {
+  const int B = N + 1, D = V + P, B2 = B * B, B3 = B2 * B;
+#define LUH(y, x, m) luh[((y) * B + (x)) * D + (m)]
+#define LQI(y, x, t, m) lQi[(((y) * B + (x)) * B + (t)) * D + (m)]
+#define LFI(t, y, x, d, m) lFi[((((t) * B + (y)) * B + (x)) * 3 + (d)) * V + (m)]
+#define RHS(t, y, x, m) rhs[(((t) * B + (y)) * B + (x)) * V + (m)]
+  for (int y = 0; y < B; y++)
+    for (int x = 0; x < B; x++)
+      for (int t = 0; t < B; t++)
+        for (int m = 0; m < D; m++) LQI(y, x, t, m) = LUH(y, x, m);
+  const int maxit = 2 * (N + 1);
+  int it;
+  for (it = 0; it < maxit; it++) {
+    memcpy(lQi_old, lQi, sizeof(double) * B3 * D);
+    for (int t = 0; t < B; t++) {
+      for (int y = 0; y < B; y++)
+        for (int x = 0; x < B; x++) {
+          double F[10];
+          orc_euler_flux(2, planar, &LQI(y, x, t, 0), F);
+          for (int d = 0; d < 2; d++)
+            for (int m = 0; m < V; m++) LFI(t, y, x, d, m) = F[5 * d + m];
+          for (int m = 0; m < V; m++) LFI(t, y, x, 2, m) = 0.0;
+        }
+      for (int y = 0; y < B; y++)
+        for (int x = 0; x < B; x++) {
+          const double w = W(N, y) * W(N, x);
+          for (int m = 0; m < V; m++) RHS(t, y, x, m) = w * exa_f0[N][t] * LUH(y, x, m);
+        }
+      for (int y = 0; y < B; y++) {
+        const double us = W(N, t) * W(N, y) * dt / dx[0];
+        for (int l = 0; l < B; l++)
+          for (int m = 0; m < V; m++)
+            for (int n = 0; n < B; n++)
+              RHS(t, y, l, m) -= us * LFI(t, y, n, 0, m) * exa_kxi[N][n][l];
+      }
+      for (int x = 0; x < B; x++) {
+        const double us = W(N, t) * W(N, x) * dt / dx[1];
+        for (int l = 0; l < B; l++)
+          for (int m = 0; m < V; m++)
+            for (int n = 0; n < B; n++)
+              RHS(t, l, x, m) -= us * LFI(t, n, x, 1, m) * exa_kxi[N][n][l];
+      }
+    }
+    for (int s = 0; s < B3; s++)
+      for (int m = 0; m < V; m++) lQi[s * D + m] = 0.0;
+    for (int y = 0; y < B; y++)
+      for (int x = 0; x < B; x++) {
+        const double iw = 1.0 / (W(N, y) * W(N, x));
+        for (int l = 0; l < B; l++)
+          for (int m = 0; m < V; m++)
+            for (int n = 0; n < B; n++)
+              LQI(y, x, l, m) += iw * RHS(n, y, x, m) * exa_ik1[N][l][n];
+      }
+    double sq = 0.0;
+    for (int i = 0; i < B3 * D; i++) sq += (lQi_old[i] - lQi[i]) * (lQi_old[i] - lQi[i]);
+    if (sq < 1e-7 * 1e-7) { it++; break; }
+  }
+  double* fx = lFhi;
+  double* fy = lFhi + B2 * V;
+  memset(lQhi, 0, sizeof(double) * B2 * D);
+  memset(lFhi, 0, sizeof(double) * 3 * B2 * V);
+  for (int y = 0; y < B; y++)
+    for (int x = 0; x < B; x++) {
+      for (int m = 0; m < V; m++)
+        for (int t = 0; t < B; t++) {
+          fx[(y * B + x) * V + m] += LFI(t, y, x, 0, m) * W(N, t);
+          fy[(x * B + y) * V + m] += LFI(t, y, x, 1, m) * W(N, t);
+        }
+      for (int m = 0; m < D; m++)
+        for (int t = 0; t < B; t++) lQhi[(y * B + x) * D + m] += LQI(y, x, t, m) * W(N, t);
+    }
+  memset(lQhbnd, 0, sizeof(double) * 4 * B * D);
+  memset(lFhbnd, 0, sizeof(double) * 4 * B * V);
+  for (int j = 0; j < B; j++) {
+    for (int k = 0; k < V; k++)
+      for (int l = 0; l < B; l++) {
+        lFhbnd[(0 * B + j) * V + k] += fx[(j * B + l) * V + k] * exa_flcoeff[N][l];
+        lFhbnd[(1 * B + j) * V + k] += fx[(j * B + l) * V + k] * exa_frcoeff[N][l];
+        lFhbnd[(2 * B + j) * V + k] += fy[(j * B + l) * V + k] * exa_flcoeff[N][l];
+        lFhbnd[(3 * B + j) * V + k] += fy[(j * B + l) * V + k] * exa_frcoeff[N][l];
+      }
+    for (int k = 0; k < D; k++)
+      for (int l = 0; l < B; l++) {
+        lQhbnd[(0 * B + j) * D + k] += lQhi[(j * B + l) * D + k] * exa_flcoeff[N][l];
+        lQhbnd[(1 * B + j) * D + k] += lQhi[(j * B + l) * D + k] * exa_frcoeff[N][l];
+        lQhbnd[(2 * B + j) * D + k] += lQhi[(l * B + j) * D + k] * exa_flcoeff[N][l];
+        lQhbnd[(3 * B + j) * D + k] += lQhi[(l * B + j) * D + k] * exa_frcoeff[N][l];
+      }
+  }
+#undef LUH
+#undef LQI
+#undef LFI
+#undef RHS
+  return it;
+}
+
+int orc_stp_nonlinear(int dim, int order, int nvar, int npar, int planar,
+                      double* lQhbnd, double* lFhbnd, double* lQi,
+                      double* lQi_old, double* rhs, double* lFi, double* lQhi,
+                      double* lFhi, const double* luh, const double* dx,
+                      double dt) {
+  if (dim == 3)
+    return stp3d(order, nvar, npar, planar, lQhbnd, lFhbnd, lQi, lQi_old, rhs,
+                 lFi, lQhi, lFhi, luh, dx, dt);
+  return stp2d(order, nvar, npar, planar, lQhbnd, lFhbnd, lQi, lQi_old, rhs,
+               lFi, lQhi, lFhi, luh, dx, dt);
+}
+
+/* ------------------------------------------------------------------ */
+/* volume integral: c/3d/volumeIntegralNonlinear.cpph:26-125,
+ *                  c/2d/volumeIntegralNonlinear.cpph:31-96 */
+void orc_volume_integral(int dim, int order, int nvar, int use_source,
+                         double* lduh, const double* lFhi, const double* dx) {
+  const int N = order, B = N + 1, V = nvar;
+  if (dim == 3) {
+    const int B3 = B * B * B;
+    const double* fx = lFhi;
+    const double* fy = lFhi + B3 * V;
+    const double* fz = lFhi + 2 * B3 * V;
+    const double* sh = lFhi + 3 * B3 * V;
+#define I4(a, b, c, m) ((((a) * B + (b)) * B + (c)) * V + (m))
+    memset(lduh, 0, sizeof(double) * B3 * V);
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++) {
+        const double us = W(N, i) * W(N, j) / dx[0];
+        for (int k = 0; k < B; k++)
+          for (int l = 0; l < V; l++)
+            for (int m = 0; m < B; m++)
+              lduh[I4(i, j, k, l)] += exa_kxi[N][k][m] * fx[I4(i, j, m, l)] * us;
+      }
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++) {
+        const double us = W(N, i) * W(N, j) / dx[1];
+        for (int k = 0; k < B; k++)
+          for (int l = 0; l < V; l++)
+            for (int m = 0; m < B; m++)
+              lduh[I4(i, k, j, l)] += exa_kxi[N][k][m] * fy[I4(i, j, m, l)] * us;
+      }
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++) {
+        const double us = W(N, i) * W(N, j) / dx[2];
+        for (int k = 0; k < B; k++)
+          for (int l = 0; l < V; l++)
+            for (int m = 0; m < B; m++)
+              lduh[I4(k, i, j, l)] += exa_kxi[N][k][m] * fz[I4(i, j, m, l)] * us;
+      }
+    if (use_source)
+      for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++)
+          for (int k = 0; k < B; k++) {
+            const double w = W(N, i) * W(N, j) * W(N, k);
+            for (int l = 0; l < V; l++) lduh[I4(i, j, k, l)] += w * sh[I4(i, j, k, l)];
+          }
+#undef I4
+  } else {
+    const int B2 = B * B;
+    const double* fx = lFhi;
+    const double* fy = lFhi + B2 * V;
+    const double* sh = lFhi + 2 * B2 * V;
+#define I3(a, b, m) (((a) * B + (b)) * V + (m))
+    memset(lduh, 0, sizeof(double) * B2 * V);
+    for (int j = 0; j < B; j++) {
+      const double us = W(N, j) / dx[0];
+      for (int k = 0; k < B; k++)
+        for (int l = 0; l < V; l++)
+          for (int m = 0; m < B; m++)
+            lduh[I3(j, k, l)] += exa_kxi[N][k][m] * fx[I3(j, m, l)] * us;
+    }
+    for (int j = 0; j < B; j++) {
+      const double us = W(N, j) / dx[1];
+      for (int k = 0; k < B; k++)
+        for (int l = 0; l < V; l++)
+          for (int m = 0; m < B; m++)
+            lduh[I3(k, j, l)] += exa_kxi[N][k][m] * fy[I3(j, m, l)] * us;
+    }
+    if (use_source)
+      for (int j = 0; j < B; j++)
+        for (int k = 0; k < B; k++) {
+          const double w = W(N, j) * W(N, k);
+          for (int l = 0; l < V; l++) lduh[I3(j, k, l)] += w * sh[I3(j, k, l)];
+        }
+#undef I3
+  }
+}
+
+/* surface integral: c/3d/surfaceIntegralNonlinear.cpph:21-85,
+ *                   c/2d/surfaceIntegralNonlinear.cpph:26-65 */
+void orc_surface_integral(int dim, int order, int nvar, double* lduh,
+                          const double* lF, const double* dx) {
+  const int N = order, B = N + 1, V = nvar;
+  if (dim == 3) {
+#define I4(a, b, c, m) ((((a) * B + (b)) * B + (c)) * V + (m))
+#define FB(f, a, b, m) ((((f) * B + (a)) * B + (b)) * V + (m))
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++) {
+        const double us = W(N, i) * W(N, j) / dx[0];
+        for (int k = 0; k < B; k++)
+          for (int l = 0; l < V; l++)
+            lduh[I4(i, j, k, l)] -= (lF[FB(1, i, j, l)] * exa_frcoeff[N][k] -
+                                     lF[FB(0, i, j, l)] * exa_flcoeff[N][k]) * us;
+      }
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++)
+        for (int k = 0; k < B; k++) {
+          const double us = W(N, i) * W(N, k) / dx[1];
+          for (int l = 0; l < V; l++)
+            lduh[I4(i, j, k, l)] -= (lF[FB(3, i, k, l)] * exa_frcoeff[N][j] -
+                                     lF[FB(2, i, k, l)] * exa_flcoeff[N][j]) * us;
+        }
+    for (int i = 0; i < B; i++)
+      for (int j = 0; j < B; j++)
+        for (int k = 0; k < B; k++) {
+          const double us = W(N, j) * W(N, k) / dx[2];
+          for (int l = 0; l < V; l++)
+            lduh[I4(i, j, k, l)] -= (lF[FB(5, j, k, l)] * exa_frcoeff[N][i] -
+                                     lF[FB(4, j, k, l)] * exa_flcoeff[N][i]) * us;
+        }
+#undef I4
+#undef FB
+  } else {
+#define I3(a, b, m) (((a) * B + (b)) * V + (m))
+#define FB(f, a, m) ((((f) * B + (a))) * V + (m))
+    for (int j = 0; j < B; j++) {
+      const double us = W(N, j) / dx[0];
+      for (int k = 0; k < B; k++)
+        for (int l = 0; l < V; l++)
+          lduh[I3(j, k, l)] -= (lF[FB(1, j, l)] * exa_frcoeff[N][k] -
+                                lF[FB(0, j, l)] * exa_flcoeff[N][k]) * us;
+    }
+    for (int j = 0; j < B; j++)
+      for (int k = 0; k < B; k++) {
+        const double us = W(N, k) / dx[1];
+        for (int l = 0; l < V; l++)
+          lduh[I3(j, k, l)] -= (lF[FB(3, k, l)] * exa_frcoeff[N][j] -
+                                lF[FB(2, k, l)] * exa_flcoeff[N][j]) * us;
+      }
+#undef I3
+#undef FB
+  }
+}
+
+/* Rusanov face flux: c/3d/riemannSolverNonlinear.cpph:37-120,
+ *                    c/2d/riemannSolverNonlinear.cpph:37-114 */
+void orc_riemann(int dim, int order, int nvar, int npar, int planar, double* FL,
+                 double* FR, const double* QL, const double* QR, int direction) {
+  const int N = order, B = N + 1, V = nvar, D = nvar + npar;
+  const int nf = dim == 3 ? B * B : B;
+  double QavL[16] = {0}, QavR[16] = {0};
+  for (int i = 0; i < nf; i++) {
+    const double w = dim == 3 ? W(N, i / B) * W(N, i % B) : W(N, i);
+    for (int k = 0; k < D; k++) {
+      QavL[k] += w * QL[i * D + k];
+      QavR[k] += w * QR[i * D + k];
+    }
+  }
+  double LL[5], LR[5];
+  orc_euler_eigenvalues(planar, QavL, direction, LL);
+  orc_euler_eigenvalues(planar, QavR, direction, LR);
+  double sL = 0.0, sR = 0.0;
+  for (int k = 0; k < 5; k++) {
+    if (fabs(LL[k]) > sL) sL = fabs(LL[k]);
+    if (fabs(LR[k]) > sR) sR = fabs(LR[k]);
+  }
+  const double smax = sL > sR ? sL : sR;
+  for (int i = 0; i < nf; i++)
+    for (int k = 0; k < V; k++) {
+      const double f = 0.5 * (FR[i * V + k] + FL[i * V + k]) -
+                       0.5 * smax * (QR[i * D + k] - QL[i * D + k]);
+      FL[i * V + k] = f;
+      FR[i * V + k] = f;
+    }
+}
+
+/* c/3d/solutionUpdate.cpph:23-47, c/2d/solutionUpdate.cpph:23-45 */
+void orc_solution_update(int dim, int order, int nvar, int npar, double* luh,
+                         const double* lduh, double dt) {
+  const int N = order, B = N + 1, V = nvar, D = nvar + npar;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  for (int s = 0; s < nn; s++) {
+    double w;
+    if (dim == 3) w = W(N, s / (B * B)) * W(N, (s / B) % B) * W(N, s % B);
+    else w = W(N, s / B) * W(N, s % B);
+    const double us = dt / w;
+    for (int l = 0; l < V; l++) luh[s * D + l] += lduh[s * V + l] * us;
+  }
+}
+
+/* c/3d/stableTimeStepSize.cpph:21-61, c/2d/stableTimeStepSize.cpph:13-56 */
+double orc_stable_dt(int dim, int order, int nvar, int npar, int planar,
+                     const double* luh, const double* dx, double cfl) {
+  const int B = order + 1, D = nvar + npar;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  double dt = DBL_MAX;
+  for (int s = 0; s < nn; s++) {
+    double den = 0.0;
+    for (int d = 0; d < dim; d++) {
+      double lam[5];
+      orc_euler_eigenvalues(planar, luh + s * D, d, lam);
+      double mx = 0.0;
+      for (int v = 0; v < nvar; v++) mx = fabs(lam[v]) > mx ? fabs(lam[v]) : mx;
+      den += mx / dx[d];
+    }
+    const double c = cfl * exa_pnpm[order] / den;
+    dt = c < dt ? c : dt;
+  }
+  return dt;
+}
+
+/* ------------------------------------------------------------------ */
+/* Uniform periodic grid driver.  Step order of the reference's non-fused
+ * time step (exahype/runners/Runner.cpp:1125-1160): dt (ADERDGSolver.cpp:
+ * 1948-2000 + global min TimeStepSizeComputation.cpp:83-109), predictor +
+ * volume integral (ADERDGSolver.cpp:1818-1946), Riemann on every face with
+ * the left cell's face 2d+1 and the right cell's face 2d (ADERDGSolver.cpp:
+ * 2744-2826), then surface integral + update (ADERDGSolver.cpp:2100-2170). */
+static long ncells_of(int dim, const int* n) {
+  return dim == 3 ? (long)n[0] * n[1] * n[2] : (long)n[0] * n[1];
+}
+
+/* dt of one cell: min over nodes of factor / sum_d(max|lambda_d|/dx_d) with
+ * factor = CFL*PNPM[N] (policy 0, the reference rule) or CFL/(2N+1)
+ * (policy 1). */
+static double cell_dt(int dim, int order, int planar, const double* luh,
+                      const double* dx, int policy, double cfl) {
+  const int B = order + 1;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const double factor = policy == 0 ? cfl * exa_pnpm[order] : cfl / (2 * order + 1);
+  double dt = DBL_MAX;
+  for (int s = 0; s < nn; s++) {
+    double den = 0.0;
+    for (int d = 0; d < dim; d++) {
+      double lam[5];
+      orc_euler_eigenvalues(planar, luh + s * 5, d, lam);
+      double mx = 0.0;
+      for (int v = 0; v < 5; v++) mx = fabs(lam[v]) > mx ? fabs(lam[v]) : mx;
+      den += mx / dx[d];
+    }
+    const double c = factor / den;
+    dt = c < dt ? c : dt;
+  }
+  return dt;
+}
+
+double orc_aderdg_grid_dt(int dim, int order, int planar, const int* n,
+                          const double* dx, const double* luh, int dt_policy,
+                          double cfl) {
+  const int B = order + 1;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const long nc = ncells_of(dim, n);
+  double dt = DBL_MAX;
+  for (long c = 0; c < nc; c++) {
+    const double d = cell_dt(dim, order, planar, luh + c * nn * 5, dx, dt_policy, cfl);
+    dt = d < dt ? d : dt;
+  }
+  return dt;
+}
+
+double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
+                            const double* dx, double* luh, int dt_policy,
+                            double cfl, double dt_fixed, int* iters,
+                            int nthreads) {
+  const int B = order + 1, V = 5;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const int nst = nn * B;
+  const int nfn = dim == 3 ? B * B : B;
+  const long nc = ncells_of(dim, n);
+  double dt;
+  if (dt_policy == 2) dt = dt_fixed;
+  else dt = orc_aderdg_grid_dt(dim, order, planar, n, dx, luh, dt_policy, cfl);
+  double* lduh = (double*)malloc(sizeof(double) * nc * nn * V);
+  double* qb = (double*)malloc(sizeof(double) * nc * 2 * dim * nfn * V);
+  double* fb = (double*)malloc(sizeof(double) * nc * 2 * dim * nfn * V);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel
+  {
+    double* lQi = (double*)malloc(sizeof(double) * nst * V);
+    double* lQo = (double*)malloc(sizeof(double) * nst * V);
+    double* rhs = (double*)malloc(sizeof(double) * nst * V);
+    double* lFi = (double*)malloc(sizeof(double) * nst * (dim + 1) * V);
+    double* lQhi = (double*)malloc(sizeof(double) * nn * V);
+    double* lFhi = (double*)malloc(sizeof(double) * nn * (dim + 1) * V);
+#pragma omp for schedule(dynamic, 16)
+    for (long c = 0; c < nc; c++) {
+      int it = orc_stp_nonlinear(dim, order, V, 0, planar, qb + c * 2 * dim * nfn * V,
+                                 fb + c * 2 * dim * nfn * V, lQi, lQo, rhs, lFi, lQhi,
+                                 lFhi, luh + c * nn * V, dx, dt);
+      if (iters) iters[c] = it;
+      orc_volume_integral(dim, order, V, 0, lduh + c * nn * V, lFhi, dx);
+    }
+    free(lQi); free(lQo); free(rhs); free(lFi); free(lQhi); free(lFhi);
+  }
+  /* faces: for each cell and direction, the face towards the +d neighbour */
+  const int fs = nfn * V;
+  for (int d = 0; d < dim; d++) {
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nc; c++) {
+      int cx = (int)(c % n[0]), cy = (int)((c / n[0]) % n[1]);
+      int cz = dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0;
+      int r[3] = {cx, cy, cz};
+      r[d] = (r[d] + 1) % n[d];
+      long cr = dim == 3 ? ((long)r[2] * n[1] + r[1]) * n[0] + r[0]
+                         : (long)r[1] * n[0] + r[0];
+      orc_riemann(dim, order, V, 0, planar,
+                  fb + (c * 2 * dim + 2 * d + 1) * fs, fb + (cr * 2 * dim + 2 * d) * fs,
+                  qb + (c * 2 * dim + 2 * d + 1) * fs, qb + (cr * 2 * dim + 2 * d) * fs, d);
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < nc; c++) {
+    orc_surface_integral(dim, order, V, lduh + c * nn * V, fb + c * 2 * dim * fs, dx);
+    orc_solution_update(dim, order, V, 0, luh + c * nn * V, lduh + c * nn * V, dt);
+  }
+  free(lduh); free(qb); free(fb);
+  return dt;
+}
+
+/* ------------------------------------------------------------------ */
+/* Counter-based noise: splitmix64 of (seed, index). */
+double orc_noise_u01(unsigned long long seed, unsigned long long idx) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (idx + 1ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+static void prim_to_cons(double rho, double u, double v, double w, double p, double* Q) {
+  Q[0] = rho;
+  Q[1] = rho * u;
+  Q[2] = rho * v;
+  Q[3] = rho * w;
+  Q[4] = p / (GAMMA - 1) + 0.5 * rho * (u * u + v * v + w * w);
+}
+
+/* Point-wise initial state (the analogue of the user's adjustPointSolution,
+ * kernels/aderdg/generic/c/3d/solutionAdjustment.cpph:18-52). */
+static void ic_point(int kind, double param, double x, double y, double noise,
+                     double* Q) {
+  const double pi = 3.14159265358979323846;
+  if (kind == 0) {
+    /* isentropic vortex (Shu), centre (0.5,0.5), length scale 0.1 */
+    const double eps = param, R = 0.1;
+    const double xb = (x - 0.5) / R, yb = (y - 0.5) / R;
+    const double r2 = xb * xb + yb * yb;
+    const double e = exp(0.5 * (1.0 - r2));
+    const double u = 1.0 - eps / (2 * pi) * yb * e;
+    const double v = 1.0 + eps / (2 * pi) * xb * e;
+    const double T = 1.0 - (GAMMA - 1) * eps * eps / (8 * GAMMA * pi * pi) * e * e;
+    const double rho = pow(T, 1.0 / (GAMMA - 1));
+    const double p = rho * T;
+    prim_to_cons(rho * (1.0 + noise), u, v, 0.0, p, Q);
+  } else {
+    const double rho = 1.0 + param * sin(2 * pi * (x + y));
+    prim_to_cons(rho * (1.0 + noise), 1.0, 1.0, 0.0, 1.0, Q);
+  }
+}
+
+void orc_aderdg_grid_ic(int dim, int order, const int* n, const double* dx,
+                        double* luh, int kind, double param,
+                        unsigned long long seed, double noise_amp) {
+  const int B = order + 1;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const long nc = ncells_of(dim, n);
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < nc; c++) {
+    const int cx = (int)(c % n[0]), cy = (int)((c / n[0]) % n[1]);
+    for (int s = 0; s < nn; s++) {
+      const int ix = s % B, iy = (s / B) % B;
+      const double x = (cx + exa_gl_nodes[order][ix]) * dx[0];
+      const double y = (cy + exa_gl_nodes[order][iy]) * dx[1];
+      const unsigned long long g = (unsigned long long)c * nn + s;
+      const double nz = noise_amp != 0.0 ? noise_amp * (2.0 * orc_noise_u01(seed, g) - 1.0) : 0.0;
+      ic_point(kind, param, x, y, nz, luh + (c * nn + s) * 5);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* FV Rusanov: kernels/finitevolumes/riemannsolvers/c/rusanov.cpph:24-83 */
+double orc_rusanov(int dim, int nvar, int npar, int planar, double* fL,
+                   double* fR, const double* qL, const double* qR, int d) {
+  (void)npar;
+  double sL[5], sR[5];
+  orc_euler_eigenvalues(planar, qL, d, sL);
+  orc_euler_eigenvalues(planar, qR, d, sR);
+  double smax = -1.0;
+  for (int i = 0; i < nvar; i++) smax = fabs(sL[i]) > smax ? fabs(sL[i]) : smax;
+  for (int i = 0; i < nvar; i++) smax = fabs(sR[i]) > smax ? fabs(sR[i]) : smax;
+  double FL[15], FR[15];
+  orc_euler_flux(dim, planar, qL, FL);
+  orc_euler_flux(dim, planar, qR, FR);
+  for (int i = 0; i < nvar; i++) {
+    double f = 0.5 * smax * (qL[i] - qR[i]);
+    f += 0.5 * (FL[5 * d + i] + FR[5 * d + i]);
+    fL[i] = f;
+    fR[i] = f;
+  }
+  return smax;
+}
+
+/* FV Godunov 2D: kernels/finitevolumes/godunov/c/2d/godunov.cpph:33-120 */
+double orc_fv_godunov_2d(int P, int g, int V, int npar, int planar,
+                         double* luh_new, const double* luh, const double* dx,
+                         double dt) {
+  const int D = V + npar, S = P + 2 * g, pb = g, pe = g + P;
+  const double h[2] = {dx[0] / P, dx[1] / P};
+  const double cfl = 0.9; /* AbstractGenericFiniteVolumesSolverHeader.template:34 */
+#define IX(j, k, l) ((((long)(j)) * S + (k)) * D + (l))
+  double fL[5], fR[5], dtmax = DBL_MAX;
+  for (int j = pb; j < pe; j++)
+    for (int k = pb - 1; k < pe; k++) {
+      const double s = orc_rusanov(2, V, npar, planar, fL, fR, luh + IX(j, k, 0), luh + IX(j, k + 1, 0), 0);
+      const double c = cfl / 2 * h[0] / s;
+      dtmax = c < dtmax ? c : dtmax;
+      for (int l = 0; l < V; l++) {
+        luh_new[IX(j, k, l)] -= dt / h[0] * fL[l];
+        luh_new[IX(j, k + 1, l)] += dt / h[0] * fR[l];
+      }
+    }
+  for (int j = pb - 1; j < pe; j++)
+    for (int k = pb; k < pe; k++) {
+      const double s = orc_rusanov(2, V, npar, planar, fL, fR, luh + IX(j, k, 0), luh + IX(j + 1, k, 0), 1);
+      const double c = cfl / 2 * h[1] / s;
+      dtmax = c < dtmax ? c : dtmax;
+      for (int l = 0; l < V; l++) {
+        luh_new[IX(j, k, l)] -= dt / h[1] * fL[l];
+        luh_new[IX(j + 1, k, l)] += dt / h[1] * fR[l];
+      }
+    }
+#undef IX
+  return dtmax;
+}
+
+/* minmod: kernels/finitevolumes/musclhancock/c/2d/musclhancock.cpph:27-40 */
+static double minmod(double a, double b) {
+  if (a * b < 0.0) return 0.0;
+  return fabs(a) < fabs(b) ? a : b;
+}
+
+/* FV MUSCL-Hancock 2D: kernels/finitevolumes/musclhancock/c/2d/
+ * musclhancock.cpph:50-240 (CFL 0.99 from musclhancock.h:29).  The ghost
+ * cells next to the patch are extrapolated but not half-step evolved
+ * (:132-170), exactly as in the reference. */
+double orc_fv_musclhancock_2d(int P, int g, int V, int npar, int planar,
+                              double* luh_new, const double* luh,
+                              const double* dx, double dt) {
+  const int D = V + npar, S = P + 2 * g, pb = g, pe = g + P;
+  const double h[2] = {dx[0] / P, dx[1] / P};
+  const double cfl = 0.99;
+  const long nv = (long)S * S * V;
+#define IX(j, k, l) ((((long)(j)) * S + (k)) * D + (l))
+#define IW(j, k, l) ((((long)(j)) * S + (k)) * V + (l))
+#define ISL(j, k, d, l) (((((long)(j)) * S + (k)) * 2 + (d)) * V + (l))
+  double* slope = (double*)calloc(nv * 2, sizeof(double));
+  double* wLx = (double*)calloc(nv, sizeof(double));
+  double* wRx = (double*)calloc(nv, sizeof(double));
+  double* wLy = (double*)calloc(nv, sizeof(double));
+  double* wRy = (double*)calloc(nv, sizeof(double));
+  double* slopet = (double*)calloc(nv, sizeof(double));
+  /* slopes :79-98 */
+  for (int j = pb; j < pe; j++)
+    for (int k = pb - 1; k < pe + 1; k++)
+      for (int l = 0; l < V; l++)
+        slope[ISL(j, k, 0, l)] = minmod(luh[IX(j, k + 1, l)] - luh[IX(j, k, l)],
+                                        luh[IX(j, k, l)] - luh[IX(j, k - 1, l)]) / h[0];
+  for (int j = pb - 1; j < pe + 1; j++)
+    for (int k = pb; k < pe; k++)
+      for (int l = 0; l < V; l++)
+        slope[ISL(j, k, 1, l)] = minmod(luh[IX(j + 1, k, l)] - luh[IX(j, k, l)],
+                                        luh[IX(j, k, l)] - luh[IX(j - 1, k, l)]) / h[1];
+  /* boundary extrapolation :100-124 */
+  for (int j = pb; j < pe; j++)
+    for (int k = pb - 1; k < pe + 1; k++)
+      for (int l = 0; l < V; l++) {
+        wLx[IW(j, k, l)] = luh[IX(j, k, l)] - 0.5 * h[0] * slope[ISL(j, k, 0, l)];
+        wRx[IW(j, k, l)] = luh[IX(j, k, l)] + 0.5 * h[0] * slope[ISL(j, k, 0, l)];
+      }
+  for (int j = pb - 1; j < pe + 1; j++)
+    for (int k = pb; k < pe; k++)
+      for (int l = 0; l < V; l++) {
+        wLy[IW(j, k, l)] = luh[IX(j, k, l)] - 0.5 * h[1] * slope[ISL(j, k, 1, l)];
+        wRy[IW(j, k, l)] = luh[IX(j, k, l)] + 0.5 * h[1] * slope[ISL(j, k, 1, l)];
+      }
+  /* half-step evolution of the interior cells :126-170 (no source) */
+  for (int j = pb; j < pe; j++)
+    for (int k = pb; k < pe; k++) {
+      double* Qt = slopet + IW(j, k, 0);
+      double F[10];
+      orc_euler_flux(2, planar, wLx + IW(j, k, 0), F);
+      for (int l = 0; l < V; l++) Qt[l] += F[l] / h[0];
+      orc_euler_flux(2, planar, wRx + IW(j, k, 0), F);
+      for (int l = 0; l < V; l++) Qt[l] -= F[l] / h[0];
+      orc_euler_flux(2, planar, wLy + IW(j, k, 0), F);
+      for (int l = 0; l < V; l++) Qt[l] += F[5 + l] / h[1];
+      orc_euler_flux(2, planar, wRy + IW(j, k, 0), F);
+      for (int l = 0; l < V; l++) Qt[l] -= F[5 + l] / h[1];
+      for (int l = 0; l < V; l++) {
+        wLx[IW(j, k, l)] += 0.5 * dt * Qt[l];
+        wRx[IW(j, k, l)] += 0.5 * dt * Qt[l];
+        wLy[IW(j, k, l)] += 0.5 * dt * Qt[l];
+        wRy[IW(j, k, l)] += 0.5 * dt * Qt[l];
+      }
+    }
+  /* Riemann problems :172-214 */
+  double fL[5], fR[5], dtmax = DBL_MAX;
+  for (int j = pb; j < pe; j++)
+    for (int k = pb - 1; k < pe; k++) {
+      const double s = orc_rusanov(2, V, 0, planar, fL, fR, wRx + IW(j, k, 0), wLx + IW(j, k + 1, 0), 0);
+      const double c = cfl / 2 * h[0] / s;
+      dtmax = c < dtmax ? c : dtmax;
+      for (int l = 0; l < V; l++) {
+        luh_new[IX(j, k, l)] -= dt / h[0] * fL[l];
+        luh_new[IX(j, k + 1, l)] += dt / h[0] * fR[l];
+      }
+    }
+  for (int j = pb - 1; j < pe; j++)
+    for (int k = pb; k < pe; k++) {
+      const double s = orc_rusanov(2, V, 0, planar, fL, fR, wRy + IW(j, k, 0), wLy + IW(j + 1, k, 0), 1);
+      const double c = cfl / 2 * h[1] / s;
+      dtmax = c < dtmax ? c : dtmax;
+      for (int l = 0; l < V; l++) {
+        luh_new[IX(j, k, l)] -= dt / h[1] * fL[l];
+        luh_new[IX(j + 1, k, l)] += dt / h[1] * fR[l];
+      }
+    }
+  free(slope); free(wLx); free(wRx); free(wLy); free(wRy); free(slopet);
+#undef IX
+#undef IW
+#undef ISL
+  return dtmax;
+}
+
+/* FV CFL: kernels/finitevolumes/commons/c/commons.cpph:26-67 */
+double orc_fv_stable_dt_2d(int P, int g, int V, int npar, int planar,
+                           const double* luh, const double* dx, double cfl) {
+  const int D = V + npar, S = P + 2 * g;
+  double dtmax = DBL_MAX;
+  for (int j = g; j < g + P; j++)
+    for (int k = g; k < g + P; k++) {
+      const double* q = luh + ((long)j * S + k) * D;
+      for (int d = 0; d < 2; d++) {
+        double lam[5], s = 0.0;
+        orc_euler_eigenvalues(planar, q, d, lam);
+        for (int v = 0; v < V; v++) s = fabs(lam[v]) > s ? fabs(lam[v]) : s;
+        const double c = cfl / 2 * (dx[d] / P) / s;
+        dtmax = c < dtmax ? c : dtmax;
+      }
+    }
+  return dtmax;
+}
+
+/* Periodic ghost layers of a single patch (stands in for the neighbour
+ * merging of commons.cpph:337-405 when the patch is its own neighbour). */
+void orc_fv_periodic_ghosts_2d(int P, int g, int D, double* luh) {
+  const int S = P + 2 * g;
+  for (int j = 0; j < S; j++)
+    for (int k = 0; k < S; k++) {
+      if (j >= g && j < g + P && k >= g && k < g + P) continue;
+      const int sj = g + ((j - g) % P + P) % P;
+      const int sk = g + ((k - g) % P + P) % P;
+      memcpy(luh + ((long)j * S + k) * D, luh + ((long)sj * S + sk) * D, sizeof(double) * D);
+    }
+}
+
+double orc_fv_patch_step_2d(int scheme, int P, int planar, double* luh,
+                            const double* dx, double dt_fixed,
+                            double* max_admissible_dt) {
+  const int g = scheme == 0 ? 1 : 2, V = 5, S = P + 2 * g;
+  orc_fv_periodic_ghosts_2d(P, g, V, luh);
+  const double dt = dt_fixed > 0 ? dt_fixed : orc_fv_stable_dt_2d(P, g, V, 0, planar, luh, dx, 0.9);
+  double* old = (double*)malloc(sizeof(double) * S * S * V);
+  memcpy(old, luh, sizeof(double) * S * S * V);
+  double adm;
+  if (scheme == 0) adm = orc_fv_godunov_2d(P, g, V, 0, planar, luh, old, dx, dt);
+  else adm = orc_fv_musclhancock_2d(P, g, V, 0, planar, luh, old, dx, dt);
+  if (max_admissible_dt) *max_admissible_dt = adm;
+  free(old);
+  return dt;
+}

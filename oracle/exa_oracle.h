@@ -1,0 +1,104 @@
+/*
+ * CPU oracle -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, FP64 restatement of ExaHyPE's generic kernels for the
+ * ADER-DG / finite-volume cell-update path, used by the test suite, the
+ * smoke check and the CPU-baseline leg of the benchmark as the checker for
+ * the CUDA library.  It is never linked into, loaded by or called from the
+ * product library (libexahype_b200.so).
+ *
+ * Parity is pinned two ways: against the reference's golden vectors
+ * (exahype/tests/kernels/testdata/generic_euler_testdata.cpp, extracted to
+ * tests/golden/) and against the reference's own generic kernels compiled
+ * from its sources into oracle/_ref (oracle/Makefile).
+ *
+ * All arrays use the reference's row-major layouts (ExaHyPE/kernels/
+ * KernelUtils.h:243-320 idx2..idx6), slowest index first:
+ *   luh     [z][y][x][nData]            (2D: [y][x][nData])
+ *   lQi     [z][y][x][t][nData]
+ *   lFi     [t][z][y][x][dim+1][nVar]
+ *   lQhi    [z][y][x][nData]
+ *   lFhi    (dim+1) blocks of B^dim*nVar: x [z][y][x], y [z][x][y],
+ *           z [y][x][z], source [z][y][x]
+ *   lQhbnd  [2*dim][B][B][nData],  lFhbnd [2*dim][B][B][nVar]
+ *   lduh    [z][y][x][nVar]
+ */
+#ifndef EXA_ORACLE_H
+#define EXA_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* PDE selector: 0 = compressible Euler with all three momenta in the
+ * pressure (ExaHyPE/exahype/tests/kernels/c/GenericEulerKernelTest3D.cpp:26-82,
+ * Demonstrators/EulerFV/MyEulerSolver.cpp:58-98); 1 = the "2.5D" planar
+ * variant whose pressure only uses the in-plane momenta
+ * (GenericEulerKernelTest2D.cpp:28-79). */
+void orc_euler_flux(int dim, int planar, const double* Q, double* F);
+void orc_euler_eigenvalues(int planar, const double* Q, int d, double* lambda);
+
+/* ---- ADER-DG, one cell, reference argument semantics ---- */
+int orc_stp_nonlinear(int dim, int order, int nvar, int npar, int planar,
+                      double* lQhbnd, double* lFhbnd,
+                      double* lQi, double* lQi_old, double* rhs, double* lFi,
+                      double* lQhi, double* lFhi,
+                      const double* luh, const double* dx, double dt);
+void orc_volume_integral(int dim, int order, int nvar, int use_source,
+                         double* lduh, const double* lFhi, const double* dx);
+void orc_surface_integral(int dim, int order, int nvar,
+                          double* lduh, const double* lFhbnd, const double* dx);
+void orc_riemann(int dim, int order, int nvar, int npar, int planar,
+                 double* FL, double* FR, const double* QL, const double* QR,
+                 int direction);
+void orc_solution_update(int dim, int order, int nvar, int npar,
+                         double* luh, const double* lduh, double dt);
+double orc_stable_dt(int dim, int order, int nvar, int npar, int planar,
+                     const double* luh, const double* dx, double cfl);
+
+/* ---- ADER-DG uniform periodic grid (n[0] x n[1] (x n[2]) cells) ---- */
+/* dt_policy: 0 = reference PNPM rule, 1 = CFL/(2N+1), 2 = fixed dt_fixed */
+double orc_aderdg_grid_dt(int dim, int order, int planar, const int* n,
+                          const double* dx, const double* luh, int dt_policy,
+                          double cfl);
+/* One full step in the reference's non-fused order.  luh is updated in
+ * place; iters (optional, one int per cell) receives Picard iterations.
+ * Returns the dt used. */
+double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
+                            const double* dx, double* luh, int dt_policy,
+                            double cfl, double dt_fixed, int* iters,
+                            int nthreads);
+/* Nodal initial condition on the grid: isentropic vortex / sine wave with
+ * seeded density noise.  kind: 0 = isentropic vortex (u=v=1 background,
+ * strength eps), 1 = density sine rho=1+amp*sin(2 pi (x+y)), u=v=1, p=1. */
+void orc_aderdg_grid_ic(int dim, int order, const int* n, const double* dx,
+                        double* luh, int kind, double param,
+                        unsigned long long seed, double noise_amp);
+
+/* ---- finite volumes, 2D patch (reference godunov / musclhancock) ---- */
+double orc_rusanov(int dim, int nvar, int npar, int planar, double* fL,
+                   double* fR, const double* qL, const double* qR, int d);
+double orc_fv_godunov_2d(int patch, int ghost, int nvar, int npar, int planar,
+                         double* luh_new, const double* luh, const double* dx,
+                         double dt);
+double orc_fv_musclhancock_2d(int patch, int ghost, int nvar, int npar,
+                              int planar, double* luh_new, const double* luh,
+                              const double* dx, double dt);
+double orc_fv_stable_dt_2d(int patch, int ghost, int nvar, int npar,
+                           int planar, const double* luh, const double* dx,
+                           double cfl);
+void orc_fv_periodic_ghosts_2d(int patch, int ghost, int ndata, double* luh);
+/* scheme: 0 godunov (ghost 1), 1 musclhancock (ghost 2).  Fills the
+ * periodic ghosts, takes dt from the stable-dt rule (CFL 0.9) unless
+ * dt_fixed > 0, updates luh in place; returns dt. */
+double orc_fv_patch_step_2d(int scheme, int patch, int planar, double* luh,
+                            const double* dx, double dt_fixed,
+                            double* max_admissible_dt);
+
+/* counter-based noise shared with the device IC kernel */
+double orc_noise_u01(unsigned long long seed, unsigned long long idx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,348 @@
+/*
+ * Harness around the reference's own generic kernels -- TEST
+ * INFRASTRUCTURE ONLY.  Built by `make -C oracle ref` from the reference
+ * sources in place (nothing is copied into this repository) into
+ * oracle/_ref/libexa_ref{2d,3d}.so; used to pin the C oracle and as the
+ * timed CPU baseline ("kind": "reference").
+ *
+ * The solver type below plays the role the reference's unit tests give the
+ * test class itself (exahype/tests/kernels/c/GenericEulerKernelTest3D.cpp:
+ * 26-132): it supplies the PDE callbacks and the compile-time constants the
+ * kernel templates read.  The grid driver reproduces the non-fused step
+ * order of exahype/runners/Runner.cpp:1125-1160 on a uniform periodic grid.
+ */
+#include <vector>
+#include <set>
+#include <thread>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "kernels/aderdg/generic/Kernels.h"
+#include "kernels/finitevolumes/riemannsolvers/c/riemannsolvers.h"
+#include "kernels/finitevolumes/commons/c/commons.h"
+#include "kernels/finitevolumes/godunov/c/godunov.h"
+#include "kernels/finitevolumes/musclhancock/c/musclhancock.h"
+#include "kernels/GaussLegendreQuadrature.h"
+#include "kernels/DGMatrices.h"
+
+namespace {
+
+struct TablesInit {
+  TablesInit() {
+    std::set<int> orders;
+    for (int i = 0; i < 10; i++) orders.insert(i);
+    kernels::initGaussLegendreNodesAndWeights(orders);
+    kernels::initDGMatrices(orders);
+  }
+};
+TablesInit tables_init;
+
+constexpr double GAMMA_ = 1.4;
+
+/* Euler PDE.  3D: all momenta in the pressure; 2D: the kernel tests'
+ * planar form (GenericEulerKernelTest2D.cpp:28-79). */
+inline double pressure(const double* Q, double irho) {
+#if DIMENSIONS == 3
+  return (GAMMA_ - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3]) * irho);
+#else
+  return (GAMMA_ - 1) * (Q[4] - 0.5 * (Q[1] * Q[1] + Q[2] * Q[2]) * irho);
+#endif
+}
+
+template <int ORDER, int NPAR, int PATCH = 8, int GHOST = 1>
+struct Euler {
+  static constexpr int NumberOfVariables = 5;
+  static constexpr int NumberOfParameters = NPAR;
+  static constexpr int Order = ORDER;
+  static constexpr int PatchSize = PATCH;
+  static constexpr int GhostLayerWidth = GHOST;
+  static constexpr double CFL = 0.9;
+
+  void flux(const double* const Q, double** F) {
+    const double irho = 1.0 / Q[0];
+    const double p = pressure(Q, irho);
+    for (int d = 0; d < DIMENSIONS; d++) {
+      double* f = F[d];
+      f[0] = Q[d + 1];
+      f[1] = irho * Q[d + 1] * Q[1];
+      f[2] = irho * Q[d + 1] * Q[2];
+      f[3] = irho * Q[d + 1] * Q[3];
+      f[d + 1] += p;
+      f[4] = irho * Q[d + 1] * (Q[4] + p);
+    }
+  }
+  void eigenvalues(const double* const Q, const int d, double* lambda) {
+    const double irho = 1.0 / Q[0];
+    const double p = pressure(Q, irho);
+    const double un = Q[d + 1] * irho;
+    const double c = std::sqrt(GAMMA_ * p * irho);
+    lambda[0] = un - c; lambda[1] = un; lambda[2] = un; lambda[3] = un; lambda[4] = un + c;
+  }
+  void fusedSource(const double* const, const double* const, double* S) {
+    for (int i = 0; i < 5; i++) S[i] = 0.0;
+  }
+  void algebraicSource(const double* const, double* S) {
+    for (int i = 0; i < 5; i++) S[i] = 0.0;
+  }
+  void nonConservativeProduct(const double* const, const double* const, double* B) {
+    for (int i = 0; i < 5; i++) B[i] = 0.0;
+  }
+  void coefficientMatrix(const double* const, const int, double* Bn) {
+    for (int i = 0; i < 25; i++) Bn[i] = 0.0;
+  }
+  void pointSource(const double* const, const double* const, const double, const double, double*, int) {}
+  void boundaryValues(const double* const, const double, const double, const int, const int,
+                      const double* const, const double* const, double*, double*) {}
+  double riemannSolver(double* fL, double* fR, const double* qL, const double* qR, int d) {
+    return kernels::finitevolumes::riemannsolvers::c::rusanov<false, true>(*this, fL, fR, qL, qR, d);
+  }
+};
+
+typedef tarch::la::Vector<DIMENSIONS, double> Vec;
+
+Vec vec(const double* dx) {
+#if DIMENSIONS == 3
+  return Vec(dx[0], dx[1], dx[2]);
+#else
+  return Vec(dx[0], dx[1]);
+#endif
+}
+
+constexpr int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+template <int N, int P>
+struct DG {
+  typedef Euler<N, P> S;
+  static constexpr int B = N + 1, V = 5, D = V + P;
+  static constexpr int NN = ipow(B, DIMENSIONS);
+  static constexpr int NF = ipow(B, DIMENSIONS - 1);
+
+  struct Temps {
+    std::vector<double> st, stf, qhi, fhi;
+    double* stp[4];
+    double* stfp[2];
+    Temps() : st(4 * NN * B * D), stf(2 * NN * B * (DIMENSIONS + 1) * V), qhi(NN * D),
+              fhi(NN * (DIMENSIONS + 1) * V) {
+      for (int i = 0; i < 4; i++) stp[i] = st.data() + i * NN * B * D;
+      for (int i = 0; i < 2; i++) stfp[i] = stf.data() + i * NN * B * (DIMENSIONS + 1) * V;
+    }
+  };
+
+  static void stp(const double* luh, double* lQi, double* lQhi, double* lFhi, double* qb,
+                  double* fb, const double* dx, double dt, Temps& t) {
+    S s;
+    double tmpvec[5];
+    kernels::aderdg::generic::c::spaceTimePredictorNonlinear<false, true, false, S>(
+        s, qb, fb, t.stp, t.stfp, t.qhi.data(), t.fhi.data(), tmpvec, luh, vec(dx), dt);
+    if (lQi) std::memcpy(lQi, t.stp[0], sizeof(double) * NN * B * D);
+    if (lQhi) std::memcpy(lQhi, t.qhi.data(), sizeof(double) * NN * D);
+    if (lFhi) std::memcpy(lFhi, t.fhi.data(), sizeof(double) * NN * (DIMENSIONS + 1) * V);
+  }
+  static void vi(double* lduh, const double* lFhi, const double* dx) {
+    kernels::aderdg::generic::c::volumeIntegralNonlinear<false, true, V, B>(lduh, lFhi, vec(dx));
+  }
+  static void si(double* lduh, const double* lFhbnd, const double* dx) {
+    kernels::aderdg::generic::c::surfaceIntegralNonlinear<V, B>(lduh, lFhbnd, vec(dx));
+  }
+  static void riemann(double* FL, double* FR, const double* QL, const double* QR, int d) {
+    S s;
+    kernels::aderdg::generic::c::riemannSolverNonlinear<false, S>(s, FL, FR, QL, QR, nullptr,
+                                                                   nullptr, nullptr, 0.0, d);
+  }
+  static void update(double* luh, const double* lduh, double dt) {
+    S s;
+    kernels::aderdg::generic::c::solutionUpdate<S>(s, luh, lduh, dt);
+  }
+  static double dt(const double* luh, const double* dx) {
+    S s;
+    double lam[5];
+    return kernels::aderdg::generic::c::stableTimeStepSize<S>(s, luh, lam, vec(dx));
+  }
+  /* one step on a uniform periodic grid (reference non-fused order) */
+  static double grid_step(const int* n, const double* dx, double* luh, int policy,
+                          double dt_fixed, int nthreads) {
+    static_assert(P == 0, "grid step without parameters");
+    const long nc = DIMENSIONS == 3 ? (long)n[0] * n[1] * n[2] : (long)n[0] * n[1];
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+    double dtv = dt_fixed;
+    if (policy != 2) {
+      double m = DBL_MAX;
+#pragma omp parallel for reduction(min : m)
+      for (long c = 0; c < nc; c++) {
+        double d = dt(luh + c * NN * D, dx);
+        if (policy == 1) d = d / kernels_pnpm() / (2 * N + 1);
+        m = d < m ? d : m;
+      }
+      dtv = m;
+    }
+    std::vector<double> lduh(nc * NN * V), qb(nc * 2 * DIMENSIONS * NF * D),
+        fb(nc * 2 * DIMENSIONS * NF * V);
+#pragma omp parallel
+    {
+      Temps t;
+#pragma omp for schedule(dynamic, 16)
+      for (long c = 0; c < nc; c++) {
+        stp(luh + c * NN * D, nullptr, nullptr, nullptr, qb.data() + c * 2 * DIMENSIONS * NF * D,
+            fb.data() + c * 2 * DIMENSIONS * NF * V, dx, dtv, t);
+        vi(lduh.data() + c * NN * V, t.fhi.data(), dx);
+      }
+    }
+    for (int d = 0; d < DIMENSIONS; d++) {
+#pragma omp parallel for
+      for (long c = 0; c < nc; c++) {
+        int r[3] = {(int)(c % n[0]), (int)((c / n[0]) % n[1]),
+                    DIMENSIONS == 3 ? (int)(c / ((long)n[0] * n[1])) : 0};
+        r[d] = (r[d] + 1) % n[d];
+        long cr = DIMENSIONS == 3 ? ((long)r[2] * n[1] + r[1]) * n[0] + r[0]
+                                  : (long)r[1] * n[0] + r[0];
+        riemann(fb.data() + (c * 2 * DIMENSIONS + 2 * d + 1) * NF * V,
+                fb.data() + (cr * 2 * DIMENSIONS + 2 * d) * NF * V,
+                qb.data() + (c * 2 * DIMENSIONS + 2 * d + 1) * NF * D,
+                qb.data() + (cr * 2 * DIMENSIONS + 2 * d) * NF * D, d);
+      }
+    }
+#pragma omp parallel for
+    for (long c = 0; c < nc; c++) {
+      si(lduh.data() + c * NN * V, fb.data() + c * 2 * DIMENSIONS * NF * V, dx);
+      update(luh + c * NN * D, lduh.data() + c * NN * V, dtv);
+    }
+    return dtv;
+  }
+  static double kernels_pnpm() {
+    static const double pnpm[10] = {1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015};
+    return pnpm[N];
+  }
+};
+
+#define EXA_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
+
+}  // namespace
+
+#if DIMENSIONS == 2
+/* One step of a single periodic FV patch with the reference's godunov
+ * (scheme 0, ghost 1) or musclhancock (scheme 1, ghost 2) kernel; the
+ * patch size is a template constant of the reference, so a fixed set is
+ * instantiated.  Runs on a thread with a 1 GiB stack because the
+ * reference keeps its MUSCL work arrays on the stack
+ * (musclhancock/c/2d/musclhancock.cpph:75,102-105). */
+template <int PS, int G>
+static double fv_step_t(int scheme, double* luh, const double* dx, double dt_fixed,
+                        double* adm) {
+  typedef Euler<0, 0, PS, G> S;
+  const int SZ = PS + 2 * G;
+  S s;
+  /* periodic ghosts */
+  for (int j = 0; j < SZ; j++)
+    for (int k = 0; k < SZ; k++) {
+      if (j >= G && j < G + PS && k >= G && k < G + PS) continue;
+      int sj = G + ((j - G) % PS + PS) % PS, sk = G + ((k - G) % PS + PS) % PS;
+      std::memcpy(luh + ((long)j * SZ + k) * 5, luh + ((long)sj * SZ + sk) * 5, 5 * sizeof(double));
+    }
+  double lam[5];
+  double dt = dt_fixed > 0 ? dt_fixed
+                           : kernels::finitevolumes::commons::c::stableTimeStepSize<S>(s, luh, lam, vec(dx));
+  std::vector<double> old(luh, luh + (long)SZ * SZ * 5);
+  double a;
+  if (scheme == 0)
+    a = kernels::finitevolumes::godunov::c::solutionUpdate<false, false, true, S>(
+        s, luh, old.data(), nullptr, nullptr, vec(dx), dt);
+  else
+    a = kernels::finitevolumes::musclhancock::c::solutionUpdate<false, false, true, S>(
+        s, luh, old.data(), nullptr, nullptr, vec(dx), dt);
+  if (adm) *adm = a;
+  return dt;
+}
+
+#endif
+
+extern "C" {
+
+int ref_stp(int order, int npar, const double* luh, double* lQi, double* lQhi, double* lFhi,
+            double* qb, double* fb, const double* dx, double dt) {
+  if (npar == 1 && order == 3) {
+    DG<3, 1>::Temps t;
+    DG<3, 1>::stp(luh, lQi, lQhi, lFhi, qb, fb, dx, dt, t);
+    return 0;
+  }
+  if (npar != 0) return -1;
+#define CASE(N) case N: { DG<N, 0>::Temps t; DG<N, 0>::stp(luh, lQi, lQhi, lFhi, qb, fb, dx, dt, t); return 0; }
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+int ref_volume_integral(int order, double* lduh, const double* lFhi, const double* dx) {
+#define CASE(N) case N: DG<N, 0>::vi(lduh, lFhi, dx); return 0;
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+int ref_surface_integral(int order, double* lduh, const double* lFhbnd, const double* dx) {
+#define CASE(N) case N: DG<N, 0>::si(lduh, lFhbnd, dx); return 0;
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+int ref_riemann(int order, int npar, double* FL, double* FR, const double* QL, const double* QR,
+                int d) {
+  if (npar == 1 && order == 3) { DG<3, 1>::riemann(FL, FR, QL, QR, d); return 0; }
+  if (npar != 0) return -1;
+#define CASE(N) case N: DG<N, 0>::riemann(FL, FR, QL, QR, d); return 0;
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+int ref_solution_update(int order, int npar, double* luh, const double* lduh, double dt) {
+  if (npar == 1 && order == 3) { DG<3, 1>::update(luh, lduh, dt); return 0; }
+  if (npar != 0) return -1;
+#define CASE(N) case N: DG<N, 0>::update(luh, lduh, dt); return 0;
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+double ref_stable_dt(int order, int npar, const double* luh, const double* dx) {
+  if (npar == 1 && order == 3) return DG<3, 1>::dt(luh, dx);
+  if (npar != 0) return -1;
+#define CASE(N) case N: return DG<N, 0>::dt(luh, dx);
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+double ref_grid_step(int order, const int* n, const double* dx, double* luh, int policy,
+                     double dt_fixed, int nthreads) {
+#define CASE(N) case N: return DG<N, 0>::grid_step(n, dx, luh, policy, dt_fixed, nthreads);
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+#if DIMENSIONS == 2
+double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double dt_fixed,
+                   double* adm) {
+  double r = -1;
+  std::thread th([&]() {
+#define PCASE(P)                                                        \
+  case P:                                                               \
+    r = scheme == 0 ? fv_step_t<P, 1>(0, luh, dx, dt_fixed, adm)        \
+                    : fv_step_t<P, 2>(1, luh, dx, dt_fixed, adm);       \
+    break;
+    switch (patch) { PCASE(8) PCASE(16) PCASE(32) PCASE(64) PCASE(128) }
+#undef PCASE
+  });
+  th.join();
+  return r;
+}
+#endif
+
+}  // extern "C"

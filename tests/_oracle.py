@@ -1,0 +1,146 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so) and, when it was
+built, of the reference's own generic kernels (oracle/_ref/libexa_ref*.so).
+
+Test infrastructure only: the product library never loads these.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, 'oracle')
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags='C_CONTIGUOUS')
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags='C_CONTIGUOUS')
+
+
+def _ensure_built():
+    so = os.path.join(ORACLE_DIR, 'liboracle.so')
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ('exa_oracle.c', 'exa_oracle.h')]
+    if not os.path.exists(so) or any(os.path.getmtime(s) > os.path.getmtime(so) for s in srcs):
+        subprocess.check_call(['make', '-s', '-C', ORACLE_DIR, 'liboracle.so'])
+    return so
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    L = C.CDLL(_ensure_built())
+    d, i = C.c_double, C.c_int
+    L.orc_euler_flux.argtypes = [i, i, _dp, _dp]
+    L.orc_euler_eigenvalues.argtypes = [i, _dp, i, _dp]
+    L.orc_stp_nonlinear.restype = i
+    L.orc_stp_nonlinear.argtypes = [i, i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d]
+    L.orc_volume_integral.argtypes = [i, i, i, i, _dp, _dp, _dp]
+    L.orc_surface_integral.argtypes = [i, i, i, _dp, _dp, _dp]
+    L.orc_riemann.argtypes = [i, i, i, i, i, _dp, _dp, _dp, _dp, i]
+    L.orc_solution_update.argtypes = [i, i, i, i, _dp, _dp, d]
+    L.orc_stable_dt.restype = d
+    L.orc_stable_dt.argtypes = [i, i, i, i, i, _dp, _dp, d]
+    L.orc_aderdg_grid_dt.restype = d
+    L.orc_aderdg_grid_dt.argtypes = [i, i, i, _ip, _dp, _dp, i, d]
+    L.orc_aderdg_grid_step.restype = d
+    L.orc_aderdg_grid_step.argtypes = [i, i, i, _ip, _dp, _dp, i, d, d, C.c_void_p, i]
+    L.orc_aderdg_grid_ic.argtypes = [i, i, _ip, _dp, _dp, i, d, C.c_ulonglong, d]
+    L.orc_rusanov.restype = d
+    L.orc_rusanov.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, i]
+    L.orc_fv_godunov_2d.restype = d
+    L.orc_fv_godunov_2d.argtypes = [i, i, i, i, i, _dp, _dp, _dp, d]
+    L.orc_fv_musclhancock_2d.restype = d
+    L.orc_fv_musclhancock_2d.argtypes = [i, i, i, i, i, _dp, _dp, _dp, d]
+    L.orc_fv_stable_dt_2d.restype = d
+    L.orc_fv_stable_dt_2d.argtypes = [i, i, i, i, i, _dp, _dp, d]
+    L.orc_fv_periodic_ghosts_2d.argtypes = [i, i, i, _dp]
+    L.orc_fv_patch_step_2d.restype = d
+    L.orc_fv_patch_step_2d.argtypes = [i, i, i, _dp, _dp, d, C.c_void_p]
+    L.orc_noise_u01.restype = d
+    L.orc_noise_u01.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    _lib = L
+    return L
+
+
+# ---------------------------------------------------------------- helpers
+def sizes(dim, order, nvar=5, npar=0):
+    B = order + 1
+    nd = nvar + npar
+    n_node = B ** dim
+    return dict(B=B, nData=nd, luh=n_node * nd, lduh=n_node * nvar,
+                lQi=n_node * B * nd, lFi=n_node * B * (dim + 1) * nvar,
+                rhs=n_node * B * nvar, lQhi=n_node * nd,
+                lFhi=n_node * (dim + 1) * nvar,
+                qbnd=2 * dim * B ** (dim - 1) * nd, fbnd=2 * dim * B ** (dim - 1) * nvar)
+
+
+def stp(dim, order, luh, dx, dt, nvar=5, npar=0, planar=0):
+    s = sizes(dim, order, nvar, npar)
+    out = {k: np.zeros(s[k]) for k in ('lQi', 'lFi', 'lQhi', 'lFhi')}
+    qb, fb = np.zeros(s['qbnd']), np.zeros(s['fbnd'])
+    old, rhs = np.zeros(s['lQi']), np.zeros(s['rhs'])
+    it = lib().orc_stp_nonlinear(dim, order, nvar, npar, planar, qb, fb, out['lQi'], old, rhs,
+                                 out['lFi'], out['lQhi'], out['lFhi'],
+                                 np.ascontiguousarray(luh, dtype=np.float64),
+                                 np.asarray(dx, dtype=np.float64), dt)
+    out.update(lQhbnd=qb, lFhbnd=fb, iters=it)
+    return out
+
+
+def grid_ic(dim, order, n, kind=0, param=5.0, seed=1234, noise=0.0, dx=None):
+    n = np.asarray(n, dtype=np.int32)
+    if dx is None:
+        dx = 1.0 / n.astype(np.float64)
+    B = order + 1
+    luh = np.zeros(int(np.prod(n)) * B ** dim * 5)
+    lib().orc_aderdg_grid_ic(dim, order, n, np.asarray(dx, dtype=np.float64), luh, kind, param,
+                             seed, noise)
+    return luh
+
+
+def grid_step(dim, order, n, luh, dt_policy=0, cfl=0.9, dt_fixed=0.0, planar=0,
+              nthreads=0, dx=None):
+    n = np.asarray(n, dtype=np.int32)
+    if dx is None:
+        dx = 1.0 / n.astype(np.float64)
+    iters = np.zeros(int(np.prod(n)), dtype=np.int32)
+    dt = lib().orc_aderdg_grid_step(dim, order, planar, n, np.asarray(dx, dtype=np.float64), luh,
+                                    dt_policy, cfl, dt_fixed, iters.ctypes.data, nthreads)
+    return dt, iters
+
+
+# ---------------------------------------------------------------- reference
+_ref = {}
+
+
+def ref_lib(dim):
+    """The reference's own kernels (oracle/_ref), or None if not built."""
+    if dim in _ref:
+        return _ref[dim]
+    so = os.path.join(ORACLE_DIR, '_ref', 'libexa_ref%dd.so' % dim)
+    L = None
+    if os.path.exists(so):
+        L = C.CDLL(so)
+        d, i = C.c_double, C.c_int
+        L.ref_stp.restype = i
+        L.ref_stp.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d]
+        L.ref_volume_integral.restype = i
+        L.ref_volume_integral.argtypes = [i, _dp, _dp, _dp]
+        L.ref_surface_integral.restype = i
+        L.ref_surface_integral.argtypes = [i, _dp, _dp, _dp]
+        L.ref_riemann.restype = i
+        L.ref_riemann.argtypes = [i, i, _dp, _dp, _dp, _dp, i]
+        L.ref_solution_update.restype = i
+        L.ref_solution_update.argtypes = [i, i, _dp, _dp, d]
+        L.ref_stable_dt.restype = d
+        L.ref_stable_dt.argtypes = [i, i, _dp, _dp]
+        L.ref_grid_step.restype = d
+        L.ref_grid_step.argtypes = [i, _ip, _dp, _dp, i, d, i]
+        if dim == 2:
+            L.ref_fv_step.restype = d
+            L.ref_fv_step.argtypes = [i, i, _dp, _dp, d, C.c_void_p]
+    _ref[dim] = L
+    return L
