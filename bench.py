@@ -1,0 +1,403 @@
+#!/usr/bin/env python3
+"""Benchmark of the ADER-DG cell-update path.
+
+Workload (one GPU): 3D compressible Euler, ADER-DG order N=4 (125 nodes per
+cell), 81^3 uniform periodic cells on the unit cube, FP64 plain path,
+isentropic vortex + seeded uniform density noise of amplitude 1e-3.  A
+"step" is one full time step of the whole grid (dt reduction, space-time
+predictor + volume integral, Riemann solves, surface integral, update).
+Metric: cell-updates/s (one cell advanced one step = 1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--n 81] [--order 4]
+
+N>1 runs one independent replica of the grid per GPU (weak scaling; the
+uniform grid has no cross-replica exchange), launched one process per GPU
+by torch.distributed.run; the timing is the max over ranks.
+
+--impl reference times the reference's own generic CPU kernels (compiled
+from its sources into oracle/_ref) on the host cores, each step a bounded
+sample of the same workload's cells.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Euler functor operation counts (exahype_b200/csrc/exa_device.cuh):
+C_FLUX = 31   # euler_flux, 3 directions
+C_EIG = 16    # euler_max_eig, one direction
+
+
+def flops_per_cell_update(dim, order, kbar, V=5):
+    """Algorithmic FLOP per cell-update (k = mean Picard iterations):
+    P_iter = d B^(d+1) V B 2 + B^(d+2) V 2 + B^(d+1) (c_F + 5V)
+    P_post = B^(d+1) V (d+2) 2 + 2d B^(d-1) V B 4 + d B^d V B 2 + d B^d V 6
+             + d B^(d-1) V 8 + B^d V 2 + B^d d (c_lambda + 3)
+    Returns (total, predictor share)."""
+    B, d = order + 1, dim
+    p_iter = d * B ** (d + 1) * V * B * 2 + B ** (d + 2) * V * 2 + B ** (d + 1) * (C_FLUX + 5 * V)
+    avg = B ** (d + 1) * V * (d + 2) * 2
+    extrap = 2 * d * B ** (d - 1) * V * B * 4
+    vi = d * B ** d * V * B * 2
+    post_corr = d * B ** d * V * 6 + d * B ** (d - 1) * V * 8 + B ** d * V * 2 + B ** d * d * (C_EIG + 3)
+    pred = kbar * p_iter + avg + extrap + vi
+    return pred + post_corr, pred
+
+
+def bytes_per_cell_update(dim, order, V=5):
+    """Algorithmic HBM bytes per cell-update: luh read+write, face Q/F
+    write + read (2 B^d V 8 + 2 (2d B^(d-1) V 8 2))."""
+    B, d = order + 1, dim
+    return 2 * B ** d * V * 8 + 2 * (2 * d * B ** (d - 1) * V * 8 * 2)
+
+
+def predictor_bytes_per_cell(dim, order, V=5):
+    """luh read, lduh write, lQhbnd + lFhbnd write."""
+    B, d = order + 1, dim
+    return 8 * (B ** d * V * 2 + 2 * 2 * d * B ** (d - 1) * V)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.index), '--query-gpu=' + self.Q, '--format=csv,noheader,nounits',
+                 '-lms', '200'], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() in ('active', '1'):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {'sm_mhz': float(np.median(sm)), 'sm_max_mhz': float(max(mx)), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), 'measured'
+    return {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0}, 'fallback'
+
+
+def ncu_traffic_per_cell():
+    """DRAM bytes per cell of k_predictor from the committed ncu summary."""
+    p = os.path.join(ROOT, 'profiles', 'k_predictor_3d_N4.md')
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith('traffic_bytes_per_cell:'):
+            try:
+                return float(line.split(':', 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_sample(order, n, state, dt, budget_s, steps=None):
+    """Times the reference's generic kernels (oracle/_ref) -- or the C oracle
+    if the reference build is absent -- on a bounded sample of the grid's
+    cells with all host threads.  Returns (cells/s, kind, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, 'tests'))
+    import _oracle as O
+    cores = os.cpu_count() or 1
+    B = order + 1
+    per = B ** 3 * 5
+    ncells = state.size // per
+    dx = np.full(3, 1.0 / n)
+    R = O.ref_lib(3)
+    if R is not None:
+        kind = 'reference'
+
+        def run(u, m):
+            R.ref_sample_step(order, m, dx, u, dt, cores)
+    else:
+        kind = 'port'
+
+        def run(u, m):
+            O.lib().orc_aderdg_sample_step(3, order, 0, m, dx, u, dt, cores)
+    m0 = min(ncells, 64 * cores)
+    u = np.ascontiguousarray(state[:m0 * per]).copy()
+    t0 = time.perf_counter()
+    run(u, m0)
+    t_cal = time.perf_counter() - t0
+    rate = m0 / max(t_cal, 1e-6)
+    nsteps = steps or 3
+    m = int(min(ncells, max(m0, rate * budget_s / nsteps)))
+    u = np.ascontiguousarray(state[:m * per]).copy()
+    times = []
+    for _ in range(nsteps):
+        t0 = time.perf_counter()
+        run(u, m)
+        times.append(time.perf_counter() - t0)
+    value = m * nsteps / sum(times)
+    sample = '%d of %d cells x %d steps (first cells of the %d^3 state, its dt)' % (m, ncells, nsteps, n)
+    return value, kind, cores, sample, times
+
+
+# ---------------------------------------------------------------- reference
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, 'tests'))
+    import _oracle as O
+    n, order = args.n, args.order
+    state = O.grid_ic(3, order, (n, n, n), kind=0, param=5.0, seed=args.seed, noise=1e-3)
+    dt = O.lib().orc_aderdg_grid_dt(3, order, 0, np.array([n, n, n], dtype=np.int32), np.full(3, 1.0 / n),
+                                    state, 0, 0.9)
+    cores = os.cpu_count() or 1
+    R = O.ref_lib(3)
+    kind = 'reference' if R is not None else 'port'
+    per = (order + 1) ** 3 * 5
+    ncells = state.size // per
+    dx = np.full(3, 1.0 / n)
+
+    def run(u, m):
+        if R is not None:
+            R.ref_sample_step(order, m, dx, u, dt, cores)
+        else:
+            O.lib().orc_aderdg_sample_step(3, order, 0, m, dx, u, dt, cores)
+    # size one step for ~2.5 s of work so K+W steps end within minutes
+    m0 = min(ncells, 64 * cores)
+    u = state[:m0 * per].copy()
+    t0 = time.perf_counter()
+    run(u, m0)
+    rate = m0 / max(time.perf_counter() - t0, 1e-6)
+    m = int(min(ncells, max(m0, rate * 2.5)))
+    u = state[:m * per].copy()
+    for _ in range(args.warmup):
+        run(u, m)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run(u, m)
+    t = time.perf_counter() - t0
+    value = m * args.steps / t
+    sample = '%d of %d cells per step (first cells of the %d^3 vortex state, its dt)' % (m, ncells, n)
+    line = {
+        'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'cell-updates/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+        'data': 'synthetic', 'config': config_dict(args, world),
+        'cpu_baseline': {'value': value, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind,
+                         'sample': sample},
+        'e2e': {'value': value, 'unit': 'cell-updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = '3D Euler ADER-DG N=4 cell-updates/s'
+
+
+def config_dict(args, world):
+    return {'workload': '3D Euler ADER-DG N=%d, %d^3 periodic cells, isentropic vortex + 1e-3 density noise'
+                        % (args.order, args.n),
+            'order': args.order, 'cells': args.n ** 3, 'nodes_per_cell': (args.order + 1) ** 3,
+            'precision': args.precision, 'dt_policy': 'CFL*PNPM[N], CFL=0.9',
+            'l2_flush': 'inputs larger than L2 (state + faces %.1f GB per GPU)' %
+                        (args.n ** 3 * (2 * 125 * 5 + 2 * 6 * 25 * 5) * 8 / 1e9 if args.order == 4 else 0),
+            'parallelism': 'replicas%d' % world}
+
+
+# ---------------------------------------------------------------- ours
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'mixed'])
+    ap.add_argument('--n', type=int, default=81)
+    ap.add_argument('--order', type=int, default=4)
+    ap.add_argument('--seed', type=int, default=2024)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=600))
+
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import exahype_b200 as E
+    from exahype_b200 import Timer
+    E.lib().exa_set_device(local)
+    n, order = args.n, args.order
+    prec = E.PREC_MIXED if args.precision == 'mixed' else E.PREC_FP64
+    grid = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
+    grid.init(kind=0, param=5.0, seed=args.seed + rank, noise=1e-3)
+    stream = grid.stream()
+
+    import ctypes as C
+    fp64_peak = C.c_double()
+    E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))
+    peaks, peak_src = measured_peaks()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    initial = grid.get_state()
+    grid.step(args.warmup)
+    st0 = grid.status()
+    grid.profile(True)
+    E.device.synchronize()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    timer = Timer()
+    l0 = E.launch_count()
+    timer.start(stream)
+    grid.step(args.steps)
+    timer.stop(stream)
+    ms = timer.elapsed_ms()
+    E.device.synchronize()
+    launches = E.launch_count() - l0
+    barrier()
+    clk = clocks.stop()
+    st1 = grid.status()
+    phases = grid.phase_times()
+    ms_max = max_over_ranks(ms)
+    ncells = grid.ncells
+    value = world * ncells * args.steps / (ms_max * 1e-3)
+    kbar = (st1['picard_iters'] - st0['picard_iters']) / (ncells * args.steps)
+    total_flop, pred_flop = flops_per_cell_update(3, order, kbar)
+    pred_ms = phases['predictor_ms'] / max(1, phases['steps'])
+    achieved_tf = pred_flop * ncells / (pred_ms * 1e-3) / 1e12
+    traffic_pc = ncu_traffic_per_cell()
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        from exahype_b200 import PinnedBuffer
+        pin = PinnedBuffer(grid.state_size)
+        pin.array[:] = initial
+        grid.profile(False)
+        barrier()
+        t2 = Timer()
+        t2.start(stream)
+        E._lib.call('exa_aderdg_grid_set_state', grid.h, pin.array.ctypes.data)
+        dts = []
+        for _ in range(args.steps):
+            dts.append(grid.step(1, want_dt=True)[0])
+        E._lib.call('exa_aderdg_grid_get_state', grid.h, pin.array.ctypes.data)
+        t2.stop(stream)
+        ms_e2e = max_over_ranks(t2.elapsed_ms())
+        barrier()
+        sb = grid.state_size * 8
+        e2e = {'value': world * ncells * args.steps / (ms_e2e * 1e-3), 'unit': 'cell-updates/s',
+               'h2d_bytes_per_step': sb / args.steps, 'd2h_bytes_per_step': 8 + sb / args.steps,
+               'note': 'one solve per timed region: state upload from pinned host memory, K steps each '
+                       'returning its dt to the host, final state download'}
+        pin.free()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        st = grid.get_state()
+        dt_now = grid.step(1, want_dt=True)[0]
+        v, kind, cores, sample, _ = cpu_sample(order, n, st, dt_now, budget_s=15.0)
+        cpu = {'value': v, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind, 'sample': sample}
+
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'cell-updates/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_max / args.steps, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': config_dict(args, world),
+            'roofline': {
+                'kernel': 'k_predictor', 'bound': 'fp64', 'achieved': achieved_tf,
+                'peak': fp64_peak.value, 'unit': 'TFLOP/s', 'frac': achieved_tf / fp64_peak.value,
+                'peak_source': 'DFMA probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)',
+                'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
+                'traffic': (traffic_pc * ncells if traffic_pc else None),
+                'ms_per_launch': pred_ms,
+                'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms']),
+            },
+            'roofline_hbm': {
+                'achieved': bytes_per_cell_update(3, order) * ncells * args.steps / (ms * 1e-3) / 1e9,
+                'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s', 'peak_source': peak_src,
+                'bytes_per_cell_update': bytes_per_cell_update(3, order)},
+            'flop_per_cell_update': total_flop,
+            'cpu_baseline': cpu,
+            'e2e': e2e,
+            'gpu_launches': launches,
+            'clocks': clk,
+        }
+        print(json.dumps(line), flush=True)
+    grid.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

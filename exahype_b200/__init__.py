@@ -1,0 +1,15 @@
+"""exahype_b200: B200-native ADER-DG / finite-volume cell-update library.
+
+The compute path is libexahype_b200.so (hand-written sm_100a CUDA behind the
+C ABI declared in include/exa_kernels.h); this package is the thin Python
+host layer over that ABI.
+"""
+from ._lib import (EXA_OK, PDE_EULER, PDE_EULER_PLANAR, PREC_FP64, PREC_MIXED, ExaError,
+                   lib)
+from .aderdg import ADERDGGrid, ADERDGSolver, BatchedADERDG, make_desc
+from .device import DeviceBuffer, PinnedBuffer, Stream, Timer, device_count, launch_count
+from .fv import FVPatches
+
+__all__ = ['ADERDGGrid', 'ADERDGSolver', 'BatchedADERDG', 'DeviceBuffer', 'PinnedBuffer', 'Stream',
+           'Timer', 'FVPatches', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
+           'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED']

@@ -1,0 +1,164 @@
+"""ctypes binding of libexahype_b200.so (the C ABI in include/exa_kernels.h).
+
+The shared library is built in-tree (``make -C exahype_b200/csrc``) and
+loaded from this package directory.  There is no fallback: if the library
+is missing every entry point raises.
+"""
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libexahype_b200.so')
+
+EXA_OK = 0
+EXA_EINVAL = 1
+EXA_ENONCONV = 2
+EXA_ENAN = 3
+EXA_ETIMEDOUT = 4
+EXA_ECUDA = 5
+EXA_ENOMEM = 6
+EXA_EBUSY = 7
+EXA_ENOTFOUND = 8
+
+PDE_EULER = 0
+PDE_EULER_PLANAR = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class ExaError(RuntimeError):
+    def __init__(self, status, where, detail=''):
+        self.status = status
+        super().__init__('%s failed: status %d (%s)%s' % (
+            where, status, _status_string(status), (': ' + detail) if detail else ''))
+
+
+class AderdgDesc(C.Structure):
+    _fields_ = [('dim', C.c_int), ('order', C.c_int), ('nvar', C.c_int), ('npar', C.c_int),
+                ('pde', C.c_int), ('precision', C.c_int), ('dx', C.c_double * 3)]
+
+
+class GridConfig(C.Structure):
+    _fields_ = [('dim', C.c_int), ('order', C.c_int), ('n', C.c_int * 3),
+                ('length', C.c_double * 3), ('pde', C.c_int), ('precision', C.c_int),
+                ('dt_policy', C.c_int), ('cfl', C.c_double), ('dt_fixed', C.c_double)]
+
+
+class FVDesc(C.Structure):
+    _fields_ = [('dim', C.c_int), ('patch', C.c_int), ('ghost', C.c_int), ('nvar', C.c_int),
+                ('npar', C.c_int), ('pde', C.c_int), ('dx', C.c_double * 3)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+vp = C.c_void_p
+i32 = C.c_int
+i64 = C.c_long
+f64 = C.c_double
+u64 = C.c_uint64
+sz = C.c_size_t
+dptr = C.POINTER(C.c_double)
+dpp = C.POINTER(C.POINTER(C.c_double))
+ipt = C.POINTER(C.c_int)
+
+# name -> (restype, argtypes); the list is the C ABI surface the tests check
+SIGNATURES = {
+    'exa_status_string': (C.c_char_p, [i32]),
+    'exa_last_error_string': (C.c_char_p, []),
+    'exa_device_count': (i32, []),
+    'exa_set_device': (i32, [i32]),
+    'exa_device_alloc': (i32, [sz, C.POINTER(vp)]),
+    'exa_device_free': (i32, [vp]),
+    'exa_host_alloc_pinned': (i32, [sz, C.POINTER(vp)]),
+    'exa_host_free_pinned': (i32, [vp]),
+    'exa_memcpy_h2d': (i32, [vp, vp, sz, vp]),
+    'exa_memcpy_d2h': (i32, [vp, vp, sz, vp]),
+    'exa_memset_device': (i32, [vp, i32, sz, vp]),
+    'exa_stream_create': (i32, [C.POINTER(vp)]),
+    'exa_stream_destroy': (i32, [vp]),
+    'exa_stream_synchronize': (i32, [vp]),
+    'exa_device_synchronize': (i32, []),
+    'exa_timer_create': (i32, [C.POINTER(vp)]),
+    'exa_timer_destroy': (i32, [vp]),
+    'exa_timer_start': (i32, [vp, vp]),
+    'exa_timer_stop': (i32, [vp, vp]),
+    'exa_timer_elapsed_ms': (i32, [vp, C.POINTER(C.c_float)]),
+    'exa_launch_count': (u64, []),
+    'exa_measure_fp64_peak': (i32, [C.POINTER(f64)]),
+    'exa_measure_copy_bandwidth': (i32, [sz, C.POINTER(f64)]),
+    'exa_aderdg_spaceTimePredictor': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dpp, dpp, dptr, dptr,
+                                            dptr, dptr, dptr, f64, dptr, ipt]),
+    'exa_aderdg_volumeIntegral': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr]),
+    'exa_aderdg_surfaceIntegral': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr]),
+    'exa_aderdg_riemannSolver': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr, dptr, dptr, dpp, dpp,
+                                       f64, i32, i32]),
+    'exa_aderdg_solutionUpdate': (i32, [C.POINTER(AderdgDesc), dptr, dptr, f64]),
+    'exa_aderdg_stableTimeStepSize': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr, dptr]),
+    'exa_aderdg_predictor_vi': (i32, [C.POINTER(AderdgDesc), i64, vp, f64, vp, vp, vp, vp, vp, vp, vp]),
+    'exa_aderdg_predictor_full': (i32, [C.POINTER(AderdgDesc), i64, vp, f64, vp, vp, vp, vp, vp, vp, vp,
+                                        vp, vp]),
+    'exa_aderdg_volume_integral': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, vp]),
+    'exa_aderdg_surface_integral': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, vp]),
+    'exa_aderdg_solution_update': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, f64, vp]),
+    'exa_aderdg_riemann_faces': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, vp, vp, vp, vp]),
+    'exa_aderdg_stable_dt': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, vp, vp]),
+    'exa_aderdg_grid_create': (i32, [C.POINTER(GridConfig), C.POINTER(vp)]),
+    'exa_aderdg_grid_destroy': (i32, [vp]),
+    'exa_aderdg_grid_footprint': (sz, [C.POINTER(GridConfig)]),
+    'exa_aderdg_grid_init': (i32, [vp, i32, f64, u64, f64]),
+    'exa_aderdg_grid_set_state': (i32, [vp, vp]),
+    'exa_aderdg_grid_get_state': (i32, [vp, vp]),
+    'exa_aderdg_grid_step': (i32, [vp, i32, vp]),
+    'exa_aderdg_grid_use_graph': (i32, [vp, i32]),
+    'exa_aderdg_grid_stream': (i32, [vp, C.POINTER(vp)]),
+    'exa_aderdg_grid_profile': (i32, [vp, i32]),
+    'exa_aderdg_grid_phase_times': (i32, [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64)]),
+    'exa_aderdg_grid_device_state': (i32, [vp, C.POINTER(vp)]),
+    'exa_aderdg_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(u64), C.POINTER(u64), C.POINTER(i32)]),
+    'exa_aderdg_grid_ncells': (i64, [vp]),
+    'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
+    'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
+    'exa_fv_stable_dt': (i32, [C.POINTER(FVDesc), i64, vp, vp, vp]),
+    'exa_fv_periodic_ghosts': (i32, [C.POINTER(FVDesc), i64, vp, vp]),
+    'exa_fv_rusanov': (i32, [i32, i32, i32, i32, dptr, dptr, dptr, dptr, i32, dptr]),
+}
+
+
+def _status_string(s):
+    if _lib is None:
+        return str(s)
+    return _lib.exa_status_string(s).decode()
+
+
+def lib():
+    """Load the library (once).  Raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError('libexahype_b200.so not found at %s; build it with '
+                               '`make -C exahype_b200/csrc -j` (no CPU fallback exists)' % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, where):
+    if status != EXA_OK:
+        detail = lib().exa_last_error_string().decode()
+        raise ExaError(status, where, detail)
+    return status
+
+
+def call(name, *args):
+    """Call an exa_* function and raise ExaError on a non-zero status."""
+    return check(getattr(lib(), name)(*args), name)

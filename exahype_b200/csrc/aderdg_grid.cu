@@ -1,0 +1,373 @@
+// Uniform periodic ADER-DG grid on one GPU: the device-side replacement for
+// the Peano spacetree + ADERDGSolver bookkeeping of the reference.
+//
+// One time step (reference non-fused order, exahype/runners/Runner.cpp:
+// 1125-1160):
+//   k_predictor   spaceTimePredictor + volumeIntegral, dt read on the device
+//   k_corrector   Riemann on all faces + surfaceIntegral + solutionUpdate,
+//                 and the next dt (min over nodes, atomic min over cells)
+//   k_commit      one thread: time += dt, log dt, dt <- next, reset slot
+// Nothing returns to the host inside a step, so a step is a fixed sequence
+// of launches that a CUDA graph replays.
+#include <cstring>
+#include <new>
+#include <float.h>
+
+#include "exa_device.cuh"
+
+namespace exa {
+double host_pnpm(int order);
+
+struct GridDev {
+  double dt;                     // dt of the current step
+  unsigned long long dt_next;    // atomic-min slot (bit pattern)
+  double time;
+  unsigned long long step;
+  unsigned long long stats[2];   // sum of Picard iterations, non-converged cells
+  int nan_flag;
+  int pad;
+};
+
+__global__ void k_commit(GridDev* g, double* dt_log, int log_cap, int fixed, double dt_fixed) {
+  const double dt = g->dt;
+  g->time += dt;
+  dt_log[g->step % (unsigned long long)log_cap] = dt;
+  g->step += 1;
+  if (fixed) {
+    g->dt = dt_fixed;
+  } else {
+    g->dt = __longlong_as_double((long long)g->dt_next);
+    g->dt_next = 0x7FF0000000000000ULL;  // +inf
+  }
+}
+
+__global__ void k_prime(GridDev* g) {
+  g->dt = __longlong_as_double((long long)g->dt_next);
+  g->dt_next = 0x7FF0000000000000ULL;
+}
+
+}  // namespace exa
+
+using namespace exa;
+
+struct exa_aderdg_grid {
+  exa_aderdg_grid_config_t cfg;
+  exa_aderdg_desc_t desc;
+  int device = 0;
+  long ncells = 0;
+  cudaStream_t st = nullptr;
+  double* luh = nullptr;
+  double* lduh = nullptr;
+  double* qb = nullptr;
+  double* fb = nullptr;
+  GridDev* gd = nullptr;
+  double* dt_log = nullptr;
+  int log_cap = 4096;
+  double dt_factor = 0;
+  bool primed = false;
+  bool use_graph = false;
+  cudaGraphExec_t graph = nullptr;
+  // optional per-phase CUDA-event timing (predictor / corrector+commit)
+  bool profile = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double ms_pred = 0, ms_corr = 0;
+  unsigned long long prof_steps = 0;
+};
+
+static size_t grid_sizes(const exa_aderdg_grid_config_t* c, long* ncells, size_t* n_luh,
+                         size_t* n_face) {
+  long nc = 1;
+  for (int i = 0; i < c->dim; i++) nc *= c->n[i];
+  const int B = c->order + 1;
+  size_t nn = 1, nf = 1;
+  for (int i = 0; i < c->dim; i++) nn *= B;
+  for (int i = 0; i < c->dim - 1; i++) nf *= B;
+  *ncells = nc;
+  *n_luh = nc * nn * kV;
+  *n_face = nc * 2 * c->dim * nf * kV;
+  return sizeof(double) * (2 * *n_luh + 2 * *n_face) + sizeof(GridDev) + 4096 * sizeof(double);
+}
+
+static exa_status_t grid_prime(exa_aderdg_grid* g) {
+  if (g->cfg.dt_policy == 2) {
+    GridDev h{};
+    h.dt = g->cfg.dt_fixed;
+    h.dt_next = 0x7FF0000000000000ULL;
+    // keep time/step/stats: only overwrite dt fields
+    cudaError_t e = cudaMemcpyAsync(&g->gd->dt, &h.dt, sizeof(double), cudaMemcpyHostToDevice, g->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+    if (e != cudaSuccess) return cuda_status(e, "prime fixed dt");
+    g->primed = true;
+    return EXA_OK;
+  }
+  const unsigned long long inf = 0x7FF0000000000000ULL;
+  cudaError_t e = cudaMemcpyAsync(&g->gd->dt_next, &inf, 8, cudaMemcpyHostToDevice, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) return cuda_status(e, "prime dt slot");
+  if (exa_status_t s = launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr,
+                                        &g->gd->dt_next, g->st))
+    return s;
+  k_prime<<<1, 1, 0, g->st>>>(g->gd);
+  count_launch();
+  if (exa_status_t s = cuda_status(cudaGetLastError(), "k_prime")) return s;
+  g->primed = true;
+  return EXA_OK;
+}
+
+static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
+  if (g->profile) cudaEventRecord(g->ev[0], g->st);
+  PredArgs a{};
+  a.ncells = g->ncells;
+  a.luh = g->luh;
+  a.dt = 0.0;
+  a.dt_dev = &g->gd->dt;
+  for (int i = 0; i < 3; i++) a.idx[i] = i < g->cfg.dim ? 1.0 / g->desc.dx[i] : 0.0;
+  a.lduh = g->lduh;
+  a.lQhbnd = g->qb;
+  a.lFhbnd = g->fb;
+  a.iters = nullptr;
+  a.stats = g->gd->stats;
+  a.precision = g->cfg.precision;
+  if (exa_status_t s = launch_predictor(g->desc, a, 0, g->st)) return s;
+  if (g->profile) cudaEventRecord(g->ev[1], g->st);
+  CorrArgs c{};
+  c.ncells = g->ncells;
+  for (int i = 0; i < 3; i++) {
+    c.n[i] = i < g->cfg.dim ? g->cfg.n[i] : 1;
+    c.dx[i] = g->desc.dx[i];
+  }
+  c.dt_dev = &g->gd->dt;
+  c.luh = g->luh;
+  c.lduh = g->lduh;
+  c.lQhbnd = g->qb;
+  c.lFhbnd = g->fb;
+  c.dt_next = g->cfg.dt_policy == 2 ? nullptr : &g->gd->dt_next;
+  c.dt_factor = g->dt_factor;
+  c.nan_flag = &g->gd->nan_flag;
+  if (exa_status_t s = launch_corrector(g->cfg.dim, g->cfg.order, g->cfg.pde, c, g->st)) return s;
+  k_commit<<<1, 1, 0, g->st>>>(g->gd, g->dt_log, g->log_cap, g->cfg.dt_policy == 2, g->cfg.dt_fixed);
+  count_launch();
+  if (exa_status_t s = cuda_status(cudaGetLastError(), "k_commit")) return s;
+  if (g->profile) {
+    cudaEventRecord(g->ev[2], g->st);
+    cudaError_t e = cudaEventSynchronize(g->ev[2]);
+    if (e != cudaSuccess) return cuda_status(e, "profile sync");
+    float a1 = 0, a2 = 0;
+    cudaEventElapsedTime(&a1, g->ev[0], g->ev[1]);
+    cudaEventElapsedTime(&a2, g->ev[1], g->ev[2]);
+    g->ms_pred += a1;
+    g->ms_corr += a2;
+    g->prof_steps++;
+  }
+  return EXA_OK;
+}
+
+extern "C" {
+
+size_t exa_aderdg_grid_footprint(const exa_aderdg_grid_config_t* cfg) {
+  if (!cfg) return 0;
+  long nc;
+  size_t a, b;
+  return grid_sizes(cfg, &nc, &a, &b);
+}
+
+exa_status_t exa_aderdg_grid_create(const exa_aderdg_grid_config_t* cfg, exa_aderdg_grid** out) {
+  if (!cfg || !out) return set_error(EXA_EINVAL, "NULL argument");
+  if (cfg->dim != 2 && cfg->dim != 3) return set_error(EXA_EINVAL, "dim must be 2 or 3");
+  if (cfg->order < 2 || cfg->order > 5) return set_error(EXA_EINVAL, "order must be in 2..5");
+  for (int i = 0; i < cfg->dim; i++)
+    if (cfg->n[i] < 1 || !(cfg->length[i] > 0)) return set_error(EXA_EINVAL, "bad grid size");
+  if (cfg->dt_policy < 0 || cfg->dt_policy > 2) return set_error(EXA_EINVAL, "bad dt_policy");
+  if (cfg->dt_policy == 2 && !(cfg->dt_fixed > 0)) return set_error(EXA_EINVAL, "dt_fixed must be > 0");
+  if (!(cfg->cfl > 0)) return set_error(EXA_EINVAL, "cfl must be > 0");
+  if (cfg->precision != EXA_PREC_FP64 && cfg->precision != EXA_PREC_MIXED)
+    return set_error(EXA_EINVAL, "bad precision");
+  exa_aderdg_grid* g = new (std::nothrow) exa_aderdg_grid;
+  if (!g) return set_error(EXA_ENOMEM, "host allocation");
+  g->cfg = *cfg;
+  g->desc.dim = cfg->dim;
+  g->desc.order = cfg->order;
+  g->desc.nvar = kV;
+  g->desc.npar = 0;
+  g->desc.pde = cfg->pde;
+  g->desc.precision = cfg->precision;
+  for (int i = 0; i < 3; i++) g->desc.dx[i] = i < cfg->dim ? cfg->length[i] / cfg->n[i] : 1.0;
+  g->dt_factor = cfg->dt_policy == 0 ? cfg->cfl * host_pnpm(cfg->order)
+                                     : cfg->cfl / (2 * cfg->order + 1);
+  cudaGetDevice(&g->device);
+  exa_status_t s = ensure_tables();
+  size_t n_luh, n_face;
+  grid_sizes(cfg, &g->ncells, &n_luh, &n_face);
+  cudaError_t e = cudaSuccess;
+  if (!s) e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->luh, n_luh * sizeof(double));
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->lduh, n_luh * sizeof(double));
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->qb, n_face * sizeof(double));
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->fb, n_face * sizeof(double));
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->gd, sizeof(GridDev));
+  if (!s && e == cudaSuccess) e = cudaMalloc(&g->dt_log, g->log_cap * sizeof(double));
+  if (!s && e == cudaSuccess) e = cudaMemsetAsync(g->gd, 0, sizeof(GridDev), g->st);
+  if (!s && e == cudaSuccess) e = cudaMemsetAsync(g->luh, 0, n_luh * sizeof(double), g->st);
+  if (!s && e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (!s && e != cudaSuccess) s = cuda_status(e, "grid allocation");
+  if (s) {
+    exa_aderdg_grid_destroy(g);
+    return s;
+  }
+  *out = g;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_destroy(exa_aderdg_grid* g) {
+  if (!g) return EXA_OK;
+  if (g->st) cudaStreamSynchronize(g->st);
+  if (g->graph) cudaGraphExecDestroy(g->graph);
+  for (int i = 0; i < 3; i++)
+    if (g->ev[i]) cudaEventDestroy(g->ev[i]);
+  cudaFree(g->luh);
+  cudaFree(g->lduh);
+  cudaFree(g->qb);
+  cudaFree(g->fb);
+  cudaFree(g->gd);
+  cudaFree(g->dt_log);
+  if (g->st) cudaStreamDestroy(g->st);
+  delete g;
+  return EXA_OK;
+}
+
+long exa_aderdg_grid_ncells(const exa_aderdg_grid* g) { return g ? g->ncells : 0; }
+
+exa_status_t exa_aderdg_grid_init(exa_aderdg_grid* g, int kind, double param, uint64_t seed,
+                                  double noise_amp) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (kind < 0 || kind > 1) return set_error(EXA_EINVAL, "unknown initial condition");
+  if (exa_status_t s = launch_grid_ic(g->cfg.dim, g->cfg.order, g->cfg.n, g->desc.dx, g->luh, kind,
+                                      param, seed, noise_amp, g->st))
+    return s;
+  g->primed = false;
+  return cuda_status(cudaStreamSynchronize(g->st), "grid init");
+}
+
+exa_status_t exa_aderdg_grid_set_state(exa_aderdg_grid* g, const double* host_luh) {
+  if (!g || !host_luh) return set_error(EXA_EINVAL, "NULL argument");
+  long nc;
+  size_t n_luh, n_face;
+  grid_sizes(&g->cfg, &nc, &n_luh, &n_face);
+  cudaError_t e = cudaMemcpyAsync(g->luh, host_luh, n_luh * sizeof(double), cudaMemcpyHostToDevice, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  g->primed = false;
+  return cuda_status(e, "grid set_state");
+}
+
+exa_status_t exa_aderdg_grid_get_state(exa_aderdg_grid* g, double* host_luh) {
+  if (!g || !host_luh) return set_error(EXA_EINVAL, "NULL argument");
+  long nc;
+  size_t n_luh, n_face;
+  grid_sizes(&g->cfg, &nc, &n_luh, &n_face);
+  cudaError_t e = cudaMemcpyAsync(host_luh, g->luh, n_luh * sizeof(double), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "grid get_state");
+}
+
+exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  g->use_graph = enable != 0;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_profile(exa_aderdg_grid* g, int enable) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (enable && !g->ev[0])
+    for (int i = 0; i < 3; i++) {
+      cudaError_t e = cudaEventCreate(&g->ev[i]);
+      if (e != cudaSuccess) return cuda_status(e, "profile events");
+    }
+  g->profile = enable != 0;
+  if (g->profile) g->use_graph = false;
+  g->ms_pred = g->ms_corr = 0;
+  g->prof_steps = 0;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_phase_times(exa_aderdg_grid* g, double* ms_predictor,
+                                         double* ms_corrector, uint64_t* steps) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (ms_predictor) *ms_predictor = g->ms_pred;
+  if (ms_corrector) *ms_corrector = g->ms_corr;
+  if (steps) *steps = g->prof_steps;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_stream(exa_aderdg_grid* g, void** stream) {
+  if (!g || !stream) return set_error(EXA_EINVAL, "NULL argument");
+  *stream = g->st;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_device_state(exa_aderdg_grid* g, double** luh_dev) {
+  if (!g || !luh_dev) return set_error(EXA_EINVAL, "NULL argument");
+  *luh_dev = g->luh;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_host) {
+  if (!g || nsteps < 0) return set_error(EXA_EINVAL, "bad argument");
+  if (dt_host && nsteps > g->log_cap) return set_error(EXA_EINVAL, "too many steps for the dt log");
+  if (!g->primed)
+    if (exa_status_t s = grid_prime(g)) return s;
+  unsigned long long step0 = 0;
+  if (dt_host) {
+    cudaError_t e = cudaMemcpyAsync(&step0, &g->gd->step, 8, cudaMemcpyDeviceToHost, g->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+    if (e != cudaSuccess) return cuda_status(e, "read step");
+  }
+  if (g->use_graph && !g->graph && nsteps > 0) {
+    cudaGraph_t graph;
+    cudaError_t e = cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e, "begin capture");
+    exa_status_t s = grid_launch_step(g);
+    e = cudaStreamEndCapture(g->st, &graph);
+    if (s) return s;
+    if (e != cudaSuccess) return cuda_status(e, "end capture");
+    e = cudaGraphInstantiate(&g->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "graph instantiate");
+  }
+  for (int i = 0; i < nsteps; i++) {
+    if (g->use_graph) {
+      cudaError_t e = cudaGraphLaunch(g->graph, g->st);
+      if (e != cudaSuccess) return cuda_status(e, "graph launch");
+      count_launch(3);
+    } else if (exa_status_t s = grid_launch_step(g)) {
+      return s;
+    }
+  }
+  if (dt_host && nsteps > 0) {
+    // copy the dt log entries of these steps (ring buffer)
+    for (int i = 0; i < nsteps; i++) {
+      const unsigned long long k = (step0 + i) % (unsigned long long)g->log_cap;
+      cudaError_t e = cudaMemcpyAsync(dt_host + i, g->dt_log + k, sizeof(double), cudaMemcpyDeviceToHost, g->st);
+      if (e != cudaSuccess) return cuda_status(e, "read dt log");
+    }
+    cudaError_t e = cudaStreamSynchronize(g->st);
+    if (e != cudaSuccess) return cuda_status(e, "step sync");
+  }
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time, uint64_t* picard_iters_sum,
+                                    uint64_t* nonconverged, int* nan_flag) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  GridDev h;
+  cudaError_t e = cudaMemcpyAsync(&h, g->gd, sizeof(GridDev), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) return cuda_status(e, "grid status");
+  if (time) *time = h.time;
+  if (picard_iters_sum) *picard_iters_sum = h.stats[0];
+  if (nonconverged) *nonconverged = h.stats[1];
+  if (nan_flag) *nan_flag = h.nan_flag;
+  if (h.nan_flag) return EXA_ENAN;
+  return EXA_OK;
+}
+
+}  // extern "C"

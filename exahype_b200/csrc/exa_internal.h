@@ -1,0 +1,88 @@
+// Internal host-side declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/exa_kernels.h"
+
+namespace exa {
+
+// Records a CUDA error (message retrievable by exa_last_error_string) and
+// maps it to EXA_ECUDA.
+exa_status_t cuda_status(cudaError_t e, const char* where);
+exa_status_t set_error(exa_status_t s, const char* msg);
+void count_launch(uint64_t n = 1);
+// Makes sure the constant-memory tables of every translation unit are
+// uploaded on the current device.
+exa_status_t ensure_tables();
+
+// Arguments of the fused predictor kernel (one struct so the launch
+// wrappers stay small).
+struct PredArgs {
+  long ncells;
+  const double* luh;
+  double dt;
+  const double* dt_dev;
+  double idx[3];     // 1/dx
+  double* lduh;
+  double* lQhbnd;
+  double* lFhbnd;
+  int* iters;
+  unsigned long long* stats;
+  // full (reference temporaries) outputs, mode 1 only
+  double* lQi;
+  double* lFi;
+  double* lQhi;
+  double* lFhi;
+  // mixed-precision error feedback (unused in FP64 mode)
+  int precision;
+};
+
+exa_status_t launch_predictor(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
+                              cudaStream_t st);
+
+// fused Riemann + surface integral + update + next-dt on a uniform periodic grid
+struct CorrArgs {
+  long ncells;
+  int n[3];
+  double dx[3];
+  const double* dt_dev;     // dt of this step
+  double* luh;
+  const double* lduh;
+  const double* lQhbnd;
+  const double* lFhbnd;
+  unsigned long long* dt_next;  // atomic-min slot for the next dt (nullable)
+  double dt_factor;             // CFL*PNPM[N] or CFL/(2N+1)
+  int* nan_flag;
+};
+exa_status_t launch_corrector(int dim, int order, int pde, const CorrArgs& a, cudaStream_t st);
+
+// per-cell stable dt (+ optional global min via atomic slot)
+exa_status_t launch_stable_dt(const exa_aderdg_desc_t& d, long ncells, const double* luh,
+                              double factor, double* dt_cell, unsigned long long* dt_min_bits,
+                              cudaStream_t st);
+exa_status_t launch_volume_integral(const exa_aderdg_desc_t& d, long ncells, double* lduh,
+                                    const double* lFhi, cudaStream_t st);
+exa_status_t launch_surface_integral(const exa_aderdg_desc_t& d, long ncells, double* lduh,
+                                     const double* lFhbnd, cudaStream_t st);
+exa_status_t launch_solution_update(const exa_aderdg_desc_t& d, long ncells, double* luh,
+                                    const double* lduh, double dt, cudaStream_t st);
+exa_status_t launch_riemann_faces(const exa_aderdg_desc_t& d, long nfaces, const int* left,
+                                  const int* right, const int* dir, const double* lQhbnd,
+                                  double* lFhbnd, cudaStream_t st);
+exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, double* luh,
+                            int kind, double param, uint64_t seed, double noise,
+                            cudaStream_t st);
+
+exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* qR, double* out);
+
+// table uploads, one per translation unit holding kernels
+exa_status_t upload_tables_predictor();
+exa_status_t upload_tables_faces();
+exa_status_t upload_tables_fv();
+// host copy of the derived tables (same bytes as the device constants)
+const void* host_dg_tables(size_t* bytes);
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace exa

@@ -1,0 +1,507 @@
+// 2D finite-volume patch kernels (EulerFV path): first-order Godunov and
+// MUSCL-Hancock with Rusanov face fluxes, FV CFL time step, periodic ghost
+// fill.  Reference:
+//   kernels/finitevolumes/godunov/c/2d/godunov.cpph:33-120
+//   kernels/finitevolumes/musclhancock/c/2d/musclhancock.cpph:50-240
+//   kernels/finitevolumes/riemannsolvers/c/rusanov.cpph:24-83
+//   kernels/finitevolumes/commons/c/commons.cpph:26-67
+//
+// Layout: a patch is (P+2g)^2 cells, row-major [y][x][nData]; patches are
+// stored back to back.  A CTA updates a TX x TY tile of interior cells; the
+// tile and its halo are staged in shared memory, every face flux is
+// computed once per tile, and each cell applies its four face contributions
+// in the reference's order (x faces, then y faces).  The reference also
+// writes the flux contributions of the patch-boundary faces into the first
+// ghost layer of luh_new; that is reproduced.  HBM traffic per cell-update
+// is the state read + write (80 B), halo re-reads excepted.
+#include <float.h>
+
+#include <vector>
+
+#include "exa_device.cuh"
+
+namespace exa {
+
+constexpr int FV_TX = 32, FV_TY = 8, FV_NT = FV_TX * FV_TY;
+
+struct FVArgs {
+  int P, g, S, npar;
+  double hx, hy;      // cell sizes
+  double dt;
+  const double* luh;  // state the fluxes are computed from
+  double* out;        // luh_new: updated in place (reference semantics)
+  unsigned long long* max_dt;  // per patch, atomic-min bit patterns (nullable)
+};
+
+// Rusanov flux of the face between qL and qR in direction d
+// (riemannsolvers/c/rusanov.cpph:24-83); returns s_max.
+template <bool PLANAR>
+__device__ __forceinline__ double rusanov(const double* qL, const double* qR, int d, double* f) {
+  const double sL = euler_max_eig<PLANAR>(qL, d), sR = euler_max_eig<PLANAR>(qR, d);
+  const double smax = fmax(sL, sR);
+  double FL[2][kV], FR[2][kV];
+  euler_flux<2, PLANAR>(qL, FL);
+  euler_flux<2, PLANAR>(qR, FR);
+#pragma unroll
+  for (int i = 0; i < kV; i++) {
+    double v = 0.5 * smax * (qL[i] - qR[i]);
+    v += 0.5 * (FL[d][i] + FR[d][i]);
+    f[i] = v;
+  }
+  return smax;
+}
+
+// ------------------------------------------------------------- Godunov
+template <bool PLANAR>
+__global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
+  constexpr int V = kV;
+  constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
+  __shared__ double su[LY * LX * V];
+  __shared__ double sfx[FV_TY * (FV_TX + 1) * V];
+  __shared__ double sfy[(FV_TY + 1) * FV_TX * V];
+  __shared__ double sred[FV_NT / 32];
+  const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
+  const long patch = blockIdx.z;
+  const double* luh = a.luh + patch * (long)S * S * D;
+  double* out = a.out + patch * (long)S * S * D;
+  const int k0 = pb + blockIdx.x * FV_TX, j0 = pb + blockIdx.y * FV_TY;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < LY * LX; i += FV_NT) {
+    const int r = i / LX, c = i % LX;
+    const int j = j0 - 1 + r, k = k0 - 1 + c;
+    if (j >= 0 && j < S && k >= 0 && k < S)
+#pragma unroll
+      for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
+  }
+  __syncthreads();
+  double dtl = DBL_MAX;
+  // x faces: between (j, k-1) and (j, k), k in [k0, k0+TX], valid for k in [pb, pe]
+  for (int i = tid; i < FV_TY * (FV_TX + 1); i += FV_NT) {
+    const int r = i / (FV_TX + 1), c = i % (FV_TX + 1);
+    const int j = j0 + r, k = k0 + c;
+    if (j < pe && k <= pe) {
+      const double s = rusanov<PLANAR>(&su[((r + 1) * LX + c) * V], &su[((r + 1) * LX + c + 1) * V], 0,
+                                       &sfx[i * V]);
+      dtl = fmin(dtl, 0.9 / 2 * a.hx / s);
+    }
+  }
+  // y faces: between (j-1, k) and (j, k), j in [j0, j0+TY], valid for j in [pb, pe]
+  for (int i = tid; i < (FV_TY + 1) * FV_TX; i += FV_NT) {
+    const int r = i / FV_TX, c = i % FV_TX;
+    const int j = j0 + r, k = k0 + c;
+    if (j <= pe && k < pe) {
+      const double s = rusanov<PLANAR>(&su[(r * LX + c + 1) * V], &su[((r + 1) * LX + c + 1) * V], 1,
+                                       &sfy[i * V]);
+      dtl = fmin(dtl, 0.9 / 2 * a.hy / s);
+    }
+  }
+  __syncthreads();
+  const double cx = a.dt / a.hx, cy = a.dt / a.hy;
+  {
+    const int r = tid / FV_TX, c = tid % FV_TX;
+    const int j = j0 + r, k = k0 + c;
+    if (j < pe && k < pe) {
+      double* o = out + ((long)j * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        double u = o[m];
+        u += cx * sfx[(r * (FV_TX + 1) + c) * V + m];
+        u -= cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
+        u += cy * sfy[(r * FV_TX + c) * V + m];
+        u -= cy * sfy[((r + 1) * FV_TX + c) * V + m];
+        o[m] = u;
+      }
+    }
+    // first ghost layer, as the reference's face loops touch it
+    if (j < pe && k0 == pb && c == 0) {
+      double* o = out + ((long)j * S + (pb - 1)) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] -= cx * sfx[(r * (FV_TX + 1)) * V + m];
+    }
+    if (j < pe && k == pe - 1) {
+      double* o = out + ((long)j * S + pe) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] += cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
+    }
+    if (k < pe && j0 == pb && r == 0) {
+      double* o = out + ((long)(pb - 1) * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] -= cy * sfy[c * V + m];
+    }
+    if (k < pe && j == pe - 1) {
+      double* o = out + ((long)pe * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] += cy * sfy[((r + 1) * FV_TX + c) * V + m];
+    }
+  }
+  if (a.max_dt) {
+    for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
+    if ((tid & 31) == 0) sred[tid >> 5] = dtl;
+    __syncthreads();
+    if (tid == 0) {
+      double m = sred[0];
+      for (int w = 1; w < FV_NT / 32; w++) m = fmin(m, sred[w]);
+      atomic_min_pos_double(&a.max_dt[patch], m);
+    }
+  }
+}
+
+// -------------------------------------------------------- MUSCL-Hancock
+__device__ __forceinline__ double minmod(double a, double b) {
+  if (a * b < 0.0) return 0.0;
+  return fabs(a) < fabs(b) ? a : b;
+}
+
+template <bool PLANAR>
+__global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
+  constexpr int V = kV;
+  // staged state: cells j0-2..j0+TY+1, k0-2..k0+TX+1
+  constexpr int LX = FV_TX + 4, LY = FV_TY + 4;
+  // extrapolated values: x-type on rows j0..j0+TY-1 (+1 ring rows for the
+  // y-face cells' evolution), cols k0-1..k0+TX; y-type similarly
+  constexpr int RX = FV_TX + 2, RY = FV_TY + 2;  // ring region (tile + 1)
+  extern __shared__ double sm[];
+  double* su = sm;                               // LY*LX*V
+  double* wLx = su + LY * LX * V;                // RY*RX*V each
+  double* wRx = wLx + RY * RX * V;
+  double* wLy = wRx + RY * RX * V;
+  double* wRy = wLy + RY * RX * V;
+  double* sfx = wRy + RY * RX * V;               // TY*(TX+1)*V
+  double* sfy = sfx + FV_TY * (FV_TX + 1) * V;   // (TY+1)*TX*V
+  double* sred = sfy + (FV_TY + 1) * FV_TX * V;
+  const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
+  const long patch = blockIdx.z;
+  const double* luh = a.luh + patch * (long)S * S * D;
+  double* out = a.out + patch * (long)S * S * D;
+  const int k0 = pb + blockIdx.x * FV_TX, j0 = pb + blockIdx.y * FV_TY;
+  const int tid = threadIdx.x;
+  const double hx = a.hx, hy = a.hy, dt = a.dt;
+  for (int i = tid; i < LY * LX; i += FV_NT) {
+    const int r = i / LX, c = i % LX;
+    const int j = j0 - 2 + r, k = k0 - 2 + c;
+    if (j >= 0 && j < S && k >= 0 && k < S)
+#pragma unroll
+      for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
+  }
+  __syncthreads();
+  // ring cells (j, k) with j in [j0-1, j0+TY], k in [k0-1, k0+TX]
+  for (int i = tid; i < RY * RX; i += FV_NT) {
+    const int rr = i / RX, rc = i % RX;
+    const int j = j0 - 1 + rr, k = k0 - 1 + rc;
+    const double* U = &su[((rr + 1) * LX + rc + 1) * V];
+    // reference slope ranges (musclhancock.cpph:79-98): x slopes for
+    // j in [pb,pe), k in [pb-1,pe+1); y slopes for j in [pb-1,pe+1), k in [pb,pe)
+    const bool has_x = j >= pb && j < pe && k >= pb - 1 && k < pe + 1;
+    const bool has_y = j >= pb - 1 && j < pe + 1 && k >= pb && k < pe;
+    const bool interior = j >= pb && j < pe && k >= pb && k < pe;
+    double lx[V], rx[V], ly[V], ry[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
+    if (has_x) {
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+        lx[m] = U[m] - 0.5 * hx * sl;
+        rx[m] = U[m] + 0.5 * hx * sl;
+      }
+    }
+    if (has_y) {
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) / hy;
+        ly[m] = U[m] - 0.5 * hy * sl;
+        ry[m] = U[m] + 0.5 * hy * sl;
+      }
+    }
+    if (interior) {
+      // half time step of the interior cells (musclhancock.cpph:126-170)
+      double Qt[V];
+      double F[2][V];
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] = 0.0;
+      euler_flux<2, PLANAR>(lx, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+      euler_flux<2, PLANAR>(rx, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+      euler_flux<2, PLANAR>(ly, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+      euler_flux<2, PLANAR>(ry, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        lx[m] += 0.5 * dt * Qt[m];
+        rx[m] += 0.5 * dt * Qt[m];
+        ly[m] += 0.5 * dt * Qt[m];
+        ry[m] += 0.5 * dt * Qt[m];
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      wLx[i * V + m] = lx[m];
+      wRx[i * V + m] = rx[m];
+      wLy[i * V + m] = ly[m];
+      wRy[i * V + m] = ry[m];
+    }
+  }
+  __syncthreads();
+  double dtl = DBL_MAX;
+  // x faces between ring col c (k = k0-1+c) and c+1, rows j0..j0+TY-1
+  for (int i = tid; i < FV_TY * (FV_TX + 1); i += FV_NT) {
+    const int r = i / (FV_TX + 1), c = i % (FV_TX + 1);
+    const int j = j0 + r, k = k0 - 1 + c;  // face between k and k+1
+    if (j < pe && k + 1 <= pe) {
+      const int il = (r + 1) * RX + c, ir = il + 1;
+      const double s = rusanov<PLANAR>(&wRx[il * V], &wLx[ir * V], 0, &sfx[i * V]);
+      dtl = fmin(dtl, 0.99 / 2 * hx / s);
+    }
+  }
+  for (int i = tid; i < (FV_TY + 1) * FV_TX; i += FV_NT) {
+    const int r = i / FV_TX, c = i % FV_TX;
+    const int j = j0 - 1 + r, k = k0 + c;  // face between j and j+1
+    if (j + 1 <= pe && k < pe) {
+      const int il = r * RX + c + 1, ir = il + RX;
+      const double s = rusanov<PLANAR>(&wRy[il * V], &wLy[ir * V], 1, &sfy[i * V]);
+      dtl = fmin(dtl, 0.99 / 2 * hy / s);
+    }
+  }
+  __syncthreads();
+  const double cx = dt / hx, cy = dt / hy;
+  {
+    const int r = tid / FV_TX, c = tid % FV_TX;
+    const int j = j0 + r, k = k0 + c;
+    if (j < pe && k < pe) {
+      double* o = out + ((long)j * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        double u = o[m];
+        u += cx * sfx[(r * (FV_TX + 1) + c) * V + m];
+        u -= cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
+        u += cy * sfy[(r * FV_TX + c) * V + m];
+        u -= cy * sfy[((r + 1) * FV_TX + c) * V + m];
+        o[m] = u;
+      }
+    }
+    if (j < pe && k0 == pb && c == 0) {
+      double* o = out + ((long)j * S + (pb - 1)) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] -= cx * sfx[(r * (FV_TX + 1)) * V + m];
+    }
+    if (j < pe && k == pe - 1) {
+      double* o = out + ((long)j * S + pe) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] += cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
+    }
+    if (k < pe && j0 == pb && r == 0) {
+      double* o = out + ((long)(pb - 1) * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] -= cy * sfy[c * V + m];
+    }
+    if (k < pe && j == pe - 1) {
+      double* o = out + ((long)pe * S + k) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] += cy * sfy[((r + 1) * FV_TX + c) * V + m];
+    }
+  }
+  if (a.max_dt) {
+    for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
+    if ((tid & 31) == 0) sred[tid >> 5] = dtl;
+    __syncthreads();
+    if (tid == 0) {
+      double m = sred[0];
+      for (int w = 1; w < FV_NT / 32; w++) m = fmin(m, sred[w]);
+      atomic_min_pos_double(&a.max_dt[patch], m);
+    }
+  }
+}
+
+constexpr size_t kMusclSmem =
+    sizeof(double) * ((FV_TY + 4) * (FV_TX + 4) * kV + 4 * (FV_TY + 2) * (FV_TX + 2) * kV +
+                      FV_TY * (FV_TX + 1) * kV + (FV_TY + 1) * FV_TX * kV + FV_NT / 32);
+
+// --------------------------------------------------------- stable dt
+template <bool PLANAR>
+__global__ void k_fv_stable_dt(FVArgs a, double* dt_patch) {
+  const int D = kV + a.npar, S = a.S, P = a.P, g = a.g;
+  const long patch = blockIdx.y;
+  const double* luh = a.luh + patch * (long)S * S * D;
+  double dtl = DBL_MAX;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)P * P; i += (long)gridDim.x * blockDim.x) {
+    const int j = g + (int)(i / P), k = g + (int)(i % P);
+    const double* q = luh + ((long)j * S + k) * D;
+    dtl = fmin(dtl, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(q, 0));
+    dtl = fmin(dtl, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(q, 1));
+  }
+  for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos_double((unsigned long long*)&dt_patch[patch], dtl);
+}
+
+__global__ void k_fv_ghosts(int P, int g, int D, long npatches, double* luh) {
+  const int S = P + 2 * g;
+  const long nghost = (long)S * S - (long)P * P;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nghost * npatches) return;
+  const long patch = gid / nghost;
+  long r = gid % nghost;
+  // enumerate ghost cells: rows [0,g) and [g+P,S) fully, then side columns
+  int j, k;
+  const long top = (long)g * S;
+  if (r < top) { j = (int)(r / S); k = (int)(r % S); }
+  else if (r < 2 * top) { r -= top; j = g + P + (int)(r / S); k = (int)(r % S); }
+  else {
+    r -= 2 * top;
+    j = g + (int)(r / (2 * g));
+    const int c = (int)(r % (2 * g));
+    k = c < g ? c : P + c;
+  }
+  const int sj = g + ((j - g) % P + P) % P, sk = g + ((k - g) % P + P) % P;
+  double* base = luh + patch * (long)S * S * D;
+  for (int m = 0; m < D; m++) base[((long)j * S + k) * D + m] = base[((long)sj * S + sk) * D + m];
+}
+
+static exa_status_t check_fv(const exa_fv_desc_t* d, int want_ghost) {
+  if (!d) return set_error(EXA_EINVAL, "NULL descriptor");
+  if (d->dim != 2) return set_error(EXA_EINVAL, "FV kernels are 2D");
+  if (d->nvar != kV || d->npar < 0 || d->npar > 8) return set_error(EXA_EINVAL, "nvar must be 5");
+  if (d->patch < 1) return set_error(EXA_EINVAL, "patch must be >= 1");
+  if (want_ghost && d->ghost < want_ghost) return set_error(EXA_EINVAL, "ghost layer too thin");
+  if (d->pde != EXA_PDE_EULER && d->pde != EXA_PDE_EULER_PLANAR) return set_error(EXA_EINVAL, "pde");
+  return ensure_tables();
+}
+
+static FVArgs fv_args(const exa_fv_desc_t* d) {
+  FVArgs a{};
+  a.P = d->patch;
+  a.g = d->ghost;
+  a.S = d->patch + 2 * d->ghost;
+  a.npar = d->npar;
+  a.hx = d->dx[0] / d->patch;
+  a.hy = d->dx[1] / d->patch;
+  return a;
+}
+
+exa_status_t upload_tables_fv() { return EXA_OK; }
+
+template <bool PLANAR>
+__global__ void k_rusanov_one(int d, const double* qL, const double* qR, double* out) {
+  // out = [f (5 values), s_max]; the 2D/3D flux only differs in the
+  // direction index, so the 3D case evaluates the flux with DIM = 3
+  double f[kV];
+  const double s = rusanov<PLANAR>(qL, qR, d > 1 ? 0 : d, f);
+  if (d > 1) {
+    const double sm = fmax(euler_max_eig<PLANAR>(qL, d), euler_max_eig<PLANAR>(qR, d));
+    double FL[3][kV], FR[3][kV];
+    euler_flux<3, PLANAR>(qL, FL);
+    euler_flux<3, PLANAR>(qR, FR);
+    for (int i = 0; i < kV; i++) {
+      double v = 0.5 * sm * (qL[i] - qR[i]);
+      v += 0.5 * (FL[d][i] + FR[d][i]);
+      out[i] = v;
+    }
+    out[kV] = sm;
+    return;
+  }
+  for (int i = 0; i < kV; i++) out[i] = f[i];
+  out[kV] = s;
+}
+
+exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* qR, double* out) {
+  if (pde == EXA_PDE_EULER_PLANAR) k_rusanov_one<true><<<1, 1>>>(d, qL, qR, out);
+  else k_rusanov_one<false><<<1, 1>>>(d, qL, qR, out);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_rusanov_one");
+}
+
+}  // namespace exa
+
+using namespace exa;
+
+extern "C" {
+
+static exa_status_t fv_update(int scheme, const exa_fv_desc_t* desc, long npatches, double* luh_new,
+                              const double* luh, double dt, double* max_dt, void* stream) {
+  if (exa_status_t s = check_fv(desc, scheme == 0 ? 1 : 2)) return s;
+  if (npatches < 0 || !luh_new || !luh) return set_error(EXA_EINVAL, "bad argument");
+  if (npatches == 0) return EXA_OK;
+  if (npatches > 65535) return set_error(EXA_EINVAL, "at most 65535 patches per call");
+  cudaStream_t st = as_stream(stream);
+  FVArgs a = fv_args(desc);
+  a.dt = dt;
+  a.luh = luh;
+  a.out = luh_new;
+  a.max_dt = (unsigned long long*)max_dt;
+  if (max_dt) {
+    // +inf bit pattern 0x7FF0000000000000 = bytes 00..00 F0 7F
+    std::vector<unsigned long long> inf(npatches, 0x7FF0000000000000ULL);
+    cudaError_t e = cudaMemcpyAsync(max_dt, inf.data(), 8 * npatches, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e, "max_dt init");
+  }
+  dim3 grid((desc->patch + FV_TX - 1) / FV_TX, (desc->patch + FV_TY - 1) / FV_TY, (unsigned)npatches);
+  const bool planar = desc->pde == EXA_PDE_EULER_PLANAR;
+  if (scheme == 0) {
+    if (planar) k_fv_godunov<true><<<grid, FV_NT, 0, st>>>(a);
+    else k_fv_godunov<false><<<grid, FV_NT, 0, st>>>(a);
+  } else {
+    static bool attr[2] = {false, false};
+    if (!attr[planar]) {
+      cudaError_t e = planar ? cudaFuncSetAttribute(k_fv_muscl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
+                             : cudaFuncSetAttribute(k_fv_muscl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
+      attr[planar] = true;
+    }
+    if (planar) k_fv_muscl<true><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    else k_fv_muscl<false><<<grid, FV_NT, kMusclSmem, st>>>(a);
+  }
+  count_launch();
+  return cuda_status(cudaGetLastError(), scheme == 0 ? "k_fv_godunov" : "k_fv_muscl");
+}
+
+exa_status_t exa_fv_godunov_update(const exa_fv_desc_t* desc, long npatches, double* luh_new,
+                                   const double* luh, double dt, double* max_dt, void* stream) {
+  return fv_update(0, desc, npatches, luh_new, luh, dt, max_dt, stream);
+}
+
+exa_status_t exa_fv_musclhancock_update(const exa_fv_desc_t* desc, long npatches, double* luh_new,
+                                        const double* luh, double dt, double* max_dt, void* stream) {
+  return fv_update(1, desc, npatches, luh_new, luh, dt, max_dt, stream);
+}
+
+exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches, const double* luh,
+                              double* dt_patch, void* stream) {
+  if (exa_status_t s = check_fv(desc, 0)) return s;
+  if (npatches < 0 || !luh || !dt_patch) return set_error(EXA_EINVAL, "bad argument");
+  if (npatches == 0) return EXA_OK;
+  cudaStream_t st = as_stream(stream);
+  std::vector<unsigned long long> inf(npatches, 0x7FF0000000000000ULL);
+  cudaError_t e = cudaMemcpyAsync(dt_patch, inf.data(), 8 * npatches, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e, "dt init");
+  FVArgs a = fv_args(desc);
+  a.luh = luh;
+  const long cells = (long)desc->patch * desc->patch;
+  unsigned bx = (unsigned)((cells + 255) / 256);
+  if (bx > 1024) bx = 1024;
+  dim3 grid(bx, (unsigned)npatches);
+  if (desc->pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<grid, 256, 0, st>>>(a, dt_patch);
+  else k_fv_stable_dt<false><<<grid, 256, 0, st>>>(a, dt_patch);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_fv_stable_dt");
+}
+
+exa_status_t exa_fv_periodic_ghosts(const exa_fv_desc_t* desc, long npatches, double* luh, void* stream) {
+  if (exa_status_t s = check_fv(desc, 0)) return s;
+  if (npatches < 0 || !luh) return set_error(EXA_EINVAL, "bad argument");
+  const int S = desc->patch + 2 * desc->ghost;
+  const long work = ((long)S * S - (long)desc->patch * desc->patch) * npatches;
+  if (work == 0) return EXA_OK;
+  k_fv_ghosts<<<(unsigned)((work + 255) / 256), 256, 0, as_stream(stream)>>>(
+      desc->patch, desc->ghost, desc->nvar + desc->npar, npatches, luh);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_fv_ghosts");
+}
+
+}  // extern "C"

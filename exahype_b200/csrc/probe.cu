@@ -1,0 +1,102 @@
+// Device capability probes used as roofline denominators by the benchmark:
+// FP64 FMA throughput (no FP64 figure is shipped with the measured peaks)
+// and a plain DRAM copy bandwidth.
+#include "exa_device.cuh"
+
+namespace exa {
+
+// 8 independent DFMA chains per thread; the result is written so the chains
+// are live.  2 FLOP per FMA.
+__global__ void k_fp64_fma(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x * 1e-7, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
+  double x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+__global__ void k_copy(const double4* __restrict__ in, double4* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+}  // namespace exa
+
+using namespace exa;
+
+extern "C" {
+
+exa_status_t exa_measure_fp64_peak(double* tflops) {
+  if (!tflops) return set_error(EXA_EINVAL, "NULL tflops");
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int threads = 256, blocks = sms * 8, iters = 2048;
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(double) * blocks * threads);
+  if (e != cudaSuccess) return cuda_status(e, "probe alloc");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_fp64_fma<<<blocks, threads>>>(out, 64, 0.999999, 1e-9);  // warm-up
+  cudaEventRecord(a);
+  k_fp64_fma<<<blocks, threads>>>(out, iters, 0.999999, 1e-9);
+  cudaEventRecord(b);
+  count_launch(2);
+  e = cudaEventSynchronize(b);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (e != cudaSuccess) return cuda_status(e, "probe fp64");
+  const double flop = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flop / (ms * 1e-3) / 1e12;
+  return EXA_OK;
+}
+
+exa_status_t exa_measure_copy_bandwidth(size_t bytes, double* gbs) {
+  if (!gbs || bytes < 1024) return set_error(EXA_EINVAL, "bad argument");
+  const size_t n = bytes / sizeof(double4);
+  double4 *in = nullptr, *out = nullptr;
+  cudaError_t e = cudaMalloc(&in, n * sizeof(double4));
+  if (e == cudaSuccess) e = cudaMalloc(&out, n * sizeof(double4));
+  if (e != cudaSuccess) {
+    cudaFree(in);
+    return cuda_status(e, "probe alloc");
+  }
+  cudaMemset(in, 0, n * sizeof(double4));
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_copy<<<sms * 4, 512>>>(in, out, n);
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(a);
+    k_copy<<<sms * 4, 512>>>(in, out, n);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) best = ms;
+  }
+  count_launch(6);
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(in);
+  cudaFree(out);
+  if (e != cudaSuccess) return cuda_status(e, "probe copy");
+  *gbs = 2.0 * n * sizeof(double4) / (best * 1e-3) / 1e9;
+  return EXA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,310 @@
+/*
+ * exahype_b200 -- C ABI of the B200 (sm_100a) ADER-DG / finite-volume
+ * cell-update library (libexahype_b200.so).
+ *
+ * The entry points mirror the generic C++ kernels of ExaHyPE
+ * (ExaHyPE/kernels/aderdg/generic/Kernels.h:86-175,
+ * kernels/finitevolumes/{godunov,musclhancock,riemannsolvers,commons}/c/*.h)
+ * and the solver methods that call them (the toolkit-generated
+ * Abstract<Solver>, Toolkit/src/eu/exahype/solvers/templates/
+ * AbstractGenericADERDGSolverHeader.template:166-177 and
+ * AbstractGenericFiniteVolumesSolverHeader.template:52-63).
+ *
+ * Conventions
+ *  - All data are FP64 in the reference's row-major per-cell layouts
+ *    (ExaHyPE/kernels/KernelUtils.h:243-320), slowest index first:
+ *      luh    [z][y][x][nVar+nPar]          (2D: [y][x][...])
+ *      lduh   [z][y][x][nVar]
+ *      lQhbnd [2*dim][B][B][nVar+nPar], lFhbnd [2*dim][B][B][nVar]
+ *      lFhi   (dim+1) blocks: x [z][y][x], y [z][x][y], z [y][x][z], source
+ *    with B = order+1.  Batched entry points take `ncells` cells stored
+ *    back to back (cell stride = size of one cell's array).
+ *  - The PDE is compiled in: compressible Euler, nVar = 5, gamma = 1.4.
+ *    PDE callbacks of the reference (flux, eigenvalues) cannot cross to
+ *    the device, so the PDE is selected by enum.
+ *  - Every function returns an exa_status_t; nothing aborts.  Device
+ *    entry points are asynchronous on `stream` (a cudaStream_t passed as
+ *    void*, NULL = legacy default stream) and never allocate.
+ *  - Kernels are reentrant; concurrent calls on different streams need
+ *    distinct output buffers, as in the reference (TBB workers with
+ *    distinct temporaries, mappings/Prediction.cpp:152).
+ */
+#ifndef EXA_KERNELS_H
+#define EXA_KERNELS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status */
+typedef int exa_status_t;
+#define EXA_OK          0
+#define EXA_EINVAL      1  /* unsupported dimension/order/size or NULL pointer */
+#define EXA_ENONCONV    2  /* Picard iteration hit 2(N+1) iterations in >= 1 cell */
+#define EXA_ENAN        3  /* a NaN/Inf was produced */
+#define EXA_ETIMEDOUT   4  /* a bounded device-side wait gave up */
+#define EXA_ECUDA       5  /* CUDA runtime error (see exa_last_error_string) */
+#define EXA_ENOMEM      6  /* device or host allocation failed */
+#define EXA_EBUSY       7  /* admission refused: not enough free slots/memory */
+#define EXA_ENOTFOUND   8  /* unknown handle / request id */
+
+const char* exa_status_string(exa_status_t s);
+const char* exa_last_error_string(void);
+
+typedef enum {
+  EXA_PDE_EULER = 0,        /* pressure from all three momenta */
+  EXA_PDE_EULER_PLANAR = 1  /* 2D "2.5D" form of the reference's kernel tests */
+} exa_pde_t;
+
+typedef enum {
+  EXA_PREC_FP64 = 0,  /* plain path: every operation in FP64 */
+  EXA_PREC_MIXED = 1  /* Picard contractions in reduced precision; update,
+                         face fluxes and dt stay FP64 */
+} exa_precision_t;
+
+/* Describes one ADER-DG solver instance (the compile-time constants of the
+ * generated Abstract<Solver>: NumberOfVariables/Parameters, Order,
+ * AbstractGenericADERDGSolverHeader.template:31-34). */
+typedef struct {
+  int dim;        /* 2 or 3 */
+  int order;      /* N; supported 2..5 (3 also with nPar = 1) */
+  int nvar;       /* must be 5 */
+  int npar;       /* 0, or 1 for the drop-in per-cell calls */
+  int pde;        /* exa_pde_t */
+  int precision;  /* exa_precision_t */
+  double dx[3];   /* cell size per dimension */
+} exa_aderdg_desc_t;
+
+/* ---------------------------------------------- device/runtime helpers */
+int exa_device_count(void);
+exa_status_t exa_set_device(int device);
+exa_status_t exa_device_alloc(size_t bytes, void** ptr);
+exa_status_t exa_device_free(void* ptr);
+exa_status_t exa_host_alloc_pinned(size_t bytes, void** ptr);
+exa_status_t exa_host_free_pinned(void* ptr);
+exa_status_t exa_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream);
+exa_status_t exa_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream);
+exa_status_t exa_memset_device(void* dst, int value, size_t bytes, void* stream);
+exa_status_t exa_stream_create(void** stream);
+exa_status_t exa_stream_destroy(void* stream);
+exa_status_t exa_stream_synchronize(void* stream);
+exa_status_t exa_device_synchronize(void);
+/* CUDA-event timer on a stream */
+exa_status_t exa_timer_create(void** timer);
+exa_status_t exa_timer_destroy(void* timer);
+exa_status_t exa_timer_start(void* timer, void* stream);
+exa_status_t exa_timer_stop(void* timer, void* stream);
+exa_status_t exa_timer_elapsed_ms(void* timer, float* ms);
+/* number of kernels this library has launched in this process */
+uint64_t exa_launch_count(void);
+/* FP64 FMA throughput of the current device in TFLOP/s, measured with a
+ * dependent-chain DFMA kernel over all SMs (a roofline denominator; the
+ * device's peak files carry no FP64 figure) */
+exa_status_t exa_measure_fp64_peak(double* tflops);
+/* DRAM copy bandwidth (read + write bytes / time) in GB/s over `bytes` */
+exa_status_t exa_measure_copy_bandwidth(size_t bytes, double* gbs);
+
+/* ---------------------------------- ADER-DG: per-cell drop-ins (host) --
+ * Same argument lists and semantics as the generated solver methods; the
+ * buffers are HOST pointers for one cell.  Each call copies to the device,
+ * runs the batched kernel on one cell and copies back (synchronous).  They
+ * exist for semantic equivalence with the reference; throughput callers use
+ * the batched device entry points below. */
+
+/* Abstract<Solver>::spaceTimePredictor
+ * (AbstractGenericADERDGSolverImplementation.template:50-124) ->
+ * kernels::aderdg::generic::c::spaceTimePredictorNonlinear
+ * (kernels/aderdg/generic/c/3d/spaceTimePredictorNonlinear.cpph:523-577).
+ * Writes lQhbnd, lFhbnd, tempUnknowns (lQhi) and tempFluxUnknowns (lFhi);
+ * if non-NULL also tempSpaceTimeUnknowns[0] (lQi) and
+ * tempSpaceTimeFluxUnknowns[0] (lFi).  tempStateSizedVectors and
+ * pointForceSources are ignored (no point sources in this PDE). */
+exa_status_t exa_aderdg_spaceTimePredictor(
+    const exa_aderdg_desc_t* desc, double* lQhbnd, double* lFhbnd,
+    double** tempSpaceTimeUnknowns, double** tempSpaceTimeFluxUnknowns,
+    double* tempUnknowns, double* tempFluxUnknowns,
+    double* tempStateSizedVectors, const double* luh, const double* dx,
+    double dt, double* pointForceSources, int* picardIterations);
+
+/* Abstract<Solver>::volumeIntegral -> volumeIntegralNonlinear
+ * (kernels/aderdg/generic/c/3d/volumeIntegralNonlinear.cpph:26-125) */
+exa_status_t exa_aderdg_volumeIntegral(const exa_aderdg_desc_t* desc,
+                                       double* lduh, const double* lFhi,
+                                       const double* dx);
+
+/* Abstract<Solver>::surfaceIntegral -> surfaceIntegralNonlinear
+ * (kernels/aderdg/generic/c/3d/surfaceIntegralNonlinear.cpph:21-85) */
+exa_status_t exa_aderdg_surfaceIntegral(const exa_aderdg_desc_t* desc,
+                                        double* lduh, const double* lFhbnd,
+                                        const double* dx);
+
+/* Abstract<Solver>::riemannSolver -> riemannSolverNonlinear<false>
+ * (kernels/aderdg/generic/c/3d/riemannSolverNonlinear.cpph:37-120).
+ * Rusanov flux; overwrites FL and FR in place with the numerical flux. */
+exa_status_t exa_aderdg_riemannSolver(
+    const exa_aderdg_desc_t* desc, double* FL, double* FR, const double* QL,
+    const double* QR, double* tempFaceUnknownsArray,
+    double** tempStateSizedVectors, double** tempStateSizedSquareMatrices,
+    double dt, int normalNonZeroIndex, int isBoundaryFace);
+
+/* Abstract<Solver>::solutionUpdate -> solutionUpdate
+ * (kernels/aderdg/generic/c/3d/solutionUpdate.cpph:23-47) */
+exa_status_t exa_aderdg_solutionUpdate(const exa_aderdg_desc_t* desc,
+                                       double* luh, const double* lduh,
+                                       double dt);
+
+/* Abstract<Solver>::stableTimeStepSize -> stableTimeStepSize
+ * (kernels/aderdg/generic/c/3d/stableTimeStepSize.cpph:21-61), CFL 0.9 */
+exa_status_t exa_aderdg_stableTimeStepSize(const exa_aderdg_desc_t* desc,
+                                           const double* luh,
+                                           double* tempEigenvalues,
+                                           const double* dx, double* dt_out);
+
+/* ------------------------------ ADER-DG: batched device entry points --
+ * Device pointers, `ncells` cells back to back, asynchronous on stream. */
+
+/* spaceTimePredictor + volumeIntegral for every cell, fused
+ * (ADERDGSolver::performPredictionAndVolumeIntegral, ADERDGSolver.cpp:
+ * 1818-1946).  dt is read from *dt_dev when dt_dev != NULL, else `dt`.
+ * picard_iters (nullable) receives the iterations per cell; stats
+ * (nullable, 2 x uint64 on the device) accumulates {sum of iterations,
+ * cells that did not converge}. */
+exa_status_t exa_aderdg_predictor_vi(const exa_aderdg_desc_t* desc, long ncells,
+                                     const double* luh, double dt,
+                                     const double* dt_dev, double* lduh,
+                                     double* lQhbnd, double* lFhbnd,
+                                     int* picard_iters, uint64_t* stats,
+                                     void* stream);
+
+/* Same as above but also writes the reference's temporaries per cell:
+ * lQi [z][y][x][t][nData], lFi [t][z][y][x][dim+1][nVar], lQhi, lFhi. */
+exa_status_t exa_aderdg_predictor_full(const exa_aderdg_desc_t* desc, long ncells,
+                                       const double* luh, double dt,
+                                       double* lQi, double* lFi, double* lQhi,
+                                       double* lFhi, double* lduh, double* lQhbnd,
+                                       double* lFhbnd, int* picard_iters,
+                                       void* stream);
+
+/* volumeIntegralNonlinear for every cell (lFhi in reference layout). */
+exa_status_t exa_aderdg_volume_integral(const exa_aderdg_desc_t* desc, long ncells,
+                                        double* lduh, const double* lFhi,
+                                        void* stream);
+
+/* surfaceIntegralNonlinear for every cell. */
+exa_status_t exa_aderdg_surface_integral(const exa_aderdg_desc_t* desc, long ncells,
+                                         double* lduh, const double* lFhbnd,
+                                         void* stream);
+
+/* solutionUpdate for every cell. */
+exa_status_t exa_aderdg_solution_update(const exa_aderdg_desc_t* desc, long ncells,
+                                        double* luh, const double* lduh,
+                                        double dt, void* stream);
+
+/* Riemann solver on an explicit list of faces (ADERDGSolver::
+ * solveRiemannProblemAtInterface, ADERDGSolver.cpp:2744-2826): face k joins
+ * the face 2*dir+1 of cell left[k] and the face 2*dir of cell right[k];
+ * both lFhbnd face blocks are overwritten with the Rusanov flux. */
+exa_status_t exa_aderdg_riemann_faces(const exa_aderdg_desc_t* desc, long nfaces,
+                                      const int* left, const int* right,
+                                      const int* dir, const double* lQhbnd,
+                                      double* lFhbnd, void* stream);
+
+/* stableTimeStepSize for every cell; dt_cell (nullable) per cell, dt_min
+ * (nullable, one double) receives the minimum over all cells (the global
+ * min-reduction of TimeStepSizeComputation.cpp:83-109,204). */
+exa_status_t exa_aderdg_stable_dt(const exa_aderdg_desc_t* desc, long ncells,
+                                  const double* luh, double* dt_cell,
+                                  double* dt_min, void* stream);
+
+/* ------------------------------------ ADER-DG: uniform periodic grid --
+ * The Peano spacetree is replaced by a uniform periodic cell array on one
+ * GPU.  A step is dt -> predictor+VI -> Riemann -> SI -> update in the
+ * reference's non-fused order (Runner.cpp:1125-1160); on the device the
+ * Riemann solve, surface integral, update and the next step's dt
+ * reduction are one fused kernel. */
+typedef struct exa_aderdg_grid exa_aderdg_grid;
+
+typedef struct {
+  int dim, order;
+  int n[3];            /* cells per dimension */
+  double length[3];    /* domain extent; dx = length/n */
+  int pde, precision;
+  int dt_policy;       /* 0: CFL*PNPM[N] (reference), 1: CFL/(2N+1), 2: fixed */
+  double cfl;          /* 0.9 in the reference's generated solvers */
+  double dt_fixed;
+} exa_aderdg_grid_config_t;
+
+exa_status_t exa_aderdg_grid_create(const exa_aderdg_grid_config_t* cfg,
+                                    exa_aderdg_grid** out);
+exa_status_t exa_aderdg_grid_destroy(exa_aderdg_grid* g);
+/* bytes of device memory a grid with this config needs */
+size_t exa_aderdg_grid_footprint(const exa_aderdg_grid_config_t* cfg);
+/* nodal initial condition on the device: kind 0 isentropic vortex
+ * (param = strength), kind 1 density sine wave (param = amplitude); both
+ * with seeded uniform density noise of relative amplitude noise_amp. */
+exa_status_t exa_aderdg_grid_init(exa_aderdg_grid* g, int kind, double param,
+                                  uint64_t seed, double noise_amp);
+exa_status_t exa_aderdg_grid_set_state(exa_aderdg_grid* g, const double* host_luh);
+exa_status_t exa_aderdg_grid_get_state(exa_aderdg_grid* g, double* host_luh);
+/* advance nsteps; dt_host (nullable) receives nsteps dt values (forces a
+ * device->host read at the end).  Returns EXA_ENAN / EXA_ENONCONV
+ * conditions through exa_aderdg_grid_status. */
+exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_host);
+/* capture one step pair in a CUDA graph and replay it for later steps */
+exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable);
+exa_status_t exa_aderdg_grid_stream(exa_aderdg_grid* g, void** stream);
+/* per-phase CUDA-event timing of every step (disables graph replay):
+ * predictor (k_predictor) and corrector (k_corrector + k_commit) */
+exa_status_t exa_aderdg_grid_profile(exa_aderdg_grid* g, int enable);
+exa_status_t exa_aderdg_grid_phase_times(exa_aderdg_grid* g, double* ms_predictor,
+                                         double* ms_corrector, uint64_t* steps);
+exa_status_t exa_aderdg_grid_device_state(exa_aderdg_grid* g, double** luh_dev);
+/* time, accumulated Picard iterations, non-converged cell count, NaN flag */
+exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time,
+                                    uint64_t* picard_iters_sum,
+                                    uint64_t* nonconverged, int* nan_flag);
+long exa_aderdg_grid_ncells(const exa_aderdg_grid* g);
+
+/* ------------------------------------------------ finite volumes (2D) --
+ * One patch of patch x patch cells with `ghost` ghost layers, layout
+ * [y][x][nData] over (patch+2*ghost)^2 cells (reference FV solvers,
+ * PatchSize / GhostLayerWidth, AbstractGenericFiniteVolumesSolverHeader.
+ * template:30-34).  Batched over `npatches` patches back to back. */
+typedef struct {
+  int dim;      /* 2 */
+  int patch;    /* PatchSize */
+  int ghost;    /* 1 for Godunov, 2 for MUSCL-Hancock */
+  int nvar, npar, pde;
+  double dx[3]; /* patch extent (cell size = dx/patch) */
+} exa_fv_desc_t;
+
+/* godunov::c::solutionUpdate (kernels/finitevolumes/godunov/c/2d/
+ * godunov.cpph:33-120): luh_new (a copy of luh on entry) is advanced in
+ * place; max_dt (nullable, device, one double per patch) receives the
+ * admissible dt.  Rusanov faces (riemannsolvers/c/rusanov.cpph:24-83). */
+exa_status_t exa_fv_godunov_update(const exa_fv_desc_t* desc, long npatches,
+                                   double* luh_new, const double* luh,
+                                   double dt, double* max_dt, void* stream);
+/* musclhancock::c::solutionUpdate (kernels/finitevolumes/musclhancock/c/
+ * 2d/musclhancock.cpph:50-240), CFL 0.99 for max_dt. */
+exa_status_t exa_fv_musclhancock_update(const exa_fv_desc_t* desc, long npatches,
+                                        double* luh_new, const double* luh,
+                                        double dt, double* max_dt, void* stream);
+/* commons::c::stableTimeStepSize (commons/c/commons.cpph:26-67), per patch */
+exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches,
+                              const double* luh, double* dt_patch, void* stream);
+/* fills the ghost layers of every patch periodically from itself */
+exa_status_t exa_fv_periodic_ghosts(const exa_fv_desc_t* desc, long npatches,
+                                    double* luh, void* stream);
+/* rusanov (riemannsolvers/c/rusanov.cpph:24-83), host drop-in, returns s_max */
+exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL,
+                            double* fR, const double* qL, const double* qR,
+                            int normalNonZero, double* s_max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXA_KERNELS_H */

@@ -629,6 +629,49 @@ double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
   return dt;
 }
 
+/* One step's per-cell work on `ncells` independent cells (CPU-baseline
+ * sample): predictor + volume integral, one Riemann solve per direction
+ * (the cell's +d face against its own -d face, i.e. a one-cell periodic
+ * domain), surface integral and update.  Same operation count per cell as
+ * orc_aderdg_grid_step. */
+void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,
+                            const double* dx, double* luh, double dt,
+                            int nthreads) {
+  const int B = order + 1, V = 5;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const int nst = nn * B, nfn = dim == 3 ? B * B : B, fs = nfn * V;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel
+  {
+    double* lQi = (double*)malloc(sizeof(double) * nst * V);
+    double* lQo = (double*)malloc(sizeof(double) * nst * V);
+    double* rhs = (double*)malloc(sizeof(double) * nst * V);
+    double* lFi = (double*)malloc(sizeof(double) * nst * (dim + 1) * V);
+    double* lQhi = (double*)malloc(sizeof(double) * nn * V);
+    double* lFhi = (double*)malloc(sizeof(double) * nn * (dim + 1) * V);
+    double* lduh = (double*)malloc(sizeof(double) * nn * V);
+    double* qb = (double*)malloc(sizeof(double) * 2 * dim * fs);
+    double* fb = (double*)malloc(sizeof(double) * 2 * dim * fs);
+#pragma omp for schedule(dynamic, 16)
+    for (long c = 0; c < ncells; c++) {
+      double* u = luh + c * nn * V;
+      orc_stp_nonlinear(dim, order, V, 0, planar, qb, fb, lQi, lQo, rhs, lFi, lQhi, lFhi, u, dx, dt);
+      orc_volume_integral(dim, order, V, 0, lduh, lFhi, dx);
+      for (int d = 0; d < dim; d++)
+        orc_riemann(dim, order, V, 0, planar, fb + (2 * d + 1) * fs, fb + (2 * d) * fs,
+                    qb + (2 * d + 1) * fs, qb + (2 * d) * fs, d);
+      orc_surface_integral(dim, order, V, lduh, fb, dx);
+      orc_solution_update(dim, order, V, 0, u, lduh, dt);
+    }
+    free(lQi); free(lQo); free(rhs); free(lFi); free(lQhi); free(lFhi);
+    free(lduh); free(qb); free(fb);
+  }
+}
+
 /* ------------------------------------------------------------------ */
 /* Counter-based noise: splitmix64 of (seed, index). */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx) {

@@ -68,6 +68,11 @@ double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
                             const double* dx, double* luh, int dt_policy,
                             double cfl, double dt_fixed, int* iters,
                             int nthreads);
+/* CPU-baseline sample: one step's per-cell work on ncells independent
+ * cells (each its own periodic neighbour). */
+void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,
+                            const double* dx, double* luh, double dt,
+                            int nthreads);
 /* Nodal initial condition on the grid: isentropic vortex / sine wave with
  * seeded density noise.  kind: 0 = isentropic vortex (u=v=1 background,
  * strength eps), 1 = density sine rho=1+amp*sin(2 pi (x+y)), u=v=1, p=1. */

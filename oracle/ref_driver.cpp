@@ -214,6 +214,31 @@ struct DG {
     }
     return dtv;
   }
+  /* per-cell work of one step on ncells independent cells (each its own
+   * periodic neighbour): the CPU-baseline sample */
+  static void sample_step(long nc, const double* dx, double* luh, double dtv, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel
+    {
+      Temps t;
+      std::vector<double> lduh(NN * V), qb(2 * DIMENSIONS * NF * D), fb(2 * DIMENSIONS * NF * V);
+#pragma omp for schedule(dynamic, 16)
+      for (long c = 0; c < nc; c++) {
+        double* u = luh + c * NN * D;
+        stp(u, nullptr, nullptr, nullptr, qb.data(), fb.data(), dx, dtv, t);
+        vi(lduh.data(), t.fhi.data(), dx);
+        for (int d = 0; d < DIMENSIONS; d++)
+          riemann(fb.data() + (2 * d + 1) * NF * V, fb.data() + (2 * d) * NF * V,
+                  qb.data() + (2 * d + 1) * NF * D, qb.data() + (2 * d) * NF * D, d);
+        si(lduh.data(), fb.data(), dx);
+        update(u, lduh.data(), dtv);
+      }
+    }
+  }
   static double kernels_pnpm() {
     static const double pnpm[10] = {1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015};
     return pnpm[N];
@@ -322,6 +347,14 @@ double ref_stable_dt(int order, int npar, const double* luh, const double* dx) {
 double ref_grid_step(int order, const int* n, const double* dx, double* luh, int policy,
                      double dt_fixed, int nthreads) {
 #define CASE(N) case N: return DG<N, 0>::grid_step(n, dx, luh, policy, dt_fixed, nthreads);
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+int ref_sample_step(int order, long ncells, const double* dx, double* luh, double dt,
+                    int nthreads) {
+#define CASE(N) case N: DG<N, 0>::sample_step(ncells, dx, luh, dt, nthreads); return 0;
   switch (order) { EXA_ORDERS(CASE) }
 #undef CASE
   return -1;

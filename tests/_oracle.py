@@ -59,6 +59,7 @@ def lib():
     L.orc_fv_periodic_ghosts_2d.argtypes = [i, i, i, _dp]
     L.orc_fv_patch_step_2d.restype = d
     L.orc_fv_patch_step_2d.argtypes = [i, i, i, _dp, _dp, d, C.c_void_p]
+    L.orc_aderdg_sample_step.argtypes = [i, i, i, C.c_long, _dp, _dp, d, i]
     L.orc_noise_u01.restype = d
     L.orc_noise_u01.argtypes = [C.c_ulonglong, C.c_ulonglong]
     _lib = L
@@ -139,6 +140,8 @@ def ref_lib(dim):
         L.ref_stable_dt.argtypes = [i, i, _dp, _dp]
         L.ref_grid_step.restype = d
         L.ref_grid_step.argtypes = [i, _ip, _dp, _dp, i, d, i]
+        L.ref_sample_step.restype = i
+        L.ref_sample_step.argtypes = [i, C.c_long, _dp, _dp, d, i]
         if dim == 2:
             L.ref_fv_step.restype = d
             L.ref_fv_step.argtypes = [i, i, _dp, _dp, d, C.c_void_p]
