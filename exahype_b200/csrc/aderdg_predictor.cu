@@ -38,9 +38,10 @@ struct PredShape {
   static constexpr int G = CellThreads<NPC>::G;   // threads per cell
   static constexpr int CPB = DIM == 3 ? 1 : (128 / G > 0 ? 128 / G : 1);
   static constexpr int NT = G * CPB;
-  // shared memory per cell: flux slice / time-averaged flux [DIM][NPC][V]
-  // and time-averaged state [NPC][D]
-  static constexpr int SM_CELL = DIM * NPC * V + NPC * D;
+  // shared memory per cell: two flux-slice buffers [2][DIM][NPC][V] (the
+  // second doubles as the time-averaged state [NPC][D] after the loop)
+  static constexpr int SM_CELL = 2 * DIM * NPC * V > DIM * NPC * V + NPC * D
+                                     ? 2 * DIM * NPC * V : DIM * NPC * V + NPC * D;
   static constexpr int SM_DOUBLES = CPB * SM_CELL + NT / 32 + 1;
 };
 
@@ -59,7 +60,7 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
   const bool valid = cell < a.ncells;
   const bool active = valid && s < NPC;
   double* sF = smem + lc * S::SM_CELL;      // [DIM][NPC][V]
-  double* sQh = sF + DIM * NPC * V;         // [NPC][D]
+  double* sQh = sF + DIM * NPC * V;         // [NPC][D] (after the loop)
   double* sred = smem + S::CPB * S::SM_CELL;
 
   // node coordinates: sd[0]=x, sd[1]=y, sd[2]=z
@@ -98,14 +99,22 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
     for (int t = 0; t < B; t++)
 #pragma unroll
       for (int m = 0; m < V; m++) acc[t][m] = 0.0;
-    double fhn[DIM][V];
+    // time-averaged flux of this iteration; a cell that converged earlier
+    // than its CTA neighbours keeps its fh (only possible when CPB > 1)
+    constexpr bool kShared = S::CPB > 1;
+    double fhn[kShared ? DIM : 1][V];
+    double(*fa)[V] = kShared ? fhn : fh;
 #pragma unroll
     for (int d = 0; d < DIM; d++)
 #pragma unroll
-      for (int m = 0; m < V; m++) fhn[d][m] = 0.0;
+      for (int m = 0; m < V; m++) fa[d][m] = 0.0;
 
 #pragma unroll
     for (int n = 0; n < B; n++) {
+      // alternate the two slice buffers: a thread writing slice n+1 has
+      // passed the barrier of slice n, which every thread reaches only after
+      // it finished reading slice n-1 (the buffer being overwritten)
+      double* sFn = sF + ((iter * B + n) & 1) * (DIM * NPC * V);
       double F[DIM][V];
       if (active) {
         double qq[5] = {q[n][0], q[n][1], q[n][2], q[n][3], q[n][4]};
@@ -116,15 +125,17 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
 #pragma unroll
           for (int m = 0; m < V; m++) F[d][m] = 0.0;
       }
+      if (!conv) {
 #pragma unroll
-      for (int d = 0; d < DIM; d++)
+        for (int d = 0; d < DIM; d++)
 #pragma unroll
-        for (int m = 0; m < V; m++) fhn[d][m] += T.w[n] * F[d][m];
+          for (int m = 0; m < V; m++) fa[d][m] += T.w[n] * F[d][m];
+      }
       if (active) {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) sF[(d * NPC + s) * V + m] = F[d][m];
+          for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = F[d][m];
         if (FULL && !conv) {
           double* lFi = a.lFi + cell * (long)NPC * B * (DIM + 1) * V;
 #pragma unroll
@@ -142,7 +153,7 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
         for (int m = 0; m < V; m++) Gm[m] = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          const double* line = sF + (d * NPC + s - sd[d] * stride[d]) * V;
+          const double* line = sFn + (d * NPC + s - sd[d] * stride[d]) * V;
 #pragma unroll
           for (int p = 0; p < B; p++) {
             const double c = dc[d][p];
@@ -155,7 +166,6 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
 #pragma unroll
           for (int m = 0; m < V; m++) acc[t][m] += T.tA[t][n] * Gm[m];
       }
-      __syncthreads();
     }
 
     // new iterate and squared increment
@@ -170,10 +180,12 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
           r += dq * dq;
           q[t][m] = qn;
         }
+      if (kShared) {
 #pragma unroll
-      for (int d = 0; d < DIM; d++)
+        for (int d = 0; d < DIM; d++)
 #pragma unroll
-        for (int m = 0; m < V; m++) fh[d][m] = fhn[d][m];
+          for (int m = 0; m < V; m++) fh[d][m] = fa[d][m];
+      }
     }
     const double res = group_sum<G>(r, sred);
     if (!conv) {
@@ -184,6 +196,7 @@ __global__ void __launch_bounds__(PredShape<DIM, N, NPAR>::NT)
   }
 
   // ---- outputs --------------------------------------------------------
+  __syncthreads();  // last slice's derivative reads are done before reuse
   if (active) {
 #pragma unroll
     for (int m = 0; m < V; m++) {
