@@ -261,6 +261,9 @@ def main():
     ap.add_argument('--seed', type=int, default=2024)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-mixed', action='store_true')
+    ap.add_argument('--tune', action='append', default=[],
+                    help='key=value tuning knob passed to exa_tune_set (see include/exa_kernels.h)')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
 
@@ -281,14 +284,10 @@ def main():
         return
 
     import exahype_b200 as E
-    from exahype_b200 import Timer
     E.lib().exa_set_device(local)
-    n, order = args.n, args.order
-    prec = E.PREC_MIXED if args.precision == 'mixed' else E.PREC_FP64
-    grid = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
-    grid.init(kind=0, param=5.0, seed=args.seed + rank, noise=1e-3)
-    stream = grid.stream()
-
+    for kv in args.tune:
+        k, v = kv.split('=')
+        E._lib.call('exa_tune_set', int(k), int(v))
     import ctypes as C
     fp64_peak = C.c_double()
     E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))
@@ -306,13 +305,70 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    initial = grid.get_state()
+    ctx = dict(E=E, args=args, rank=rank, world=world, local=local, barrier=barrier,
+               max_over_ranks=max_over_ranks, fp64_peak=fp64_peak.value)
+    primary = 'mixed' if args.precision == 'mixed' else 'fp64'
+    res = measure(ctx, primary, with_e2e=not args.no_e2e)
+    other = None
+    if args.precision == 'fp64' and not args.no_mixed:
+        other = measure(ctx, 'mixed', with_e2e=False)
+        other['accuracy'] = mixed_accuracy(ctx, steps=min(50, args.warmup + args.steps))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample, _ = cpu_sample(args.order, args.n, res['state'], res['dt'], budget_s=15.0)
+        cpu = {'value': v, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind, 'sample': sample}
+
+    if rank == 0:
+        ncells = res['ncells']
+        line = {
+            'metric': METRIC, 'value': res['value'], 'unit': 'cell-updates/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': res['ms_per_step'],
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f64' if primary == 'fp64' else 'f64+f32', 'data': 'synthetic',
+            'config': config_dict(args, world),
+            'roofline': res['roofline'],
+            'roofline_hbm': {
+                'achieved': bytes_per_cell_update(3, args.order) * ncells / (res['ms_per_step'] * 1e-3) / 1e9,
+                'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s', 'peak_source': peak_src,
+                'bytes_per_cell_update': bytes_per_cell_update(3, args.order)},
+            'flop_per_cell_update': res['flop_per_cell_update'],
+            'cpu_baseline': cpu,
+            'e2e': res.get('e2e'),
+            'gpu_launches': res['launches'],
+            'clocks': res['clocks'],
+        }
+        if other is not None:
+            line['mixed'] = {
+                'value': other['value'], 'unit': 'cell-updates/s', 'ms_per_step': other['ms_per_step'],
+                'speedup_vs_fp64': other['value'] / res['value'], 'roofline': other['roofline'],
+                'accuracy_vs_fp64': other['accuracy'], 'gpu_launches': other['launches'],
+                'clocks': other['clocks'],
+                'form': 'Picard deviations dq = q - luh and dF = F(q) - F(luh) in FP32 (FP32 accumulate); '
+                        'luh, F(luh) and its derivative, the update, Riemann fluxes, faces and dt in FP64'}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure(ctx, precision, with_e2e):
+    """Time K steps of the grid on this rank (W untimed warm-up steps
+    first); returns the rank-0 view of the numbers."""
+    E, args = ctx['E'], ctx['args']
+    from exahype_b200 import Timer
+    n, order = args.n, args.order
+    prec = E.PREC_MIXED if precision == 'mixed' else E.PREC_FP64
+    grid = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
+    grid.init(kind=0, param=5.0, seed=args.seed + ctx['rank'], noise=1e-3)
+    stream = grid.stream()
+    initial = grid.get_state() if with_e2e else None
     grid.step(args.warmup)
     st0 = grid.status()
     grid.profile(True)
     E.device.synchronize()
-    barrier()
-    clocks = ClockSampler(local)
+    ctx['barrier']()
+    clocks = ClockSampler(ctx['local'])
     clocks.start()
     timer = Timer()
     l0 = E.launch_count()
@@ -322,81 +378,83 @@ def main():
     ms = timer.elapsed_ms()
     E.device.synchronize()
     launches = E.launch_count() - l0
-    barrier()
+    ctx['barrier']()
     clk = clocks.stop()
     st1 = grid.status()
     phases = grid.phase_times()
-    ms_max = max_over_ranks(ms)
+    ms_max = ctx['max_over_ranks'](ms)
     ncells = grid.ncells
-    value = world * ncells * args.steps / (ms_max * 1e-3)
+    value = ctx['world'] * ncells * args.steps / (ms_max * 1e-3)
     kbar = (st1['picard_iters'] - st0['picard_iters']) / (ncells * args.steps)
     total_flop, pred_flop = flops_per_cell_update(3, order, kbar)
     pred_ms = phases['predictor_ms'] / max(1, phases['steps'])
-    achieved_tf = pred_flop * ncells / (pred_ms * 1e-3) / 1e12
-    traffic_pc = ncu_traffic_per_cell()
-
-    # ---- end to end through the public API with host buffers
-    e2e = None
-    if not args.no_e2e:
+    achieved = pred_flop * ncells / (pred_ms * 1e-3) / 1e12
+    traffic_pc = ncu_traffic_per_cell() if precision == 'fp64' else None
+    out = dict(value=value, ms_per_step=ms_max / args.steps, ncells=ncells, launches=launches, clocks=clk,
+               flop_per_cell_update=total_flop)
+    if precision == 'fp64':
+        out['roofline'] = {
+            'kernel': 'k_predictor', 'bound': 'fp64', 'achieved': achieved, 'peak': ctx['fp64_peak'],
+            'unit': 'TFLOP/s', 'frac': achieved / ctx['fp64_peak'],
+            'peak_source': 'DFMA probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)',
+            'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
+            'traffic': (traffic_pc * ncells if traffic_pc else None), 'ms_per_launch': pred_ms,
+            'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}
+    else:
+        out['roofline'] = {
+            'kernel': 'k_predictor_mixed', 'bound': 'fp64+fp32', 'achieved_equiv_fp64_flop': achieved,
+            'unit': 'TFLOP/s', 'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
+            'ms_per_launch': pred_ms, 'frac_of_fp64_peak': achieved / ctx['fp64_peak'],
+            'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}
+    if with_e2e:
         from exahype_b200 import PinnedBuffer
         pin = PinnedBuffer(grid.state_size)
         pin.array[:] = initial
         grid.profile(False)
-        barrier()
+        ctx['barrier']()
         t2 = Timer()
         t2.start(stream)
         E._lib.call('exa_aderdg_grid_set_state', grid.h, pin.array.ctypes.data)
-        dts = []
         for _ in range(args.steps):
-            dts.append(grid.step(1, want_dt=True)[0])
+            grid.step(1, want_dt=True)
         E._lib.call('exa_aderdg_grid_get_state', grid.h, pin.array.ctypes.data)
         t2.stop(stream)
-        ms_e2e = max_over_ranks(t2.elapsed_ms())
-        barrier()
+        ms_e2e = ctx['max_over_ranks'](t2.elapsed_ms())
+        ctx['barrier']()
         sb = grid.state_size * 8
-        e2e = {'value': world * ncells * args.steps / (ms_e2e * 1e-3), 'unit': 'cell-updates/s',
-               'h2d_bytes_per_step': sb / args.steps, 'd2h_bytes_per_step': 8 + sb / args.steps,
-               'note': 'one solve per timed region: state upload from pinned host memory, K steps each '
-                       'returning its dt to the host, final state download'}
+        out['e2e'] = {'value': ctx['world'] * ncells * args.steps / (ms_e2e * 1e-3), 'unit': 'cell-updates/s',
+                      'h2d_bytes_per_step': sb / args.steps, 'd2h_bytes_per_step': 8 + sb / args.steps,
+                      'note': 'one solve per timed region: state upload from pinned host memory, K steps each '
+                              'returning its dt to the host, final state download'}
         pin.free()
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        st = grid.get_state()
-        dt_now = grid.step(1, want_dt=True)[0]
-        v, kind, cores, sample, _ = cpu_sample(order, n, st, dt_now, budget_s=15.0)
-        cpu = {'value': v, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind, 'sample': sample}
-
-    if rank == 0:
-        line = {
-            'metric': METRIC, 'value': value, 'unit': 'cell-updates/s', 'n_gpus': world, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': ms_max / args.steps, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': config_dict(args, world),
-            'roofline': {
-                'kernel': 'k_predictor', 'bound': 'fp64', 'achieved': achieved_tf,
-                'peak': fp64_peak.value, 'unit': 'TFLOP/s', 'frac': achieved_tf / fp64_peak.value,
-                'peak_source': 'DFMA probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)',
-                'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
-                'traffic': (traffic_pc * ncells if traffic_pc else None),
-                'ms_per_launch': pred_ms,
-                'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms']),
-            },
-            'roofline_hbm': {
-                'achieved': bytes_per_cell_update(3, order) * ncells * args.steps / (ms * 1e-3) / 1e9,
-                'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s', 'peak_source': peak_src,
-                'bytes_per_cell_update': bytes_per_cell_update(3, order)},
-            'flop_per_cell_update': total_flop,
-            'cpu_baseline': cpu,
-            'e2e': e2e,
-            'gpu_launches': launches,
-            'clocks': clk,
-        }
-        print(json.dumps(line), flush=True)
+    if ctx['rank'] == 0 and precision == 'fp64':
+        out['state'] = grid.get_state()
+        out['dt'] = grid.step(1, want_dt=True)[0]
     grid.destroy()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    return out
+
+
+def mixed_accuracy(ctx, steps):
+    """Relative L2 / Linf of the mixed-precision state against the FP64 path
+    after every step, both started from the identical state."""
+    E, args = ctx['E'], ctx['args']
+    from exahype_b200.device import diff_norms
+    n, order = args.n, args.order
+    a = E.ADERDGGrid(3, order, (n, n, n), precision=E.PREC_FP64)
+    b = E.ADERDGGrid(3, order, (n, n, n), precision=E.PREC_MIXED)
+    for g in (a, b):
+        g.init(kind=0, param=5.0, seed=args.seed + ctx['rank'], noise=1e-3)
+    l2, linf = [], []
+    for _ in range(steps):
+        a.step(1)
+        b.step(1)
+        e = diff_norms(b.device_state_ptr(), a.device_state_ptr(), a.state_size)
+        l2.append(e['rel_l2'])
+        linf.append(e['rel_linf'])
+    a.destroy()
+    b.destroy()
+    return {'steps': steps, 'rel_l2_per_step': l2, 'rel_linf_per_step': linf, 'max_rel_l2': max(l2),
+            'max_rel_linf': max(linf), 'target_rel_l2': 1e-8}
 
 
 if __name__ == '__main__':

@@ -364,6 +364,7 @@ static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int
 
 exa_status_t launch_predictor(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
                               cudaStream_t st) {
+  if (!full && d.precision == EXA_PREC_MIXED) return launch_predictor_mixed(d, a, st);
   if (d.dim == 3) {
     switch (d.order) {
       case 2: return launch_dn<3, 2>(d, a, full, st);

@@ -30,6 +30,14 @@ exa_status_t cuda_status(cudaError_t e, const char* where) {
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<int> g_tune[kTuneCount] = {};
+static std::atomic<unsigned> g_tune_set{0};
+
+int tune_get(int key, int dflt) {
+  if (key < 0 || key >= kTuneCount) return dflt;
+  return (g_tune_set.load() >> key) & 1u ? g_tune[key].load() : dflt;
+}
+
 double host_pnpm(int order);
 
 static std::mutex g_tables_mu;
@@ -43,6 +51,7 @@ exa_status_t ensure_tables() {
   if (g_tables_done[dev & 255]) return EXA_OK;
   exa_status_t s;
   if ((s = upload_tables_predictor())) return s;
+  if ((s = upload_tables_predictor_mixed())) return s;
   if ((s = upload_tables_faces())) return s;
   if ((s = upload_tables_fv())) return s;
   g_tables_done[dev & 255] = true;
@@ -220,6 +229,15 @@ exa_status_t exa_timer_elapsed_ms(void* timer, float* ms) {
   return cuda_status(e, "event elapsed");
 }
 uint64_t exa_launch_count(void) { return g_launches.load(); }
+
+exa_status_t exa_tune_set(int key, int value) {
+  if (key < 0 || key >= kTuneCount) return set_error(EXA_EINVAL, "unknown tuning key");
+  g_tune[key].store(value);
+  g_tune_set.fetch_or(1u << key);
+  return EXA_OK;
+}
+
+int exa_tune_get(int key) { return tune_get(key, -1); }
 
 // --------------------------------------------------- per-cell drop-ins
 static exa_aderdg_desc_t with_dx(const exa_aderdg_desc_t* d, const double* dx) {

@@ -7,6 +7,10 @@
 
 namespace exa {
 
+// Process-wide tuning knobs (set through exa_tune_set, read by launchers).
+enum TuneKey { kTuneMixedOccupancy = 0, kTuneFp64Occupancy = 1, kTuneCount = 8 };
+int tune_get(int key, int dflt);
+
 // Records a CUDA error (message retrievable by exa_last_error_string) and
 // maps it to EXA_ECUDA.
 exa_status_t cuda_status(cudaError_t e, const char* where);
@@ -40,6 +44,7 @@ struct PredArgs {
 
 exa_status_t launch_predictor(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
                               cudaStream_t st);
+exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& a, cudaStream_t st);
 
 // fused Riemann + surface integral + update + next-dt on a uniform periodic grid
 struct CorrArgs {
@@ -78,6 +83,7 @@ exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* 
 
 // table uploads, one per translation unit holding kernels
 exa_status_t upload_tables_predictor();
+exa_status_t upload_tables_predictor_mixed();
 exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 // host copy of the derived tables (same bytes as the device constants)

@@ -132,3 +132,11 @@ def launch_count():
 
 def synchronize():
     call('exa_device_synchronize')
+
+
+def diff_norms(a_ptr, b_ptr, n, stream=None):
+    """Relative L2 / Linf of device array a against b (n doubles), computed on
+    the device; returns dict(rel_l2, rel_linf, abs_l2, abs_linf)."""
+    out = (C.c_double * 4)()
+    call('exa_diff_norms', a_ptr, b_ptr, int(n), out, stream)
+    return dict(rel_l2=out[0], rel_linf=out[1], abs_l2=out[2], abs_linf=out[3])

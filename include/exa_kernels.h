@@ -100,10 +100,20 @@ exa_status_t exa_timer_stop(void* timer, void* stream);
 exa_status_t exa_timer_elapsed_ms(void* timer, float* ms);
 /* number of kernels this library has launched in this process */
 uint64_t exa_launch_count(void);
+/* Tuning knobs chosen by the autotuner (exahype_b200/autotune.py) or the
+ * user; process-wide.  Keys: 0 = register budget of the 3D order-4 mixed
+ * predictor (1: cap for 3 CTAs/SM, 0: unconstrained), 1 = the same for the
+ * FP64 predictor.  exa_tune_get returns -1 for keys never set. */
+exa_status_t exa_tune_set(int key, int value);
+int exa_tune_get(int key);
 /* FP64 FMA throughput of the current device in TFLOP/s, measured with a
  * dependent-chain DFMA kernel over all SMs (a roofline denominator; the
  * device's peak files carry no FP64 figure) */
 exa_status_t exa_measure_fp64_peak(double* tflops);
+/* Error norms of device array a against reference b (n doubles): out[0]
+ * relative L2 ||a-b||/||b||, out[1] relative Linf max|a-b|/max|b|,
+ * out[2] ||a-b||, out[3] max|a-b|.  Synchronous on stream. */
+exa_status_t exa_diff_norms(const double* a, const double* b, size_t n, double* out, void* stream);
 /* DRAM copy bandwidth (read + write bytes / time) in GB/s over `bytes` */
 exa_status_t exa_measure_copy_bandwidth(size_t bytes, double* gbs);
 
