@@ -446,8 +446,8 @@ def mixed_accuracy(ctx, steps):
         g.init(kind=0, param=5.0, seed=args.seed + ctx['rank'], noise=1e-3)
     l2, linf = [], []
     for _ in range(steps):
-        a.step(1)
-        b.step(1)
+        a.step(1, want_dt=True)  # synchronises the grid's stream
+        b.step(1, want_dt=True)
         e = diff_norms(b.device_state_ptr(), a.device_state_ptr(), a.state_size)
         l2.append(e['rel_l2'])
         linf.append(e['rel_linf'])

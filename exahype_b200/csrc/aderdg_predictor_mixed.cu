@@ -320,7 +320,7 @@ static exa_status_t launch_mixed_t(const PredArgs& a, cudaStream_t st) {
 exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& a, cudaStream_t st) {
   if (d.npar != 0) return set_error(EXA_EINVAL, "mixed precision: npar must be 0");
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
-  const bool occ = tune_get(kTuneMixedOccupancy, 1) != 0;
+  const bool occ = tune_get(kTuneMixedOccupancy, 0) != 0;
   if (d.dim == 3 && !planar) {
     switch (d.order) {
       case 2: return launch_mixed_t<3, 2, false, 1>(a, st);

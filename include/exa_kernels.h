@@ -102,8 +102,8 @@ exa_status_t exa_timer_elapsed_ms(void* timer, float* ms);
 uint64_t exa_launch_count(void);
 /* Tuning knobs chosen by the autotuner (exahype_b200/autotune.py) or the
  * user; process-wide.  Keys: 0 = register budget of the 3D order-4 mixed
- * predictor (1: cap for 3 CTAs/SM, 0: unconstrained), 1 = the same for the
- * FP64 predictor.  exa_tune_get returns -1 for keys never set. */
+ * predictor (1: cap for 3 CTAs/SM, 0: unconstrained, the default), 1 = the
+ * same for the FP64 predictor.  exa_tune_get returns -1 for keys never set. */
 exa_status_t exa_tune_set(int key, int value);
 int exa_tune_get(int key);
 /* FP64 FMA throughput of the current device in TFLOP/s, measured with a
