@@ -4,7 +4,7 @@
  *
  * The entry points mirror the generic C++ kernels of ExaHyPE
  * (ExaHyPE/kernels/aderdg/generic/Kernels.h:86-175,
- * kernels/finitevolumes/{godunov,musclhancock,riemannsolvers,commons}/c/*.h)
+ * kernels/finitevolumes/{godunov,musclhancock,riemannsolvers,commons}/c/)
  * and the solver methods that call them (the toolkit-generated
  * Abstract<Solver>, Toolkit/src/eu/exahype/solvers/templates/
  * AbstractGenericADERDGSolverHeader.template:166-177 and
