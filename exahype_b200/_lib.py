@@ -93,6 +93,8 @@ SIGNATURES = {
     'exa_diff_norms': (i32, [vp, vp, sz, C.POINTER(f64), vp]),
     'exa_aderdg_spaceTimePredictor': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dpp, dpp, dptr, dptr,
                                             dptr, dptr, dptr, f64, dptr, ipt]),
+    'exa_aderdg_spaceTimePredictor_noalloc': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dpp, dpp, dptr,
+                                                    dptr, dptr, dptr, dptr, f64, dptr, ipt]),
     'exa_aderdg_volumeIntegral': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr]),
     'exa_aderdg_surfaceIntegral': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr]),
     'exa_aderdg_riemannSolver': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dptr, dptr, dptr, dpp, dpp,

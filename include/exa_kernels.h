@@ -139,6 +139,28 @@ exa_status_t exa_aderdg_spaceTimePredictor(
     double* tempStateSizedVectors, const double* luh, const double* dx,
     double dt, double* pointForceSources, int* picardIterations);
 
+/* Allocation-free variant of exa_aderdg_spaceTimePredictor (same arguments,
+ * same results).  It has no counterpart in the reference: it exists for
+ * callers that must not trigger a device allocation -- code running while a
+ * CUDA graph is captured (cudaMalloc is not permitted there), many host
+ * threads calling per-cell kernels at once (cudaMalloc/cudaFree take a
+ * device-wide lock and cudaFree synchronises the device), or processes whose
+ * device memory is already handed out by a pool allocator.  The cell is
+ * staged through a file-scope device array of 65536 doubles (512 KiB) that
+ * every GPU holds from library load to process exit; every supported cell
+ * (order 2..5, 2D/3D, nPar <= 1) fits, larger requests get EXA_EINVAL.
+ * The first call on a device performs a one-time set-up (looks up the
+ * array's device address, uploads the operator tables); make that first call
+ * before any stream capture.  All calls on a device share the one array and
+ * keep the last call's contents; calls of this process are serialised by a
+ * lock, any other overlap on the GPU races.  Synchronous, like the drop-in. */
+exa_status_t exa_aderdg_spaceTimePredictor_noalloc(
+    const exa_aderdg_desc_t* desc, double* lQhbnd, double* lFhbnd,
+    double** tempSpaceTimeUnknowns, double** tempSpaceTimeFluxUnknowns,
+    double* tempUnknowns, double* tempFluxUnknowns,
+    double* tempStateSizedVectors, const double* luh, const double* dx,
+    double dt, double* pointForceSources, int* picardIterations);
+
 /* Abstract<Solver>::volumeIntegral -> volumeIntegralNonlinear
  * (kernels/aderdg/generic/c/3d/volumeIntegralNonlinear.cpph:26-125) */
 exa_status_t exa_aderdg_volumeIntegral(const exa_aderdg_desc_t* desc,
