@@ -12,9 +12,13 @@
 //    dF = F(q) - F0 is rounded to FP32, exchanged through shared memory (half
 //    the bytes of the FP64 path) and contracted with the derivative and the
 //    time matrix in FP32 with FP32 accumulation (twice the FMA rate);
-//  * the new iterate, the squared-increment convergence test, the time
-//    averages, face extrapolation and volume integral are FP64, as are the
-//    Riemann solves, surface integral, update and dt (k_corrector).
+//  * the FP64 part of every iterate is fixed (luh and D.F0 do not change
+//    between Picard iterations), so the new deviation dq = base - dt acc and
+//    its squared increment are formed in FP32 from an FP64-derived base;
+//  * the time averages, face extrapolation and volume integral are FP64, as
+//    are the Riemann solves, surface integral, update and dt (k_corrector);
+//  * time slices are software-pipelined: the FP64 flux of slice n+1 is
+//    computed between the same barriers as the FP32 derivative of slice n.
 #include "exa_device.cuh"
 
 namespace exa {
@@ -101,16 +105,44 @@ __global__ void __launch_bounds__(MixShape<DIM, N>::NT, MINB)
 #pragma unroll
     for (int p = 0; p < B; p++) dcf[d][p] = active ? (float)(T.deriv[sd[d]][p] * a.idx[d]) : 0.f;
 
+  // First Picard deviation (all time nodes share luh, so F = F0 and the
+  // FP64 part of every iterate is the same):
+  //   base[t] = (c0[t] - 1) luh - dt (sum_n tA[t][n]) D.F0
+  // kept in FP32 (an O(dt) quantity); an iterate is dq = base - dt acc.
+  float base[B][V];
+#pragma unroll
+  for (int t = 0; t < B; t++) {
+    double tas = 0.0;
+#pragma unroll
+    for (int n = 0; n < B; n++) tas += T.tA[t][n];
+#pragma unroll
+    for (int m = 0; m < V; m++) base[t][m] = (float)((T.c0[t] - 1.0) * lu[m] - dt * tas * G0[m]);
+  }
+  const float dtf = (float)dt;
+
   float dq[B][V];
 #pragma unroll
   for (int t = 0; t < B; t++)
 #pragma unroll
     for (int m = 0; m < V; m++) dq[t][m] = 0.f;
 
+  // FP64 flux of time slice n from luh + dq[n], returned as the FP32 deviation
+  auto slice_flux = [&](int n, float (*dF)[V]) {
+    double qq[V], F[DIM][V];
+#pragma unroll
+    for (int m = 0; m < V; m++) qq[m] = lu[m] + (double)dq[n][m];
+    euler_flux<DIM, PLANAR>(qq, F);
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int m = 0; m < V; m++) dF[d][m] = (float)(F[d][m] - F0[d][m]);
+  };
+
   constexpr bool kShared = S::CPB > 1;
   float fhd[DIM][V];
   int it = 0;
   bool conv = false;
+  int buf = 0;  // slice buffer parity, alternates every slice
   for (int iter = 0; iter < MAXIT; iter++) {
     float acc[B][V];
 #pragma unroll
@@ -124,38 +156,47 @@ __global__ void __launch_bounds__(MixShape<DIM, N>::NT, MINB)
 #pragma unroll
       for (int m = 0; m < V; m++) fa[d][m] = 0.f;
 
-#pragma unroll
-    for (int n = 0; n < B; n++) {
-      float* sFn = sFf + ((iter * B + n) & 1) * S::SLICE_F;
+    // prologue: flux of slice 0
+    {
       float dF[DIM][V];
-      if (active) {
-        double qq[V], F[DIM][V];
-#pragma unroll
-        for (int m = 0; m < V; m++) qq[m] = lu[m] + (double)dq[n][m];
-        euler_flux<DIM, PLANAR>(qq, F);
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) dF[d][m] = (float)(F[d][m] - F0[d][m]);
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = dF[d][m];
-      } else {
+      if (active) slice_flux(0, dF);
+      else
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int m = 0; m < V; m++) dF[d][m] = 0.f;
-      }
+      float* sFn = sFf + buf * S::SLICE_F;
+      if (active)
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = dF[d][m];
       if (!conv) {
-        const float wn = (float)T.w[n];
+        const float wn = (float)T.w[0];
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dF[d][m], fa[d][m]);
       }
       __syncthreads();
+    }
+#pragma unroll
+    for (int n = 0; n < B; n++) {
+      // Software pipeline: the FP64 flux chain of slice n+1 and the shared-
+      // memory derivative of slice n sit between the same two barriers, so
+      // they overlap.  Slice n+1 goes to the other buffer, whose slice n-1
+      // every thread finished reading before the previous barrier.
+      float dFn[DIM][V];
+      if (n + 1 < B) {
+        if (active) slice_flux(n + 1, dFn);
+        else
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int m = 0; m < V; m++) dFn[d][m] = 0.f;
+      }
       if (active) {
+        const float* sFn = sFf + buf * S::SLICE_F;
         float Gm[V];
 #pragma unroll
         for (int m = 0; m < V; m++) Gm[m] = 0.f;
@@ -176,32 +217,45 @@ __global__ void __launch_bounds__(MixShape<DIM, N>::NT, MINB)
           for (int m = 0; m < V; m++) acc[t][m] = fmaf(ta, Gm[m], acc[t][m]);
         }
       }
+      if (n + 1 < B) {
+        buf ^= 1;
+        float* sFo = sFf + buf * S::SLICE_F;
+        if (active)
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int m = 0; m < V; m++) sFo[(d * NPC + s) * V + m] = dFn[d][m];
+        if (!conv) {
+          const float wn = (float)T.w[n + 1];
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dFn[d][m], fa[d][m]);
+        }
+        __syncthreads();
+      }
     }
+    buf ^= 1;  // the next iteration's slice 0 goes to the other buffer
 
-    // new iterate in FP64: q = c0 luh - dt (sum_n tA[t][n] G0 + acc)
-    double r = 0.0;
+    // new iterate dq = base - dt acc (FP32) and its squared increment
+    float r = 0.f;
     if (active && !conv) {
 #pragma unroll
-      for (int t = 0; t < B; t++) {
-        double tas = 0.0;
-#pragma unroll
-        for (int n = 0; n < B; n++) tas += T.tA[t][n];
+      for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) {
-          const double qn = T.c0[t] * lu[m] - dt * (tas * G0[m] + (double)acc[t][m]);
-          const double dqn = qn - lu[m];
-          const double diff = dqn - (double)dq[t][m];
-          r += diff * diff;
-          dq[t][m] = (float)dqn;
+          const float dqn = fmaf(-dtf, acc[t][m], base[t][m]);
+          const float diff = dqn - dq[t][m];
+          r = fmaf(diff, diff, r);
+          dq[t][m] = dqn;
         }
-      }
       if (kShared)
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int m = 0; m < V; m++) fhd[d][m] = fa[d][m];
     }
-    const double res = group_sum<G>(r, sred);
+    const double res = group_sum<G>((double)r, sred);
     if (!conv) {
       it = iter + 1;
       if (res < 1e-7 * 1e-7) conv = true;
