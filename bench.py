@@ -262,6 +262,9 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
+    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble'],
+                    help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves')
+    ap.add_argument('--nsolves', type=int, default=512)
     ap.add_argument('--tune', action='append', default=[],
                     help='key=value tuning knob passed to exa_tune_set (see include/exa_kernels.h)')
     args = ap.parse_args()
@@ -276,6 +279,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=600))
 
+    if args.workload == 'ensemble':
+        run_ensemble(args, rank, world, dist)
+        return
     if args.impl == 'reference':
         run_reference(args, rank, world)
         if dist:
@@ -455,6 +461,74 @@ def mixed_accuracy(ctx, steps):
     b.destroy()
     return {'steps': steps, 'rel_l2_per_step': l2, 'rel_linf_per_step': linf, 'max_rel_l2': max(l2),
             'max_rel_linf': max(linf), 'target_rel_l2': 1e-8}
+
+
+# ---------------------------------------------------------------- ensemble
+def ensemble_mix(nsolves, seed):
+    """Seeded ensemble: grid side ~U{9..81}, order ~U{2..5}, sine-wave
+    density amplitude ~U(0.05, 0.3)."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(2, 6)), int(rng.integers(9, 82)), float(rng.uniform(0.05, 0.3)), int(1000 + i))
+            for i in range(nsolves)]
+
+
+def run_ensemble(args, rank, world, dist):
+    """All solves advanced by one persistent launch per step (CUDA-graph
+    replayed), schedule picked by the autotuner; FP64 and mixed precision."""
+    import exahype_b200 as E
+    from exahype_b200 import Timer
+    from exahype_b200.autotune import tune_ensemble
+    E.lib().exa_set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    mix = ensemble_mix(args.nsolves, args.seed + rank)
+    out = {}
+    for prec_name, prec in (('fp64', E.PREC_FP64), ('mixed', E.PREC_MIXED)):
+        cfgs = [E.solve_config(o, (n, n), ic_kind=1, ic_param=amp, seed=sd, noise=0.0) for o, n, amp, sd in mix]
+        arena = int(sum(E.ensemble.footprint(c) for c in cfgs) * 1.05) + (1 << 24)
+        ens = E.Ensemble(len(cfgs), arena, precision=prec)
+        for c in cfgs:
+            assert ens.add(c) is not None
+        best, table = tune_ensemble(ens, steps=3)
+        ens.use_graph(True)
+        ens.step(args.warmup)
+        ens.synchronize()
+        st0 = ens.status()
+        if dist:
+            dist.barrier()
+        t = Timer()
+        s = ens.stream()
+        l0 = E.launch_count()
+        t.start(s)
+        ens.step(args.steps)
+        t.stop(s)
+        ms = t.elapsed_ms()
+        launches = E.launch_count() - l0
+        st1 = ens.status()
+        cells = ens.active_cells()
+        steps_done = (st1['steps'] - st0['steps']).astype(np.int64)
+        updates = sum(int(steps_done[sl]) * c.n[0] * c.n[1] for sl, c in ens.cfgs.items())
+        out[prec_name] = {'value': updates / (ms * 1e-3), 'ms_per_step': ms / args.steps, 'cells': cells,
+                          'launches_per_step': launches / args.steps, 'tuned': {'ctas_per_sm': best[0],
+                          'grab': best[1], 'order_policy': best[2]}, 'tuning_table': table}
+        if prec_name == 'fp64':
+            ref_states = {sl: ens.get_state(sl) for sl in list(ens.cfgs)[:16]}
+        else:
+            errs = [float(np.linalg.norm(ens.get_state(sl) - r) / np.linalg.norm(r)) for sl, r in ref_states.items()]
+            out['mixed']['max_rel_l2_vs_fp64_first16'] = max(errs)
+        ens.destroy()
+    if rank == 0:
+        line = {'metric': '2D Euler ADER-DG ensemble cell-updates/s (512 solves, N in 2..5, 9^2..81^2 cells)',
+                'value': out['fp64']['value'] * world, 'unit': 'cell-updates/s', 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': out['fp64']['ms_per_step'],
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic', 'config': {'workload': 'ensemble of %d 2D solves, one persistent launch per '
+                                                            'step in a CUDA graph' % args.nsolves,
+                                                'cells': out['fp64']['cells']},
+                'fp64': out['fp64'], 'mixed': out['mixed'],
+                'mixed_speedup': out['mixed']['value'] / out['fp64']['value']}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 if __name__ == '__main__':

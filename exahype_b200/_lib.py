@@ -123,6 +123,21 @@ SIGNATURES = {
     'exa_aderdg_grid_device_state': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(u64), C.POINTER(u64), C.POINTER(i32)]),
     'exa_aderdg_grid_ncells': (i64, [vp]),
+    'exa_ensemble_footprint': (sz, [vp]),
+    'exa_ensemble_create': (i32, [i32, i32, sz, C.POINTER(vp)]),
+    'exa_ensemble_destroy': (i32, [vp]),
+    'exa_ensemble_add': (i32, [vp, vp, C.c_longlong, C.POINTER(i32)]),
+    'exa_ensemble_remove': (i32, [vp, i32]),
+    'exa_ensemble_step': (i32, [vp, i32]),
+    'exa_ensemble_use_graph': (i32, [vp, i32]),
+    'exa_ensemble_tune': (i32, [vp, i32, i32, i32]),
+    'exa_ensemble_synchronize': (i32, [vp]),
+    'exa_ensemble_stream': (i32, [vp, C.POINTER(vp)]),
+    'exa_ensemble_get_state': (i32, [vp, i32, vp]),
+    'exa_ensemble_device_state': (i32, [vp, i32, C.POINTER(vp)]),
+    'exa_ensemble_status': (i32, [vp, vp, vp, vp, vp, vp]),
+    'exa_ensemble_active_cells': (i64, [vp]),
+    'exa_ensemble_info': (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_stable_dt': (i32, [C.POINTER(FVDesc), i64, vp, vp, vp]),

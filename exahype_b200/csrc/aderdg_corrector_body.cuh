@@ -1,0 +1,182 @@
+// Corrector body (Riemann + surface integral + update + next dt, see
+// aderdg_faces.cu); shared by k_corrector and the ensemble kernel.
+#pragma once
+#include "exa_device.cuh"
+
+namespace exa {
+
+template <int DIM, int N>
+struct CellShape {
+  static constexpr int B = N + 1;
+  static constexpr int V = kV;
+  static constexpr int NPC = ipow(B, DIM);
+  static constexpr int NF = ipow(B, DIM - 1);
+  static constexpr int NFACE = 2 * DIM;
+  static constexpr int G = CellThreads<NPC>::G;
+  static constexpr int CPB = DIM == 3 ? 1 : (128 / G > 0 ? 128 / G : 1);
+  static constexpr int NT = G * CPB;
+};
+
+// dynamic shared memory (doubles) of one corrector CTA
+template <int DIM, int N>
+struct CorrShapeSmem {
+  using S = CellShape<DIM, N>;
+  static constexpr int value =
+      S::CPB * (4 * S::NFACE * S::NF * S::V + S::NFACE * 2 * S::V + S::NFACE) + S::NT / 32 + 1;
+};
+
+// face-node index of node s on the faces normal to direction d
+template <int DIM, int B>
+__device__ __forceinline__ int face_node(const int* sd, int d) {
+  if (DIM == 3) {
+    if (d == 0) return sd[2] * B + sd[1];
+    if (d == 1) return sd[2] * B + sd[0];
+    return sd[1] * B + sd[0];
+  }
+  return d == 0 ? sd[1] : sd[0];
+}
+
+// weight of face node j (product of the GL weights of its coordinates)
+template <int DIM, int B>
+__device__ __forceinline__ double face_weight(const DGConst& T, int j) {
+  return DIM == 3 ? T.w[j / B] * T.w[j % B] : T.w[j];
+}
+
+// ---------------------------------------------------------------- corrector
+template <int DIM, int N, bool PLANAR>
+__device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, double* smem) {
+  using S = CellShape<DIM, N>;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, NF = S::NF, NFACE = S::NFACE, G = S::G;
+  constexpr int FV = NFACE * NF * V;
+  const DGConst& T = c_dg[N];
+  const int lc = threadIdx.x / G;
+  const int s = threadIdx.x % G;
+  const long cell = block * S::CPB + lc;
+  const bool valid = cell < a.ncells;
+  double* sQo = smem + lc * (4 * FV + NFACE * 2 * V + NFACE);
+  double* sQn = sQo + FV;
+  double* sFo = sQn + FV;
+  double* sFn = sFo + FV;
+  double* sAv = sFn + FV;            // [NFACE][2 (own, neighbour)][V]
+  double* sSm = sAv + NFACE * 2 * V;  // [NFACE]
+  double* sred = smem + S::CPB * (4 * FV + NFACE * 2 * V + NFACE);
+
+  int cc[3] = {0, 0, 0};
+  if (valid) {
+    cc[0] = (int)(cell % a.n[0]);
+    cc[1] = (int)((cell / a.n[0]) % a.n[1]);
+    cc[2] = DIM == 3 ? (int)(cell / ((long)a.n[0] * a.n[1])) : 0;
+  }
+  // load own faces and the matching faces of the neighbours
+  if (valid) {
+    const double* qo = a.lQhbnd + cell * FV;
+    const double* fo = a.lFhbnd + cell * FV;
+    for (int k = s; k < FV; k += G) {
+      const int f = k / (NF * V), r = k % (NF * V);
+      const int d = f >> 1;
+      int nc[3] = {cc[0], cc[1], cc[2]};
+      nc[d] = (f & 1) ? (nc[d] + 1 == a.n[d] ? 0 : nc[d] + 1) : (nc[d] == 0 ? a.n[d] - 1 : nc[d] - 1);
+      const long nb = DIM == 3 ? ((long)nc[2] * a.n[1] + nc[1]) * a.n[0] + nc[0]
+                               : (long)nc[1] * a.n[0] + nc[0];
+      const long off = nb * FV + (f ^ 1) * NF * V + r;
+      sQo[k] = qo[k];
+      sFo[k] = fo[k];
+      sQn[k] = a.lQhbnd[off];
+      sFn[k] = a.lFhbnd[off];
+    }
+  }
+  __syncthreads();
+  // face-averaged states (riemannSolverNonlinear.cpph:52-69)
+  if (valid) {
+    for (int k = s; k < NFACE * 2 * V; k += G) {
+      const int f = k / (2 * V), side = (k / V) & 1, m = k % V;
+      const double* Q = (side ? sQn : sQo) + f * NF * V;
+      double acc = 0.0;
+#pragma unroll
+      for (int j = 0; j < NF; j++) acc += face_weight<DIM, B>(T, j) * Q[j * V + m];
+      sAv[k] = acc;
+    }
+  }
+  __syncthreads();
+  // smax per face (:71-81)
+  if (valid && s < NFACE) {
+    const int f = s, d = f >> 1;
+    double qa[5], qb[5];
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      qa[m] = sAv[(f * 2 + 0) * V + m];
+      qb[m] = sAv[(f * 2 + 1) * V + m];
+    }
+    sSm[f] = fmax(euler_max_eig<PLANAR>(qa, d), euler_max_eig<PLANAR>(qb, d));
+  }
+  __syncthreads();
+  // Rusanov flux (:83-115): F = (FL+FR)/2 - smax/2 (QR-QL); left = lower cell
+  if (valid) {
+    for (int k = s; k < FV; k += G) {
+      const int f = k / (NF * V);
+      const bool own_left = f & 1;  // face 2d+1: this cell is the left one
+      const double ql = own_left ? sQo[k] : sQn[k];
+      const double qr = own_left ? sQn[k] : sQo[k];
+      const double fl = own_left ? sFo[k] : sFn[k];
+      const double fr = own_left ? sFn[k] : sFo[k];
+      sFo[k] = 0.5 * (fr + fl) - 0.5 * sSm[f] * (qr - ql);
+    }
+  }
+  __syncthreads();
+  double dtc = DBL_MAX;
+  if (valid && s < NPC) {
+    int sd[3];
+    sd[0] = s % B;
+    sd[1] = (s / B) % B;
+    sd[2] = DIM == 3 ? s / (B * B) : 0;
+    const double* lduh = a.lduh + cell * (long)NPC * V;
+    double* luh = a.luh + cell * (long)NPC * V;
+    double v[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) v[m] = lduh[s * V + m];
+    // surface integral (surfaceIntegralNonlinear.cpph:21-85)
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      double us = 1.0 / a.dx[d];
+      double wprod = 1.0;
+#pragma unroll
+      for (int e = DIM - 1; e >= 0; e--)
+        if (e != d) wprod *= T.w[sd[e]];
+      us = wprod / a.dx[d];
+      const int j = face_node<DIM, B>(sd, d);
+      const double cr = T.fr[sd[d]], cl = T.fl[sd[d]];
+      const double* FR_ = sFo + ((2 * d + 1) * NF + j) * V;
+      const double* FL_ = sFo + ((2 * d) * NF + j) * V;
+#pragma unroll
+      for (int m = 0; m < V; m++) v[m] -= (FR_[m] * cr - FL_[m] * cl) * us;
+    }
+    // solution update (solutionUpdate.cpph:23-47)
+    double W = 1.0;
+#pragma unroll
+    for (int e = DIM - 1; e >= 0; e--) W *= T.w[sd[e]];
+    const double dt = *a.dt_dev;
+    const double us = dt / W;
+    double q[V];
+    bool finite = true;
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      q[m] = luh[s * V + m] + v[m] * us;
+      luh[s * V + m] = q[m];
+      finite = finite && isfinite(q[m]);
+    }
+    if (!finite && a.nan_flag) atomicOr(a.nan_flag, 1);
+    // next step's stable dt at this node (stableTimeStepSize.cpph:21-61)
+    if (a.dt_next) {
+      double den = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) den += euler_max_eig<PLANAR>(q, d) / a.dx[d];
+      dtc = a.dt_factor / den;
+    }
+  }
+  if (a.dt_next) {
+    const double cm = group_min<G>(dtc, sred);
+    if (valid && s == 0) atomic_min_pos_double(a.dt_next, cm);
+  }
+}
+
+}  // namespace exa

@@ -52,6 +52,7 @@ exa_status_t ensure_tables() {
   exa_status_t s;
   if ((s = upload_tables_predictor())) return s;
   if ((s = upload_tables_predictor_mixed())) return s;
+  if ((s = upload_tables_ensemble())) return s;
   if ((s = upload_tables_faces())) return s;
   if ((s = upload_tables_fv())) return s;
   g_tables_done[dev & 255] = true;

@@ -84,6 +84,7 @@ exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* 
 // table uploads, one per translation unit holding kernels
 exa_status_t upload_tables_predictor();
 exa_status_t upload_tables_predictor_mixed();
+exa_status_t upload_tables_ensemble();
 exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 // host copy of the derived tables (same bytes as the device constants)

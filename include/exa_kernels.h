@@ -300,6 +300,53 @@ exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time,
                                     uint64_t* nonconverged, int* nan_flag);
 long exa_aderdg_grid_ncells(const exa_aderdg_grid* g);
 
+/* ------------------------------------ ADER-DG: ensemble of 2D solves --
+ * Many independent uniform periodic 2D grids (each its own order 2..5, size,
+ * dt and step budget -- the per-solver state of ADERDGSolver.cpp:557-585)
+ * advanced together by ONE cooperative persistent kernel per step: CTAs take
+ * work items (a block of cells of one solve) from an atomic counter through
+ * the predictor phase, a grid-wide barrier, the corrector phase, a barrier,
+ * and a per-solve commit.  Device memory comes from an arena allocated at
+ * creation; adding a solve fails with EXA_EBUSY when its footprint does not
+ * fit (admission by footprint). */
+typedef struct exa_ensemble exa_ensemble;
+
+typedef struct {
+  int order;          /* 2..5 */
+  int n[2];           /* cells */
+  double length[2];   /* domain extent */
+  int pde;            /* exa_pde_t */
+  int dt_policy;      /* as exa_aderdg_grid_config_t */
+  double cfl, dt_fixed;
+  int ic_kind;        /* 0 isentropic vortex, 1 density sine wave */
+  double ic_param;    /* vortex strength / sine amplitude */
+  uint64_t seed;
+  double noise;       /* relative density noise amplitude */
+} exa_solve_config_t;
+
+size_t exa_ensemble_footprint(const exa_solve_config_t* cfg);
+exa_status_t exa_ensemble_create(int precision, int max_solves, size_t arena_bytes,
+                                 exa_ensemble** out);
+exa_status_t exa_ensemble_destroy(exa_ensemble* e);
+/* steps: step budget (< 0 unlimited); the solve stops after it */
+exa_status_t exa_ensemble_add(exa_ensemble* e, const exa_solve_config_t* cfg, long long steps,
+                              int* slot);
+exa_status_t exa_ensemble_remove(exa_ensemble* e, int slot);
+exa_status_t exa_ensemble_step(exa_ensemble* e, int nsteps);
+exa_status_t exa_ensemble_use_graph(exa_ensemble* e, int enable);
+/* schedule knobs: persistent CTAs per SM (0 = max resident), work items per
+ * atomic grab, work order (0 = costly orders first, 1 = solve order) */
+exa_status_t exa_ensemble_tune(exa_ensemble* e, int ctas_per_sm, int grab, int order_policy);
+exa_status_t exa_ensemble_synchronize(exa_ensemble* e);
+exa_status_t exa_ensemble_stream(exa_ensemble* e, void** stream);
+exa_status_t exa_ensemble_get_state(exa_ensemble* e, int slot, double* host_luh);
+exa_status_t exa_ensemble_device_state(exa_ensemble* e, int slot, double** luh_dev);
+exa_status_t exa_ensemble_status(exa_ensemble* e, double* time, uint64_t* steps_done, int* active,
+                                 uint64_t* picard, int* nan_flag);
+long exa_ensemble_active_cells(exa_ensemble* e);
+exa_status_t exa_ensemble_info(exa_ensemble* e, int* grid_ctas, int* nitems,
+                               size_t* arena_free_bytes);
+
 /* ------------------------------------------------ finite volumes (2D) --
  * One patch of patch x patch cells with `ghost` ghost layers, layout
  * [y][x][nData] over (patch+2*ghost)^2 cells (reference FV solvers,

@@ -1,0 +1,116 @@
+"""Ensemble of independent 2D solves in one persistent launch per step."""
+import numpy as np
+import pytest
+
+import exahype_b200 as E
+from exahype_b200.device import diff_norms
+
+pytestmark = pytest.mark.gpu
+
+MIX = [  # order, n, ic_kind, ic_param, pde, seed
+    (2, (9, 9), 1, 0.05, E.PDE_EULER, 1),
+    (3, (27, 27), 1, 0.2, E.PDE_EULER, 2),
+    (4, (13, 17), 0, 5.0, E.PDE_EULER, 3),
+    (5, (11, 9), 1, 0.3, E.PDE_EULER_PLANAR, 4),
+    (3, (40, 12), 0, 5.0, E.PDE_EULER, 5),
+    (2, (81, 81), 1, 0.1, E.PDE_EULER, 6),
+]
+
+
+def cfg(order, n, kind, param, pde, seed, noise=1e-3):
+    return E.solve_config(order, n, pde=pde, ic_kind=kind, ic_param=param, seed=seed, noise=noise)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+def test_ensemble_matches_single_grids():
+    ens = E.Ensemble(16, 1 << 28)
+    slots = [ens.add(cfg(*m)) for m in MIX]
+    ens.step(8)
+    ens.synchronize()
+    st = ens.status()
+    for sl, (order, n, kind, param, pde, seed) in zip(slots, MIX):
+        g = E.ADERDGGrid(2, order, n, pde=pde)
+        g.init(kind=kind, param=param, seed=seed, noise=1e-3)
+        g.step(8)
+        ref = g.get_state()
+        got = ens.get_state(sl)
+        assert rel(got, ref) < 1e-13, (order, n, rel(got, ref))
+        assert abs(st['time'][sl] - g.status()['time']) <= 1e-13 * g.status()['time']
+        assert st['steps'][sl] == 8
+        g.destroy()
+    ens.destroy()
+
+
+def test_ensemble_step_budget_and_graph():
+    a = E.Ensemble(8, 1 << 26)
+    b = E.Ensemble(8, 1 << 26)
+    b.use_graph(True)
+    budgets = [3, 7, -1]
+    for ens in (a, b):
+        for m, k in zip(MIX[:3], budgets):
+            ens.add(cfg(*m), steps=k)
+    for _ in range(5):
+        a.step(2)
+        b.step(2)
+        a.status()
+        b.status()  # drops finished solves before the next step
+    sa, sb = a.status(), b.status()
+    assert list(sa['steps'][:3]) == [3, 7, 10]
+    assert list(sa['active'][:3]) == [0, 0, 1]
+    for sl in range(3):
+        assert np.array_equal(a.get_state(sl), b.get_state(sl))
+    a.destroy()
+    b.destroy()
+
+
+def test_result_identical_alone_and_in_mix():
+    alone = E.Ensemble(4, 1 << 26)
+    mixed = E.Ensemble(16, 1 << 28)
+    target = (4, (13, 17), 0, 5.0, E.PDE_EULER, 3)
+    s_alone = alone.add(cfg(*target), steps=6)
+    for m in MIX[:2]:
+        mixed.add(cfg(*m), steps=9)
+    s_mix = mixed.add(cfg(*target), steps=6)
+    for m in MIX[4:]:
+        mixed.add(cfg(*m), steps=4)
+    for _ in range(9):
+        alone.step(1)
+        mixed.step(1)
+        alone.status()
+        mixed.status()
+    assert np.array_equal(alone.get_state(s_alone), mixed.get_state(s_mix))
+    alone.destroy()
+    mixed.destroy()
+
+
+def test_admission_by_footprint():
+    c = cfg(5, (60, 60), 1, 0.2, E.PDE_EULER, 9)
+    fp = E.ensemble.footprint(c)
+    ens = E.Ensemble(4, int(fp * 1.5))
+    s0 = ens.add(c)
+    assert s0 is not None
+    assert ens.add(c) is None  # does not fit: EXA_EBUSY
+    ens.remove(s0)
+    assert ens.add(c) is not None
+    ens.destroy()
+
+
+@pytest.mark.parametrize('seed', [0])
+def test_mixed_ensemble_vs_fp64(seed):
+    a = E.Ensemble(16, 1 << 28, precision=E.PREC_FP64)
+    b = E.Ensemble(16, 1 << 28, precision=E.PREC_MIXED)
+    sa = [a.add(cfg(*m)) for m in MIX]
+    sb = [b.add(cfg(*m)) for m in MIX]
+    for _ in range(10):
+        a.step(1)
+        b.step(1)
+    a.synchronize()
+    b.synchronize()
+    for x, y in zip(sa, sb):
+        e = diff_norms(b.device_state_ptr(y), a.device_state_ptr(x), a.state_size(x))
+        assert e['rel_l2'] <= 1e-8, e
+    a.destroy()
+    b.destroy()
