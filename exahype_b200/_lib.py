@@ -138,6 +138,15 @@ SIGNATURES = {
     'exa_ensemble_status': (i32, [vp, vp, vp, vp, vp, vp]),
     'exa_ensemble_active_cells': (i64, [vp]),
     'exa_ensemble_info': (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
+    'exa_server_footprint': (sz, [vp]),
+    'exa_server_create': (i32, [sz, i32, i32, C.POINTER(vp)]),
+    'exa_server_destroy': (i32, [vp]),
+    'exa_server_submit': (i32, [vp, vp, C.POINTER(u64)]),
+    'exa_server_tick': (i32, [vp, C.POINTER(i32)]),
+    'exa_server_completed': (i32, [vp, C.POINTER(u64), i32, C.POINTER(i32)]),
+    'exa_server_result_size': (sz, [vp, u64]),
+    'exa_server_result': (i32, [vp, u64, vp, C.POINTER(f64), C.POINTER(C.c_longlong)]),
+    'exa_server_info': (i32, [vp, C.POINTER(i32), C.POINTER(C.c_long), C.POINTER(sz)]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_stable_dt': (i32, [C.POINTER(FVDesc), i64, vp, vp, vp]),

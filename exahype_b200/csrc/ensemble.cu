@@ -393,6 +393,20 @@ static exa_status_t configure_grid(exa_ensemble* e) {
   return EXA_OK;
 }
 
+namespace exa {
+bool ens_arena_alloc(exa_ensemble* e, size_t bytes, char** ptr, size_t* off) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  if (!arena_alloc(e, align256(bytes), off)) return false;
+  *ptr = e->arena + *off;
+  return true;
+}
+void ens_arena_free(exa_ensemble* e, size_t off, size_t bytes) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  arena_free(e, off, align256(bytes));
+}
+cudaStream_t ens_stream(exa_ensemble* e) { return e->st; }
+}  // namespace exa
+
 extern "C" {
 
 size_t exa_ensemble_footprint(const exa_solve_config_t* cfg) {

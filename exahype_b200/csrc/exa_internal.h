@@ -79,6 +79,15 @@ exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, 
                             int kind, double param, uint64_t seed, double noise,
                             cudaStream_t st);
 
+exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, double* luh, double* luh_new,
+                                 unsigned long long* dt_slot, double* time, cudaStream_t st);
+exa_status_t launch_fv_ic(const exa_fv_desc_t& d, double* luh, double amp, uint64_t seed, double noise,
+                          cudaStream_t st);
+// arena of an ensemble, shared with the serving engine
+bool ens_arena_alloc(exa_ensemble* e, size_t bytes, char** ptr, size_t* off);
+void ens_arena_free(exa_ensemble* e, size_t off, size_t bytes);
+cudaStream_t ens_stream(exa_ensemble* e);
+
 exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* qR, double* out);
 
 // table uploads, one per translation unit holding kernels

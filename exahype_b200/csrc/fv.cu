@@ -28,6 +28,7 @@ struct FVArgs {
   int P, g, S, npar;
   double hx, hy;      // cell sizes
   double dt;
+  const double* dt_dev;  // when non-null, dt is read here (device-resident stepping)
   const double* luh;  // state the fluxes are computed from
   double* out;        // luh_new: updated in place (reference semantics)
   unsigned long long* max_dt;  // per patch, atomic-min bit patterns (nullable)
@@ -96,7 +97,8 @@ __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
     }
   }
   __syncthreads();
-  const double cx = a.dt / a.hx, cy = a.dt / a.hy;
+  const double dtv = a.dt_dev ? *a.dt_dev : a.dt;
+  const double cx = dtv / a.hx, cy = dtv / a.hy;
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
   double* out = a.out + patch * (long)S * S * D;
   const int k0 = pb + blockIdx.x * FV_TX, j0 = pb + blockIdx.y * FV_TY;
   const int tid = threadIdx.x;
-  const double hx = a.hx, hy = a.hy, dt = a.dt;
+  const double hx = a.hx, hy = a.hy, dt = a.dt_dev ? *a.dt_dev : a.dt;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
     const int j = j0 - 2 + r, k = k0 - 2 + c;
@@ -384,6 +386,112 @@ static FVArgs fv_args(const exa_fv_desc_t* d) {
 }
 
 exa_status_t upload_tables_fv() { return EXA_OK; }
+
+// ghost fill of one patch plus reset of its dt slot to +inf
+__global__ void k_fv_ghosts_reset(int P, int g, int D, double* luh, unsigned long long* dt_slot) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dt_slot = 0x7FF0000000000000ULL;
+  const int S = P + 2 * g;
+  const long nghost = (long)S * S - (long)P * P;
+  const long r0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r0 >= nghost) return;
+  long r = r0;
+  int j, k;
+  const long top = (long)g * S;
+  if (r < top) { j = (int)(r / S); k = (int)(r % S); }
+  else if (r < 2 * top) { r -= top; j = g + P + (int)(r / S); k = (int)(r % S); }
+  else {
+    r -= 2 * top;
+    j = g + (int)(r / (2 * g));
+    const int c = (int)(r % (2 * g));
+    k = c < g ? c : P + c;
+  }
+  const int sj = g + ((j - g) % P + P) % P, sk = g + ((k - g) % P + P) % P;
+  for (int m = 0; m < D; m++) luh[((long)j * S + k) * D + m] = luh[((long)sj * S + sk) * D + m];
+}
+
+__global__ void k_fv_commit(const double* dt, double* time) { *time += *dt; }
+
+__device__ __forceinline__ double fv_noise_u01(unsigned long long seed, unsigned long long idx) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (idx + 1ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  z = z ^ (z >> 31);
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// cell-centred density sine wave rho = 1 + amp sin(2 pi (x + y)), u = v = 1,
+// p = 1, with seeded relative density noise; ghosts are filled by the step
+__global__ void k_fv_ic(int P, int g, int D, double hx, double hy, double amp, unsigned long long seed,
+                        double noise, double* luh) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int S = P + 2 * g;
+  if (i >= (long)S * S) return;
+  const int j = (int)(i / S), k = (int)(i % S);
+  const double x = (k - g + 0.5) * hx, y = (j - g + 0.5) * hy;
+  const double pi = 3.14159265358979323846;
+  double rho = 1.0 + amp * sin(2 * pi * (x + y));
+  if (noise != 0.0) rho *= 1.0 + noise * (2.0 * fv_noise_u01(seed, (unsigned long long)i) - 1.0);
+  double* q = luh + i * D;
+  q[0] = rho;
+  q[1] = rho;
+  q[2] = rho;
+  q[3] = 0.0;
+  q[4] = 1.0 / (kGamma - 1) + rho;  // p/(g-1) + rho (u^2+v^2)/2 with u = v = 1
+  for (int m = kV; m < D; m++) q[m] = 0.0;
+}
+
+exa_status_t launch_fv_ic(const exa_fv_desc_t& d, double* luh, double amp, uint64_t seed, double noise,
+                          cudaStream_t st) {
+  const int S = d.patch + 2 * d.ghost;
+  const long n = (long)S * S;
+  k_fv_ic<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d.patch, d.ghost, d.nvar + d.npar, d.dx[0] / d.patch,
+                                                       d.dx[1] / d.patch, amp, seed, noise, luh);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_fv_ic");
+}
+
+// One device-resident step of a single periodic patch: ghosts, CFL dt
+// (commons::stableTimeStepSize rule) into dt_slot, luh_new = luh, scheme
+// update reading dt from the slot, time += dt.  No host synchronisation.
+exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, double* luh, double* luh_new,
+                                 unsigned long long* dt_slot, double* time, cudaStream_t st) {
+  FVArgs a = fv_args(&d);
+  const int S = a.S;
+  const long nghost = (long)S * S - (long)d.patch * d.patch;
+  k_fv_ghosts_reset<<<(unsigned)((nghost + 255) / 256), 256, 0, st>>>(d.patch, d.ghost, d.nvar + d.npar, luh,
+                                                                   dt_slot);
+  a.luh = luh;
+  const long cells = (long)d.patch * d.patch;
+  unsigned bx = (unsigned)((cells + 255) / 256);
+  if (bx > 1024) bx = 1024;
+  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
+  if (planar) k_fv_stable_dt<true><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)dt_slot);
+  else k_fv_stable_dt<false><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)dt_slot);
+  cudaError_t e = cudaMemcpyAsync(luh_new, luh, sizeof(double) * S * S * (d.nvar + d.npar),
+                                  cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return cuda_status(e, "fv copy");
+  a.out = luh_new;
+  a.dt_dev = (const double*)dt_slot;
+  a.max_dt = nullptr;
+  dim3 grid((d.patch + FV_TX - 1) / FV_TX, (d.patch + FV_TY - 1) / FV_TY, 1);
+  if (scheme == 0) {
+    if (planar) k_fv_godunov<true><<<grid, FV_NT, 0, st>>>(a);
+    else k_fv_godunov<false><<<grid, FV_NT, 0, st>>>(a);
+  } else {
+    static bool attr[2] = {false, false};
+    if (!attr[planar]) {
+      e = planar ? cudaFuncSetAttribute(k_fv_muscl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
+                 : cudaFuncSetAttribute(k_fv_muscl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
+      attr[planar] = true;
+    }
+    if (planar) k_fv_muscl<true><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    else k_fv_muscl<false><<<grid, FV_NT, kMusclSmem, st>>>(a);
+  }
+  k_fv_commit<<<1, 1, 0, st>>>((const double*)dt_slot, time);
+  count_launch(5);
+  return cuda_status(cudaGetLastError(), "fv patch step");
+}
 
 template <bool PLANAR>
 __global__ void k_rusanov_one(int d, const double* qL, const double* qR, double* out) {

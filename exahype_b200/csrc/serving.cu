@@ -1,0 +1,259 @@
+// Serving engine: continuous batching of solve requests on one GPU.
+//
+// Requests are 2D ADER-DG solves or 2D finite-volume (Godunov / MUSCL-
+// Hancock) periodic patches with a step budget.  Admission is by device
+// memory footprint out of one arena (the ensemble's): a request that does
+// not fit is refused with EXA_EBUSY and the caller retries after others
+// finish.  Admitted requests stay resident on the device until their result
+// is collected.  Every tick advances every active request by one step:
+//   * all ADER-DG requests together in the ensemble's single persistent
+//     launch (one launch regardless of how many requests are active);
+//   * each FV request as a device-resident patch step on a second stream,
+//     so FV work overlaps the ADER-DG launch.
+// A request that arrives while others run joins at the next tick; its
+// arithmetic is independent of its neighbours (per-request dt and state),
+// so its result is the same alone or in any mix.
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "exa_device.cuh"
+
+using namespace exa;
+
+namespace {
+struct Req {
+  uint64_t id = 0;
+  exa_request_t r{};
+  // ADER-DG
+  int slot = -1;
+  // FV
+  exa_fv_desc_t fv{};
+  double* luh = nullptr;
+  double* luh_new = nullptr;
+  unsigned long long* dt_slot = nullptr;  // scalars: [0] dt bits, [1] time
+  size_t off = 0, bytes = 0;
+  long long steps_left = 0;
+  long long steps_done = 0;
+  bool done = false;
+};
+
+size_t fv_bytes(const exa_request_t* r) {
+  const int g = r->fv_scheme == 0 ? 1 : 2;
+  const size_t S = (size_t)r->fv_patch + 2 * g;
+  const size_t state = ((S * S * kV * 8) + 255) & ~size_t(255);
+  return 2 * state + 256;
+}
+}  // namespace
+
+struct exa_server {
+  exa_ensemble* ens = nullptr;
+  cudaStream_t fv_st = nullptr;
+  int precision = 0;
+  int max_requests = 0;
+  uint64_t next_id = 1;
+  std::map<uint64_t, Req> live;
+  std::vector<uint64_t> completed;
+  std::mutex mu;
+  std::vector<double> st_time;
+  std::vector<uint64_t> st_steps, st_picard;
+  std::vector<int> st_active, st_nan;
+};
+
+extern "C" {
+
+size_t exa_server_footprint(const exa_request_t* r) {
+  if (!r) return 0;
+  if (r->kind == EXA_REQ_ADERDG) return exa_ensemble_footprint(&r->dg);
+  if (r->kind == EXA_REQ_FV) {
+    if (r->fv_patch < 1) return 0;
+    return fv_bytes(r);
+  }
+  return 0;
+}
+
+exa_status_t exa_server_create(size_t hbm_budget, int max_requests, int precision, exa_server** out) {
+  if (!out || max_requests < 1) return set_error(EXA_EINVAL, "bad server arguments");
+  exa_server* s = new (std::nothrow) exa_server;
+  if (!s) return set_error(EXA_ENOMEM, "host allocation");
+  s->precision = precision;
+  s->max_requests = max_requests;
+  exa_status_t st = exa_ensemble_create(precision, max_requests, hbm_budget, &s->ens);
+  if (!st) st = cuda_status(cudaStreamCreateWithFlags(&s->fv_st, cudaStreamNonBlocking), "fv stream");
+  if (st) {
+    exa_server_destroy(s);
+    return st;
+  }
+  exa_ensemble_use_graph(s->ens, 1);
+  s->st_time.resize(max_requests);
+  s->st_steps.resize(max_requests);
+  s->st_picard.resize(max_requests);
+  s->st_active.resize(max_requests);
+  s->st_nan.resize(max_requests);
+  *out = s;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_destroy(exa_server* s) {
+  if (!s) return EXA_OK;
+  if (s->fv_st) {
+    cudaStreamSynchronize(s->fv_st);
+    cudaStreamDestroy(s->fv_st);
+  }
+  if (s->ens) exa_ensemble_destroy(s->ens);
+  delete s;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* id) {
+  if (!s || !r || !id) return set_error(EXA_EINVAL, "NULL argument");
+  if (r->steps < 1) return set_error(EXA_EINVAL, "steps must be >= 1");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if ((int)s->live.size() >= s->max_requests) return set_error(EXA_EBUSY, "request slots full");
+  Req q;
+  q.id = s->next_id;
+  q.r = *r;
+  q.steps_left = r->steps;
+  if (r->kind == EXA_REQ_ADERDG) {
+    int slot = -1;
+    exa_status_t st = exa_ensemble_add(s->ens, &r->dg, r->steps, &slot);
+    if (st) return st;  // EXA_EBUSY when the footprint does not fit
+    q.slot = slot;
+  } else if (r->kind == EXA_REQ_FV) {
+    if (r->fv_patch < 1 || r->fv_scheme < 0 || r->fv_scheme > 1 || !(r->fv_length > 0))
+      return set_error(EXA_EINVAL, "bad FV request");
+    q.fv = exa_fv_desc_t{2, r->fv_patch, r->fv_scheme == 0 ? 1 : 2, kV, 0, r->dg.pde,
+                         {r->fv_length, r->fv_length, 1.0}};
+    q.bytes = fv_bytes(r);
+    char* p = nullptr;
+    if (!ens_arena_alloc(s->ens, q.bytes, &p, &q.off))
+      return set_error(EXA_EBUSY, "not enough free device memory in the arena");
+    const size_t S = (size_t)q.fv.patch + 2 * q.fv.ghost;
+    const size_t state = ((S * S * kV * 8) + 255) & ~size_t(255);
+    q.luh = (double*)p;
+    q.luh_new = (double*)(p + state);
+    q.dt_slot = (unsigned long long*)(p + 2 * state);
+    cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 16, s->fv_st);
+    exa_status_t st = e == cudaSuccess ? launch_fv_ic(q.fv, q.luh, r->dg.ic_param, r->dg.seed, r->dg.noise, s->fv_st)
+                                       : cuda_status(e, "fv scalars");
+    if (st) {
+      ens_arena_free(s->ens, q.off, q.bytes);
+      return st;
+    }
+  } else {
+    return set_error(EXA_EINVAL, "unknown request kind");
+  }
+  s->next_id++;
+  *id = q.id;
+  s->live[q.id] = q;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  bool any_dg = false;
+  for (auto& kv : s->live)
+    if (!kv.second.done && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
+  if (any_dg)
+    if (exa_status_t st = exa_ensemble_step(s->ens, 1)) return st;
+  for (auto& kv : s->live) {
+    Req& q = kv.second;
+    if (q.done || q.r.kind != EXA_REQ_FV) continue;
+    if (exa_status_t st = fv_patch_step_async(q.r.fv_scheme, q.fv, q.luh, q.luh_new, q.dt_slot,
+                                              (double*)(q.dt_slot + 1), s->fv_st))
+      return st;
+    std::swap(q.luh, q.luh_new);
+    q.steps_done++;
+    if (--q.steps_left == 0) q.done = true;
+  }
+  exa_status_t st = EXA_OK;
+  if (any_dg) {
+    st = exa_ensemble_status(s->ens, s->st_time.data(), s->st_steps.data(), s->st_active.data(),
+                             s->st_picard.data(), s->st_nan.data());
+    if (st && st != EXA_ENAN) return st;
+  }
+  cudaError_t e = cudaStreamSynchronize(s->fv_st);
+  if (e != cudaSuccess) return cuda_status(e, "fv stream");
+  int n = 0;
+  for (auto& kv : s->live) {
+    Req& q = kv.second;
+    if (q.r.kind == EXA_REQ_ADERDG && !q.done && any_dg && !s->st_active[q.slot]) {
+      q.done = true;
+      q.steps_done = (long long)s->st_steps[q.slot];
+    }
+    if (q.done && std::find(s->completed.begin(), s->completed.end(), q.id) == s->completed.end()) {
+      s->completed.push_back(q.id);
+      n++;
+    }
+  }
+  if (ncompleted) *ncompleted = n;
+  return st;
+}
+
+exa_status_t exa_server_completed(exa_server* s, uint64_t* ids, int cap, int* n) {
+  if (!s || !n || (cap > 0 && !ids)) return set_error(EXA_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  int k = 0;
+  while (k < cap && !s->completed.empty()) {
+    ids[k++] = s->completed.front();
+    s->completed.erase(s->completed.begin());
+  }
+  *n = k;
+  return EXA_OK;
+}
+
+size_t exa_server_result_size(exa_server* s, uint64_t id) {
+  if (!s) return 0;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return 0;
+  const Req& q = it->second;
+  if (q.r.kind == EXA_REQ_ADERDG) {
+    const int B = q.r.dg.order + 1;
+    return (size_t)q.r.dg.n[0] * q.r.dg.n[1] * B * B * kV;
+  }
+  const size_t S = (size_t)q.fv.patch + 2 * q.fv.ghost;
+  return S * S * kV;
+}
+
+exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, double* sim_time,
+                               long long* steps_done) {
+  if (!s || !host_out) return set_error(EXA_EINVAL, "NULL argument");
+  const size_t n = exa_server_result_size(s, id);
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  Req& q = it->second;
+  if (!q.done) return set_error(EXA_EBUSY, "request still running");
+  exa_status_t st = EXA_OK;
+  if (q.r.kind == EXA_REQ_ADERDG) {
+    st = exa_ensemble_get_state(s->ens, q.slot, host_out);
+    if (sim_time) *sim_time = s->st_time[q.slot];
+    if (!st) st = exa_ensemble_remove(s->ens, q.slot);
+  } else {
+    double scal[2];
+    cudaError_t e = cudaMemcpyAsync(host_out, q.luh, n * sizeof(double), cudaMemcpyDeviceToHost, s->fv_st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(scal, q.dt_slot, 16, cudaMemcpyDeviceToHost, s->fv_st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->fv_st);
+    if (e != cudaSuccess) return cuda_status(e, "fv result");
+    if (sim_time) *sim_time = scal[1];
+    ens_arena_free(s->ens, q.off, q.bytes);
+  }
+  if (steps_done) *steps_done = q.steps_done;
+  s->live.erase(it);
+  return st;
+}
+
+exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_cells,
+                             size_t* arena_free_bytes) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (live_requests) *live_requests = (int)s->live.size();
+  if (active_dg_cells) *active_dg_cells = exa_ensemble_active_cells(s->ens);
+  return exa_ensemble_info(s->ens, nullptr, nullptr, arena_free_bytes);
+}
+
+}  // extern "C"

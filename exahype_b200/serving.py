@@ -1,0 +1,157 @@
+"""Serving loop over the C++ engine (exa_server_* in include/exa_kernels.h):
+a seeded Poisson stream of solve requests, a host-side admission queue for
+requests that do not fit yet, continuous batching (every tick advances all
+admitted requests by one step), and time-to-solution accounting."""
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _lib
+from ._lib import call, lib
+from .ensemble import SolveConfig, solve_config
+
+REQ_ADERDG = 0
+REQ_FV = 1
+
+
+class Request(C.Structure):
+    _fields_ = [('kind', C.c_int), ('dg', SolveConfig), ('fv_scheme', C.c_int), ('fv_patch', C.c_int),
+                ('fv_length', C.c_double), ('steps', C.c_longlong)]
+
+
+def dg_request(order, n, steps, ic_param=0.2, seed=0, noise=0.0, pde=_lib.PDE_EULER):
+    r = Request()
+    r.kind = REQ_ADERDG
+    r.dg = solve_config(order, (n, n), pde=pde, ic_kind=1, ic_param=ic_param, seed=seed, noise=noise)
+    r.steps = steps
+    return r
+
+
+def fv_request(patch, steps, scheme=1, ic_param=0.2, seed=0, noise=0.0, length=1.0, pde=_lib.PDE_EULER):
+    r = Request()
+    r.kind = REQ_FV
+    r.dg = solve_config(2, (1, 1), pde=pde, ic_param=ic_param, seed=seed, noise=noise)
+    r.fv_scheme, r.fv_patch, r.fv_length, r.steps = scheme, patch, length, steps
+    return r
+
+
+def footprint(req):
+    return int(lib().exa_server_footprint(C.byref(req)))
+
+
+class Server:
+    def __init__(self, hbm_budget, max_requests=512, precision=_lib.PREC_FP64):
+        h = C.c_void_p()
+        call('exa_server_create', int(hbm_budget), int(max_requests), int(precision), C.byref(h))
+        self.h = h
+
+    def submit(self, req):
+        """Returns the request id, or None if it does not fit right now."""
+        rid = C.c_uint64()
+        st = lib().exa_server_submit(self.h, C.byref(req), C.byref(rid))
+        if st == _lib.EXA_EBUSY:
+            return None
+        _lib.check(st, 'exa_server_submit')
+        return rid.value
+
+    def tick(self):
+        n = C.c_int()
+        st = lib().exa_server_tick(self.h, C.byref(n))
+        if st not in (_lib.EXA_OK, _lib.EXA_ENAN):
+            _lib.check(st, 'exa_server_tick')
+        return n.value
+
+    def completed(self, cap=4096):
+        ids = (C.c_uint64 * cap)()
+        n = C.c_int()
+        call('exa_server_completed', self.h, ids, cap, C.byref(n))
+        return [ids[i] for i in range(n.value)]
+
+    def result(self, rid):
+        size = int(lib().exa_server_result_size(self.h, C.c_uint64(rid)))
+        out = np.empty(size)
+        t, steps = C.c_double(), C.c_longlong()
+        call('exa_server_result', self.h, C.c_uint64(rid), out.ctypes.data, C.byref(t), C.byref(steps))
+        return out, t.value, steps.value
+
+    def info(self):
+        live, cells, free = C.c_int(), C.c_long(), C.c_size_t()
+        call('exa_server_info', self.h, C.byref(live), C.byref(cells), C.byref(free))
+        return dict(live=live.value, active_dg_cells=cells.value, arena_free=free.value)
+
+    def destroy(self):
+        if self.h:
+            call('exa_server_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def request_mix(n, seed, dg_fraction=0.25):
+    """Seeded request mix: ADER-DG (order ~U{2..5}, side log-uniform in
+    [9, 243], steps ~U{20..200}) and FV MUSCL-Hancock (side log-uniform in
+    [64, 1024], steps ~U{20..200})."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        steps = int(rng.integers(20, 201))
+        if rng.random() < dg_fraction:
+            side = int(round(np.exp(rng.uniform(np.log(9), np.log(243)))))
+            out.append(('dg', dg_request(int(rng.integers(2, 6)), side, steps, ic_param=float(rng.uniform(0.05, 0.3)),
+                                         seed=10_000 + i)))
+        else:
+            side = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+            out.append(('fv', fv_request(side, steps, scheme=1, ic_param=float(rng.uniform(0.05, 0.3)),
+                                         seed=20_000 + i)))
+    return out
+
+
+def run_poisson(server, requests, rate, seed, collect=False, time_limit=None):
+    """Releases `requests` at seeded Poisson arrival times (rate per second,
+    host wall clock), ticks the server continuously, and returns per-request
+    time-to-solution (completion - arrival) plus throughput numbers."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(requests)))
+    t0 = time.perf_counter()
+    queue = []          # indices waiting for admission
+    live = {}           # id -> index
+    done = {}           # index -> (completion time, sim time, steps, state or None)
+    nxt = 0
+    cell_updates = 0
+    ticks = 0
+    while len(done) < len(requests):
+        now = time.perf_counter() - t0
+        if time_limit and now > time_limit:
+            break
+        while nxt < len(requests) and arrivals[nxt] <= now:
+            queue.append(nxt)
+            nxt += 1
+        still = []
+        for i in queue:
+            rid = server.submit(requests[i][1])
+            if rid is None:
+                still.append(i)
+            else:
+                live[rid] = i
+        queue = still
+        if not live:
+            if nxt < len(requests):
+                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.01)))
+            continue
+        server.tick()
+        ticks += 1
+        for rid in server.completed():
+            i = live.pop(rid)
+            state, sim_t, steps = server.result(rid)
+            r = requests[i][1]
+            cells = r.dg.n[0] * r.dg.n[1] if r.kind == REQ_ADERDG else r.fv_patch * r.fv_patch
+            cell_updates += cells * steps
+            done[i] = (time.perf_counter() - t0, sim_t, steps, state if collect else None)
+    wall = time.perf_counter() - t0
+    lat = np.array([done[i][0] - arrivals[i] for i in sorted(done)])
+    return dict(latency=lat, done=done, arrivals=arrivals, wall=wall, ticks=ticks, cell_updates=cell_updates)

@@ -347,6 +347,40 @@ long exa_ensemble_active_cells(exa_ensemble* e);
 exa_status_t exa_ensemble_info(exa_ensemble* e, int* grid_ctas, int* nitems,
                                size_t* arena_free_bytes);
 
+/* -------------------------------------------------------- serving --
+ * Continuous batching of solve requests: admission by device-memory
+ * footprint (EXA_EBUSY when a request does not fit now), state resident on
+ * the device until the result is collected, every tick advances every
+ * active request one step (all ADER-DG requests in one persistent launch,
+ * FV patches on a second stream that overlaps it). */
+typedef struct exa_server exa_server;
+
+#define EXA_REQ_ADERDG 0
+#define EXA_REQ_FV 1
+
+typedef struct {
+  int kind;               /* EXA_REQ_ADERDG or EXA_REQ_FV */
+  exa_solve_config_t dg;  /* ADER-DG solve; for FV: pde, ic_param, seed, noise */
+  int fv_scheme;          /* 0 Godunov, 1 MUSCL-Hancock */
+  int fv_patch;           /* cells per side */
+  double fv_length;       /* domain extent */
+  long long steps;        /* step budget (>= 1) */
+} exa_request_t;
+
+size_t exa_server_footprint(const exa_request_t* r);
+exa_status_t exa_server_create(size_t hbm_budget, int max_requests, int precision, exa_server** out);
+exa_status_t exa_server_destroy(exa_server* s);
+exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* id);
+exa_status_t exa_server_tick(exa_server* s, int* ncompleted);
+exa_status_t exa_server_completed(exa_server* s, uint64_t* ids, int cap, int* n);
+size_t exa_server_result_size(exa_server* s, uint64_t id);
+/* copies the final state (ADER-DG: [cell][y][x][var]; FV: the patch incl.
+ * ghosts, [y][x][var]) and releases the request's device memory */
+exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, double* sim_time,
+                               long long* steps_done);
+exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_cells,
+                             size_t* arena_free_bytes);
+
 /* ------------------------------------------------ finite volumes (2D) --
  * One patch of patch x patch cells with `ghost` ghost layers, layout
  * [y][x][nData] over (patch+2*ghost)^2 cells (reference FV solvers,

@@ -1,0 +1,124 @@
+"""Serving engine: admission by footprint, continuous batching, results
+identical alone and in a mix, FV requests against the oracle."""
+import numpy as np
+import pytest
+
+import _oracle as O
+import exahype_b200 as E
+from exahype_b200 import serving as S
+
+pytestmark = pytest.mark.gpu
+
+
+def run_to_completion(server, reqs, submit_at=None):
+    """Submits reqs[i] at tick submit_at[i] (0 by default), ticks until all
+    finish; returns {i: state}."""
+    submit_at = submit_at or [0] * len(reqs)
+    ids, out, tick = {}, {}, 0
+    while len(out) < len(reqs):
+        for i, r in enumerate(reqs):
+            if i not in ids.values() and submit_at[i] <= tick:
+                rid = server.submit(r)
+                if rid is not None:
+                    ids[rid] = i
+        server.tick()
+        tick += 1
+        for rid in server.completed():
+            out[ids[rid]] = server.result(rid)
+        assert tick < 10000
+    return out
+
+
+def test_results_identical_alone_and_in_mix():
+    x_dg = S.dg_request(4, 15, 12, ic_param=0.25, seed=3, noise=1e-3)
+    x_fv = S.fv_request(48, 9, scheme=1, ic_param=0.2, seed=4, noise=1e-3)
+    alone = {}
+    for name, r in (('dg', x_dg), ('fv', x_fv)):
+        srv = S.Server(1 << 28)
+        alone[name] = run_to_completion(srv, [r])[0]
+        srv.destroy()
+    others = [S.dg_request(2, 30, 20, seed=5), S.fv_request(100, 5, scheme=0, seed=6),
+              S.dg_request(5, 9, 7, seed=7), S.fv_request(64, 15, scheme=1, seed=8),
+              S.dg_request(3, 40, 3, seed=9)]
+    reqs = others[:2] + [x_dg] + others[2:4] + [x_fv] + others[4:]
+    srv = S.Server(1 << 29)
+    got = run_to_completion(srv, reqs, submit_at=[0, 1, 2, 2, 4, 3, 5])
+    srv.destroy()
+    for name, i in (('dg', 2), ('fv', 5)):
+        a, b = alone[name], got[i]
+        assert np.array_equal(a[0], b[0]), name
+        assert a[1] == b[1] and a[2] == b[2]
+
+
+def test_dg_request_matches_grid():
+    r = S.dg_request(3, 21, 10, ic_param=0.2, seed=11, noise=1e-3)
+    srv = S.Server(1 << 28)
+    state, t, steps = run_to_completion(srv, [r])[0]
+    srv.destroy()
+    g = E.ADERDGGrid(2, 3, (21, 21))
+    g.init(kind=1, param=0.2, seed=11, noise=1e-3)
+    g.step(10)
+    ref = g.get_state()
+    assert steps == 10
+    assert np.linalg.norm(state - ref) / np.linalg.norm(ref) < 1e-13
+    assert abs(t - g.status()['time']) <= 1e-13 * t
+    g.destroy()
+
+
+def fv_ic(P, g, amp, length=1.0):
+    Sz = P + 2 * g
+    h = length / P
+    j, k = np.mgrid[0:Sz, 0:Sz]
+    x, y = (k - g + 0.5) * h, (j - g + 0.5) * h
+    rho = 1.0 + amp * np.sin(2 * np.pi * (x + y))
+    q = np.zeros((Sz, Sz, 5))
+    q[..., 0] = rho
+    q[..., 1] = rho
+    q[..., 2] = rho
+    q[..., 4] = 1.0 / 0.4 + rho
+    return q.ravel()
+
+
+@pytest.mark.parametrize('scheme', [0, 1])
+def test_fv_request_matches_oracle(scheme):
+    P, steps, amp = 40, 12, 0.2
+    g = 1 if scheme == 0 else 2
+    srv = S.Server(1 << 26)
+    state, t, n = run_to_completion(srv, [S.fv_request(P, steps, scheme=scheme, ic_param=amp, noise=0.0)])[0]
+    srv.destroy()
+    ref = fv_ic(P, g, amp)
+    tr = 0.0
+    for _ in range(steps):
+        tr += O.lib().orc_fv_patch_step_2d(scheme, P, 0, ref, np.array([1.0, 1.0]), 0.0, None)
+    # compare the interior (ghosts are refreshed at the start of each step)
+    Sz = P + 2 * g
+    a = state.reshape(Sz, Sz, 5)[g:g + P, g:g + P]
+    b = ref.reshape(Sz, Sz, 5)[g:g + P, g:g + P]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    assert abs(t - tr) <= 1e-12 * tr and n == steps
+
+
+def test_admission_waits_for_memory():
+    big = S.dg_request(5, 60, 4, seed=1)
+    fp = S.footprint(big)
+    srv = S.Server(int(fp * 1.6))
+    a = srv.submit(big)
+    assert a is not None
+    assert srv.submit(S.dg_request(5, 60, 4, seed=2)) is None  # EXA_EBUSY: does not fit
+    for _ in range(4):
+        srv.tick()
+    assert srv.completed() == [a]
+    srv.result(a)
+    assert srv.submit(S.dg_request(5, 60, 4, seed=2)) is not None
+    srv.destroy()
+
+
+def test_poisson_stream_small():
+    reqs = [S.dg_request(2 + (i % 4), 9 + 3 * i, 20 + i, seed=i) if i % 3 else S.fv_request(64 + 8 * i, 20, seed=i)
+            for i in range(12)]
+    srv = S.Server(1 << 29)
+    res = S.run_poisson(srv, [('x', r) for r in reqs], rate=200.0, seed=0)
+    srv.destroy()
+    assert len(res['done']) == 12
+    assert (res['latency'] > 0).all()
+    assert res['cell_updates'] > 0
