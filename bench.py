@@ -262,8 +262,12 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
-    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble'],
-                    help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves')
+    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving'],
+                    help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
+                         'serving: Poisson stream of solve requests')
+    ap.add_argument('--requests', type=int, default=400)
+    ap.add_argument('--rate', type=float, default=200.0)
+    ap.add_argument('--dg-fraction', type=float, default=0.25)
     ap.add_argument('--nsolves', type=int, default=512)
     ap.add_argument('--tune', action='append', default=[],
                     help='key=value tuning knob passed to exa_tune_set (see include/exa_kernels.h)')
@@ -281,6 +285,9 @@ def main():
 
     if args.workload == 'ensemble':
         run_ensemble(args, rank, world, dist)
+        return
+    if args.workload == 'serving':
+        run_serving(args, rank, world, dist)
         return
     if args.impl == 'reference':
         run_reference(args, rank, world)
@@ -525,6 +532,52 @@ def run_ensemble(args, rank, world, dist):
                                                 'cells': out['fp64']['cells']},
                 'fp64': out['fp64'], 'mixed': out['mixed'],
                 'mixed_speedup': out['mixed']['value'] / out['fp64']['value']}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- serving
+def run_serving(args, rank, world, dist):
+    """Seeded Poisson stream of solve requests (ADER-DG 2D N=2..5, sides
+    9..243 log-uniform, 20-200 steps; FV MUSCL-Hancock patches 64..1024
+    log-uniform, 20-200 steps), continuous batching on one GPU."""
+    import exahype_b200 as E
+    from exahype_b200 import serving as S
+    E.lib().exa_set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    reqs = S.request_mix(args.requests, seed=args.seed + rank, dg_fraction=args.dg_fraction)
+    budget = 64 << 30
+    srv = S.Server(budget, max_requests=1024)
+    # warm-up: a few small requests through every code path
+    S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
+                  rate=1e4, seed=1)
+    if dist:
+        dist.barrier()
+    res = S.run_poisson(srv, reqs, rate=args.rate, seed=args.seed + 17 + rank)
+    srv.destroy()
+    lat = res['latency']
+    kinds = [reqs[i][0] for i in sorted(res['done'])]
+    dg_lat = np.array([l for l, k in zip(lat, kinds) if k == 'dg'])
+    fv_lat = np.array([l for l, k in zip(lat, kinds) if k == 'fv'])
+    if rank == 0:
+        line = {'metric': 'serving p99 time-to-solution (Poisson %.0f req/s, ADER-DG + FV MUSCL-Hancock mix)' % args.rate,
+                'value': float(np.percentile(lat, 99)), 'unit': 's', 'higher_is_better': False,
+                'n_gpus': world, 'steps': None, 'warmup': 5, 'dtype': 'f64', 'data': 'synthetic',
+                'scaling': 'weak', 'vs_baseline': None,
+                'p50_s': float(np.percentile(lat, 50)), 'p99_s': float(np.percentile(lat, 99)),
+                'p50_dg_s': float(np.percentile(dg_lat, 50)) if len(dg_lat) else None,
+                'p99_dg_s': float(np.percentile(dg_lat, 99)) if len(dg_lat) else None,
+                'p50_fv_s': float(np.percentile(fv_lat, 50)) if len(fv_lat) else None,
+                'p99_fv_s': float(np.percentile(fv_lat, 99)) if len(fv_lat) else None,
+                'aggregate_cell_updates_per_s': res['cell_updates'] / res['wall'],
+                'requests': len(reqs), 'completed': len(res['done']), 'wall_s': res['wall'],
+                'ticks': res['ticks'], 'offered_rate_per_s': args.rate,
+                'achieved_rate_per_s': len(res['done']) / res['wall'],
+                'config': {'workload': 'serving', 'dg_fraction': args.dg_fraction,
+                           'dg': 'order U{2..5}, side log-U[9,243], steps U{20..200}',
+                           'fv': 'MUSCL-Hancock, side log-U[64,1024], steps U{20..200}',
+                           'hbm_budget_gb': budget / 2 ** 30}}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
