@@ -239,13 +239,20 @@ METRIC = '3D Euler ADER-DG N=4 cell-updates/s'
 
 
 def config_dict(args, world):
-    return {'workload': '3D Euler ADER-DG N=%d, %d^3 periodic cells, isentropic vortex + 1e-3 density noise'
-                        % (args.order, args.n),
-            'order': args.order, 'cells': args.n ** 3, 'nodes_per_cell': (args.order + 1) ** 3,
+    if world == 1:
+        wl = '3D Euler ADER-DG N=%d, %d^3 periodic cells, isentropic vortex + 1e-3 density noise' % (
+            args.order, args.n)
+    else:
+        wl = ('3D Euler ADER-DG N=%d, one periodic %dx%dx%d grid cut into %d z-slabs of %d^3 cells, '
+              'isentropic vortex + 1e-3 density noise' % (args.order, args.n, args.n, args.n * world, world,
+                                                          args.n))
+    return {'workload': wl,
+            'order': args.order, 'cells': args.n ** 3 * world, 'cells_per_gpu': args.n ** 3,
+            'nodes_per_cell': (args.order + 1) ** 3,
             'precision': args.precision, 'dt_policy': 'CFL*PNPM[N], CFL=0.9',
             'l2_flush': 'inputs larger than L2 (state + faces %.1f GB per GPU)' %
                         (args.n ** 3 * (2 * 125 * 5 + 2 * 6 * 25 * 5) * 8 / 1e9 if args.order == 4 else 0),
-            'parallelism': 'replicas%d' % world}
+            'parallelism': 'slab-z%d (NCCL face-layer exchange + dt min)' % world if world > 1 else 'single'}
 
 
 # ---------------------------------------------------------------- ours
@@ -278,10 +285,20 @@ def main():
     world = int(os.environ.get('WORLD_SIZE', '1'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
     dist = None
+    cpu_group = None
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=600))
+        if args.workload == 'grid3d' and args.impl == 'ours':
+            # one grid cut into slabs: face layers and the dt minimum move over
+            # NCCL; host-side barriers and maxima over a gloo group
+            torch.cuda.set_device(local)
+            dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device('cuda', local))
+            cpu_group = dist.new_group(backend='gloo')
+        else:
+            dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=600))
 
     if args.workload == 'ensemble':
         run_ensemble(args, rank, world, dist)
@@ -308,17 +325,17 @@ def main():
 
     def barrier():
         if dist:
-            dist.barrier()
+            dist.barrier(group=cpu_group)
 
     def max_over_ranks(x):
         if not dist:
             return x
         import torch
         t = torch.tensor([x], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX, group=cpu_group)
         return float(t.item())
 
-    ctx = dict(E=E, args=args, rank=rank, world=world, local=local, barrier=barrier,
+    ctx = dict(E=E, args=args, rank=rank, world=world, local=local, barrier=barrier, dist=dist,
                max_over_ranks=max_over_ranks, fp64_peak=fp64_peak.value)
     primary = 'mixed' if args.precision == 'mixed' else 'fp64'
     res = measure(ctx, primary, with_e2e=not args.no_e2e)
@@ -361,8 +378,74 @@ def main():
                         'luh, F(luh) and its derivative, the update, Riemann fluxes, faces and dt in FP64'}
         print(json.dumps(line), flush=True)
     if dist:
-        dist.barrier()
+        dist.barrier(group=cpu_group)
         dist.destroy_process_group()
+
+
+class GridRun:
+    """The timed grid of this rank.  One GPU: the whole n^3 periodic grid
+    (CUDA-graph replay of its steps).  N GPUs: slab `rank` of one periodic
+    n x n x (n N) grid (n^3 cells per GPU, weak scaling), its boundary face
+    layers and the dt minimum exchanged over NCCL every step."""
+
+    def __init__(self, ctx, prec):
+        E, args = ctx['E'], ctx['args']
+        n, order, world = args.n, args.order, ctx['world']
+        ic = dict(kind=0, param=5.0, seed=args.seed, noise=1e-3)
+        self.slab = None
+        if world == 1:
+            self.g = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
+            self.g.init(**ic)
+        else:
+            from exahype_b200 import slab as SL
+            self.SL = SL
+            self.slab = SL.SlabGrid(3, order, (n, n, n * world), ctx['rank'], world,
+                                    length=(1.0, 1.0, float(world)), precision=prec)
+            self.slab.init(**ic)
+            self.g = self.slab.grid
+            self.ring = SL.DistRing(ctx['dist'])
+            self.primed = False
+        self.ncells = self.g.ncells
+        self.state_size = self.g.state_size
+
+    def step(self, k, per_step_read=False):
+        """k steps; per_step_read: each step returns its dt (one GPU) or the
+        grid's scalar status (slabs) to the host."""
+        if self.slab is None:
+            if per_step_read:
+                for _ in range(k):
+                    self.g.step(1, want_dt=True)
+            else:
+                self.g.step(k)
+            return
+        if not self.primed:
+            self.SL.prime(self.ring, self.slab)
+            self.primed = True
+        for _ in range(k if per_step_read else 1):
+            self.SL.step(self.ring, self.slab, 1 if per_step_read else k)
+            if per_step_read:
+                self.g.status()
+
+    def set_state_ptr(self, ptr):
+        self.E_call('exa_aderdg_grid_set_state', ptr)
+        if self.slab is not None:
+            self.primed = False
+
+    def get_state_ptr(self, ptr):
+        self.E_call('exa_aderdg_grid_get_state', ptr)
+
+    def E_call(self, name, ptr):
+        from exahype_b200 import _lib
+        _lib.call(name, self.g.h, ptr)
+
+    def per_step_d2h_bytes(self):
+        return 8 if self.slab is None else 56
+
+    def destroy(self):
+        if self.slab is not None:
+            self.slab.destroy()
+        else:
+            self.g.destroy()
 
 
 def measure(ctx, precision, with_e2e):
@@ -372,11 +455,11 @@ def measure(ctx, precision, with_e2e):
     from exahype_b200 import Timer
     n, order = args.n, args.order
     prec = E.PREC_MIXED if precision == 'mixed' else E.PREC_FP64
-    grid = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
-    grid.init(kind=0, param=5.0, seed=args.seed + ctx['rank'], noise=1e-3)
+    run = GridRun(ctx, prec)
+    grid = run.g
     stream = grid.stream()
     initial = grid.get_state() if with_e2e else None
-    grid.step(args.warmup)
+    run.step(args.warmup)
     st0 = grid.status()
     grid.profile(True)
     E.device.synchronize()
@@ -386,7 +469,7 @@ def measure(ctx, precision, with_e2e):
     timer = Timer()
     l0 = E.launch_count()
     timer.start(stream)
-    grid.step(args.steps)
+    run.step(args.steps)
     timer.stop(stream)
     ms = timer.elapsed_ms()
     E.device.synchronize()
@@ -396,7 +479,7 @@ def measure(ctx, precision, with_e2e):
     st1 = grid.status()
     phases = grid.phase_times()
     ms_max = ctx['max_over_ranks'](ms)
-    ncells = grid.ncells
+    ncells = run.ncells
     value = ctx['world'] * ncells * args.steps / (ms_max * 1e-3)
     kbar = (st1['picard_iters'] - st0['picard_iters']) / (ncells * args.steps)
     total_flop, pred_flop = flops_per_cell_update(3, order, kbar)
@@ -427,23 +510,23 @@ def measure(ctx, precision, with_e2e):
         ctx['barrier']()
         t2 = Timer()
         t2.start(stream)
-        E._lib.call('exa_aderdg_grid_set_state', grid.h, pin.array.ctypes.data)
-        for _ in range(args.steps):
-            grid.step(1, want_dt=True)
-        E._lib.call('exa_aderdg_grid_get_state', grid.h, pin.array.ctypes.data)
+        run.set_state_ptr(pin.array.ctypes.data)
+        run.step(args.steps, per_step_read=True)
+        run.get_state_ptr(pin.array.ctypes.data)
         t2.stop(stream)
         ms_e2e = ctx['max_over_ranks'](t2.elapsed_ms())
         ctx['barrier']()
         sb = grid.state_size * 8
         out['e2e'] = {'value': ctx['world'] * ncells * args.steps / (ms_e2e * 1e-3), 'unit': 'cell-updates/s',
-                      'h2d_bytes_per_step': sb / args.steps, 'd2h_bytes_per_step': 8 + sb / args.steps,
+                      'h2d_bytes_per_step': sb / args.steps,
+                      'd2h_bytes_per_step': run.per_step_d2h_bytes() + sb / args.steps,
                       'note': 'one solve per timed region: state upload from pinned host memory, K steps each '
                               'returning its dt to the host, final state download'}
         pin.free()
-    if ctx['rank'] == 0 and precision == 'fp64':
+    if ctx['rank'] == 0 and precision == 'fp64' and ctx['world'] == 1:
         out['state'] = grid.get_state()
         out['dt'] = grid.step(1, want_dt=True)[0]
-    grid.destroy()
+    run.destroy()
     return out
 
 

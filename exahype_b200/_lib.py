@@ -123,6 +123,12 @@ SIGNATURES = {
     'exa_aderdg_grid_device_state': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(u64), C.POINTER(u64), C.POINTER(i32)]),
     'exa_aderdg_grid_ncells': (i64, [vp]),
+    'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
+    'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                                           C.POINTER(sz)]),
+    'exa_aderdg_grid_dt_slot': (i32, [vp, C.POINTER(vp)]),
+    'exa_aderdg_grid_phase': (i32, [vp, i32]),
+    'exa_aderdg_grid_init_slab': (i32, [vp, i32, f64, u64, f64, i32, i32]),
     'exa_ensemble_footprint': (sz, [vp]),
     'exa_ensemble_create': (i32, [i32, i32, sz, C.POINTER(vp)]),
     'exa_ensemble_destroy': (i32, [vp]),

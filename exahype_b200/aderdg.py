@@ -202,6 +202,30 @@ class ADERDGGrid:
         call('exa_aderdg_grid_device_state', self.h, C.byref(p))
         return p
 
+    # -- slab decomposition (see exahype_b200.slab) --
+    def set_halo(self, enable=True):
+        call('exa_aderdg_grid_set_halo', self.h, int(enable))
+
+    def halo_buffers(self):
+        """(send_lo, send_hi, recv_lo, recv_hi) device pointers and the
+        number of doubles in each."""
+        p = [C.c_void_p() for _ in range(4)]
+        n = C.c_size_t()
+        call('exa_aderdg_grid_halo_buffers', self.h, *[C.byref(x) for x in p], C.byref(n))
+        return [x.value for x in p], int(n.value)
+
+    def dt_slot_ptr(self):
+        p = C.c_void_p()
+        call('exa_aderdg_grid_dt_slot', self.h, C.byref(p))
+        return p.value
+
+    def phase(self, phase):
+        call('exa_aderdg_grid_phase', self.h, int(phase))
+
+    def init_slab(self, rank, nranks, kind=0, param=5.0, seed=1234, noise=0.0):
+        call('exa_aderdg_grid_init_slab', self.h, int(kind), float(param), int(seed), float(noise),
+             int(rank), int(nranks))
+
     def status(self):
         t, it, nc, nan = C.c_double(), C.c_uint64(), C.c_uint64(), C.c_int()
         st = lib().exa_aderdg_grid_status(self.h, C.byref(t), C.byref(it), C.byref(nc), C.byref(nan))

@@ -74,13 +74,22 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     for (int k = s; k < FV; k += G) {
       const int f = k / (NF * V), r = k % (NF * V);
       const int d = f >> 1;
+      sQo[k] = qo[k];
+      sFo[k] = fo[k];
+      const bool up = f & 1;
+      if (d == DIM - 1 && a.halo_lo && (up ? cc[d] + 1 == a.n[d] : cc[d] == 0)) {
+        // across a slab boundary: the adjacent slab's face data
+        const long lc = DIM == 3 ? (long)cc[1] * a.n[0] + cc[0] : cc[0];
+        const double* h = (up ? a.halo_hi : a.halo_lo) + lc * 2 * NF * V;
+        sQn[k] = h[r];
+        sFn[k] = h[NF * V + r];
+        continue;
+      }
       int nc[3] = {cc[0], cc[1], cc[2]};
-      nc[d] = (f & 1) ? (nc[d] + 1 == a.n[d] ? 0 : nc[d] + 1) : (nc[d] == 0 ? a.n[d] - 1 : nc[d] - 1);
+      nc[d] = up ? (nc[d] + 1 == a.n[d] ? 0 : nc[d] + 1) : (nc[d] == 0 ? a.n[d] - 1 : nc[d] - 1);
       const long nb = DIM == 3 ? ((long)nc[2] * a.n[1] + nc[1]) * a.n[0] + nc[0]
                                : (long)nc[1] * a.n[0] + nc[0];
       const long off = nb * FV + (f ^ 1) * NF * V + r;
-      sQo[k] = qo[k];
-      sFo[k] = fo[k];
       sQn[k] = a.lQhbnd[off];
       sFn[k] = a.lFhbnd[off];
     }

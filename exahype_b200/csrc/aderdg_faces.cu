@@ -319,6 +319,7 @@ __device__ __forceinline__ double noise_u01(unsigned long long seed, unsigned lo
 
 struct ICArgs {
   long ncells;
+  long cell_offset;
   int dim, B, order, kind;
   int n[3];
   double dx[3];
@@ -330,14 +331,15 @@ __global__ void k_grid_ic(ICArgs a, double* luh) {
   const int nn = a.dim == 3 ? a.B * a.B * a.B : a.B * a.B;
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= a.ncells * nn) return;
-  const long c = gid / nn;
+  const long c = gid / nn + a.cell_offset;  // index in the whole domain
   const int s = (int)(gid % nn);
   const int cx = (int)(c % a.n[0]), cy = (int)((c / a.n[0]) % a.n[1]);
+  const unsigned long long node = (unsigned long long)c * nn + s;
   const int ix = s % a.B, iy = (s / a.B) % a.B;
   const double* nodes = c_dg[a.order].nodes;
   const double x = (cx + nodes[ix]) * a.dx[0];
   const double y = (cy + nodes[iy]) * a.dx[1];
-  const double nz = a.noise != 0.0 ? a.noise * (2.0 * noise_u01(a.seed, (unsigned long long)gid) - 1.0) : 0.0;
+  const double nz = a.noise != 0.0 ? a.noise * (2.0 * noise_u01(a.seed, node) - 1.0) : 0.0;
   const double pi = 3.14159265358979323846;
   double rho, u, v, p;
   if (a.kind == 0) {
@@ -367,8 +369,9 @@ __global__ void k_grid_ic(ICArgs a, double* luh) {
 
 exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, double* luh,
                             int kind, double param, uint64_t seed, double noise,
-                            cudaStream_t st) {
+                            cudaStream_t st, long cell_offset, int n_last_global) {
   ICArgs a;
+  a.cell_offset = cell_offset;
   a.dim = dim;
   a.order = order;
   a.B = order + 1;
@@ -379,6 +382,9 @@ exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, 
     a.dx[i] = dx[i];
     a.ncells *= a.n[i];
   }
+  // coordinates come from the whole-domain index: the last dimension spans
+  // n_last_global cells there
+  if (n_last_global > 0) a.n[dim - 1] = n_last_global;
   a.param = param;
   a.noise = noise;
   a.seed = seed;

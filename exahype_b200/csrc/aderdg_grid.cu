@@ -46,6 +46,25 @@ __global__ void k_prime(GridDev* g) {
   g->dt_next = 0x7FF0000000000000ULL;
 }
 
+// Slab boundary faces -> send buffers.  The lowest layer's lower face of the
+// last dimension (face 2(dim-1)) goes to the slab below, the highest layer's
+// upper face (face 2(dim-1)+1) to the slab above; both as
+// [layer cell][Q | F][face node][var].  One thread per double of a face.
+__global__ void k_halo_pack(long layer, long ncells, int fv, int nfv, int fdim, const double* qb,
+                            const double* fb, double* send_lo, double* send_hi) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 2 * layer * nfv) return;
+  const bool hi = gid >= layer * nfv;
+  const long k = hi ? gid - layer * nfv : gid;
+  const long lc = k / nfv;
+  const int r = (int)(k % nfv);
+  const long cell = hi ? ncells - layer + lc : lc;
+  const long src = cell * fv + (long)(2 * fdim + (hi ? 1 : 0)) * nfv + r;
+  double* dst = (hi ? send_hi : send_lo) + lc * 2 * nfv;
+  dst[r] = qb[src];
+  dst[nfv + r] = fb[src];
+}
+
 }  // namespace exa
 
 using namespace exa;
@@ -62,6 +81,10 @@ struct exa_aderdg_grid {
   double* fb = nullptr;
   GridDev* gd = nullptr;
   double* dt_log = nullptr;
+  // slab decomposition (exa_aderdg_grid_set_halo): send / receive buffers
+  double* halo = nullptr;  // send_lo | send_hi | recv_lo | recv_hi
+  long layer = 0;          // cells in one layer of the last dimension
+  size_t halo_count = 0;   // doubles per buffer
   int log_cap = 4096;
   double dt_factor = 0;
   bool primed = false;
@@ -114,8 +137,7 @@ static exa_status_t grid_prime(exa_aderdg_grid* g) {
   return EXA_OK;
 }
 
-static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
-  if (g->profile) cudaEventRecord(g->ev[0], g->st);
+static exa_status_t grid_predict(exa_aderdg_grid* g) {
   PredArgs a{};
   a.ncells = g->ncells;
   a.luh = g->luh;
@@ -129,7 +151,20 @@ static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
   a.stats = g->gd->stats;
   a.precision = g->cfg.precision;
   if (exa_status_t s = launch_predictor(g->desc, a, 0, g->st)) return s;
-  if (g->profile) cudaEventRecord(g->ev[1], g->st);
+  if (g->halo) {
+    const int B = g->cfg.order + 1;
+    const int nfv = (g->cfg.dim == 3 ? B * B : B) * kV;
+    const long work = 2 * g->layer * nfv;
+    k_halo_pack<<<(unsigned)((work + 255) / 256), 256, 0, g->st>>>(
+        g->layer, g->ncells, 2 * g->cfg.dim * nfv, nfv, g->cfg.dim - 1, g->qb, g->fb, g->halo,
+        g->halo + g->halo_count);
+    count_launch();
+    if (exa_status_t s = cuda_status(cudaGetLastError(), "k_halo_pack")) return s;
+  }
+  return EXA_OK;
+}
+
+static exa_status_t grid_correct(exa_aderdg_grid* g) {
   CorrArgs c{};
   c.ncells = g->ncells;
   for (int i = 0; i < 3; i++) {
@@ -144,10 +179,25 @@ static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
   c.dt_next = g->cfg.dt_policy == 2 ? nullptr : &g->gd->dt_next;
   c.dt_factor = g->dt_factor;
   c.nan_flag = &g->gd->nan_flag;
-  if (exa_status_t s = launch_corrector(g->cfg.dim, g->cfg.order, g->cfg.pde, c, g->st)) return s;
+  if (g->halo) {
+    c.halo_lo = g->halo + 2 * g->halo_count;
+    c.halo_hi = g->halo + 3 * g->halo_count;
+  }
+  return launch_corrector(g->cfg.dim, g->cfg.order, g->cfg.pde, c, g->st);
+}
+
+static exa_status_t grid_commit(exa_aderdg_grid* g) {
   k_commit<<<1, 1, 0, g->st>>>(g->gd, g->dt_log, g->log_cap, g->cfg.dt_policy == 2, g->cfg.dt_fixed);
   count_launch();
-  if (exa_status_t s = cuda_status(cudaGetLastError(), "k_commit")) return s;
+  return cuda_status(cudaGetLastError(), "k_commit");
+}
+
+static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
+  if (g->profile) cudaEventRecord(g->ev[0], g->st);
+  if (exa_status_t s = grid_predict(g)) return s;
+  if (g->profile) cudaEventRecord(g->ev[1], g->st);
+  if (exa_status_t s = grid_correct(g)) return s;
+  if (exa_status_t s = grid_commit(g)) return s;
   if (g->profile) {
     cudaEventRecord(g->ev[2], g->st);
     cudaError_t e = cudaEventSynchronize(g->ev[2]);
@@ -230,6 +280,7 @@ exa_status_t exa_aderdg_grid_destroy(exa_aderdg_grid* g) {
   cudaFree(g->fb);
   cudaFree(g->gd);
   cudaFree(g->dt_log);
+  cudaFree(g->halo);
   if (g->st) cudaStreamDestroy(g->st);
   delete g;
   return EXA_OK;
@@ -312,6 +363,8 @@ exa_status_t exa_aderdg_grid_device_state(exa_aderdg_grid* g, double** luh_dev) 
 
 exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_host) {
   if (!g || nsteps < 0) return set_error(EXA_EINVAL, "bad argument");
+  if (g->halo)
+    return set_error(EXA_EINVAL, "a grid with slab halos advances through exa_aderdg_grid_phase");
   if (dt_host && nsteps > g->log_cap) return set_error(EXA_EINVAL, "too many steps for the dt log");
   if (!g->primed)
     if (exa_status_t s = grid_prime(g)) return s;
@@ -368,6 +421,117 @@ exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time, uint64_t* 
   if (nan_flag) *nan_flag = h.nan_flag;
   if (h.nan_flag) return EXA_ENAN;
   return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_init_slab(exa_aderdg_grid* g, int kind, double param, uint64_t seed,
+                                       double noise_amp, int rank, int nranks) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (kind < 0 || kind > 1) return set_error(EXA_EINVAL, "unknown initial condition");
+  if (nranks < 1 || rank < 0 || rank >= nranks) return set_error(EXA_EINVAL, "bad slab rank");
+  const int last = g->cfg.n[g->cfg.dim - 1];
+  if (exa_status_t s = launch_grid_ic(g->cfg.dim, g->cfg.order, g->cfg.n, g->desc.dx, g->luh, kind,
+                                      param, seed, noise_amp, g->st, (long)rank * g->ncells,
+                                      last * nranks))
+    return s;
+  g->primed = false;
+  return cuda_status(cudaStreamSynchronize(g->st), "grid init");
+}
+
+exa_status_t exa_aderdg_grid_set_halo(exa_aderdg_grid* g, int enable) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (g->graph) {
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  if (!enable) {
+    cudaStreamSynchronize(g->st);
+    cudaFree(g->halo);
+    g->halo = nullptr;
+    g->halo_count = 0;
+    return EXA_OK;
+  }
+  if (g->halo) return EXA_OK;
+  const int B = g->cfg.order + 1;
+  const size_t nfv = (size_t)(g->cfg.dim == 3 ? B * B : B) * kV;
+  g->layer = g->ncells / g->cfg.n[g->cfg.dim - 1];
+  g->halo_count = (size_t)g->layer * 2 * nfv;
+  cudaError_t e = cudaMalloc(&g->halo, 4 * g->halo_count * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->halo, 0, 4 * g->halo_count * sizeof(double), g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) {
+    cudaFree(g->halo);
+    g->halo = nullptr;
+    g->halo_count = 0;
+    return cuda_status(e, "halo buffers");
+  }
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_halo_buffers(exa_aderdg_grid* g, double** send_lo, double** send_hi,
+                                          double** recv_lo, double** recv_hi, size_t* count) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (!g->halo) return set_error(EXA_EINVAL, "grid has no slab halos");
+  if (send_lo) *send_lo = g->halo;
+  if (send_hi) *send_hi = g->halo + g->halo_count;
+  if (recv_lo) *recv_lo = g->halo + 2 * g->halo_count;
+  if (recv_hi) *recv_hi = g->halo + 3 * g->halo_count;
+  if (count) *count = g->halo_count;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_dt_slot(exa_aderdg_grid* g, uint64_t** slot) {
+  if (!g || !slot) return set_error(EXA_EINVAL, "NULL argument");
+  *slot = (uint64_t*)&g->gd->dt_next;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_phase(exa_aderdg_grid* g, int phase) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  switch (phase) {
+    case EXA_PHASE_PRIME_LOCAL: {
+      if (g->cfg.dt_policy == 2) return set_error(EXA_EINVAL, "fixed dt needs no priming");
+      const unsigned long long inf = 0x7FF0000000000000ULL;
+      cudaError_t e = cudaMemcpyAsync(&g->gd->dt_next, &inf, 8, cudaMemcpyHostToDevice, g->st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+      if (e != cudaSuccess) return cuda_status(e, "prime dt slot");
+      return launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr, &g->gd->dt_next, g->st);
+    }
+    case EXA_PHASE_PRIME_COMMIT:
+      if (g->cfg.dt_policy == 2) return grid_prime(g);
+      k_prime<<<1, 1, 0, g->st>>>(g->gd);
+      count_launch();
+      if (exa_status_t s = cuda_status(cudaGetLastError(), "k_prime")) return s;
+      g->primed = true;
+      return EXA_OK;
+    case EXA_PHASE_PREDICT: {
+      if (!g->primed) return set_error(EXA_EINVAL, "grid dt not primed");
+      if (g->profile) cudaEventRecord(g->ev[0], g->st);
+      exa_status_t s = grid_predict(g);
+      if (g->profile) cudaEventRecord(g->ev[1], g->st);
+      return s;
+    }
+    case EXA_PHASE_CORRECT:
+      if (!g->primed) return set_error(EXA_EINVAL, "grid dt not primed");
+      return grid_correct(g);
+    case EXA_PHASE_COMMIT: {
+      if (!g->primed) return set_error(EXA_EINVAL, "grid dt not primed");
+      if (exa_status_t s = grid_commit(g)) return s;
+      if (g->profile) {
+        // predictor, then everything after it (exchange wait, corrector, commit)
+        cudaEventRecord(g->ev[2], g->st);
+        cudaError_t e = cudaEventSynchronize(g->ev[2]);
+        if (e != cudaSuccess) return cuda_status(e, "profile sync");
+        float a1 = 0, a2 = 0;
+        cudaEventElapsedTime(&a1, g->ev[0], g->ev[1]);
+        cudaEventElapsedTime(&a2, g->ev[1], g->ev[2]);
+        g->ms_pred += a1;
+        g->ms_corr += a2;
+        g->prof_steps++;
+      }
+      return EXA_OK;
+    }
+  }
+  return set_error(EXA_EINVAL, "unknown phase");
 }
 
 }  // extern "C"

@@ -59,6 +59,13 @@ struct CorrArgs {
   unsigned long long* dt_next;  // atomic-min slot for the next dt (nullable)
   double dt_factor;             // CFL*PNPM[N] or CFL/(2N+1)
   int* nan_flag;
+  // Slab decomposition along the last dimension: when set, the neighbours
+  // across the lower / upper end of that dimension are not the periodic
+  // wrap-around cells but face data received from the adjacent slabs,
+  // [layer cell][Q | F][face nodes][var] (layer cell = index within the
+  // boundary layer).  NULL = periodic.
+  const double* halo_lo;
+  const double* halo_hi;
 };
 exa_status_t launch_corrector(int dim, int order, int pde, const CorrArgs& a, cudaStream_t st);
 
@@ -75,9 +82,12 @@ exa_status_t launch_solution_update(const exa_aderdg_desc_t& d, long ncells, dou
 exa_status_t launch_riemann_faces(const exa_aderdg_desc_t& d, long nfaces, const int* left,
                                   const int* right, const int* dir, const double* lQhbnd,
                                   double* lFhbnd, cudaStream_t st);
+// cell_offset / n_last_global place a slab of the last dimension inside a
+// larger domain (global cell index = local + cell_offset); 0 / n[dim-1] for
+// a whole domain.
 exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, double* luh,
                             int kind, double param, uint64_t seed, double noise,
-                            cudaStream_t st);
+                            cudaStream_t st, long cell_offset = 0, int n_last_global = 0);
 
 exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, double* luh, double* luh_new,
                                  unsigned long long* dt_slot, double* time, cudaStream_t st);

@@ -300,6 +300,48 @@ exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time,
                                     uint64_t* nonconverged, int* nan_flag);
 long exa_aderdg_grid_ncells(const exa_aderdg_grid* g);
 
+/* ---- Slab decomposition of one grid over several GPUs ----
+ * The reference distributes its spacetree over MPI ranks inside Peano: per
+ * remote face, ADERDGSolver::sendDataToNeighbour (exahype/solvers/
+ * ADERDGSolver.cpp:3379) sends that face's lQhbnd and lFhbnd, and the
+ * receiving rank's mergeWithNeighbourData (:3451) solves the Riemann problem
+ * with the received data (:3521, solveRiemannProblemAtInterface :3539), so
+ * both ranks solve every boundary face.  Here a periodic grid is
+ * cut into slabs along its last dimension (z in 3D, y in 2D), one slab per
+ * GPU; each slab is an exa_aderdg_grid of the slab's size with halos on.
+ * Per step the host (any transport: NCCL, a peer copy, a local copy)
+ *   1. exa_aderdg_grid_phase(PREDICT): predictor; the slab's boundary faces
+ *      are packed into send_lo (lower end) and send_hi (upper end);
+ *   2. moves send_hi of slab r into recv_lo of slab r+1 and send_lo of slab
+ *      r into recv_hi of slab r-1 (periodic in r);
+ *   3. exa_aderdg_grid_phase(CORRECT): Riemann / surface integral / update,
+ *      faces across the slab ends taken from recv_lo / recv_hi; the slab's
+ *      minimum next dt lands in the dt slot (uint64 bit pattern of a
+ *      positive double, so an unsigned or signed integer MIN reduction over
+ *      slabs gives the global minimum);
+ *   4. reduces the dt slot with MIN over slabs, then phase(COMMIT).
+ * Before the first step: phase(PRIME_LOCAL), MIN reduction of the slot,
+ * phase(PRIME_COMMIT).  All phases are stream-ordered on the grid's stream.
+ * The result equals the undivided periodic grid's bit for bit (both sides of
+ * a slab-boundary face solve the same Riemann problem from the same data). */
+enum {
+  EXA_PHASE_PREDICT = 0,
+  EXA_PHASE_CORRECT = 1,
+  EXA_PHASE_COMMIT = 2,
+  EXA_PHASE_PRIME_LOCAL = 3,
+  EXA_PHASE_PRIME_COMMIT = 4
+};
+exa_status_t exa_aderdg_grid_set_halo(exa_aderdg_grid* g, int enable);
+/* device buffers of `count` doubles each, [layer cell][Q | F][face node][var] */
+exa_status_t exa_aderdg_grid_halo_buffers(exa_aderdg_grid* g, double** send_lo, double** send_hi,
+                                          double** recv_lo, double** recv_hi, size_t* count);
+exa_status_t exa_aderdg_grid_dt_slot(exa_aderdg_grid* g, uint64_t** slot);
+exa_status_t exa_aderdg_grid_phase(exa_aderdg_grid* g, int phase);
+/* initial condition of slab `rank` of `nranks` (coordinates and noise of
+ * the whole domain; the grid's n and length are the slab's) */
+exa_status_t exa_aderdg_grid_init_slab(exa_aderdg_grid* g, int kind, double param, uint64_t seed,
+                                       double noise_amp, int rank, int nranks);
+
 /* ------------------------------------ ADER-DG: ensemble of 2D solves --
  * Many independent uniform periodic 2D grids (each its own order 2..5, size,
  * dt and step budget -- the per-solver state of ADERDGSolver.cpp:557-585)

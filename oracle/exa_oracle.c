@@ -629,6 +629,89 @@ double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
   return dt;
 }
 
+/* Slab decomposition (test oracle of the multi-GPU slab driver): the same
+ * per-cell and per-face calls as orc_aderdg_grid_step, with the faces across
+ * the ends of the last dimension solved against received face data. */
+void orc_aderdg_slab_predict(int dim, int order, int planar, const int* n,
+                             const double* dx, const double* luh, double dt,
+                             double* lduh, double* qb, double* fb,
+                             double* send_lo, double* send_hi) {
+  const int B = order + 1, V = 5;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const int nst = nn * B;
+  const int nfn = dim == 3 ? B * B : B;
+  const int fs = nfn * V;
+  const long nc = ncells_of(dim, n);
+  const long layer = nc / n[dim - 1];
+  double* lQi = (double*)malloc(sizeof(double) * nst * V);
+  double* lQo = (double*)malloc(sizeof(double) * nst * V);
+  double* rhs = (double*)malloc(sizeof(double) * nst * V);
+  double* lFi = (double*)malloc(sizeof(double) * nst * (dim + 1) * V);
+  double* lQhi = (double*)malloc(sizeof(double) * nn * V);
+  double* lFhi = (double*)malloc(sizeof(double) * nn * (dim + 1) * V);
+  for (long c = 0; c < nc; c++) {
+    orc_stp_nonlinear(dim, order, V, 0, planar, qb + c * 2 * dim * fs, fb + c * 2 * dim * fs,
+                      lQi, lQo, rhs, lFi, lQhi, lFhi, luh + c * nn * V, dx, dt);
+    orc_volume_integral(dim, order, V, 0, lduh + c * nn * V, lFhi, dx);
+  }
+  free(lQi); free(lQo); free(rhs); free(lFi); free(lQhi); free(lFhi);
+  const int d = dim - 1;
+  for (long lc = 0; lc < layer; lc++) {
+    const long lo = lc, hi = nc - layer + lc;
+    memcpy(send_lo + lc * 2 * fs, qb + (lo * 2 * dim + 2 * d) * fs, sizeof(double) * fs);
+    memcpy(send_lo + lc * 2 * fs + fs, fb + (lo * 2 * dim + 2 * d) * fs, sizeof(double) * fs);
+    memcpy(send_hi + lc * 2 * fs, qb + (hi * 2 * dim + 2 * d + 1) * fs, sizeof(double) * fs);
+    memcpy(send_hi + lc * 2 * fs + fs, fb + (hi * 2 * dim + 2 * d + 1) * fs, sizeof(double) * fs);
+  }
+}
+
+void orc_aderdg_slab_correct(int dim, int order, int planar, const int* n,
+                             const double* dx, double* luh, double* lduh,
+                             double* qb, double* fb, const double* recv_lo,
+                             const double* recv_hi, double dt) {
+  const int B = order + 1, V = 5;
+  const int nn = dim == 3 ? B * B * B : B * B;
+  const int nfn = dim == 3 ? B * B : B;
+  const int fs = nfn * V;
+  const long nc = ncells_of(dim, n);
+  const long layer = nc / n[dim - 1];
+  double* tmp = (double*)malloc(sizeof(double) * fs);
+  for (int d = 0; d < dim; d++) {
+    for (long c = 0; c < nc; c++) {
+      int r[3] = {(int)(c % n[0]), (int)((c / n[0]) % n[1]),
+                  dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0};
+      double* FLo = fb + (c * 2 * dim + 2 * d + 1) * fs;
+      const double* QLo = qb + (c * 2 * dim + 2 * d + 1) * fs;
+      if (d == dim - 1 && r[d] + 1 == n[d]) {
+        /* upper slab end: the slab above's lowest-layer face */
+        const double* h = recv_hi + (c - (nc - layer)) * 2 * fs;
+        memcpy(tmp, h + fs, sizeof(double) * fs);
+        orc_riemann(dim, order, V, 0, planar, FLo, tmp, QLo, h, d);
+      } else {
+        r[d] = (r[d] + 1) % n[d];
+        long cr = dim == 3 ? ((long)r[2] * n[1] + r[1]) * n[0] + r[0] : (long)r[1] * n[0] + r[0];
+        orc_riemann(dim, order, V, 0, planar, FLo, fb + (cr * 2 * dim + 2 * d) * fs, QLo,
+                    qb + (cr * 2 * dim + 2 * d) * fs, d);
+      }
+    }
+  }
+  /* lower slab end: the slab below's highest-layer face against our own */
+  {
+    const int d = dim - 1;
+    for (long lc = 0; lc < layer; lc++) {
+      const double* h = recv_lo + lc * 2 * fs;
+      memcpy(tmp, h + fs, sizeof(double) * fs);
+      orc_riemann(dim, order, V, 0, planar, tmp, fb + (lc * 2 * dim + 2 * d) * fs, h,
+                  qb + (lc * 2 * dim + 2 * d) * fs, d);
+    }
+  }
+  free(tmp);
+  for (long c = 0; c < nc; c++) {
+    orc_surface_integral(dim, order, V, lduh + c * nn * V, fb + c * 2 * dim * fs, dx);
+    orc_solution_update(dim, order, V, 0, luh + c * nn * V, lduh + c * nn * V, dt);
+  }
+}
+
 /* One step's per-cell work on `ncells` independent cells (CPU-baseline
  * sample): predictor + volume integral, one Riemann solve per direction
  * (the cell's +d face against its own -d face, i.e. a one-cell periodic

@@ -68,6 +68,23 @@ double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
                             const double* dx, double* luh, int dt_policy,
                             double cfl, double dt_fixed, int* iters,
                             int nthreads);
+/* Slab of a periodic grid cut along its last dimension (n = the slab's
+ * cells).  predict: predictor + volume integral of every cell into lduh,
+ * face data into qb/fb ([cell][2 dim][face nodes][var]), and the slab's
+ * boundary faces packed as [layer cell][Q | F][face nodes][var]: face
+ * 2(dim-1) of the lowest layer into send_lo, face 2(dim-1)+1 of the highest
+ * into send_hi.  correct: Riemann on every face (faces across the slab ends
+ * against recv_lo / recv_hi, the adjacent slabs' packed faces), surface
+ * integral and update of luh.  Same per-face arithmetic as
+ * orc_aderdg_grid_step, so slabs reproduce the undivided grid exactly. */
+void orc_aderdg_slab_predict(int dim, int order, int planar, const int* n,
+                             const double* dx, const double* luh, double dt,
+                             double* lduh, double* qb, double* fb,
+                             double* send_lo, double* send_hi);
+void orc_aderdg_slab_correct(int dim, int order, int planar, const int* n,
+                             const double* dx, double* luh, double* lduh,
+                             double* qb, double* fb, const double* recv_lo,
+                             const double* recv_hi, double dt);
 /* CPU-baseline sample: one step's per-cell work on ncells independent
  * cells (each its own periodic neighbour). */
 void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,
