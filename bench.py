@@ -269,9 +269,10 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
-    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving'],
+    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving', 'fv'],
                     help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
-                         'serving: Poisson stream of solve requests')
+                         'serving: Poisson stream of solve requests; fv: one periodic 2D FV patch')
+    ap.add_argument('--fv-patch', type=int, default=8192)
     ap.add_argument('--requests', type=int, default=400)
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--dg-fraction', type=float, default=0.25)
@@ -305,6 +306,9 @@ def main():
         return
     if args.workload == 'serving':
         run_serving(args, rank, world, dist)
+        return
+    if args.workload == 'fv':
+        run_fv(args, rank, world, dist)
         return
     if args.impl == 'reference':
         run_reference(args, rank, world)
@@ -615,6 +619,109 @@ def run_ensemble(args, rank, world, dist):
                                                 'cells': out['fp64']['cells']},
                 'fp64': out['fp64'], 'mixed': out['mixed'],
                 'mixed_speedup': out['mixed']['value'] / out['fp64']['value']}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- FV
+# Algorithmic FP64 work per FV cell-update (C_FLUX = 31 per flux vector,
+# C_EIG = 16 per max-eigenvalue, as for ADER-DG):
+#   Godunov: 2 Rusanov faces (2 eig + 2 flux + 20) + update (40) + next dt (2 eig + 4)
+#   MUSCL-Hancock: + minmod slopes / extrapolation (70) + half-step (4 flux + 60)
+
+def fv_flop_per_cell(scheme):
+    faces = 2 * (2 * 16 + 2 * 31 + 20)
+    base = faces + 40 + (2 * 16 + 4)
+    return base if scheme == 0 else base + 70 + 4 * 31 + 60
+
+
+def run_fv(args, rank, world, dist):
+    """One periodic 2D FV patch per GPU (replicas over GPUs), MUSCL-Hancock
+    (headline) and Godunov, fused device-resident steps."""
+    import exahype_b200 as E
+    from exahype_b200 import PinnedBuffer, Timer
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    E.lib().exa_set_device(local)
+    import ctypes as C
+    fp64_peak = C.c_double()
+    E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))
+    peaks, peak_src = measured_peaks()
+    P = args.fv_patch
+    out = {}
+    for scheme, name in ((1, 'musclhancock'), (0, 'godunov')):
+        g = E.FVGrid(scheme, P)
+        g.init(amp=0.2, seed=args.seed + rank, noise=1e-3)
+        q0 = g.get_state() if scheme == 1 else None
+        g.step(args.warmup)
+        stream = g.stream()
+        E.device.synchronize()
+        if dist:
+            dist.barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        t = Timer()
+        l0 = E.launch_count()
+        t.start(stream)
+        g.step(args.steps)
+        t.stop(stream)
+        ms = t.elapsed_ms()
+        launches = E.launch_count() - l0
+        clk = clocks.stop()
+        if dist:
+            import torch
+            x = torch.tensor([ms], dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            ms = float(x.item())
+        cells = P * P
+        ups = world * cells * args.steps / (ms * 1e-3)
+        per = ms / args.steps
+        bytes_alg = 80.0 * cells  # state read + write per cell-update
+        flop = fv_flop_per_cell(scheme) * cells
+        hbm = bytes_alg / (per * 1e-3) / 1e9
+        tf = flop / (per * 1e-3) / 1e12
+        r = {'value': ups, 'ms_per_step': per, 'gpu_launches': launches, 'clocks': clk,
+             'roofline': {'kernel': 'k_fv_muscl<fused>' if scheme else 'k_fv_godunov<fused>',
+                          'bound': 'hbm', 'achieved': hbm, 'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s',
+                          'frac': hbm / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None,
+                          'peak_source': peak_src, 'bytes_per_cell_update': 80,
+                          'fp64_achieved_tflops': tf, 'fp64_peak_tflops': fp64_peak.value,
+                          'fp64_frac': tf / fp64_peak.value, 'flop_per_cell_update': fv_flop_per_cell(scheme),
+                          'note': 'step time includes the one-thread commit launch'}}
+        if scheme == 1:
+            pin = PinnedBuffer(g.state_size)
+            pin.array[:] = q0
+            if dist:
+                dist.barrier()
+            t2 = Timer()
+            t2.start(stream)
+            E._lib.call('exa_fv_grid_set_state', g.h, pin.array.ctypes.data)
+            for _ in range(args.steps):
+                g.step(1)
+                g.status()
+            E._lib.call('exa_fv_grid_get_state', g.h, pin.array.ctypes.data)
+            t2.stop(stream)
+            ms2 = t2.elapsed_ms()
+            sb = g.state_size * 8
+            r['e2e'] = {'value': world * cells * args.steps / (ms2 * 1e-3), 'unit': 'cell-updates/s',
+                        'h2d_bytes_per_step': sb / args.steps, 'd2h_bytes_per_step': 16 + sb / args.steps,
+                        'note': 'state upload from pinned host memory, K steps each returning time and dt '
+                                'to the host, final state download'}
+            pin.free()
+        out[name] = r
+        g.destroy()
+    if rank == 0:
+        m = out['musclhancock']
+        line = {'metric': '2D Euler FV MUSCL-Hancock cell-updates/s', 'value': m['value'],
+                'unit': 'cell-updates/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+                'ms_per_step': m['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak',
+                'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': 'one periodic %d^2 FV patch per GPU, density sine + 1e-3 noise' % P,
+                           'l2_flush': 'inputs larger than L2 (%.1f GB per state copy)' % ((P + 4) ** 2 * 40 / 1e9),
+                           'parallelism': 'replicas%d' % world if world > 1 else 'single'},
+                'roofline': m['roofline'], 'e2e': m.get('e2e'), 'gpu_launches': m['gpu_launches'],
+                'clocks': m['clocks'], 'godunov': out['godunov']}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

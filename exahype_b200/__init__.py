@@ -9,8 +9,8 @@ from ._lib import (EXA_OK, PDE_EULER, PDE_EULER_PLANAR, PREC_FP64, PREC_MIXED, E
 from .aderdg import ADERDGGrid, ADERDGSolver, BatchedADERDG, make_desc
 from .device import DeviceBuffer, PinnedBuffer, Stream, Timer, device_count, launch_count
 from .ensemble import Ensemble, solve_config
-from .fv import FVPatches
+from .fv import FVGrid, FVPatches
 
 __all__ = ['ADERDGGrid', 'ADERDGSolver', 'BatchedADERDG', 'DeviceBuffer', 'PinnedBuffer', 'Stream',
-           'Timer', 'FVPatches', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
+           'Timer', 'FVPatches', 'FVGrid', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
            'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED']

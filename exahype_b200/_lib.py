@@ -123,6 +123,16 @@ SIGNATURES = {
     'exa_aderdg_grid_device_state': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(u64), C.POINTER(u64), C.POINTER(i32)]),
     'exa_aderdg_grid_ncells': (i64, [vp]),
+    'exa_fv_grid_create': (i32, [i32, i32, f64, i32, C.POINTER(vp)]),
+    'exa_fv_grid_destroy': (i32, [vp]),
+    'exa_fv_grid_state_size': (sz, [vp]),
+    'exa_fv_grid_init': (i32, [vp, f64, u64, f64]),
+    'exa_fv_grid_set_state': (i32, [vp, vp]),
+    'exa_fv_grid_get_state': (i32, [vp, vp]),
+    'exa_fv_grid_step': (i32, [vp, i32]),
+    'exa_fv_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(f64)]),
+    'exa_fv_grid_stream': (i32, [vp, C.POINTER(vp)]),
+    'exa_fv_grid_device_state': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                            C.POINTER(sz)]),

@@ -89,8 +89,12 @@ exa_status_t launch_grid_ic(int dim, int order, const int* n, const double* dx, 
                             int kind, double param, uint64_t seed, double noise,
                             cudaStream_t st, long cell_offset = 0, int n_last_global = 0);
 
-exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, double* luh, double* luh_new,
-                                 unsigned long long* dt_slot, double* time, cudaStream_t st);
+// Device-resident single periodic patch; slots = 3 x 64-bit scalars
+// ([0] dt, [1] time, [2] next dt), time must start at 0 (caller zeroes it).
+exa_status_t fv_patch_prime_async(const exa_fv_desc_t& d, const double* luh, unsigned long long* slots,
+                                  cudaStream_t st);
+exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const double* luh, double* luh_new,
+                                 unsigned long long* slots, cudaStream_t st);
 exa_status_t launch_fv_ic(const exa_fv_desc_t& d, double* luh, double amp, uint64_t seed, double noise,
                           cudaStream_t st);
 // arena of an ensemble, shared with the serving engine

@@ -16,6 +16,9 @@
 // is the state read + write (80 B), halo re-reads excepted.
 #include <float.h>
 
+#include <cstring>
+#include <new>
+#include <utility>
 #include <vector>
 
 #include "exa_device.cuh"
@@ -32,7 +35,20 @@ struct FVArgs {
   const double* luh;  // state the fluxes are computed from
   double* out;        // luh_new: updated in place (reference semantics)
   unsigned long long* max_dt;  // per patch, atomic-min bit patterns (nullable)
+  unsigned long long* next_dt;  // fused steps: CFL dt of the new state (atomic min)
 };
+
+// Periodic index of a cell coordinate of a single patch with ghost width g:
+// ghost coordinates map to the interior cell a ghost fill would copy.
+__device__ __forceinline__ int fv_wrap(int j, int g, int P) { return g + ((j - g) % P + P) % P; }
+
+// Fused steps (FUSED = true) of a single periodic patch: the tile is loaded
+// straight from the periodic interior (no ghost fill, no luh_new copy), the
+// new state is luh + face contributions written once, and the new state's
+// CFL dt (the commons::stableTimeStepSize rule that the next step starts
+// with) is reduced into next_dt.  Ghost layers of `out` are not written.
+// Per cell-update HBM traffic: one state read, one state write.
+
 
 // Rusanov flux of the face between qL and qR in direction d
 // (riemannsolvers/c/rusanov.cpph:24-83); returns s_max.
@@ -53,7 +69,7 @@ __device__ __forceinline__ double rusanov(const double* qL, const double* qR, in
 }
 
 // ------------------------------------------------------------- Godunov
-template <bool PLANAR>
+template <bool PLANAR, bool FUSED>
 __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
   constexpr int V = kV;
   constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
@@ -69,7 +85,11 @@ __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
   const int tid = threadIdx.x;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
-    const int j = j0 - 1 + r, k = k0 - 1 + c;
+    int j = j0 - 1 + r, k = k0 - 1 + c;
+    if (FUSED) {
+      j = fv_wrap(j, pb, a.P);
+      k = fv_wrap(k, pb, a.P);
+    }
     if (j >= 0 && j < S && k >= 0 && k < S)
 #pragma unroll
       for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
@@ -99,20 +119,33 @@ __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
   __syncthreads();
   const double dtv = a.dt_dev ? *a.dt_dev : a.dt;
   const double cx = dtv / a.hx, cy = dtv / a.hy;
+  double dtn = DBL_MAX;
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
     if (j < pe && k < pe) {
       double* o = out + ((long)j * S + k) * D;
+      const double* uc = &su[((r + 1) * LX + c + 1) * V];
+      double un[V];
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        double u = o[m];
+        double u = FUSED ? uc[m] : o[m];
         u += cx * sfx[(r * (FV_TX + 1) + c) * V + m];
         u -= cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
         u += cy * sfy[(r * FV_TX + c) * V + m];
         u -= cy * sfy[((r + 1) * FV_TX + c) * V + m];
         o[m] = u;
+        un[m] = u;
       }
+      if (FUSED) {
+        dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(un, 0));
+        dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(un, 1));
+      }
+    }
+    if (FUSED) {
+      for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
+      if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
+      return;
     }
     // first ghost layer, as the reference's face loops touch it
     if (j < pe && k0 == pb && c == 0) {
@@ -154,7 +187,7 @@ __device__ __forceinline__ double minmod(double a, double b) {
   return fabs(a) < fabs(b) ? a : b;
 }
 
-template <bool PLANAR>
+template <bool PLANAR, bool FUSED>
 __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
   constexpr int V = kV;
   // staged state: cells j0-2..j0+TY+1, k0-2..k0+TX+1
@@ -180,7 +213,11 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
   const double hx = a.hx, hy = a.hy, dt = a.dt_dev ? *a.dt_dev : a.dt;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
-    const int j = j0 - 2 + r, k = k0 - 2 + c;
+    int j = j0 - 2 + r, k = k0 - 2 + c;
+    if (FUSED) {
+      j = fv_wrap(j, pb, a.P);
+      k = fv_wrap(k, pb, a.P);
+    }
     if (j >= 0 && j < S && k >= 0 && k < S)
 #pragma unroll
       for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
@@ -272,20 +309,33 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
   }
   __syncthreads();
   const double cx = dt / hx, cy = dt / hy;
+  double dtn = DBL_MAX;
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
     if (j < pe && k < pe) {
       double* o = out + ((long)j * S + k) * D;
+      const double* uc = &su[((r + 2) * LX + c + 2) * V];
+      double un[V];
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        double u = o[m];
+        double u = FUSED ? uc[m] : o[m];
         u += cx * sfx[(r * (FV_TX + 1) + c) * V + m];
         u -= cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
         u += cy * sfy[(r * FV_TX + c) * V + m];
         u -= cy * sfy[((r + 1) * FV_TX + c) * V + m];
         o[m] = u;
+        un[m] = u;
       }
+      if (FUSED) {
+        dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(un, 0));
+        dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(un, 1));
+      }
+    }
+    if (FUSED) {
+      for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
+      if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
+      return;
     }
     if (j < pe && k0 == pb && c == 0) {
       double* o = out + ((long)j * S + (pb - 1)) * D;
@@ -387,29 +437,19 @@ static FVArgs fv_args(const exa_fv_desc_t* d) {
 
 exa_status_t upload_tables_fv() { return EXA_OK; }
 
-// ghost fill of one patch plus reset of its dt slot to +inf
-__global__ void k_fv_ghosts_reset(int P, int g, int D, double* luh, unsigned long long* dt_slot) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *dt_slot = 0x7FF0000000000000ULL;
-  const int S = P + 2 * g;
-  const long nghost = (long)S * S - (long)P * P;
-  const long r0 = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r0 >= nghost) return;
-  long r = r0;
-  int j, k;
-  const long top = (long)g * S;
-  if (r < top) { j = (int)(r / S); k = (int)(r % S); }
-  else if (r < 2 * top) { r -= top; j = g + P + (int)(r / S); k = (int)(r % S); }
-  else {
-    r -= 2 * top;
-    j = g + (int)(r / (2 * g));
-    const int c = (int)(r % (2 * g));
-    k = c < g ? c : P + c;
-  }
-  const int sj = g + ((j - g) % P + P) % P, sk = g + ((k - g) % P + P) % P;
-  for (int m = 0; m < D; m++) luh[((long)j * S + k) * D + m] = luh[((long)sj * S + sk) * D + m];
+// Scalars of a device-resident periodic patch (3 x 64 bit):
+// [0] dt of the current step, [1] simulated time, [2] next dt (atomic min).
+__global__ void k_fv_slots_init(unsigned long long* s) {
+  s[0] = 0x7FF0000000000000ULL;
+  s[2] = 0x7FF0000000000000ULL;
 }
 
-__global__ void k_fv_commit(const double* dt, double* time) { *time += *dt; }
+__global__ void k_fv_commit(unsigned long long* s) {
+  double* time = (double*)(s + 1);
+  *time += __longlong_as_double((long long)s[0]);
+  s[0] = s[2];
+  s[2] = 0x7FF0000000000000ULL;
+}
 
 __device__ __forceinline__ double fv_noise_u01(unsigned long long seed, unsigned long long idx) {
   unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (idx + 1ULL);
@@ -450,46 +490,51 @@ exa_status_t launch_fv_ic(const exa_fv_desc_t& d, double* luh, double amp, uint6
   return cuda_status(cudaGetLastError(), "k_fv_ic");
 }
 
-// One device-resident step of a single periodic patch: ghosts, CFL dt
-// (commons::stableTimeStepSize rule) into dt_slot, luh_new = luh, scheme
-// update reading dt from the slot, time += dt.  No host synchronisation.
-exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, double* luh, double* luh_new,
-                                 unsigned long long* dt_slot, double* time, cudaStream_t st) {
+// Device-resident stepping of a single periodic patch.  prime: the CFL dt
+// (commons::stableTimeStepSize rule) of the current state into slot [0].
+// step: one fused update (periodic tile loads, luh_new = luh + fluxes, next
+// dt of the new state into slot [2]), then commit (time += dt, dt <- next).
+// No host synchronisation; two launches per step.
+exa_status_t fv_patch_prime_async(const exa_fv_desc_t& d, const double* luh, unsigned long long* slots,
+                                  cudaStream_t st) {
   FVArgs a = fv_args(&d);
-  const int S = a.S;
-  const long nghost = (long)S * S - (long)d.patch * d.patch;
-  k_fv_ghosts_reset<<<(unsigned)((nghost + 255) / 256), 256, 0, st>>>(d.patch, d.ghost, d.nvar + d.npar, luh,
-                                                                   dt_slot);
   a.luh = luh;
+  k_fv_slots_init<<<1, 1, 0, st>>>(slots);
   const long cells = (long)d.patch * d.patch;
   unsigned bx = (unsigned)((cells + 255) / 256);
   if (bx > 1024) bx = 1024;
-  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
-  if (planar) k_fv_stable_dt<true><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)dt_slot);
-  else k_fv_stable_dt<false><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)dt_slot);
-  cudaError_t e = cudaMemcpyAsync(luh_new, luh, sizeof(double) * S * S * (d.nvar + d.npar),
-                                  cudaMemcpyDeviceToDevice, st);
-  if (e != cudaSuccess) return cuda_status(e, "fv copy");
+  if (d.pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots);
+  else k_fv_stable_dt<false><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots);
+  count_launch(2);
+  return cuda_status(cudaGetLastError(), "fv prime");
+}
+
+exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const double* luh, double* luh_new,
+                                 unsigned long long* slots, cudaStream_t st) {
+  FVArgs a = fv_args(&d);
+  a.luh = luh;
   a.out = luh_new;
-  a.dt_dev = (const double*)dt_slot;
+  a.dt_dev = (const double*)slots;
+  a.next_dt = slots + 2;
   a.max_dt = nullptr;
+  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
   dim3 grid((d.patch + FV_TX - 1) / FV_TX, (d.patch + FV_TY - 1) / FV_TY, 1);
   if (scheme == 0) {
-    if (planar) k_fv_godunov<true><<<grid, FV_NT, 0, st>>>(a);
-    else k_fv_godunov<false><<<grid, FV_NT, 0, st>>>(a);
+    if (planar) k_fv_godunov<true, true><<<grid, FV_NT, 0, st>>>(a);
+    else k_fv_godunov<false, true><<<grid, FV_NT, 0, st>>>(a);
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      e = planar ? cudaFuncSetAttribute(k_fv_muscl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
-                 : cudaFuncSetAttribute(k_fv_muscl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      cudaError_t e = planar ? cudaFuncSetAttribute(k_fv_muscl<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
+                             : cudaFuncSetAttribute(k_fv_muscl<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
-    if (planar) k_fv_muscl<true><<<grid, FV_NT, kMusclSmem, st>>>(a);
-    else k_fv_muscl<false><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    if (planar) k_fv_muscl<true, true><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    else k_fv_muscl<false, true><<<grid, FV_NT, kMusclSmem, st>>>(a);
   }
-  k_fv_commit<<<1, 1, 0, st>>>((const double*)dt_slot, time);
-  count_launch(5);
+  k_fv_commit<<<1, 1, 0, st>>>(slots);
+  count_launch(2);
   return cuda_status(cudaGetLastError(), "fv patch step");
 }
 
@@ -551,18 +596,18 @@ static exa_status_t fv_update(int scheme, const exa_fv_desc_t* desc, long npatch
   dim3 grid((desc->patch + FV_TX - 1) / FV_TX, (desc->patch + FV_TY - 1) / FV_TY, (unsigned)npatches);
   const bool planar = desc->pde == EXA_PDE_EULER_PLANAR;
   if (scheme == 0) {
-    if (planar) k_fv_godunov<true><<<grid, FV_NT, 0, st>>>(a);
-    else k_fv_godunov<false><<<grid, FV_NT, 0, st>>>(a);
+    if (planar) k_fv_godunov<true, false><<<grid, FV_NT, 0, st>>>(a);
+    else k_fv_godunov<false, false><<<grid, FV_NT, 0, st>>>(a);
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      cudaError_t e = planar ? cudaFuncSetAttribute(k_fv_muscl<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
-                             : cudaFuncSetAttribute(k_fv_muscl<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      cudaError_t e = planar ? cudaFuncSetAttribute(k_fv_muscl<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
+                             : cudaFuncSetAttribute(k_fv_muscl<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
-    if (planar) k_fv_muscl<true><<<grid, FV_NT, kMusclSmem, st>>>(a);
-    else k_fv_muscl<false><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    if (planar) k_fv_muscl<true, false><<<grid, FV_NT, kMusclSmem, st>>>(a);
+    else k_fv_muscl<false, false><<<grid, FV_NT, kMusclSmem, st>>>(a);
   }
   count_launch();
   return cuda_status(cudaGetLastError(), scheme == 0 ? "k_fv_godunov" : "k_fv_muscl");
@@ -610,6 +655,125 @@ exa_status_t exa_fv_periodic_ghosts(const exa_fv_desc_t* desc, long npatches, do
       desc->patch, desc->ghost, desc->nvar + desc->npar, npatches, luh);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_fv_ghosts");
+}
+
+// ------------------------------------------------ device-resident FV domain
+}  // extern "C"
+
+struct exa_fv_grid {
+  int scheme = 0;
+  exa_fv_desc_t desc{};
+  cudaStream_t st = nullptr;
+  double* luh = nullptr;
+  double* luh_new = nullptr;
+  unsigned long long* slots = nullptr;  // [0] dt, [1] time, [2] next dt, [3] steps
+  size_t count = 0;                     // doubles per state copy
+  bool primed = false;
+};
+
+extern "C" {
+
+exa_status_t exa_fv_grid_create(int scheme, int patch, double length, int pde, exa_fv_grid** out) {
+  if (!out) return set_error(EXA_EINVAL, "NULL argument");
+  if (scheme != 0 && scheme != 1) return set_error(EXA_EINVAL, "scheme must be 0 (Godunov) or 1 (MUSCL-Hancock)");
+  if (!(length > 0)) return set_error(EXA_EINVAL, "length must be > 0");
+  exa_fv_desc_t d{2, patch, scheme == 0 ? 1 : 2, kV, 0, pde, {length, length, 1.0}};
+  if (exa_status_t s = check_fv(&d, d.ghost)) return s;
+  exa_fv_grid* g = new (std::nothrow) exa_fv_grid;
+  if (!g) return set_error(EXA_ENOMEM, "host allocation");
+  g->scheme = scheme;
+  g->desc = d;
+  const size_t S = (size_t)patch + 2 * d.ghost;
+  g->count = S * S * kV;
+  cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&g->luh, g->count * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&g->luh_new, g->count * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&g->slots, 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->luh, 0, g->count * sizeof(double), g->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->luh_new, 0, g->count * sizeof(double), g->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->slots, 0, 4 * sizeof(unsigned long long), g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) {
+    exa_fv_grid_destroy(g);
+    return cuda_status(e, "fv grid allocation");
+  }
+  *out = g;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_grid_destroy(exa_fv_grid* g) {
+  if (!g) return EXA_OK;
+  if (g->st) cudaStreamSynchronize(g->st);
+  cudaFree(g->luh);
+  cudaFree(g->luh_new);
+  cudaFree(g->slots);
+  if (g->st) cudaStreamDestroy(g->st);
+  delete g;
+  return EXA_OK;
+}
+
+size_t exa_fv_grid_state_size(const exa_fv_grid* g) { return g ? g->count : 0; }
+
+exa_status_t exa_fv_grid_init(exa_fv_grid* g, double amp, uint64_t seed, double noise) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (exa_status_t s = launch_fv_ic(g->desc, g->luh, amp, seed, noise, g->st)) return s;
+  g->primed = false;
+  return cuda_status(cudaStreamSynchronize(g->st), "fv grid init");
+}
+
+exa_status_t exa_fv_grid_set_state(exa_fv_grid* g, const double* host) {
+  if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
+  cudaError_t e = cudaMemcpyAsync(g->luh, host, g->count * sizeof(double), cudaMemcpyHostToDevice, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  g->primed = false;
+  return cuda_status(e, "fv grid set_state");
+}
+
+exa_status_t exa_fv_grid_get_state(exa_fv_grid* g, double* host) {
+  if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
+  cudaError_t e = cudaMemcpyAsync(host, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "fv grid get_state");
+}
+
+exa_status_t exa_fv_grid_step(exa_fv_grid* g, int nsteps) {
+  if (!g || nsteps < 0) return set_error(EXA_EINVAL, "bad argument");
+  if (!g->primed) {
+    if (exa_status_t s = fv_patch_prime_async(g->desc, g->luh, g->slots, g->st)) return s;
+    g->primed = true;
+  }
+  for (int i = 0; i < nsteps; i++) {
+    if (exa_status_t s = fv_patch_step_async(g->scheme, g->desc, g->luh, g->luh_new, g->slots, g->st))
+      return s;
+    std::swap(g->luh, g->luh_new);
+  }
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_grid_status(exa_fv_grid* g, double* time, double* dt_next) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(h, g->slots, 16, cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) return cuda_status(e, "fv grid status");
+  double t, dt;
+  memcpy(&dt, &h[0], 8);
+  memcpy(&t, &h[1], 8);
+  if (time) *time = t;
+  if (dt_next) *dt_next = g->primed ? dt : 0.0;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_grid_stream(exa_fv_grid* g, void** stream) {
+  if (!g || !stream) return set_error(EXA_EINVAL, "NULL argument");
+  *stream = g->st;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev) {
+  if (!g || !luh_dev) return set_error(EXA_EINVAL, "NULL argument");
+  *luh_dev = g->luh;
+  return EXA_OK;
 }
 
 }  // extern "C"

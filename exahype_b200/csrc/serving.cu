@@ -33,7 +33,7 @@ struct Req {
   exa_fv_desc_t fv{};
   double* luh = nullptr;
   double* luh_new = nullptr;
-  unsigned long long* dt_slot = nullptr;  // scalars: [0] dt bits, [1] time
+  unsigned long long* dt_slot = nullptr;  // scalars: [0] dt bits, [1] time, [2] next dt bits
   size_t off = 0, bytes = 0;
   long long steps_left = 0;
   long long steps_done = 0;
@@ -135,9 +135,10 @@ exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* 
     q.luh = (double*)p;
     q.luh_new = (double*)(p + state);
     q.dt_slot = (unsigned long long*)(p + 2 * state);
-    cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 16, s->fv_st);
+    cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 24, s->fv_st);
     exa_status_t st = e == cudaSuccess ? launch_fv_ic(q.fv, q.luh, r->dg.ic_param, r->dg.seed, r->dg.noise, s->fv_st)
                                        : cuda_status(e, "fv scalars");
+    if (!st) st = fv_patch_prime_async(q.fv, q.luh, q.dt_slot, s->fv_st);
     if (st) {
       ens_arena_free(s->ens, q.off, q.bytes);
       return st;
@@ -162,8 +163,7 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
   for (auto& kv : s->live) {
     Req& q = kv.second;
     if (q.done || q.r.kind != EXA_REQ_FV) continue;
-    if (exa_status_t st = fv_patch_step_async(q.r.fv_scheme, q.fv, q.luh, q.luh_new, q.dt_slot,
-                                              (double*)(q.dt_slot + 1), s->fv_st))
+    if (exa_status_t st = fv_patch_step_async(q.r.fv_scheme, q.fv, q.luh, q.luh_new, q.dt_slot, s->fv_st))
       return st;
     std::swap(q.luh, q.luh_new);
     q.steps_done++;

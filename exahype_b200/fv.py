@@ -52,3 +52,64 @@ def rusanov(fL, fR, qL, qR, normalNonZero, dim=2, pde=_lib.PDE_EULER):
          np.ascontiguousarray(qL).ctypes.data_as(dp), np.ascontiguousarray(qR).ctypes.data_as(dp),
          int(normalNonZero), C.byref(s))
     return s.value
+
+
+class FVGrid:
+    """Device-resident periodic 2D FV domain (one patch, fused steps)."""
+
+    def __init__(self, scheme, patch, length=1.0, pde=_lib.PDE_EULER):
+        h = C.c_void_p()
+        call('exa_fv_grid_create', int(scheme), int(patch), float(length), int(pde), C.byref(h))
+        self.h = h
+        self.scheme, self.patch = scheme, patch
+        self.ghost = 1 if scheme == GODUNOV else 2
+        self.side = patch + 2 * self.ghost
+        self.state_size = int(_lib.lib().exa_fv_grid_state_size(h))
+        self.ncells = patch * patch
+
+    def init(self, amp=0.2, seed=1, noise=0.0):
+        call('exa_fv_grid_init', self.h, float(amp), int(seed), float(noise))
+
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.size == self.state_size
+        call('exa_fv_grid_set_state', self.h, q.ctypes.data)
+
+    def get_state(self):
+        out = np.empty(self.state_size)
+        call('exa_fv_grid_get_state', self.h, out.ctypes.data)
+        return out
+
+    def interior(self, q=None):
+        q = self.get_state() if q is None else q
+        g, P = self.ghost, self.patch
+        return q.reshape(self.side, self.side, 5)[g:g + P, g:g + P]
+
+    def step(self, nsteps=1):
+        call('exa_fv_grid_step', self.h, int(nsteps))
+
+    def status(self):
+        t, dt = C.c_double(), C.c_double()
+        call('exa_fv_grid_status', self.h, C.byref(t), C.byref(dt))
+        return dict(time=t.value, dt_next=dt.value)
+
+    def stream(self):
+        s = C.c_void_p()
+        call('exa_fv_grid_stream', self.h, C.byref(s))
+        return s
+
+    def device_state_ptr(self):
+        p = C.c_void_p()
+        call('exa_fv_grid_device_state', self.h, C.byref(p))
+        return p
+
+    def destroy(self):
+        if self.h:
+            call('exa_fv_grid_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -454,6 +454,31 @@ exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches,
 /* fills the ghost layers of every patch periodically from itself */
 exa_status_t exa_fv_periodic_ghosts(const exa_fv_desc_t* desc, long npatches,
                                     double* luh, void* stream);
+/* ---- Device-resident periodic FV domain ----
+ * One periodic 2D patch of patch x patch cells (plus the scheme's ghost
+ * width: 1 Godunov, 2 MUSCL-Hancock) over [0,length)^2, stepped on the
+ * device with the reference's per-step semantics: dt = the
+ * commons::stableTimeStepSize rule (commons.cpph:26-67) on the current
+ * state, then godunov/musclhancock::solutionUpdate (godunov.cpph:33-120,
+ * musclhancock.cpph:50-240) with periodic ghost values.  Two launches per
+ * step: a fused update that loads tiles straight from the periodic interior
+ * and also reduces the next dt, and a one-thread commit.  State layout
+ * [y][x][var] with ghosts; ghost cells of a stepped state are not
+ * meaningful.  Initial condition: rho = 1 + amp sin(2 pi (x+y)), u = v = 1,
+ * p = 1, with seeded relative density noise. */
+typedef struct exa_fv_grid exa_fv_grid;
+exa_status_t exa_fv_grid_create(int scheme, int patch, double length, int pde, exa_fv_grid** out);
+exa_status_t exa_fv_grid_destroy(exa_fv_grid* g);
+size_t exa_fv_grid_state_size(const exa_fv_grid* g);
+exa_status_t exa_fv_grid_init(exa_fv_grid* g, double amp, uint64_t seed, double noise);
+exa_status_t exa_fv_grid_set_state(exa_fv_grid* g, const double* host);
+exa_status_t exa_fv_grid_get_state(exa_fv_grid* g, double* host);
+exa_status_t exa_fv_grid_step(exa_fv_grid* g, int nsteps);
+/* simulated time and the dt the next step will take */
+exa_status_t exa_fv_grid_status(exa_fv_grid* g, double* time, double* dt_next);
+exa_status_t exa_fv_grid_stream(exa_fv_grid* g, void** stream);
+exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev);
+
 /* rusanov (riemannsolvers/c/rusanov.cpph:24-83), host drop-in, returns s_max */
 exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL,
                             double* fR, const double* qL, const double* qR,
