@@ -89,6 +89,7 @@ SIGNATURES = {
     'exa_tune_set': (i32, [i32, i32]),
     'exa_tune_get': (i32, [i32]),
     'exa_measure_fp64_peak': (i32, [C.POINTER(f64)]),
+    'exa_measure_fp64_tensor_peak': (i32, [C.POINTER(f64)]),
     'exa_measure_copy_bandwidth': (i32, [sz, C.POINTER(f64)]),
     'exa_diff_norms': (i32, [vp, vp, sz, C.POINTER(f64), vp]),
     'exa_aderdg_spaceTimePredictor': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dpp, dpp, dptr, dptr,

@@ -17,8 +17,10 @@ struct PredShape {
   static constexpr int NT = G * CPB;
   // shared memory per cell: two flux-slice buffers [2][DIM][NPC][V] (the
   // second doubles as the time-averaged state [NPC][D] after the loop)
-  static constexpr int SM_CELL = 2 * DIM * NPC * V > DIM * NPC * V + NPC * D
-                                     ? 2 * DIM * NPC * V : DIM * NPC * V + NPC * D;
+  // one flux slice, padded to keep 16-byte alignment of the second buffer
+  static constexpr int SLICE_D = (DIM * NPC * V + 1) & ~1;
+  static constexpr int SM_CELL = ((2 * SLICE_D > DIM * NPC * V + NPC * D ? 2 * SLICE_D
+                                                                         : DIM * NPC * V + NPC * D) + 1) & ~1;
   static constexpr int SM_DOUBLES = CPB * SM_CELL + NT / 32 + 1;
 };
 
@@ -92,7 +94,7 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
       // alternate the two slice buffers: a thread writing slice n+1 has
       // passed the barrier of slice n, which every thread reaches only after
       // it finished reading slice n-1 (the buffer being overwritten)
-      double* sFn = sF + ((iter * B + n) & 1) * (DIM * NPC * V);
+      double* sFn = sF + ((iter * B + n) & 1) * S::SLICE_D;
       double F[DIM][V];
       if (active) {
         double qq[5] = {q[n][0], q[n][1], q[n][2], q[n][3], q[n][4]};
@@ -111,9 +113,16 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
       }
       if (active) {
 #pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = F[d][m];
+        for (int d = 0; d < DIM; d++) {
+          // split slice layout: components (0,1) and (2,3) as 16-byte pairs,
+          // component 4 alone, each [DIM][NPC] (conflict-free 16-byte loads)
+          double2* p01 = reinterpret_cast<double2*>(sFn);
+          double2* p23 = p01 + DIM * NPC;
+          double* p4 = reinterpret_cast<double*>(p23 + DIM * NPC);
+          p01[d * NPC + s] = make_double2(F[d][0], F[d][1]);
+          p23[d * NPC + s] = make_double2(F[d][2], F[d][3]);
+          p4[d * NPC + s] = F[d][4];
+        }
         if (FULL && !conv) {
           double* lFi = a.lFi + cell * (long)NPC * B * (DIM + 1) * V;
 #pragma unroll
@@ -131,12 +140,20 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
         for (int m = 0; m < V; m++) Gm[m] = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          const double* line = sFn + (d * NPC + s - sd[d] * stride[d]) * V;
+          const int l0 = d * NPC + s - sd[d] * stride[d];
+          const double2* p01 = reinterpret_cast<const double2*>(sFn) + l0;
+          const double2* p23 = p01 + DIM * NPC;
+          const double* p4 = reinterpret_cast<const double*>(reinterpret_cast<const double2*>(sFn) + 2 * DIM * NPC) + l0;
 #pragma unroll
           for (int p = 0; p < B; p++) {
             const double c = dc[d][p];
-#pragma unroll
-            for (int m = 0; m < V; m++) Gm[m] += c * line[p * stride[d] * V + m];
+            const double2 v01 = p01[p * stride[d]];
+            const double2 v23 = p23[p * stride[d]];
+            Gm[0] += c * v01.x;
+            Gm[1] += c * v01.y;
+            Gm[2] += c * v23.x;
+            Gm[3] += c * v23.y;
+            Gm[4] += c * p4[p * stride[d]];
           }
         }
 #pragma unroll

@@ -1,0 +1,312 @@
+// Mixed-precision predictor, line-owner contraction (same operator and
+// arithmetic format as predictor_mixed_block: FP32 Picard deviations over
+// an FP64 base, difference-form FP32 flux deviations, FP64 outputs).
+//
+// What changes is who contracts what.  In predictor_mixed_block every node
+// thread gathers its 3 x B flux deviations along its three lines from
+// shared memory for every time slice, so each stored value is read B times
+// and the kernel is bound by shared-memory bandwidth.  Here each thread
+// also owns one (line, variable) task per direction: it reads the B values
+// of its line once per slice, applies the B x B derivative matrix (uniform
+// constants) and stores the B outputs into a per-iteration buffer that
+// holds every slice.  After the last slice each node thread sums its three
+// directions and applies the time matrix.  Shared-memory traffic per Picard iteration drops from
+// B^(d+1) * (d B V) loads to about 4 B^(d+1) V (flux store + line load +
+// output store + node load per direction).
+//
+// Tasks: per direction NPC/B lines x V variables; thread k < tasks holds
+// task k (line index fastest, so the lanes of a warp read distinct banks);
+// cells whose task count exceeds the thread count take two tasks per thread.
+#pragma once
+#include "exa_device.cuh"
+#include "aderdg_predictor_mixed_body.cuh"
+
+namespace exa {
+
+template <int DIM, int N>
+struct LineShape {
+  using M = MixShape<DIM, N>;
+  static constexpr int B = N + 1;
+  static constexpr int V = kV;
+  static constexpr int NPC = M::NPC;
+  static constexpr int G = M::G;
+  static constexpr int CPB = M::CPB;
+  static constexpr int NT = M::NT;
+  static constexpr int L = NPC / B;              // lines per direction
+  static constexpr int TPD = L * V;              // tasks per direction
+  static constexpr int TPT = (TPD + G - 1) / G;  // tasks per thread
+  // per cell, in floats: flux slices [2][DIM][NPC][V], line outputs
+  // [DIM][B (slice)][V][NPC], base deviations [B][V][NPC]
+  static constexpr int F_SLICE = DIM * NPC * V;
+  static constexpr int X_SIZE = DIM * B * V * NPC;
+  static constexpr int BASE_SIZE = B * V * NPC;
+  static constexpr int LOOP_F = 2 * F_SLICE + X_SIZE + BASE_SIZE;
+  static constexpr int STAGE_F = 2 * (DIM + 1) * NPC * V;  // FP64 staging, in floats
+  static constexpr int CELL_F = ((LOOP_F > STAGE_F ? LOOP_F : STAGE_F) + 1) & ~1;  // keep doubles aligned
+  static constexpr int SM_DOUBLES = CPB * CELL_F / 2 + NT / 32 + 1;
+};
+
+// node index of point p on line c of direction d
+template <int B, int D>
+__device__ __forceinline__ int line_node(int c, int p) {
+  constexpr int SD = D == 0 ? 1 : (D == 1 ? B : B * B);
+  return (c / SD) * SD * B + (c % SD) + p * SD;
+}
+
+template <int DIM, int N, bool PLANAR>
+__device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, long block, double* smem) {
+  using S = LineShape<DIM, N>;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, L = S::L, TPD = S::TPD, TPT = S::TPT;
+  constexpr int MAXIT = 2 * (N + 1);
+  const DGConst& T = c_dg[N];
+
+  const int lc = threadIdx.x / G;
+  const int s = threadIdx.x % G;
+  const long cell = block * S::CPB + lc;
+  const bool valid = cell < a.ncells;
+  const bool active = valid && s < NPC;
+  float* cf = reinterpret_cast<float*>(smem) + lc * S::CELL_F;
+  double* sD = reinterpret_cast<double*>(cf);  // FP64 staging (before / after the loop)
+  float* sF = cf;                              // [2][DIM][NPC][V]
+  float* sX = cf + 2 * S::F_SLICE;             // [DIM][B][V][NPC]
+  float* sB = sX + S::X_SIZE;                  // [B][V][NPC]
+  double* sred = smem + S::CPB * S::CELL_F / 2;
+
+  int sd[3];
+  sd[0] = s % B;
+  sd[1] = (s / B) % B;
+  sd[2] = DIM == 3 ? s / (B * B) : 0;
+  const int stride[3] = {1, B, B * B};
+
+  double lu[V];
+  {
+    const double* luh = a.luh + cell * (long)NPC * V;
+#pragma unroll
+    for (int m = 0; m < V; m++) lu[m] = active ? luh[s * V + m] : (m == 0 ? 1.0 : (m == 4 ? 2.5 : 0.0));
+  }
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+
+  // FP64 base flux and its derivative (once per cell)
+  {
+    double F0[DIM][V];
+    euler_flux<DIM, PLANAR>(lu, F0);
+    if (active)
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m];
+  }
+  __syncthreads();
+  double G0[V];
+#pragma unroll
+  for (int m = 0; m < V; m++) G0[m] = 0.0;
+  if (active) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
+#pragma unroll
+      for (int p = 0; p < B; p++) {
+        const double c = T.deriv[sd[d]][p] * a.idx[d];
+#pragma unroll
+        for (int m = 0; m < V; m++) G0[m] += c * line[p * stride[d] * V + m];
+      }
+    }
+  }
+  __syncthreads();  // the staging area becomes the loop buffers
+
+  // base deviations (c0[t] - 1) luh - dt (sum_n tA[t][n]) D.F0, FP32, in
+  // this node's slots of sB
+  if (active)
+#pragma unroll
+    for (int t = 0; t < B; t++) {
+      double tas = 0.0;
+#pragma unroll
+      for (int n = 0; n < B; n++) tas += T.tA[t][n];
+#pragma unroll
+      for (int m = 0; m < V; m++) sB[(t * V + m) * NPC + s] = (float)((T.c0[t] - 1.0) * lu[m] - dt * tas * G0[m]);
+    }
+  const float dtf = (float)dt;
+  float idxf[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) idxf[d] = (float)a.idx[d];
+
+  // FP32 base quantities of the difference-form flux (see
+  // predictor_mixed_block for the formulas)
+  float r0f, m0f[3], u0f[3], H0f, h0f;
+  {
+    const double irho = 1.0 / lu[0];
+    const double p0 = euler_pressure<PLANAR>(lu, irho);
+    r0f = (float)lu[0];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      m0f[k] = (float)lu[k + 1];
+      u0f[k] = (float)(lu[k + 1] * irho);
+    }
+    H0f = (float)(lu[4] + p0);
+    h0f = (float)((lu[4] + p0) * irho);
+  }
+
+  float dq[B][V];
+#pragma unroll
+  for (int t = 0; t < B; t++)
+#pragma unroll
+    for (int m = 0; m < V; m++) dq[t][m] = 0.f;
+
+  auto slice_flux = [&](int n, float (*dF)[V]) {
+    const float* dv = dq[n];
+    const float r1 = __frcp_rn(r0f + dv[0]);
+    float m1[3], w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      m1[k] = m0f[k] + dv[k + 1];
+      w[k] = fmaf(-u0f[k], dv[0], dv[k + 1]);
+    }
+    float k2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < (PLANAR ? 2 : 3); k++) k2 = fmaf(m0f[k], w[k], fmaf(dv[k + 1], m1[k], k2));
+    const float dp = (float)(kGamma - 1.0) * fmaf(-0.5f * k2, r1, dv[4]);
+    const float dH = dv[4] + dp;
+    const float H1 = H0f + dH;
+    const float e = fmaf(-h0f, dv[0], dH);
+#pragma unroll
+    for (int j = 0; j < DIM; j++) {
+      dF[j][0] = dv[j + 1];
+#pragma unroll
+      for (int k = 0; k < 3; k++) dF[j][k + 1] = fmaf(m0f[j], w[k], dv[j + 1] * m1[k]) * r1;
+      dF[j][j + 1] += dp;
+      dF[j][4] = fmaf(m0f[j], e, dv[j + 1] * H1) * r1;
+    }
+  };
+
+  // this thread's tasks: (line c, variable m) per direction
+  int tc[TPT], tm[TPT];
+  bool tv[TPT];
+#pragma unroll
+  for (int r = 0; r < TPT; r++) {
+    const int k = s + r * G;
+    tv[r] = valid && k < TPD;
+    tc[r] = tv[r] ? k % L : 0;
+    tm[r] = tv[r] ? k / L : 0;
+  }
+
+  // time-weighted flux deviations of the last iteration; with several cells
+  // per CTA a cell that converged keeps the sum of its last iteration while
+  // the others continue (its fluxes are then recomputed from the final
+  // iterate and must not replace it)
+  constexpr bool kShared = S::CPB > 1;
+  float fa[DIM][V];
+  float fkeep[kShared ? DIM : 1][V];
+  int it = 0;
+  bool conv = false;
+  int buf = 0;
+  for (int iter = 0; iter < MAXIT; iter++) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int m = 0; m < V; m++) fa[d][m] = 0.f;
+
+#pragma unroll
+    for (int n = 0; n < B; n++) {
+      // node threads: flux deviation of slice n into buffer buf (whose
+      // previous contents, slice n-2, every thread read before the last
+      // barrier)
+      {
+        float dF[DIM][V];
+        if (active) slice_flux(n, dF);
+        float* sFn = sF + buf * S::F_SLICE;
+        if (active)
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = dF[d][m];
+        if (active) {
+          const float wn = (float)T.w[n];
+#pragma unroll
+          for (int d = 0; d < DIM; d++)
+#pragma unroll
+            for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dF[d][m], fa[d][m]);
+        }
+      }
+      __syncthreads();
+      // line tasks: derivative along the line (uniform constant matrix);
+      // the B outputs go straight to sX [d][n][m][node] (a region disjoint
+      // from the flux buffers, read by the node threads after the last slice)
+      {
+        const float* sFn = sF + buf * S::F_SLICE;
+#pragma unroll
+        for (int r = 0; r < TPT; r++) {
+          if (!tv[r]) continue;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            float fl[B];
+#pragma unroll
+            for (int p = 0; p < B; p++) {
+              const int node = d == 0 ? line_node<B, 0>(tc[r], p)
+                                      : (d == 1 ? line_node<B, 1>(tc[r], p) : line_node<B, 2>(tc[r], p));
+              fl[p] = sFn[(d * NPC + node) * V + tm[r]];
+            }
+            float* xo = sX + ((d * B + n) * V + tm[r]) * NPC;
+#pragma unroll
+            for (int i = 0; i < B; i++) {
+              float g = 0.f;
+#pragma unroll
+              for (int p = 0; p < B; p++) g = fmaf((float)T.deriv[i][p], fl[p], g);
+              const int node = d == 0 ? line_node<B, 0>(tc[r], i)
+                                      : (d == 1 ? line_node<B, 1>(tc[r], i) : line_node<B, 2>(tc[r], i));
+              xo[node] = g;
+            }
+          }
+        }
+      }
+      buf ^= 1;
+    }
+
+    __syncthreads();
+
+    // node threads: sum of directions, time matrix, new deviation
+    float r2 = 0.f;
+    if (active && !conv) {
+      float acc[B][V];
+#pragma unroll
+      for (int t = 0; t < B; t++)
+#pragma unroll
+        for (int m = 0; m < V; m++) acc[t][m] = 0.f;
+#pragma unroll
+      for (int n = 0; n < B; n++)
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          float g = 0.f;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) g = fmaf(idxf[d], sX[((d * B + n) * V + m) * NPC + s], g);
+#pragma unroll
+          for (int t = 0; t < B; t++) acc[t][m] = fmaf((float)T.tA[t][n], g, acc[t][m]);
+        }
+#pragma unroll
+      for (int t = 0; t < B; t++)
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          const float dqn = fmaf(-dtf, acc[t][m], sB[(t * V + m) * NPC + s]);
+          const float diff = dqn - dq[t][m];
+          r2 = fmaf(diff, diff, r2);
+          dq[t][m] = dqn;
+        }
+      if (kShared)
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int m = 0; m < V; m++) fkeep[d][m] = fa[d][m];
+    }
+    const double res = group_sum<G>((double)r2, sred);
+    if (!conv) {
+      it = iter + 1;
+      if (res < 1e-7 * 1e-7) conv = true;
+    }
+    if (__syncthreads_and(conv || !valid)) break;
+  }
+
+  // fa holds the weighted flux-deviation sum of the last iteration (the
+  // reference averages the fluxes of the last iteration's input iterate)
+  mixed_outputs<DIM, N, PLANAR>(a, cell, s, valid, active, dq, kShared ? fkeep : fa, sD, it, conv);
+}
+
+}  // namespace exa

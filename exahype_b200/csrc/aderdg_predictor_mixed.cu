@@ -21,6 +21,7 @@
 //    computed between the same barriers as the FP32 derivative of slice n.
 #include "exa_device.cuh"
 #include "aderdg_predictor_mixed_body.cuh"
+#include "aderdg_predictor_lines_body.cuh"
 
 namespace exa {
 
@@ -50,15 +51,78 @@ static exa_status_t launch_mixed_t(const PredArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_predictor_mixed launch");
 }
 
+template <int DIM, int N, bool PLANAR, int MINB>
+__global__ void __launch_bounds__(LineShape<DIM, N>::NT, MINB) k_predictor_mixed_lines(PredArgs a) {
+  extern __shared__ double smem[];
+  predictor_mixed_lines_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
+}
+
+template <int DIM, int N, bool PLANAR, int MINB>
+static exa_status_t launch_lines_t(const PredArgs& a, cudaStream_t st) {
+  using S = LineShape<DIM, N>;
+  auto kern = k_predictor_mixed_lines<DIM, N, PLANAR, MINB>;
+  const size_t smem = sizeof(double) * S::SM_DOUBLES;
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "mixed predictor (lines) attribute");
+    attr_done[dev & 63] = true;
+  }
+  const long nblocks = (a.ncells + S::CPB - 1) / S::CPB;
+  if (nblocks <= 0) return EXA_OK;
+  kern<<<(unsigned)nblocks, S::NT, smem, st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_predictor_mixed_lines launch");
+}
+
+// line-owner variant (aderdg_predictor_lines_body.cuh)
+static exa_status_t launch_predictor_mixed_lines(const exa_aderdg_desc_t& d, const PredArgs& a,
+                                                 cudaStream_t st) {
+  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
+  if (d.dim == 3 && !planar) {
+    switch (d.order) {
+      case 2: return launch_lines_t<3, 2, false, 1>(a, st);
+      case 3: return launch_lines_t<3, 3, false, 1>(a, st);
+      case 4: {
+        const int occ = tune_get(kTuneMixedOccupancy, 0);
+        if (occ == 1) return launch_lines_t<3, 4, false, 1>(a, st);
+        if (occ >= 4) return launch_lines_t<3, 4, false, 4>(a, st);
+        return launch_lines_t<3, 4, false, 3>(a, st);
+      }
+      case 5: return launch_lines_t<3, 5, false, 1>(a, st);
+    }
+  } else if (d.dim == 2) {
+    switch (d.order) {
+      case 2: return planar ? launch_lines_t<2, 2, true, 1>(a, st) : launch_lines_t<2, 2, false, 1>(a, st);
+      case 3: return planar ? launch_lines_t<2, 3, true, 1>(a, st) : launch_lines_t<2, 3, false, 1>(a, st);
+      case 4: return planar ? launch_lines_t<2, 4, true, 1>(a, st) : launch_lines_t<2, 4, false, 1>(a, st);
+      case 5: return planar ? launch_lines_t<2, 5, true, 1>(a, st) : launch_lines_t<2, 5, false, 1>(a, st);
+    }
+  }
+  return set_error(EXA_EINVAL, "unsupported dim/order for the mixed predictor");
+}
+
 exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& a, cudaStream_t st) {
+  // knob 2: 1 = node-gather contraction, 2 = line-owner contraction,
+  // default: line-owner for 3D order 4, node-gather elsewhere
+  const int variant = tune_get(kTuneMixedVariant, 0);
+  if (d.npar == 0 && (variant == 2 || (variant == 0 && d.dim == 3 && d.order == 4)))
+    return launch_predictor_mixed_lines(d, a, st);
   if (d.npar != 0) return set_error(EXA_EINVAL, "mixed precision: npar must be 0");
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
-  const bool occ = tune_get(kTuneMixedOccupancy, 0) != 0;
+  // knob: minimum resident CTAs per SM for 3D N=4 (register cap 255 / 170 / 128)
+  const int occ = tune_get(kTuneMixedOccupancy, 0);
   if (d.dim == 3 && !planar) {
     switch (d.order) {
       case 2: return launch_mixed_t<3, 2, false, 1>(a, st);
       case 3: return launch_mixed_t<3, 3, false, 1>(a, st);
-      case 4: return occ ? launch_mixed_t<3, 4, false, 3>(a, st) : launch_mixed_t<3, 4, false, 1>(a, st);
+      case 4:
+        // default 3 CTAs/SM (168 registers, no spills): measured fastest
+        if (occ >= 4) return launch_mixed_t<3, 4, false, 4>(a, st);
+        if (occ == 1) return launch_mixed_t<3, 4, false, 1>(a, st);
+        return launch_mixed_t<3, 4, false, 3>(a, st);
       case 5: return launch_mixed_t<3, 5, false, 1>(a, st);
     }
   } else if (d.dim == 2) {

@@ -15,236 +15,99 @@ struct MixShape {
   static constexpr int CPB = DIM == 3 ? 1 : (128 / G > 0 ? 128 / G : 1);
   static constexpr int NT = G * CPB;
   // per cell, in doubles: max(two FP32 slice buffers, FP64 staging of the
-  // time-averaged flux [DIM][NPC][V] + state [NPC][V])
-  static constexpr int SLICE_F = DIM * NPC * V;  // floats per slice
+  // time-averaged flux [DIM][NPC][V] + state [NPC][V]).  A slice stores a
+  // node's 5 values in 6 floats so that (0,1) and (2,3) load as 8-byte pairs.
+  // A slice holds the flux deviations of every node and direction as
+  // components 0-3 ([DIM][NPC] float4, one 16-byte load per node) followed
+  // by component 4 ([DIM][NPC] float); both parts padded to 16 bytes.
+  static constexpr int S4 = DIM * NPC * 4;
+  static constexpr int S1 = (DIM * NPC + 3) & ~3;
+  static constexpr int SLICE_F = S4 + S1;  // floats per slice, a multiple of 4
+  // per-node FP32 base deviations [NPC][B][VP], live through the Picard loop
+  static constexpr int VP = 6;
+  static constexpr int BASE_D = NPC * B * VP / 2;
   static constexpr int STAGE_D = (DIM + 1) * NPC * V;
-  static constexpr int SM_CELL = SLICE_F > STAGE_D ? SLICE_F : STAGE_D;  // 2 float slices = SLICE_F doubles
+  static constexpr int LOOP_D = SLICE_F + BASE_D;  // 2 float slices = SLICE_F doubles
+  static constexpr int SM_CELL = ((LOOP_D > STAGE_D ? LOOP_D : STAGE_D) + 1) & ~1;  // 16-byte cells
   static constexpr int SM_DOUBLES = CPB * SM_CELL + NT / 32 + 1;
 };
 
-// MINB: minimum resident CTAs per SM requested from the register
-// allocator (1 = unconstrained; 3 trades a small spill for occupancy).
+// Five FP32 components as two packed pairs and a single: (0,1), (2,3), 4.
+// The pairs go through the sm_100 packed FP32 pipe (__ffma2_rn: two
+// round-to-nearest fmaf in one instruction, bitwise equal to two fmaf).
+struct F5 {
+  float2 a, b;
+  float c;
+};
+
+__device__ __forceinline__ F5 f5_zero() { return F5{make_float2(0.f, 0.f), make_float2(0.f, 0.f), 0.f}; }
+
+// acc += s * x
+__device__ __forceinline__ void f5_fma(float s, const F5& x, F5& acc) {
+  const float2 ss = make_float2(s, s);
+  acc.a = __ffma2_rn(ss, x.a, acc.a);
+  acc.b = __ffma2_rn(ss, x.b, acc.b);
+  acc.c = fmaf(s, x.c, acc.c);
+}
+
+// acc += s * (node values at p, 6-float stride, 8-byte aligned)
+__device__ __forceinline__ void f5_fma_smem(float s, const float* p, F5& acc) {
+  const float2 ss = make_float2(s, s);
+  acc.a = __ffma2_rn(ss, *reinterpret_cast<const float2*>(p), acc.a);
+  acc.b = __ffma2_rn(ss, *reinterpret_cast<const float2*>(p + 2), acc.b);
+  acc.c = fmaf(s, p[4], acc.c);
+}
+
+// acc += s * (components 0-3 at p4 (16-byte aligned), component 4 at p1)
+__device__ __forceinline__ void f5_fma_split(float s, const float* p4, const float* p1, F5& acc) {
+  const float2 ss = make_float2(s, s);
+  const float4 v = *reinterpret_cast<const float4*>(p4);
+  acc.a = __ffma2_rn(ss, make_float2(v.x, v.y), acc.a);
+  acc.b = __ffma2_rn(ss, make_float2(v.z, v.w), acc.b);
+  acc.c = fmaf(s, *p1, acc.c);
+}
+
+__device__ __forceinline__ void f5_store_split(float* p4, float* p1, const F5& x) {
+  *reinterpret_cast<float4*>(p4) = make_float4(x.a.x, x.a.y, x.b.x, x.b.y);
+  *p1 = x.c;
+}
+
+__device__ __forceinline__ void f5_store(float* p, const F5& x) {
+  *reinterpret_cast<float2*>(p) = x.a;
+  *reinterpret_cast<float2*>(p + 2) = x.b;
+  p[4] = x.c;
+}
+
+__device__ __forceinline__ float f5_get(const F5& x, int m) {
+  return m == 0 ? x.a.x : m == 1 ? x.a.y : m == 2 ? x.b.x : m == 3 ? x.b.y : x.c;
+}
+
+// FP64 outputs of a mixed-precision predictor cell (every thread of the CTA
+// calls it): time-averaged state and flux from luh, F(luh) and the FP32
+// deviations of the last Picard iterate (dqv: state per time node, fdv: the
+// weighted time sum of the flux deviations of the last iteration), then the
+// volume integral into lduh and the face extrapolations into lQhbnd/lFhbnd
+// (all FP64, the reference's formulas); sD is the cell's FP64 staging area
+// [DIM][NPC][V] flux + [NPC][V] state.
 template <int DIM, int N, bool PLANAR>
-__device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long block, double* smem) {
+__device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int s, bool valid, bool active,
+                                              const float (*dqv)[kV], const float (*fdv)[kV], double* sD,
+                                              int it, bool conv) {
   using S = MixShape<DIM, N>;
   constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G;
-  constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
-
-  const int lc = threadIdx.x / G;
-  const int s = threadIdx.x % G;
-  const long cell = block * S::CPB + lc;
-  const bool valid = cell < a.ncells;
-  const bool active = valid && s < NPC;
-  double* sD = smem + lc * S::SM_CELL;       // FP64 staging [DIM][NPC][V] + [NPC][V]
-  float* sFf = reinterpret_cast<float*>(sD);  // two FP32 slices [2][DIM][NPC][V]
   double* sQh = sD + DIM * NPC * V;
-  double* sred = smem + S::CPB * S::SM_CELL;
-
   int sd[3];
   sd[0] = s % B;
   sd[1] = (s / B) % B;
   sd[2] = DIM == 3 ? s / (B * B) : 0;
   const int stride[3] = {1, B, B * B};
-
-  double lu[V];
   const double* luh = a.luh + cell * (long)NPC * V;
+  double lu[V], F0[DIM][V];
+  __syncthreads();
 #pragma unroll
   for (int m = 0; m < V; m++) lu[m] = active ? luh[s * V + m] : (m == 0 ? 1.0 : (m == 4 ? 2.5 : 0.0));
-  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
-
-  // base flux F0 = F(luh) and its derivative G0 (FP64, once per cell)
-  double F0[DIM][V];
   euler_flux<DIM, PLANAR>(lu, F0);
-  if (active)
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m];
-  __syncthreads();
-  double G0[V];
-#pragma unroll
-  for (int m = 0; m < V; m++) G0[m] = 0.0;
-  if (active) {
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
-#pragma unroll
-      for (int p = 0; p < B; p++) {
-        const double c = T.deriv[sd[d]][p] * a.idx[d];
-#pragma unroll
-        for (int m = 0; m < V; m++) G0[m] += c * line[p * stride[d] * V + m];
-      }
-    }
-  }
-  __syncthreads();  // staging area is reused for the FP32 slices
-
-  float dcf[DIM][B];
-#pragma unroll
-  for (int d = 0; d < DIM; d++)
-#pragma unroll
-    for (int p = 0; p < B; p++) dcf[d][p] = active ? (float)(T.deriv[sd[d]][p] * a.idx[d]) : 0.f;
-
-  // First Picard deviation (all time nodes share luh, so F = F0 and the
-  // FP64 part of every iterate is the same):
-  //   base[t] = (c0[t] - 1) luh - dt (sum_n tA[t][n]) D.F0
-  // kept in FP32 (an O(dt) quantity); an iterate is dq = base - dt acc.
-  float base[B][V];
-#pragma unroll
-  for (int t = 0; t < B; t++) {
-    double tas = 0.0;
-#pragma unroll
-    for (int n = 0; n < B; n++) tas += T.tA[t][n];
-#pragma unroll
-    for (int m = 0; m < V; m++) base[t][m] = (float)((T.c0[t] - 1.0) * lu[m] - dt * tas * G0[m]);
-  }
-  const float dtf = (float)dt;
-
-  float dq[B][V];
-#pragma unroll
-  for (int t = 0; t < B; t++)
-#pragma unroll
-    for (int m = 0; m < V; m++) dq[t][m] = 0.f;
-
-  // FP64 flux of time slice n from luh + dq[n], returned as the FP32 deviation
-  auto slice_flux = [&](int n, float (*dF)[V]) {
-    double qq[V], F[DIM][V];
-#pragma unroll
-    for (int m = 0; m < V; m++) qq[m] = lu[m] + (double)dq[n][m];
-    euler_flux<DIM, PLANAR>(qq, F);
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int m = 0; m < V; m++) dF[d][m] = (float)(F[d][m] - F0[d][m]);
-  };
-
-  constexpr bool kShared = S::CPB > 1;
-  float fhd[DIM][V];
-  int it = 0;
-  bool conv = false;
-  int buf = 0;  // slice buffer parity, alternates every slice
-  for (int iter = 0; iter < MAXIT; iter++) {
-    float acc[B][V];
-#pragma unroll
-    for (int t = 0; t < B; t++)
-#pragma unroll
-      for (int m = 0; m < V; m++) acc[t][m] = 0.f;
-    float fhn[kShared ? DIM : 1][V];
-    float(*fa)[V] = kShared ? fhn : fhd;
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int m = 0; m < V; m++) fa[d][m] = 0.f;
-
-    // prologue: flux of slice 0
-    {
-      float dF[DIM][V];
-      if (active) slice_flux(0, dF);
-      else
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) dF[d][m] = 0.f;
-      float* sFn = sFf + buf * S::SLICE_F;
-      if (active)
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = dF[d][m];
-      if (!conv) {
-        const float wn = (float)T.w[0];
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dF[d][m], fa[d][m]);
-      }
-      __syncthreads();
-    }
-#pragma unroll
-    for (int n = 0; n < B; n++) {
-      // Software pipeline: the FP64 flux chain of slice n+1 and the shared-
-      // memory derivative of slice n sit between the same two barriers, so
-      // they overlap.  Slice n+1 goes to the other buffer, whose slice n-1
-      // every thread finished reading before the previous barrier.
-      float dFn[DIM][V];
-      if (n + 1 < B) {
-        if (active) slice_flux(n + 1, dFn);
-        else
-#pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int m = 0; m < V; m++) dFn[d][m] = 0.f;
-      }
-      if (active) {
-        const float* sFn = sFf + buf * S::SLICE_F;
-        float Gm[V];
-#pragma unroll
-        for (int m = 0; m < V; m++) Gm[m] = 0.f;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-          const float* line = sFn + (d * NPC + s - sd[d] * stride[d]) * V;
-#pragma unroll
-          for (int p = 0; p < B; p++) {
-            const float c = dcf[d][p];
-#pragma unroll
-            for (int m = 0; m < V; m++) Gm[m] = fmaf(c, line[p * stride[d] * V + m], Gm[m]);
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < B; t++) {
-          const float ta = (float)T.tA[t][n];
-#pragma unroll
-          for (int m = 0; m < V; m++) acc[t][m] = fmaf(ta, Gm[m], acc[t][m]);
-        }
-      }
-      if (n + 1 < B) {
-        buf ^= 1;
-        float* sFo = sFf + buf * S::SLICE_F;
-        if (active)
-#pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int m = 0; m < V; m++) sFo[(d * NPC + s) * V + m] = dFn[d][m];
-        if (!conv) {
-          const float wn = (float)T.w[n + 1];
-#pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dFn[d][m], fa[d][m]);
-        }
-        __syncthreads();
-      }
-    }
-    buf ^= 1;  // the next iteration's slice 0 goes to the other buffer
-
-    // new iterate dq = base - dt acc (FP32) and its squared increment
-    float r = 0.f;
-    if (active && !conv) {
-#pragma unroll
-      for (int t = 0; t < B; t++)
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          const float dqn = fmaf(-dtf, acc[t][m], base[t][m]);
-          const float diff = dqn - dq[t][m];
-          r = fmaf(diff, diff, r);
-          dq[t][m] = dqn;
-        }
-      if (kShared)
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) fhd[d][m] = fa[d][m];
-    }
-    const double res = group_sum<G>((double)r, sred);
-    if (!conv) {
-      it = iter + 1;
-      if (res < 1e-7 * 1e-7) conv = true;
-    }
-    if (__syncthreads_and(conv || !valid)) break;
-  }
-
-  // ---- FP64 outputs ------------------------------------------------------
-  __syncthreads();
   double wsum = 0.0;
 #pragma unroll
   for (int t = 0; t < B; t++) wsum += T.w[t];
@@ -253,13 +116,13 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
     for (int m = 0; m < V; m++) {
       double qh = lu[m] * wsum;
 #pragma unroll
-      for (int t = 0; t < B; t++) qh += (double)dq[t][m] * T.w[t];
+      for (int t = 0; t < B; t++) qh += (double)dqv[t][m] * T.w[t];
       sQh[s * V + m] = qh;
     }
 #pragma unroll
     for (int d = 0; d < DIM; d++)
 #pragma unroll
-      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m] * wsum + (double)fhd[d][m];
+      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m] * wsum + (double)fdv[d][m];
   }
   __syncthreads();
   if (!valid) return;
@@ -329,6 +192,262 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
       if (!conv) atomicAdd(&a.stats[1], 1ull);
     }
   }
+}
+
+
+template <int DIM, int N, bool PLANAR>
+__device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long block, double* smem) {
+  using S = MixShape<DIM, N>;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G;
+  constexpr int MAXIT = 2 * (N + 1);
+  const DGConst& T = c_dg[N];
+
+  const int lc = threadIdx.x / G;
+  const int s = threadIdx.x % G;
+  const long cell = block * S::CPB + lc;
+  const bool valid = cell < a.ncells;
+  const bool active = valid && s < NPC;
+  double* sD = smem + lc * S::SM_CELL;       // FP64 staging [DIM][NPC][V] + [NPC][V]
+  float* sFf = reinterpret_cast<float*>(sD);  // two FP32 slices (S4 + S1 floats each)
+  float* sBase = reinterpret_cast<float*>(sD + S::SLICE_F) + s * B * S::VP;  // this node's [B][VP]
+  double* sred = smem + S::CPB * S::SM_CELL;
+
+  int sd[3];
+  sd[0] = s % B;
+  sd[1] = (s / B) % B;
+  sd[2] = DIM == 3 ? s / (B * B) : 0;
+  const int stride[3] = {1, B, B * B};
+
+  double lu[V];
+  const double* luh = a.luh + cell * (long)NPC * V;
+#pragma unroll
+  for (int m = 0; m < V; m++) lu[m] = active ? luh[s * V + m] : (m == 0 ? 1.0 : (m == 4 ? 2.5 : 0.0));
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+
+  // base flux F0 = F(luh) and its derivative G0 (FP64, once per cell)
+  double F0[DIM][V];
+  euler_flux<DIM, PLANAR>(lu, F0);
+  if (active)
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m];
+  __syncthreads();
+  double G0[V];
+#pragma unroll
+  for (int m = 0; m < V; m++) G0[m] = 0.0;
+  if (active) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
+#pragma unroll
+      for (int p = 0; p < B; p++) {
+        const double c = T.deriv[sd[d]][p] * a.idx[d];
+#pragma unroll
+        for (int m = 0; m < V; m++) G0[m] += c * line[p * stride[d] * V + m];
+      }
+    }
+  }
+  __syncthreads();  // staging area is reused for the FP32 slices
+
+  float dcf[DIM][B];
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int p = 0; p < B; p++) dcf[d][p] = active ? (float)(T.deriv[sd[d]][p] * a.idx[d]) : 0.f;
+
+  // First Picard deviation (all time nodes share luh, so F = F0 and the
+  // FP64 part of every iterate is the same):
+  //   base[t] = (c0[t] - 1) luh - dt (sum_n tA[t][n]) D.F0
+  // kept in FP32 (an O(dt) quantity); an iterate is dq = base - dt acc.
+  // (in this thread's shared-memory slot: read once per iteration, it does
+  // not need registers across the loop)
+  if (active)
+#pragma unroll
+    for (int t = 0; t < B; t++) {
+      double tas = 0.0;
+#pragma unroll
+      for (int n = 0; n < B; n++) tas += T.tA[t][n];
+      float bv[V];
+#pragma unroll
+      for (int m = 0; m < V; m++) bv[m] = (float)((T.c0[t] - 1.0) * lu[m] - dt * tas * G0[m]);
+      f5_store(sBase + t * S::VP, F5{make_float2(bv[0], bv[1]), make_float2(bv[2], bv[3]), bv[4]});
+    }
+  const float dtf = (float)dt;
+
+  F5 dq[B];
+#pragma unroll
+  for (int t = 0; t < B; t++) dq[t] = f5_zero();
+
+  // Flux deviation dF = F(luh + dq[n]) - F(luh) of time slice n, computed
+  // directly in FP32 from algebraically exact difference formulas (no FP64
+  // flux, no conversions inside the Picard loop).  With q1 = q0 + d,
+  // rho1 = rho0 + d_rho, m1 = m0 + d_m, w = d_m - u0 d_rho, H = E + p,
+  // h0 = H0 / rho0:
+  //   d(m_j m_k / rho) = (m0_j w_k + d_mj m1_k) / rho1
+  //   d(|m|^2 / 2 rho) = sum_k (m0_k w_k + d_mk m1_k) / (2 rho1)
+  //   d(m_j H / rho)    = (m0_j (dH - h0 d_rho) + d_mj H1) / rho1
+  // Every term is a product of a base quantity (FP64 rounded once to FP32)
+  // and a deviation, so the FP32 rounding error is relative to dF, not to
+  // F: the same accuracy as evaluating F in FP64 and rounding F - F0.
+  float r0f, m0f[3], u0f[3], H0f, h0f;
+  {
+    const double irho = 1.0 / lu[0];
+    const double p0 = euler_pressure<PLANAR>(lu, irho);
+    r0f = (float)lu[0];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      m0f[k] = (float)lu[k + 1];
+      u0f[k] = (float)(lu[k + 1] * irho);
+    }
+    H0f = (float)(lu[4] + p0);
+    h0f = (float)((lu[4] + p0) * irho);
+  }
+  auto slice_flux = [&](int n, F5* dF) {
+    const float dv[V] = {dq[n].a.x, dq[n].a.y, dq[n].b.x, dq[n].b.y, dq[n].c};
+    const float r1 = __frcp_rn(r0f + dv[0]);
+    float m1[3], w[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      m1[k] = m0f[k] + dv[k + 1];
+      w[k] = fmaf(-u0f[k], dv[0], dv[k + 1]);
+    }
+    float k2 = 0.f;
+#pragma unroll
+    for (int k = 0; k < (PLANAR ? 2 : 3); k++) k2 = fmaf(m0f[k], w[k], fmaf(dv[k + 1], m1[k], k2));
+    const float dp = (float)(kGamma - 1.0) * fmaf(-0.5f * k2, r1, dv[4]);
+    const float dH = dv[4] + dp;
+    const float H1 = H0f + dH;
+    const float e = fmaf(-h0f, dv[0], dH);
+#pragma unroll
+    for (int j = 0; j < DIM; j++) {
+      float f[V];
+      f[0] = dv[j + 1];
+#pragma unroll
+      for (int k = 0; k < 3; k++) f[k + 1] = fmaf(m0f[j], w[k], dv[j + 1] * m1[k]) * r1;
+      f[j + 1] += dp;
+      f[4] = fmaf(m0f[j], e, dv[j + 1] * H1) * r1;
+      dF[j] = F5{make_float2(f[0], f[1]), make_float2(f[2], f[3]), f[4]};
+    }
+  };
+
+  constexpr bool kShared = S::CPB > 1;
+  constexpr int VP = S::VP;
+  F5 fhd[DIM];
+  int it = 0;
+  bool conv = false;
+  int buf = 0;  // slice buffer parity, alternates every slice
+  for (int iter = 0; iter < MAXIT; iter++) {
+    F5 acc[B];
+#pragma unroll
+    for (int t = 0; t < B; t++) acc[t] = f5_zero();
+    F5 fhn[kShared ? DIM : 1];
+    F5* fa = kShared ? fhn : fhd;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) fa[d] = f5_zero();
+
+    // prologue: flux of slice 0
+    {
+      F5 dF[DIM];
+      if (active) slice_flux(0, dF);
+      else
+#pragma unroll
+        for (int d = 0; d < DIM; d++) dF[d] = f5_zero();
+      float* sFn = sFf + buf * S::SLICE_F;
+      if (active)
+#pragma unroll
+        for (int d = 0; d < DIM; d++) f5_store_split(sFn + (d * NPC + s) * 4, sFn + S::S4 + d * NPC + s, dF[d]);
+      if (!conv) {
+        const float wn = (float)T.w[0];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) f5_fma(wn, dF[d], fa[d]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int n = 0; n < B; n++) {
+      // derivative of slice n (buffer buf), then the flux of slice n+1 into
+      // the other buffer, whose slice n-1 every thread finished reading
+      // before the previous barrier; one barrier per slice
+      if (active) {
+        const float* sFn = sFf + buf * S::SLICE_F;
+        F5 Gm = f5_zero();
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const int l0 = d * NPC + s - sd[d] * stride[d];
+          const float* line4 = sFn + l0 * 4;
+          const float* line1 = sFn + S::S4 + l0;
+#pragma unroll
+          for (int p = 0; p < B; p++) f5_fma_split(dcf[d][p], line4 + p * stride[d] * 4, line1 + p * stride[d], Gm);
+        }
+#pragma unroll
+        for (int t = 0; t < B; t++) f5_fma((float)T.tA[t][n], Gm, acc[t]);
+      }
+      if (n + 1 < B) {
+        F5 dFn[DIM];
+        if (active) slice_flux(n + 1, dFn);
+        else
+#pragma unroll
+          for (int d = 0; d < DIM; d++) dFn[d] = f5_zero();
+        buf ^= 1;
+        float* sFo = sFf + buf * S::SLICE_F;
+        if (active)
+#pragma unroll
+          for (int d = 0; d < DIM; d++) f5_store_split(sFo + (d * NPC + s) * 4, sFo + S::S4 + d * NPC + s, dFn[d]);
+        if (!conv) {
+          const float wn = (float)T.w[n + 1];
+#pragma unroll
+          for (int d = 0; d < DIM; d++) f5_fma(wn, dFn[d], fa[d]);
+        }
+        __syncthreads();
+      }
+    }
+    buf ^= 1;  // the next iteration's slice 0 goes to the other buffer
+
+    // new iterate dq = base - dt acc (FP32) and its squared increment
+    float r = 0.f;
+    if (active && !conv) {
+      float2 r2 = make_float2(0.f, 0.f);
+      const float2 mdt = make_float2(-dtf, -dtf);
+#pragma unroll
+      for (int t = 0; t < B; t++) {
+        const float* bt = sBase + t * VP;
+        F5 dqn;
+        dqn.a = __ffma2_rn(mdt, acc[t].a, *reinterpret_cast<const float2*>(bt));
+        dqn.b = __ffma2_rn(mdt, acc[t].b, *reinterpret_cast<const float2*>(bt + 2));
+        dqn.c = fmaf(-dtf, acc[t].c, bt[4]);
+        const float2 da = make_float2(dqn.a.x - dq[t].a.x, dqn.a.y - dq[t].a.y);
+        const float2 db = make_float2(dqn.b.x - dq[t].b.x, dqn.b.y - dq[t].b.y);
+        const float dc = dqn.c - dq[t].c;
+        r2 = __ffma2_rn(da, da, r2);
+        r2 = __ffma2_rn(db, db, r2);
+        r = fmaf(dc, dc, r);
+        dq[t] = dqn;
+      }
+      r += r2.x + r2.y;
+      if (kShared)
+#pragma unroll
+        for (int d = 0; d < DIM; d++) fhd[d] = fa[d];
+    }
+    const double res = group_sum<G>((double)r, sred);
+    if (!conv) {
+      it = iter + 1;
+      if (res < 1e-7 * 1e-7) conv = true;
+    }
+    if (__syncthreads_and(conv || !valid)) break;
+  }
+
+  // ---- FP64 outputs ------------------------------------------------------
+  float dqv[B][V], fdv[DIM][V];
+#pragma unroll
+  for (int t = 0; t < B; t++)
+#pragma unroll
+    for (int m = 0; m < V; m++) dqv[t][m] = f5_get(dq[t], m);
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+#pragma unroll
+    for (int m = 0; m < V; m++) fdv[d][m] = f5_get(fhd[d], m);
+  mixed_outputs<DIM, N, PLANAR>(a, cell, s, valid, active, dqv, fdv, sD, it, conv);
 }
 
 }  // namespace exa

@@ -20,6 +20,28 @@ __global__ void k_fp64_fma(double* out, int iters, double a, double b) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
 }
 
+// FP64 tensor-core (DMMA, mma.sync m8n8k4 f64) throughput: 4 independent
+// accumulator fragments per warp, operands held in registers.
+__global__ void k_dmma(double* out, int iters, double a0, double b0) {
+  double a = a0 + threadIdx.x * 1e-9, b = b0 - threadIdx.x * 1e-9;
+  double c[4][2];
+#pragma unroll
+  for (int k = 0; k < 4; k++) c[k][0] = c[k][1] = 0.0;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                     : "+d"(c[k][0]), "+d"(c[k][1])
+                     : "d"(a), "d"(b));
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) s += c[k][0] + c[k][1];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 __global__ void k_copy(const double4* __restrict__ in, double4* __restrict__ out, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = in[i];
@@ -82,6 +104,36 @@ exa_status_t exa_measure_fp64_peak(double* tflops) {
   cudaFree(out);
   if (e != cudaSuccess) return cuda_status(e, "probe fp64");
   const double flop = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  *tflops = flop / (ms * 1e-3) / 1e12;
+  return EXA_OK;
+}
+
+exa_status_t exa_measure_fp64_tensor_peak(double* tflops) {
+  if (!tflops) return set_error(EXA_EINVAL, "NULL tflops");
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int threads = 256, blocks = sms * 4, iters = 1024;
+  double* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(double) * blocks * threads);
+  if (e != cudaSuccess) return cuda_status(e, "probe alloc");
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_dmma<<<blocks, threads>>>(out, 16, 1e-3, 1e-3);  // warm-up
+  cudaEventRecord(a);
+  k_dmma<<<blocks, threads>>>(out, iters, 1e-3, 1e-3);
+  cudaEventRecord(b);
+  count_launch(2);
+  e = cudaEventSynchronize(b);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  if (e != cudaSuccess) return cuda_status(e, "probe dmma");
+  const double warps = (double)blocks * threads / 32;
+  const double flop = 2.0 * 8 * 8 * 4 * 8 * 4 * (double)iters * warps;
   *tflops = flop / (ms * 1e-3) / 1e12;
   return EXA_OK;
 }

@@ -102,14 +102,19 @@ exa_status_t exa_timer_elapsed_ms(void* timer, float* ms);
 uint64_t exa_launch_count(void);
 /* Tuning knobs chosen by the autotuner (exahype_b200/autotune.py) or the
  * user; process-wide.  Keys: 0 = register budget of the 3D order-4 mixed
- * predictor (1: cap for 3 CTAs/SM, 0: unconstrained, the default), 1 = the
- * same for the FP64 predictor.  exa_tune_get returns -1 for keys never set. */
+ * predictor as minimum resident CTAs per SM (1: unconstrained; 3: 168
+ * registers, the default; 4: 128 registers), 1 = the FP64 predictor's
+ * (0: unconstrained; non-zero: cap for 3 CTAs/SM), 2 = contraction of the
+ * mixed predictor (1: node-gather, 2: line-owner; 0: line-owner for 3D
+ * order 4, node-gather otherwise).  exa_tune_get returns -1 for keys never set. */
 exa_status_t exa_tune_set(int key, int value);
 int exa_tune_get(int key);
 /* FP64 FMA throughput of the current device in TFLOP/s, measured with a
  * dependent-chain DFMA kernel over all SMs (a roofline denominator; the
  * device's peak files carry no FP64 figure) */
 exa_status_t exa_measure_fp64_peak(double* tflops);
+/* FP64 tensor-core (mma.sync m8n8k4 f64) throughput of this GPU, TFLOP/s */
+exa_status_t exa_measure_fp64_tensor_peak(double* tflops);
 /* Error norms of device array a against reference b (n doubles): out[0]
  * relative L2 ||a-b||/||b||, out[1] relative Linf max|a-b|/max|b|,
  * out[2] ||a-b||, out[3] max|a-b|.  Synchronous on stream. */

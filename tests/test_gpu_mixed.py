@@ -20,7 +20,17 @@ pytestmark = pytest.mark.gpu
     (2, 5, (9, 9), 0, 20),
     (2, 2, (20, 20), 1, 30),
 ])
-def test_mixed_vs_fp64_per_step(dim, order, n, kind, steps):
+@pytest.mark.parametrize('variant', [1, 2])
+def test_mixed_vs_fp64_per_step(dim, order, n, kind, steps, variant):
+    # variant (tuning key 2): 1 = node-gather contraction, 2 = line-owner
+    E._lib.call('exa_tune_set', 2, variant)
+    try:
+        _mixed_vs_fp64(dim, order, n, kind, steps)
+    finally:
+        E._lib.call('exa_tune_set', 2, 0)
+
+
+def _mixed_vs_fp64(dim, order, n, kind, steps):
     a = E.ADERDGGrid(dim, order, n, precision=E.PREC_FP64)
     b = E.ADERDGGrid(dim, order, n, precision=E.PREC_MIXED)
     param = 5.0 if kind == 0 else 0.2
