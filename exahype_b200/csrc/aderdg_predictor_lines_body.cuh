@@ -35,10 +35,36 @@ struct LineShape {
   static constexpr int L = NPC / B;              // lines per direction
   static constexpr int TPD = L * V;              // tasks per direction
   static constexpr int TPT = (TPD + G - 1) / G;  // tasks per thread
-  // per cell, in floats: flux slices [2][DIM][NPC][V], line outputs
-  // [DIM][B (slice)][V][NPC], base deviations [B][V][NPC]
-  static constexpr int F_SLICE = DIM * NPC * V;
-  static constexpr int X_SIZE = DIM * B * V * NPC;
+  // Shared-memory layouts, per direction d (in floats):
+  //  * flux slice part of d: [NPC][V] (node-major) or [V][MS] (variable-
+  //    major, row stride MS >= NPC);
+  //  * line outputs of d: [B (slice)][V][XMS] (row stride XMS >= NPC);
+  //  * task numbering of d: 0 = line fastest, then variable; 1 = first line
+  //    coordinate, variable, second line coordinate; 2 = variable fastest.
+  // For 3D order 4 these were chosen by an exhaustive search of the bank
+  // mapping so that the node-lane stores/loads and the line-lane loads/
+  // stores of every direction are free of bank conflicts (one wavefront per
+  // warp access); other shapes use the plain layout.
+  static constexpr bool kTuned = DIM == 3 && N == 4;
+  __host__ __device__ static constexpr bool flux_vmajor(int d) { return kTuned && d < 2; }
+  __host__ __device__ static constexpr int flux_ms(int d) { return kTuned ? (d == 0 ? 125 : 133) : NPC; }
+  __host__ __device__ static constexpr int flux_size(int d) { return flux_vmajor(d) ? V * flux_ms(d) : NPC * V; }
+  __host__ __device__ static constexpr int flux_off(int d) {
+    return (d > 0 ? flux_size(0) : 0) + (d > 1 ? flux_size(1) : 0);
+  }
+  static constexpr int F_SLICE = (flux_off(DIM - 1) + flux_size(DIM - 1) + 3) & ~3;
+  __host__ __device__ static constexpr int x_ms(int d) { return kTuned ? (d == 0 ? 125 : (d == 1 ? 133 : 141)) : NPC; }
+  __host__ __device__ static constexpr int x_off(int d) {
+    return (d > 0 ? B * V * x_ms(0) : 0) + (d > 1 ? B * V * x_ms(1) : 0);
+  }
+  static constexpr int X_SIZE = x_off(DIM - 1) + B * V * x_ms(DIM - 1);
+  __host__ __device__ static constexpr int order(int d) { return kTuned ? d : 0; }
+  __device__ static __forceinline__ int flux_addr(int d, int node, int m) {
+    return flux_off(d) + (flux_vmajor(d) ? m * flux_ms(d) + node : node * V + m);
+  }
+  __device__ static __forceinline__ int x_addr(int d, int n, int m, int node) {
+    return x_off(d) + (n * V + m) * x_ms(d) + node;
+  }
   static constexpr int BASE_SIZE = B * V * NPC;
   static constexpr int LOOP_F = 2 * F_SLICE + X_SIZE + BASE_SIZE;
   static constexpr int STAGE_F = 2 * (DIM + 1) * NPC * V;  // FP64 staging, in floats
@@ -59,6 +85,7 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
   constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, L = S::L, TPD = S::TPD, TPT = S::TPT;
   constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
+  const DGConstF& TF = c_dgf[N];
 
   const int lc = threadIdx.x / G;
   const int s = threadIdx.x % G;
@@ -68,7 +95,7 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
   float* cf = reinterpret_cast<float*>(smem) + lc * S::CELL_F;
   double* sD = reinterpret_cast<double*>(cf);  // FP64 staging (before / after the loop)
   float* sF = cf;                              // [2][DIM][NPC][V]
-  float* sX = cf + 2 * S::F_SLICE;             // [DIM][B][V][NPC]
+  float* sX = cf + 2 * S::F_SLICE;             // line outputs (S::x_addr)
   float* sB = sX + S::X_SIZE;                  // [B][V][NPC]
   double* sred = smem + S::CPB * S::CELL_F / 2;
 
@@ -179,14 +206,28 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
   };
 
   // this thread's tasks: (line c, variable m) per direction
-  int tc[TPT], tm[TPT];
+  int tc[TPT][DIM], tm[TPT][DIM];
   bool tv[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
     const int k = s + r * G;
     tv[r] = valid && k < TPD;
-    tc[r] = tv[r] ? k % L : 0;
-    tm[r] = tv[r] ? k / L : 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      int c = 0, m = 0;
+      if (S::order(d) == 1) {  // first line coordinate, variable, second
+        c = (k % B) + B * (k / (B * V));
+        m = (k / B) % V;
+      } else if (S::order(d) == 2) {  // variable fastest
+        c = k / V;
+        m = k % V;
+      } else {
+        c = k % L;
+        m = k / L;
+      }
+      tc[r][d] = tv[r] ? c : 0;
+      tm[r][d] = tv[r] ? m : 0;
+    }
   }
 
   // time-weighted flux deviations of the last iteration; with several cells
@@ -218,9 +259,9 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
 #pragma unroll
           for (int d = 0; d < DIM; d++)
 #pragma unroll
-            for (int m = 0; m < V; m++) sFn[(d * NPC + s) * V + m] = dF[d][m];
+            for (int m = 0; m < V; m++) sFn[S::flux_addr(d, s, m)] = dF[d][m];
         if (active) {
-          const float wn = (float)T.w[n];
+          const float wn = TF.w[n];
 #pragma unroll
           for (int d = 0; d < DIM; d++)
 #pragma unroll
@@ -241,18 +282,31 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
             float fl[B];
 #pragma unroll
             for (int p = 0; p < B; p++) {
-              const int node = d == 0 ? line_node<B, 0>(tc[r], p)
-                                      : (d == 1 ? line_node<B, 1>(tc[r], p) : line_node<B, 2>(tc[r], p));
-              fl[p] = sFn[(d * NPC + node) * V + tm[r]];
+              const int node = d == 0 ? line_node<B, 0>(tc[r][d], p)
+                                      : (d == 1 ? line_node<B, 1>(tc[r][d], p) : line_node<B, 2>(tc[r][d], p));
+              fl[p] = sFn[S::flux_addr(d, node, tm[r][d])];
             }
-            float* xo = sX + ((d * B + n) * V + tm[r]) * NPC;
+            float* xo = sX + S::x_addr(d, n, tm[r][d], 0);
+            // outputs in pairs (i, i+1) on the packed FP32 pipe; each output
+            // is the same fma chain over p as a scalar loop
+            constexpr int NP = B / 2;
+            float2 gp[NP];
+            float gs = 0.f;
+#pragma unroll
+            for (int q = 0; q < NP; q++) gp[q] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int p = 0; p < B; p++) {
+              const float2 fp = make_float2(fl[p], fl[p]);
+#pragma unroll
+              for (int q = 0; q < NP; q++)
+                gp[q] = __ffma2_rn(*reinterpret_cast<const float2*>(&TF.derivT[p][2 * q]), fp, gp[q]);
+              if (B & 1) gs = fmaf(TF.derivT[p][B - 1], fl[p], gs);
+            }
 #pragma unroll
             for (int i = 0; i < B; i++) {
-              float g = 0.f;
-#pragma unroll
-              for (int p = 0; p < B; p++) g = fmaf((float)T.deriv[i][p], fl[p], g);
-              const int node = d == 0 ? line_node<B, 0>(tc[r], i)
-                                      : (d == 1 ? line_node<B, 1>(tc[r], i) : line_node<B, 2>(tc[r], i));
+              const float g = (B & 1) && i == B - 1 ? gs : ((i & 1) ? gp[i / 2].y : gp[i / 2].x);
+              const int node = d == 0 ? line_node<B, 0>(tc[r][d], i)
+                                      : (d == 1 ? line_node<B, 1>(tc[r][d], i) : line_node<B, 2>(tc[r][d], i));
               xo[node] = g;
             }
           }
@@ -266,26 +320,27 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
     // node threads: sum of directions, time matrix, new deviation
     float r2 = 0.f;
     if (active && !conv) {
-      float acc[B][V];
+      F5 acc[B];
 #pragma unroll
-      for (int t = 0; t < B; t++)
+      for (int t = 0; t < B; t++) acc[t] = f5_zero();
 #pragma unroll
-        for (int m = 0; m < V; m++) acc[t][m] = 0.f;
-#pragma unroll
-      for (int n = 0; n < B; n++)
+      for (int n = 0; n < B; n++) {
+        float g[V];
 #pragma unroll
         for (int m = 0; m < V; m++) {
-          float g = 0.f;
+          g[m] = 0.f;
 #pragma unroll
-          for (int d = 0; d < DIM; d++) g = fmaf(idxf[d], sX[((d * B + n) * V + m) * NPC + s], g);
-#pragma unroll
-          for (int t = 0; t < B; t++) acc[t][m] = fmaf((float)T.tA[t][n], g, acc[t][m]);
+          for (int d = 0; d < DIM; d++) g[m] = fmaf(idxf[d], sX[S::x_addr(d, n, m, s)], g[m]);
         }
+        const F5 gn{make_float2(g[0], g[1]), make_float2(g[2], g[3]), g[4]};
+#pragma unroll
+        for (int t = 0; t < B; t++) f5_fma(TF.tA[t][n], gn, acc[t]);
+      }
 #pragma unroll
       for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) {
-          const float dqn = fmaf(-dtf, acc[t][m], sB[(t * V + m) * NPC + s]);
+          const float dqn = fmaf(-dtf, f5_get(acc[t], m), sB[(t * V + m) * NPC + s]);
           const float diff = dqn - dq[t][m];
           r2 = fmaf(diff, diff, r2);
           dq[t][m] = dqn;

@@ -139,7 +139,12 @@ exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& 
 exa_status_t upload_tables_predictor_mixed() {
   size_t bytes = 0;
   const void* h = host_dg_tables(&bytes);
-  return cuda_status(cudaMemcpyToSymbol(c_dg, h, bytes), "upload tables (mixed predictor)");
+  cudaError_t e = cudaMemcpyToSymbol(c_dg, h, bytes);
+  if (e == cudaSuccess) {
+    const void* hf = host_dg_tables_f(&bytes);
+    e = cudaMemcpyToSymbol(c_dgf, hf, bytes);
+  }
+  return cuda_status(e, "upload tables (mixed predictor)");
 }
 
 }  // namespace exa

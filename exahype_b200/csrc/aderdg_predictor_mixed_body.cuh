@@ -201,6 +201,7 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
   constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G;
   constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
+  const DGConstF& TF = c_dgf[N];
 
   const int lc = threadIdx.x / G;
   const int s = threadIdx.x % G;
@@ -358,7 +359,7 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
 #pragma unroll
         for (int d = 0; d < DIM; d++) f5_store_split(sFn + (d * NPC + s) * 4, sFn + S::S4 + d * NPC + s, dF[d]);
       if (!conv) {
-        const float wn = (float)T.w[0];
+        const float wn = TF.w[0];
 #pragma unroll
         for (int d = 0; d < DIM; d++) f5_fma(wn, dF[d], fa[d]);
       }
@@ -381,7 +382,7 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
           for (int p = 0; p < B; p++) f5_fma_split(dcf[d][p], line4 + p * stride[d] * 4, line1 + p * stride[d], Gm);
         }
 #pragma unroll
-        for (int t = 0; t < B; t++) f5_fma((float)T.tA[t][n], Gm, acc[t]);
+        for (int t = 0; t < B; t++) f5_fma(TF.tA[t][n], Gm, acc[t]);
       }
       if (n + 1 < B) {
         F5 dFn[DIM];
@@ -395,7 +396,7 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
 #pragma unroll
           for (int d = 0; d < DIM; d++) f5_store_split(sFo + (d * NPC + s) * 4, sFo + S::S4 + d * NPC + s, dFn[d]);
         if (!conv) {
-          const float wn = (float)T.w[n + 1];
+          const float wn = TF.w[n + 1];
 #pragma unroll
           for (int d = 0; d < DIM; d++) f5_fma(wn, dFn[d], fa[d]);
         }

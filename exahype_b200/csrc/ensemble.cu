@@ -214,7 +214,12 @@ __global__ void k_solve_prime(SolveDev* sv) {
 exa_status_t upload_tables_ensemble() {
   size_t bytes = 0;
   const void* h = host_dg_tables(&bytes);
-  return cuda_status(cudaMemcpyToSymbol(c_dg, h, bytes), "upload tables (ensemble)");
+  cudaError_t e = cudaMemcpyToSymbol(c_dg, h, bytes);
+  if (e == cudaSuccess) {
+    const void* hf = host_dg_tables_f(&bytes);
+    e = cudaMemcpyToSymbol(c_dgf, hf, bytes);
+  }
+  return cuda_status(e, "upload tables (ensemble)");
 }
 
 }  // namespace exa

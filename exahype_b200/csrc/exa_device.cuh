@@ -31,6 +31,16 @@ struct DGConst {
 // uploads the same bytes into each (exa::upload_tables_*).
 static __constant__ DGConst c_dg[kMaxOrder + 1];
 
+// FP32 copies (rounded from the FP64 tables) for the mixed-precision Picard
+// loop, so its FMAs take constant-bank operands without conversions.
+struct DGConstF {
+  float w[10];
+  float deriv[10][10];
+  float derivT[10][10];  // derivT[p][l] = deriv[l][p] (pairs of outputs adjacent)
+  float tA[10][10];
+};
+static __constant__ DGConstF c_dgf[kMaxOrder + 1];
+
 // ------------------------------------------------------------------ PDE
 // Compressible Euler, gamma = 1.4.  PLANAR selects the "2.5D" pressure
 // p = (g-1)(E - (j_x^2+j_y^2)/(2 rho)) of the reference's 2D kernel tests

@@ -112,6 +112,7 @@ exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 // host copy of the derived tables (same bytes as the device constants)
 const void* host_dg_tables(size_t* bytes);
+const void* host_dg_tables_f(size_t* bytes);  // FP32 copies (DGConstF)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 

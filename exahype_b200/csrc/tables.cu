@@ -11,6 +11,7 @@
 namespace exa {
 
 static DGConst g_tables[kMaxOrder + 1];
+static DGConstF g_tables_f[kMaxOrder + 1];
 static std::once_flag g_once;
 
 static void build() {
@@ -40,6 +41,15 @@ static void build() {
       T.c0[t] = c;
     }
     T.pnpm = exa_pnpm[N];
+    DGConstF& F = g_tables_f[N];
+    for (int i = 0; i < 10; i++) {
+      F.w[i] = (float)T.w[i];
+      for (int j = 0; j < 10; j++) {
+        F.deriv[i][j] = (float)T.deriv[i][j];
+        F.derivT[j][i] = (float)T.deriv[i][j];
+        F.tA[i][j] = (float)T.tA[i][j];
+      }
+    }
   }
 }
 
@@ -47,6 +57,12 @@ const void* host_dg_tables(size_t* bytes) {
   std::call_once(g_once, build);
   if (bytes) *bytes = sizeof(g_tables);
   return g_tables;
+}
+
+const void* host_dg_tables_f(size_t* bytes) {
+  std::call_once(g_once, build);
+  if (bytes) *bytes = sizeof(g_tables_f);
+  return g_tables_f;
 }
 
 double host_pnpm(int order) { return exa_pnpm[order]; }
