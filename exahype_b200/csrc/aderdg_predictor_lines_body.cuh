@@ -67,17 +67,10 @@ struct LineShape {
   }
   static constexpr int BASE_SIZE = B * V * NPC;
   static constexpr int LOOP_F = 2 * F_SLICE + X_SIZE + BASE_SIZE;
-  static constexpr int STAGE_F = 2 * (DIM + 1) * NPC * V;  // FP64 staging, in floats
+  static constexpr int STAGE_F = 2 * M::STAGE_D;  // FP64 staging (mixed_outputs), in floats
   static constexpr int CELL_F = ((LOOP_F > STAGE_F ? LOOP_F : STAGE_F) + 1) & ~1;  // keep doubles aligned
   static constexpr int SM_DOUBLES = CPB * CELL_F / 2 + NT / 32 + 1;
 };
-
-// node index of point p on line c of direction d
-template <int B, int D>
-__device__ __forceinline__ int line_node(int c, int p) {
-  constexpr int SD = D == 0 ? 1 : (D == 1 ? B : B * B);
-  return (c / SD) * SD * B + (c % SD) + p * SD;
-}
 
 template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, long block, double* smem) {
@@ -205,8 +198,11 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
     }
   };
 
-  // this thread's tasks: (line c, variable m) per direction
-  int tc[TPT][DIM], tm[TPT][DIM];
+  // this thread's tasks: (line c, variable m) per direction, kept as the
+  // shared-memory offsets of the line's first point in the flux slice
+  // (fbase) and in the line-output buffer (xbase); the other points follow
+  // at compile-time strides
+  int fbase[TPT][DIM], xbase[TPT][DIM];
   bool tv[TPT];
 #pragma unroll
   for (int r = 0; r < TPT; r++) {
@@ -225,8 +221,10 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
         c = k % L;
         m = k / L;
       }
-      tc[r][d] = tv[r] ? c : 0;
-      tm[r][d] = tv[r] ? m : 0;
+      if (!tv[r]) c = m = 0;
+      const int n0 = d == 0 ? line_node<B, 0>(c, 0) : (d == 1 ? line_node<B, 1>(c, 0) : line_node<B, 2>(c, 0));
+      fbase[r][d] = S::flux_addr(d, n0, m);
+      xbase[r][d] = S::x_addr(d, 0, m, n0);
     }
   }
 
@@ -279,14 +277,12 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
           if (!tv[r]) continue;
 #pragma unroll
           for (int d = 0; d < DIM; d++) {
+            const int SD = d == 0 ? 1 : (d == 1 ? B : B * B);  // node stride along the line
+            const int FSTEP = S::flux_vmajor(d) ? SD : SD * V;
             float fl[B];
 #pragma unroll
-            for (int p = 0; p < B; p++) {
-              const int node = d == 0 ? line_node<B, 0>(tc[r][d], p)
-                                      : (d == 1 ? line_node<B, 1>(tc[r][d], p) : line_node<B, 2>(tc[r][d], p));
-              fl[p] = sFn[S::flux_addr(d, node, tm[r][d])];
-            }
-            float* xo = sX + S::x_addr(d, n, tm[r][d], 0);
+            for (int p = 0; p < B; p++) fl[p] = sFn[fbase[r][d] + p * FSTEP];
+            float* xo = sX + xbase[r][d] + n * V * S::x_ms(d);
             // outputs in pairs (i, i+1) on the packed FP32 pipe; each output
             // is the same fma chain over p as a scalar loop
             constexpr int NP = B / 2;
@@ -305,9 +301,7 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
 #pragma unroll
             for (int i = 0; i < B; i++) {
               const float g = (B & 1) && i == B - 1 ? gs : ((i & 1) ? gp[i / 2].y : gp[i / 2].x);
-              const int node = d == 0 ? line_node<B, 0>(tc[r][d], i)
-                                      : (d == 1 ? line_node<B, 1>(tc[r][d], i) : line_node<B, 2>(tc[r][d], i));
-              xo[node] = g;
+              xo[i * SD] = g;
             }
           }
         }

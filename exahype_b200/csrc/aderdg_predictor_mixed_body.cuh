@@ -26,7 +26,7 @@ struct MixShape {
   // per-node FP32 base deviations [NPC][B][VP], live through the Picard loop
   static constexpr int VP = 6;
   static constexpr int BASE_D = NPC * B * VP / 2;
-  static constexpr int STAGE_D = (DIM + 1) * NPC * V;
+  static constexpr int STAGE_D = (2 * DIM + 1) * NPC * V;  // output staging (mixed_outputs)
   static constexpr int LOOP_D = SLICE_F + BASE_D;  // 2 float slices = SLICE_F doubles
   static constexpr int SM_CELL = ((LOOP_D > STAGE_D ? LOOP_D : STAGE_D) + 1) & ~1;  // 16-byte cells
   static constexpr int SM_DOUBLES = CPB * SM_CELL + NT / 32 + 1;
@@ -82,36 +82,50 @@ __device__ __forceinline__ float f5_get(const F5& x, int m) {
   return m == 0 ? x.a.x : m == 1 ? x.a.y : m == 2 ? x.b.x : m == 3 ? x.b.y : x.c;
 }
 
+// node index of point p on line c of direction d (line c: the other
+// coordinates a + B b, in x, y, z order without d)
+template <int B, int D>
+__device__ __forceinline__ int line_node(int c, int p) {
+  constexpr int SD = D == 0 ? 1 : (D == 1 ? B : B * B);
+  return (c / SD) * SD * B + (c % SD) + p * SD;
+}
+
 // FP64 outputs of a mixed-precision predictor cell (every thread of the CTA
-// calls it): time-averaged state and flux from luh, F(luh) and the FP32
+// calls it): time-averaged state Qh and flux Fh from luh, F(luh) and the FP32
 // deviations of the last Picard iterate (dqv: state per time node, fdv: the
 // weighted time sum of the flux deviations of the last iteration), then the
-// volume integral into lduh and the face extrapolations into lQhbnd/lFhbnd
-// (all FP64, the reference's formulas); sD is the cell's FP64 staging area
-// [DIM][NPC][V] flux + [NPC][V] state.
+// face extrapolations into lQhbnd/lFhbnd and the volume integral into lduh
+// (the reference's formulas, FP64).
+//
+// Both are contractions along lines, so they run as line tasks (direction
+// d, line c, variable m; the same numbering as the line-owner predictor):
+// a task reads the B values of Qh and Fh_d on its line once and produces
+// the two face values of that line (the face node of line c is c) and the
+// B line sums  sum_p Kxi[i][p] Fh_d[p]  of the volume integral, which the
+// node threads weight and sum over directions.  sD: the cell's FP64 staging
+// area, MixShape::STAGE_D doubles: Qh [NPC][V], Fh [DIM][NPC][V],
+// volume-integral line sums [DIM][NPC][V].
 template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int s, bool valid, bool active,
                                               const float (*dqv)[kV], const float (*fdv)[kV], double* sD,
                                               int it, bool conv) {
   using S = MixShape<DIM, N>;
-  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, NF = S::NF;
+  constexpr int L = NPC / B, TPD = L * V, TPT = (TPD + G - 1) / G;
   const DGConst& T = c_dg[N];
-  double* sQh = sD + DIM * NPC * V;
-  int sd[3];
-  sd[0] = s % B;
-  sd[1] = (s / B) % B;
-  sd[2] = DIM == 3 ? s / (B * B) : 0;
-  const int stride[3] = {1, B, B * B};
+  double* sQh = sD;                     // [NPC][V]
+  double* sFh = sD + NPC * V;           // [DIM][NPC][V]
+  double* sVI = sFh + DIM * NPC * V;    // [DIM][NPC][V]
   const double* luh = a.luh + cell * (long)NPC * V;
-  double lu[V], F0[DIM][V];
-  __syncthreads();
-#pragma unroll
-  for (int m = 0; m < V; m++) lu[m] = active ? luh[s * V + m] : (m == 0 ? 1.0 : (m == 4 ? 2.5 : 0.0));
-  euler_flux<DIM, PLANAR>(lu, F0);
-  double wsum = 0.0;
-#pragma unroll
-  for (int t = 0; t < B; t++) wsum += T.w[t];
+  __syncthreads();  // the caller's loop buffers overlap the staging area
   if (active) {
+    double lu[V], F0[DIM][V];
+#pragma unroll
+    for (int m = 0; m < V; m++) lu[m] = luh[s * V + m];
+    euler_flux<DIM, PLANAR>(lu, F0);
+    double wsum = 0.0;
+#pragma unroll
+    for (int t = 0; t < B; t++) wsum += T.w[t];
 #pragma unroll
     for (int m = 0; m < V; m++) {
       double qh = lu[m] * wsum;
@@ -122,12 +136,59 @@ __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int 
 #pragma unroll
     for (int d = 0; d < DIM; d++)
 #pragma unroll
-      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m] * wsum + (double)fdv[d][m];
+      for (int m = 0; m < V; m++) sFh[(d * NPC + s) * V + m] = F0[d][m] * wsum + (double)fdv[d][m];
+  }
+  __syncthreads();
+  if (valid) {
+    double* qb = a.lQhbnd + cell * (long)2 * DIM * NF * V;
+    double* fb = a.lFhbnd + cell * (long)2 * DIM * NF * V;
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      const int k = s + r * G;
+      if (k >= TPD) continue;
+      const int c = k % L, m = k / L;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        double q[B], f[B];
+#pragma unroll
+        for (int p = 0; p < B; p++) {
+          const int node = d == 0 ? line_node<B, 0>(c, p) : (d == 1 ? line_node<B, 1>(c, p) : line_node<B, 2>(c, p));
+          q[p] = sQh[node * V + m];
+          f[p] = sFh[(d * NPC + node) * V + m];
+        }
+        // faces 2d (FLCoeff) and 2d+1 (FRCoeff) of line c
+        double ql = 0.0, qr = 0.0, fl = 0.0, fr = 0.0;
+#pragma unroll
+        for (int p = 0; p < B; p++) {
+          ql += q[p] * T.fl[p];
+          qr += q[p] * T.fr[p];
+          fl += f[p] * T.fl[p];
+          fr += f[p] * T.fr[p];
+        }
+        qb[((2 * d) * NF + c) * V + m] = ql;
+        qb[((2 * d + 1) * NF + c) * V + m] = qr;
+        fb[((2 * d) * NF + c) * V + m] = fl;
+        fb[((2 * d + 1) * NF + c) * V + m] = fr;
+        // volume-integral line sums
+#pragma unroll
+        for (int i = 0; i < B; i++) {
+          double v = 0.0;
+#pragma unroll
+          for (int p = 0; p < B; p++) v += T.kxi[i][p] * f[p];
+          const int node = d == 0 ? line_node<B, 0>(c, i) : (d == 1 ? line_node<B, 1>(c, i) : line_node<B, 2>(c, i));
+          sVI[(d * NPC + node) * V + m] = v;
+        }
+      }
+    }
   }
   __syncthreads();
   if (!valid) return;
-
   if (active) {
+    // lduh[s] = sum_d (idx_d prod_{e != d} w[s_e]) sum_p Kxi[s_d][p] Fh_d(s_d -> p)
+    int sd[3];
+    sd[0] = s % B;
+    sd[1] = (s / B) % B;
+    sd[2] = DIM == 3 ? s / (B * B) : 0;
     double* lduh = a.lduh + cell * (long)NPC * V;
     double out[V];
 #pragma unroll
@@ -138,52 +199,11 @@ __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int 
 #pragma unroll
       for (int e = 0; e < DIM; e++)
         if (e != d) us *= T.w[sd[e]];
-      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
 #pragma unroll
-      for (int p = 0; p < B; p++) {
-        const double k = T.kxi[sd[d]][p];
-#pragma unroll
-        for (int m = 0; m < V; m++) out[m] += k * line[p * stride[d] * V + m] * us;
-      }
+      for (int m = 0; m < V; m++) out[m] += sVI[(d * NPC + s) * V + m] * us;
     }
 #pragma unroll
     for (int m = 0; m < V; m++) lduh[s * V + m] = out[m];
-  }
-  {
-    constexpr int NF = S::NF;
-    double* qb = a.lQhbnd + cell * (long)2 * DIM * NF * V;
-    double* fb = a.lFhbnd + cell * (long)2 * DIM * NF * V;
-    for (int k = s; k < 2 * DIM * NF; k += G) {
-      const int f = k / NF, j = k % NF, d = f >> 1, side = f & 1;
-      int base, st;
-      if (DIM == 3) {
-        const int ia = j / B, ib = j % B;
-        if (d == 0) { base = (ia * B + ib) * B; st = 1; }
-        else if (d == 1) { base = ia * B * B + ib; st = B; }
-        else { base = ia * B + ib; st = B * B; }
-      } else {
-        if (d == 0) { base = j * B; st = 1; }
-        else { base = j; st = B; }
-      }
-      double vq[V], vf[V];
-#pragma unroll
-      for (int m = 0; m < V; m++) { vq[m] = 0.0; vf[m] = 0.0; }
-#pragma unroll
-      for (int l = 0; l < B; l++) {
-        const double c = side ? T.fr[l] : T.fl[l];
-        const int node = base + l * st;
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          vq[m] += sQh[node * V + m] * c;
-          vf[m] += sD[(d * NPC + node) * V + m] * c;
-        }
-      }
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        qb[(f * NF + j) * V + m] = vq[m];
-        fb[(f * NF + j) * V + m] = vf[m];
-      }
-    }
   }
   if (s == 0) {
     if (a.iters) a.iters[cell] = it;
@@ -193,7 +213,6 @@ __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int 
     }
   }
 }
-
 
 template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long block, double* smem) {
