@@ -26,6 +26,7 @@
 //    integral from shared memory; outputs are lduh, lQhbnd, lFhbnd.
 #include "exa_device.cuh"
 #include "aderdg_predictor_body.cuh"
+#include "aderdg_predictor_fp64_lines_body.cuh"
 
 namespace exa {
 
@@ -57,10 +58,45 @@ static exa_status_t launch_t(const PredArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_predictor launch");
 }
 
+template <int DIM, int N, bool PLANAR>
+__global__ void __launch_bounds__(Fp64LineShape<DIM, N>::NT) k_predictor_lines(PredArgs a) {
+  extern __shared__ double smem[];
+  predictor_fp64_lines_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
+}
+
+template <int DIM, int N, bool PLANAR>
+static exa_status_t launch_lines_fp64(const PredArgs& a, cudaStream_t st) {
+  using S = Fp64LineShape<DIM, N>;
+  auto kern = k_predictor_lines<DIM, N, PLANAR>;
+  const size_t smem = sizeof(double) * S::SM_DOUBLES;
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "predictor (lines) attribute");
+    attr_done[dev & 63] = true;
+  }
+  const long nblocks = (a.ncells + S::CPB - 1) / S::CPB;
+  if (nblocks <= 0) return EXA_OK;
+  if (nblocks > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
+  kern<<<(unsigned)nblocks, S::NT, smem, st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_predictor_lines launch");
+}
+
 template <int DIM, int N>
 static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
                               cudaStream_t st) {
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
+  // knob 3: 1 = node-gather, 2 = line-owner contraction (FP64, not for the
+  // reference-temporaries mode); default: line-owner for 3D order 4
+  // (measured faster there), node-gather elsewhere
+  const int variant = tune_get(kTuneFp64Variant, 0);
+  if (d.npar == 0 && !full && (variant == 2 || (variant == 0 && DIM == 3 && N == 4))) {
+    if (DIM == 3 && planar) return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
+    return planar ? launch_lines_fp64<DIM, N, true>(a, st) : launch_lines_fp64<DIM, N, false>(a, st);
+  }
   if (d.npar == 0) {
     if (DIM == 2 && planar)
       return full ? launch_t<DIM, N, 0, true, 1>(a, st) : launch_t<DIM, N, 0, true, 0>(a, st);

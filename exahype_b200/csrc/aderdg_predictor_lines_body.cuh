@@ -92,12 +92,6 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
   float* sB = sX + S::X_SIZE;                  // [B][V][NPC]
   double* sred = smem + S::CPB * S::CELL_F / 2;
 
-  int sd[3];
-  sd[0] = s % B;
-  sd[1] = (s / B) % B;
-  sd[2] = DIM == 3 ? s / (B * B) : 0;
-  const int stride[3] = {1, B, B * B};
-
   double lu[V];
   {
     const double* luh = a.luh + cell * (long)NPC * V;
@@ -107,32 +101,8 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
 
   // FP64 base flux and its derivative (once per cell)
-  {
-    double F0[DIM][V];
-    euler_flux<DIM, PLANAR>(lu, F0);
-    if (active)
-#pragma unroll
-      for (int d = 0; d < DIM; d++)
-#pragma unroll
-        for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m];
-  }
-  __syncthreads();
   double G0[V];
-#pragma unroll
-  for (int m = 0; m < V; m++) G0[m] = 0.0;
-  if (active) {
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
-#pragma unroll
-      for (int p = 0; p < B; p++) {
-        const double c = T.deriv[sd[d]][p] * a.idx[d];
-#pragma unroll
-        for (int m = 0; m < V; m++) G0[m] += c * line[p * stride[d] * V + m];
-      }
-    }
-  }
-  __syncthreads();  // the staging area becomes the loop buffers
+  mixed_base_derivative<DIM, N, PLANAR>(a, lu, s, valid, active, sD, G0);
 
   // base deviations (c0[t] - 1) luh - dt (sum_n tA[t][n]) D.F0, FP32, in
   // this node's slots of sB

@@ -90,6 +90,64 @@ __device__ __forceinline__ int line_node(int c, int p) {
   return (c / SD) * SD * B + (c % SD) + p * SD;
 }
 
+// Derivative G0 = sum_d (1/dx_d) D_d F(luh) of a mixed-precision predictor
+// cell's base flux (FP64, once per cell; every thread of the CTA calls it).
+// Line tasks (direction d, line c, variable m) read the B flux values of
+// their line once and store the B line sums (uniform derivative matrix);
+// each node thread then weights and sums its DIM line sums.  sD: the cell's
+// FP64 staging area (2 DIM NPC V doubles).  Returns G0 of node s.
+template <int DIM, int N, bool PLANAR>
+__device__ __forceinline__ void mixed_base_derivative(const PredArgs& a, const double* lu, int s, bool valid,
+                                                      bool active, double* sD, double* G0) {
+  using S = MixShape<DIM, N>;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G;
+  constexpr int L = NPC / B, TPD = L * V, TPT = (TPD + G - 1) / G;
+  const DGConst& T = c_dg[N];
+  double* sF0 = sD;                // [DIM][NPC][V]
+  double* sG = sD + DIM * NPC * V;  // [DIM][NPC][V]
+  if (active) {
+    double F0[DIM][V];
+    euler_flux<DIM, PLANAR>(lu, F0);
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int m = 0; m < V; m++) sF0[(d * NPC + s) * V + m] = F0[d][m];
+  }
+  __syncthreads();
+  if (valid) {
+#pragma unroll
+    for (int r = 0; r < TPT; r++) {
+      const int k = s + r * G;
+      if (k >= TPD) continue;
+      const int c = k % L, m = k / L;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        const int SD = d == 0 ? 1 : (d == 1 ? B : B * B);
+        const int n0 = d == 0 ? line_node<B, 0>(c, 0) : (d == 1 ? line_node<B, 1>(c, 0) : line_node<B, 2>(c, 0));
+        double f[B];
+#pragma unroll
+        for (int p = 0; p < B; p++) f[p] = sF0[(d * NPC + n0 + p * SD) * V + m];
+#pragma unroll
+        for (int i = 0; i < B; i++) {
+          double g = 0.0;
+#pragma unroll
+          for (int p = 0; p < B; p++) g += T.deriv[i][p] * f[p];
+          sG[(d * NPC + n0 + i * SD) * V + m] = g;
+        }
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int m = 0; m < V; m++) G0[m] = 0.0;
+  if (active)
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+#pragma unroll
+      for (int m = 0; m < V; m++) G0[m] += a.idx[d] * sG[(d * NPC + s) * V + m];
+  __syncthreads();  // the staging area becomes the caller's loop buffers
+}
+
 // FP64 outputs of a mixed-precision predictor cell (every thread of the CTA
 // calls it): time-averaged state Qh and flux Fh from luh, F(luh) and the FP32
 // deviations of the last Picard iterate (dqv: state per time node, fdv: the
@@ -105,17 +163,19 @@ __device__ __forceinline__ int line_node(int c, int p) {
 // node threads weight and sum over directions.  sD: the cell's FP64 staging
 // area, MixShape::STAGE_D doubles: Qh [NPC][V], Fh [DIM][NPC][V],
 // volume-integral line sums [DIM][NPC][V].
+template <int DIM, int N>
+__device__ __forceinline__ void dg_line_outputs(const PredArgs& a, long cell, int s, bool valid, bool active,
+                                                double* sD, int it, bool conv);
+
 template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int s, bool valid, bool active,
                                               const float (*dqv)[kV], const float (*fdv)[kV], double* sD,
                                               int it, bool conv) {
   using S = MixShape<DIM, N>;
-  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, NF = S::NF;
-  constexpr int L = NPC / B, TPD = L * V, TPT = (TPD + G - 1) / G;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC;
   const DGConst& T = c_dg[N];
-  double* sQh = sD;                     // [NPC][V]
-  double* sFh = sD + NPC * V;           // [DIM][NPC][V]
-  double* sVI = sFh + DIM * NPC * V;    // [DIM][NPC][V]
+  double* sQh = sD;            // [NPC][V]
+  double* sFh = sD + NPC * V;  // [DIM][NPC][V]
   const double* luh = a.luh + cell * (long)NPC * V;
   __syncthreads();  // the caller's loop buffers overlap the staging area
   if (active) {
@@ -138,6 +198,23 @@ __device__ __forceinline__ void mixed_outputs(const PredArgs& a, long cell, int 
 #pragma unroll
       for (int m = 0; m < V; m++) sFh[(d * NPC + s) * V + m] = F0[d][m] * wsum + (double)fdv[d][m];
   }
+  dg_line_outputs<DIM, N>(a, cell, s, valid, active, sD, it, conv);
+}
+
+// Face extrapolations and volume integral of a predictor cell from the
+// FP64 staging area written by the caller (Qh [NPC][V], Fh [DIM][NPC][V];
+// every thread of the CTA calls it after the caller's stores): see
+// mixed_outputs.
+template <int DIM, int N>
+__device__ __forceinline__ void dg_line_outputs(const PredArgs& a, long cell, int s, bool valid, bool active,
+                                                double* sD, int it, bool conv) {
+  using S = MixShape<DIM, N>;
+  constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, NF = S::NF;
+  constexpr int L = NPC / B, TPD = L * V, TPT = (TPD + G - 1) / G;
+  const DGConst& T = c_dg[N];
+  double* sQh = sD;                     // [NPC][V]
+  double* sFh = sD + NPC * V;           // [DIM][NPC][V]
+  double* sVI = sFh + DIM * NPC * V;    // [DIM][NPC][V]
   __syncthreads();
   if (valid) {
     double* qb = a.lQhbnd + cell * (long)2 * DIM * NF * V;
@@ -245,30 +322,8 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
 
   // base flux F0 = F(luh) and its derivative G0 (FP64, once per cell)
-  double F0[DIM][V];
-  euler_flux<DIM, PLANAR>(lu, F0);
-  if (active)
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int m = 0; m < V; m++) sD[(d * NPC + s) * V + m] = F0[d][m];
-  __syncthreads();
   double G0[V];
-#pragma unroll
-  for (int m = 0; m < V; m++) G0[m] = 0.0;
-  if (active) {
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      const double* line = sD + (d * NPC + s - sd[d] * stride[d]) * V;
-#pragma unroll
-      for (int p = 0; p < B; p++) {
-        const double c = T.deriv[sd[d]][p] * a.idx[d];
-#pragma unroll
-        for (int m = 0; m < V; m++) G0[m] += c * line[p * stride[d] * V + m];
-      }
-    }
-  }
-  __syncthreads();  // staging area is reused for the FP32 slices
+  mixed_base_derivative<DIM, N, PLANAR>(a, lu, s, valid, active, sD, G0);
 
   float dcf[DIM][B];
 #pragma unroll

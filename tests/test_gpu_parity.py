@@ -166,10 +166,20 @@ def test_grid_ic_matches_oracle():
     (2, 4, (6, 9), 0, 1, 1, 10),
     (2, 5, (5, 5), 1, 0, 0, 10),
 ])
-def test_grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps):
+@pytest.mark.parametrize('variant', [1, 2])
+def test_grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps, variant):
     """Every step is compared with the oracle stepping the identical input
     state (per-step parity, relative L2 <= 1e-12); a second oracle copy runs
-    free for all steps to bound the accumulated drift."""
+    free for all steps to bound the accumulated drift.  variant (tuning key
+    3): FP64 predictor contraction, 1 = node-gather, 2 = line-owner."""
+    E._lib.call('exa_tune_set', 3, variant)
+    try:
+        _grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps)
+    finally:
+        E._lib.call('exa_tune_set', 3, 0)
+
+
+def _grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps):
     pde = E.PDE_EULER_PLANAR if planar else E.PDE_EULER
     g = E.ADERDGGrid(dim, order, n, pde=pde, dt_policy=policy)
     param = 5.0 if kind == 0 else 0.2
