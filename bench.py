@@ -130,8 +130,8 @@ def measured_peaks():
 
 
 def ncu_traffic_per_cell():
-    """DRAM bytes per cell of k_predictor from the committed ncu summary."""
-    p = os.path.join(ROOT, 'profiles', 'k_predictor_3d_N4.md')
+    """DRAM bytes per cell of the FP64 predictor from the committed ncu summary."""
+    p = os.path.join(ROOT, 'profiles', 'k_predictor_lines_3d_N4.md')
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -494,7 +494,7 @@ def measure(ctx, precision, with_e2e):
                flop_per_cell_update=total_flop)
     if precision == 'fp64':
         out['roofline'] = {
-            'kernel': 'k_predictor', 'bound': 'fp64', 'achieved': achieved, 'peak': ctx['fp64_peak'],
+            'kernel': 'k_predictor_lines', 'bound': 'fp64', 'achieved': achieved, 'peak': ctx['fp64_peak'],
             'unit': 'TFLOP/s', 'frac': achieved / ctx['fp64_peak'],
             'peak_source': 'DFMA probe measured in this run (MEASURED_PEAKS.json has no FP64 figure)',
             'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
@@ -502,7 +502,7 @@ def measure(ctx, precision, with_e2e):
             'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}
     else:
         out['roofline'] = {
-            'kernel': 'k_predictor_mixed', 'bound': 'fp64+fp32', 'achieved_equiv_fp64_flop': achieved,
+            'kernel': 'k_predictor_mixed_lines', 'bound': 'fp64+fp32', 'achieved_equiv_fp64_flop': achieved,
             'unit': 'TFLOP/s', 'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
             'ms_per_launch': pred_ms, 'frac_of_fp64_peak': achieved / ctx['fp64_peak'],
             'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}
