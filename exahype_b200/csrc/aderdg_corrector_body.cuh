@@ -67,33 +67,54 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     cc[1] = (int)((cell / a.n[0]) % a.n[1]);
     cc[2] = DIM == 3 ? (int)(cell / ((long)a.n[0] * a.n[1])) : 0;
   }
-  // load own faces and the matching faces of the neighbours
+  // Own faces and the matching faces of the neighbours -> shared memory,
+  // as asynchronous 8-byte copies (cp.async): every copy of the CTA is in
+  // flight at once without holding registers.  The node's luh and lduh are
+  // loaded into registers meanwhile (needed after the face phases).
   if (valid) {
     const double* qo = a.lQhbnd + cell * FV;
     const double* fo = a.lFhbnd + cell * FV;
-    for (int k = s; k < FV; k += G) {
-      const int f = k / (NF * V), r = k % (NF * V);
+#pragma unroll
+    for (int f = 0; f < NFACE; f++) {
+      // the neighbour across face f and where its matching face f^1 lives
       const int d = f >> 1;
-      sQo[k] = qo[k];
-      sFo[k] = fo[k];
       const bool up = f & 1;
+      const double* nq;
+      const double* nf;
       if (d == DIM - 1 && a.halo_lo && (up ? cc[d] + 1 == a.n[d] : cc[d] == 0)) {
         // across a slab boundary: the adjacent slab's face data
-        const long lc = DIM == 3 ? (long)cc[1] * a.n[0] + cc[0] : cc[0];
-        const double* h = (up ? a.halo_hi : a.halo_lo) + lc * 2 * NF * V;
-        sQn[k] = h[r];
-        sFn[k] = h[NF * V + r];
-        continue;
+        const long lc2 = DIM == 3 ? (long)cc[1] * a.n[0] + cc[0] : cc[0];
+        const double* h = (up ? a.halo_hi : a.halo_lo) + lc2 * 2 * NF * V;
+        nq = h;
+        nf = h + NF * V;
+      } else {
+        int nc[3] = {cc[0], cc[1], cc[2]};
+        nc[d] = up ? (nc[d] + 1 == a.n[d] ? 0 : nc[d] + 1) : (nc[d] == 0 ? a.n[d] - 1 : nc[d] - 1);
+        const long nb = DIM == 3 ? ((long)nc[2] * a.n[1] + nc[1]) * a.n[0] + nc[0]
+                                 : (long)nc[1] * a.n[0] + nc[0];
+        nq = a.lQhbnd + nb * FV + (f ^ 1) * NF * V;
+        nf = a.lFhbnd + nb * FV + (f ^ 1) * NF * V;
       }
-      int nc[3] = {cc[0], cc[1], cc[2]};
-      nc[d] = up ? (nc[d] + 1 == a.n[d] ? 0 : nc[d] + 1) : (nc[d] == 0 ? a.n[d] - 1 : nc[d] - 1);
-      const long nb = DIM == 3 ? ((long)nc[2] * a.n[1] + nc[1]) * a.n[0] + nc[0]
-                               : (long)nc[1] * a.n[0] + nc[0];
-      const long off = nb * FV + (f ^ 1) * NF * V + r;
-      sQn[k] = a.lQhbnd[off];
-      sFn[k] = a.lFhbnd[off];
+      for (int r = s; r < NF * V; r += G) {
+        const int k = f * NF * V + r;
+        cp_async8(sQo + k, qo + k);
+        cp_async8(sFo + k, fo + k);
+        cp_async8(sQn + k, nq + r);
+        cp_async8(sFn + k, nf + r);
+      }
     }
   }
+  double v_lduh[V], v_luh[V];
+  if (valid && s < NPC) {
+    const double* lduh = a.lduh + cell * (long)NPC * V;
+    const double* luh = a.luh + cell * (long)NPC * V;
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      v_lduh[m] = lduh[s * V + m];
+      v_luh[m] = luh[s * V + m];
+    }
+  }
+  cp_async_commit_wait_all();
   __syncthreads();
   // face-averaged states (riemannSolverNonlinear.cpph:52-69)
   if (valid) {
@@ -138,11 +159,10 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     sd[0] = s % B;
     sd[1] = (s / B) % B;
     sd[2] = DIM == 3 ? s / (B * B) : 0;
-    const double* lduh = a.lduh + cell * (long)NPC * V;
     double* luh = a.luh + cell * (long)NPC * V;
     double v[V];
 #pragma unroll
-    for (int m = 0; m < V; m++) v[m] = lduh[s * V + m];
+    for (int m = 0; m < V; m++) v[m] = v_lduh[m];
     // surface integral (surfaceIntegralNonlinear.cpph:21-85)
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
@@ -169,7 +189,7 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     bool finite = true;
 #pragma unroll
     for (int m = 0; m < V; m++) {
-      q[m] = luh[s * V + m] + v[m] * us;
+      q[m] = v_luh[m] + v[m] * us;
       luh[s * V + m] = q[m];
       finite = finite && isfinite(q[m]);
     }

@@ -81,6 +81,17 @@ __device__ __forceinline__ double euler_max_eig(const double* q, int d) {
   return fmax(fabs(un - c), fmax(fabs(un), fabs(un + c)));
 }
 
+// ------------------------------------------------------ async copies
+// 8-byte global -> shared copy that completes asynchronously (cp.async,
+// sm_80+), and the wait for all of this thread's outstanding copies.
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
 // ------------------------------------------------------------ reductions
 // Sum over groups of G consecutive threads (G a power of two <= 32, or a
 // multiple of 32).  Every thread of a group returns the bitwise identical

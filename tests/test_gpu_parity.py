@@ -63,7 +63,9 @@ def test_predictor_batched_vs_oracle(dim, order, planar):
 
 def test_predictor_vi_matches_full():
     """The production (fused) predictor writes the same lduh/faces as the
-    reference-temporaries variant, and its stats count the iterations."""
+    reference-temporaries variant (to rounding: for 3D order 4 the production
+    path uses the line-owner contraction, which sums in another order), and
+    its stats count the iterations."""
     rng = np.random.default_rng(7)
     dim, order, ncells = 3, 4, 150
     B = order + 1
@@ -81,7 +83,7 @@ def test_predictor_vi_matches_full():
                      a['fbnd'])
     K.predictor_vi(ncells, luh, 1e-4, b['lduh'], b['qbnd'], b['fbnd'], iters=it, stats=stats)
     for k in ('lduh', 'qbnd', 'fbnd'):
-        assert np.array_equal(a[k].download(), b[k].download()), k
+        assert rel(b[k].download(), a[k].download()) < 1e-13, k
     st = stats.download()
     assert int(st[0]) == int(it.download().astype(np.int64).sum())
 
