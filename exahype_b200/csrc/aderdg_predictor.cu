@@ -90,10 +90,11 @@ static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int
                               cudaStream_t st) {
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
   // knob 3: 1 = node-gather, 2 = line-owner contraction (FP64, not for the
-  // reference-temporaries mode); default: line-owner for 3D order 4
-  // (measured faster there), node-gather elsewhere
+  // reference-temporaries mode); default: line-owner for orders >= 4, where
+  // it measured faster in 2D and 3D (for orders 2-3 the cell has more
+  // line tasks than threads and node-gather wins)
   const int variant = tune_get(kTuneFp64Variant, 0);
-  if (d.npar == 0 && !full && (variant == 2 || (variant == 0 && DIM == 3 && N == 4))) {
+  if (d.npar == 0 && !full && (variant == 2 || (variant == 0 && N >= 4))) {
     if (DIM == 3 && planar) return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
     return planar ? launch_lines_fp64<DIM, N, true>(a, st) : launch_lines_fp64<DIM, N, false>(a, st);
   }

@@ -106,9 +106,10 @@ static exa_status_t launch_predictor_mixed_lines(const exa_aderdg_desc_t& d, con
 
 exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& a, cudaStream_t st) {
   // knob 2: 1 = node-gather contraction, 2 = line-owner contraction,
-  // default: line-owner for 3D order 4, node-gather elsewhere
+  // default: line-owner for orders >= 4 (measured faster in 2D and 3D),
+  // node-gather for orders 2-3
   const int variant = tune_get(kTuneMixedVariant, 0);
-  if (d.npar == 0 && (variant == 2 || (variant == 0 && d.dim == 3 && d.order == 4)))
+  if (d.npar == 0 && (variant == 2 || (variant == 0 && d.order >= 4)))
     return launch_predictor_mixed_lines(d, a, st);
   if (d.npar != 0) return set_error(EXA_EINVAL, "mixed precision: npar must be 0");
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;

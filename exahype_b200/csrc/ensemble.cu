@@ -25,6 +25,8 @@
 #include "exa_device.cuh"
 #include "aderdg_predictor_body.cuh"
 #include "aderdg_predictor_mixed_body.cuh"
+#include "aderdg_predictor_lines_body.cuh"
+#include "aderdg_predictor_fp64_lines_body.cuh"
 #include "aderdg_corrector_body.cuh"
 
 namespace cg = cooperative_groups;
@@ -70,16 +72,18 @@ struct EnsArgs {
 
 constexpr int kEnsNT = 128;
 
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+// orders whose predictor runs the line-owner contraction (as the stand-alone
+// kernels do by default: measured faster from order 4 on)
+template <int N>
+constexpr bool ens_lines() { return N >= 4; }
 // shared memory (doubles) the largest 2D order needs in either phase
 template <int N>
 constexpr int ens_smem_n() {
-  return PredShape<2, N, 0>::SM_DOUBLES > MixShape<2, N>::SM_DOUBLES
-             ? (PredShape<2, N, 0>::SM_DOUBLES > CorrShapeSmem<2, N>::value ? PredShape<2, N, 0>::SM_DOUBLES
-                                                                           : CorrShapeSmem<2, N>::value)
-             : (MixShape<2, N>::SM_DOUBLES > CorrShapeSmem<2, N>::value ? MixShape<2, N>::SM_DOUBLES
-                                                                        : CorrShapeSmem<2, N>::value);
+  return cmax(cmax(ens_lines<N>() ? Fp64LineShape<2, N>::SM_DOUBLES : PredShape<2, N, 0>::SM_DOUBLES,
+                   ens_lines<N>() ? LineShape<2, N>::SM_DOUBLES : MixShape<2, N>::SM_DOUBLES),
+              CorrShapeSmem<2, N>::value);
 }
-constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int kEnsSmemDoubles = cmax(cmax(ens_smem_n<2>(), ens_smem_n<3>()), cmax(ens_smem_n<4>(), ens_smem_n<5>()));
 
 __device__ __forceinline__ PredArgs pred_args(const SolveDev& sv, int precision) {
@@ -126,8 +130,13 @@ __device__ __forceinline__ CorrArgs corr_args(SolveDev& sv) {
 template <int N, bool PLANAR, int PREC>
 __device__ __noinline__ void ens_pred(const SolveDev* sv, int block, double* smem, int precision) {
   const PredArgs a = pred_args(*sv, precision);
-  if (PREC) predictor_mixed_block<2, N, PLANAR>(a, block, smem);
-  else predictor_block<2, N, 0, PLANAR, 0>(a, block, smem);
+  if constexpr (ens_lines<N>()) {
+    if (PREC) predictor_mixed_lines_block<2, N, PLANAR>(a, block, smem);
+    else predictor_fp64_lines_block<2, N, PLANAR>(a, block, smem);
+  } else {
+    if (PREC) predictor_mixed_block<2, N, PLANAR>(a, block, smem);
+    else predictor_block<2, N, 0, PLANAR, 0>(a, block, smem);
+  }
 }
 
 template <int N, bool PLANAR>
