@@ -4,8 +4,8 @@ The compute path is libexahype_b200.so (hand-written sm_100a CUDA behind the
 C ABI declared in include/exa_kernels.h); this package is the thin Python
 host layer over that ABI.
 """
-from ._lib import (EXA_OK, PDE_EULER, PDE_EULER_PLANAR, PREC_FP64, PREC_MIXED, ExaError,
-                   lib)
+from ._lib import (BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, EXA_OK, PDE_EULER, PDE_EULER_PLANAR, PREC_FP64,
+                   PREC_MIXED, ExaError, lib)
 from .aderdg import ADERDGGrid, ADERDGSolver, BatchedADERDG, make_desc
 from .device import DeviceBuffer, PinnedBuffer, Stream, Timer, device_count, launch_count
 from .ensemble import Ensemble, solve_config
@@ -13,4 +13,5 @@ from .fv import FVGrid, FVPatches
 
 __all__ = ['ADERDGGrid', 'ADERDGSolver', 'BatchedADERDG', 'DeviceBuffer', 'PinnedBuffer', 'Stream',
            'Timer', 'FVPatches', 'FVGrid', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
-           'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED']
+           'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED', 'BC_PERIODIC', 'BC_OUTFLOW',
+           'BC_REFLECT']

@@ -25,6 +25,9 @@ PDE_EULER = 0
 PDE_EULER_PLANAR = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
+BC_PERIODIC = 0
+BC_OUTFLOW = 1
+BC_REFLECT = 2
 
 
 class ExaError(RuntimeError):
@@ -135,6 +138,7 @@ SIGNATURES = {
     'exa_fv_grid_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_fv_grid_device_state': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
+    'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                            C.POINTER(sz)]),
     'exa_aderdg_grid_dt_slot': (i32, [vp, C.POINTER(vp)]),

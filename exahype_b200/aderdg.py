@@ -202,6 +202,12 @@ class ADERDGGrid:
         call('exa_aderdg_grid_device_state', self.h, C.byref(p))
         return p
 
+    def set_boundary(self, bc):
+        """Boundary rule per dimension: _lib.BC_PERIODIC / BC_OUTFLOW /
+        BC_REFLECT (see exa_aderdg_grid_set_boundary)."""
+        arr = (C.c_int * 3)(*(list(bc) + [0] * (3 - len(bc))))
+        call('exa_aderdg_grid_set_boundary', self.h, arr)
+
     # -- slab decomposition (see exahype_b200.slab) --
     def set_halo(self, enable=True):
         call('exa_aderdg_grid_set_halo', self.h, int(enable))

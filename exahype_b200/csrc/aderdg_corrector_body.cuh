@@ -81,7 +81,18 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
       const bool up = f & 1;
       const double* nq;
       const double* nf;
-      if (d == DIM - 1 && a.halo_lo && (up ? cc[d] + 1 == a.n[d] : cc[d] == 0)) {
+      const bool at_end = up ? cc[d] + 1 == a.n[d] : cc[d] == 0;
+      if (at_end && a.bc[d] != 0) {
+        // domain boundary: the outside state is formed below from this
+        // cell's own face data
+        for (int r = s; r < NF * V; r += G) {
+          const int k = f * NF * V + r;
+          cp_async8(sQo + k, qo + k);
+          cp_async8(sFo + k, fo + k);
+        }
+        continue;
+      }
+      if (d == DIM - 1 && a.halo_lo && at_end) {
         // across a slab boundary: the adjacent slab's face data
         const long lc2 = DIM == 3 ? (long)cc[1] * a.n[0] + cc[0] : cc[0];
         const double* h = (up ? a.halo_hi : a.halo_lo) + lc2 * 2 * NF * V;
@@ -116,6 +127,36 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
   }
   cp_async_commit_wait_all();
   __syncthreads();
+  if (a.bc_any) {
+    // outside states of domain-boundary faces, one thread per face node
+    if (valid)
+      for (int k = s; k < NFACE * NF; k += G) {
+        const int f = k / NF, j = k % NF, d = f >> 1;
+        const bool up = f & 1;
+        if (a.bc[d] == 0 || !(up ? cc[d] + 1 == a.n[d] : cc[d] == 0)) continue;
+        const int o = (f * NF + j) * V;
+        if (a.bc[d] == EXA_BC_OUTFLOW) {
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            sQn[o + m] = sQo[o + m];
+            sFn[o + m] = sFo[o + m];
+          }
+        } else {  // EXA_BC_REFLECT
+          double qo_[V];
+#pragma unroll
+          for (int m = 0; m < V; m++) qo_[m] = sQo[o + m];
+          qo_[d + 1] = -qo_[d + 1];
+          double F[3][V];
+          euler_flux<DIM, PLANAR>(qo_, F);
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            sQn[o + m] = qo_[m];
+            sFn[o + m] = F[d][m];
+          }
+        }
+      }
+    __syncthreads();
+  }
   // face-averaged states (riemannSolverNonlinear.cpph:52-69)
   if (valid) {
     for (int k = s; k < NFACE * 2 * V; k += G) {

@@ -85,6 +85,7 @@ struct exa_aderdg_grid {
   double* halo = nullptr;  // send_lo | send_hi | recv_lo | recv_hi
   long layer = 0;          // cells in one layer of the last dimension
   size_t halo_count = 0;   // doubles per buffer
+  int bc[3] = {0, 0, 0};   // EXA_BC_* per dimension
   int log_cap = 4096;
   double dt_factor = 0;
   bool primed = false;
@@ -182,6 +183,10 @@ static exa_status_t grid_correct(exa_aderdg_grid* g) {
   if (g->halo) {
     c.halo_lo = g->halo + 2 * g->halo_count;
     c.halo_hi = g->halo + 3 * g->halo_count;
+  }
+  for (int i = 0; i < 3; i++) {
+    c.bc[i] = i < g->cfg.dim ? g->bc[i] : 0;
+    c.bc_any |= c.bc[i] != 0;
   }
   return launch_corrector(g->cfg.dim, g->cfg.order, g->cfg.pde, c, g->st);
 }
@@ -437,8 +442,24 @@ exa_status_t exa_aderdg_grid_init_slab(exa_aderdg_grid* g, int kind, double para
   return cuda_status(cudaStreamSynchronize(g->st), "grid init");
 }
 
+exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc) {
+  if (!g || !bc) return set_error(EXA_EINVAL, "NULL argument");
+  for (int i = 0; i < g->cfg.dim; i++)
+    if (bc[i] < EXA_BC_PERIODIC || bc[i] > EXA_BC_REFLECT) return set_error(EXA_EINVAL, "unknown boundary rule");
+  if (g->halo && bc[g->cfg.dim - 1] != EXA_BC_PERIODIC)
+    return set_error(EXA_EINVAL, "slab halos need a periodic last dimension");
+  for (int i = 0; i < 3; i++) g->bc[i] = i < g->cfg.dim ? bc[i] : 0;
+  if (g->graph) {  // the captured step holds the old arguments
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  return EXA_OK;
+}
+
 exa_status_t exa_aderdg_grid_set_halo(exa_aderdg_grid* g, int enable) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (enable && g->bc[g->cfg.dim - 1] != EXA_BC_PERIODIC)
+    return set_error(EXA_EINVAL, "slab halos need a periodic last dimension");
   if (g->graph) {
     cudaGraphExecDestroy(g->graph);
     g->graph = nullptr;

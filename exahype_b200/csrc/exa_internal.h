@@ -66,6 +66,10 @@ struct CorrArgs {
   // boundary layer).  NULL = periodic.
   const double* halo_lo;
   const double* halo_hi;
+  // boundary rule per dimension (EXA_BC_*; 0 = periodic) and whether any
+  // dimension is not periodic (uniform over the CTA: guards a barrier)
+  int bc[3];
+  int bc_any;
 };
 exa_status_t launch_corrector(int dim, int order, int pde, const CorrArgs& a, cudaStream_t st);
 

@@ -292,6 +292,20 @@ exa_status_t exa_aderdg_grid_get_state(exa_aderdg_grid* g, double* host_luh);
 exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_host);
 /* capture one step pair in a CUDA graph and replay it for later steps */
 exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable);
+/* Boundary conditions per dimension (both ends), replacing the periodic
+ * wrap.  The reference applies the user's boundaryValues hook at every face
+ * node of a domain-boundary face (aderdg/generic/c/3d/boundaryConditions.cpph:
+ * 24-85) and solves the Riemann problem between the cell's face data and the
+ * returned outside state, the outside taken as the left state on faces 2d
+ * and as the right state on faces 2d+1 (ADERDGSolver.cpp:2854-2925
+ * applyBoundaryConditions).  PDE hooks cannot cross to the device, so the
+ * outside state is one of these built-in rules:
+ *   EXA_BC_OUTFLOW: QOut = QIn, FOut = FIn (the EulerFV demonstrator's rule,
+ *     Demonstrators/EulerFV/MyEulerSolver.cpp:87-98);
+ *   EXA_BC_REFLECT: QOut = QIn with the normal momentum negated, FOut = the
+ *     normal flux of QOut (slip wall). */
+enum { EXA_BC_PERIODIC = 0, EXA_BC_OUTFLOW = 1, EXA_BC_REFLECT = 2 };
+exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc);
 exa_status_t exa_aderdg_grid_stream(exa_aderdg_grid* g, void** stream);
 /* per-phase CUDA-event timing of every step (disables graph replay):
  * predictor (k_predictor) and corrector (k_corrector + k_commit) */

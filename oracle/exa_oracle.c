@@ -566,10 +566,41 @@ double orc_aderdg_grid_dt(int dim, int order, int planar, const int* n,
   return dt;
 }
 
+/* Outside state of a domain-boundary face node (the built-in stand-ins for
+ * the reference's boundaryValues hook, boundaryConditions.cpph:24-85):
+ * bc 1 = outflow (copy in -> out), bc 2 = reflecting wall (normal momentum
+ * negated, normal flux of the reflected state). */
+static void orc_boundary_values(int dim, int planar, int bc, int d, const double* qin,
+                                const double* fin, double* qout, double* fout) {
+  int m;
+  if (bc == 1) {
+    for (m = 0; m < 5; m++) {
+      qout[m] = qin[m];
+      fout[m] = fin[m];
+    }
+    return;
+  }
+  {
+    double F[3 * 5];
+    for (m = 0; m < 5; m++) qout[m] = qin[m];
+    qout[d + 1] = -qout[d + 1];
+    orc_euler_flux(dim, planar, qout, F);
+    for (m = 0; m < 5; m++) fout[m] = F[d * 5 + m];
+  }
+}
+
 double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
                             const double* dx, double* luh, int dt_policy,
                             double cfl, double dt_fixed, int* iters,
                             int nthreads) {
+  return orc_aderdg_grid_step_bc(dim, order, planar, n, dx, luh, dt_policy, cfl, dt_fixed, iters,
+                                 nthreads, NULL);
+}
+
+double orc_aderdg_grid_step_bc(int dim, int order, int planar, const int* n,
+                               const double* dx, double* luh, int dt_policy,
+                               double cfl, double dt_fixed, int* iters,
+                               int nthreads, const int* bc) {
   const int B = order + 1, V = 5;
   const int nn = dim == 3 ? B * B * B : B * B;
   const int nst = nn * B;
@@ -604,14 +635,37 @@ double orc_aderdg_grid_step(int dim, int order, int planar, const int* n,
     }
     free(lQi); free(lQo); free(rhs); free(lFi); free(lQhi); free(lFhi);
   }
-  /* faces: for each cell and direction, the face towards the +d neighbour */
+  /* faces: for each cell and direction, the face towards the +d neighbour;
+   * with a boundary rule in direction d, the faces on the domain ends are
+   * solved against the outside state instead (applyBoundaryConditions,
+   * ADERDGSolver.cpp:2854-2925: outside = left state on faces 2d, right
+   * state on faces 2d+1) */
   const int fs = nfn * V;
   for (int d = 0; d < dim; d++) {
+    const int bcd = bc ? bc[d] : 0;
 #pragma omp parallel for schedule(static)
     for (long c = 0; c < nc; c++) {
       int cx = (int)(c % n[0]), cy = (int)((c / n[0]) % n[1]);
       int cz = dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0;
       int r[3] = {cx, cy, cz};
+      if (bcd) {
+        const int j0 = r[d];
+        if (j0 == 0) {
+          double* FR = fb + (c * 2 * dim + 2 * d) * fs;
+          const double* QR = qb + (c * 2 * dim + 2 * d) * fs;
+          double qo[125 * 5], fo[125 * 5];
+          for (int j = 0; j < nfn; j++) orc_boundary_values(dim, planar, bcd, d, QR + j * V, FR + j * V, qo + j * V, fo + j * V);
+          orc_riemann(dim, order, V, 0, planar, fo, FR, qo, QR, d);
+        }
+        if (j0 + 1 == n[d]) {
+          double* FL = fb + (c * 2 * dim + 2 * d + 1) * fs;
+          const double* QL = qb + (c * 2 * dim + 2 * d + 1) * fs;
+          double qo[125 * 5], fo[125 * 5];
+          for (int j = 0; j < nfn; j++) orc_boundary_values(dim, planar, bcd, d, QL + j * V, FL + j * V, qo + j * V, fo + j * V);
+          orc_riemann(dim, order, V, 0, planar, FL, fo, QL, qo, d);
+          continue;
+        }
+      }
       r[d] = (r[d] + 1) % n[d];
       long cr = dim == 3 ? ((long)r[2] * n[1] + r[1]) * n[0] + r[0]
                          : (long)r[1] * n[0] + r[0];

@@ -85,6 +85,12 @@ void orc_aderdg_slab_correct(int dim, int order, int planar, const int* n,
                              const double* dx, double* luh, double* lduh,
                              double* qb, double* fb, const double* recv_lo,
                              const double* recv_hi, double dt);
+/* As orc_aderdg_grid_step with a boundary rule per dimension (NULL or 0 =
+ * periodic, 1 = outflow, 2 = reflecting wall; see orc_boundary_values). */
+double orc_aderdg_grid_step_bc(int dim, int order, int planar, const int* n,
+                               const double* dx, double* luh, int dt_policy,
+                               double cfl, double dt_fixed, int* iters,
+                               int nthreads, const int* bc);
 /* CPU-baseline sample: one step's per-cell work on ncells independent
  * cells (each its own periodic neighbour). */
 void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,

@@ -47,6 +47,8 @@ def lib():
     L.orc_aderdg_grid_dt.argtypes = [i, i, i, _ip, _dp, _dp, i, d]
     L.orc_aderdg_grid_step.restype = d
     L.orc_aderdg_grid_step.argtypes = [i, i, i, _ip, _dp, _dp, i, d, d, C.c_void_p, i]
+    L.orc_aderdg_grid_step_bc.restype = d
+    L.orc_aderdg_grid_step_bc.argtypes = [i, i, i, _ip, _dp, _dp, i, d, d, C.c_void_p, i, C.c_void_p]
     L.orc_aderdg_grid_ic.argtypes = [i, i, _ip, _dp, _dp, i, d, C.c_ulonglong, d]
     L.orc_rusanov.restype = d
     L.orc_rusanov.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, i]
@@ -105,13 +107,15 @@ def grid_ic(dim, order, n, kind=0, param=5.0, seed=1234, noise=0.0, dx=None):
 
 
 def grid_step(dim, order, n, luh, dt_policy=0, cfl=0.9, dt_fixed=0.0, planar=0,
-              nthreads=0, dx=None):
+              nthreads=0, dx=None, bc=None):
     n = np.asarray(n, dtype=np.int32)
     if dx is None:
         dx = 1.0 / n.astype(np.float64)
     iters = np.zeros(int(np.prod(n)), dtype=np.int32)
-    dt = lib().orc_aderdg_grid_step(dim, order, planar, n, np.asarray(dx, dtype=np.float64), luh,
-                                    dt_policy, cfl, dt_fixed, iters.ctypes.data, nthreads)
+    bcs = np.asarray(list(bc) + [0] * (3 - len(bc)), dtype=np.int32) if bc is not None else None
+    dt = lib().orc_aderdg_grid_step_bc(dim, order, planar, n, np.asarray(dx, dtype=np.float64), luh,
+                                       dt_policy, cfl, dt_fixed, iters.ctypes.data, nthreads,
+                                       bcs.ctypes.data if bcs is not None else None)
     return dt, iters
 
 

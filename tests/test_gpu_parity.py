@@ -217,3 +217,37 @@ def test_grid_graph_replay_is_bitwise_identical():
     assert np.array_equal(da, db)
     assert np.array_equal(a.get_state(), b.get_state())
     assert a.status()['time'] == b.status()['time']
+
+
+@pytest.mark.parametrize('dim,order,n,bc,steps', [
+    (2, 3, (9, 7), (1, 1), 8),
+    (2, 4, (6, 8), (2, 1), 6),
+    (2, 2, (10, 5), (2, 2), 8),
+    (3, 4, (4, 3, 5), (1, 2, 1), 4),
+    (3, 3, (3, 4, 3), (2, 2, 2), 4),
+])
+def test_grid_boundary_conditions_vs_oracle(dim, order, n, bc, steps):
+    """Outflow / reflecting-wall boundaries (exa_aderdg_grid_set_boundary)
+    against the oracle's boundary rules, per step from the identical state."""
+    g = E.ADERDGGrid(dim, order, n)
+    g.set_boundary(bc)
+    g.init(kind=0, param=5.0, seed=8, noise=1e-3)
+    u = g.get_state()
+    for s in range(steps):
+        dt_gpu = g.step(1, want_dt=True)[0]
+        dt_ref, _ = O.grid_step(dim, order, n, u, bc=bc)
+        assert abs(dt_gpu - dt_ref) <= 1e-13 * dt_ref, (s, dt_gpu, dt_ref)
+        got = g.get_state()
+        assert rel(got, u) < TOL, (s, rel(got, u))
+        u = got.copy()
+    g.destroy()
+
+
+def test_grid_boundary_rejects_bad_rule():
+    g = E.ADERDGGrid(2, 3, (4, 4))
+    with pytest.raises(E.ExaError):
+        g.set_boundary((0, 7))
+    g.set_halo(True)
+    with pytest.raises(E.ExaError):
+        g.set_boundary((1, 1))  # slab halos need a periodic last dimension
+    g.destroy()
