@@ -711,6 +711,29 @@ def run_fv(args, rank, world, dist):
             pin.free()
         out[name] = r
         g.destroy()
+    # the reference's FV layout: a grid of 10x10-subcell patches exchanging
+    # ghost layers every step (EulerFV demonstrator patch size)
+    for scheme, name in ((1, 'musclhancock_patches10'), (0, 'godunov_patches10')):
+        npx = max(1, P // 10)
+        g = E.FVPatchGrid(scheme, 10, npx, npx)
+        g.init(amp=0.2, seed=args.seed + rank, noise=1e-3)
+        g.step(args.warmup)
+        stream = g.stream()
+        E.device.synchronize()
+        if dist:
+            dist.barrier()
+        t = Timer()
+        l0 = E.launch_count()
+        t.start(stream)
+        g.step(args.steps)
+        t.stop(stream)
+        ms = t.elapsed_ms()
+        launches = E.launch_count() - l0
+        cells = g.ncells
+        out[name] = {'value': world * cells * args.steps / (ms * 1e-3), 'ms_per_step': ms / args.steps,
+                     'cells': cells, 'patches': npx * npx, 'gpu_launches': launches,
+                     'hbm_gbs_algorithmic': 80.0 * cells / (ms / args.steps * 1e-3) / 1e9}
+        g.destroy()
     if rank == 0:
         m = out['musclhancock']
         line = {'metric': '2D Euler FV MUSCL-Hancock cell-updates/s', 'value': m['value'],
@@ -721,7 +744,9 @@ def run_fv(args, rank, world, dist):
                            'l2_flush': 'inputs larger than L2 (%.1f GB per state copy)' % ((P + 4) ** 2 * 40 / 1e9),
                            'parallelism': 'replicas%d' % world if world > 1 else 'single'},
                 'roofline': m['roofline'], 'e2e': m.get('e2e'), 'gpu_launches': m['gpu_launches'],
-                'clocks': m['clocks'], 'godunov': out['godunov']}
+                'clocks': m['clocks'], 'godunov': out['godunov'],
+                'patch_grid_10': {'musclhancock': out['musclhancock_patches10'],
+                                  'godunov': out['godunov_patches10']}}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -9,9 +9,9 @@ from ._lib import (BC_OUTFLOW, BC_PERIODIC, BC_REFLECT, EXA_OK, PDE_EULER, PDE_E
 from .aderdg import ADERDGGrid, ADERDGSolver, BatchedADERDG, make_desc
 from .device import DeviceBuffer, PinnedBuffer, Stream, Timer, device_count, launch_count
 from .ensemble import Ensemble, solve_config
-from .fv import FVGrid, FVPatches
+from .fv import FVGrid, FVPatchGrid, FVPatches
 
 __all__ = ['ADERDGGrid', 'ADERDGSolver', 'BatchedADERDG', 'DeviceBuffer', 'PinnedBuffer', 'Stream',
-           'Timer', 'FVPatches', 'FVGrid', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
+           'Timer', 'FVPatches', 'FVGrid', 'FVPatchGrid', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
            'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED', 'BC_PERIODIC', 'BC_OUTFLOW',
            'BC_REFLECT']

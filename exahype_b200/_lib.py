@@ -137,6 +137,15 @@ SIGNATURES = {
     'exa_fv_grid_status': (i32, [vp, C.POINTER(f64), C.POINTER(f64)]),
     'exa_fv_grid_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_fv_grid_device_state': (i32, [vp, C.POINTER(vp)]),
+    'exa_fv_patchgrid_create': (i32, [i32, i32, i32, i32, f64, i32, C.POINTER(vp)]),
+    'exa_fv_patchgrid_destroy': (i32, [vp]),
+    'exa_fv_patchgrid_state_size': (sz, [vp]),
+    'exa_fv_patchgrid_init': (i32, [vp, f64, u64, f64]),
+    'exa_fv_patchgrid_set_state': (i32, [vp, vp]),
+    'exa_fv_patchgrid_get_state': (i32, [vp, vp]),
+    'exa_fv_patchgrid_step': (i32, [vp, i32]),
+    'exa_fv_patchgrid_status': (i32, [vp, C.POINTER(f64), C.POINTER(f64)]),
+    'exa_fv_patchgrid_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),

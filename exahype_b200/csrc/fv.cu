@@ -545,7 +545,7 @@ constexpr size_t kMusclPeriodicSmem =
 
 // --------------------------------------------------------- stable dt
 template <bool PLANAR>
-__global__ void k_fv_stable_dt(FVArgs a, double* dt_patch) {
+__global__ void k_fv_stable_dt(FVArgs a, double* dt_patch, int one_slot) {
   const int D = kV + a.npar, S = a.S, P = a.P, g = a.g;
   const long patch = blockIdx.y;
   const double* luh = a.luh + patch * (long)S * S * D;
@@ -557,7 +557,8 @@ __global__ void k_fv_stable_dt(FVArgs a, double* dt_patch) {
     dtl = fmin(dtl, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(q, 1));
   }
   for (int o = 16; o > 0; o >>= 1) dtl = fmin(dtl, __shfl_xor_sync(0xffffffffu, dtl, o));
-  if ((threadIdx.x & 31) == 0) atomic_min_pos_double((unsigned long long*)&dt_patch[patch], dtl);
+  if ((threadIdx.x & 31) == 0)
+    atomic_min_pos_double((unsigned long long*)&dt_patch[one_slot ? 0 : patch], dtl);
 }
 
 __global__ void k_fv_ghosts(int P, int g, int D, long npatches, double* luh) {
@@ -672,8 +673,8 @@ exa_status_t fv_patch_prime_async(const exa_fv_desc_t& d, const double* luh, uns
   const long cells = (long)d.patch * d.patch;
   unsigned bx = (unsigned)((cells + 255) / 256);
   if (bx > 1024) bx = 1024;
-  if (d.pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots);
-  else k_fv_stable_dt<false><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots);
+  if (d.pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots, 0);
+  else k_fv_stable_dt<false><<<dim3(bx, 1), 256, 0, st>>>(a, (double*)slots, 0);
   count_launch(2);
   return cuda_status(cudaGetLastError(), "fv prime");
 }
@@ -812,8 +813,8 @@ exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches, const do
   unsigned bx = (unsigned)((cells + 255) / 256);
   if (bx > 1024) bx = 1024;
   dim3 grid(bx, (unsigned)npatches);
-  if (desc->pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<grid, 256, 0, st>>>(a, dt_patch);
-  else k_fv_stable_dt<false><<<grid, 256, 0, st>>>(a, dt_patch);
+  if (desc->pde == EXA_PDE_EULER_PLANAR) k_fv_stable_dt<true><<<grid, 256, 0, st>>>(a, dt_patch, 0);
+  else k_fv_stable_dt<false><<<grid, 256, 0, st>>>(a, dt_patch, 0);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_fv_stable_dt");
 }
@@ -946,6 +947,250 @@ exa_status_t exa_fv_grid_stream(exa_fv_grid* g, void** stream) {
 exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev) {
   if (!g || !luh_dev) return set_error(EXA_EINVAL, "NULL argument");
   *luh_dev = g->luh;
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------- grid of periodic patches
+// The reference's finite-volume layout: a uniform grid of cells, each with
+// its own patch of patch^2 subcells and g ghost layers; per step the ghost
+// layers facing a neighbour are copied from the neighbour's boundary layers
+// (ghostLayerFilling, kernels/finitevolumes/commons/c/commons.cpph:337-405,
+// called per face by FiniteVolumesSolver::mergeNeighbours,
+// FiniteVolumesSolver.cpp:659-686; corner ghosts are not filled there and
+// the stencils never read them), then every patch takes the same
+// Godunov / MUSCL-Hancock step with the global minimum dt.  Here the patch
+// grid is periodic, npx x npy patches stored back to back (patch-major,
+// x fastest), which is the batched FV entry points' layout.
+namespace exa {
+
+// one thread per face-ghost cell of every patch
+__global__ void k_fv_patch_exchange(int P, int g, int D, int npx, int npy, double* luh) {
+  const int S = P + 2 * g;
+  const long per = 4L * g * P;  // face ghosts per patch: left, right, bottom, top
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= per * npx * npy) return;
+  const long patch = gid / per;
+  const int r = (int)(gid % per);
+  const int side = r / (g * P), i = (r / g) % P, k = r % g;  // i along the face, k across
+  const int px = (int)(patch % npx), py = (int)(patch / npx);
+  int j, x, nj, nx, qx = px, qy = py;  // destination (j, x) and source (nj, nx) in patch (qx, qy)
+  if (side == 0) {        // left ghosts <- left neighbour's right boundary layer
+    j = g + i; x = k; qx = (px + npx - 1) % npx; nj = j; nx = P + k;
+  } else if (side == 1) { // right ghosts <- right neighbour's left boundary layer
+    j = g + i; x = g + P + k; qx = (px + 1) % npx; nj = j; nx = g + k;
+  } else if (side == 2) { // bottom ghosts <- lower neighbour's top boundary layer
+    j = k; x = g + i; qy = (py + npy - 1) % npy; nj = P + k; nx = x;
+  } else {                // top ghosts <- upper neighbour's bottom boundary layer
+    j = g + P + k; x = g + i; qy = (py + 1) % npy; nj = g + k; nx = x;
+  }
+  const long src_patch = (long)qy * npx + qx;
+  double* dst = luh + (patch * S * S + (long)j * S + x) * D;
+  const double* src = luh + (src_patch * S * S + (long)nj * S + nx) * D;
+  for (int m = 0; m < D; m++) dst[m] = src[m];
+}
+
+// density sine wave of the whole domain on every patch (global coordinates
+// and noise index), ghosts included
+__global__ void k_fv_patch_ic(int P, int g, int D, int npx, int npy, double hx, double hy, double amp,
+                              unsigned long long seed, double noise, double* luh) {
+  const int S = P + 2 * g;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long)S * S * npx * npy) return;
+  const long patch = gid / ((long)S * S);
+  const int c = (int)(gid % ((long)S * S));
+  const int j = c / S, k = c % S;
+  const int px = (int)(patch % npx), py = (int)(patch / npx);
+  const double x = (px * P + k - g + 0.5) * hx, y = (py * P + j - g + 0.5) * hy;
+  const double pi = 3.14159265358979323846;
+  double rho = 1.0 + amp * sin(2 * pi * (x + y));
+  if (noise != 0.0) rho *= 1.0 + noise * (2.0 * fv_noise_u01(seed, (unsigned long long)gid) - 1.0);
+  double* q = luh + gid * D;
+  q[0] = rho;
+  q[1] = rho;
+  q[2] = rho;
+  q[3] = 0.0;
+  q[4] = 1.0 / (kGamma - 1) + rho;
+  for (int m = kV; m < D; m++) q[m] = 0.0;
+}
+
+}  // namespace exa
+
+struct exa_fv_patchgrid {
+  int scheme = 0, npx = 0, npy = 0;
+  exa_fv_desc_t desc{};
+  cudaStream_t st = nullptr;
+  double* luh = nullptr;
+  double* luh_new = nullptr;
+  unsigned long long* slots = nullptr;  // [0] dt, [1] time
+  size_t count = 0;
+  long npatches = 0;
+  bool primed = false;
+};
+
+namespace exa {
+__global__ void k_fv_slot_reset(unsigned long long* s) { s[0] = 0x7FF0000000000000ULL; }
+__global__ void k_fv_time_add(unsigned long long* s) {
+  double* time = (double*)(s + 1);
+  *time += __longlong_as_double((long long)s[0]);
+}
+}  // namespace exa
+
+static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
+  using namespace exa;
+  const exa_fv_desc_t& d = g->desc;
+  const int S = d.patch + 2 * d.ghost;
+  const long nex = 4L * d.ghost * d.patch * g->npatches;
+  k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy, g->luh);
+  // dt: the CFL rule (commons::stableTimeStepSize) minimised over every patch
+  k_fv_slot_reset<<<1, 1, 0, g->st>>>(g->slots);
+  FVArgs a = fv_args(&d);
+  const long cells = (long)d.patch * d.patch;
+  unsigned bx = (unsigned)((cells + 255) / 256);
+  if (bx > 64) bx = 64;
+  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
+  const long per = (long)S * S * kV;
+  constexpr long kChunk = 65535;  // grid y / z limit: patches per launch
+  for (long p0 = 0; p0 < g->npatches; p0 += kChunk) {
+    const unsigned np = (unsigned)(g->npatches - p0 < kChunk ? g->npatches - p0 : kChunk);
+    a.luh = g->luh + p0 * per;
+    if (planar) k_fv_stable_dt<true><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+    else k_fv_stable_dt<false><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+    count_launch();
+  }
+  cudaError_t e = cudaMemcpyAsync(g->luh_new, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToDevice, g->st);
+  if (e != cudaSuccess) return cuda_status(e, "fv patch copy");
+  a.dt_dev = (const double*)g->slots;
+  a.max_dt = nullptr;
+  if (g->scheme == 1) {
+    static bool attr[2] = {false, false};
+    if (!attr[planar]) {
+      e = planar ? cudaFuncSetAttribute(k_fv_muscl<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
+                 : cudaFuncSetAttribute(k_fv_muscl<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
+      attr[planar] = true;
+    }
+  }
+  for (long p0 = 0; p0 < g->npatches; p0 += kChunk) {
+    const unsigned np = (unsigned)(g->npatches - p0 < kChunk ? g->npatches - p0 : kChunk);
+    a.luh = g->luh + p0 * per;
+    a.out = g->luh_new + p0 * per;
+    dim3 grid((d.patch + FV_TX - 1) / FV_TX, (d.patch + FV_TY - 1) / FV_TY, np);
+    if (g->scheme == 0) {
+      if (planar) k_fv_godunov<true, false><<<grid, FV_NT, 0, g->st>>>(a);
+      else k_fv_godunov<false, false><<<grid, FV_NT, 0, g->st>>>(a);
+    } else {
+      if (planar) k_fv_muscl<true, false><<<grid, FV_NT, kMusclSmem, g->st>>>(a);
+      else k_fv_muscl<false, false><<<grid, FV_NT, kMusclSmem, g->st>>>(a);
+    }
+    count_launch();
+  }
+  k_fv_time_add<<<1, 1, 0, g->st>>>(g->slots);
+  count_launch(3);
+  std::swap(g->luh, g->luh_new);
+  return cuda_status(cudaGetLastError(), "fv patch grid step");
+}
+
+extern "C" {
+
+exa_status_t exa_fv_patchgrid_create(int scheme, int patch, int npx, int npy, double length, int pde,
+                                     exa_fv_patchgrid** out) {
+  if (!out) return set_error(EXA_EINVAL, "NULL argument");
+  if (scheme != 0 && scheme != 1) return set_error(EXA_EINVAL, "scheme must be 0 (Godunov) or 1 (MUSCL-Hancock)");
+  if (npx < 1 || npy < 1 || !(length > 0)) return set_error(EXA_EINVAL, "bad patch grid");
+  // desc.dx is the patch (cell) extent: length / number of patches
+  exa_fv_desc_t d{2, patch, scheme == 0 ? 1 : 2, kV, 0, pde, {length / npx, length / npy, 1.0}};
+  if (exa_status_t s = check_fv(&d, d.ghost)) return s;
+  if (patch < d.ghost) return set_error(EXA_EINVAL, "patch smaller than its ghost width");
+  exa_fv_patchgrid* g = new (std::nothrow) exa_fv_patchgrid;
+  if (!g) return set_error(EXA_ENOMEM, "host allocation");
+  g->scheme = scheme;
+  g->npx = npx;
+  g->npy = npy;
+  g->desc = d;
+  g->npatches = (long)npx * npy;
+  const size_t S = (size_t)patch + 2 * d.ghost;
+  g->count = S * S * kV * g->npatches;
+  cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&g->luh, g->count * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&g->luh_new, g->count * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&g->slots, 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->slots, 0, 2 * sizeof(unsigned long long), g->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->luh, 0, g->count * sizeof(double), g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) {
+    exa_fv_patchgrid_destroy(g);
+    return cuda_status(e, "fv patch grid allocation");
+  }
+  *out = g;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_patchgrid_destroy(exa_fv_patchgrid* g) {
+  if (!g) return EXA_OK;
+  if (g->st) cudaStreamSynchronize(g->st);
+  cudaFree(g->luh);
+  cudaFree(g->luh_new);
+  cudaFree(g->slots);
+  if (g->st) cudaStreamDestroy(g->st);
+  delete g;
+  return EXA_OK;
+}
+
+size_t exa_fv_patchgrid_state_size(const exa_fv_patchgrid* g) { return g ? g->count : 0; }
+
+exa_status_t exa_fv_patchgrid_init(exa_fv_patchgrid* g, double amp, uint64_t seed, double noise) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  const exa_fv_desc_t& d = g->desc;
+  const long n = (long)(d.patch + 2 * d.ghost) * (d.patch + 2 * d.ghost) * g->npatches;
+  k_fv_patch_ic<<<(unsigned)((n + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy,
+                                                               d.dx[0] / d.patch, d.dx[1] / d.patch, amp,
+                                                               seed, noise, g->luh);
+  count_launch();
+  cudaError_t e = cudaMemsetAsync(g->slots, 0, 2 * sizeof(unsigned long long), g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "fv patch grid init");
+}
+
+exa_status_t exa_fv_patchgrid_set_state(exa_fv_patchgrid* g, const double* host) {
+  if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
+  cudaError_t e = cudaMemcpyAsync(g->luh, host, g->count * sizeof(double), cudaMemcpyHostToDevice, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "fv patch grid set_state");
+}
+
+exa_status_t exa_fv_patchgrid_get_state(exa_fv_patchgrid* g, double* host) {
+  if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
+  cudaError_t e = cudaMemcpyAsync(host, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "fv patch grid get_state");
+}
+
+exa_status_t exa_fv_patchgrid_step(exa_fv_patchgrid* g, int nsteps) {
+  if (!g || nsteps < 0) return set_error(EXA_EINVAL, "bad argument");
+  for (int i = 0; i < nsteps; i++)
+    if (exa_status_t s = fv_patchgrid_step_one(g)) return s;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_patchgrid_status(exa_fv_patchgrid* g, double* time, double* last_dt) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  unsigned long long h[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(h, g->slots, 16, cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) return cuda_status(e, "fv patch grid status");
+  double t, dt;
+  memcpy(&dt, &h[0], 8);
+  memcpy(&t, &h[1], 8);
+  if (time) *time = t;
+  if (last_dt) *last_dt = dt;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_patchgrid_stream(exa_fv_patchgrid* g, void** stream) {
+  if (!g || !stream) return set_error(EXA_EINVAL, "NULL argument");
+  *stream = g->st;
   return EXA_OK;
 }
 

@@ -113,3 +113,62 @@ class FVGrid:
             self.destroy()
         except Exception:
             pass
+
+
+class FVPatchGrid:
+    """Device-resident periodic grid of npx x npy FV patches (the reference's
+    FV layout: per-cell patches with ghost layers exchanged every step)."""
+
+    def __init__(self, scheme, patch, npx, npy, length=1.0, pde=_lib.PDE_EULER):
+        h = C.c_void_p()
+        call('exa_fv_patchgrid_create', int(scheme), int(patch), int(npx), int(npy), float(length), int(pde),
+             C.byref(h))
+        self.h = h
+        self.scheme, self.patch, self.npx, self.npy = scheme, patch, npx, npy
+        self.ghost = 1 if scheme == GODUNOV else 2
+        self.side = patch + 2 * self.ghost
+        self.state_size = int(_lib.lib().exa_fv_patchgrid_state_size(h))
+        self.ncells = patch * patch * npx * npy
+
+    def init(self, amp=0.2, seed=1, noise=0.0):
+        call('exa_fv_patchgrid_init', self.h, float(amp), int(seed), float(noise))
+
+    def set_state(self, q):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        assert q.size == self.state_size
+        call('exa_fv_patchgrid_set_state', self.h, q.ctypes.data)
+
+    def get_state(self):
+        out = np.empty(self.state_size)
+        call('exa_fv_patchgrid_get_state', self.h, out.ctypes.data)
+        return out
+
+    def interiors(self, q=None):
+        """[npy][npx][patch][patch][5] view of the patch interiors."""
+        q = self.get_state() if q is None else q
+        g, P, S = self.ghost, self.patch, self.side
+        return q.reshape(self.npy, self.npx, S, S, 5)[:, :, g:g + P, g:g + P]
+
+    def step(self, nsteps=1):
+        call('exa_fv_patchgrid_step', self.h, int(nsteps))
+
+    def status(self):
+        t, dt = C.c_double(), C.c_double()
+        call('exa_fv_patchgrid_status', self.h, C.byref(t), C.byref(dt))
+        return dict(time=t.value, last_dt=dt.value)
+
+    def stream(self):
+        s = C.c_void_p()
+        call('exa_fv_patchgrid_stream', self.h, C.byref(s))
+        return s
+
+    def destroy(self):
+        if self.h:
+            call('exa_fv_patchgrid_destroy', self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -498,6 +498,33 @@ exa_status_t exa_fv_grid_status(exa_fv_grid* g, double* time, double* dt_next);
 exa_status_t exa_fv_grid_stream(exa_fv_grid* g, void** stream);
 exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev);
 
+/* ---- Device-resident grid of FV patches (the reference's FV layout) ----
+ * npx x npy periodic patches of patch x patch subcells (+ ghost layers: 1
+ * Godunov, 2 MUSCL-Hancock) over [0,length)^2, stored back to back (x
+ * fastest) like the batched FV entry points.  One step: face ghost layers
+ * copied from the neighbouring patches' boundary layers (ghostLayerFilling,
+ * kernels/finitevolumes/commons/c/commons.cpph:337-405, per face as in
+ * FiniteVolumesSolver::mergeNeighbours, FiniteVolumesSolver.cpp:659-686),
+ * dt = the CFL rule minimised over every patch, then each patch's
+ * godunov/musclhancock::solutionUpdate with that dt (the reference's
+ * in-place semantics: luh_new = luh, then updated).  The patches do not
+ * reproduce one big patch exactly: MUSCL-Hancock does not half-step-evolve
+ * ghost cells, so faces between patches see unevolved neighbour states, as
+ * in the reference.  Initial condition as exa_fv_grid_init, on the whole
+ * domain. */
+typedef struct exa_fv_patchgrid exa_fv_patchgrid;
+exa_status_t exa_fv_patchgrid_create(int scheme, int patch, int npx, int npy, double length, int pde,
+                                     exa_fv_patchgrid** out);
+exa_status_t exa_fv_patchgrid_destroy(exa_fv_patchgrid* g);
+size_t exa_fv_patchgrid_state_size(const exa_fv_patchgrid* g);
+exa_status_t exa_fv_patchgrid_init(exa_fv_patchgrid* g, double amp, uint64_t seed, double noise);
+exa_status_t exa_fv_patchgrid_set_state(exa_fv_patchgrid* g, const double* host);
+exa_status_t exa_fv_patchgrid_get_state(exa_fv_patchgrid* g, double* host);
+exa_status_t exa_fv_patchgrid_step(exa_fv_patchgrid* g, int nsteps);
+/* simulated time and the dt of the last step */
+exa_status_t exa_fv_patchgrid_status(exa_fv_patchgrid* g, double* time, double* last_dt);
+exa_status_t exa_fv_patchgrid_stream(exa_fv_patchgrid* g, void** stream);
+
 /* rusanov (riemannsolvers/c/rusanov.cpph:24-83), host drop-in, returns s_max */
 exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL,
                             double* fR, const double* qL, const double* qR,

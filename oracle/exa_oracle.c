@@ -809,6 +809,48 @@ void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,
   }
 }
 
+/* Grid of npx x npy periodic patches (back to back, x fastest), one step:
+ * face ghost layers from the neighbouring patches' boundary layers
+ * (ghostLayerFilling, kernels/finitevolumes/commons/c/commons.cpph:337-405),
+ * dt = min over patches of the CFL rule, then every patch's solutionUpdate
+ * with luh_new = luh beforehand (FiniteVolumesSolver.cpp:529-531).
+ * dx = the patch extent.  Returns the dt used. */
+double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
+                                double* luh, const double* dx) {
+  const int g = scheme == 0 ? 1 : 2, V = 5, S = P + 2 * g;
+  const long per = (long)S * S * V, np = (long)npx * npy;
+  long p;
+  for (p = 0; p < np; p++) {
+    const int px = (int)(p % npx), py = (int)(p / npx);
+    double* u = luh + p * per;
+    const double* L = luh + ((long)py * npx + (px + npx - 1) % npx) * per;
+    const double* R = luh + ((long)py * npx + (px + 1) % npx) * per;
+    const double* Bm = luh + ((long)((py + npy - 1) % npy) * npx + px) * per;
+    const double* T = luh + ((long)((py + 1) % npy) * npx + px) * per;
+    int i, k;
+    for (i = g; i < g + P; i++)
+      for (k = 0; k < g; k++) {
+        memcpy(u + ((long)i * S + k) * V, L + ((long)i * S + P + k) * V, sizeof(double) * V);
+        memcpy(u + ((long)i * S + g + P + k) * V, R + ((long)i * S + g + k) * V, sizeof(double) * V);
+        memcpy(u + ((long)k * S + i) * V, Bm + ((long)(P + k) * S + i) * V, sizeof(double) * V);
+        memcpy(u + ((long)(g + P + k) * S + i) * V, T + ((long)(g + k) * S + i) * V, sizeof(double) * V);
+      }
+  }
+  double dt = DBL_MAX;
+  for (p = 0; p < np; p++) {
+    const double d = orc_fv_stable_dt_2d(P, g, V, 0, planar, luh + p * per, dx, 0.9);
+    if (d < dt) dt = d;
+  }
+  double* old = (double*)malloc(sizeof(double) * per);
+  for (p = 0; p < np; p++) {
+    memcpy(old, luh + p * per, sizeof(double) * per);
+    if (scheme == 0) orc_fv_godunov_2d(P, g, V, 0, planar, luh + p * per, old, dx, dt);
+    else orc_fv_musclhancock_2d(P, g, V, 0, planar, luh + p * per, old, dx, dt);
+  }
+  free(old);
+  return dt;
+}
+
 /* ------------------------------------------------------------------ */
 /* Counter-based noise: splitmix64 of (seed, index). */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx) {

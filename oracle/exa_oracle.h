@@ -124,6 +124,9 @@ double orc_fv_patch_step_2d(int scheme, int patch, int planar, double* luh,
                             double* max_admissible_dt);
 
 /* counter-based noise shared with the device IC kernel */
+/* one step of a periodic npx x npy grid of FV patches (dx = patch extent) */
+double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
+                                double* luh, const double* dx);
 double orc_noise_u01(unsigned long long seed, unsigned long long idx);
 
 #ifdef __cplusplus

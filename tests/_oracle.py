@@ -64,6 +64,8 @@ def lib():
     L.orc_aderdg_sample_step.argtypes = [i, i, i, C.c_long, _dp, _dp, d, i]
     L.orc_aderdg_slab_predict.argtypes = [i, i, i, _ip, _dp, _dp, d, _dp, _dp, _dp, _dp, _dp]
     L.orc_aderdg_slab_correct.argtypes = [i, i, i, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d]
+    L.orc_fv_patchgrid_step_2d.restype = d
+    L.orc_fv_patchgrid_step_2d.argtypes = [i, i, i, i, i, _dp, _dp]
     L.orc_noise_u01.restype = d
     L.orc_noise_u01.argtypes = [C.c_ulonglong, C.c_ulonglong]
     _lib = L

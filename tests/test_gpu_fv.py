@@ -163,3 +163,24 @@ def test_fv_grid_noise_and_restart():
     grid.step(3)
     assert np.array_equal(grid.interior(), a)
     grid.destroy()
+
+
+@pytest.mark.parametrize('scheme', [0, 1])
+@pytest.mark.parametrize('P,npx,npy', [(10, 3, 4), (7, 2, 2), (16, 1, 3)])
+def test_fv_patch_grid_vs_oracle(scheme, P, npx, npy):
+    """Grid of patches with ghost exchange (the EulerFV layout, patch 10)
+    against the oracle's per-patch ghostLayerFilling + step, per step."""
+    g = E.FVPatchGrid(scheme, P, npx, npy)
+    g.init(amp=0.2, seed=3, noise=1e-3)
+    u = g.get_state()
+    dx = np.array([1.0 / npx, 1.0 / npy])
+    t = 0.0
+    for s in range(5):
+        g.step(1)
+        t += O.lib().orc_fv_patchgrid_step_2d(scheme, P, npx, npy, 0, u, dx)
+        got = g.get_state()
+        a, b = g.interiors(got), g.interiors(u)
+        assert rel(a, b) < 1e-13, (s, rel(a, b))
+        u = got.copy()  # next step from the GPU state
+    assert abs(g.status()['time'] - t) <= 1e-12 * t
+    g.destroy()
