@@ -1017,16 +1017,136 @@ __global__ void k_fv_patch_ic(int P, int g, int D, int npx, int npy, double hx, 
 
 }  // namespace exa
 
+namespace exa {
+// Small patches (patch <= 16, the reference's per-cell FV patches): one CTA
+// of 128 threads per patch.  The whole patch with its ghosts (contiguous in
+// memory) is staged in shared memory, MUSCL-Hancock's ring cells compute
+// their evolved face extrapolations, and every interior cell evaluates its
+// own four face fluxes, applies them in the reference's order and writes
+// only the interior of the output; the new state's CFL dt is reduced in the
+// same pass.  Same arithmetic per cell as the tile kernels.
+constexpr int FVS_NT = 128;
+constexpr int kFvSmallMax = 16;
+
+template <bool PLANAR, int SCHEME>
+__global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
+  constexpr int V = kV;
+  extern __shared__ double sm[];
+  const int P = a.P, g = a.g, S = a.S, D = V + a.npar, pb = g, pe = g + P;
+  const int R = P + 2;  // ring side (MUSCL)
+  double* su = sm;       // [S][S][V]
+  double* wLx = su + S * S * V;
+  double* wRx = wLx + R * R * V;
+  double* wLy = wRx + R * R * V;
+  double* wRy = wLy + R * R * V;
+  const long patch = blockIdx.x;
+  const double* luh = a.luh + patch * (long)S * S * D;
+  double* out = a.out + patch * (long)S * S * D;
+  const int tid = threadIdx.x;
+  const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
+  for (int i = tid; i < S * S * V; i += FVS_NT) su[i] = luh[i];  // D == V: no parameters here
+  __syncthreads();
+  if (SCHEME == 1) {
+    for (int i = tid; i < R * R; i += FVS_NT) {
+      const int j = pb - 1 + i / R, k = pb - 1 + i % R;
+      const double* U = &su[(j * S + k) * V];
+      const bool has_x = j >= pb && j < pe;
+      const bool has_y = k >= pb && k < pe;
+      const bool interior = has_x && has_y;
+      double lx[V], rx[V], ly[V], ry[V];
+#pragma unroll
+      for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
+      if (has_x) {
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+          lx[m] = U[m] - 0.5 * hx * sl;
+          rx[m] = U[m] + 0.5 * hx * sl;
+        }
+      }
+      if (has_y) {
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          const double sl = minmod(U[S * V + m] - U[m], U[m] - U[-S * V + m]) / hy;
+          ly[m] = U[m] - 0.5 * hy * sl;
+          ry[m] = U[m] + 0.5 * hy * sl;
+        }
+      }
+      if (interior) {
+        double Qt[V];
+        double F[2][V];
+#pragma unroll
+        for (int m = 0; m < V; m++) Qt[m] = 0.0;
+        euler_flux<2, PLANAR>(lx, F);
+#pragma unroll
+        for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+        euler_flux<2, PLANAR>(rx, F);
+#pragma unroll
+        for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+        euler_flux<2, PLANAR>(ly, F);
+#pragma unroll
+        for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+        euler_flux<2, PLANAR>(ry, F);
+#pragma unroll
+        for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          lx[m] += 0.5 * dt * Qt[m];
+          rx[m] += 0.5 * dt * Qt[m];
+          ly[m] += 0.5 * dt * Qt[m];
+          ry[m] += 0.5 * dt * Qt[m];
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        wLx[i * V + m] = lx[m];
+        wRx[i * V + m] = rx[m];
+        wLy[i * V + m] = ly[m];
+        wRy[i * V + m] = ry[m];
+      }
+    }
+    __syncthreads();
+  }
+  const double cx = dt / hx, cy = dt / hy;
+  double dtn = DBL_MAX;
+  for (int i = tid; i < P * P; i += FVS_NT) {
+    const int j = pb + i / P, k = pb + i % P;
+    const double* U = &su[(j * S + k) * V];
+    double fxl[V], fxr[V], fyb[V], fyt[V];
+    if (SCHEME == 0) {
+      rusanov<PLANAR>(U - V, U, 0, fxl);
+      rusanov<PLANAR>(U, U + V, 0, fxr);
+      rusanov<PLANAR>(U - S * V, U, 1, fyb);
+      rusanov<PLANAR>(U, U + S * V, 1, fyt);
+    } else {
+      const int ic = (j - pb + 1) * R + (k - pb + 1);
+      rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
+      rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
+      rusanov<PLANAR>(&wRy[(ic - R) * V], &wLy[ic * V], 1, fyb);
+      rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + R) * V], 1, fyt);
+    }
+    fv_update_store_dt<PLANAR>(a, out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
+  }
+  for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
+  if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
+}
+
+inline size_t fv_small_smem(int P, int g, int scheme) {
+  const size_t S = P + 2 * g, R = P + 2;
+  return sizeof(double) * (S * S * kV + (scheme == 1 ? 4 * R * R * kV : 0));
+}
+}  // namespace exa
+
 struct exa_fv_patchgrid {
   int scheme = 0, npx = 0, npy = 0;
   exa_fv_desc_t desc{};
   cudaStream_t st = nullptr;
   double* luh = nullptr;
   double* luh_new = nullptr;
-  unsigned long long* slots = nullptr;  // [0] dt, [1] time
+  unsigned long long* slots = nullptr;  // [0] dt, [1] time, [2] next dt, [3] last dt
   size_t count = 0;
   long npatches = 0;
-  bool primed = false;
+  bool primed = false;  // slot [0] holds the CFL dt of the current state (small-patch path)
 };
 
 namespace exa {
@@ -1034,6 +1154,15 @@ __global__ void k_fv_slot_reset(unsigned long long* s) { s[0] = 0x7FF00000000000
 __global__ void k_fv_time_add(unsigned long long* s) {
   double* time = (double*)(s + 1);
   *time += __longlong_as_double((long long)s[0]);
+  s[3] = s[0];
+}
+// fused small-patch steps: time += dt, last <- dt, dt <- next, next <- +inf
+__global__ void k_fv_patch_commit(unsigned long long* s) {
+  double* time = (double*)(s + 1);
+  *time += __longlong_as_double((long long)s[0]);
+  s[3] = s[0];
+  s[0] = s[2];
+  s[2] = 0x7FF0000000000000ULL;
 }
 }  // namespace exa
 
@@ -1043,13 +1172,46 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
   const int S = d.patch + 2 * d.ghost;
   const long nex = 4L * d.ghost * d.patch * g->npatches;
   k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy, g->luh);
+  count_launch();
+  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
+  if (d.patch <= kFvSmallMax && d.npar == 0) {
+    // small patches: one fused launch per step (dt of this state from the
+    // previous update, or primed once), the commit rotates the dt slots
+    FVArgs a = fv_args(&d);
+    if (!g->primed) {
+      k_fv_slots_init<<<1, 1, 0, g->st>>>(g->slots);
+      a.luh = g->luh;
+      const long per0 = (long)S * S * kV;
+      for (long p0 = 0; p0 < g->npatches; p0 += 65535) {
+        const unsigned np = (unsigned)(g->npatches - p0 < 65535 ? g->npatches - p0 : 65535);
+        a.luh = g->luh + p0 * per0;
+        if (planar) k_fv_stable_dt<true><<<dim3(1, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+        else k_fv_stable_dt<false><<<dim3(1, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+        count_launch();
+      }
+      g->primed = true;
+    }
+    a.luh = g->luh;
+    a.out = g->luh_new;
+    a.dt_dev = (const double*)g->slots;
+    a.next_dt = g->slots + 2;
+    const size_t smem = fv_small_smem(d.patch, d.ghost, g->scheme);
+    auto kern = g->scheme == 0 ? (planar ? k_fv_patch_small<true, 0> : k_fv_patch_small<false, 0>)
+                               : (planar ? k_fv_patch_small<true, 1> : k_fv_patch_small<false, 1>);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "small patch attribute");
+    kern<<<(unsigned)g->npatches, FVS_NT, smem, g->st>>>(a);
+    k_fv_patch_commit<<<1, 1, 0, g->st>>>(g->slots);
+    count_launch(2);
+    std::swap(g->luh, g->luh_new);
+    return cuda_status(cudaGetLastError(), "fv patch grid step");
+  }
   // dt: the CFL rule (commons::stableTimeStepSize) minimised over every patch
   k_fv_slot_reset<<<1, 1, 0, g->st>>>(g->slots);
   FVArgs a = fv_args(&d);
   const long cells = (long)d.patch * d.patch;
   unsigned bx = (unsigned)((cells + 255) / 256);
   if (bx > 64) bx = 64;
-  const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
   const long per = (long)S * S * kV;
   constexpr long kChunk = 65535;  // grid y / z limit: patches per launch
   for (long p0 = 0; p0 < g->npatches; p0 += kChunk) {
@@ -1087,7 +1249,7 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
     count_launch();
   }
   k_fv_time_add<<<1, 1, 0, g->st>>>(g->slots);
-  count_launch(3);
+  count_launch(2);
   std::swap(g->luh, g->luh_new);
   return cuda_status(cudaGetLastError(), "fv patch grid step");
 }
@@ -1115,8 +1277,8 @@ exa_status_t exa_fv_patchgrid_create(int scheme, int patch, int npx, int npy, do
   cudaError_t e = cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&g->luh, g->count * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&g->luh_new, g->count * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&g->slots, 2 * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMemsetAsync(g->slots, 0, 2 * sizeof(unsigned long long), g->st);
+  if (e == cudaSuccess) e = cudaMalloc(&g->slots, 4 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->slots, 0, 4 * sizeof(unsigned long long), g->st);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->luh, 0, g->count * sizeof(double), g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   if (e != cudaSuccess) {
@@ -1148,7 +1310,8 @@ exa_status_t exa_fv_patchgrid_init(exa_fv_patchgrid* g, double amp, uint64_t see
                                                                d.dx[0] / d.patch, d.dx[1] / d.patch, amp,
                                                                seed, noise, g->luh);
   count_launch();
-  cudaError_t e = cudaMemsetAsync(g->slots, 0, 2 * sizeof(unsigned long long), g->st);
+  g->primed = false;
+  cudaError_t e = cudaMemsetAsync(g->slots, 0, 4 * sizeof(unsigned long long), g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   return cuda_status(e, "fv patch grid init");
 }
@@ -1157,6 +1320,7 @@ exa_status_t exa_fv_patchgrid_set_state(exa_fv_patchgrid* g, const double* host)
   if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
   cudaError_t e = cudaMemcpyAsync(g->luh, host, g->count * sizeof(double), cudaMemcpyHostToDevice, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  g->primed = false;
   return cuda_status(e, "fv patch grid set_state");
 }
 
@@ -1176,12 +1340,12 @@ exa_status_t exa_fv_patchgrid_step(exa_fv_patchgrid* g, int nsteps) {
 
 exa_status_t exa_fv_patchgrid_status(exa_fv_patchgrid* g, double* time, double* last_dt) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
-  unsigned long long h[2] = {0, 0};
-  cudaError_t e = cudaMemcpyAsync(h, g->slots, 16, cudaMemcpyDeviceToHost, g->st);
+  unsigned long long h[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(h, g->slots, 32, cudaMemcpyDeviceToHost, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   if (e != cudaSuccess) return cuda_status(e, "fv patch grid status");
   double t, dt;
-  memcpy(&dt, &h[0], 8);
+  memcpy(&dt, &h[3], 8);
   memcpy(&t, &h[1], 8);
   if (time) *time = t;
   if (last_dt) *last_dt = dt;

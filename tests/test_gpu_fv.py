@@ -166,7 +166,7 @@ def test_fv_grid_noise_and_restart():
 
 
 @pytest.mark.parametrize('scheme', [0, 1])
-@pytest.mark.parametrize('P,npx,npy', [(10, 3, 4), (7, 2, 2), (16, 1, 3)])
+@pytest.mark.parametrize('P,npx,npy', [(10, 3, 4), (7, 2, 2), (16, 1, 3), (20, 2, 1)])
 def test_fv_patch_grid_vs_oracle(scheme, P, npx, npy):
     """Grid of patches with ghost exchange (the EulerFV layout, patch 10)
     against the oracle's per-patch ghostLayerFilling + step, per step."""
