@@ -146,6 +146,8 @@ SIGNATURES = {
     'exa_fv_patchgrid_step': (i32, [vp, i32]),
     'exa_fv_patchgrid_status': (i32, [vp, C.POINTER(f64), C.POINTER(f64)]),
     'exa_fv_patchgrid_stream': (i32, [vp, C.POINTER(vp)]),
+    'exa_aderdg_amr_prolongation': (i32, [i32, i32, i32, i64, vp, vp, vp, i32, vp, vp]),
+    'exa_aderdg_amr_restriction': (i32, [i32, i32, i32, i64, vp, vp, i32, vp, vp]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),

@@ -250,3 +250,17 @@ class ADERDGGrid:
             self.destroy()
         except Exception:
             pass
+
+
+def amr_prolongation(k, order, count, fine, coarse, level_delta, index, coarse_item=None, nvar=5,
+                     stream=None):
+    """volume/faceUnknownsProlongation for `count` items (DeviceBuffer
+    arguments; index: int32 [count][3]; see exa_aderdg_amr_prolongation)."""
+    call('exa_aderdg_amr_prolongation', int(k), int(order), int(nvar), int(count), fine.ptr, coarse.ptr,
+         coarse_item.ptr if coarse_item is not None else None, int(level_delta), index.ptr, stream)
+
+
+def amr_restriction(k, order, count, coarse, fine, level_delta, index, nvar=5, stream=None):
+    """volume/faceUnknownsRestriction: coarse[i] += R(fine[i])."""
+    call('exa_aderdg_amr_restriction', int(k), int(order), int(nvar), int(count), coarse.ptr, fine.ptr,
+         int(level_delta), index.ptr, stream)

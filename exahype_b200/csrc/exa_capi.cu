@@ -51,6 +51,7 @@ exa_status_t ensure_tables() {
   if (g_tables_done[dev & 255]) return EXA_OK;
   exa_status_t s;
   if ((s = upload_tables_predictor())) return s;
+  if ((s = upload_tables_amr())) return s;
   if ((s = upload_tables_predictor_mixed())) return s;
   if ((s = upload_tables_ensemble())) return s;
   if ((s = upload_tables_faces())) return s;

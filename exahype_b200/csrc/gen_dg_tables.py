@@ -101,6 +101,10 @@ def derive(order):
         'dudx': [[round13(dudx[l][k]) for k in range(b)] for l in range(b)],
         'ik1': [[round13(ik1[k, l]) for l in range(b)] for k in range(b)],
         'f0': [float(lagrange(xs, k, 0)) for k in range(b)],
+        # fine-grid projector (3:1 refinement): fgp[s][n][m] = coarse basis
+        # polynomial n at node m of subinterval s, phi_n((s + x_m) / 3)
+        'fgp': [[[round13(lagrange(xs, n, (sub + xs[m]) / 3)) for m in range(b)] for n in range(b)]
+                for sub in range(3)],
         'flcoeff': [float(lagrange(xs, k, 0)) for k in range(b)],
         'frcoeff': [float(lagrange(xs, k, 1)) for k in range(b)],
     }
@@ -141,6 +145,18 @@ def write_header(path):
                 out.append('    {' + ', '.join(_fmt(v) for v in row) + '},\n')
             out.append('  },\n')
         out.append('};\n')
+    out.append('EXA_TABLE_QUAL double exa_fgp[%d][3][%d][%d] = {\n' % (D, D, D))
+    for n in range(D):
+        out.append('  {\n')
+        for sub in range(3):
+            out.append('    {\n')
+            m = tabs[n]['fgp'][sub]
+            for k in range(D):
+                row = (m[k] if k < len(m) else []) + [0.0] * (D - (len(m[k]) if k < len(m) else 0))
+                out.append('      {' + ', '.join(_fmt(v) for v in row) + '},\n')
+            out.append('    },\n')
+        out.append('  },\n')
+    out.append('};\n')
     # CFL safety factors for ADER-DG of order N (reference
     # kernels/aderdg/generic/c/3d/stableTimeStepSize.cpph:33-34)
     out.append('EXA_TABLE_QUAL double exa_pnpm[10] = {1.0, 0.33, 0.17, 0.1, 0.069, '

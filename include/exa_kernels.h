@@ -319,6 +319,26 @@ exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time,
                                     uint64_t* nonconverged, int* nan_flag);
 long exa_aderdg_grid_ncells(const exa_aderdg_grid* g);
 
+/* ---- AMR transfer operators ----
+ * volume/faceUnknownsProlongation and ...Restriction
+ * (kernels/aderdg/generic/c/{2d,3d}/amrRoutines.cpph, declared in
+ * kernels/aderdg/generic/Kernels.h:169-205) for `count` items on the device:
+ * item i moves nodal data of k node dimensions (k = dim for cell volumes
+ * luh, dim-1 for face arrays lQhbnd / lFhbnd), [node][var] with nvar values
+ * per node, between a coarse cell (face) and its descendant level_delta
+ * levels down (3:1 refinement per level); index[3 i + d] in
+ * [0, 3^level_delta) is the descendant's position along direction d (the
+ * reference's subcellIndex / subfaceIndex).
+ * prolongation: fine[i] = P(coarse[coarse_item ? coarse_item[i] : i]);
+ * restriction:  coarse[i] += R(fine[i]) (the reference adds each child's
+ * contribution into the parent; outputs of different items must not
+ * alias).  Orders 1..6; arrays of B^k nvar doubles per item, back to back. */
+exa_status_t exa_aderdg_amr_prolongation(int k, int order, int nvar, long count, double* fine,
+                                         const double* coarse, const long* coarse_item, int level_delta,
+                                         const int* index, void* stream);
+exa_status_t exa_aderdg_amr_restriction(int k, int order, int nvar, long count, double* coarse,
+                                        const double* fine, int level_delta, const int* index, void* stream);
+
 /* ---- Slab decomposition of one grid over several GPUs ----
  * The reference distributes its spacetree over MPI ranks inside Peano: per
  * remote face, ADERDGSolver::sendDataToNeighbour (exahype/solvers/

@@ -851,6 +851,115 @@ double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
   return dt;
 }
 
+/* ---- AMR transfer operators (kernels/aderdg/generic/c/{2d,3d}/amrRoutines.cpph) ----
+ * k-dimensional nodal arrays [n_{k-1}]...[n_0][var] (node index 0 fastest),
+ * 3:1 refinement per level with the fine-grid projector
+ * P[s][n][m] = phi_n((s + x_m) / 3) (DGMatrices.cpp fineGridProjector1d). */
+static long ipow_l(long b, int e) { long r = 1; while (e-- > 0) r *= b; return r; }
+
+/* single level: out[m] (+)= sum_n in[n] * prod_d P[s_d][n_d][m_d] */
+static void amr_prolong1(int k, int order, int nvar, double* out, const double* in, const int* s) {
+  const int B = order + 1;
+  const long nn = ipow_l(B, k);
+  long m, n;
+  int v, d;
+  for (m = 0; m < nn; m++)
+    for (v = 0; v < nvar; v++) {
+      double acc = 0.0;
+      /* loop order of the reference: outer node index slowest */
+      for (n = 0; n < nn; n++) {
+        long mm = m, nr = n;
+        double t = in[n * nvar + v];
+        for (d = 0; d < k; d++) {
+          t *= exa_fgp[order][s[d]][nr % B][mm % B];
+          mm /= B;
+          nr /= B;
+        }
+        acc += t;
+      }
+      out[m * nvar + v] += acc;
+    }
+}
+
+/* single level: out[m] (+)= sum_n (prod w[n_d]) (prod P[s_d][m_d][n_d]) in[n]
+ *                        / prod w[m_d] / 3^k */
+static void amr_restrict1(int k, int order, int nvar, double* out, const double* in, const int* s) {
+  const int B = order + 1;
+  const long nn = ipow_l(B, k);
+  const double* w = exa_gl_weights[order];
+  long m, n;
+  int v, d;
+  for (m = 0; m < nn; m++)
+    for (v = 0; v < nvar; v++) {
+      double acc = 0.0;
+      for (n = 0; n < nn; n++) {
+        long mm, nr = n;
+        double t = 1.0;
+        for (d = 0; d < k; d++) { t *= w[nr % B]; nr /= B; }
+        mm = m; nr = n;
+        for (d = 0; d < k; d++) {
+          t *= exa_fgp[order][s[d]][mm % B][nr % B];
+          mm /= B;
+          nr /= B;
+        }
+        t *= in[n * nvar + v];
+        mm = m;
+        for (d = 0; d < k; d++) { t /= w[mm % B]; mm /= B; }
+        t /= (double)ipow_l(3, k);
+        acc += t;
+      }
+      out[m * nvar + v] += acc;
+    }
+}
+
+void orc_amr_prolongation(int k, int order, int nvar, double* fine, const double* coarse,
+                          int level_delta, const int* index) {
+  const int B = order + 1;
+  const long nn = ipow_l(B, k) * nvar;
+  double* a = (double*)malloc(sizeof(double) * nn);
+  double* b = (double*)malloc(sizeof(double) * nn);
+  int cur[3] = {0, 0, 0}, sub[3], d, l;
+  memcpy(a, coarse, sizeof(double) * nn);
+  for (d = 0; d < k; d++) cur[d] = index[d];
+  for (l = 1; l <= level_delta; l++) {
+    const long sig = ipow_l(3, level_delta - l);
+    for (d = 0; d < k; d++) {
+      sub[d] = (int)(cur[d] / sig);
+      cur[d] = (int)(cur[d] % sig);
+    }
+    memset(b, 0, sizeof(double) * nn);
+    amr_prolong1(k, order, nvar, b, a, sub);
+    { double* t = a; a = b; b = t; }
+  }
+  memcpy(fine, a, sizeof(double) * nn);
+  free(a);
+  free(b);
+}
+
+void orc_amr_restriction(int k, int order, int nvar, double* coarse, const double* fine,
+                         int level_delta, const int* index) {
+  const int B = order + 1;
+  const long nn = ipow_l(B, k) * nvar;
+  double* a = (double*)malloc(sizeof(double) * nn);
+  double* b = (double*)malloc(sizeof(double) * nn);
+  int cur[3] = {0, 0, 0}, sub[3], d, l;
+  long i;
+  memcpy(a, fine, sizeof(double) * nn);
+  for (d = 0; d < k; d++) cur[d] = index[d];
+  for (l = 1; l <= level_delta; l++) {
+    for (d = 0; d < k; d++) {
+      sub[d] = cur[d] % 3;
+      cur[d] /= 3;
+    }
+    memset(b, 0, sizeof(double) * nn);
+    amr_restrict1(k, order, nvar, b, a, sub);
+    { double* t = a; a = b; b = t; }
+  }
+  for (i = 0; i < nn; i++) coarse[i] += a[i];
+  free(a);
+  free(b);
+}
+
 /* ------------------------------------------------------------------ */
 /* Counter-based noise: splitmix64 of (seed, index). */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx) {

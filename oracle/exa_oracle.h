@@ -124,6 +124,17 @@ double orc_fv_patch_step_2d(int scheme, int patch, int planar, double* luh,
                             double* max_admissible_dt);
 
 /* counter-based noise shared with the device IC kernel */
+/* AMR transfer between a coarse cell (or face) and its fine descendant
+ * `level_delta` levels down (3:1 per level), for k-dimensional nodal arrays
+ * [node][var] (k = dim for cell volumes, dim-1 for faces); index[d] in
+ * [0, 3^level_delta) = the descendant's position in direction d.
+ * Prolongation overwrites `fine`; restriction ADDS the fine contribution
+ * to `coarse` (the reference accumulates the 3^(k level_delta) children).
+ * volume/faceUnknownsProlongation / ...Restriction, amrRoutines.cpph. */
+void orc_amr_prolongation(int k, int order, int nvar, double* fine, const double* coarse,
+                          int level_delta, const int* index);
+void orc_amr_restriction(int k, int order, int nvar, double* coarse, const double* fine,
+                         int level_delta, const int* index);
 /* one step of a periodic npx x npy grid of FV patches (dx = patch extent) */
 double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
                                 double* luh, const double* dx);

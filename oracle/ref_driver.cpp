@@ -378,4 +378,28 @@ double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double 
 }
 #endif
 
+/* AMR transfer operators of the reference (amrRoutines.cpph), nVar = 5,
+ * nPar = 0, from level 0 to level `level_delta`.  what: 0 volume
+ * prolongation (out_q = luhFine), 1 volume restriction (out_q += ...),
+ * 2 face prolongation (out_q/out_f = lQhbnd/lFhbnd of the fine face),
+ * 3 face restriction (accumulates). */
+int ref_amr(int what, int order, double* out_q, double* out_f, const double* in_q, const double* in_f,
+            int level_delta, const int* index) {
+  tarch::la::Vector<DIMENSIONS, int> vi;
+  tarch::la::Vector<DIMENSIONS - 1, int> fi;
+  for (int d = 0; d < DIMENSIONS; d++) vi[d] = index[d];
+  for (int d = 0; d < DIMENSIONS - 1; d++) fi[d] = index[d];
+  namespace K = kernels::aderdg::generic::c;
+#define CASE(N)                                                                                     \
+  case N:                                                                                           \
+    if (what == 0) K::volumeUnknownsProlongation<5, 0, N + 1>(out_q, in_q, 0, level_delta, vi);     \
+    else if (what == 1) K::volumeUnknownsRestriction<5, 0, N + 1>(out_q, in_q, 0, level_delta, vi); \
+    else if (what == 2) K::faceUnknownsProlongation<5, 0, N + 1>(out_q, out_f, in_q, in_f, 0, level_delta, fi); \
+    else K::faceUnknownsRestriction<5, 0, N + 1>(out_q, out_f, in_q, in_f, 0, level_delta, fi);    \
+    return 0;
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
 }  // extern "C"

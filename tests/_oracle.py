@@ -64,6 +64,8 @@ def lib():
     L.orc_aderdg_sample_step.argtypes = [i, i, i, C.c_long, _dp, _dp, d, i]
     L.orc_aderdg_slab_predict.argtypes = [i, i, i, _ip, _dp, _dp, d, _dp, _dp, _dp, _dp, _dp]
     L.orc_aderdg_slab_correct.argtypes = [i, i, i, _ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d]
+    L.orc_amr_prolongation.argtypes = [i, i, i, _dp, _dp, i, _ip]
+    L.orc_amr_restriction.argtypes = [i, i, i, _dp, _dp, i, _ip]
     L.orc_fv_patchgrid_step_2d.restype = d
     L.orc_fv_patchgrid_step_2d.argtypes = [i, i, i, i, i, _dp, _dp]
     L.orc_noise_u01.restype = d
@@ -134,6 +136,9 @@ def ref_lib(dim):
     if os.path.exists(so):
         L = C.CDLL(so)
         d, i = C.c_double, C.c_int
+        if hasattr(L, 'ref_amr'):
+            L.ref_amr.restype = i
+            L.ref_amr.argtypes = [i, i, _dp, _dp, _dp, _dp, i, _ip]
         L.ref_stp.restype = i
         L.ref_stp.argtypes = [i, i, _dp, _dp, _dp, _dp, _dp, _dp, _dp, d]
         L.ref_volume_integral.restype = i

@@ -73,12 +73,15 @@ def extract_dg_tables(ref):
             out['%s/%d' % (name, n)] = np.full((b, b), np.nan)
         for name in ('F0', 'FLCoeff', 'FRCoeff'):
             out['%s/%d' % (name, n)] = np.full(b, np.nan)
+        out['fgp/%d' % n] = np.full((3, b, b), np.nan)
         out['weights/%d' % n] = np.full(b, np.nan)
         out['nodes/%d' % n] = np.full(b, np.nan)
     for m in re.finditer(r'\b(Kxi|iK1|dudx)\[(\d)\]\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', src):
         out['%s/%s' % (m.group(1), m.group(2))][int(m.group(3)), int(m.group(4))] = float(m.group(5))
     for m in re.finditer(r'\b(F0|FLCoeff|FRCoeff)\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', src):
         out['%s/%s' % (m.group(1), m.group(2))][int(m.group(3))] = float(m.group(4))
+    for m in re.finditer(r'fineGridProjector1d\[(\d)\]\[(\d)\]\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', src):
+        out['fgp/%s' % m.group(1)][int(m.group(2)), int(m.group(3)), int(m.group(4))] = float(m.group(5))
     for m in re.finditer(r'gaussLegendre(Weights|Nodes)\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', gsrc):
         key = ('weights' if m.group(1) == 'Weights' else 'nodes') + '/' + m.group(2)
         out[key][int(m.group(3))] = float(m.group(4))

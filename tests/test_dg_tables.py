@@ -35,6 +35,10 @@ def test_tables_match_reference(tables, ref, order):
         assert np.abs(a - b).max() <= 2e-13 * scale, mine
         exact = np.mean(a == b)
         assert exact > 0.85, (mine, exact)
+    # fine-grid projector of 3:1 refinement (DGMatrices.cpp fineGridProjector1d)
+    a, b = np.array(t['fgp']), ref['fgp/%d' % order]
+    assert np.abs(a - b).max() <= 2e-14 * max(1.0, np.abs(b).max()), 'fgp'
+    assert np.mean(a == b) > 0.95, 'fgp'
     for mine, theirs in (('f0', 'F0'), ('flcoeff', 'FLCoeff'), ('frcoeff', 'FRCoeff'),
                          ('gl_weights', 'weights'), ('gl_nodes', 'nodes')):
         a, b = np.array(t[mine]), ref['%s/%d' % (theirs, order)]
