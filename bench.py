@@ -269,7 +269,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
-    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving', 'fv'],
+    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving', 'fv', 'amr'],
                     help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
                          'serving: Poisson stream of solve requests; fv: one periodic 2D FV patch')
     ap.add_argument('--fv-patch', type=int, default=8192)
@@ -309,6 +309,9 @@ def main():
         return
     if args.workload == 'fv':
         run_fv(args, rank, world, dist)
+        return
+    if args.workload == 'amr':
+        run_amr(args, rank, world, dist)
         return
     if args.impl == 'reference':
         run_reference(args, rank, world)
@@ -747,6 +750,53 @@ def run_fv(args, rank, world, dist):
                 'clocks': m['clocks'], 'godunov': out['godunov'],
                 'patch_grid_10': {'musclhancock': out['musclhancock_patches10'],
                                   'godunov': out['godunov_patches10']}}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- AMR
+def run_amr(args, rank, world, dist):
+    """AMR transfer operators on 3D N=4 cells: every coarse cell prolonged
+    into one descendant and every fine cell restricted into its own parent
+    slot (one level), items resident on the GPU."""
+    import exahype_b200 as E
+    from exahype_b200 import DeviceBuffer, Timer
+    from exahype_b200.aderdg import amr_prolongation, amr_restriction
+    E.lib().exa_set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    peaks, peak_src = measured_peaks()
+    k, order, count = 3, args.order, 200000
+    n = (order + 1) ** k * 5
+    rng = np.random.default_rng(args.seed)
+    coarse = DeviceBuffer.from_array(rng.standard_normal(count * n))
+    fine = DeviceBuffer(count * n)
+    idx = np.zeros((count, 3), np.int32)
+    idx[:, :k] = rng.integers(0, 3, size=(count, k))
+    d_i = DeviceBuffer.from_array(idx)
+    out = {}
+    for name, fn in (('prolongation', lambda: amr_prolongation(k, order, count, fine, coarse, 1, d_i)),
+                     ('restriction', lambda: amr_restriction(k, order, count, coarse, fine, 1, d_i))):
+        for _ in range(args.warmup):
+            fn()
+        E.device.synchronize()
+        t = Timer()
+        t.start(None)
+        for _ in range(args.steps):
+            fn()
+        t.stop(None)
+        ms = t.elapsed_ms() / args.steps
+        moved = count * n * 8 * (2 if name == 'prolongation' else 3)  # read in (+ read out) + write out
+        out[name] = {'ms_per_call': ms, 'items_per_s': world * count / (ms * 1e-3),
+                     'hbm_gbs': moved / (ms * 1e-3) / 1e9,
+                     'hbm_frac': moved / (ms * 1e-3) / 1e9 / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None}
+    if rank == 0:
+        line = {'metric': 'AMR volume transfers (3D N=%d, one level) items/s' % order,
+                'value': out['prolongation']['items_per_s'], 'unit': 'items/s', 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': out['prolongation']['ms_per_call'],
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic', 'config': {'workload': '%d cells of 3D N=%d, random child index' % (count, order)},
+                'roofline': {'bound': 'hbm', 'peak_source': peak_src}, **out}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
