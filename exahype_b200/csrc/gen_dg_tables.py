@@ -78,6 +78,34 @@ def dlagrange(xs, k, x):
     return s
 
 
+def gauss_lobatto_unit(n):
+    """n-point Gauss-Lobatto nodes on [0,1] in the reference's order,
+    descending from 1 to 0 (GaussLobattoQuadrature.cpp:47-160); the
+    1-point rule is the midpoint, as there."""
+    if n == 1:
+        return [mp.mpf(1) / 2]
+    # interior nodes: roots of P'_{n-1} on [-1,1], by Newton from the
+    # Chebyshev-Gauss-Lobatto guesses
+    m = n - 1
+    xs = []
+    for i in range(1, m):
+        x = -mp.cos(mp.pi * i / m)
+        for _ in range(200):
+            p0, p1 = mp.mpf(1), x
+            for k in range(2, m + 1):
+                p0, p1 = p1, ((2 * k - 1) * x * p1 - (k - 1) * p0) / k
+            # P'_m and P''_m from the Legendre ODE
+            dp = m * (x * p1 - p0) / (x * x - 1)
+            d2p = (2 * x * dp - m * (m + 1) * p1) / (1 - x * x)
+            step = dp / d2p
+            x -= step
+            if abs(step) < mp.mpf(10) ** -55:
+                break
+        xs.append(x)
+    pts = [mp.mpf(-1)] + xs + [mp.mpf(1)]
+    return sorted([(1 + x) / 2 for x in pts], reverse=True)
+
+
 def round13(v):
     """Round to 13 significant digits (the precision of the reference's
     stiffness tables), then to the nearest double."""
@@ -94,7 +122,7 @@ def derive(order):
         for l in range(b):
             k1[k, l] = lagrange(xs, k, 1) * lagrange(xs, l, 1) - kxi[k][l]
     ik1 = k1 ** -1
-    return {
+    out = {
         'gl_nodes': [float(x) for x in xs],
         'gl_weights': [float(w) for w in ws],
         'kxi': [[round13(kxi[k][l]) for l in range(b)] for k in range(b)],
@@ -107,6 +135,51 @@ def derive(order):
                 for sub in range(3)],
         'flcoeff': [float(lagrange(xs, k, 0)) for k in range(b)],
         'frcoeff': [float(lagrange(xs, k, 1)) for k in range(b)],
+        'lob_nodes': [float(x) for x in gauss_lobatto_unit(b)],
+    }
+    out.update(derive_limiter(xs, ws))
+    return out
+
+
+def derive_limiter(xs, ws):
+    """Projections between the nodal DG basis of one cell and its FV
+    subcell patch of S = 2N+1 subcells per direction (the reference builds
+    them at start-up, LimiterProjectionMatrices.cpp:40-140):
+
+    * uh2lim[k][i] -- mean of phi_k over subcell i, [i/S, (i+1)/S] (the
+      reference integrates with the B-point Gauss-Legendre rule, exact for
+      degree N);
+    * uh2lob[k][i] -- phi_k at Gauss-Lobatto node i (descending order);
+    * lim2uh[i][k] -- the conservative least-squares inverse: for subcell
+      means L, u = sum_i L_i lim2uh[i][:] minimises
+      sum_i (sum_k uh2lim[k][i] u_k - L_i)^2 subject to
+      sum_k w_k u_k = sum_i L_i / S (the cell mean is kept).  Solved from
+      the bordered normal equations [[2 U U^T, -w], [w^T, 0]].
+    All three are kept at full double precision (the reference computes
+    them in double at run time)."""
+    b = len(xs)
+    s = 2 * (b - 1) + 1
+    dxi = mp.mpf(1) / s
+    uh2lim = [[mp.fsum(ws[j] * lagrange(xs, k, i * dxi + dxi * xs[j]) for j in range(b))
+               for i in range(s)] for k in range(b)]
+    lob = gauss_lobatto_unit(b)
+    uh2lob = [[lagrange(xs, k, lob[i]) for i in range(b)] for k in range(b)]
+    a = mp.matrix(b + 1, b + 1)
+    for i in range(b):
+        for j in range(b):
+            a[i, j] = 2 * mp.fsum(uh2lim[i][k] * uh2lim[j][k] for k in range(s))
+        a[i, b] = -ws[i]
+        a[b, i] = ws[i]
+    ia = a ** -1
+    lim2uh = [[None] * b for _ in range(s)]
+    for i in range(s):
+        rhs = [2 * uh2lim[j][i] for j in range(b)] + [dxi]
+        for k in range(b):
+            lim2uh[i][k] = mp.fsum(ia[k, m] * rhs[m] for m in range(b + 1))
+    return {
+        'uh2lim': [[float(v) for v in row] for row in uh2lim],
+        'uh2lob': [[float(v) for v in row] for row in uh2lob],
+        'lim2uh': [[float(v) for v in row] for row in lim2uh],
     }
 
 
@@ -157,6 +230,25 @@ def write_header(path):
             out.append('    },\n')
         out.append('  },\n')
     out.append('};\n')
+    # limiter projections (subcell count S = 2N+1 <= 19)
+    S = 2 * MAX_ORDER + 1
+    out.append('#define EXA_LIM_MAX_SUBCELLS %d\n' % S)
+    out.append('EXA_TABLE_QUAL double exa_lob_nodes[%d][%d] = {\n' % (D, D))
+    for n in range(D):
+        row = tabs[n]['lob_nodes'] + [0.0] * (D - len(tabs[n]['lob_nodes']))
+        out.append('  {' + ', '.join(_fmt(v) for v in row) + '},\n')
+    out.append('};\n')
+    for name, rows, cols in (('uh2lim', D, S), ('uh2lob', D, D), ('lim2uh', S, D)):
+        out.append('EXA_TABLE_QUAL double exa_%s[%d][%d][%d] = {\n' % (name, D, rows, cols))
+        for n in range(D):
+            out.append('  {\n')
+            m = tabs[n][name]
+            for k in range(rows):
+                row = list(m[k]) if k < len(m) else []
+                row = row + [0.0] * (cols - len(row))
+                out.append('    {' + ', '.join(_fmt(v) for v in row) + '},\n')
+            out.append('  },\n')
+        out.append('};\n')
     # CFL safety factors for ADER-DG of order N (reference
     # kernels/aderdg/generic/c/3d/stableTimeStepSize.cpph:33-34)
     out.append('EXA_TABLE_QUAL double exa_pnpm[10] = {1.0, 0.33, 0.17, 0.1, 0.069, '

@@ -1223,3 +1223,161 @@ double orc_fv_patch_step_2d(int scheme, int P, int planar, double* luh,
   free(old);
   return dt;
 }
+
+/* ------------------------------------------------------------------ */
+/* A-posteriori subcell limiter (kernels/limiter/generic/c/Limiter.cpp).
+ * Direct tensor sums in the reference's loop order; tables uh2lim, uh2lob,
+ * lim2uh are the projections of LimiterProjectionMatrices.cpp:40-140 from
+ * dg_tables.h. */
+static int lim_subcells(int order) { return 2 * order + 1; }
+
+/* projectOnFVLimiterSpace, Limiter.cpp:23-64 */
+void orc_limiter_project_on_fv(int dim, int order, int nvar, int ghost, const double* luh,
+                               double* lim) {
+  const int B = order + 1, S = lim_subcells(order), SG = S + 2 * ghost;
+  const int B3 = dim == 3 ? B : 1, S3 = dim == 3 ? S : 1, G3 = dim == 3 ? ghost : 0;
+  const double(*U)[EXA_LIM_MAX_SUBCELLS] = exa_uh2lim[order];
+  int x, y, z, v, ix, iy, iz;
+  for (z = G3; z < S3 + G3; z++)
+    for (y = ghost; y < S + ghost; y++)
+      for (x = ghost; x < S + ghost; x++)
+        for (v = 0; v < nvar; v++) {
+          double acc = 0.0;
+          for (iz = 0; iz < B3; iz++)
+            for (iy = 0; iy < B; iy++)
+              for (ix = 0; ix < B; ix++) {
+                double t = luh[((iz * B + iy) * B + ix) * nvar + v];
+                if (dim == 3) t *= U[iz][z - G3];
+                acc += t * U[iy][y - ghost] * U[ix][x - ghost];
+              }
+          lim[(((long)z * SG + y) * SG + x) * nvar + v] = acc;
+        }
+}
+
+/* projectOnDGSpace, Limiter.cpp:67-110 */
+void orc_limiter_project_on_dg(int dim, int order, int nvar, int ghost, const double* lim,
+                               double* luh) {
+  const int B = order + 1, S = lim_subcells(order), SG = S + 2 * ghost;
+  const int B3 = dim == 3 ? B : 1, S3 = dim == 3 ? S : 1, G3 = dim == 3 ? ghost : 0;
+  const double(*L)[10] = exa_lim2uh[order];
+  int x, y, z, v, ix, iy, iz;
+  for (z = 0; z < B3; z++)
+    for (y = 0; y < B; y++)
+      for (x = 0; x < B; x++)
+        for (v = 0; v < nvar; v++) {
+          double acc = 0.0;
+          for (iz = G3; iz < S3 + G3; iz++)
+            for (iy = ghost; iy < S + ghost; iy++)
+              for (ix = ghost; ix < S + ghost; ix++) {
+                double t = lim[(((long)iz * SG + iy) * SG + ix) * nvar + v];
+                if (dim == 3) t *= L[iz - G3][z];
+                acc += t * L[iy - ghost][y] * L[ix - ghost][x];
+              }
+          luh[((z * B + y) * B + x) * nvar + v] = acc;
+        }
+}
+
+/* min/max of the observables (= first nobs values) over a tensor-product
+ * evaluation of luh with the 1D table T[k][i] (n points per direction) */
+static void lim_eval_min_max(int dim, int order, int nvar, int nobs, const double* luh,
+                             const double* T, int tstride, int n, double* mn, double* mx) {
+  const int B = order + 1, B3 = dim == 3 ? B : 1, n3 = dim == 3 ? n : 1;
+  int x, y, z, v, ix, iy, iz;
+  for (z = 0; z < n3; z++)
+    for (y = 0; y < n; y++)
+      for (x = 0; x < n; x++)
+        for (v = 0; v < nobs; v++) {
+          double acc = 0.0;
+          for (iz = 0; iz < B3; iz++)
+            for (iy = 0; iy < B; iy++)
+              for (ix = 0; ix < B; ix++) {
+                double t = luh[((iz * B + iy) * B + ix) * nvar + v];
+                if (dim == 3) t *= T[iz * tstride + z];
+                acc += t * T[iy * tstride + y] * T[ix * tstride + x];
+              }
+          if (acc < mn[v]) mn[v] = acc;
+          if (acc > mx[v]) mx[v] = acc;
+        }
+}
+
+/* findCellLocalMinAndMax, Limiter.cpp:212-251, with
+ * compareWithADERDGSolutionAtGaussLobattoNodes (:258-306) and
+ * compareWithADERDGSolutionAtFVSubcellCenters (:312-368) */
+static void lim_cell_local_min_max(int dim, int order, int nvar, int nobs, const double* luh,
+                                   double* mn, double* mx) {
+  const int B = order + 1, npts = dim == 3 ? B * B * B : B * B;
+  int i, v;
+  for (v = 0; v < nobs; v++) {
+    mn[v] = DBL_MAX;
+    mx[v] = -DBL_MAX;
+  }
+  for (i = 0; i < npts; i++)
+    for (v = 0; v < nobs; v++) {
+      const double q = luh[i * nvar + v];
+      if (q < mn[v]) mn[v] = q;
+      if (q > mx[v]) mx[v] = q;
+    }
+  lim_eval_min_max(dim, order, nvar, nobs, luh, &exa_uh2lob[order][0][0], 10, B, mn, mx);
+  lim_eval_min_max(dim, order, nvar, nobs, luh, &exa_uh2lim[order][0][0],
+                   EXA_LIM_MAX_SUBCELLS, lim_subcells(order), mn, mx);
+}
+
+static void lim_copy_to_faces(int dim, int nobs, double* obs_min, double* obs_max) {
+  int f, v;
+  for (f = 1; f < 2 * dim; f++)
+    for (v = 0; v < nobs; v++) {
+      obs_min[f * nobs + v] = obs_min[v];
+      obs_max[f * nobs + v] = obs_max[v];
+    }
+}
+
+void orc_limiter_local_min_max(int dim, int order, int nvar, int nobs, const double* luh,
+                               double* obs_min, double* obs_max) {
+  lim_cell_local_min_max(dim, order, nvar, nobs, luh, obs_min, obs_max);
+  lim_copy_to_faces(dim, nobs, obs_min, obs_max);
+}
+
+/* findCellLocalLimiterMinAndMax, Limiter.cpp:170-207 */
+void orc_limiter_fv_min_max(int dim, int order, int nvar, int nobs, int ghost,
+                            const double* lim, double* obs_min, double* obs_max) {
+  const int S = lim_subcells(order), SG = S + 2 * ghost;
+  const int S3 = dim == 3 ? S : 1, G3 = dim == 3 ? ghost : 0;
+  int x, y, z, v;
+  for (v = 0; v < nobs; v++) {
+    obs_min[v] = DBL_MAX;
+    obs_max[v] = -DBL_MAX;
+  }
+  for (z = G3; z < S3 + G3; z++)
+    for (y = ghost; y < S + ghost; y++)
+      for (x = ghost; x < S + ghost; x++)
+        for (v = 0; v < nobs; v++) {
+          const double q = lim[(((long)z * SG + y) * SG + x) * nvar + v];
+          if (q < obs_min[v]) obs_min[v] = q;
+          if (q > obs_max[v]) obs_max[v] = q;
+        }
+  lim_copy_to_faces(dim, nobs, obs_min, obs_max);
+}
+
+/* discreteMaximumPrincipleAndMinAndMaxSearch, Limiter.cpp:113-167 */
+int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, double relaxation,
+                    double difference_scaling, double* obs_min, double* obs_max) {
+  double mn[64], mx[64];
+  int ok = 1, v, i;
+  if (nobs > 64) return 0;
+  lim_cell_local_min_max(dim, order, nvar, nobs, luh, mn, mx);
+  for (v = 0; v < nobs; v++) {
+    double bmin = obs_min[v], bmax = obs_max[v], sd;
+    for (i = 1; i < 2 * dim; i++) {
+      bmin = fmin(bmin, obs_min[i * nobs + v]);
+      bmax = fmax(bmax, obs_max[i * nobs + v]);
+    }
+    sd = (bmax - bmin) * difference_scaling;
+    sd = fmax(sd, relaxation);
+    if (mn[v] < bmin - sd || mx[v] > bmax + sd) ok = 0;
+    obs_min[v] = mn[v];
+    obs_max[v] = mx[v];
+    obs_min[v + nobs] = bmin;
+    obs_max[v + nobs] = bmax;
+  }
+  return ok;
+}

@@ -123,7 +123,6 @@ double orc_fv_patch_step_2d(int scheme, int patch, int planar, double* luh,
                             const double* dx, double dt_fixed,
                             double* max_admissible_dt);
 
-/* counter-based noise shared with the device IC kernel */
 /* AMR transfer between a coarse cell (or face) and its fine descendant
  * `level_delta` levels down (3:1 per level), for k-dimensional nodal arrays
  * [node][var] (k = dim for cell volumes, dim-1 for faces); index[d] in
@@ -138,6 +137,34 @@ void orc_amr_restriction(int k, int order, int nvar, double* coarse, const doubl
 /* one step of a periodic npx x npy grid of FV patches (dx = patch extent) */
 double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
                                 double* luh, const double* dx);
+
+/* A-posteriori subcell limiter, kernels/limiter/generic/c/Limiter.cpp, for
+ * one cell of order N (B = N+1 nodes, S = 2N+1 subcells per direction):
+ *   luh  [z][y][x][nvar] (B^dim points),
+ *   lim  [z][y][x][nvar] ((S+2g)^dim points, g = ghost layer width; the
+ *        projections read / write the interior only).
+ * Observables are the first nobs variables (the generated solvers' default
+ * mapDiscreteMaximumPrincipleObservables,
+ * AbstractGenericADERDGSolverHeader.template:159-163).  Min/max arrays are
+ * [2 dim][nobs] per cell (face-major, as ADERDGCellDescription's
+ * solutionMin/solutionMax). */
+void orc_limiter_project_on_fv(int dim, int order, int nvar, int ghost, const double* luh,
+                               double* lim);
+void orc_limiter_project_on_dg(int dim, int order, int nvar, int ghost, const double* lim,
+                               double* luh);
+/* findCellLocalMinAndMax (nodes, Gauss-Lobatto points, subcell means) into
+ * face 0, copied to every face (LimitingADERDGSolver::determineSolverMinAndMax) */
+void orc_limiter_local_min_max(int dim, int order, int nvar, int nobs, const double* luh,
+                               double* obs_min, double* obs_max);
+/* findCellLocalLimiterMinAndMax, copied to every face
+ * (LimitingADERDGSolver::determineLimiterMinAndMax) */
+void orc_limiter_fv_min_max(int dim, int order, int nvar, int nobs, int ghost,
+                            const double* lim, double* obs_min, double* obs_max);
+/* discreteMaximumPrincipleAndMinAndMaxSearch; returns 1 if satisfied */
+int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, double relaxation,
+                    double difference_scaling, double* obs_min, double* obs_max);
+
+/* counter-based noise shared with the device IC kernel */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx);
 
 #ifdef __cplusplus

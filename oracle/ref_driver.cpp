@@ -26,6 +26,10 @@
 #include "kernels/finitevolumes/musclhancock/c/musclhancock.h"
 #include "kernels/GaussLegendreQuadrature.h"
 #include "kernels/DGMatrices.h"
+#include "kernels/GaussLobattoQuadrature.h"
+#include "kernels/LimiterProjectionMatrices.h"
+#include "kernels/limiter/generic/Limiter.h"
+#include "exahype/solvers/ADERDGSolver.h"
 
 namespace {
 
@@ -35,6 +39,8 @@ struct TablesInit {
     for (int i = 0; i < 10; i++) orders.insert(i);
     kernels::initGaussLegendreNodesAndWeights(orders);
     kernels::initDGMatrices(orders);
+    kernels::initGaussLobattoNodesAndWeights(orders);
+    kernels::initLimiterProjectionMatrices(orders);
   }
 };
 TablesInit tables_init;
@@ -400,6 +406,42 @@ int ref_amr(int what, int order, double* out_q, double* out_f, const double* in_
   switch (order) { EXA_ORDERS(CASE) }
 #undef CASE
   return -1;
+}
+
+/* The reference's a-posteriori limiter kernels (kernels/limiter/generic/c/
+ * Limiter.cpp) for one cell, driven through the solver stand-in of
+ * ref_shim/exahype/solvers/ADERDGSolver.h.  what: 0 projectOnFVLimiterSpace
+ * (in = luh, out = lim), 1 projectOnDGSpace (in = lim, out = luh),
+ * 2 findCellLocalMinAndMax (in = luh), 3 findCellLocalLimiterMinAndMax
+ * (in = lim), 4 discreteMaximumPrincipleAndMinAndMaxSearch (in = luh;
+ * obs_min/obs_max are the [2 dim][nobs] in/out blocks; returns 1 if the
+ * DMP holds). */
+int ref_limiter(int what, int order, int nvar, int nobs, int ghost, const double* in, double* out,
+                double* obs_min, double* obs_max, double relaxation, double difference_scaling) {
+  namespace L = kernels::limiter::generic::c;
+  const exahype::solvers::ADERDGSolver solver(nvar, order + 1, nobs);
+  switch (what) {
+    case 0: L::projectOnFVLimiterSpace(in, nvar, order + 1, ghost, out); return 0;
+    case 1: L::projectOnDGSpace(in, nvar, order + 1, ghost, out); return 0;
+    case 2: L::findCellLocalMinAndMax(in, &solver, obs_min, obs_max); return 0;
+    case 3: L::findCellLocalLimiterMinAndMax(in, &solver, ghost, obs_min, obs_max); return 0;
+    case 4:
+      return L::discreteMaximumPrincipleAndMinAndMaxSearch(in, &solver, relaxation, difference_scaling,
+                                                            obs_min, obs_max) ? 1 : 0;
+  }
+  return -1;
+}
+
+/* The limiter projection tables as the reference builds them at start-up
+ * (LimiterProjectionMatrices.cpp:40-140) and its Gauss-Lobatto nodes:
+ * uh2lim [B][S], uh2lob [B][B], lim2uh [S][B], lob [B]. */
+int ref_limiter_tables(int order, double* uh2lim, double* uh2lob, double* lim2uh, double* lob) {
+  const int B = order + 1, S = 2 * order + 1;
+  for (int i = 0; i < B * S; i++) uh2lim[i] = kernels::uh2lim[order][i];
+  for (int i = 0; i < B * B; i++) uh2lob[i] = kernels::uh2lob[order][i];
+  for (int i = 0; i < S * B; i++) lim2uh[i] = kernels::lim2uh[order][i];
+  for (int i = 0; i < B; i++) lob[i] = kernels::gaussLobattoNodes[order][i];
+  return 0;
 }
 
 }  // extern "C"

@@ -70,6 +70,12 @@ def lib():
     L.orc_fv_patchgrid_step_2d.argtypes = [i, i, i, i, i, _dp, _dp]
     L.orc_noise_u01.restype = d
     L.orc_noise_u01.argtypes = [C.c_ulonglong, C.c_ulonglong]
+    L.orc_limiter_project_on_fv.argtypes = [i, i, i, i, _dp, _dp]
+    L.orc_limiter_project_on_dg.argtypes = [i, i, i, i, _dp, _dp]
+    L.orc_limiter_local_min_max.argtypes = [i, i, i, i, _dp, _dp, _dp]
+    L.orc_limiter_fv_min_max.argtypes = [i, i, i, i, i, _dp, _dp, _dp]
+    L.orc_limiter_dmp.restype = i
+    L.orc_limiter_dmp.argtypes = [i, i, i, i, _dp, d, d, _dp, _dp]
     _lib = L
     return L
 
@@ -123,6 +129,74 @@ def grid_step(dim, order, n, luh, dt_policy=0, cfl=0.9, dt_fixed=0.0, planar=0,
     return dt, iters
 
 
+def lim_sizes(dim, order, nvar=5, ghost=0):
+    B, S = order + 1, 2 * order + 1
+    return dict(B=B, S=S, luh=B ** dim * nvar, lim=(S + 2 * ghost) ** dim * nvar)
+
+
+def limiter_project_on_fv(dim, order, luh, nvar=5, ghost=0, lim=None):
+    """projectOnFVLimiterSpace of every cell of luh ([cell][B^dim][nvar])."""
+    s = lim_sizes(dim, order, nvar, ghost)
+    luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1, s['luh'])
+    out = np.zeros((luh.shape[0], s['lim'])) if lim is None else lim.reshape(-1, s['lim'])
+    for c in range(luh.shape[0]):
+        row = np.ascontiguousarray(out[c])
+        lib().orc_limiter_project_on_fv(dim, order, nvar, ghost, np.ascontiguousarray(luh[c]), row)
+        out[c] = row
+    return out.ravel()
+
+
+def limiter_project_on_dg(dim, order, lim, nvar=5, ghost=0):
+    s = lim_sizes(dim, order, nvar, ghost)
+    lim = np.ascontiguousarray(lim, dtype=np.float64).reshape(-1, s['lim'])
+    out = np.zeros((lim.shape[0], s['luh']))
+    for c in range(lim.shape[0]):
+        row = np.zeros(s['luh'])
+        lib().orc_limiter_project_on_dg(dim, order, nvar, ghost, np.ascontiguousarray(lim[c]), row)
+        out[c] = row
+    return out.ravel()
+
+
+def limiter_local_min_max(dim, order, luh, nvar=5, nobs=5):
+    s = lim_sizes(dim, order, nvar)
+    luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1, s['luh'])
+    mn = np.zeros((luh.shape[0], 2 * dim * nobs))
+    mx = np.zeros_like(mn)
+    for c in range(luh.shape[0]):
+        a, b = np.zeros(2 * dim * nobs), np.zeros(2 * dim * nobs)
+        lib().orc_limiter_local_min_max(dim, order, nvar, nobs, np.ascontiguousarray(luh[c]), a, b)
+        mn[c], mx[c] = a, b
+    return mn.ravel(), mx.ravel()
+
+
+def limiter_fv_min_max(dim, order, lim, nvar=5, nobs=5, ghost=0):
+    s = lim_sizes(dim, order, nvar, ghost)
+    lim = np.ascontiguousarray(lim, dtype=np.float64).reshape(-1, s['lim'])
+    mn = np.zeros((lim.shape[0], 2 * dim * nobs))
+    mx = np.zeros_like(mn)
+    for c in range(lim.shape[0]):
+        a, b = np.zeros(2 * dim * nobs), np.zeros(2 * dim * nobs)
+        lib().orc_limiter_fv_min_max(dim, order, nvar, nobs, ghost, np.ascontiguousarray(lim[c]), a, b)
+        mn[c], mx[c] = a, b
+    return mn.ravel(), mx.ravel()
+
+
+def limiter_dmp(dim, order, luh, bmin, bmax, relax, scaling, nvar=5, nobs=5):
+    """discreteMaximumPrincipleAndMinAndMaxSearch per cell; returns
+    (ok[cell], new bmin, new bmax)."""
+    s = lim_sizes(dim, order, nvar)
+    luh = np.ascontiguousarray(luh, dtype=np.float64).reshape(-1, s['luh'])
+    bmin = np.array(bmin, dtype=np.float64).reshape(luh.shape[0], -1)
+    bmax = np.array(bmax, dtype=np.float64).reshape(luh.shape[0], -1)
+    ok = np.zeros(luh.shape[0], dtype=np.int32)
+    for c in range(luh.shape[0]):
+        a, b = np.ascontiguousarray(bmin[c]), np.ascontiguousarray(bmax[c])
+        ok[c] = lib().orc_limiter_dmp(dim, order, nvar, nobs, np.ascontiguousarray(luh[c]), relax,
+                                      scaling, a, b)
+        bmin[c], bmax[c] = a, b
+    return ok, bmin.ravel(), bmax.ravel()
+
+
 # ---------------------------------------------------------------- reference
 _ref = {}
 
@@ -136,6 +210,12 @@ def ref_lib(dim):
     if os.path.exists(so):
         L = C.CDLL(so)
         d, i = C.c_double, C.c_int
+        if hasattr(L, 'ref_limiter'):
+            L.ref_limiter.restype = i
+            L.ref_limiter.argtypes = [i, i, i, i, i, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      d, d]
+            L.ref_limiter_tables.restype = i
+            L.ref_limiter_tables.argtypes = [i, _dp, _dp, _dp, _dp]
         if hasattr(L, 'ref_amr'):
             L.ref_amr.restype = i
             L.ref_amr.argtypes = [i, i, _dp, _dp, _dp, _dp, i, _ip]

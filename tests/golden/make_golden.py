@@ -11,10 +11,14 @@ argument, default ``/root/reference``).  It writes, next to this script:
   ``GenericEulerKernelTest{2D,3D}.cpp`` checks its generic kernels against
   (order 3, 5 variables, 1 material parameter, eps 1e-10).
 * ``dg_tables_ref.npz`` -- the reference's hard-coded Gauss-Legendre rule
-  (``ExaHyPE/kernels/GaussLegendreQuadrature.cpp:33-164``) and DG operator
-  tables (``ExaHyPE/kernels/DGMatrices.cpp:82-3116``), keyed
+  (``ExaHyPE/kernels/GaussLegendreQuadrature.cpp:33-164``), Gauss-Lobatto
+  nodes (``ExaHyPE/kernels/GaussLobattoQuadrature.cpp:47-160``) and DG
+  operator tables (``ExaHyPE/kernels/DGMatrices.cpp:82-3116``), keyed
   ``<table>/<order>`` as dense arrays, used to pin this project's own
   derivation of the tables.
+* ``limiter_2d.npz`` / ``limiter_3d.npz`` -- the limiter projection
+  known-answer arrays of
+  ``ExaHyPE/exahype/tests/kernels/testdata/limiter_testdata.cpp``.
 
 The fixtures are data only; nothing under ``tests/`` reads the reference
 tree at test time.
@@ -41,7 +45,7 @@ def _parse_arrays(text):
             body = re.sub(r'//[^\n]*|/\*.*?\*/', ' ', m.group(5), flags=re.S)
             vals = [float(v) for v in re.split(r'[,\s]+', body.strip()) if v]
             n = int(m.group(4))
-            assert len(vals) == n, (m.group(3), len(vals), n)
+            assert len(vals) in (n, 0), (m.group(3), len(vals), n)  # `= {}`: no data
             yield ns_stack[-1], m.group(3), np.array(vals)
         else:
             if ns_stack:
@@ -85,9 +89,37 @@ def extract_dg_tables(ref):
     for m in re.finditer(r'gaussLegendre(Weights|Nodes)\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', gsrc):
         key = ('weights' if m.group(1) == 'Weights' else 'nodes') + '/' + m.group(2)
         out[key][int(m.group(3))] = float(m.group(4))
+    lsrc = open(os.path.join(ref, 'ExaHyPE/kernels/GaussLobattoQuadrature.cpp')).read()
+    for n in range(10):
+        out['lob_nodes/%d' % n] = np.full(n + 1, np.nan)
+    for m in re.finditer(r'gaussLobattoNodes\s*\[(\d)\]\[(\d)\]\s*=\s*([-+0-9.eE]+);', lsrc):
+        out['lob_nodes/%s' % m.group(1)][int(m.group(2))] = float(m.group(3))
     for k, v in out.items():
         assert not np.isnan(v).any(), k
     np.savez_compressed(os.path.join(HERE, 'dg_tables_ref.npz'), **out)
+    return out
+
+
+def extract_limiter(ref):
+    """Known-answer data of the limiter projections,
+    ExaHyPE/exahype/tests/kernels/testdata/limiter_testdata.cpp (order 3,
+    5 variables; 2D block from `#ifdef Dim2`, 3D block from `#ifdef Dim3`):
+    testFromLuhConversion::{luh_in, lob_out, lim_out} and
+    testToLuhConversion::{lim_in, luh_out}.  (The reference's
+    LimiterKernelTest.cpp keeps the checks that would use them commented
+    out.)"""
+    path = os.path.join(ref, 'ExaHyPE/exahype/tests/kernels/testdata/limiter_testdata.cpp')
+    text = open(path).read()
+    i2 = text.index('#ifdef Dim2')
+    i3 = text.index('#ifdef Dim3')
+    out = {}
+    for tag, block in (('2d', text[i2:i3]), ('3d', text[i3:])):
+        arrays = {}
+        for ns, name, vals in _parse_arrays(block):
+            if vals.size:
+                arrays['%s/%s' % (ns, name)] = vals
+        out[tag] = arrays
+        np.savez_compressed(os.path.join(HERE, 'limiter_%s.npz' % tag), **arrays)
     return out
 
 
@@ -95,5 +127,7 @@ if __name__ == '__main__':
     ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
     ge = extract_generic_euler(ref)
     tabs = extract_dg_tables(ref)
+    lim = extract_limiter(ref)
+    print('limiter 2d arrays:', sorted(lim['2d']), ' 3d arrays:', sorted(lim['3d']))
     print('generic_euler 2d arrays:', len(ge['2d']), ' 3d arrays:', len(ge['3d']),
           ' dg tables:', len(tabs))

@@ -40,7 +40,8 @@ def test_tables_match_reference(tables, ref, order):
     assert np.abs(a - b).max() <= 2e-14 * max(1.0, np.abs(b).max()), 'fgp'
     assert np.mean(a == b) > 0.95, 'fgp'
     for mine, theirs in (('f0', 'F0'), ('flcoeff', 'FLCoeff'), ('frcoeff', 'FRCoeff'),
-                         ('gl_weights', 'weights'), ('gl_nodes', 'nodes')):
+                         ('gl_weights', 'weights'), ('gl_nodes', 'nodes'),
+                         ('lob_nodes', 'lob_nodes')):
         a, b = np.array(t[mine]), ref['%s/%d' % (theirs, order)]
         assert np.abs(a - b).max() <= 2e-14 * max(1.0, np.abs(b).max()), mine
 
