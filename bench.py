@@ -269,7 +269,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
-    ap.add_argument('--workload', default='grid3d', choices=['grid3d', 'ensemble', 'serving', 'fv', 'amr'],
+    ap.add_argument('--workload', default='grid3d',
+                    choices=['grid3d', 'ensemble', 'serving', 'fv', 'amr', 'limiter'],
                     help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
                          'serving: Poisson stream of solve requests; fv: one periodic 2D FV patch')
     ap.add_argument('--fv-patch', type=int, default=8192)
@@ -277,6 +278,7 @@ def main():
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--dg-fraction', type=float, default=0.25)
     ap.add_argument('--nsolves', type=int, default=512)
+    ap.add_argument('--limiter-cells', type=int, default=131072)
     ap.add_argument('--tune', action='append', default=[],
                     help='key=value tuning knob passed to exa_tune_set (see include/exa_kernels.h)')
     args = ap.parse_args()
@@ -312,6 +314,9 @@ def main():
         return
     if args.workload == 'amr':
         run_amr(args, rank, world, dist)
+        return
+    if args.workload == 'limiter':
+        run_limiter(args, rank, world, dist)
         return
     if args.impl == 'reference':
         run_reference(args, rank, world)
@@ -797,6 +802,87 @@ def run_amr(args, rank, world, dist):
                 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
                 'data': 'synthetic', 'config': {'workload': '%d cells of 3D N=%d, random child index' % (count, order)},
                 'roofline': {'bound': 'hbm', 'peak_source': peak_src}, **out}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_limiter(args, rank, world, dist):
+    """Limiter kernels on 3D N=4 cells resident on the GPU: DG -> FV subcell
+    projection into patches with one ghost layer, FV -> DG projection back,
+    and the DMP check with its min/max search (5 observables); inputs larger
+    than L2."""
+    import ctypes as C
+    import exahype_b200 as E
+    from exahype_b200 import DeviceBuffer, Timer, limiter
+    E.lib().exa_set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    peaks, peak_src = measured_peaks()
+    dim, order, count, ghost, V = 3, args.order, args.limiter_cells, 1, 5
+    B, S = order + 1, 2 * order + 1
+    n_luh, n_lim = B ** dim * V, (S + 2 * ghost) ** dim * V
+    rng = np.random.default_rng(args.seed)
+    luh_h = rng.uniform(0.5, 2.0, count * n_luh)
+    luh = DeviceBuffer.from_array(luh_h)
+    lim = DeviceBuffer(count * n_lim)
+    lim.zero()
+    back = DeviceBuffer(count * n_luh)
+    nb = 2 * dim * V
+    bmin = DeviceBuffer.from_array(np.full(count * nb, 0.4))
+    bmax = DeviceBuffer.from_array(np.full(count * nb, 2.2))
+    ok = DeviceBuffer(count, dtype=np.int32)
+    lu_b, li_b = n_luh * 8, S ** dim * V * 8
+    kernels = (
+        ('project_on_fv', lambda: limiter.project_on_fv(dim, order, count, luh, lim, ghost=ghost), lu_b + li_b),
+        ('project_on_dg', lambda: limiter.project_on_dg(dim, order, count, lim, back, ghost=ghost), lu_b + li_b),
+        ('dmp', lambda: limiter.dmp(dim, order, count, luh, bmin, bmax, ok, 1e-4, 1e-3),
+         lu_b + 2 * nb * 8 + 2 * 2 * V * 8 + 4),
+    )
+    out = {}
+    for name, fn, bytes_per_cell in kernels:
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        E.device.synchronize()
+        t = Timer()
+        t.start(None)
+        for _ in range(args.steps):
+            fn()
+        t.stop(None)
+        ms = t.elapsed_ms() / args.steps
+        gbs = count * bytes_per_cell / (ms * 1e-3) / 1e9
+        out[name] = {'ms_per_call': ms, 'cells_per_s': world * count / (ms * 1e-3),
+                     'bytes_per_cell': bytes_per_cell, 'hbm_gbs': gbs,
+                     'hbm_frac': gbs / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None}
+    # CPU baseline: the reference's own Limiter.cpp (oracle/_ref) on a sample
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        so = os.path.join(ROOT, 'oracle', '_ref', 'libexa_ref3d.so')
+        if os.path.exists(so):
+            R = C.CDLL(so)
+            R.ref_limiter.restype = C.c_int
+            R.ref_limiter.argtypes = [C.c_int] * 5 + [C.c_void_p] * 4 + [C.c_double] * 2
+            sample = 256
+            src = np.ascontiguousarray(luh_h[:sample * n_luh])
+            dst = np.zeros(n_lim)
+            t0 = time.perf_counter()
+            for c in range(sample):
+                R.ref_limiter(0, order, V, V, ghost, src[c * n_luh:].ctypes.data, dst.ctypes.data, None, None,
+                              0.0, 0.0)
+            dt = time.perf_counter() - t0
+            cpu = {'value': sample / dt, 'unit': 'cells/s', 'cores': 1, 'kind': 'reference',
+                   'sample': 'projectOnFVLimiterSpace of %d cells, one thread' % sample}
+    if rank == 0:
+        line = {'metric': 'limiter DG->FV subcell projection (3D N=%d) cells/s' % order,
+                'value': out['project_on_fv']['cells_per_s'], 'unit': 'cells/s', 'n_gpus': world,
+                'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': out['project_on_fv']['ms_per_call'],
+                'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+                'data': 'synthetic',
+                'config': {'workload': '%d cells of 3D N=%d, patches of %d^3 subcells + %d ghost layer'
+                           % (count, order, S, ghost), 'l2': 'inputs larger than L2'},
+                'roofline': {'bound': 'hbm', 'achieved': out['project_on_fv']['hbm_gbs'],
+                             'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s',
+                             'frac': out['project_on_fv']['hbm_frac'], 'peak_source': peak_src},
+                'cpu_baseline': cpu, 'kernels': out}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -10,8 +10,9 @@ from .aderdg import ADERDGGrid, ADERDGSolver, BatchedADERDG, make_desc
 from .device import DeviceBuffer, PinnedBuffer, Stream, Timer, device_count, launch_count
 from .ensemble import Ensemble, solve_config
 from .fv import FVGrid, FVPatchGrid, FVPatches
+from . import limiter
 
 __all__ = ['ADERDGGrid', 'ADERDGSolver', 'BatchedADERDG', 'DeviceBuffer', 'PinnedBuffer', 'Stream',
            'Timer', 'FVPatches', 'FVGrid', 'FVPatchGrid', 'Ensemble', 'solve_config', 'ExaError', 'lib', 'make_desc', 'device_count', 'launch_count',
            'EXA_OK', 'PDE_EULER', 'PDE_EULER_PLANAR', 'PREC_FP64', 'PREC_MIXED', 'BC_PERIODIC', 'BC_OUTFLOW',
-           'BC_REFLECT']
+           'BC_REFLECT', 'limiter']

@@ -148,6 +148,16 @@ SIGNATURES = {
     'exa_fv_patchgrid_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_aderdg_amr_prolongation': (i32, [i32, i32, i32, i64, vp, vp, vp, i32, vp, vp]),
     'exa_aderdg_amr_restriction': (i32, [i32, i32, i32, i64, vp, vp, i32, vp, vp]),
+    'exa_limiter_project_on_fv': (i32, [i32, i32, i32, i32, i64, vp, vp, vp]),
+    'exa_limiter_project_on_dg': (i32, [i32, i32, i32, i32, i64, vp, vp, vp]),
+    'exa_limiter_local_min_max': (i32, [i32, i32, i32, i32, i64, vp, vp, vp, vp]),
+    'exa_limiter_fv_min_max': (i32, [i32, i32, i32, i32, i32, i64, vp, vp, vp, vp]),
+    'exa_limiter_dmp': (i32, [i32, i32, i32, i32, i64, vp, f64, f64, vp, vp, vp, vp]),
+    'exa_limiter_projectOnFVLimiterSpace': (i32, [i32, dptr, i32, i32, i32, dptr]),
+    'exa_limiter_projectOnDGSpace': (i32, [i32, dptr, i32, i32, i32, dptr]),
+    'exa_limiter_findCellLocalMinAndMax': (i32, [i32, dptr, i32, i32, i32, dptr, dptr]),
+    'exa_limiter_discreteMaximumPrincipleAndMinAndMaxSearch': (i32, [i32, dptr, i32, i32, i32, f64, f64, dptr, dptr,
+                                                                     C.POINTER(i32)]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),

@@ -1,5 +1,6 @@
 // C ABI of libexahype_b200: runtime helpers, per-cell drop-ins, batched
 // device entry points and the uniform periodic ADER-DG grid.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -52,6 +53,7 @@ exa_status_t ensure_tables() {
   exa_status_t s;
   if ((s = upload_tables_predictor())) return s;
   if ((s = upload_tables_amr())) return s;
+  if ((s = upload_tables_limiter())) return s;
   if ((s = upload_tables_predictor_mixed())) return s;
   if ((s = upload_tables_ensemble())) return s;
   if ((s = upload_tables_faces())) return s;
@@ -499,6 +501,89 @@ exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL, do
   if (st) return st;
   for (int i = 0; i < nvar; i++) fL[i] = fR[i] = out[i];
   if (s_max) *s_max = out[kV];
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ limiter: per-cell drop-ins
+// kernels::limiter::generic::c (Limiter.cpp) argument lists on HOST
+// pointers for one cell, run through the batched device kernels.
+extern "C" {
+
+static long lim_points(int dim, int n) { return dim == 3 ? (long)n * n * n : (long)n * n; }
+
+exa_status_t exa_limiter_projectOnFVLimiterSpace(int dim, const double* luh, int numberOfVariables,
+                                                 int basisSize, int ghostLayerWidth, double* lim) {
+  if (!luh || !lim || (dim != 2 && dim != 3) || basisSize < 2 || ghostLayerWidth < 0 || numberOfVariables < 1)
+    return set_error(EXA_EINVAL, "projectOnFVLimiterSpace: bad arguments");
+  const int S = 2 * basisSize - 1, SG = S + 2 * ghostLayerWidth;
+  HostArr arr[2] = {{luh, nullptr, (size_t)(lim_points(dim, basisSize) * numberOfVariables)},
+                    {lim, lim, (size_t)(lim_points(dim, SG) * numberOfVariables)}};
+  return run_one_cell(arr, 2, [&](double** p) {
+    return exa_limiter_project_on_fv(dim, basisSize - 1, numberOfVariables, ghostLayerWidth, 1, p[0], p[1],
+                                     nullptr);
+  });
+}
+
+exa_status_t exa_limiter_projectOnDGSpace(int dim, const double* lim, int numberOfVariables, int basisSize,
+                                          int ghostLayerWidth, double* luh) {
+  if (!luh || !lim || (dim != 2 && dim != 3) || basisSize < 2 || ghostLayerWidth < 0 || numberOfVariables < 1)
+    return set_error(EXA_EINVAL, "projectOnDGSpace: bad arguments");
+  const int S = 2 * basisSize - 1, SG = S + 2 * ghostLayerWidth;
+  HostArr arr[2] = {{lim, nullptr, (size_t)(lim_points(dim, SG) * numberOfVariables)},
+                    {nullptr, luh, (size_t)(lim_points(dim, basisSize) * numberOfVariables)}};
+  return run_one_cell(arr, 2, [&](double** p) {
+    return exa_limiter_project_on_dg(dim, basisSize - 1, numberOfVariables, ghostLayerWidth, 1, p[0], p[1],
+                                     nullptr);
+  });
+}
+
+exa_status_t exa_limiter_findCellLocalMinAndMax(int dim, const double* luh, int numberOfVariables,
+                                                int basisSize, int numberOfObservables,
+                                                double* localMinPerObservable, double* localMaxPerObservable) {
+  if (!luh || !localMinPerObservable || !localMaxPerObservable || (dim != 2 && dim != 3) || basisSize < 2 ||
+      numberOfObservables < 1 || numberOfObservables > numberOfVariables)
+    return set_error(EXA_EINVAL, "findCellLocalMinAndMax: bad arguments");
+  // the reference writes numberOfObservables values; the batched kernel
+  // fills all 2 dim face blocks, of which the first is returned
+  const size_t nb = (size_t)2 * dim * numberOfObservables;
+  std::vector<double> mn(nb), mx(nb);
+  HostArr arr[3] = {{luh, nullptr, (size_t)(lim_points(dim, basisSize) * numberOfVariables)},
+                    {nullptr, mn.data(), nb},
+                    {nullptr, mx.data(), nb}};
+  exa_status_t s = run_one_cell(arr, 3, [&](double** p) {
+    return exa_limiter_local_min_max(dim, basisSize - 1, numberOfVariables, numberOfObservables, 1, p[0], p[1], p[2],
+                                     nullptr);
+  });
+  if (s) return s;
+  std::copy_n(mn.data(), numberOfObservables, localMinPerObservable);
+  std::copy_n(mx.data(), numberOfObservables, localMaxPerObservable);
+  return EXA_OK;
+}
+
+exa_status_t exa_limiter_discreteMaximumPrincipleAndMinAndMaxSearch(
+    int dim, const double* luh, int numberOfVariables, int basisSize, int numberOfObservables,
+    double relaxationParameter, double differenceScaling, double* boundaryMinPerObservable,
+    double* boundaryMaxPerObservable, int* discreteMaximumPrincipleSatisfied) {
+  if (!luh || !boundaryMinPerObservable || !boundaryMaxPerObservable || !discreteMaximumPrincipleSatisfied ||
+      (dim != 2 && dim != 3) || basisSize < 2 || numberOfObservables < 1 || numberOfObservables > numberOfVariables)
+    return set_error(EXA_EINVAL, "discreteMaximumPrincipleAndMinAndMaxSearch: bad arguments");
+  const size_t nb = (size_t)2 * dim * numberOfObservables;
+  double verdict = 0.0;  // device int in a double-sized slot
+  HostArr arr[4] = {{luh, nullptr, (size_t)(lim_points(dim, basisSize) * numberOfVariables)},
+                    {boundaryMinPerObservable, boundaryMinPerObservable, nb},
+                    {boundaryMaxPerObservable, boundaryMaxPerObservable, nb},
+                    {nullptr, &verdict, 1}};
+  exa_status_t s = run_one_cell(arr, 4, [&](double** p) {
+    return exa_limiter_dmp(dim, basisSize - 1, numberOfVariables, numberOfObservables, 1, p[0],
+                           relaxationParameter, differenceScaling, p[1], p[2], reinterpret_cast<int*>(p[3]),
+                           nullptr);
+  });
+  if (s) return s;
+  int ok = 0;
+  std::memcpy(&ok, &verdict, sizeof(int));
+  *discreteMaximumPrincipleSatisfied = ok;
   return EXA_OK;
 }
 

@@ -115,6 +115,7 @@ exa_status_t upload_tables_ensemble();
 exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 exa_status_t upload_tables_amr();
+exa_status_t upload_tables_limiter();
 // host copy of the derived tables (same bytes as the device constants)
 const void* host_dg_tables(size_t* bytes);
 const void* host_dg_tables_f(size_t* bytes);  // FP32 copies (DGConstF)

@@ -339,6 +339,63 @@ exa_status_t exa_aderdg_amr_prolongation(int k, int order, int nvar, long count,
 exa_status_t exa_aderdg_amr_restriction(int k, int order, int nvar, long count, double* coarse,
                                         const double* fine, int level_delta, const int* index, void* stream);
 
+/* ---- A-posteriori subcell limiter ----
+ * kernels/limiter/generic/c/Limiter.cpp (declared in
+ * kernels/limiter/generic/Limiter.h:41-130) for `ncells` cells on the
+ * device.  Per cell: luh [z][y][x][nvar] with B = order+1 points per
+ * direction; lim [z][y][x][nvar] with S + 2 g points per direction, S =
+ * 2 order + 1 subcells and g = ghost_layer_width (the FV solver's ghost
+ * layer, 1 Godunov / 2 MUSCL-Hancock); the projections touch only the
+ * interior of lim.  Observables are the first nobs variables (the default
+ * mapDiscreteMaximumPrincipleObservables of the generated solvers,
+ * AbstractGenericADERDGSolverHeader.template:159-163); obs_min / obs_max
+ * hold [2 dim][nobs] per cell (ADERDGCellDescription solutionMin /
+ * solutionMax).  Orders 1..6, nvar 1..64. */
+
+/* projectOnFVLimiterSpace (Limiter.cpp:23-64): lim interior = subcell
+ * means of the DG polynomial (uh2lim of LimiterProjectionMatrices.cpp). */
+exa_status_t exa_limiter_project_on_fv(int dim, int order, int nvar, int ghost_layer_width, long ncells,
+                                       const double* luh, double* lim, void* stream);
+/* projectOnDGSpace (Limiter.cpp:67-110): conservative least-squares
+ * reconstruction of the nodal values from the subcell means (lim2uh). */
+exa_status_t exa_limiter_project_on_dg(int dim, int order, int nvar, int ghost_layer_width, long ncells,
+                                       const double* lim, double* luh, void* stream);
+/* findCellLocalMinAndMax (Limiter.cpp:212-251): extrema of the observables
+ * over the nodes, the Gauss-Lobatto points and the subcell means, written
+ * to every face block (LimitingADERDGSolver::determineSolverMinAndMax,
+ * LimitingADERDGSolver.cpp:1080-1116). */
+exa_status_t exa_limiter_local_min_max(int dim, int order, int nvar, int nobs, long ncells, const double* luh,
+                                       double* obs_min, double* obs_max, void* stream);
+/* findCellLocalLimiterMinAndMax (Limiter.cpp:170-207) over the interior of
+ * lim, written to every face block (determineLimiterMinAndMax,
+ * LimitingADERDGSolver.cpp:1118-1150). */
+exa_status_t exa_limiter_fv_min_max(int dim, int order, int nvar, int nobs, int ghost_layer_width, long ncells,
+                                    const double* lim, double* obs_min, double* obs_max, void* stream);
+/* discreteMaximumPrincipleAndMinAndMaxSearch (Limiter.cpp:113-167): on
+ * entry obs_min/obs_max hold the bounds merged from the neighbours per
+ * face; dmp_ok[cell] = 1 if every observable of the new solution stays
+ * within [min - d, max + d], d = max(relaxation, difference_scaling (max -
+ * min)); face block 0 receives the new cell extrema, face block 1 the
+ * merged bounds (as in the reference).  nobs >= 1. */
+exa_status_t exa_limiter_dmp(int dim, int order, int nvar, int nobs, long ncells, const double* luh,
+                             double relaxation, double difference_scaling, double* obs_min, double* obs_max,
+                             int* dmp_ok, void* stream);
+
+/* Per-cell drop-ins with the reference's argument lists (HOST pointers,
+ * synchronous; the limiter kernels take the dimension from the build, here
+ * it is an argument). */
+exa_status_t exa_limiter_projectOnFVLimiterSpace(int dim, const double* luh, int numberOfVariables,
+                                                 int basisSize, int ghostLayerWidth, double* lim);
+exa_status_t exa_limiter_projectOnDGSpace(int dim, const double* lim, int numberOfVariables, int basisSize,
+                                          int ghostLayerWidth, double* luh);
+exa_status_t exa_limiter_findCellLocalMinAndMax(int dim, const double* luh, int numberOfVariables,
+                                                int basisSize, int numberOfObservables,
+                                                double* localMinPerObservable, double* localMaxPerObservable);
+exa_status_t exa_limiter_discreteMaximumPrincipleAndMinAndMaxSearch(
+    int dim, const double* luh, int numberOfVariables, int basisSize, int numberOfObservables,
+    double relaxationParameter, double differenceScaling, double* boundaryMinPerObservable,
+    double* boundaryMaxPerObservable, int* discreteMaximumPrincipleSatisfied);
+
 /* ---- Slab decomposition of one grid over several GPUs ----
  * The reference distributes its spacetree over MPI ranks inside Peano: per
  * remote face, ADERDGSolver::sendDataToNeighbour (exahype/solvers/
