@@ -303,6 +303,12 @@ def main():
         else:
             dist.init_process_group('gloo', timeout=datetime.timedelta(seconds=600))
 
+    if args.impl == 'ours':
+        import exahype_b200 as E
+        E.lib().exa_set_device(local)
+        for kv in args.tune:
+            k, v = kv.split('=')
+            E._lib.call('exa_tune_set', int(k), int(v))
     if args.workload == 'ensemble':
         run_ensemble(args, rank, world, dist)
         return
@@ -327,9 +333,6 @@ def main():
 
     import exahype_b200 as E
     E.lib().exa_set_device(local)
-    for kv in args.tune:
-        k, v = kv.split('=')
-        E._lib.call('exa_tune_set', int(k), int(v))
     import ctypes as C
     fp64_peak = C.c_double()
     E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))

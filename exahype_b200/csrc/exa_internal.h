@@ -8,7 +8,14 @@
 namespace exa {
 
 // Process-wide tuning knobs (set through exa_tune_set, read by launchers).
-enum TuneKey { kTuneMixedOccupancy = 0, kTuneFp64Occupancy = 1, kTuneMixedVariant = 2, kTuneFp64Variant = 3, kTuneCount = 8 };
+enum TuneKey {
+  kTuneMixedOccupancy = 0,
+  kTuneFp64Occupancy = 1,
+  kTuneMixedVariant = 2,
+  kTuneFp64Variant = 3,
+  kTuneLimiterCellsPerCta = 4,
+  kTuneCount = 8
+};
 int tune_get(int key, int dflt);
 
 // Records a CUDA error (message retrievable by exa_last_error_string) and

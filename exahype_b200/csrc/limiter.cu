@@ -56,19 +56,29 @@ __device__ __forceinline__ double lim_coef(int p, int m) {
   return c_lim[B - 1].lim2uh[p][m];
 }
 
+// std::min / std::max semantics: (b < a) ? b : a and (a < b) ? b : a
+__device__ __forceinline__ double lim_min(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double lim_max(double a, double b) { return a < b ? b : a; }
+
 // One 1D pass: applies table TAB (NI inputs -> NO outputs, T[p][m]) along
 // direction D of a point array of extents EX x EY x EZ (x fastest), for
 // `ncell` cells and variables v < nv.  Input point p of cell c starts at
-// in + c * cs_in + p * ps_in.  out.put(c, x, y, z, v, value) receives every
-// output (with the D coordinate replaced by the output index);
-// out.line_done(item) closes each line.
+// in + c * cs_in + p * ps_in.  Each thread takes (cell, line, variable)
+// items, the variable fastest, starting with item (threadIdx.x - t0) mod NT
+// (t0 lets a pass continue where the previous pass of the same phase left
+// the threads); it hands the inputs and the NO outputs of its line to
+// out.line<D>(c, x, y, z, v, inputs, outputs, item) with the D coordinate
+// of (x, y, z) 0.  Strides and counts are plain ints: with the variable
+// count a compile-time constant in the caller they fold into immediate
+// offsets.
 template <int TAB, int B, int EX, int EY, int EZ, int D, int NO, class Out>
-__device__ __forceinline__ void lim_pass(const double* in, int ps_in, int cs_in, int ncell, int nv, Out& out) {
+__device__ __forceinline__ void lim_pass(const double* in, int ps_in, int cs_in, int ncell, int nv, Out& out,
+                                         int t0 = 0) {
   constexpr int NI = D == 0 ? EX : (D == 1 ? EY : EZ);
   constexpr int LINES = EX * EY * EZ / NI;
   constexpr int SD = D == 0 ? 1 : (D == 1 ? EX : EX * EY);
   const int items = ncell * LINES * nv;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
+  for (int it = (threadIdx.x + kLimNT - t0 % kLimNT) % kLimNT; it < items; it += kLimNT) {
     const int v = it % nv;
     const int line = (it / nv) % LINES;
     const int c = it / (nv * LINES);
@@ -87,87 +97,126 @@ __device__ __forceinline__ void lim_pass(const double* in, int ps_in, int cs_in,
     double a[NI];
 #pragma unroll
     for (int p = 0; p < NI; p++) a[p] = src[p * SD * ps_in];
+    double o[NO];
 #pragma unroll
     for (int m = 0; m < NO; m++) {
       double acc = 0.0;
 #pragma unroll
       for (int p = 0; p < NI; p++) acc = fma(lim_coef<TAB, B>(p, m), a[p], acc);
-      if (D == 0) out.put(c, m, y, z, v, acc);
-      else if (D == 1) out.put(c, x, m, z, v, acc);
-      else out.put(c, x, y, m, v, acc);
+      o[m] = acc;
     }
-    out.line_done(it);
+    out.template line<D, NI, NO>(c, x, y, z, v, a, o, it);
   }
 }
 
-// writes a pass's outputs to a shared-memory array of extents OX x OY x OZ
+// writes a pass's outputs to a shared-memory array of extents ox x oy x .
 struct SmemOut {
   double* base;
   int ps, cs, ox, oy;
-  __device__ __forceinline__ void put(int c, int x, int y, int z, int v, double val) {
-    base[c * cs + ((z * oy + y) * ox + x) * ps + v] = val;
+  template <int D, int NI, int NO>
+  __device__ __forceinline__ void line(int c, int x, int y, int z, int v, const double (&)[NI],
+                                       const double (&o)[NO], int) {
+    double* p = base + c * cs + ((z * oy + y) * ox + x) * ps + v;
+    const int st = D == 0 ? ps : (D == 1 ? ox * ps : ox * oy * ps);
+#pragma unroll
+    for (int m = 0; m < NO; m++) p[m * st] = o[m];
   }
-  __device__ __forceinline__ void line_done(int) {}
 };
 
-// writes to the interior of ghosted global patches (or plain luh arrays)
+// writes to the interior of ghosted global patches (or plain luh arrays:
+// off = 0, ext = B)
+template <int DIM>
 struct GlobalOut {
   double* base;  // first cell of the CTA
   long cs;       // doubles per cell
-  int nvar, ext, off, dim;
-  __device__ __forceinline__ void put(int c, int x, int y, int z, int v, double val) {
-    const long p = dim == 3 ? ((long)(z + off) * ext + (y + off)) * ext + (x + off)
-                            : (long)(y + off) * ext + (x + off);
-    base[c * cs + p * nvar + v] = val;
+  int nvar, ext, off;
+  template <int D, int NI, int NO>
+  __device__ __forceinline__ void line(int c, int x, int y, int z, int v, const double (&)[NI],
+                                       const double (&o)[NO], int) {
+    const long pt = DIM == 3 ? ((long)(z + off) * ext + (y + off)) * ext + (x + off) : (long)(y + off) * ext + (x + off);
+    double* p = base + c * cs + pt * nvar + v;
+    const long st = (D == 0 ? 1L : (D == 1 ? (long)ext : (long)ext * ext)) * nvar;
+#pragma unroll
+    for (int m = 0; m < NO; m++) p[m * st] = o[m];
   }
-  __device__ __forceinline__ void line_done(int) {}
 };
 
-// running min/max of the outputs of a line, stored per item at its end
+// extrema of the outputs of a line, stored per item
 struct MinMaxOut {
   double* pmn;
   double* pmx;
-  double mn = DBL_MAX, mx = -DBL_MAX;
-  __device__ __forceinline__ void put(int, int, int, int, int, double val) {
-    mn = fmin(mn, val);
-    mx = fmax(mx, val);
-  }
-  __device__ __forceinline__ void line_done(int it) {
+  template <int D, int NI, int NO>
+  __device__ __forceinline__ void line(int, int, int, int, int, const double (&)[NI], const double (&o)[NO],
+                                       int it) {
+    double mn = o[0], mx = o[0];
+#pragma unroll
+    for (int m = 1; m < NO; m++) {
+      mn = lim_min(mn, o[m]);
+      mx = lim_max(mx, o[m]);
+    }
     pmn[it] = mn;
     pmx[it] = mx;
-    mn = DBL_MAX;
-    mx = -DBL_MAX;
+  }
+};
+
+// a shared-memory store plus the extrema of the pass's INPUT line (the
+// nodes themselves, seen by the first pass over luh)
+struct SmemOutInputMinMax {
+  SmemOut s;
+  double* pmn;
+  double* pmx;
+  template <int D, int NI, int NO>
+  __device__ __forceinline__ void line(int c, int x, int y, int z, int v, const double (&a)[NI],
+                                       const double (&o)[NO], int it) {
+    s.line<D, NI, NO>(c, x, y, z, v, a, o, it);
+    double mn = a[0], mx = a[0];
+#pragma unroll
+    for (int p = 1; p < NI; p++) {
+      mn = lim_min(mn, a[p]);
+      mx = lim_max(mx, a[p]);
+    }
+    pmn[it] = mn;
+    pmx[it] = mx;
   }
 };
 
 // cooperative copy of `n` doubles (global -> shared)
 __device__ __forceinline__ void lim_copy_in(double* dst, const double* src, long n) {
-  for (long i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  for (long i = threadIdx.x; i < n; i += kLimNT) dst[i] = src[i];
 }
+
+template <int B>
+struct LimOcc {
+  // resident CTAs per SM the kernels are compiled for (register budget of
+  // 64 / 85 / 255 per thread: the least that compiles without spills)
+  static constexpr int value = B <= 4 ? 4 : (B == 5 ? 3 : 1);
+};
 
 // ------------------------------------------------------------ DG -> FV
-// shared memory per cell (doubles): luh, pass-x result, pass-y result (3D)
+// shared memory per cell (doubles per variable): luh, pass-x and pass-y
+// results (3D)
 template <int DIM, int B>
 __host__ __device__ constexpr int lim_to_fv_cell_doubles_per_var() {
-  return DIM == 3 ? B * B * B + B * B * (2 * B - 1) + B * (2 * B - 1) * (2 * B - 1)
-                  : B * B + B * (2 * B - 1);
+  return DIM == 3 ? B * B * B + B * B * (2 * B - 1) + B * (2 * B - 1) * (2 * B - 1) : B * B + B * (2 * B - 1);
 }
 
-template <int DIM, int B>
-__global__ void __launch_bounds__(kLimNT) k_lim_to_fv(int nvar, int ghost, long ncells, int cpb, const double* luh,
-                                                      double* lim) {
+// NVT: the variable count when known at compile time (0 = runtime nvar)
+template <int DIM, int B, int NVT>
+__global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
+    k_lim_to_fv(int nvar_rt, int ghost, long ncells, int cpb, const double* luh, double* lim) {
   constexpr int S = 2 * B - 1;
+  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
+  const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
   const int nc = (int)min((long)cpb, ncells - c0);
-  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
   const int SG = S + 2 * ghost;
   const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
   double* A = sm;
   double* T1 = A + cpb * NPC * nvar;
   lim_copy_in(A, luh + c0 * NPC * nvar, (long)nc * NPC * nvar);
   __syncthreads();
-  GlobalOut go{lim + c0 * lim_cell, lim_cell, nvar, SG, ghost, DIM};
+  GlobalOut<DIM> go{lim + c0 * lim_cell, lim_cell, nvar, SG, ghost};
   if (DIM == 2) {
     SmemOut o1{T1, nvar, S * B * nvar, S, B};
     lim_pass<kTabUh2Lim, B, B, B, 1, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
@@ -186,56 +235,70 @@ __global__ void __launch_bounds__(kLimNT) k_lim_to_fv(int nvar, int ghost, long 
 }
 
 // interior subcells of nc ghosted patches -> shared [c][z][y][x][nvar]
-// (rows of S * nvar contiguous doubles)
+// (rows of S * nvar contiguous doubles); each thread keeps four loads in
+// flight before it stores them
 template <int DIM, int S>
-__device__ __forceinline__ void lim_stage_interior(double* A, const double* lim, long lim_cell, int nvar, int ghost,
-                                                   int nc) {
+__device__ __forceinline__ void lim_stage_interior(double* A, const double* __restrict__ lim, long lim_cell, int nvar,
+                                                   int ghost, int nc) {
   const int SG = S + 2 * ghost;
   const int rowlen = S * nvar;
   constexpr int rows = DIM == 3 ? S * S : S;
-  const long total = (long)nc * rows * rowlen;
-  for (long i = threadIdx.x; i < total; i += blockDim.x) {
-    const int k = (int)(i % rowlen);
-    const long r = i / rowlen;
-    const int row = (int)(r % rows);
-    const long c = r / rows;
-    const int yy = row % S, zz = row / S;
-    const long p = DIM == 3 ? ((long)(zz + ghost) * SG + (yy + ghost)) * SG + ghost : (long)(yy + ghost) * SG + ghost;
-    A[(c * rows + row) * rowlen + k] = lim[c * lim_cell + p * nvar + k];
+  constexpr int U = 4;
+  const int total = nc * rows * rowlen;
+  for (int i0 = threadIdx.x; i0 < total; i0 += U * kLimNT) {
+    double r[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int i = i0 + u * kLimNT;
+      if (i < total) {
+        const int k = i % rowlen;
+        const int q = i / rowlen;
+        const int row = q % rows;
+        const int c = q / rows;
+        const int yy = row % S, zz = row / S;
+        const long p = DIM == 3 ? ((long)(zz + ghost) * SG + (yy + ghost)) * SG + ghost : (long)(yy + ghost) * SG + ghost;
+        r[u] = __ldg(lim + c * lim_cell + p * nvar + k);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (i0 + u * kLimNT < total) A[i0 + u * kLimNT] = r[u];
   }
 }
 
 // ------------------------------------------------------------ FV -> DG
+// shared memory per cell (doubles per variable): the staged subcells (later
+// reused for the pass-y result) and the pass-x result
 template <int DIM, int B>
 __host__ __device__ constexpr int lim_to_dg_cell_doubles_per_var() {
-  return DIM == 3 ? (2 * B - 1) * (2 * B - 1) * (2 * B - 1) + (2 * B - 1) * (2 * B - 1) * B +
-                        (2 * B - 1) * B * B
+  return DIM == 3 ? (2 * B - 1) * (2 * B - 1) * (2 * B - 1) + (2 * B - 1) * (2 * B - 1) * B
                   : (2 * B - 1) * (2 * B - 1) + (2 * B - 1) * B;
 }
 
-template <int DIM, int B>
-__global__ void __launch_bounds__(kLimNT) k_lim_to_dg(int nvar, int ghost, long ncells, int cpb, const double* lim,
-                                                      double* luh) {
+template <int DIM, int B, int NVT>
+__global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
+    k_lim_to_dg(int nvar_rt, int ghost, long ncells, int cpb, const double* lim, double* luh) {
   constexpr int S = 2 * B - 1;
+  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
+  constexpr int NS = DIM == 3 ? S * S * S : S * S;
+  const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
   const int nc = (int)min((long)cpb, ncells - c0);
-  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
-  constexpr int NS = DIM == 3 ? S * S * S : S * S;
   const int SG = S + 2 * ghost;
   const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
   double* A = sm;  // interior subcells [c][z][y][x][v]
   double* T1 = A + cpb * NS * nvar;
   lim_stage_interior<DIM, S>(A, lim + c0 * lim_cell, lim_cell, nvar, ghost, nc);
   __syncthreads();
-  GlobalOut go{luh + c0 * NPC * nvar, (long)NPC * nvar, nvar, B, 0, DIM};
+  GlobalOut<DIM> go{luh + c0 * NPC * nvar, (long)NPC * nvar, nvar, B, 0};
   if (DIM == 2) {
     SmemOut o1{T1, nvar, S * B * nvar, B, S};
     lim_pass<kTabLim2Uh, B, S, S, 1, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
     __syncthreads();
     lim_pass<kTabLim2Uh, B, B, S, 1, 1, B>(T1, nvar, S * B * nvar, nc, nvar, go);
   } else {
-    double* T2 = T1 + cpb * S * S * B * nvar;
+    double* T2 = A;  // the staged subcells are dead after pass x
     SmemOut o1{T1, nvar, S * S * B * nvar, B, S};
     lim_pass<kTabLim2Uh, B, S, S, S, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
     __syncthreads();
@@ -247,97 +310,106 @@ __global__ void __launch_bounds__(kLimNT) k_lim_to_dg(int nvar, int ghost, long 
 }
 
 // ------------------------------------------------ min/max and the DMP
-// Per cell: luh (nvar per point) + two scratch arrays for the observables +
-// per-line partial extrema of the two final passes.
+// The Gauss-Lobatto (B -> B) and subcell (B -> S) evaluations run side by
+// side, pass by pass; the first pass also takes the extrema of the nodes
+// (its input lines).  Per cell and observable, shared memory holds: the
+// pass-x results of both (B^3 + B^2 S), the pass-y result of the subcells
+// (B S^2) and of the Lobatto points (B^3, in the luh staging area, dead after
+// pass x), and the per-line extrema of nodes, Lobatto points and subcells.
 template <int DIM, int B>
-__host__ __device__ constexpr int lim_mm_scratch_per_obs() {
-  // pass-x and pass-y results of the subcell projection (the larger one)
-  return DIM == 3 ? B * B * (2 * B - 1) + B * (2 * B - 1) * (2 * B - 1) : B * (2 * B - 1);
-}
-template <int DIM, int B>
-__host__ __device__ constexpr int lim_mm_lines() {
-  // final-pass lines: Gauss-Lobatto (B^(dim-1)) + subcells (S^(dim-1))
-  return DIM == 3 ? B * B + (2 * B - 1) * (2 * B - 1) : B + (2 * B - 1);
-}
-
-// Projects the observables of the staged cells with table TAB (B -> NO per
-// direction); the extrema of every final-pass line land in pmn/pmx[item].
-template <int DIM, int B, int TAB, int NO>
-__device__ __forceinline__ void lim_mm_project(const double* A, int nvar, int nobs, int nc, double* T1, double* T2,
-                                               double* pmn, double* pmx) {
-  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
-  MinMaxOut mm{pmn, pmx};
-  if (DIM == 2) {
-    SmemOut o1{T1, nobs, NO * B * nobs, NO, B};
-    lim_pass<TAB, B, B, B, 1, 0, NO>(A, nvar, NPC * nvar, nc, nobs, o1);
-    __syncthreads();
-    lim_pass<TAB, B, NO, B, 1, 1, NO>(T1, nobs, NO * B * nobs, nc, nobs, mm);
-  } else {
-    SmemOut o1{T1, nobs, B * B * NO * nobs, NO, B};
-    lim_pass<TAB, B, B, B, B, 0, NO>(A, nvar, NPC * nvar, nc, nobs, o1);
-    __syncthreads();
-    SmemOut o2{T2, nobs, B * NO * NO * nobs, NO, NO};
-    lim_pass<TAB, B, NO, B, B, 1, NO>(T1, nobs, B * B * NO * nobs, nc, nobs, o2);
-    __syncthreads();
-    lim_pass<TAB, B, NO, NO, B, 2, NO>(T2, nobs, B * NO * NO * nobs, nc, nobs, mm);
+struct LimMM {
+  static constexpr int S = 2 * B - 1;
+  static constexpr int NPC = DIM == 3 ? B * B * B : B * B;
+  static constexpr int XL = DIM == 3 ? B * B * B : B * B;  // Lobatto pass-x result
+  static constexpr int XS = DIM == 3 ? B * B * S : B * S;  // subcell pass-x result
+  static constexpr int YS = DIM == 3 ? B * S * S : 0;      // subcell pass-y result
+  static constexpr int NODE_LINES = DIM == 3 ? B * B : B;  // pass-x lines
+  static constexpr int LOB_LINES = DIM == 3 ? B * B : B;   // final Lobatto lines
+  static constexpr int SUB_LINES = DIM == 3 ? S * S : S;   // final subcell lines
+  static constexpr int LINES = NODE_LINES + LOB_LINES + SUB_LINES;
+  // doubles per cell
+  __host__ __device__ static constexpr int doubles(int nvar, int nobs) {
+    return NPC * nvar + (XL + XS + YS + 2 * LINES) * nobs;
   }
-  __syncthreads();
-}
+};
 
 // mode 0: findCellLocalMinAndMax, result copied to all faces;
 // mode 1: discreteMaximumPrincipleAndMinAndMaxSearch (obs_min/max in/out,
 //         dmp_ok[cell] = 1 if the DMP holds).
-template <int DIM, int B>
-__global__ void __launch_bounds__(kLimNT) k_lim_min_max(int mode, int nvar, int nobs, long ncells, int cpb,
-                                                        const double* luh, double relaxation, double scaling,
-                                                        double* obs_min, double* obs_max, int* dmp_ok) {
-  constexpr int S = 2 * B - 1;
-  constexpr int NPC = DIM == 3 ? B * B * B : B * B;
-  constexpr int LOB_LINES = DIM == 3 ? B * B : B;
-  constexpr int SUB_LINES = DIM == 3 ? S * S : S;
-  constexpr int LINES = LOB_LINES + SUB_LINES;
-  constexpr int NF = 2 * DIM;
+template <int DIM, int B, int NVT>
+__global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
+    k_lim_min_max(int mode, int nvar_rt, int nobs_rt, long ncells, int cpb, const double* luh, double relaxation,
+                  double scaling, double* obs_min, double* obs_max, int* dmp_ok) {
+  using M = LimMM<DIM, B>;
+  constexpr int S = M::S, NPC = M::NPC, NF = 2 * DIM;
+  const int nvar = NVT ? NVT : nvar_rt;
+  const int nobs = NVT ? NVT : nobs_rt;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
   const int nc = (int)min((long)cpb, ncells - c0);
-  double* A = sm;
-  double* T1 = A + cpb * NPC * nvar;
-  double* T2 = T1 + cpb * (DIM == 3 ? B * B * S : B * S) * nobs;
-  double* pmn = T1 + cpb * lim_mm_scratch_per_obs<DIM, B>() * nobs;  // [c][LINES][nobs]
-  double* pmx = pmn + cpb * LINES * nobs;
+  double* A = sm;                         // luh, later the Lobatto pass-y result
+  double* XL = A + cpb * NPC * nvar;      // [c][z][y][x][obs]
+  double* XS = XL + cpb * M::XL * nobs;
+  double* YS = XS + cpb * M::XS * nobs;
+  double* pmn = YS + cpb * M::YS * nobs;  // [node | lob | sub lines]
+  double* pmx = pmn + cpb * M::LINES * nobs;
+  double* pn_mn = pmn;                    // node lines   [c][line][obs]
+  double* pl_mn = pmn + cpb * M::NODE_LINES * nobs;
+  double* ps_mn = pl_mn + cpb * M::LOB_LINES * nobs;
+  double* pn_mx = pmx;
+  double* pl_mx = pmx + cpb * M::NODE_LINES * nobs;
+  double* ps_mx = pl_mx + cpb * M::LOB_LINES * nobs;
   if (mode == 1)
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) dmp_ok[c0 + c] = 1;
+    for (int c = threadIdx.x; c < nc; c += kLimNT) dmp_ok[c0 + c] = 1;
   lim_copy_in(A, luh + c0 * NPC * nvar, (long)nc * NPC * nvar);
   __syncthreads();
-  // line extrema: Gauss-Lobatto lines in [0, cpb LOB_LINES nobs), subcell
-  // lines after them (items numbered (cell, line, observable))
-  lim_mm_project<DIM, B, kTabUh2Lob, B>(A, nvar, nobs, nc, T1, T2, pmn, pmx);
-  lim_mm_project<DIM, B, kTabUh2Lim, S>(A, nvar, nobs, nc, T1, T2, pmn + cpb * LOB_LINES * nobs,
-                                         pmx + cpb * LOB_LINES * nobs);
-  // reduction: one warp per (cell, observable)
+  const int ix = nc * M::NODE_LINES * nobs;  // items of one pass-x
+  if (DIM == 2) {
+    SmemOutInputMinMax ol{{XL, nobs, B * B * nobs, B, B}, pn_mn, pn_mx};
+    lim_pass<kTabUh2Lob, B, B, B, 1, 0, B>(A, nvar, NPC * nvar, nc, nobs, ol);
+    SmemOut os{XS, nobs, S * B * nobs, S, B};
+    lim_pass<kTabUh2Lim, B, B, B, 1, 0, S>(A, nvar, NPC * nvar, nc, nobs, os, ix);
+    __syncthreads();
+    MinMaxOut ml{pl_mn, pl_mx}, ms{ps_mn, ps_mx};
+    lim_pass<kTabUh2Lob, B, B, B, 1, 1, B>(XL, nobs, B * B * nobs, nc, nobs, ml);
+    lim_pass<kTabUh2Lim, B, S, B, 1, 1, S>(XS, nobs, S * B * nobs, nc, nobs, ms, nc * B * nobs);
+  } else {
+    SmemOutInputMinMax ol{{XL, nobs, B * B * B * nobs, B, B}, pn_mn, pn_mx};
+    lim_pass<kTabUh2Lob, B, B, B, B, 0, B>(A, nvar, NPC * nvar, nc, nobs, ol);
+    SmemOut os{XS, nobs, B * B * S * nobs, S, B};
+    lim_pass<kTabUh2Lim, B, B, B, B, 0, S>(A, nvar, NPC * nvar, nc, nobs, os, ix);
+    __syncthreads();
+    double* YL = A;  // luh is dead after pass x
+    SmemOut yl{YL, nobs, B * B * B * nobs, B, B};
+    lim_pass<kTabUh2Lob, B, B, B, B, 1, B>(XL, nobs, B * B * B * nobs, nc, nobs, yl);
+    SmemOut ys{YS, nobs, B * S * S * nobs, S, S};
+    lim_pass<kTabUh2Lim, B, S, B, B, 1, S>(XS, nobs, B * B * S * nobs, nc, nobs, ys, nc * B * B * nobs);
+    __syncthreads();
+    MinMaxOut ml{pl_mn, pl_mx}, ms{ps_mn, ps_mx};
+    lim_pass<kTabUh2Lob, B, B, B, B, 2, B>(YL, nobs, B * B * B * nobs, nc, nobs, ml);
+    lim_pass<kTabUh2Lim, B, S, S, B, 2, S>(YS, nobs, B * S * S * nobs, nc, nobs, ms, nc * B * B * nobs);
+  }
+  __syncthreads();
+  // reduction: one warp per (cell, observable) over its line extrema
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  for (int pair = warp; pair < nc * nobs; pair += blockDim.x / 32) {
+  for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
     const int c = pair / nobs, v = pair % nobs;
     double mn = DBL_MAX, mx = -DBL_MAX;
-    for (int p = lane; p < NPC; p += 32) {
-      const double q = A[(c * NPC + p) * nvar + v];
-      mn = fmin(mn, q);
-      mx = fmax(mx, q);
-    }
-    for (int l = lane; l < LOB_LINES; l += 32) {
-      const int k = (c * LOB_LINES + l) * nobs + v;
-      mn = fmin(mn, pmn[k]);
-      mx = fmax(mx, pmx[k]);
-    }
-    for (int l = lane; l < SUB_LINES; l += 32) {
-      const int k = cpb * LOB_LINES * nobs + (c * SUB_LINES + l) * nobs + v;
-      mn = fmin(mn, pmn[k]);
-      mx = fmax(mx, pmx[k]);
+    for (int l = lane; l < M::LINES; l += 32) {
+      int k;
+      if (l < M::NODE_LINES) k = (c * M::NODE_LINES + l) * nobs + v;
+      else if (l < M::NODE_LINES + M::LOB_LINES)
+        k = cpb * M::NODE_LINES * nobs + (c * M::LOB_LINES + l - M::NODE_LINES) * nobs + v;
+      else
+        k = cpb * (M::NODE_LINES + M::LOB_LINES) * nobs +
+            (c * M::SUB_LINES + l - M::NODE_LINES - M::LOB_LINES) * nobs + v;
+      mn = lim_min(mn, pmn[k]);
+      mx = lim_max(mx, pmx[k]);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = lim_min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      mx = lim_max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
     if (lane != 0) continue;
     double* bmn = obs_min + (c0 + c) * NF * nobs;
@@ -350,10 +422,10 @@ __global__ void __launch_bounds__(kLimNT) k_lim_min_max(int mode, int nvar, int 
     } else {
       double lo = bmn[v], hi = bmx[v];
       for (int f = 1; f < NF; f++) {
-        lo = fmin(lo, bmn[f * nobs + v]);
-        hi = fmax(hi, bmx[f * nobs + v]);
+        lo = lim_min(lo, bmn[f * nobs + v]);
+        hi = lim_max(hi, bmx[f * nobs + v]);
       }
-      const double sd = fmax((hi - lo) * scaling, relaxation);
+      const double sd = lim_max((hi - lo) * scaling, relaxation);
       if (mn < lo - sd || mx > hi + sd) atomicAnd(dmp_ok + c0 + c, 0);
       bmn[v] = mn;
       bmx[v] = mx;
@@ -378,18 +450,18 @@ __global__ void __launch_bounds__(kLimNT) k_lim_fv_min_max(int nvar, int nobs, i
   lim_stage_interior<DIM, S>(sm, lim + c0 * lim_cell, lim_cell, nvar, ghost, nc);
   __syncthreads();
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  for (int pair = warp; pair < nc * nobs; pair += blockDim.x / 32) {
+  for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
     const int c = pair / nobs, v = pair % nobs;
     double mn = DBL_MAX, mx = -DBL_MAX;
     for (int p = lane; p < NS; p += 32) {
       const double q = sm[((long)c * NS + p) * nvar + v];
-      mn = fmin(mn, q);
-      mx = fmax(mx, q);
+      mn = lim_min(mn, q);
+      mx = lim_max(mx, q);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = lim_min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+      mx = lim_max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
     if (lane == 0)
       for (int f = 0; f < 2 * DIM; f++) {
@@ -399,17 +471,13 @@ __global__ void __launch_bounds__(kLimNT) k_lim_fv_min_max(int nvar, int nobs, i
   }
 }
 
-template <int DIM, int B>
-__host__ __device__ constexpr int lim_mm_doubles(int nvar, int nobs) {
-  return (DIM == 3 ? B * B * B : B * B) * nvar + (lim_mm_scratch_per_obs<DIM, B>() + 2 * lim_mm_lines<DIM, B>()) * nobs;
-}
-
-// cells per CTA: enough final-pass items for two rounds of the CTA's
-// threads, within the shared-memory budget
-static int lim_cpb(long items_per_cell, long smem_per_cell, long ncells) {
+// cells per CTA: enough items for two rounds of the final pass, within a
+// shared-memory budget that leaves room for `occ` resident CTAs per SM
+static int lim_cpb(long items_per_cell, long smem_per_cell, long ncells, int occ) {
   long cpb = (2 * kLimNT + items_per_cell - 1) / items_per_cell;
   if (cpb > 64) cpb = 64;
-  const long cap = kLimMaxSmem / smem_per_cell;
+  long cap = (220L * 1024 / occ) / smem_per_cell;
+  if (cap < 1) cap = 1;
   if (cpb > cap) cpb = cap;
   if (cpb > ncells) cpb = ncells;
   return (int)(cpb < 1 ? 1 : cpb);
@@ -417,7 +485,12 @@ static int lim_cpb(long items_per_cell, long smem_per_cell, long ncells) {
 
 enum LimOp { kLimToFv = 0, kLimToDg = 1, kLimMinMax = 2, kLimDmp = 3, kLimFvMinMax = 4 };
 
-template <int DIM, int B>
+template <class K>
+static cudaError_t lim_prepare(K kern, size_t smem) {
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <int DIM, int B, int NVT>
 static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, const double* in, double* out,
                             double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st) {
   constexpr int S = 2 * B - 1;
@@ -432,35 +505,49 @@ static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, 
     per_cell = (long)(DIM == 3 ? S * S * S : S * S) * nvar;
     items = 32L * nobs;
   } else {
-    per_cell = lim_mm_doubles<DIM, B>(nvar, nobs);
-    items = (long)lim_mm_lines<DIM, B>() * nobs;
+    per_cell = LimMM<DIM, B>::doubles(nvar, nobs);
+    items = (long)LimMM<DIM, B>::SUB_LINES * nobs;
   }
   per_cell *= (long)sizeof(double);
   if (per_cell > kLimMaxSmem) return set_error(EXA_EINVAL, "limiter: cell too large for shared memory");
-  const int cpb = lim_cpb(items, per_cell, ncells);
+  int cpb = lim_cpb(items, per_cell, ncells, LimOcc<B>::value);
+  const int cpb_set = tune_get(kTuneLimiterCellsPerCta, 0);
+  if (cpb_set > 0 && (long)cpb_set * per_cell <= kLimMaxSmem) cpb = cpb_set;
   const size_t smem = (size_t)cpb * per_cell;
   const long nblk = (ncells + cpb - 1) / cpb;
   if (nblk > 0x7fffffffL) return set_error(EXA_EINVAL, "limiter: too many cells");
   cudaError_t e = cudaSuccess;
   if (op == kLimToFv) {
-    e = cudaFuncSetAttribute(k_lim_to_fv<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_lim_to_fv<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
+    e = lim_prepare(k_lim_to_fv<DIM, B, NVT>, smem);
+    if (e == cudaSuccess)
+      k_lim_to_fv<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
   } else if (op == kLimToDg) {
-    e = cudaFuncSetAttribute(k_lim_to_dg<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_lim_to_dg<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
+    e = lim_prepare(k_lim_to_dg<DIM, B, NVT>, smem);
+    if (e == cudaSuccess)
+      k_lim_to_dg<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
   } else if (op == kLimFvMinMax) {
-    e = cudaFuncSetAttribute(k_lim_fv_min_max<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = lim_prepare(k_lim_fv_min_max<DIM, B>, smem);
     if (e == cudaSuccess)
       k_lim_fv_min_max<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, nobs, ghost, ncells, cpb, in, mn, mx);
   } else {
-    e = cudaFuncSetAttribute(k_lim_min_max<DIM, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = lim_prepare(k_lim_min_max<DIM, B, NVT>, smem);
     if (e == cudaSuccess)
-      k_lim_min_max<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(op == kLimDmp ? 1 : 0, nvar, nobs, ncells, cpb, in,
-                                                                   relax, scaling, mn, mx, ok);
+      k_lim_min_max<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(op == kLimDmp ? 1 : 0, nvar, nobs, ncells,
+                                                                       cpb, in, relax, scaling, mn, mx, ok);
   }
   if (e != cudaSuccess) return cuda_status(e, "limiter: shared-memory attribute");
   count_launch();
   return cuda_status(cudaGetLastError(), "limiter kernel");
+}
+
+// the Euler case (5 variables, 5 observables) runs kernels specialised for
+// it; any other count the generic ones
+template <int DIM, int B>
+static exa_status_t lim_run_nv(int op, int nvar, int nobs, int ghost, long ncells, const double* in, double* out,
+                               double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st) {
+  const bool five = nvar == 5 && (op < kLimMinMax || op == kLimFvMinMax || nobs == 5);
+  if (five) return lim_run<DIM, B, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+  return lim_run<DIM, B, 0>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
 }
 
 template <int DIM>
@@ -468,12 +555,12 @@ static exa_status_t lim_dispatch(int op, int order, int nvar, int nobs, int ghos
                                  double* out, double* mn, double* mx, int* ok, double relax, double scaling,
                                  cudaStream_t st) {
   switch (order) {
-    case 1: return lim_run<DIM, 2>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 2: return lim_run<DIM, 3>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 3: return lim_run<DIM, 4>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 4: return lim_run<DIM, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 5: return lim_run<DIM, 6>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 6: return lim_run<DIM, 7>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 1: return lim_run_nv<DIM, 2>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 2: return lim_run_nv<DIM, 3>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 3: return lim_run_nv<DIM, 4>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 4: return lim_run_nv<DIM, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 5: return lim_run_nv<DIM, 6>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 6: return lim_run_nv<DIM, 7>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
   }
   return set_error(EXA_EINVAL, "limiter: order must be in 1..6");
 }

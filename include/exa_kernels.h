@@ -106,7 +106,9 @@ uint64_t exa_launch_count(void);
  * registers, the default; 4: 128 registers), 1 = the FP64 predictor's
  * (0: unconstrained; non-zero: cap for 3 CTAs/SM), 2 = contraction of the
  * mixed predictor (1: node-gather, 2: line-owner; 0: line-owner for orders
- * >= 4, node-gather otherwise), 3 = the same for the FP64 predictor.  exa_tune_get returns -1 for keys never set. */
+ * >= 4, node-gather otherwise), 3 = the same for the FP64 predictor,
+ * 4 = cells per CTA of the limiter kernels (0: automatic).  exa_tune_get
+ * returns -1 for keys never set. */
 exa_status_t exa_tune_set(int key, int value);
 int exa_tune_get(int key);
 /* FP64 FMA throughput of the current device in TFLOP/s, measured with a
