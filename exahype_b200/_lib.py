@@ -48,6 +48,12 @@ class GridConfig(C.Structure):
                 ('dt_policy', C.c_int), ('cfl', C.c_double), ('dt_fixed', C.c_double)]
 
 
+class LimiterConfig(C.Structure):
+    _fields_ = [('scheme', C.c_int), ('nobs', C.c_int), ('relaxation', C.c_double),
+                ('difference_scaling', C.c_double), ('steps_till_cured', C.c_int),
+                ('check_admissibility', C.c_int)]
+
+
 class FVDesc(C.Structure):
     _fields_ = [('dim', C.c_int), ('patch', C.c_int), ('ghost', C.c_int), ('nvar', C.c_int),
                 ('npar', C.c_int), ('pde', C.c_int), ('dx', C.c_double * 3)]
@@ -158,6 +164,9 @@ SIGNATURES = {
     'exa_limiter_findCellLocalMinAndMax': (i32, [i32, dptr, i32, i32, i32, dptr, dptr]),
     'exa_limiter_discreteMaximumPrincipleAndMinAndMaxSearch': (i32, [i32, dptr, i32, i32, i32, f64, f64, dptr, dptr,
                                                                      C.POINTER(i32)]),
+    'exa_aderdg_grid_set_limiter': (i32, [vp, vp]),
+    'exa_aderdg_grid_limiter_status': (i32, [vp, vp, vp]),
+    'exa_aderdg_grid_limiter_bounds': (i32, [vp, vp, vp]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),

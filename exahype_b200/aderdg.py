@@ -208,6 +208,36 @@ class ADERDGGrid:
         arr = (C.c_int * 3)(*(list(bc) + [0] * (3 - len(bc))))
         call('exa_aderdg_grid_set_boundary', self.h, arr)
 
+    # -- a-posteriori subcell limiter (exa_aderdg_grid_set_limiter) --
+    def set_limiter(self, scheme=0, nobs=5, relaxation=1e-4, difference_scaling=1e-3, steps_till_cured=0,
+                    check_admissibility=True, enable=True):
+        """Limiting ADER-DG (2D, periodic): DMP + admissibility check of every
+        step's DG candidate, subcell FV recomputation (scheme 0 Godunov, 1
+        MUSCL-Hancock) of troubled cells and their neighbours."""
+        if not enable:
+            call('exa_aderdg_grid_set_limiter', self.h, None)
+            self.nobs = None
+            return
+        c = _lib.LimiterConfig(int(scheme), int(nobs), float(relaxation), float(difference_scaling),
+                               int(steps_till_cured), int(bool(check_admissibility)))
+        call('exa_aderdg_grid_set_limiter', self.h, C.addressof(c))
+        self.nobs = int(nobs)
+
+    def limiter_status(self):
+        """(status per cell: Ok 0 .. Troubled 5, counts [patches, FV cells,
+        Troubled cells]) of the last step"""
+        st = np.zeros(self.ncells, dtype=np.int32)
+        counts = np.zeros(3, dtype=np.int32)
+        call('exa_aderdg_grid_limiter_status', self.h, st.ctypes.data, counts.ctypes.data)
+        return st, counts
+
+    def limiter_bounds(self):
+        """DMP bounds for the next step: (min, max), [cell][4][nobs] each"""
+        mn = np.zeros(self.ncells * 4 * self.nobs)
+        mx = np.zeros_like(mn)
+        call('exa_aderdg_grid_limiter_bounds', self.h, mn.ctypes.data, mx.ctypes.data)
+        return mn, mx
+
     # -- slab decomposition (see exahype_b200.slab) --
     def set_halo(self, enable=True):
         call('exa_aderdg_grid_set_halo', self.h, int(enable))

@@ -96,6 +96,24 @@ struct exa_aderdg_grid {
   cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
   double ms_pred = 0, ms_corr = 0;
   unsigned long long prof_steps = 0;
+  uint64_t graph_launches = 3;  // kernels in one captured step
+  // a-posteriori subcell limiter (exa_aderdg_grid_set_limiter)
+  bool lim_on = false;
+  exa_limiter_config_t lim_cfg{};
+  int lim_ghost = 0;
+  void* lim_block = nullptr;    // one allocation, carved below
+  double* lim_prev = nullptr;   // luh before the step
+  double* lim_patch = nullptr;  // subcell patches [cell][(S + 2g)^2][V]
+  double* lim_bmin = nullptr;   // [cell][4 faces][nobs]
+  double* lim_bmax = nullptr;
+  double* lim_loc = nullptr;    // [cell][min | max][nobs]
+  int* lim_ok = nullptr;        // DMP and admissibility verdict per cell
+  int* lim_status = nullptr;
+  int* lim_status_tmp = nullptr;
+  int* lim_cure = nullptr;
+  int* lim_list_patch = nullptr;
+  int* lim_list_fv = nullptr;
+  int* lim_counts = nullptr;    // patches, FV cells, Troubled cells
 };
 
 static size_t grid_sizes(const exa_aderdg_grid_config_t* c, long* ncells, size_t* n_luh,
@@ -177,9 +195,11 @@ static exa_status_t grid_correct(exa_aderdg_grid* g) {
   c.lduh = g->lduh;
   c.lQhbnd = g->qb;
   c.lFhbnd = g->fb;
-  c.dt_next = g->cfg.dt_policy == 2 ? nullptr : &g->gd->dt_next;
+  // with the limiter the candidate may be unusable in troubled cells: the
+  // next dt and the NaN check come after the limiting
+  c.dt_next = (g->cfg.dt_policy == 2 || g->lim_on) ? nullptr : &g->gd->dt_next;
   c.dt_factor = g->dt_factor;
-  c.nan_flag = &g->gd->nan_flag;
+  c.nan_flag = g->lim_on ? nullptr : &g->gd->nan_flag;
   if (g->halo) {
     c.halo_lo = g->halo + 2 * g->halo_count;
     c.halo_hi = g->halo + 3 * g->halo_count;
@@ -191,6 +211,70 @@ static exa_status_t grid_correct(exa_aderdg_grid* g) {
   return launch_corrector(g->cfg.dim, g->cfg.order, g->cfg.pde, c, g->st);
 }
 
+// The limiting part of a step (LimitingADERDGSolver: updateLimiterStatus-
+// AndMinAndMaxAfterSolutionUpdate, then the local recomputation of the
+// cells whose dominant solver is the FV solver), after the DG candidate:
+//   DMP (bounds merged from the previous step) + admissibility -> status;
+//   subcell patches of the previous solution for every cell with status >=
+//   NeighbourOfTroubled3; one FV step on the patches of the cells with status
+//   >= NeighbourOfTroubled2, projected back onto their DG polynomials;
+//   new extrema (FV patch for those cells, nodes / Lobatto points / subcells
+//   of the candidate for the others) merged over faces; the next dt from the
+//   final state.
+static exa_status_t grid_limit(exa_aderdg_grid* g) {
+  const exa_limiter_config_t& L = g->lim_cfg;
+  const int dim = g->cfg.dim, order = g->cfg.order, nobs = L.nobs;
+  const int S = 2 * order + 1, npc = (order + 1) * (order + 1);
+  const int planar = g->cfg.pde == EXA_PDE_EULER_PLANAR;
+  if (exa_status_t s = limiter_launch(kLimDmp, dim, order, kV, nobs, 0, g->ncells, g->luh, nullptr, g->lim_bmin,
+                                      g->lim_bmax, g->lim_ok, L.relaxation, L.difference_scaling, g->st, nullptr,
+                                      nullptr))
+    return s;
+  if (exa_status_t s = limiting_status(g->cfg.n[0], g->cfg.n[1], npc, planar, L.check_admissibility,
+                                       L.steps_till_cured, g->luh, g->lim_ok, g->lim_status, g->lim_status_tmp,
+                                       g->lim_cure, g->lim_list_patch, g->lim_list_fv, g->lim_counts, g->st))
+    return s;
+  if (exa_status_t s = limiter_launch(kLimToFv, dim, order, kV, 0, g->lim_ghost, g->ncells, g->lim_prev,
+                                      g->lim_patch, nullptr, nullptr, nullptr, 0, 0, g->st, g->lim_list_patch,
+                                      g->lim_counts + 0))
+    return s;
+  if (exa_status_t s = fv_subcell_step(L.scheme, planar, S, g->lim_ghost, g->cfg.n[0], g->cfg.n[1],
+                                       g->desc.dx[0] / S, g->desc.dx[1] / S, g->lim_patch, g->lim_list_fv,
+                                       g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
+    return s;
+  if (exa_status_t s = limiter_launch(kLimToDg, dim, order, kV, 0, g->lim_ghost, g->ncells, g->lim_patch, g->luh,
+                                      nullptr, nullptr, nullptr, 0, 0, g->st, g->lim_list_fv, g->lim_counts + 1))
+    return s;
+  if (exa_status_t s = limiter_launch(kLimFvMinMax, dim, order, kV, nobs, g->lim_ghost, g->ncells, g->lim_patch,
+                                      nullptr, g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, g->lim_list_fv,
+                                      g->lim_counts + 1))
+    return s;
+  if (exa_status_t s = limiting_merge_bounds(g->cfg.n[0], g->cfg.n[1], nobs, g->lim_bmin, g->lim_bmax, g->lim_loc,
+                                             g->st))
+    return s;
+  if (exa_status_t s = limiting_check_finite(npc, g->luh, g->lim_list_fv, g->lim_counts + 1, &g->gd->nan_flag, g->st))
+    return s;
+  if (g->cfg.dt_policy != 2)
+    return launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr, &g->gd->dt_next, g->st);
+  return EXA_OK;
+}
+
+// extrema of the current state merged over faces (the bounds of the first
+// DMP check), all cells Ok
+static exa_status_t grid_limiter_reset(exa_aderdg_grid* g) {
+  const int nobs = g->lim_cfg.nobs;
+  cudaError_t e = cudaMemsetAsync(g->lim_status, 0, g->ncells * sizeof(int), g->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->lim_cure, 0, g->ncells * sizeof(int), g->st);
+  if (e != cudaSuccess) return cuda_status(e, "limiter reset");
+  if (exa_status_t s = limiter_launch(kLimMinMax, g->cfg.dim, g->cfg.order, kV, nobs, 0, g->ncells, g->luh, nullptr,
+                                      g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, nullptr, nullptr))
+    return s;
+  if (exa_status_t s = limiting_merge_bounds(g->cfg.n[0], g->cfg.n[1], nobs, g->lim_bmin, g->lim_bmax, g->lim_loc,
+                                             g->st))
+    return s;
+  return cuda_status(cudaStreamSynchronize(g->st), "limiter reset");
+}
+
 static exa_status_t grid_commit(exa_aderdg_grid* g) {
   k_commit<<<1, 1, 0, g->st>>>(g->gd, g->dt_log, g->log_cap, g->cfg.dt_policy == 2, g->cfg.dt_fixed);
   count_launch();
@@ -199,9 +283,18 @@ static exa_status_t grid_commit(exa_aderdg_grid* g) {
 
 static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
   if (g->profile) cudaEventRecord(g->ev[0], g->st);
+  if (g->lim_on) {
+    long nc;
+    size_t n_luh, n_face;
+    grid_sizes(&g->cfg, &nc, &n_luh, &n_face);
+    cudaError_t e = cudaMemcpyAsync(g->lim_prev, g->luh, n_luh * sizeof(double), cudaMemcpyDeviceToDevice, g->st);
+    if (e != cudaSuccess) return cuda_status(e, "limiter: keep previous solution");
+  }
   if (exa_status_t s = grid_predict(g)) return s;
   if (g->profile) cudaEventRecord(g->ev[1], g->st);
   if (exa_status_t s = grid_correct(g)) return s;
+  if (g->lim_on)
+    if (exa_status_t s = grid_limit(g)) return s;
   if (exa_status_t s = grid_commit(g)) return s;
   if (g->profile) {
     cudaEventRecord(g->ev[2], g->st);
@@ -286,6 +379,7 @@ exa_status_t exa_aderdg_grid_destroy(exa_aderdg_grid* g) {
   cudaFree(g->gd);
   cudaFree(g->dt_log);
   cudaFree(g->halo);
+  cudaFree(g->lim_block);
   if (g->st) cudaStreamDestroy(g->st);
   delete g;
   return EXA_OK;
@@ -301,6 +395,8 @@ exa_status_t exa_aderdg_grid_init(exa_aderdg_grid* g, int kind, double param, ui
                                       param, seed, noise_amp, g->st))
     return s;
   g->primed = false;
+  if (g->lim_on)
+    if (exa_status_t s = grid_limiter_reset(g)) return s;
   return cuda_status(cudaStreamSynchronize(g->st), "grid init");
 }
 
@@ -312,6 +408,8 @@ exa_status_t exa_aderdg_grid_set_state(exa_aderdg_grid* g, const double* host_lu
   cudaError_t e = cudaMemcpyAsync(g->luh, host_luh, n_luh * sizeof(double), cudaMemcpyHostToDevice, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   g->primed = false;
+  if (e == cudaSuccess && g->lim_on)
+    if (exa_status_t s = grid_limiter_reset(g)) return s;
   return cuda_status(e, "grid set_state");
 }
 
@@ -383,7 +481,9 @@ exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_hos
     cudaGraph_t graph;
     cudaError_t e = cudaStreamBeginCapture(g->st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_status(e, "begin capture");
+    const uint64_t l0 = exa_launch_count();
     exa_status_t s = grid_launch_step(g);
+    g->graph_launches = exa_launch_count() - l0;
     e = cudaStreamEndCapture(g->st, &graph);
     if (s) return s;
     if (e != cudaSuccess) return cuda_status(e, "end capture");
@@ -395,7 +495,7 @@ exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_hos
     if (g->use_graph) {
       cudaError_t e = cudaGraphLaunch(g->graph, g->st);
       if (e != cudaSuccess) return cuda_status(e, "graph launch");
-      count_launch(3);
+      count_launch(g->graph_launches);
     } else if (exa_status_t s = grid_launch_step(g)) {
       return s;
     }
@@ -448,12 +548,97 @@ exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc) {
     if (bc[i] < EXA_BC_PERIODIC || bc[i] > EXA_BC_REFLECT) return set_error(EXA_EINVAL, "unknown boundary rule");
   if (g->halo && bc[g->cfg.dim - 1] != EXA_BC_PERIODIC)
     return set_error(EXA_EINVAL, "slab halos need a periodic last dimension");
+  if (g->lim_on)
+    for (int i = 0; i < g->cfg.dim; i++)
+      if (bc[i] != EXA_BC_PERIODIC) return set_error(EXA_EINVAL, "the limiter needs periodic boundaries");
   for (int i = 0; i < 3; i++) g->bc[i] = i < g->cfg.dim ? bc[i] : 0;
   if (g->graph) {  // the captured step holds the old arguments
     cudaGraphExecDestroy(g->graph);
     g->graph = nullptr;
   }
   return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_config_t* cfg) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (g->graph) {  // the captured step changes
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  if (!cfg) {
+    cudaStreamSynchronize(g->st);
+    cudaFree(g->lim_block);
+    g->lim_block = nullptr;
+    g->lim_on = false;
+    return EXA_OK;
+  }
+  if (g->cfg.dim != 2) return set_error(EXA_EINVAL, "limiter: 2D grids only");
+  if (g->halo) return set_error(EXA_EINVAL, "limiter: not with slab halos");
+  if (g->bc[0] != EXA_BC_PERIODIC || g->bc[1] != EXA_BC_PERIODIC)
+    return set_error(EXA_EINVAL, "limiter: periodic boundaries only");
+  if (cfg->scheme != 0 && cfg->scheme != 1) return set_error(EXA_EINVAL, "limiter: scheme must be 0 or 1");
+  if (cfg->nobs < 1 || cfg->nobs > kV) return set_error(EXA_EINVAL, "limiter: nobs must be in 1..5");
+  if (!(cfg->relaxation >= 0) || !(cfg->difference_scaling >= 0))
+    return set_error(EXA_EINVAL, "limiter: DMP parameters must not be negative");
+  if (cfg->steps_till_cured < 0) return set_error(EXA_EINVAL, "limiter: steps_till_cured must not be negative");
+  cudaStreamSynchronize(g->st);
+  cudaFree(g->lim_block);
+  g->lim_block = nullptr;
+  g->lim_on = false;
+  g->lim_cfg = *cfg;
+  g->lim_ghost = cfg->scheme == 0 ? 1 : 2;
+  const long n = g->ncells;
+  const int B = g->cfg.order + 1, SG = 2 * g->cfg.order + 1 + 2 * g->lim_ghost;
+  const size_t d_prev = (size_t)n * B * B * kV, d_patch = (size_t)n * SG * SG * kV;
+  const size_t d_b = (size_t)n * 4 * cfg->nobs, d_loc = (size_t)n * 2 * cfg->nobs;
+  const size_t doubles = d_prev + d_patch + 2 * d_b + d_loc;
+  const size_t ints = 6 * (size_t)n + 4;
+  cudaError_t e = cudaMalloc(&g->lim_block, doubles * sizeof(double) + ints * sizeof(int));
+  if (e != cudaSuccess) return cuda_status(e, "limiter allocation");
+  double* p = static_cast<double*>(g->lim_block);
+  g->lim_prev = p;
+  p += d_prev;
+  g->lim_patch = p;
+  p += d_patch;
+  g->lim_bmin = p;
+  p += d_b;
+  g->lim_bmax = p;
+  p += d_b;
+  g->lim_loc = p;
+  p += d_loc;
+  int* q = reinterpret_cast<int*>(p);
+  g->lim_ok = q;
+  g->lim_status = q + n;
+  g->lim_status_tmp = q + 2 * n;
+  g->lim_cure = q + 3 * n;
+  g->lim_list_patch = q + 4 * n;
+  g->lim_list_fv = q + 5 * n;
+  g->lim_counts = q + 6 * n;
+  e = cudaMemsetAsync(g->lim_patch, 0, d_patch * sizeof(double), g->st);
+  if (e != cudaSuccess) return cuda_status(e, "limiter allocation");
+  g->lim_on = true;
+  return grid_limiter_reset(g);
+}
+
+exa_status_t exa_aderdg_grid_limiter_status(exa_aderdg_grid* g, int* host_status, int* counts) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (!g->lim_on) return set_error(EXA_EINVAL, "limiter not enabled");
+  cudaError_t e = cudaSuccess;
+  if (host_status)
+    e = cudaMemcpyAsync(host_status, g->lim_status, g->ncells * sizeof(int), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess && counts) e = cudaMemcpyAsync(counts, g->lim_counts, 3 * sizeof(int), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "limiter status");
+}
+
+exa_status_t exa_aderdg_grid_limiter_bounds(exa_aderdg_grid* g, double* host_min, double* host_max) {
+  if (!g || !host_min || !host_max) return set_error(EXA_EINVAL, "NULL argument");
+  if (!g->lim_on) return set_error(EXA_EINVAL, "limiter not enabled");
+  const size_t bytes = (size_t)g->ncells * 4 * g->lim_cfg.nobs * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(host_min, g->lim_bmin, bytes, cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host_max, g->lim_bmax, bytes, cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "limiter bounds");
 }
 
 exa_status_t exa_aderdg_grid_set_halo(exa_aderdg_grid* g, int enable) {

@@ -123,6 +123,32 @@ exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 exa_status_t upload_tables_amr();
 exa_status_t upload_tables_limiter();
+
+// FV step (scheme 0 Godunov, 1 MUSCL-Hancock) on the subcell patches
+// lim[cell] (P subcells + g ghost layers per direction, 5 variables) of the
+// cells list[0 .. *count) of a periodic npx x npy grid: face ghosts from the
+// neighbour cells' patches, then the update in place with *dt_dev (fv.cu)
+exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int npy, double hx, double hy,
+                             double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
+                             cudaStream_t st);
+
+// limiting-grid bookkeeping (limiting.cu): status from the DMP /
+// admissibility verdicts with spreading and the cell lists; the merge of
+// the per-cell extrema over faces; a finiteness check of listed cells
+exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibility, int steps_till_cured,
+                             const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
+                             int* list_fv, int* counts, cudaStream_t st);
+exa_status_t limiting_merge_bounds(int nx, int ny, int nobs, double* bmin, double* bmax, double* loc,
+                                   cudaStream_t st);
+exa_status_t limiting_check_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag,
+                                   cudaStream_t st);
+
+// limiter kernels (limiter.cu) on all cells, or on cells list[0 .. *count)
+// when list / count (device) are given
+enum LimiterOp { kLimToFv = 0, kLimToDg = 1, kLimMinMax = 2, kLimDmp = 3, kLimFvMinMax = 4 };
+exa_status_t limiter_launch(int op, int dim, int order, int nvar, int nobs, int ghost, long ncells, const double* in,
+                            double* out, double* mn, double* mx, int* ok, double relax, double scaling,
+                            cudaStream_t st, const int* list, const int* count);
 // host copy of the derived tables (same bytes as the device constants)
 const void* host_dg_tables(size_t* bytes);
 const void* host_dg_tables_f(size_t* bytes);  // FP32 copies (DGConstF)

@@ -36,6 +36,9 @@ struct FVArgs {
   double* out;        // luh_new: updated in place (reference semantics)
   unsigned long long* max_dt;  // per patch, atomic-min bit patterns (nullable)
   unsigned long long* next_dt;  // fused steps: CFL dt of the new state (atomic min)
+  // optional patch selection of k_fv_patch_small: patches list[0 .. *count)
+  const int* list;
+  const int* count;
 };
 
 // Periodic index of a cell coordinate of a single patch with ghost width g:
@@ -1039,7 +1042,8 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
   double* wRx = wLx + R * R * V;
   double* wLy = wRx + R * R * V;
   double* wRy = wLy + R * R * V;
-  const long patch = blockIdx.x;
+  if (a.count && (int)blockIdx.x >= *a.count) return;
+  const long patch = a.list ? (long)a.list[blockIdx.x] : (long)blockIdx.x;
   const double* luh = a.luh + patch * (long)S * S * D;
   double* out = a.out + patch * (long)S * S * D;
   const int tid = threadIdx.x;
@@ -1128,12 +1132,76 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
     fv_update_store_dt<PLANAR>(a, out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
   }
   for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
-  if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
+  if ((tid & 31) == 0 && a.next_dt) atomic_min_pos_double(a.next_dt, dtn);
 }
 
 inline size_t fv_small_smem(int P, int g, int scheme) {
   const size_t S = P + 2 * g, R = P + 2;
   return sizeof(double) * (S * S * kV + (scheme == 1 ? 4 * R * R * kV : 0));
+}
+
+// Subcell patches of the limiting ADER-DG grid: patch `cell` of a periodic
+// npx x npy grid of cells.  Face ghosts of the listed patches from the face
+// neighbours' boundary layers (grid-stride over list entries x ghosts).
+__global__ void k_fv_subcell_exchange(int P, int g, int npx, int npy, double* lim, const int* list,
+                                      const int* count) {
+  const int S = P + 2 * g;
+  const long per = 4L * g * P;
+  const long total = (long)*count * per;
+  for (long gid = (long)blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += (long)gridDim.x * blockDim.x) {
+    const long patch = list[gid / per];
+    const int r = (int)(gid % per);
+    const int side = r / (g * P), i = (r / g) % P, k = r % g;
+    const int px = (int)(patch % npx), py = (int)(patch / npx);
+    int j, x, nj, nx, qx = px, qy = py;
+    if (side == 0) {
+      j = g + i; x = k; qx = (px + npx - 1) % npx; nj = j; nx = P + k;
+    } else if (side == 1) {
+      j = g + i; x = g + P + k; qx = (px + 1) % npx; nj = j; nx = g + k;
+    } else if (side == 2) {
+      j = k; x = g + i; qy = (py + npy - 1) % npy; nj = P + k; nx = x;
+    } else {
+      j = g + P + k; x = g + i; qy = (py + 1) % npy; nj = g + k; nx = x;
+    }
+    const long src_patch = (long)qy * npx + qx;
+    double* dst = lim + (patch * S * S + (long)j * S + x) * kV;
+    const double* src = lim + (src_patch * S * S + (long)nj * S + nx) * kV;
+#pragma unroll
+    for (int m = 0; m < kV; m++) dst[m] = src[m];
+  }
+}
+
+exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int npy, double hx, double hy,
+                             double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
+                             cudaStream_t st) {
+  if (P > kFvSmallMax || (scheme == 0 && g < 1) || (scheme == 1 && g < 2))
+    return set_error(EXA_EINVAL, "subcell FV: patch too large or ghost layer too thin");
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_fv_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, npx, npy, lim, list, count);
+  count_launch();
+  if (exa_status_t s = cuda_status(cudaGetLastError(), "k_fv_subcell_exchange")) return s;
+  FVArgs a{};
+  a.P = P;
+  a.g = g;
+  a.S = P + 2 * g;
+  a.hx = hx;
+  a.hy = hy;
+  a.dt_dev = dt_dev;
+  a.luh = lim;
+  a.out = lim;  // in place: each CTA stages its patch before it writes the interior
+  a.list = list;
+  a.count = count;
+  const size_t smem = fv_small_smem(P, g, scheme);
+  auto kern = scheme == 0 ? (planar ? k_fv_patch_small<true, 0> : k_fv_patch_small<false, 0>)
+                          : (planar ? k_fv_patch_small<true, 1> : k_fv_patch_small<false, 1>);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_status(e, "subcell FV attribute");
+  if (maxcells > 0x7fffffffL) return set_error(EXA_EINVAL, "subcell FV: too many cells");
+  kern<<<(unsigned)maxcells, FVS_NT, smem, st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_fv_patch_small (subcells)");
 }
 }  // namespace exa
 

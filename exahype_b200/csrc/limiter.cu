@@ -127,14 +127,17 @@ struct SmemOut {
 // off = 0, ext = B)
 template <int DIM>
 struct GlobalOut {
-  double* base;  // first cell of the CTA
+  double* base;  // cell 0 of the array
   long cs;       // doubles per cell
   int nvar, ext, off;
+  long c0;       // first cell (selection index) of the CTA
+  const int* list;
   template <int D, int NI, int NO>
   __device__ __forceinline__ void line(int c, int x, int y, int z, int v, const double (&)[NI],
                                        const double (&o)[NO], int) {
     const long pt = DIM == 3 ? ((long)(z + off) * ext + (y + off)) * ext + (x + off) : (long)(y + off) * ext + (x + off);
-    double* p = base + c * cs + pt * nvar + v;
+    const long cell = list ? (long)list[c0 + c] : c0 + c;
+    double* p = base + cell * cs + pt * nvar + v;
     const long st = (D == 0 ? 1L : (D == 1 ? (long)ext : (long)ext * ext)) * nvar;
 #pragma unroll
     for (int m = 0; m < NO; m++) p[m * st] = o[m];
@@ -192,6 +195,31 @@ struct LimOcc {
   static constexpr int value = B <= 4 ? 4 : (B == 5 ? 3 : 1);
 };
 
+// Optional cell selection: the kernels run on cells list[0 .. *count) (at
+// most ncells) instead of cells 0 .. ncells; a device-resident count lets a
+// fixed launch sequence serve a selection that changes from step to step.
+struct LimSel {
+  const int* list = nullptr;
+  const int* count = nullptr;
+  __device__ __forceinline__ long cells(long ncells) const {
+    return count ? min(ncells, (long)*count) : ncells;
+  }
+  __device__ __forceinline__ long cell(long k) const { return list ? (long)list[k] : k; }
+};
+
+// copies the selected cells' input arrays (n doubles each) to shared memory
+__device__ __forceinline__ void lim_copy_cells(double* dst, const double* src, int n, long c0, int nc,
+                                               const LimSel& sel) {
+  if (!sel.list) {
+    lim_copy_in(dst, src + c0 * n, (long)nc * n);
+    return;
+  }
+  for (int i = threadIdx.x; i < nc * n; i += kLimNT) {
+    const int c = i / n;
+    dst[i] = src[sel.cell(c0 + c) * n + (i - c * n)];
+  }
+}
+
 // ------------------------------------------------------------ DG -> FV
 // shared memory per cell (doubles per variable): luh, pass-x and pass-y
 // results (3D)
@@ -203,20 +231,22 @@ __host__ __device__ constexpr int lim_to_fv_cell_doubles_per_var() {
 // NVT: the variable count when known at compile time (0 = runtime nvar)
 template <int DIM, int B, int NVT>
 __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
-    k_lim_to_fv(int nvar_rt, int ghost, long ncells, int cpb, const double* luh, double* lim) {
+    k_lim_to_fv(int nvar_rt, int ghost, long ncells, int cpb, const double* luh, double* lim, LimSel sel) {
   constexpr int S = 2 * B - 1;
   constexpr int NPC = DIM == 3 ? B * B * B : B * B;
   const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
-  const int nc = (int)min((long)cpb, ncells - c0);
+  const long nce = sel.cells(ncells);
+  if (c0 >= nce) return;
+  const int nc = (int)min((long)cpb, nce - c0);
   const int SG = S + 2 * ghost;
   const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
   double* A = sm;
   double* T1 = A + cpb * NPC * nvar;
-  lim_copy_in(A, luh + c0 * NPC * nvar, (long)nc * NPC * nvar);
+  lim_copy_cells(A, luh, NPC * nvar, c0, nc, sel);
   __syncthreads();
-  GlobalOut<DIM> go{lim + c0 * lim_cell, lim_cell, nvar, SG, ghost};
+  GlobalOut<DIM> go{lim, lim_cell, nvar, SG, ghost, c0, sel.list};
   if (DIM == 2) {
     SmemOut o1{T1, nvar, S * B * nvar, S, B};
     lim_pass<kTabUh2Lim, B, B, B, 1, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
@@ -239,7 +269,7 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
 // flight before it stores them
 template <int DIM, int S>
 __device__ __forceinline__ void lim_stage_interior(double* A, const double* __restrict__ lim, long lim_cell, int nvar,
-                                                   int ghost, int nc) {
+                                                   int ghost, long c0, int nc, const LimSel& sel) {
   const int SG = S + 2 * ghost;
   const int rowlen = S * nvar;
   constexpr int rows = DIM == 3 ? S * S : S;
@@ -257,7 +287,7 @@ __device__ __forceinline__ void lim_stage_interior(double* A, const double* __re
         const int c = q / rows;
         const int yy = row % S, zz = row / S;
         const long p = DIM == 3 ? ((long)(zz + ghost) * SG + (yy + ghost)) * SG + ghost : (long)(yy + ghost) * SG + ghost;
-        r[u] = __ldg(lim + c * lim_cell + p * nvar + k);
+        r[u] = __ldg(lim + sel.cell(c0 + c) * lim_cell + p * nvar + k);
       }
     }
 #pragma unroll
@@ -277,21 +307,23 @@ __host__ __device__ constexpr int lim_to_dg_cell_doubles_per_var() {
 
 template <int DIM, int B, int NVT>
 __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
-    k_lim_to_dg(int nvar_rt, int ghost, long ncells, int cpb, const double* lim, double* luh) {
+    k_lim_to_dg(int nvar_rt, int ghost, long ncells, int cpb, const double* lim, double* luh, LimSel sel) {
   constexpr int S = 2 * B - 1;
   constexpr int NPC = DIM == 3 ? B * B * B : B * B;
   constexpr int NS = DIM == 3 ? S * S * S : S * S;
   const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
-  const int nc = (int)min((long)cpb, ncells - c0);
+  const long nce = sel.cells(ncells);
+  if (c0 >= nce) return;
+  const int nc = (int)min((long)cpb, nce - c0);
   const int SG = S + 2 * ghost;
   const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
   double* A = sm;  // interior subcells [c][z][y][x][v]
   double* T1 = A + cpb * NS * nvar;
-  lim_stage_interior<DIM, S>(A, lim + c0 * lim_cell, lim_cell, nvar, ghost, nc);
+  lim_stage_interior<DIM, S>(A, lim, lim_cell, nvar, ghost, c0, nc, sel);
   __syncthreads();
-  GlobalOut<DIM> go{luh + c0 * NPC * nvar, (long)NPC * nvar, nvar, B, 0};
+  GlobalOut<DIM> go{luh, (long)NPC * nvar, nvar, B, 0, c0, sel.list};
   if (DIM == 2) {
     SmemOut o1{T1, nvar, S * B * nvar, B, S};
     lim_pass<kTabLim2Uh, B, S, S, 1, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
@@ -439,15 +471,18 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
 // one warp per (cell, observable), written to every face block
 template <int DIM, int B>
 __global__ void __launch_bounds__(kLimNT) k_lim_fv_min_max(int nvar, int nobs, int ghost, long ncells, int cpb,
-                                                           const double* lim, double* obs_min, double* obs_max) {
+                                                           const double* lim, double* obs_min, double* obs_max,
+                                                           LimSel sel) {
   constexpr int S = 2 * B - 1;
   constexpr int NS = DIM == 3 ? S * S * S : S * S;
   extern __shared__ double sm[];
   const long c0 = (long)blockIdx.x * cpb;
-  const int nc = (int)min((long)cpb, ncells - c0);
+  const long nce = sel.cells(ncells);
+  if (c0 >= nce) return;
+  const int nc = (int)min((long)cpb, nce - c0);
   const int SG = S + 2 * ghost;
   const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
-  lim_stage_interior<DIM, S>(sm, lim + c0 * lim_cell, lim_cell, nvar, ghost, nc);
+  lim_stage_interior<DIM, S>(sm, lim, lim_cell, nvar, ghost, c0, nc, sel);
   __syncthreads();
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
@@ -465,8 +500,8 @@ __global__ void __launch_bounds__(kLimNT) k_lim_fv_min_max(int nvar, int nobs, i
     }
     if (lane == 0)
       for (int f = 0; f < 2 * DIM; f++) {
-        obs_min[((c0 + c) * 2 * DIM + f) * nobs + v] = mn;
-        obs_max[((c0 + c) * 2 * DIM + f) * nobs + v] = mx;
+        obs_min[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mn;
+        obs_max[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mx;
       }
   }
 }
@@ -483,8 +518,6 @@ static int lim_cpb(long items_per_cell, long smem_per_cell, long ncells, int occ
   return (int)(cpb < 1 ? 1 : cpb);
 }
 
-enum LimOp { kLimToFv = 0, kLimToDg = 1, kLimMinMax = 2, kLimDmp = 3, kLimFvMinMax = 4 };
-
 template <class K>
 static cudaError_t lim_prepare(K kern, size_t smem) {
   return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -492,7 +525,8 @@ static cudaError_t lim_prepare(K kern, size_t smem) {
 
 template <int DIM, int B, int NVT>
 static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, const double* in, double* out,
-                            double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st) {
+                            double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st,
+                            LimSel sel) {
   constexpr int S = 2 * B - 1;
   long per_cell, items;
   if (op == kLimToFv) {
@@ -520,15 +554,16 @@ static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, 
   if (op == kLimToFv) {
     e = lim_prepare(k_lim_to_fv<DIM, B, NVT>, smem);
     if (e == cudaSuccess)
-      k_lim_to_fv<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
+      k_lim_to_fv<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out, sel);
   } else if (op == kLimToDg) {
     e = lim_prepare(k_lim_to_dg<DIM, B, NVT>, smem);
     if (e == cudaSuccess)
-      k_lim_to_dg<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out);
+      k_lim_to_dg<DIM, B, NVT><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, ghost, ncells, cpb, in, out, sel);
   } else if (op == kLimFvMinMax) {
     e = lim_prepare(k_lim_fv_min_max<DIM, B>, smem);
     if (e == cudaSuccess)
-      k_lim_fv_min_max<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, nobs, ghost, ncells, cpb, in, mn, mx);
+      k_lim_fv_min_max<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, nobs, ghost, ncells, cpb, in, mn, mx,
+                                                                       sel);
   } else {
     e = lim_prepare(k_lim_min_max<DIM, B, NVT>, smem);
     if (e == cudaSuccess)
@@ -544,30 +579,31 @@ static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, 
 // it; any other count the generic ones
 template <int DIM, int B>
 static exa_status_t lim_run_nv(int op, int nvar, int nobs, int ghost, long ncells, const double* in, double* out,
-                               double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st) {
+                               double* mn, double* mx, int* ok, double relax, double scaling, cudaStream_t st,
+                               LimSel sel) {
   const bool five = nvar == 5 && (op < kLimMinMax || op == kLimFvMinMax || nobs == 5);
-  if (five) return lim_run<DIM, B, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-  return lim_run<DIM, B, 0>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+  if (five) return lim_run<DIM, B, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+  return lim_run<DIM, B, 0>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
 }
 
 template <int DIM>
 static exa_status_t lim_dispatch(int op, int order, int nvar, int nobs, int ghost, long ncells, const double* in,
                                  double* out, double* mn, double* mx, int* ok, double relax, double scaling,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, LimSel sel) {
   switch (order) {
-    case 1: return lim_run_nv<DIM, 2>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 2: return lim_run_nv<DIM, 3>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 3: return lim_run_nv<DIM, 4>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 4: return lim_run_nv<DIM, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 5: return lim_run_nv<DIM, 6>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
-    case 6: return lim_run_nv<DIM, 7>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+    case 1: return lim_run_nv<DIM, 2>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+    case 2: return lim_run_nv<DIM, 3>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+    case 3: return lim_run_nv<DIM, 4>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+    case 4: return lim_run_nv<DIM, 5>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+    case 5: return lim_run_nv<DIM, 6>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+    case 6: return lim_run_nv<DIM, 7>(op, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
   }
   return set_error(EXA_EINVAL, "limiter: order must be in 1..6");
 }
 
 static exa_status_t lim_entry(int op, int dim, int order, int nvar, int nobs, int ghost, long ncells,
                               const double* in, double* out, double* mn, double* mx, int* ok, double relax,
-                              double scaling, void* stream) {
+                              double scaling, void* stream, LimSel sel = LimSel()) {
   if (exa_status_t s = ensure_tables()) return s;
   if (dim != 2 && dim != 3) return set_error(EXA_EINVAL, "limiter: dim must be 2 or 3");
   if (nvar < 1 || nvar > 64) return set_error(EXA_EINVAL, "limiter: nvar must be in 1..64");
@@ -585,8 +621,18 @@ static exa_status_t lim_entry(int op, int dim, int order, int nvar, int nobs, in
   }
   if (ncells == 0) return EXA_OK;
   cudaStream_t st = as_stream(stream);
-  return dim == 2 ? lim_dispatch<2>(op, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st)
-                  : lim_dispatch<3>(op, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st);
+  return dim == 2 ? lim_dispatch<2>(op, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel)
+                  : lim_dispatch<3>(op, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling, st, sel);
+}
+
+exa_status_t limiter_launch(int op, int dim, int order, int nvar, int nobs, int ghost, long ncells, const double* in,
+                            double* out, double* mn, double* mx, int* ok, double relax, double scaling,
+                            cudaStream_t st, const int* list, const int* count) {
+  LimSel sel;
+  sel.list = list;
+  sel.count = count;
+  return lim_entry(op, dim, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling,
+                   reinterpret_cast<void*>(st), sel);
 }
 
 exa_status_t upload_tables_limiter() {

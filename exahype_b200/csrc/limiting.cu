@@ -1,0 +1,165 @@
+// Cell-status and bookkeeping kernels of the limiting ADER-DG grid (the
+// a-posteriori subcell limiter of exahype/solvers/LimitingADERDGSolver.cpp on
+// a uniform periodic 2D grid).  Per step, after the unlimited DG candidate:
+//   k_lim_admissible   physical admissibility of the candidate (positive
+//                      density and pressure at every node), folded into the
+//                      DMP verdict (LimitingADERDGSolver.cpp:839-876,
+//                      1028-1048)
+//   k_lim_base_status  Troubled for cells that fail; cells that were
+//                      Troubled stay so for steps-till-cured more steps, then
+//                      become NeighbourOfTroubled1 (determineLimiterStatus-
+//                      AfterSolutionUpdate, :933-991)
+//   k_lim_spread       one face-neighbour hop of status spreading: a cell
+//                      takes max(own, neighbour - 1) (ADERDGSolver.cpp
+//                      mergeWithLimiterStatus :2482-2500)
+//   k_lim_lists        the cells that need a subcell patch (status >=
+//                      NeighbourOfTroubled3) and the cells the FV solver
+//                      updates (status >= NeighbourOfTroubled2)
+//   k_lim_local /      the new cell-local extrema and their merge with the
+//   k_lim_merge        face neighbours' (mergeSolutionMinMaxOnFace,
+//                      LimitingADERDGSolver.cpp:1792-1853)
+// Status values follow ADERDGCellDescription::LimiterStatus: Ok 0,
+// NeighbourOfTroubled4 1, ..3 2, ..2 3, ..1 4, Troubled 5.
+#include "exa_device.cuh"
+
+namespace exa {
+
+constexpr int kLimTroubled = 5, kLimNT1 = 4, kLimNT2 = 3, kLimNT3 = 2;
+
+__global__ void k_lim_admissible(int npc, long ncells, int planar, const double* luh, int* ok) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const double* q = luh + c * npc * kV;
+  bool good = true;
+  for (int i = 0; i < npc; i++, q += kV) {
+    const double rho = q[0];
+    const double j2 = planar ? q[1] * q[1] + q[2] * q[2] : q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    const double p = (kGamma - 1.0) * (q[4] - 0.5 * j2 / rho);
+    good = good && rho > 0.0 && p > 0.0 && isfinite(p);
+  }
+  if (!good) ok[c] = 0;
+}
+
+__global__ void k_lim_base_status(long ncells, const int* ok, int* status, int* cure, int steps_till_cured) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  int base = 0;
+  if (!ok[c]) {
+    cure[c] = steps_till_cured + 1;
+    base = kLimTroubled;
+  } else if (status[c] == kLimTroubled) {
+    const int left = cure[c] - 1;
+    if (left <= 0) {
+      base = kLimNT1;
+      cure[c] = steps_till_cured;
+    } else {
+      base = kLimTroubled;
+      cure[c] = left;
+    }
+  }
+  status[c] = base;
+}
+
+__global__ void k_lim_spread(int nx, int ny, const int* in, int* out) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (long)nx * ny) return;
+  const int x = (int)(c % nx), y = (int)(c / nx);
+  const int xl = x == 0 ? nx - 1 : x - 1, xr = x + 1 == nx ? 0 : x + 1;
+  const int yb = y == 0 ? ny - 1 : y - 1, yt = y + 1 == ny ? 0 : y + 1;
+  int nb = in[(long)y * nx + xl];
+  nb = max(nb, in[(long)y * nx + xr]);
+  nb = max(nb, in[(long)yb * nx + x]);
+  nb = max(nb, in[(long)yt * nx + x]);
+  out[c] = max(in[c], nb - 1);
+}
+
+// counts[0]: cells with a subcell patch, counts[1]: FV-updated cells,
+// counts[2]: Troubled cells
+__global__ void k_lim_lists(long ncells, const int* status, int* list_patch, int* list_fv, int* counts) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int s = status[c];
+  if (s >= kLimNT3) list_patch[atomicAdd(counts + 0, 1)] = (int)c;
+  if (s >= kLimNT2) list_fv[atomicAdd(counts + 1, 1)] = (int)c;
+  if (s == kLimTroubled) atomicAdd(counts + 2, 1);
+}
+
+// face block 0 of the per-cell extrema -> loc [cell][min | max][nobs]
+__global__ void k_lim_local(long ncells, int nobs, const double* bmin, const double* bmax, double* loc) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ncells * nobs) return;
+  const long c = k / nobs;
+  const int v = (int)(k % nobs);
+  loc[(c * 2 + 0) * nobs + v] = bmin[c * 4 * nobs + v];
+  loc[(c * 2 + 1) * nobs + v] = bmax[c * 4 * nobs + v];
+}
+
+// face f of a cell: extrema of the cell and of its neighbour across f
+// (faces 0 left, 1 right, 2 bottom, 3 top)
+__global__ void k_lim_merge(int nx, int ny, int nobs, const double* loc, double* bmin, double* bmax) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long ncells = (long)nx * ny;
+  if (k >= ncells * 4 * nobs) return;
+  const int v = (int)(k % nobs);
+  const int f = (int)((k / nobs) % 4);
+  const long c = k / (4 * nobs);
+  const int x = (int)(c % nx), y = (int)(c / nx);
+  long nb;
+  if (f == 0) nb = (long)y * nx + (x == 0 ? nx - 1 : x - 1);
+  else if (f == 1) nb = (long)y * nx + (x + 1 == nx ? 0 : x + 1);
+  else if (f == 2) nb = (long)(y == 0 ? ny - 1 : y - 1) * nx + x;
+  else nb = (long)(y + 1 == ny ? 0 : y + 1) * nx + x;
+  const double mo = loc[(c * 2) * nobs + v], mn = loc[(nb * 2) * nobs + v];
+  const double xo = loc[(c * 2 + 1) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
+  bmin[k] = mn < mo ? mn : mo;
+  bmax[k] = xo < xn ? xn : xo;
+}
+
+// NaN / Inf in the final state of the FV-updated cells
+__global__ void k_lim_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag) {
+  const long total = (long)*count * npc * kV;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (long)gridDim.x * blockDim.x) {
+    const long cell = list[k / (npc * kV)];
+    if (!isfinite(luh[cell * npc * kV + k % (npc * kV)])) atomicOr(nan_flag, 1);
+  }
+}
+
+static unsigned blocks(long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
+
+exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibility, int steps_till_cured,
+                             const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
+                             int* list_fv, int* counts, cudaStream_t st) {
+  const long n = (long)nx * ny;
+  if (admissibility) k_lim_admissible<<<blocks(n, 256), 256, 0, st>>>(npc, n, planar, luh, ok);
+  k_lim_base_status<<<blocks(n, 256), 256, 0, st>>>(n, ok, status, cure, steps_till_cured);
+  // four hops: Troubled (5) reaches NeighbourOfTroubled4 (1)
+  for (int h = 0; h < 4; h++) {
+    k_lim_spread<<<blocks(n, 256), 256, 0, st>>>(nx, ny, (h & 1) ? status_tmp : status, (h & 1) ? status : status_tmp);
+  }
+  cudaError_t e = cudaMemsetAsync(counts, 0, 3 * sizeof(int), st);
+  if (e != cudaSuccess) return cuda_status(e, "limiter counters");
+  k_lim_lists<<<blocks(n, 256), 256, 0, st>>>(n, status, list_patch, list_fv, counts);
+  count_launch(6 + (admissibility ? 1 : 0));
+  return cuda_status(cudaGetLastError(), "limiter status kernels");
+}
+
+exa_status_t limiting_merge_bounds(int nx, int ny, int nobs, double* bmin, double* bmax, double* loc,
+                                   cudaStream_t st) {
+  const long n = (long)nx * ny;
+  k_lim_local<<<blocks(n * nobs, 256), 256, 0, st>>>(n, nobs, bmin, bmax, loc);
+  k_lim_merge<<<blocks(n * 4 * nobs, 256), 256, 0, st>>>(nx, ny, nobs, loc, bmin, bmax);
+  count_launch(2);
+  return cuda_status(cudaGetLastError(), "limiter bound merge");
+}
+
+exa_status_t limiting_check_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag,
+                                   cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_lim_finite<<<(unsigned)(2 * sms), 256, 0, st>>>(npc, luh, list, count, nan_flag);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_lim_finite");
+}
+
+}  // namespace exa

@@ -383,6 +383,41 @@ exa_status_t exa_limiter_dmp(int dim, int order, int nvar, int nobs, long ncells
                              double relaxation, double difference_scaling, double* obs_min, double* obs_max,
                              int* dmp_ok, void* stream);
 
+/* ---- Limiting ADER-DG on the uniform grid ----
+ * exahype::solvers::LimitingADERDGSolver (exahype/solvers/
+ * LimitingADERDGSolver.cpp) on a periodic 2D exa_aderdg_grid: each step the
+ * unlimited DG candidate is checked by the DMP (bounds: the cell's and its
+ * face neighbours' extrema of the previous step) and, if enabled, by
+ * physical admissibility (positive density and pressure at every node);
+ * failing cells become Troubled, their status spreads over four face hops
+ * (NeighbourOfTroubled1..4), the cells Troubled .. NeighbourOfTroubled2
+ * recompute the step with the FV scheme on 2N+1 subcells per direction
+ * started from the previous solution (ghost subcells from the neighbour
+ * cells' projected previous solutions, NeighbourOfTroubled3 included) and
+ * project the result back (LimitingADERDGSolver::recomputeSolution,
+ * :1378-1441); the next bounds and the next dt come from the final state.
+ * Parameters as in the reference's solver specification. */
+typedef struct {
+  int scheme;                /* subcell FV scheme: 0 Godunov, 1 MUSCL-Hancock */
+  int nobs;                  /* dmp-observables: the first nobs variables, 1..5 */
+  double relaxation;         /* dmp-relaxation-parameter (delta_0) */
+  double difference_scaling; /* dmp-difference-scaling (epsilon) */
+  int steps_till_cured;      /* steps-till-cured */
+  int check_admissibility;   /* 1: density and pressure > 0 at every node */
+} exa_limiter_config_t;
+
+/* Enables (cfg != NULL) or disables the limiter of a grid.  Needs a 2D grid
+ * with periodic boundaries and no slab halos; allocates the limiter state
+ * (previous solution, subcell patches, bounds, statuses) and sets every
+ * cell Ok with bounds from the current state (also after init/set_state). */
+exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_config_t* cfg);
+/* status per cell (nullable host array of ncells ints, LimiterStatus values
+ * Ok 0 .. Troubled 5) and counts[3] (nullable): cells with a subcell patch,
+ * FV-updated cells, Troubled cells, of the last step */
+exa_status_t exa_aderdg_grid_limiter_status(exa_aderdg_grid* g, int* host_status, int* counts);
+/* the DMP bounds for the next step, [cell][4 faces][nobs] each */
+exa_status_t exa_aderdg_grid_limiter_bounds(exa_aderdg_grid* g, double* host_min, double* host_max);
+
 /* Per-cell drop-ins with the reference's argument lists (HOST pointers,
  * synchronous; the limiter kernels take the dimension from the build, here
  * it is an argument). */

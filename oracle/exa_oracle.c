@@ -1381,3 +1381,157 @@ int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, d
   }
   return ok;
 }
+
+/* ------------------------------------------------------------------ */
+/* Limiting ADER-DG on a periodic 2D grid: LimitingADERDGSolver
+ * (exahype/solvers/LimitingADERDGSolver.cpp) restated for a uniform mesh
+ * with global time stepping, on top of the restated kernels above. */
+static long lim_nb(const int* n, long c, int f) {
+  const int x = (int)(c % n[0]), y = (int)(c / n[0]);
+  if (f == 0) return (long)y * n[0] + (x == 0 ? n[0] - 1 : x - 1);
+  if (f == 1) return (long)y * n[0] + (x + 1 == n[0] ? 0 : x + 1);
+  if (f == 2) return (long)(y == 0 ? n[1] - 1 : y - 1) * n[0] + x;
+  return (long)(y + 1 == n[1] ? 0 : y + 1) * n[0] + x;
+}
+
+/* mergeSolutionMinMaxOnFace (:1792-1853): face f keeps the extrema of the
+ * cell (face block 0) and of its neighbour across f */
+static void lim_merge_bounds(const int* n, int nobs, double* bmin, double* bmax) {
+  const long nc = (long)n[0] * n[1];
+  double* loc = (double*)malloc(sizeof(double) * nc * 2 * nobs);
+  long c;
+  int f, v;
+  for (c = 0; c < nc; c++)
+    for (v = 0; v < nobs; v++) {
+      loc[(c * 2) * nobs + v] = bmin[c * 4 * nobs + v];
+      loc[(c * 2 + 1) * nobs + v] = bmax[c * 4 * nobs + v];
+    }
+  for (c = 0; c < nc; c++)
+    for (f = 0; f < 4; f++) {
+      const long nb = lim_nb(n, c, f);
+      for (v = 0; v < nobs; v++) {
+        const double mo = loc[(c * 2) * nobs + v], mn = loc[(nb * 2) * nobs + v];
+        const double xo = loc[(c * 2 + 1) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
+        bmin[(c * 4 + f) * nobs + v] = mn < mo ? mn : mo;
+        bmax[(c * 4 + f) * nobs + v] = xo < xn ? xn : xo;
+      }
+    }
+  free(loc);
+}
+
+void orc_limiting_initial_bounds_2d(int order, const int* n, const double* luh, int nobs, double* bmin,
+                                    double* bmax) {
+  const long nc = (long)n[0] * n[1];
+  const int npc = (order + 1) * (order + 1);
+  long c;
+  for (c = 0; c < nc; c++)
+    orc_limiter_local_min_max(2, order, 5, nobs, luh + c * npc * 5, bmin + c * 4 * nobs, bmax + c * 4 * nobs);
+  lim_merge_bounds(n, nobs, bmin, bmax);
+}
+
+/* positive density and pressure at every node */
+static int lim_admissible(int npc, int planar, const double* q) {
+  int i;
+  for (i = 0; i < npc; i++, q += 5) {
+    const double j2 = planar ? q[1] * q[1] + q[2] * q[2] : q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    const double p = (GAMMA - 1) * (q[4] - 0.5 * j2 / q[0]);
+    if (!(q[0] > 0.0 && p > 0.0 && isfinite(p))) return 0;
+  }
+  return 1;
+}
+
+double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int planar, double* luh,
+                                 int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
+                                 double relaxation, double difference_scaling, int steps_till_cured,
+                                 int admissibility, double dt, int dt_policy, double cfl, int* counts) {
+  const int B = order + 1, npc = B * B, V = 5, S = 2 * order + 1, g = scheme == 0 ? 1 : 2, SG = S + 2 * g;
+  const long nc = (long)n[0] * n[1], cell_d = (long)npc * V, patch_d = (long)SG * SG * V;
+  double* prev = (double*)malloc(sizeof(double) * nc * cell_d);
+  double* patch = (double*)calloc(nc * patch_d, sizeof(double));
+  double* old = (double*)malloc(sizeof(double) * patch_d);
+  int* tmp = (int*)malloc(sizeof(int) * nc);
+  int cnt[3] = {0, 0, 0};
+  long c;
+  int h, f, i, k, m;
+  memcpy(prev, luh, sizeof(double) * nc * cell_d);
+  /* 1. unlimited DG candidate */
+  orc_aderdg_grid_step(2, order, planar, n, dx, luh, 2, cfl, dt, NULL, 0);
+  /* 2. DMP + admissibility -> status (determineLimiterStatusAfterSolutionUpdate) */
+  for (c = 0; c < nc; c++) {
+    int ok = orc_limiter_dmp(2, order, V, nobs, luh + c * cell_d, relaxation, difference_scaling,
+                             bmin + c * 4 * nobs, bmax + c * 4 * nobs);
+    if (admissibility && !lim_admissible(npc, planar, luh + c * cell_d)) ok = 0;
+    if (!ok) {
+      cure[c] = steps_till_cured + 1;
+      tmp[c] = 5;
+    } else if (status[c] == 5) {
+      if (cure[c] - 1 <= 0) {
+        tmp[c] = 4;
+        cure[c] = steps_till_cured;
+      } else {
+        tmp[c] = 5;
+        cure[c] -= 1;
+      }
+    } else {
+      tmp[c] = 0;
+    }
+  }
+  /* spreading: four face-neighbour hops, status = max(own, neighbour - 1) */
+  for (h = 0; h < 4; h++) {
+    for (c = 0; c < nc; c++) {
+      int s = tmp[c];
+      for (f = 0; f < 4; f++) {
+        const int t = tmp[lim_nb(n, c, f)] - 1;
+        if (t > s) s = t;
+      }
+      status[c] = s;
+    }
+    memcpy(tmp, status, sizeof(int) * nc);
+  }
+  /* 3. subcell patches of the previous solution (status >= NeighbourOfTroubled3) */
+  for (c = 0; c < nc; c++) {
+    if (status[c] >= 2) {
+      orc_limiter_project_on_fv(2, order, V, g, prev + c * cell_d, patch + c * patch_d);
+      cnt[0]++;
+    }
+    if (status[c] >= 3) cnt[1]++;
+    if (status[c] == 5) cnt[2]++;
+  }
+  /* 4. face ghosts of the FV cells' patches from the neighbours' patches
+   * (FiniteVolumesSolver::mergeNeighbours / ghostLayerFilling) */
+  for (c = 0; c < nc; c++) {
+    if (status[c] < 3) continue;
+    double* P = patch + c * patch_d;
+    const double* L = patch + lim_nb(n, c, 0) * patch_d;
+    const double* R = patch + lim_nb(n, c, 1) * patch_d;
+    const double* D = patch + lim_nb(n, c, 2) * patch_d;
+    const double* U = patch + lim_nb(n, c, 3) * patch_d;
+    for (i = 0; i < S; i++)
+      for (k = 0; k < g; k++)
+        for (m = 0; m < V; m++) {
+          P[((g + i) * SG + k) * V + m] = L[((g + i) * SG + S + k) * V + m];
+          P[((g + i) * SG + g + S + k) * V + m] = R[((g + i) * SG + g + k) * V + m];
+          P[(k * SG + g + i) * V + m] = D[((S + k) * SG + g + i) * V + m];
+          P[((g + S + k) * SG + g + i) * V + m] = U[((g + k) * SG + g + i) * V + m];
+        }
+  }
+  /* 5. FV step on those patches, projection back, limiter extrema
+   * (recomputeSolution :1378-1441, determineLimiterMinAndMax :1118-1150) */
+  for (c = 0; c < nc; c++) {
+    if (status[c] < 3) continue;
+    double* P = patch + c * patch_d;
+    memcpy(old, P, sizeof(double) * patch_d);
+    if (scheme == 0) orc_fv_godunov_2d(S, g, V, 0, planar, P, old, dx, dt);
+    else orc_fv_musclhancock_2d(S, g, V, 0, planar, P, old, dx, dt);
+    orc_limiter_project_on_dg(2, order, V, g, P, luh + c * cell_d);
+    orc_limiter_fv_min_max(2, order, V, nobs, g, P, bmin + c * 4 * nobs, bmax + c * 4 * nobs);
+  }
+  /* 6. next bounds */
+  lim_merge_bounds(n, nobs, bmin, bmax);
+  if (counts) memcpy(counts, cnt, sizeof(cnt));
+  free(prev);
+  free(patch);
+  free(old);
+  free(tmp);
+  return orc_aderdg_grid_dt(2, order, planar, n, dx, luh, dt_policy, cfl);
+}
