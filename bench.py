@@ -811,6 +811,52 @@ def run_amr(args, rank, world, dist):
         dist.destroy_process_group()
 
 
+def explosion_state(order, n, radius=0.25):
+    """nodal Euler state of a periodic unit square, cells x fastest: density
+    1 / pressure 1 inside the circle of `radius` around the centre, 0.125 /
+    0.1 outside, at rest"""
+    xi = (np.polynomial.legendre.leggauss(order + 1)[0] + 1) / 2
+    X = (np.arange(n)[None, :, None, None] + xi[None, None, None, :]) / n
+    Y = (np.arange(n)[:, None, None, None] + xi[None, None, :, None]) / n
+    X, Y = np.broadcast_arrays(X, Y)
+    inside = (X - 0.5) ** 2 + (Y - 0.5) ** 2 < radius ** 2
+    q = np.zeros(X.shape + (5,))
+    q[..., 0] = np.where(inside, 1.0, 0.125)
+    q[..., 4] = np.where(inside, 1.0, 0.1) / 0.4
+    return q.reshape(-1)
+
+
+def limiting_grid_measure(E, Timer, args, order=3, n=729, steps=20):
+    """ms per step of the limiting grid and of the same grid unlimited"""
+    res = {'workload': '%d^2 cells 2D N=%d, cylindrical explosion, Godunov subcells' % (n, order),
+           'steps': steps}
+    state = explosion_state(order, n)
+    for name in ('unlimited', 'limited'):
+        g = E.ADERDGGrid(2, order, (n, n), length=(1.0, 1.0))
+        g.set_state(state)
+        if name == 'limited':
+            g.set_limiter()
+        g.use_graph(True)
+        g.step(max(args.warmup, 3))
+        stream = g.stream()
+        t = Timer()
+        l0 = E.launch_count()
+        t.start(stream)
+        g.step(steps)
+        t.stop(stream)
+        ms = t.elapsed_ms() / steps
+        E.device.synchronize()
+        res[name] = {'ms_per_step': ms, 'cell_updates_per_s': n * n / (ms * 1e-3),
+                     'gpu_launches_per_step': (E.launch_count() - l0) / steps}
+        if name == 'limited':
+            _, counts = g.limiter_status()
+            res[name].update({'cells_with_patch': int(counts[0]), 'fv_cells': int(counts[1]),
+                              'troubled_cells': int(counts[2])})
+        del g
+    res['limiting_overhead'] = res['limited']['ms_per_step'] / res['unlimited']['ms_per_step'] - 1
+    return res
+
+
 def run_limiter(args, rank, world, dist):
     """Limiter kernels on 3D N=4 cells resident on the GPU: DG -> FV subcell
     projection into patches with one ghost layer, FV -> DG projection back,
@@ -856,6 +902,9 @@ def run_limiter(args, rank, world, dist):
         out[name] = {'ms_per_call': ms, 'cells_per_s': world * count / (ms * 1e-3),
                      'bytes_per_cell': bytes_per_cell, 'hbm_gbs': gbs,
                      'hbm_frac': gbs / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None}
+    # limiting ADER-DG grid: 2D N=3 cylindrical explosion (discontinuous
+    # density and pressure), with and without the limiter, graph-replayed
+    lg = limiting_grid_measure(E, Timer, args)
     # CPU baseline: the reference's own Limiter.cpp (oracle/_ref) on a sample
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -885,7 +934,7 @@ def run_limiter(args, rank, world, dist):
                 'roofline': {'bound': 'hbm', 'achieved': out['project_on_fv']['hbm_gbs'],
                              'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s',
                              'frac': out['project_on_fv']['hbm_frac'], 'peak_source': peak_src},
-                'cpu_baseline': cpu, 'kernels': out}
+                'cpu_baseline': cpu, 'kernels': out, 'limiting_grid': lg}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -188,6 +188,29 @@ __global__ void k_stable_dt(NodeArgs a, const double* luh, double* dt_cell,
   }
 }
 
+// global minimum only: grid-stride over all nodes (consecutive threads read
+// consecutive nodes), one atomic per CTA
+__global__ void k_stable_dt_min(NodeArgs a, const double* luh, unsigned long long* dt_min) {
+  __shared__ double wmin[8];
+  const int nn = a.dim == 3 ? a.B * a.B * a.B : a.B * a.B;
+  const long total = a.ncells * nn;
+  double dt = DBL_MAX;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const double* q = luh + i * a.D;
+    double den = 0.0;
+    for (int d = 0; d < a.dim; d++)
+      den += (a.planar ? euler_max_eig<true>(q, d) : euler_max_eig<false>(q, d)) / a.dx[d];
+    dt = fmin(dt, a.factor / den);
+  }
+  for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = dt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) dt = fmin(dt, wmin[w]);
+    atomic_min_pos_double(dt_min, dt);
+  }
+}
+
 // Rusanov on a face list; one warp per face, in place on lFhbnd
 __global__ void k_riemann_faces(NodeArgs a, long nfaces, const int* left, const int* right,
                                 const int* dir, const double* lQhbnd, double* lFhbnd) {
@@ -291,6 +314,16 @@ exa_status_t launch_stable_dt(const exa_aderdg_desc_t& d, long ncells, const dou
   NodeArgs a = node_args(d, ncells);
   a.factor = factor;
   if (ncells == 0) return EXA_OK;
+  if (!dt_cell && dt_min) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long nodes = ncells * (d.dim == 3 ? a.B * a.B * a.B : a.B * a.B);
+    const long blocks = (nodes + 255) / 256;
+    k_stable_dt_min<<<(unsigned)(blocks < 8L * sms ? blocks : 8L * sms), 256, 0, st>>>(a, luh, dt_min);
+    count_launch();
+    return cuda_status(cudaGetLastError(), "k_stable_dt_min");
+  }
   k_stable_dt<<<grid_for(ncells * 32, 256), 256, 0, st>>>(a, luh, dt_cell, dt_min);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_stable_dt");

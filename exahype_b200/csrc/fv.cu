@@ -1042,97 +1042,102 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
   double* wRx = wLx + R * R * V;
   double* wLy = wRx + R * R * V;
   double* wRy = wLy + R * R * V;
-  if (a.count && (int)blockIdx.x >= *a.count) return;
-  const long patch = a.list ? (long)a.list[blockIdx.x] : (long)blockIdx.x;
-  const double* luh = a.luh + patch * (long)S * S * D;
-  double* out = a.out + patch * (long)S * S * D;
-  const int tid = threadIdx.x;
-  const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
-  for (int i = tid; i < S * S * V; i += FVS_NT) su[i] = luh[i];  // D == V: no parameters here
-  __syncthreads();
-  if (SCHEME == 1) {
-    for (int i = tid; i < R * R; i += FVS_NT) {
-      const int j = pb - 1 + i / R, k = pb - 1 + i % R;
-      const double* U = &su[(j * S + k) * V];
-      const bool has_x = j >= pb && j < pe;
-      const bool has_y = k >= pb && k < pe;
-      const bool interior = has_x && has_y;
-      double lx[V], rx[V], ly[V], ry[V];
-#pragma unroll
-      for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
-      if (has_x) {
-#pragma unroll
+  // one patch per iteration: patch blockIdx.x, or with a selection the
+  // entries blockIdx.x, blockIdx.x + gridDim.x, ... of the list
+  const long npatch = a.count ? (long)*a.count : (long)gridDim.x;
+  for (long e = blockIdx.x; e < npatch; e += gridDim.x) {
+    const long patch = a.list ? (long)a.list[e] : e;
+    const double* luh = a.luh + patch * (long)S * S * D;
+    double* out = a.out + patch * (long)S * S * D;
+    const int tid = threadIdx.x;
+    const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
+    for (int i = tid; i < S * S * V; i += FVS_NT) su[i] = luh[i];  // D == V: no parameters here
+    __syncthreads();
+    if (SCHEME == 1) {
+      for (int i = tid; i < R * R; i += FVS_NT) {
+        const int j = pb - 1 + i / R, k = pb - 1 + i % R;
+        const double* U = &su[(j * S + k) * V];
+        const bool has_x = j >= pb && j < pe;
+        const bool has_y = k >= pb && k < pe;
+        const bool interior = has_x && has_y;
+        double lx[V], rx[V], ly[V], ry[V];
+  #pragma unroll
+        for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
+        if (has_x) {
+  #pragma unroll
+          for (int m = 0; m < V; m++) {
+            const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+            lx[m] = U[m] - 0.5 * hx * sl;
+            rx[m] = U[m] + 0.5 * hx * sl;
+          }
+        }
+        if (has_y) {
+  #pragma unroll
+          for (int m = 0; m < V; m++) {
+            const double sl = minmod(U[S * V + m] - U[m], U[m] - U[-S * V + m]) / hy;
+            ly[m] = U[m] - 0.5 * hy * sl;
+            ry[m] = U[m] + 0.5 * hy * sl;
+          }
+        }
+        if (interior) {
+          double Qt[V];
+          double F[2][V];
+  #pragma unroll
+          for (int m = 0; m < V; m++) Qt[m] = 0.0;
+          euler_flux<2, PLANAR>(lx, F);
+  #pragma unroll
+          for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+          euler_flux<2, PLANAR>(rx, F);
+  #pragma unroll
+          for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+          euler_flux<2, PLANAR>(ly, F);
+  #pragma unroll
+          for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+          euler_flux<2, PLANAR>(ry, F);
+  #pragma unroll
+          for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+  #pragma unroll
+          for (int m = 0; m < V; m++) {
+            lx[m] += 0.5 * dt * Qt[m];
+            rx[m] += 0.5 * dt * Qt[m];
+            ly[m] += 0.5 * dt * Qt[m];
+            ry[m] += 0.5 * dt * Qt[m];
+          }
+        }
+  #pragma unroll
         for (int m = 0; m < V; m++) {
-          const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
-          lx[m] = U[m] - 0.5 * hx * sl;
-          rx[m] = U[m] + 0.5 * hx * sl;
+          wLx[i * V + m] = lx[m];
+          wRx[i * V + m] = rx[m];
+          wLy[i * V + m] = ly[m];
+          wRy[i * V + m] = ry[m];
         }
       }
-      if (has_y) {
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          const double sl = minmod(U[S * V + m] - U[m], U[m] - U[-S * V + m]) / hy;
-          ly[m] = U[m] - 0.5 * hy * sl;
-          ry[m] = U[m] + 0.5 * hy * sl;
-        }
-      }
-      if (interior) {
-        double Qt[V];
-        double F[2][V];
-#pragma unroll
-        for (int m = 0; m < V; m++) Qt[m] = 0.0;
-        euler_flux<2, PLANAR>(lx, F);
-#pragma unroll
-        for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
-        euler_flux<2, PLANAR>(rx, F);
-#pragma unroll
-        for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
-        euler_flux<2, PLANAR>(ly, F);
-#pragma unroll
-        for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
-        euler_flux<2, PLANAR>(ry, F);
-#pragma unroll
-        for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          lx[m] += 0.5 * dt * Qt[m];
-          rx[m] += 0.5 * dt * Qt[m];
-          ly[m] += 0.5 * dt * Qt[m];
-          ry[m] += 0.5 * dt * Qt[m];
-        }
-      }
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        wLx[i * V + m] = lx[m];
-        wRx[i * V + m] = rx[m];
-        wLy[i * V + m] = ly[m];
-        wRy[i * V + m] = ry[m];
-      }
+      __syncthreads();
     }
+    const double cx = dt / hx, cy = dt / hy;
+    double dtn = DBL_MAX;
+    for (int i = tid; i < P * P; i += FVS_NT) {
+      const int j = pb + i / P, k = pb + i % P;
+      const double* U = &su[(j * S + k) * V];
+      double fxl[V], fxr[V], fyb[V], fyt[V];
+      if (SCHEME == 0) {
+        rusanov<PLANAR>(U - V, U, 0, fxl);
+        rusanov<PLANAR>(U, U + V, 0, fxr);
+        rusanov<PLANAR>(U - S * V, U, 1, fyb);
+        rusanov<PLANAR>(U, U + S * V, 1, fyt);
+      } else {
+        const int ic = (j - pb + 1) * R + (k - pb + 1);
+        rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
+        rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
+        rusanov<PLANAR>(&wRy[(ic - R) * V], &wLy[ic * V], 1, fyb);
+        rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + R) * V], 1, fyt);
+      }
+      fv_update_store_dt<PLANAR>(a, out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
+    }
+    for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
+    if ((tid & 31) == 0 && a.next_dt) atomic_min_pos_double(a.next_dt, dtn);
     __syncthreads();
   }
-  const double cx = dt / hx, cy = dt / hy;
-  double dtn = DBL_MAX;
-  for (int i = tid; i < P * P; i += FVS_NT) {
-    const int j = pb + i / P, k = pb + i % P;
-    const double* U = &su[(j * S + k) * V];
-    double fxl[V], fxr[V], fyb[V], fyt[V];
-    if (SCHEME == 0) {
-      rusanov<PLANAR>(U - V, U, 0, fxl);
-      rusanov<PLANAR>(U, U + V, 0, fxr);
-      rusanov<PLANAR>(U - S * V, U, 1, fyb);
-      rusanov<PLANAR>(U, U + S * V, 1, fyt);
-    } else {
-      const int ic = (j - pb + 1) * R + (k - pb + 1);
-      rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
-      rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
-      rusanov<PLANAR>(&wRy[(ic - R) * V], &wLy[ic * V], 1, fyb);
-      rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + R) * V], 1, fyt);
-    }
-    fv_update_store_dt<PLANAR>(a, out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
-  }
-  for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
-  if ((tid & 31) == 0 && a.next_dt) atomic_min_pos_double(a.next_dt, dtn);
 }
 
 inline size_t fv_small_smem(int P, int g, int scheme) {
@@ -1198,8 +1203,8 @@ exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int 
                           : (planar ? k_fv_patch_small<true, 1> : k_fv_patch_small<false, 1>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e, "subcell FV attribute");
-  if (maxcells > 0x7fffffffL) return set_error(EXA_EINVAL, "subcell FV: too many cells");
-  kern<<<(unsigned)maxcells, FVS_NT, smem, st>>>(a);
+  const long grid = maxcells < 16L * sms ? maxcells : 16L * sms;  // CTAs loop over the listed patches
+  kern<<<(unsigned)grid, FVS_NT, smem, st>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_fv_patch_small (subcells)");
 }

@@ -236,31 +236,34 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
   constexpr int NPC = DIM == 3 ? B * B * B : B * B;
   const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
-  const long c0 = (long)blockIdx.x * cpb;
   const long nce = sel.cells(ncells);
-  if (c0 >= nce) return;
-  const int nc = (int)min((long)cpb, nce - c0);
-  const int SG = S + 2 * ghost;
-  const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
-  double* A = sm;
-  double* T1 = A + cpb * NPC * nvar;
-  lim_copy_cells(A, luh, NPC * nvar, c0, nc, sel);
-  __syncthreads();
-  GlobalOut<DIM> go{lim, lim_cell, nvar, SG, ghost, c0, sel.list};
-  if (DIM == 2) {
-    SmemOut o1{T1, nvar, S * B * nvar, S, B};
-    lim_pass<kTabUh2Lim, B, B, B, 1, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
+  // one cell block per iteration (a single one unless a selection launched
+  // fewer CTAs than blocks)
+  for (long c0 = (long)blockIdx.x * cpb; c0 < nce; c0 += (long)gridDim.x * cpb) {
+    const int nc = (int)min((long)cpb, nce - c0);
+    const int SG = S + 2 * ghost;
+    const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
+    double* A = sm;
+    double* T1 = A + cpb * NPC * nvar;
+    lim_copy_cells(A, luh, NPC * nvar, c0, nc, sel);
     __syncthreads();
-    lim_pass<kTabUh2Lim, B, S, B, 1, 1, S>(T1, nvar, S * B * nvar, nc, nvar, go);
-  } else {
-    double* T2 = T1 + cpb * B * B * S * nvar;
-    SmemOut o1{T1, nvar, B * B * S * nvar, S, B};
-    lim_pass<kTabUh2Lim, B, B, B, B, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
+    GlobalOut<DIM> go{lim, lim_cell, nvar, SG, ghost, c0, sel.list};
+    if (DIM == 2) {
+      SmemOut o1{T1, nvar, S * B * nvar, S, B};
+      lim_pass<kTabUh2Lim, B, B, B, 1, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
+      __syncthreads();
+      lim_pass<kTabUh2Lim, B, S, B, 1, 1, S>(T1, nvar, S * B * nvar, nc, nvar, go);
+    } else {
+      double* T2 = T1 + cpb * B * B * S * nvar;
+      SmemOut o1{T1, nvar, B * B * S * nvar, S, B};
+      lim_pass<kTabUh2Lim, B, B, B, B, 0, S>(A, nvar, NPC * nvar, nc, nvar, o1);
+      __syncthreads();
+      SmemOut o2{T2, nvar, B * S * S * nvar, S, S};
+      lim_pass<kTabUh2Lim, B, S, B, B, 1, S>(T1, nvar, B * B * S * nvar, nc, nvar, o2);
+      __syncthreads();
+      lim_pass<kTabUh2Lim, B, S, S, B, 2, S>(T2, nvar, B * S * S * nvar, nc, nvar, go);
+    }
     __syncthreads();
-    SmemOut o2{T2, nvar, B * S * S * nvar, S, S};
-    lim_pass<kTabUh2Lim, B, S, B, B, 1, S>(T1, nvar, B * B * S * nvar, nc, nvar, o2);
-    __syncthreads();
-    lim_pass<kTabUh2Lim, B, S, S, B, 2, S>(T2, nvar, B * S * S * nvar, nc, nvar, go);
   }
 }
 
@@ -313,31 +316,34 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
   constexpr int NS = DIM == 3 ? S * S * S : S * S;
   const int nvar = NVT ? NVT : nvar_rt;
   extern __shared__ double sm[];
-  const long c0 = (long)blockIdx.x * cpb;
   const long nce = sel.cells(ncells);
-  if (c0 >= nce) return;
-  const int nc = (int)min((long)cpb, nce - c0);
-  const int SG = S + 2 * ghost;
-  const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
-  double* A = sm;  // interior subcells [c][z][y][x][v]
-  double* T1 = A + cpb * NS * nvar;
-  lim_stage_interior<DIM, S>(A, lim, lim_cell, nvar, ghost, c0, nc, sel);
-  __syncthreads();
-  GlobalOut<DIM> go{luh, (long)NPC * nvar, nvar, B, 0, c0, sel.list};
-  if (DIM == 2) {
-    SmemOut o1{T1, nvar, S * B * nvar, B, S};
-    lim_pass<kTabLim2Uh, B, S, S, 1, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
+  // one cell block per iteration (a single one unless a selection launched
+  // fewer CTAs than blocks)
+  for (long c0 = (long)blockIdx.x * cpb; c0 < nce; c0 += (long)gridDim.x * cpb) {
+    const int nc = (int)min((long)cpb, nce - c0);
+    const int SG = S + 2 * ghost;
+    const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
+    double* A = sm;  // interior subcells [c][z][y][x][v]
+    double* T1 = A + cpb * NS * nvar;
+    lim_stage_interior<DIM, S>(A, lim, lim_cell, nvar, ghost, c0, nc, sel);
     __syncthreads();
-    lim_pass<kTabLim2Uh, B, B, S, 1, 1, B>(T1, nvar, S * B * nvar, nc, nvar, go);
-  } else {
-    double* T2 = A;  // the staged subcells are dead after pass x
-    SmemOut o1{T1, nvar, S * S * B * nvar, B, S};
-    lim_pass<kTabLim2Uh, B, S, S, S, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
+    GlobalOut<DIM> go{luh, (long)NPC * nvar, nvar, B, 0, c0, sel.list};
+    if (DIM == 2) {
+      SmemOut o1{T1, nvar, S * B * nvar, B, S};
+      lim_pass<kTabLim2Uh, B, S, S, 1, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
+      __syncthreads();
+      lim_pass<kTabLim2Uh, B, B, S, 1, 1, B>(T1, nvar, S * B * nvar, nc, nvar, go);
+    } else {
+      double* T2 = A;  // the staged subcells are dead after pass x
+      SmemOut o1{T1, nvar, S * S * B * nvar, B, S};
+      lim_pass<kTabLim2Uh, B, S, S, S, 0, B>(A, nvar, NS * nvar, nc, nvar, o1);
+      __syncthreads();
+      SmemOut o2{T2, nvar, S * B * B * nvar, B, B};
+      lim_pass<kTabLim2Uh, B, B, S, S, 1, B>(T1, nvar, S * S * B * nvar, nc, nvar, o2);
+      __syncthreads();
+      lim_pass<kTabLim2Uh, B, B, B, S, 2, B>(T2, nvar, S * B * B * nvar, nc, nvar, go);
+    }
     __syncthreads();
-    SmemOut o2{T2, nvar, S * B * B * nvar, B, B};
-    lim_pass<kTabLim2Uh, B, B, S, S, 1, B>(T1, nvar, S * S * B * nvar, nc, nvar, o2);
-    __syncthreads();
-    lim_pass<kTabLim2Uh, B, B, B, S, 2, B>(T2, nvar, S * B * B * nvar, nc, nvar, go);
   }
 }
 
@@ -422,7 +428,10 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
     lim_pass<kTabUh2Lim, B, S, S, B, 2, S>(YS, nobs, B * S * S * nobs, nc, nobs, ms, nc * B * B * nobs);
   }
   __syncthreads();
-  // reduction: one warp per (cell, observable) over its line extrema
+  // reduction: one warp per (cell, observable) over its line extrema, into
+  // shared memory (the Lobatto pass-x area is free again) ...
+  double* red_mn = XL;
+  double* red_mx = XL + cpb * nobs;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
     const int c = pair / nobs, v = pair % nobs;
@@ -443,7 +452,17 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
       mn = lim_min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
       mx = lim_max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
-    if (lane != 0) continue;
+    if (lane == 0) {
+      red_mn[pair] = mn;
+      red_mx[pair] = mx;
+    }
+  }
+  __syncthreads();
+  // ... then one thread per (cell, observable) for the face blocks and the
+  // DMP, so that the global accesses of all pairs are in flight together
+  for (int pair = threadIdx.x; pair < nc * nobs; pair += kLimNT) {
+    const int c = pair / nobs, v = pair % nobs;
+    const double mn = red_mn[pair], mx = red_mx[pair];
     double* bmn = obs_min + (c0 + c) * NF * nobs;
     double* bmx = obs_max + (c0 + c) * NF * nobs;
     if (mode == 0) {
@@ -476,33 +495,36 @@ __global__ void __launch_bounds__(kLimNT) k_lim_fv_min_max(int nvar, int nobs, i
   constexpr int S = 2 * B - 1;
   constexpr int NS = DIM == 3 ? S * S * S : S * S;
   extern __shared__ double sm[];
-  const long c0 = (long)blockIdx.x * cpb;
   const long nce = sel.cells(ncells);
-  if (c0 >= nce) return;
-  const int nc = (int)min((long)cpb, nce - c0);
-  const int SG = S + 2 * ghost;
-  const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
-  lim_stage_interior<DIM, S>(sm, lim, lim_cell, nvar, ghost, c0, nc, sel);
-  __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
-    const int c = pair / nobs, v = pair % nobs;
-    double mn = DBL_MAX, mx = -DBL_MAX;
-    for (int p = lane; p < NS; p += 32) {
-      const double q = sm[((long)c * NS + p) * nvar + v];
-      mn = lim_min(mn, q);
-      mx = lim_max(mx, q);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mn = lim_min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-      mx = lim_max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    }
-    if (lane == 0)
-      for (int f = 0; f < 2 * DIM; f++) {
-        obs_min[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mn;
-        obs_max[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mx;
+  // one cell block per iteration (a single one unless a selection launched
+  // fewer CTAs than blocks)
+  for (long c0 = (long)blockIdx.x * cpb; c0 < nce; c0 += (long)gridDim.x * cpb) {
+    const int nc = (int)min((long)cpb, nce - c0);
+    const int SG = S + 2 * ghost;
+    const long lim_cell = (long)nvar * (DIM == 3 ? SG * SG * SG : SG * SG);
+    lim_stage_interior<DIM, S>(sm, lim, lim_cell, nvar, ghost, c0, nc, sel);
+    __syncthreads();
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int pair = warp; pair < nc * nobs; pair += kLimNT / 32) {
+      const int c = pair / nobs, v = pair % nobs;
+      double mn = DBL_MAX, mx = -DBL_MAX;
+      for (int p = lane; p < NS; p += 32) {
+        const double q = sm[((long)c * NS + p) * nvar + v];
+        mn = lim_min(mn, q);
+        mx = lim_max(mx, q);
       }
+  #pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        mn = lim_min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = lim_max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      }
+      if (lane == 0)
+        for (int f = 0; f < 2 * DIM; f++) {
+          obs_min[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mn;
+          obs_max[(sel.cell(c0 + c) * 2 * DIM + f) * nobs + v] = mx;
+        }
+    }
+    __syncthreads();
   }
 }
 
@@ -548,7 +570,14 @@ static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, 
   const int cpb_set = tune_get(kTuneLimiterCellsPerCta, 0);
   if (cpb_set > 0 && (long)cpb_set * per_cell <= kLimMaxSmem) cpb = cpb_set;
   const size_t smem = (size_t)cpb * per_cell;
-  const long nblk = (ncells + cpb - 1) / cpb;
+  long nblk = (ncells + cpb - 1) / cpb;
+  if (sel.count) {
+    // a selection usually holds a few cells: CTAs loop over the blocks
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    nblk = nblk < 4L * sms ? nblk : 4L * sms;
+  }
   if (nblk > 0x7fffffffL) return set_error(EXA_EINVAL, "limiter: too many cells");
   cudaError_t e = cudaSuccess;
   if (op == kLimToFv) {

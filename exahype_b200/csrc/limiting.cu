@@ -27,17 +27,13 @@ namespace exa {
 constexpr int kLimTroubled = 5, kLimNT1 = 4, kLimNT2 = 3, kLimNT3 = 2;
 
 __global__ void k_lim_admissible(int npc, long ncells, int planar, const double* luh, int* ok) {
-  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
-  const double* q = luh + c * npc * kV;
-  bool good = true;
-  for (int i = 0; i < npc; i++, q += kV) {
-    const double rho = q[0];
-    const double j2 = planar ? q[1] * q[1] + q[2] * q[2] : q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-    const double p = (kGamma - 1.0) * (q[4] - 0.5 * j2 / rho);
-    good = good && rho > 0.0 && p > 0.0 && isfinite(p);
-  }
-  if (!good) ok[c] = 0;
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // node
+  if (i >= ncells * npc) return;
+  const double* q = luh + i * kV;
+  const double rho = q[0];
+  const double j2 = planar ? q[1] * q[1] + q[2] * q[2] : q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  const double p = (kGamma - 1.0) * (q[4] - 0.5 * j2 / rho);
+  if (!(rho > 0.0 && p > 0.0 && isfinite(p))) ok[i / npc] = 0;
 }
 
 __global__ void k_lim_base_status(long ncells, const int* ok, int* status, int* cure, int steps_till_cured) {
@@ -95,24 +91,23 @@ __global__ void k_lim_local(long ncells, int nobs, const double* bmin, const dou
 }
 
 // face f of a cell: extrema of the cell and of its neighbour across f
-// (faces 0 left, 1 right, 2 bottom, 3 top)
+// (faces 0 left, 1 right, 2 bottom, 3 top); one thread per (cell, observable)
 __global__ void k_lim_merge(int nx, int ny, int nobs, const double* loc, double* bmin, double* bmax) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long ncells = (long)nx * ny;
-  if (k >= ncells * 4 * nobs) return;
+  if (k >= ncells * nobs) return;
   const int v = (int)(k % nobs);
-  const int f = (int)((k / nobs) % 4);
-  const long c = k / (4 * nobs);
+  const long c = k / nobs;
   const int x = (int)(c % nx), y = (int)(c / nx);
-  long nb;
-  if (f == 0) nb = (long)y * nx + (x == 0 ? nx - 1 : x - 1);
-  else if (f == 1) nb = (long)y * nx + (x + 1 == nx ? 0 : x + 1);
-  else if (f == 2) nb = (long)(y == 0 ? ny - 1 : y - 1) * nx + x;
-  else nb = (long)(y + 1 == ny ? 0 : y + 1) * nx + x;
-  const double mo = loc[(c * 2) * nobs + v], mn = loc[(nb * 2) * nobs + v];
-  const double xo = loc[(c * 2 + 1) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
-  bmin[k] = mn < mo ? mn : mo;
-  bmax[k] = xo < xn ? xn : xo;
+  const long nb[4] = {(long)y * nx + (x == 0 ? nx - 1 : x - 1), (long)y * nx + (x + 1 == nx ? 0 : x + 1),
+                      (long)(y == 0 ? ny - 1 : y - 1) * nx + x, (long)(y + 1 == ny ? 0 : y + 1) * nx + x};
+  const double mo = loc[(c * 2) * nobs + v], xo = loc[(c * 2 + 1) * nobs + v];
+#pragma unroll
+  for (int f = 0; f < 4; f++) {
+    const double mn = loc[(nb[f] * 2) * nobs + v], xn = loc[(nb[f] * 2 + 1) * nobs + v];
+    bmin[(c * 4 + f) * nobs + v] = mn < mo ? mn : mo;
+    bmax[(c * 4 + f) * nobs + v] = xo < xn ? xn : xo;
+  }
 }
 
 // NaN / Inf in the final state of the FV-updated cells
@@ -130,7 +125,7 @@ exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibil
                              const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
                              int* list_fv, int* counts, cudaStream_t st) {
   const long n = (long)nx * ny;
-  if (admissibility) k_lim_admissible<<<blocks(n, 256), 256, 0, st>>>(npc, n, planar, luh, ok);
+  if (admissibility) k_lim_admissible<<<blocks(n * npc, 256), 256, 0, st>>>(npc, n, planar, luh, ok);
   k_lim_base_status<<<blocks(n, 256), 256, 0, st>>>(n, ok, status, cure, steps_till_cured);
   // four hops: Troubled (5) reaches NeighbourOfTroubled4 (1)
   for (int h = 0; h < 4; h++) {
@@ -147,7 +142,7 @@ exa_status_t limiting_merge_bounds(int nx, int ny, int nobs, double* bmin, doubl
                                    cudaStream_t st) {
   const long n = (long)nx * ny;
   k_lim_local<<<blocks(n * nobs, 256), 256, 0, st>>>(n, nobs, bmin, bmax, loc);
-  k_lim_merge<<<blocks(n * 4 * nobs, 256), 256, 0, st>>>(nx, ny, nobs, loc, bmin, bmax);
+  k_lim_merge<<<blocks(n * nobs, 256), 256, 0, st>>>(nx, ny, nobs, loc, bmin, bmax);
   count_launch(2);
   return cuda_status(cudaGetLastError(), "limiter bound merge");
 }
