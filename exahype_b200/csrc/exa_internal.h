@@ -132,6 +132,17 @@ exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int 
                              double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
                              cudaStream_t st);
 
+// 3D finite volumes (fv3d.cu): one CTA per patch of P^3 cells + g ghost
+// layers, [z][y][x][D]; h = cell sizes; dt read from dt_dev when non-null;
+// optional patch selection list[0 .. *count) (then npatches bounds it)
+exa_status_t fv3_update(int scheme, int P, int g, int D, const double* h, long npatches, double* luh_new,
+                        const double* luh, double dt, const double* dt_dev, double* max_dt, const int* list,
+                        const int* count, cudaStream_t st);
+exa_status_t fv3_stable_dt(int P, int g, int D, const double* h, long npatches, const double* luh, double* dt_patch,
+                           cudaStream_t st);
+exa_status_t fv3_periodic_ghosts(int P, int g, int D, long npatches, double* luh, cudaStream_t st);
+size_t fv3_smem(int P, int g, int scheme);
+
 // limiting-grid bookkeeping (limiting.cu): status from the DMP /
 // admissibility verdicts with spreading and the cell lists; the merge of
 // the per-cell extrema over faces; a finiteness check of listed cells

@@ -589,7 +589,8 @@ __global__ void k_fv_ghosts(int P, int g, int D, long npatches, double* luh) {
 
 static exa_status_t check_fv(const exa_fv_desc_t* d, int want_ghost) {
   if (!d) return set_error(EXA_EINVAL, "NULL descriptor");
-  if (d->dim != 2) return set_error(EXA_EINVAL, "FV kernels are 2D");
+  if (d->dim != 2 && d->dim != 3) return set_error(EXA_EINVAL, "dim must be 2 or 3");
+  if (d->dim == 3 && d->pde != EXA_PDE_EULER) return set_error(EXA_EINVAL, "3D FV: pde must be EXA_PDE_EULER");
   if (d->nvar != kV || d->npar < 0 || d->npar > 8) return set_error(EXA_EINVAL, "nvar must be 5");
   if (d->patch < 1) return set_error(EXA_EINVAL, "patch must be >= 1");
   if (want_ghost && d->ghost < want_ghost) return set_error(EXA_EINVAL, "ghost layer too thin");
@@ -758,6 +759,17 @@ static exa_status_t fv_update(int scheme, const exa_fv_desc_t* desc, long npatch
   if (npatches == 0) return EXA_OK;
   if (npatches > 65535) return set_error(EXA_EINVAL, "at most 65535 patches per call");
   cudaStream_t st = as_stream(stream);
+  if (desc->dim == 3) {
+    if (max_dt) {
+      std::vector<unsigned long long> inf(npatches, 0x7FF0000000000000ULL);
+      cudaError_t e = cudaMemcpyAsync(max_dt, inf.data(), 8 * npatches, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return cuda_status(e, "max_dt init");
+    }
+    const double h[3] = {desc->dx[0] / desc->patch, desc->dx[1] / desc->patch, desc->dx[2] / desc->patch};
+    return fv3_update(scheme, desc->patch, desc->ghost, desc->nvar + desc->npar, h, npatches, luh_new, luh, dt,
+                      nullptr, max_dt, nullptr, nullptr, st);
+  }
   FVArgs a = fv_args(desc);
   a.dt = dt;
   a.luh = luh;
@@ -810,6 +822,10 @@ exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches, const do
   cudaError_t e = cudaMemcpyAsync(dt_patch, inf.data(), 8 * npatches, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_status(e, "dt init");
+  if (desc->dim == 3) {
+    const double h[3] = {desc->dx[0] / desc->patch, desc->dx[1] / desc->patch, desc->dx[2] / desc->patch};
+    return fv3_stable_dt(desc->patch, desc->ghost, desc->nvar + desc->npar, h, npatches, luh, dt_patch, st);
+  }
   FVArgs a = fv_args(desc);
   a.luh = luh;
   const long cells = (long)desc->patch * desc->patch;
@@ -825,6 +841,10 @@ exa_status_t exa_fv_stable_dt(const exa_fv_desc_t* desc, long npatches, const do
 exa_status_t exa_fv_periodic_ghosts(const exa_fv_desc_t* desc, long npatches, double* luh, void* stream) {
   if (exa_status_t s = check_fv(desc, 0)) return s;
   if (npatches < 0 || !luh) return set_error(EXA_EINVAL, "bad argument");
+  if (desc->dim == 3) {
+    if (npatches == 0) return EXA_OK;
+    return fv3_periodic_ghosts(desc->patch, desc->ghost, desc->nvar + desc->npar, npatches, luh, as_stream(stream));
+  }
   const int S = desc->patch + 2 * desc->ghost;
   const long work = ((long)S * S - (long)desc->patch * desc->patch) * npatches;
   if (work == 0) return EXA_OK;

@@ -12,9 +12,9 @@ GODUNOV = 0
 MUSCLHANCOCK = 1
 
 
-def make_fv_desc(patch, ghost, dx, pde=_lib.PDE_EULER, npar=0):
+def make_fv_desc(patch, ghost, dx, pde=_lib.PDE_EULER, npar=0, dim=2):
     d = FVDesc()
-    d.dim, d.patch, d.ghost, d.nvar, d.npar, d.pde = 2, patch, ghost, 5, npar, pde
+    d.dim, d.patch, d.ghost, d.nvar, d.npar, d.pde = dim, patch, ghost, 5, npar, pde
     dx = list(dx) + [1.0] * (3 - len(dx))
     for i in range(3):
         d.dx[i] = float(dx[i])
@@ -24,10 +24,10 @@ def make_fv_desc(patch, ghost, dx, pde=_lib.PDE_EULER, npar=0):
 class FVPatches:
     """Batched FV entry points on `npatches` patches (DeviceBuffer args)."""
 
-    def __init__(self, patch, ghost, dx, pde=_lib.PDE_EULER, npar=0):
-        self.desc = make_fv_desc(patch, ghost, dx, pde, npar)
-        self.patch, self.ghost = patch, ghost
-        self.cells_per_patch = (patch + 2 * ghost) ** 2
+    def __init__(self, patch, ghost, dx, pde=_lib.PDE_EULER, npar=0, dim=2):
+        self.desc = make_fv_desc(patch, ghost, dx, pde, npar, dim)
+        self.patch, self.ghost, self.dim = patch, ghost, dim
+        self.cells_per_patch = (patch + 2 * ghost) ** dim
 
     def godunov_update(self, npatches, luh_new, luh, dt, max_dt=None, stream=None):
         call('exa_fv_godunov_update', C.byref(self.desc), npatches, luh_new.ptr, luh.ptr, float(dt),

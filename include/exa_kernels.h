@@ -562,7 +562,7 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
  * PatchSize / GhostLayerWidth, AbstractGenericFiniteVolumesSolverHeader.
  * template:30-34).  Batched over `npatches` patches back to back. */
 typedef struct {
-  int dim;      /* 2 */
+  int dim;      /* 2, or 3 (EXA_PDE_EULER; patch <= 12 Godunov, <= 10 MUSCL-Hancock) */
   int patch;    /* PatchSize */
   int ghost;    /* 1 for Godunov, 2 for MUSCL-Hancock */
   int nvar, npar, pde;
@@ -570,7 +570,9 @@ typedef struct {
 } exa_fv_desc_t;
 
 /* godunov::c::solutionUpdate (kernels/finitevolumes/godunov/c/2d/
- * godunov.cpph:33-120): luh_new (a copy of luh on entry) is advanced in
+ * godunov.cpph:33-120; 3D: godunov/c/3d/godunov.cpph:35-143, with
+ * musclhancock/c/3d/musclhancock.cpph:50-311 and commons.cpph:410-455 for
+ * the two below): luh_new (a copy of luh on entry) is advanced in
  * place; max_dt (nullable, device, one double per patch) receives the
  * admissible dt.  Rusanov faces (riemannsolvers/c/rusanov.cpph:24-83). */
 exa_status_t exa_fv_godunov_update(const exa_fv_desc_t* desc, long npatches,

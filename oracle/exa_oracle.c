@@ -1535,3 +1535,143 @@ double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int 
   free(tmp);
   return orc_aderdg_grid_dt(2, order, planar, n, dx, luh, dt_policy, cfl);
 }
+
+/* ------------------------------------------------------------------ */
+/* 3D finite volumes on one patch, [z][y][x][D] with S = P + 2g per axis. */
+#define I3(S, D, i, j, k, l) (((((long)(i)) * (S) + (j)) * (S) + (k)) * (D) + (l))
+
+/* godunov::c::solutionUpdate, 3D (godunov/c/3d/godunov.cpph:35-143): x, y,
+ * then z faces; luh_new (a copy of luh) is updated in place */
+double orc_fv_godunov_3d(int P, int g, int V, int npar, double* luh_new, const double* luh, const double* dx,
+                         double dt) {
+  const int D = V + npar, S = P + 2 * g, pb = g, pe = g + P;
+  const double h[3] = {dx[0] / P, dx[1] / P, dx[2] / P};
+  const double cfl = 0.9;
+  double fL[5], fR[5], dtmax = DBL_MAX;
+  int i, j, k, l, d;
+  for (d = 0; d < 3; d++)
+    for (i = pb - (d == 2); i < pe; i++)
+      for (j = pb - (d == 1); j < pe; j++)
+        for (k = pb - (d == 0); k < pe; k++) {
+          const int i2 = i + (d == 2), j2 = j + (d == 1), k2 = k + (d == 0);
+          const double s = orc_rusanov(3, V, npar, 0, fL, fR, luh + I3(S, D, i, j, k, 0), luh + I3(S, D, i2, j2, k2, 0), d);
+          const double c = cfl / 3 * h[d] / s;
+          dtmax = c < dtmax ? c : dtmax;
+          for (l = 0; l < V; l++) {
+            luh_new[I3(S, D, i, j, k, l)] -= dt / h[d] * fL[l];
+            luh_new[I3(S, D, i2, j2, k2, l)] += dt / h[d] * fR[l];
+          }
+        }
+  return dtmax;
+}
+
+/* musclhancock::c::solutionUpdate, 3D (musclhancock/c/3d/musclhancock.cpph:
+ * 50-311): minmod slopes, face extrapolation, half-step evolution of the
+ * interior cells only, Rusanov on the evolved face values; CFL 0.99 */
+double orc_fv_musclhancock_3d(int P, int g, int V, int npar, double* luh_new, const double* luh, const double* dx,
+                              double dt) {
+  const int D = V + npar, S = P + 2 * g, pb = g, pe = g + P;
+  const double h[3] = {dx[0] / P, dx[1] / P, dx[2] / P};
+  const double cfl = 0.99;
+  const long nv = (long)S * S * S * V;
+  double* slope = (double*)calloc(nv * 3, sizeof(double));
+  double* wL[3];
+  double* wR[3];
+  double* slopet = (double*)calloc(nv, sizeof(double));
+  double fL[5], fR[5], dtmax = DBL_MAX;
+  int i, j, k, l, d;
+  for (d = 0; d < 3; d++) {
+    wL[d] = (double*)calloc(nv, sizeof(double));
+    wR[d] = (double*)calloc(nv, sizeof(double));
+  }
+#define ISL3(i, j, k, d, l) ((((((long)(i)) * S + (j)) * S + (k)) * 3 + (d)) * V + (l))
+  /* slopes and face values: direction d over the interior, with one ring
+   * cell on each side along d (:70-150) */
+  for (d = 0; d < 3; d++)
+    for (i = pb - (d == 2); i < pe + (d == 2); i++)
+      for (j = pb - (d == 1); j < pe + (d == 1); j++)
+        for (k = pb - (d == 0); k < pe + (d == 0); k++) {
+          const int di = d == 2, dj = d == 1, dk = d == 0;
+          for (l = 0; l < V; l++) {
+            const double u = luh[I3(S, D, i, j, k, l)];
+            const double sl = minmod(luh[I3(S, D, i + di, j + dj, k + dk, l)] - u,
+                                     u - luh[I3(S, D, i - di, j - dj, k - dk, l)]) / h[d];
+            slope[ISL3(i, j, k, d, l)] = sl;
+            wL[d][I3(S, V, i, j, k, l)] = u - 0.5 * h[d] * sl;
+            wR[d][I3(S, V, i, j, k, l)] = u + 0.5 * h[d] * sl;
+          }
+        }
+  /* half-step evolution increment of the interior cells (:152-205) */
+  for (i = pb; i < pe; i++)
+    for (j = pb; j < pe; j++)
+      for (k = pb; k < pe; k++) {
+        double* Qt = slopet + I3(S, V, i, j, k, 0);
+        double F[15];
+        for (d = 0; d < 3; d++) {
+          orc_euler_flux(3, 0, wL[d] + I3(S, V, i, j, k, 0), F);
+          for (l = 0; l < V; l++) Qt[l] += F[5 * d + l] / h[d];
+          orc_euler_flux(3, 0, wR[d] + I3(S, V, i, j, k, 0), F);
+          for (l = 0; l < V; l++) Qt[l] -= F[5 * d + l] / h[d];
+        }
+        for (l = 0; l < V; l++)
+          for (d = 0; d < 3; d++) {
+            wL[d][I3(S, V, i, j, k, l)] += 0.5 * dt * Qt[l];
+            wR[d][I3(S, V, i, j, k, l)] += 0.5 * dt * Qt[l];
+          }
+      }
+  /* Riemann problems (:207-290) */
+  for (d = 0; d < 3; d++)
+    for (i = pb - (d == 2); i < pe; i++)
+      for (j = pb - (d == 1); j < pe; j++)
+        for (k = pb - (d == 0); k < pe; k++) {
+          const int i2 = i + (d == 2), j2 = j + (d == 1), k2 = k + (d == 0);
+          const double s = orc_rusanov(3, V, 0, 0, fL, fR, wR[d] + I3(S, V, i, j, k, 0), wL[d] + I3(S, V, i2, j2, k2, 0), d);
+          const double c = cfl / 3 * h[d] / s;
+          dtmax = c < dtmax ? c : dtmax;
+          for (l = 0; l < V; l++) {
+            luh_new[I3(S, D, i, j, k, l)] -= dt / h[d] * fL[l];
+            luh_new[I3(S, D, i2, j2, k2, l)] += dt / h[d] * fR[l];
+          }
+        }
+#undef ISL3
+  free(slope);
+  free(slopet);
+  for (d = 0; d < 3; d++) {
+    free(wL[d]);
+    free(wR[d]);
+  }
+  return dtmax;
+}
+
+/* commons::c::stableTimeStepSize, 3D (commons.cpph:410-455) */
+double orc_fv_stable_dt_3d(int P, int g, int V, int npar, const double* luh, const double* dx, double cfl) {
+  const int D = V + npar, S = P + 2 * g;
+  double dtmax = DBL_MAX, lam[5];
+  int i, j, k, d, l;
+  for (i = g; i < g + P; i++)
+    for (j = g; j < g + P; j++)
+      for (k = g; k < g + P; k++)
+        for (d = 0; d < 3; d++) {
+          double s = 0.0;
+          orc_euler_eigenvalues(0, luh + I3(S, D, i, j, k, 0), d, lam);
+          for (l = 0; l < 5; l++) s = fabs(lam[l]) > s ? fabs(lam[l]) : s;
+          {
+            const double c = cfl / 3 * (dx[d] / P) / s;
+            dtmax = c < dtmax ? c : dtmax;
+          }
+        }
+  return dtmax;
+}
+
+/* periodic ghost layers of a single patch (every ghost cell, corners too) */
+void orc_fv_periodic_ghosts_3d(int P, int g, int D, double* luh) {
+  const int S = P + 2 * g;
+  int i, j, k;
+  for (i = 0; i < S; i++)
+    for (j = 0; j < S; j++)
+      for (k = 0; k < S; k++) {
+        const int si = g + ((i - g) % P + P) % P, sj = g + ((j - g) % P + P) % P, sk = g + ((k - g) % P + P) % P;
+        if (si == i && sj == j && sk == k) continue;
+        memcpy(luh + I3(S, D, i, j, k, 0), luh + I3(S, D, si, sj, sk, 0), sizeof(double) * D);
+      }
+}

@@ -134,6 +134,16 @@ void orc_amr_prolongation(int k, int order, int nvar, double* fine, const double
                           int level_delta, const int* index);
 void orc_amr_restriction(int k, int order, int nvar, double* coarse, const double* fine,
                          int level_delta, const int* index);
+/* 3D counterparts on one patch of P^3 cells + g ghost layers ([z][y][x][D],
+ * D = nvar + npar), the 3D Euler PDE (godunov/c/3d/godunov.cpph:35-143,
+ * musclhancock/c/3d/musclhancock.cpph:50-311, commons.cpph:410-455). */
+double orc_fv_godunov_3d(int patch, int ghost, int nvar, int npar, double* luh_new, const double* luh,
+                         const double* dx, double dt);
+double orc_fv_musclhancock_3d(int patch, int ghost, int nvar, int npar, double* luh_new, const double* luh,
+                              const double* dx, double dt);
+double orc_fv_stable_dt_3d(int patch, int ghost, int nvar, int npar, const double* luh, const double* dx,
+                           double cfl);
+void orc_fv_periodic_ghosts_3d(int patch, int ghost, int ndata, double* luh);
 /* one step of a periodic npx x npy grid of FV patches (dx = patch extent) */
 double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
                                 double* luh, const double* dx);

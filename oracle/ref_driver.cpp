@@ -292,6 +292,40 @@ static double fv_step_t(int scheme, double* luh, const double* dx, double dt_fix
 
 #endif
 
+#if DIMENSIONS == 3
+/* 3D counterpart of fv_step_t (godunov/c/3d, musclhancock/c/3d) on one
+ * periodic patch; the MUSCL work arrays of the reference live on the stack
+ * (musclhancock/c/3d/musclhancock.cpph:74-118), small patches only. */
+template <int PS, int G>
+static double fv_step3_t(int scheme, double* luh, const double* dx, double dt_fixed, double* adm) {
+  typedef Euler<0, 0, PS, G> S;
+  const int SZ = PS + 2 * G;
+  S s;
+  for (int i = 0; i < SZ; i++)
+    for (int j = 0; j < SZ; j++)
+      for (int k = 0; k < SZ; k++) {
+        const int si = G + ((i - G) % PS + PS) % PS, sj = G + ((j - G) % PS + PS) % PS,
+                  sk = G + ((k - G) % PS + PS) % PS;
+        if (si == i && sj == j && sk == k) continue;
+        std::memcpy(luh + (((long)i * SZ + j) * SZ + k) * 5, luh + (((long)si * SZ + sj) * SZ + sk) * 5,
+                    5 * sizeof(double));
+      }
+  double lam[5];
+  double dt = dt_fixed > 0 ? dt_fixed
+                           : kernels::finitevolumes::commons::c::stableTimeStepSize<S>(s, luh, lam, vec(dx));
+  std::vector<double> old(luh, luh + (long)SZ * SZ * SZ * 5);
+  double a;
+  if (scheme == 0)
+    a = kernels::finitevolumes::godunov::c::solutionUpdate<false, false, true, S>(
+        s, luh, old.data(), nullptr, nullptr, vec(dx), dt);
+  else
+    a = kernels::finitevolumes::musclhancock::c::solutionUpdate<false, false, true, S>(
+        s, luh, old.data(), nullptr, nullptr, vec(dx), dt);
+  if (adm) *adm = a;
+  return dt;
+}
+#endif
+
 extern "C" {
 
 int ref_stp(int order, int npar, const double* luh, double* lQi, double* lQhi, double* lFhi,
@@ -377,6 +411,25 @@ double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double 
                     : fv_step_t<P, 2>(1, luh, dx, dt_fixed, adm);       \
     break;
     switch (patch) { PCASE(8) PCASE(16) PCASE(32) PCASE(64) PCASE(128) }
+#undef PCASE
+  });
+  th.join();
+  return r;
+}
+#endif
+
+#if DIMENSIONS == 3
+/* one step of a periodic 3D patch (patch 4, 5, 7 or 9) with the reference's
+ * 3D godunov (scheme 0, ghost 1) or musclhancock (scheme 1, ghost 2) */
+double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double dt_fixed, double* adm) {
+  double r = -1;
+  std::thread th([&]() {
+#define PCASE(P)                                                          \
+  case P:                                                                 \
+    r = scheme == 0 ? fv_step3_t<P, 1>(0, luh, dx, dt_fixed, adm)         \
+                    : fv_step3_t<P, 2>(1, luh, dx, dt_fixed, adm);        \
+    break;
+    switch (patch) { PCASE(4) PCASE(5) PCASE(7) PCASE(9) }
 #undef PCASE
   });
   th.join();

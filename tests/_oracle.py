@@ -76,6 +76,13 @@ def lib():
     L.orc_limiter_fv_min_max.argtypes = [i, i, i, i, i, _dp, _dp, _dp]
     L.orc_limiter_dmp.restype = i
     L.orc_limiter_dmp.argtypes = [i, i, i, i, _dp, d, d, _dp, _dp]
+    L.orc_fv_godunov_3d.restype = d
+    L.orc_fv_godunov_3d.argtypes = [i, i, i, i, _dp, _dp, _dp, d]
+    L.orc_fv_musclhancock_3d.restype = d
+    L.orc_fv_musclhancock_3d.argtypes = [i, i, i, i, _dp, _dp, _dp, d]
+    L.orc_fv_stable_dt_3d.restype = d
+    L.orc_fv_stable_dt_3d.argtypes = [i, i, i, i, _dp, _dp, d]
+    L.orc_fv_periodic_ghosts_3d.argtypes = [i, i, i, _dp]
     L.orc_limiting_grid_step_2d.restype = d
     L.orc_limiting_grid_step_2d.argtypes = [i, _ip, _dp, i, _dp, _ip, _ip, _dp, _dp, i, i, d, d, i, i, d, i, d,
                                             C.c_void_p]
@@ -271,7 +278,7 @@ def ref_lib(dim):
         L.ref_grid_step.argtypes = [i, _ip, _dp, _dp, i, d, i]
         L.ref_sample_step.restype = i
         L.ref_sample_step.argtypes = [i, C.c_long, _dp, _dp, d, i]
-        if dim == 2:
+        if hasattr(L, 'ref_fv_step'):
             L.ref_fv_step.restype = d
             L.ref_fv_step.argtypes = [i, i, _dp, _dp, d, C.c_void_p]
     _ref[dim] = L
