@@ -211,7 +211,7 @@ class ADERDGGrid:
     # -- a-posteriori subcell limiter (exa_aderdg_grid_set_limiter) --
     def set_limiter(self, scheme=0, nobs=5, relaxation=1e-4, difference_scaling=1e-3, steps_till_cured=0,
                     check_admissibility=True, enable=True):
-        """Limiting ADER-DG (2D, periodic): DMP + admissibility check of every
+        """Limiting ADER-DG (periodic 2D or 3D): DMP + admissibility check of every
         step's DG candidate, subcell FV recomputation (scheme 0 Godunov, 1
         MUSCL-Hancock) of troubled cells and their neighbours."""
         if not enable:
@@ -232,8 +232,8 @@ class ADERDGGrid:
         return st, counts
 
     def limiter_bounds(self):
-        """DMP bounds for the next step: (min, max), [cell][4][nobs] each"""
-        mn = np.zeros(self.ncells * 4 * self.nobs)
+        """DMP bounds for the next step: (min, max), [cell][2 dim][nobs] each"""
+        mn = np.zeros(self.ncells * 2 * self.dim * self.nobs)
         mx = np.zeros_like(mn)
         call('exa_aderdg_grid_limiter_bounds', self.h, mn.ctypes.data, mx.ctypes.data)
         return mn, mx

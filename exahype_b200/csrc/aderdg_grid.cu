@@ -225,7 +225,7 @@ static exa_status_t grid_correct(exa_aderdg_grid* g) {
 static exa_status_t grid_limit(exa_aderdg_grid* g) {
   const exa_limiter_config_t& L = g->lim_cfg;
   const int dim = g->cfg.dim, order = g->cfg.order, nobs = L.nobs;
-  const int S = 2 * order + 1, npc = (order + 1) * (order + 1);
+  const int S = 2 * order + 1, npc = dim == 3 ? (order + 1) * (order + 1) * (order + 1) : (order + 1) * (order + 1);
   const int planar = g->cfg.pde == EXA_PDE_EULER_PLANAR;
   // the DMP pass also checks admissibility and takes every cell's stable dt
   // of the candidate (the final state for all but the FV-updated cells)
@@ -235,7 +235,7 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
                                       nullptr, L.check_admissibility ? 0 : -1, dt_on ? g->lim_dt : nullptr,
                                       g->dt_factor, g->desc.dx, planar))
     return s;
-  if (exa_status_t s = limiting_status(g->cfg.n[0], g->cfg.n[1], npc, planar, 0,
+  if (exa_status_t s = limiting_status(dim, g->cfg.n, npc, planar, 0,
                                        L.steps_till_cured, g->luh, g->lim_ok, g->lim_status, g->lim_status_tmp,
                                        g->lim_cure, g->lim_list_patch, g->lim_list_fv, g->lim_counts, g->st))
     return s;
@@ -243,10 +243,17 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
                                       g->lim_patch, nullptr, nullptr, nullptr, 0, 0, g->st, g->lim_list_patch,
                                       g->lim_counts + 0))
     return s;
-  if (exa_status_t s = fv_subcell_step(L.scheme, planar, S, g->lim_ghost, g->cfg.n[0], g->cfg.n[1],
-                                       g->desc.dx[0] / S, g->desc.dx[1] / S, g->lim_patch, g->lim_list_fv,
-                                       g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
-    return s;
+  if (dim == 2) {
+    if (exa_status_t s = fv_subcell_step(L.scheme, planar, S, g->lim_ghost, g->cfg.n[0], g->cfg.n[1],
+                                         g->desc.dx[0] / S, g->desc.dx[1] / S, g->lim_patch, g->lim_list_fv,
+                                         g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
+      return s;
+  } else {
+    const double h[3] = {g->desc.dx[0] / S, g->desc.dx[1] / S, g->desc.dx[2] / S};
+    if (exa_status_t s = fv3_subcell_step(L.scheme, S, g->lim_ghost, g->cfg.n, h, g->lim_patch, g->lim_list_fv,
+                                          g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
+      return s;
+  }
   if (exa_status_t s = limiter_launch(kLimToDg, dim, order, kV, 0, g->lim_ghost, g->ncells, g->lim_patch, g->luh,
                                       nullptr, nullptr, nullptr, 0, 0, g->st, g->lim_list_fv, g->lim_counts + 1))
     return s;
@@ -254,13 +261,12 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
                                       nullptr, g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, g->lim_list_fv,
                                       g->lim_counts + 1))
     return s;
-  if (exa_status_t s = limiting_merge_bounds(g->cfg.n[0], g->cfg.n[1], nobs, g->lim_bmin, g->lim_bmax, g->lim_loc,
-                                             g->st))
+  if (exa_status_t s = limiting_merge_bounds(dim, g->cfg.n, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
     return s;
   if (exa_status_t s = limiting_check_finite(npc, g->luh, g->lim_list_fv, g->lim_counts + 1, &g->gd->nan_flag, g->st))
     return s;
   if (dt_on)
-    return limiting_next_dt(npc, planar, g->luh, g->lim_list_fv, g->lim_counts + 1, g->ncells, g->lim_dt,
+    return limiting_next_dt(dim, npc, planar, g->luh, g->lim_list_fv, g->lim_counts + 1, g->ncells, g->lim_dt,
                             g->dt_factor, g->desc.dx, &g->gd->dt_next, g->st);
   return EXA_OK;
 }
@@ -275,8 +281,7 @@ static exa_status_t grid_limiter_reset(exa_aderdg_grid* g) {
   if (exa_status_t s = limiter_launch(kLimMinMax, g->cfg.dim, g->cfg.order, kV, nobs, 0, g->ncells, g->luh, nullptr,
                                       g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, nullptr, nullptr))
     return s;
-  if (exa_status_t s = limiting_merge_bounds(g->cfg.n[0], g->cfg.n[1], nobs, g->lim_bmin, g->lim_bmax, g->lim_loc,
-                                             g->st))
+  if (exa_status_t s = limiting_merge_bounds(g->cfg.dim, g->cfg.n, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
     return s;
   return cuda_status(cudaStreamSynchronize(g->st), "limiter reset");
 }
@@ -578,10 +583,15 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
     g->lim_on = false;
     return EXA_OK;
   }
-  if (g->cfg.dim != 2) return set_error(EXA_EINVAL, "limiter: 2D grids only");
   if (g->halo) return set_error(EXA_EINVAL, "limiter: not with slab halos");
-  if (g->bc[0] != EXA_BC_PERIODIC || g->bc[1] != EXA_BC_PERIODIC)
-    return set_error(EXA_EINVAL, "limiter: periodic boundaries only");
+  for (int i = 0; i < g->cfg.dim; i++)
+    if (g->bc[i] != EXA_BC_PERIODIC) return set_error(EXA_EINVAL, "limiter: periodic boundaries only");
+  if (g->cfg.dim == 3) {
+    // one CTA stages a subcell patch with its ghosts (fv3d.cu)
+    const int S = 2 * g->cfg.order + 1, gw = cfg->scheme == 0 ? 1 : 2;
+    if (fv3_smem(S, gw, cfg->scheme) > 200 * 1024)
+      return set_error(EXA_EINVAL, "limiter: 3D subcell patch too large (MUSCL-Hancock needs order <= 5)");
+  }
   if (cfg->scheme != 0 && cfg->scheme != 1) return set_error(EXA_EINVAL, "limiter: scheme must be 0 or 1");
   if (cfg->nobs < 1 || cfg->nobs > kV) return set_error(EXA_EINVAL, "limiter: nobs must be in 1..5");
   if (!(cfg->relaxation >= 0) || !(cfg->difference_scaling >= 0))
@@ -595,8 +605,10 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
   g->lim_ghost = cfg->scheme == 0 ? 1 : 2;
   const long n = g->ncells;
   const int B = g->cfg.order + 1, SG = 2 * g->cfg.order + 1 + 2 * g->lim_ghost;
-  const size_t d_prev = (size_t)n * B * B * kV, d_patch = (size_t)n * SG * SG * kV;
-  const size_t d_b = (size_t)n * 4 * cfg->nobs, d_loc = (size_t)n * 2 * cfg->nobs;
+  const size_t npc = g->cfg.dim == 3 ? (size_t)B * B * B : (size_t)B * B;
+  const size_t spc = g->cfg.dim == 3 ? (size_t)SG * SG * SG : (size_t)SG * SG;
+  const size_t d_prev = (size_t)n * npc * kV, d_patch = (size_t)n * spc * kV;
+  const size_t d_b = (size_t)n * 2 * g->cfg.dim * cfg->nobs, d_loc = (size_t)n * 2 * cfg->nobs;
   const size_t doubles = d_prev + d_patch + 2 * d_b + d_loc + (size_t)n;
   const size_t ints = 6 * (size_t)n + 4;
   cudaError_t e = cudaMalloc(&g->lim_block, doubles * sizeof(double) + ints * sizeof(int));
@@ -642,7 +654,7 @@ exa_status_t exa_aderdg_grid_limiter_status(exa_aderdg_grid* g, int* host_status
 exa_status_t exa_aderdg_grid_limiter_bounds(exa_aderdg_grid* g, double* host_min, double* host_max) {
   if (!g || !host_min || !host_max) return set_error(EXA_EINVAL, "NULL argument");
   if (!g->lim_on) return set_error(EXA_EINVAL, "limiter not enabled");
-  const size_t bytes = (size_t)g->ncells * 4 * g->lim_cfg.nobs * sizeof(double);
+  const size_t bytes = (size_t)g->ncells * 2 * g->cfg.dim * g->lim_cfg.nobs * sizeof(double);
   cudaError_t e = cudaMemcpyAsync(host_min, g->lim_bmin, bytes, cudaMemcpyDeviceToHost, g->st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(host_max, g->lim_bmax, bytes, cudaMemcpyDeviceToHost, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);

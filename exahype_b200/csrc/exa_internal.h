@@ -127,10 +127,13 @@ exa_status_t upload_tables_limiter();
 // FV step (scheme 0 Godunov, 1 MUSCL-Hancock) on the subcell patches
 // lim[cell] (P subcells + g ghost layers per direction, 5 variables) of the
 // cells list[0 .. *count) of a periodic npx x npy grid: face ghosts from the
-// neighbour cells' patches, then the update in place with *dt_dev (fv.cu)
+// neighbour cells' patches, then the update in place with *dt_dev (fv.cu);
+// the 3D counterpart on an n[0] x n[1] x n[2] grid (fv3d.cu)
 exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int npy, double hx, double hy,
                              double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
                              cudaStream_t st);
+exa_status_t fv3_subcell_step(int scheme, int P, int g, const int* n, const double* h, double* lim, const int* list,
+                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st);
 
 // 3D finite volumes (fv3d.cu): one CTA per patch of P^3 cells + g ghost
 // layers, [z][y][x][D]; h = cell sizes; dt read from dt_dev when non-null;
@@ -146,14 +149,14 @@ size_t fv3_smem(int P, int g, int scheme);
 // limiting-grid bookkeeping (limiting.cu): status from the DMP /
 // admissibility verdicts with spreading and the cell lists; the merge of
 // the per-cell extrema over faces; a finiteness check of listed cells
-exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibility, int steps_till_cured,
+exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int admissibility, int steps_till_cured,
                              const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
                              int* list_fv, int* counts, cudaStream_t st);
-exa_status_t limiting_merge_bounds(int nx, int ny, int nobs, double* bmin, double* bmax, double* loc,
+exa_status_t limiting_merge_bounds(int dim, const int* ncell, int nobs, double* bmin, double* bmax, double* loc,
                                    cudaStream_t st);
-exa_status_t limiting_next_dt(int npc, int planar, const double* luh, const int* list, const int* count, long ncells,
-                              double* dt_cell, double factor, const double* dx, unsigned long long* dt_min,
-                              cudaStream_t st);
+exa_status_t limiting_next_dt(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
+                              long ncells, double* dt_cell, double factor, const double* dx,
+                              unsigned long long* dt_min, cudaStream_t st);
 exa_status_t limiting_check_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag,
                                    cudaStream_t st);
 

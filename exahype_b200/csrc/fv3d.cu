@@ -266,6 +266,58 @@ exa_status_t fv3_update(int scheme, int P, int g, int D, const double* h, long n
   return cuda_status(cudaGetLastError(), "k_fv3_patch");
 }
 
+// face ghosts of the listed 3D subcell patches from the face neighbours'
+// boundary layers (periodic grid of n[0] x n[1] x n[2] cells, x fastest);
+// grid-stride over list entries x face ghosts
+__global__ void k_fv3_subcell_exchange(int P, int g, int nx, int ny, int nz, double* lim, const int* list,
+                                       const int* count) {
+  const int S = P + 2 * g;
+  const long S3 = (long)S * S * S;
+  const long per = 6L * g * P * P;  // face ghosts per patch
+  const long total = (long)*count * per;
+  for (long gid = (long)blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += (long)gridDim.x * blockDim.x) {
+    const long patch = list[gid / per];
+    int r = (int)(gid % per);
+    const int f = r / (g * P * P);  // face 2 d + side
+    r %= g * P * P;
+    const int layer = r / (P * P), a = (r / P) % P, b = r % P;  // layer across, (a, b) along the face
+    const int d = f >> 1;
+    const bool up = f & 1;
+    int x = (int)(patch % nx), y = (int)((patch / nx) % ny), z = (int)(patch / ((long)nx * ny));
+    // destination (i, j, k) = (z, y, x) subcell in this patch, source in the neighbour
+    int di[3], si[3];  // [z][y][x] coordinates
+    const int ghost = up ? g + P + layer : layer;        // ghost coordinate along d
+    const int src = up ? g + layer : P + layer;           // neighbour's boundary layer
+    const int ax = 2 - d;                                 // coordinate index of direction d in (z, y, x)
+    const int o1 = ax == 0 ? 1 : 0, o2 = ax == 2 ? 1 : 2;  // the two other coordinates
+    di[ax] = ghost;
+    si[ax] = src;
+    di[o1] = si[o1] = g + a;
+    di[o2] = si[o2] = g + b;
+    if (d == 0) x = up ? (x + 1 == nx ? 0 : x + 1) : (x == 0 ? nx - 1 : x - 1);
+    else if (d == 1) y = up ? (y + 1 == ny ? 0 : y + 1) : (y == 0 ? ny - 1 : y - 1);
+    else z = up ? (z + 1 == nz ? 0 : z + 1) : (z == 0 ? nz - 1 : z - 1);
+    const long nbp = ((long)z * ny + y) * nx + x;
+    double* dst = lim + patch * S3 * kV + (((long)di[0] * S + di[1]) * S + di[2]) * kV;
+    const double* s = lim + nbp * S3 * kV + (((long)si[0] * S + si[1]) * S + si[2]) * kV;
+#pragma unroll
+    for (int m = 0; m < kV; m++) dst[m] = s[m];
+  }
+}
+
+exa_status_t fv3_subcell_step(int scheme, int P, int g, const int* n, const double* h, double* lim, const int* list,
+                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st) {
+  if ((scheme == 0 && g < 1) || (scheme == 1 && g < 2)) return set_error(EXA_EINVAL, "subcell FV: ghost layer too thin");
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_fv3_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, n[0], n[1], n[2], lim, list, count);
+  count_launch();
+  if (exa_status_t s = cuda_status(cudaGetLastError(), "k_fv3_subcell_exchange")) return s;
+  // in place: each CTA stages its patch before it writes
+  return fv3_update(scheme, P, g, kV, h, maxcells, lim, lim, 0.0, dt_dev, nullptr, list, count, st);
+}
+
 exa_status_t fv3_stable_dt(int P, int g, int D, const double* h, long npatches, const double* luh, double* dt_patch,
                            cudaStream_t st) {
   if (npatches > 65535) return set_error(EXA_EINVAL, "at most 65535 patches per call");

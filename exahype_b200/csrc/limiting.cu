@@ -1,6 +1,6 @@
 // Cell-status and bookkeeping kernels of the limiting ADER-DG grid (the
 // a-posteriori subcell limiter of exahype/solvers/LimitingADERDGSolver.cpp on
-// a uniform periodic 2D grid).  Per step, after the unlimited DG candidate:
+// a uniform periodic 2D or 3D grid).  Per step, after the unlimited DG candidate:
 //   k_lim_admissible   physical admissibility of the candidate (positive
 //                      density and pressure at every node), folded into the
 //                      DMP verdict (LimitingADERDGSolver.cpp:839-876,
@@ -58,16 +58,27 @@ __global__ void k_lim_base_status(long ncells, const int* ok, int* status, int* 
   status[c] = base;
 }
 
-__global__ void k_lim_spread(int nx, int ny, const int* in, int* out) {
+// grid of n.x x n.y x n.z cells (n.z = 1 in 2D), x fastest, periodic
+struct LimGrid {
+  int nx, ny, nz, dim;
+  __host__ __device__ __forceinline__ long cells() const { return (long)nx * ny * nz; }
+  // the neighbour across face f = 2 d + (0 lower, 1 upper)
+  __device__ __forceinline__ long nb(long c, int f) const {
+    int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((long)nx * ny));
+    const int d = f >> 1;
+    const bool up = f & 1;
+    if (d == 0) x = up ? (x + 1 == nx ? 0 : x + 1) : (x == 0 ? nx - 1 : x - 1);
+    else if (d == 1) y = up ? (y + 1 == ny ? 0 : y + 1) : (y == 0 ? ny - 1 : y - 1);
+    else z = up ? (z + 1 == nz ? 0 : z + 1) : (z == 0 ? nz - 1 : z - 1);
+    return ((long)z * ny + y) * nx + x;
+  }
+};
+
+__global__ void k_lim_spread(LimGrid G, const int* in, int* out) {
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= (long)nx * ny) return;
-  const int x = (int)(c % nx), y = (int)(c / nx);
-  const int xl = x == 0 ? nx - 1 : x - 1, xr = x + 1 == nx ? 0 : x + 1;
-  const int yb = y == 0 ? ny - 1 : y - 1, yt = y + 1 == ny ? 0 : y + 1;
-  int nb = in[(long)y * nx + xl];
-  nb = max(nb, in[(long)y * nx + xr]);
-  nb = max(nb, in[(long)yb * nx + x]);
-  nb = max(nb, in[(long)yt * nx + x]);
+  if (c >= G.cells()) return;
+  int nb = 0;
+  for (int f = 0; f < 2 * G.dim; f++) nb = max(nb, in[G.nb(c, f)]);
   out[c] = max(in[c], nb - 1);
 }
 
@@ -83,32 +94,29 @@ __global__ void k_lim_lists(long ncells, const int* status, int* list_patch, int
 }
 
 // face block 0 of the per-cell extrema -> loc [cell][min | max][nobs]
-__global__ void k_lim_local(long ncells, int nobs, const double* bmin, const double* bmax, double* loc) {
+__global__ void k_lim_local(long ncells, int nf, int nobs, const double* bmin, const double* bmax, double* loc) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ncells * nobs) return;
   const long c = k / nobs;
   const int v = (int)(k % nobs);
-  loc[(c * 2 + 0) * nobs + v] = bmin[c * 4 * nobs + v];
-  loc[(c * 2 + 1) * nobs + v] = bmax[c * 4 * nobs + v];
+  loc[(c * 2 + 0) * nobs + v] = bmin[c * nf * nobs + v];
+  loc[(c * 2 + 1) * nobs + v] = bmax[c * nf * nobs + v];
 }
 
-// face f of a cell: extrema of the cell and of its neighbour across f
-// (faces 0 left, 1 right, 2 bottom, 3 top); one thread per (cell, observable)
-__global__ void k_lim_merge(int nx, int ny, int nobs, const double* loc, double* bmin, double* bmax) {
+// face f of a cell: extrema of the cell and of its neighbour across f; one
+// thread per (cell, observable)
+__global__ void k_lim_merge(LimGrid G, int nobs, const double* loc, double* bmin, double* bmax) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long ncells = (long)nx * ny;
-  if (k >= ncells * nobs) return;
+  if (k >= G.cells() * nobs) return;
   const int v = (int)(k % nobs);
   const long c = k / nobs;
-  const int x = (int)(c % nx), y = (int)(c / nx);
-  const long nb[4] = {(long)y * nx + (x == 0 ? nx - 1 : x - 1), (long)y * nx + (x + 1 == nx ? 0 : x + 1),
-                      (long)(y == 0 ? ny - 1 : y - 1) * nx + x, (long)(y + 1 == ny ? 0 : y + 1) * nx + x};
+  const int nf = 2 * G.dim;
   const double mo = loc[(c * 2) * nobs + v], xo = loc[(c * 2 + 1) * nobs + v];
-#pragma unroll
-  for (int f = 0; f < 4; f++) {
-    const double mn = loc[(nb[f] * 2) * nobs + v], xn = loc[(nb[f] * 2 + 1) * nobs + v];
-    bmin[(c * 4 + f) * nobs + v] = mn < mo ? mn : mo;
-    bmax[(c * 4 + f) * nobs + v] = xo < xn ? xn : xo;
+  for (int f = 0; f < nf; f++) {
+    const long nb = G.nb(c, f);
+    const double mn = loc[(nb * 2) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
+    bmin[(c * nf + f) * nobs + v] = mn < mo ? mn : mo;
+    bmax[(c * nf + f) * nobs + v] = xo < xn ? xn : xo;
   }
 }
 
@@ -123,8 +131,8 @@ __global__ void k_lim_finite(int npc, const double* luh, const int* list, const 
 
 // stable dt of the FV-updated cells' final state (one warp per listed cell,
 // the rule of k_stable_dt), over their candidate values in dt_cell
-__global__ void k_lim_dt_listed(int npc, int planar, const double* luh, const int* list, const int* count,
-                                double* dt_cell, double factor, double dx0, double dx1) {
+__global__ void k_lim_dt_listed(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
+                                double* dt_cell, double factor, double dx0, double dx1, double dx2) {
   const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const long n = *count;
@@ -136,6 +144,7 @@ __global__ void k_lim_dt_listed(int npc, int planar, const double* luh, const in
       double den = 0.0;
       den += (planar ? euler_max_eig<true>(q, 0) : euler_max_eig<false>(q, 0)) / dx0;
       den += (planar ? euler_max_eig<true>(q, 1) : euler_max_eig<false>(q, 1)) / dx1;
+      if (dim == 3) den += euler_max_eig<false>(q, 2) / dx2;
       dt = fmin(dt, factor / den);
     }
     for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
@@ -160,28 +169,39 @@ __global__ void k_lim_dt_reduce(long n, const double* dt_cell, unsigned long lon
 
 static unsigned blocks(long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
-exa_status_t limiting_next_dt(int npc, int planar, const double* luh, const int* list, const int* count, long ncells,
-                              double* dt_cell, double factor, const double* dx, unsigned long long* dt_min,
-                              cudaStream_t st) {
+exa_status_t limiting_next_dt(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
+                              long ncells, double* dt_cell, double factor, const double* dx,
+                              unsigned long long* dt_min, cudaStream_t st) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_lim_dt_listed<<<(unsigned)(4 * sms), 256, 0, st>>>(npc, planar, luh, list, count, dt_cell, factor, dx[0], dx[1]);
+  k_lim_dt_listed<<<(unsigned)(4 * sms), 256, 0, st>>>(dim, npc, planar, luh, list, count, dt_cell, factor, dx[0],
+                                                       dx[1], dim == 3 ? dx[2] : 1.0);
   const long nb = blocks(ncells, 256);
   k_lim_dt_reduce<<<(unsigned)(nb < 2L * sms ? nb : 2L * sms), 256, 0, st>>>(ncells, dt_cell, dt_min);
   count_launch(2);
   return cuda_status(cudaGetLastError(), "limiter next dt");
 }
 
-exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibility, int steps_till_cured,
+static LimGrid lim_grid(int dim, const int* n) {
+  LimGrid G;
+  G.nx = n[0];
+  G.ny = n[1];
+  G.nz = dim == 3 ? n[2] : 1;
+  G.dim = dim;
+  return G;
+}
+
+exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int admissibility, int steps_till_cured,
                              const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
                              int* list_fv, int* counts, cudaStream_t st) {
-  const long n = (long)nx * ny;
+  const LimGrid G = lim_grid(dim, ncell);
+  const long n = (long)G.nx * G.ny * G.nz;
   if (admissibility) k_lim_admissible<<<blocks(n * npc, 256), 256, 0, st>>>(npc, n, planar, luh, ok);
   k_lim_base_status<<<blocks(n, 256), 256, 0, st>>>(n, ok, status, cure, steps_till_cured);
   // four hops: Troubled (5) reaches NeighbourOfTroubled4 (1)
   for (int h = 0; h < 4; h++) {
-    k_lim_spread<<<blocks(n, 256), 256, 0, st>>>(nx, ny, (h & 1) ? status_tmp : status, (h & 1) ? status : status_tmp);
+    k_lim_spread<<<blocks(n, 256), 256, 0, st>>>(G, (h & 1) ? status_tmp : status, (h & 1) ? status : status_tmp);
   }
   cudaError_t e = cudaMemsetAsync(counts, 0, 3 * sizeof(int), st);
   if (e != cudaSuccess) return cuda_status(e, "limiter counters");
@@ -190,11 +210,12 @@ exa_status_t limiting_status(int nx, int ny, int npc, int planar, int admissibil
   return cuda_status(cudaGetLastError(), "limiter status kernels");
 }
 
-exa_status_t limiting_merge_bounds(int nx, int ny, int nobs, double* bmin, double* bmax, double* loc,
+exa_status_t limiting_merge_bounds(int dim, const int* ncell, int nobs, double* bmin, double* bmax, double* loc,
                                    cudaStream_t st) {
-  const long n = (long)nx * ny;
-  k_lim_local<<<blocks(n * nobs, 256), 256, 0, st>>>(n, nobs, bmin, bmax, loc);
-  k_lim_merge<<<blocks(n * nobs, 256), 256, 0, st>>>(nx, ny, nobs, loc, bmin, bmax);
+  const LimGrid G = lim_grid(dim, ncell);
+  const long n = (long)G.nx * G.ny * G.nz;
+  k_lim_local<<<blocks(n * nobs, 256), 256, 0, st>>>(n, 2 * dim, nobs, bmin, bmax, loc);
+  k_lim_merge<<<blocks(n * nobs, 256), 256, 0, st>>>(G, nobs, loc, bmin, bmax);
   count_launch(2);
   return cuda_status(cudaGetLastError(), "limiter bound merge");
 }

@@ -385,7 +385,7 @@ exa_status_t exa_limiter_dmp(int dim, int order, int nvar, int nobs, long ncells
 
 /* ---- Limiting ADER-DG on the uniform grid ----
  * exahype::solvers::LimitingADERDGSolver (exahype/solvers/
- * LimitingADERDGSolver.cpp) on a periodic 2D exa_aderdg_grid: each step the
+ * LimitingADERDGSolver.cpp) on a periodic exa_aderdg_grid (2D or 3D): each step the
  * unlimited DG candidate is checked by the DMP (bounds: the cell's and its
  * face neighbours' extrema of the previous step) and, if enabled, by
  * physical admissibility (positive density and pressure at every node);
@@ -406,16 +406,17 @@ typedef struct {
   int check_admissibility;   /* 1: density and pressure > 0 at every node */
 } exa_limiter_config_t;
 
-/* Enables (cfg != NULL) or disables the limiter of a grid.  Needs a 2D grid
- * with periodic boundaries and no slab halos; allocates the limiter state
- * (previous solution, subcell patches, bounds, statuses) and sets every
- * cell Ok with bounds from the current state (also after init/set_state). */
+/* Enables (cfg != NULL) or disables the limiter of a grid.  Needs periodic
+ * boundaries and no slab halos (3D MUSCL-Hancock subcells: order <= 5);
+ * allocates the limiter state (previous solution, one subcell patch per
+ * cell, bounds, statuses) and sets every cell Ok with bounds from the
+ * current state (also after init/set_state). */
 exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_config_t* cfg);
 /* status per cell (nullable host array of ncells ints, LimiterStatus values
  * Ok 0 .. Troubled 5) and counts[3] (nullable): cells with a subcell patch,
  * FV-updated cells, Troubled cells, of the last step */
 exa_status_t exa_aderdg_grid_limiter_status(exa_aderdg_grid* g, int* host_status, int* counts);
-/* the DMP bounds for the next step, [cell][4 faces][nobs] each */
+/* the DMP bounds for the next step, [cell][2 dim faces][nobs] each */
 exa_status_t exa_aderdg_grid_limiter_bounds(exa_aderdg_grid* g, double* host_min, double* host_max);
 
 /* Per-cell drop-ins with the reference's argument lists (HOST pointers,
@@ -562,7 +563,7 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
  * PatchSize / GhostLayerWidth, AbstractGenericFiniteVolumesSolverHeader.
  * template:30-34).  Batched over `npatches` patches back to back. */
 typedef struct {
-  int dim;      /* 2, or 3 (EXA_PDE_EULER; patch <= 12 Godunov, <= 10 MUSCL-Hancock) */
+  int dim;      /* 2, or 3 (EXA_PDE_EULER; a patch with its ghosts in 200 KB: patch <= 15 Godunov, <= 11 MUSCL-Hancock) */
   int patch;    /* PatchSize */
   int ghost;    /* 1 for Godunov, 2 for MUSCL-Hancock */
   int nvar, npar, pde;

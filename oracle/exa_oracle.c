@@ -1383,50 +1383,57 @@ int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, d
 }
 
 /* ------------------------------------------------------------------ */
-/* Limiting ADER-DG on a periodic 2D grid: LimitingADERDGSolver
+/* Limiting ADER-DG on a periodic 2D or 3D grid: LimitingADERDGSolver
  * (exahype/solvers/LimitingADERDGSolver.cpp) restated for a uniform mesh
- * with global time stepping, on top of the restated kernels above. */
-static long lim_nb(const int* n, long c, int f) {
-  const int x = (int)(c % n[0]), y = (int)(c / n[0]);
-  if (f == 0) return (long)y * n[0] + (x == 0 ? n[0] - 1 : x - 1);
-  if (f == 1) return (long)y * n[0] + (x + 1 == n[0] ? 0 : x + 1);
-  if (f == 2) return (long)(y == 0 ? n[1] - 1 : y - 1) * n[0] + x;
-  return (long)(y + 1 == n[1] ? 0 : y + 1) * n[0] + x;
+ * with global time stepping, on top of the restated kernels above.  Cells
+ * x fastest; n[2] is ignored in 2D. */
+static long lim_nb(int dim, const int* n, long c, int f) {
+  int x = (int)(c % n[0]), y = (int)((c / n[0]) % n[1]);
+  int z = dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0;
+  const int d = f >> 1, up = f & 1;
+  if (d == 0) x = up ? (x + 1 == n[0] ? 0 : x + 1) : (x == 0 ? n[0] - 1 : x - 1);
+  else if (d == 1) y = up ? (y + 1 == n[1] ? 0 : y + 1) : (y == 0 ? n[1] - 1 : y - 1);
+  else z = up ? (z + 1 == n[2] ? 0 : z + 1) : (z == 0 ? n[2] - 1 : z - 1);
+  return ((long)z * n[1] + y) * n[0] + x;
 }
+
+static long lim_ncells(int dim, const int* n) { return (long)n[0] * n[1] * (dim == 3 ? n[2] : 1); }
 
 /* mergeSolutionMinMaxOnFace (:1792-1853): face f keeps the extrema of the
  * cell (face block 0) and of its neighbour across f */
-static void lim_merge_bounds(const int* n, int nobs, double* bmin, double* bmax) {
-  const long nc = (long)n[0] * n[1];
+static void lim_merge_bounds(int dim, const int* n, int nobs, double* bmin, double* bmax) {
+  const long nc = lim_ncells(dim, n);
+  const int nf = 2 * dim;
   double* loc = (double*)malloc(sizeof(double) * nc * 2 * nobs);
   long c;
   int f, v;
   for (c = 0; c < nc; c++)
     for (v = 0; v < nobs; v++) {
-      loc[(c * 2) * nobs + v] = bmin[c * 4 * nobs + v];
-      loc[(c * 2 + 1) * nobs + v] = bmax[c * 4 * nobs + v];
+      loc[(c * 2) * nobs + v] = bmin[c * nf * nobs + v];
+      loc[(c * 2 + 1) * nobs + v] = bmax[c * nf * nobs + v];
     }
   for (c = 0; c < nc; c++)
-    for (f = 0; f < 4; f++) {
-      const long nb = lim_nb(n, c, f);
+    for (f = 0; f < nf; f++) {
+      const long nb = lim_nb(dim, n, c, f);
       for (v = 0; v < nobs; v++) {
         const double mo = loc[(c * 2) * nobs + v], mn = loc[(nb * 2) * nobs + v];
         const double xo = loc[(c * 2 + 1) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
-        bmin[(c * 4 + f) * nobs + v] = mn < mo ? mn : mo;
-        bmax[(c * 4 + f) * nobs + v] = xo < xn ? xn : xo;
+        bmin[(c * nf + f) * nobs + v] = mn < mo ? mn : mo;
+        bmax[(c * nf + f) * nobs + v] = xo < xn ? xn : xo;
       }
     }
   free(loc);
 }
 
-void orc_limiting_initial_bounds_2d(int order, const int* n, const double* luh, int nobs, double* bmin,
-                                    double* bmax) {
-  const long nc = (long)n[0] * n[1];
-  const int npc = (order + 1) * (order + 1);
+void orc_limiting_initial_bounds(int dim, int order, const int* n, const double* luh, int nobs, double* bmin,
+                                 double* bmax) {
+  const long nc = lim_ncells(dim, n);
+  const int B = order + 1, npc = dim == 3 ? B * B * B : B * B;
   long c;
   for (c = 0; c < nc; c++)
-    orc_limiter_local_min_max(2, order, 5, nobs, luh + c * npc * 5, bmin + c * 4 * nobs, bmax + c * 4 * nobs);
-  lim_merge_bounds(n, nobs, bmin, bmax);
+    orc_limiter_local_min_max(dim, order, 5, nobs, luh + c * npc * 5, bmin + c * 2 * dim * nobs,
+                              bmax + c * 2 * dim * nobs);
+  lim_merge_bounds(dim, n, nobs, bmin, bmax);
 }
 
 /* positive density and pressure at every node */
@@ -1440,26 +1447,33 @@ static int lim_admissible(int npc, int planar, const double* q) {
   return 1;
 }
 
-double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int planar, double* luh,
-                                 int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
-                                 double relaxation, double difference_scaling, int steps_till_cured,
-                                 int admissibility, double dt, int dt_policy, double cfl, int* counts) {
-  const int B = order + 1, npc = B * B, V = 5, S = 2 * order + 1, g = scheme == 0 ? 1 : 2, SG = S + 2 * g;
-  const long nc = (long)n[0] * n[1], cell_d = (long)npc * V, patch_d = (long)SG * SG * V;
+/* point (z, y, x) of a [S]^dim patch */
+static long lim_pt(int dim, int SG, int z, int y, int x) {
+  return dim == 3 ? ((long)z * SG + y) * SG + x : (long)y * SG + x;
+}
+
+double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx, int planar, double* luh,
+                              int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
+                              double relaxation, double difference_scaling, int steps_till_cured, int admissibility,
+                              double dt, int dt_policy, double cfl, int* counts) {
+  const int B = order + 1, npc = dim == 3 ? B * B * B : B * B, V = 5, S = 2 * order + 1;
+  const int g = scheme == 0 ? 1 : 2, SG = S + 2 * g, nf = 2 * dim;
+  const long nc = lim_ncells(dim, n), cell_d = (long)npc * V;
+  const long patch_d = (long)(dim == 3 ? SG * SG * SG : SG * SG) * V;
   double* prev = (double*)malloc(sizeof(double) * nc * cell_d);
   double* patch = (double*)calloc(nc * patch_d, sizeof(double));
   double* old = (double*)malloc(sizeof(double) * patch_d);
   int* tmp = (int*)malloc(sizeof(int) * nc);
   int cnt[3] = {0, 0, 0};
   long c;
-  int h, f, i, k, m;
+  int h, f, a, b, k, m;
   memcpy(prev, luh, sizeof(double) * nc * cell_d);
   /* 1. unlimited DG candidate */
-  orc_aderdg_grid_step(2, order, planar, n, dx, luh, 2, cfl, dt, NULL, 0);
+  orc_aderdg_grid_step(dim, order, planar, n, dx, luh, 2, cfl, dt, NULL, 0);
   /* 2. DMP + admissibility -> status (determineLimiterStatusAfterSolutionUpdate) */
   for (c = 0; c < nc; c++) {
-    int ok = orc_limiter_dmp(2, order, V, nobs, luh + c * cell_d, relaxation, difference_scaling,
-                             bmin + c * 4 * nobs, bmax + c * 4 * nobs);
+    int ok = orc_limiter_dmp(dim, order, V, nobs, luh + c * cell_d, relaxation, difference_scaling,
+                             bmin + c * nf * nobs, bmax + c * nf * nobs);
     if (admissibility && !lim_admissible(npc, planar, luh + c * cell_d)) ok = 0;
     if (!ok) {
       cure[c] = steps_till_cured + 1;
@@ -1480,8 +1494,8 @@ double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int 
   for (h = 0; h < 4; h++) {
     for (c = 0; c < nc; c++) {
       int s = tmp[c];
-      for (f = 0; f < 4; f++) {
-        const int t = tmp[lim_nb(n, c, f)] - 1;
+      for (f = 0; f < nf; f++) {
+        const int t = tmp[lim_nb(dim, n, c, f)] - 1;
         if (t > s) s = t;
       }
       status[c] = s;
@@ -1491,7 +1505,7 @@ double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int 
   /* 3. subcell patches of the previous solution (status >= NeighbourOfTroubled3) */
   for (c = 0; c < nc; c++) {
     if (status[c] >= 2) {
-      orc_limiter_project_on_fv(2, order, V, g, prev + c * cell_d, patch + c * patch_d);
+      orc_limiter_project_on_fv(dim, order, V, g, prev + c * cell_d, patch + c * patch_d);
       cnt[0]++;
     }
     if (status[c] >= 3) cnt[1]++;
@@ -1502,18 +1516,27 @@ double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int 
   for (c = 0; c < nc; c++) {
     if (status[c] < 3) continue;
     double* P = patch + c * patch_d;
-    const double* L = patch + lim_nb(n, c, 0) * patch_d;
-    const double* R = patch + lim_nb(n, c, 1) * patch_d;
-    const double* D = patch + lim_nb(n, c, 2) * patch_d;
-    const double* U = patch + lim_nb(n, c, 3) * patch_d;
-    for (i = 0; i < S; i++)
-      for (k = 0; k < g; k++)
-        for (m = 0; m < V; m++) {
-          P[((g + i) * SG + k) * V + m] = L[((g + i) * SG + S + k) * V + m];
-          P[((g + i) * SG + g + S + k) * V + m] = R[((g + i) * SG + g + k) * V + m];
-          P[(k * SG + g + i) * V + m] = D[((S + k) * SG + g + i) * V + m];
-          P[((g + S + k) * SG + g + i) * V + m] = U[((g + k) * SG + g + i) * V + m];
-        }
+    for (f = 0; f < nf; f++) {
+      const int d = f >> 1, up = f & 1;
+      const double* N = patch + lim_nb(dim, n, c, f) * patch_d;
+      const int zmax = dim == 3 ? S : 1;
+      for (a = 0; a < zmax; a++)
+        for (b = 0; b < S; b++)
+          for (k = 0; k < g; k++) {
+            /* coordinates along the face: (a, b) over the two other axes */
+            int dz, dy, dxx, sz, sy, sx;
+            const int gh = up ? g + S + k : k, src = up ? g + k : S + k;
+            if (d == 0) {
+              dz = sz = dim == 3 ? g + a : 0; dy = sy = g + b; dxx = gh; sx = src;
+            } else if (d == 1) {
+              dz = sz = dim == 3 ? g + a : 0; dxx = sx = g + b; dy = gh; sy = src;
+            } else {
+              dy = sy = g + a; dxx = sx = g + b; dz = gh; sz = src;
+            }
+            for (m = 0; m < V; m++)
+              P[lim_pt(dim, SG, dz, dy, dxx) * V + m] = N[lim_pt(dim, SG, sz, sy, sx) * V + m];
+          }
+    }
   }
   /* 5. FV step on those patches, projection back, limiter extrema
    * (recomputeSolution :1378-1441, determineLimiterMinAndMax :1118-1150) */
@@ -1521,19 +1544,24 @@ double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int 
     if (status[c] < 3) continue;
     double* P = patch + c * patch_d;
     memcpy(old, P, sizeof(double) * patch_d);
-    if (scheme == 0) orc_fv_godunov_2d(S, g, V, 0, planar, P, old, dx, dt);
-    else orc_fv_musclhancock_2d(S, g, V, 0, planar, P, old, dx, dt);
-    orc_limiter_project_on_dg(2, order, V, g, P, luh + c * cell_d);
-    orc_limiter_fv_min_max(2, order, V, nobs, g, P, bmin + c * 4 * nobs, bmax + c * 4 * nobs);
+    if (dim == 2) {
+      if (scheme == 0) orc_fv_godunov_2d(S, g, V, 0, planar, P, old, dx, dt);
+      else orc_fv_musclhancock_2d(S, g, V, 0, planar, P, old, dx, dt);
+    } else {
+      if (scheme == 0) orc_fv_godunov_3d(S, g, V, 0, P, old, dx, dt);
+      else orc_fv_musclhancock_3d(S, g, V, 0, P, old, dx, dt);
+    }
+    orc_limiter_project_on_dg(dim, order, V, g, P, luh + c * cell_d);
+    orc_limiter_fv_min_max(dim, order, V, nobs, g, P, bmin + c * nf * nobs, bmax + c * nf * nobs);
   }
   /* 6. next bounds */
-  lim_merge_bounds(n, nobs, bmin, bmax);
+  lim_merge_bounds(dim, n, nobs, bmin, bmax);
   if (counts) memcpy(counts, cnt, sizeof(cnt));
   free(prev);
   free(patch);
   free(old);
   free(tmp);
-  return orc_aderdg_grid_dt(2, order, planar, n, dx, luh, dt_policy, cfl);
+  return orc_aderdg_grid_dt(dim, order, planar, n, dx, luh, dt_policy, cfl);
 }
 
 /* ------------------------------------------------------------------ */

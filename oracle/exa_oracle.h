@@ -174,24 +174,25 @@ void orc_limiter_fv_min_max(int dim, int order, int nvar, int nobs, int ghost,
 int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, double relaxation,
                     double difference_scaling, double* obs_min, double* obs_max);
 
-/* One step of the limiting ADER-DG grid (periodic 2D, n[0] x n[1] cells,
- * order N, 5 variables), a restatement of LimitingADERDGSolver's step on a
- * uniform mesh: DG candidate with dt; DMP against bmin/bmax ([cell][4][nobs],
- * updated in place to the next step's bounds) and, if `admissibility`,
- * positive density and pressure at every node; statuses (status / cure per
- * cell, in/out; Ok 0 .. Troubled 5) with four hops of spreading; subcell FV
- * recomputation (scheme 0 Godunov, 1 MUSCL-Hancock) from the previous
- * solution for status >= 3, ghost subcells from the neighbours' projected
- * previous solutions (status >= 2); counts (nullable) = {cells with a patch,
- * FV cells, Troubled cells}.  Returns the next dt (orc_aderdg_grid_dt with
- * dt_policy / cfl on the final state). */
-double orc_limiting_grid_step_2d(int order, const int* n, const double* dx, int planar, double* luh,
-                                 int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
-                                 double relaxation, double difference_scaling, int steps_till_cured,
-                                 int admissibility, double dt, int dt_policy, double cfl, int* counts);
+/* One step of the limiting ADER-DG grid (periodic 2D or 3D, n[0] x n[1]
+ * (x n[2]) cells, order N, 5 variables), a restatement of
+ * LimitingADERDGSolver's step on a uniform mesh: DG candidate with dt; DMP
+ * against bmin/bmax ([cell][2 dim][nobs], updated in place to the next
+ * step's bounds) and, if `admissibility`, positive density and pressure at
+ * every node; statuses (status / cure per cell, in/out; Ok 0 .. Troubled 5)
+ * with four hops of spreading; subcell FV recomputation (scheme 0 Godunov,
+ * 1 MUSCL-Hancock) from the previous solution for status >= 3, ghost
+ * subcells from the neighbours' projected previous solutions (status >= 2);
+ * counts (nullable) = {cells with a patch, FV cells, Troubled cells}.
+ * Returns the next dt (orc_aderdg_grid_dt with dt_policy / cfl on the final
+ * state). */
+double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx, int planar, double* luh,
+                              int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
+                              double relaxation, double difference_scaling, int steps_till_cured, int admissibility,
+                              double dt, int dt_policy, double cfl, int* counts);
 /* bounds of the first DMP check: local extrema merged over faces */
-void orc_limiting_initial_bounds_2d(int order, const int* n, const double* luh, int nobs, double* bmin,
-                                    double* bmax);
+void orc_limiting_initial_bounds(int dim, int order, const int* n, const double* luh, int nobs, double* bmin,
+                                 double* bmax);
 
 /* counter-based noise shared with the device IC kernel */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx);

@@ -46,3 +46,20 @@ def smooth(order, n, length=(1.0, 1.0), amp=0.1):
     q[..., 2] = rho
     q[..., 4] = 1.0 / (GAMMA - 1) + 0.5 * 2 * rho
     return q.reshape(-1)
+
+
+def explosion3d(order, n, radius=0.25, inner=(1.0, 1.0), outer=(0.125, 0.1)):
+    """Spherical explosion in the periodic unit cube (cells x fastest, per
+    cell [z][y][x][variable])."""
+    xi = nodes(order)
+    nx, ny, nz = n
+    B = order + 1
+    X = (np.arange(nx)[None, None, :, None, None, None] + xi[None, None, None, None, None, :]) / nx
+    Y = (np.arange(ny)[None, :, None, None, None, None] + xi[None, None, None, None, :, None]) / ny
+    Z = (np.arange(nz)[:, None, None, None, None, None] + xi[None, None, None, :, None, None]) / nz
+    X, Y, Z = np.broadcast_arrays(X, Y, Z)  # [cz][cy][cx][iz][iy][ix]
+    inside = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2 < radius ** 2
+    q = np.zeros(X.shape + (5,))
+    q[..., 0] = np.where(inside, inner[0], outer[0])
+    q[..., 4] = np.where(inside, inner[1], outer[1]) / (GAMMA - 1)
+    return q.reshape(nz * ny * nx * B ** 3 * 5)

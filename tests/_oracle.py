@@ -83,10 +83,10 @@ def lib():
     L.orc_fv_stable_dt_3d.restype = d
     L.orc_fv_stable_dt_3d.argtypes = [i, i, i, i, _dp, _dp, d]
     L.orc_fv_periodic_ghosts_3d.argtypes = [i, i, i, _dp]
-    L.orc_limiting_grid_step_2d.restype = d
-    L.orc_limiting_grid_step_2d.argtypes = [i, _ip, _dp, i, _dp, _ip, _ip, _dp, _dp, i, i, d, d, i, i, d, i, d,
-                                            C.c_void_p]
-    L.orc_limiting_initial_bounds_2d.argtypes = [i, _ip, _dp, i, _dp, _dp]
+    L.orc_limiting_grid_step.restype = d
+    L.orc_limiting_grid_step.argtypes = [i, i, _ip, _dp, i, _dp, _ip, _ip, _dp, _dp, i, i, d, d, i, i, d, i, d,
+                                         C.c_void_p]
+    L.orc_limiting_initial_bounds.argtypes = [i, i, _ip, _dp, i, _dp, _dp]
     _lib = L
     return L
 
@@ -209,34 +209,38 @@ def limiter_dmp(dim, order, luh, bmin, bmax, relax, scaling, nvar=5, nobs=5):
 
 
 class LimitingGrid:
-    """Oracle state of the limiting ADER-DG grid (periodic 2D): the
-    restated step of orc_limiting_grid_step_2d with the same parameters as
+    """Oracle state of the limiting ADER-DG grid (periodic 2D or 3D): the
+    restated step of orc_limiting_grid_step with the same parameters as
     ADERDGGrid.set_limiter."""
 
-    def __init__(self, order, n, luh, length=(1.0, 1.0), scheme=0, nobs=5, relaxation=1e-4,
+    def __init__(self, order, n, luh, length=None, scheme=0, nobs=5, relaxation=1e-4,
                  difference_scaling=1e-3, steps_till_cured=0, check_admissibility=True, dt_policy=0, cfl=0.9,
                  planar=0):
-        self.order, self.n = order, np.asarray(n, dtype=np.int32)
-        self.dx = np.array([length[0] / n[0], length[1] / n[1]])
+        self.dim = len(n)
+        length = length or (1.0,) * self.dim
+        self.order = order
+        self.n = np.asarray(list(n) + [1] * (3 - self.dim), dtype=np.int32)
+        self.dx = np.array([length[i] / n[i] for i in range(self.dim)] + [1.0] * (3 - self.dim))
         self.luh = np.array(luh, dtype=np.float64)
-        nc = int(n[0] * n[1])
+        nc = int(np.prod(n))
+        nf = 2 * self.dim
         self.status = np.zeros(nc, dtype=np.int32)
         self.cure = np.zeros(nc, dtype=np.int32)
-        self.bmin = np.zeros(nc * 4 * nobs)
-        self.bmax = np.zeros(nc * 4 * nobs)
+        self.bmin = np.zeros(nc * nf * nobs)
+        self.bmax = np.zeros(nc * nf * nobs)
         self.p = (scheme, nobs, relaxation, difference_scaling, steps_till_cured, int(check_admissibility))
         self.dt_policy, self.cfl, self.planar = dt_policy, cfl, planar
-        lib().orc_limiting_initial_bounds_2d(order, self.n, self.luh, nobs, self.bmin, self.bmax)
-        self.dt = lib().orc_aderdg_grid_dt(2, order, planar, self.n, self.dx, self.luh, dt_policy, cfl)
+        lib().orc_limiting_initial_bounds(self.dim, order, self.n, self.luh, nobs, self.bmin, self.bmax)
+        self.dt = lib().orc_aderdg_grid_dt(self.dim, order, planar, self.n, self.dx, self.luh, dt_policy, cfl)
         self.counts = np.zeros(3, dtype=np.int32)
 
     def step(self):
         """one step with the current dt; returns the dt taken"""
         dt = self.dt
         s, nobs, rel, sc, cured, adm = self.p
-        self.dt = lib().orc_limiting_grid_step_2d(self.order, self.n, self.dx, self.planar, self.luh, self.status,
-                                                  self.cure, self.bmin, self.bmax, s, nobs, rel, sc, cured, adm,
-                                                  dt, self.dt_policy, self.cfl, self.counts.ctypes.data)
+        self.dt = lib().orc_limiting_grid_step(self.dim, self.order, self.n, self.dx, self.planar, self.luh,
+                                               self.status, self.cure, self.bmin, self.bmax, s, nobs, rel, sc,
+                                               cured, adm, dt, self.dt_policy, self.cfl, self.counts.ctypes.data)
         return dt
 
 
