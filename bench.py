@@ -826,13 +826,29 @@ def explosion_state(order, n, radius=0.25):
     return q.reshape(-1)
 
 
-def limiting_grid_measure(E, Timer, args, order=3, n=729, steps=20):
+def explosion_state_3d(order, n, radius=0.25):
+    """3D counterpart of explosion_state (sphere in the periodic unit cube)"""
+    xi = (np.polynomial.legendre.leggauss(order + 1)[0] + 1) / 2
+    c = np.arange(n)
+    X = (c[None, None, :, None, None, None] + xi[None, None, None, None, None, :]) / n
+    Y = (c[None, :, None, None, None, None] + xi[None, None, None, None, :, None]) / n
+    Z = (c[:, None, None, None, None, None] + xi[None, None, None, :, None, None]) / n
+    X, Y, Z = np.broadcast_arrays(X, Y, Z)
+    inside = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2 < radius ** 2
+    q = np.zeros(X.shape + (5,))
+    q[..., 0] = np.where(inside, 1.0, 0.125)
+    q[..., 4] = np.where(inside, 1.0, 0.1) / 0.4
+    return q.reshape(-1)
+
+
+def limiting_grid_measure(E, Timer, args, order=3, n=729, steps=20, dim=2):
     """ms per step of the limiting grid and of the same grid unlimited"""
-    res = {'workload': '%d^2 cells 2D N=%d, cylindrical explosion, Godunov subcells' % (n, order),
+    res = {'workload': '%d^%d cells %dD N=%d, %s explosion, Godunov subcells'
+                       % (n, dim, dim, order, 'cylindrical' if dim == 2 else 'spherical'),
            'steps': steps}
-    state = explosion_state(order, n)
+    state = explosion_state(order, n) if dim == 2 else explosion_state_3d(order, n)
     for name in ('unlimited', 'limited'):
-        g = E.ADERDGGrid(2, order, (n, n), length=(1.0, 1.0))
+        g = E.ADERDGGrid(dim, order, (n,) * dim, length=(1.0,) * dim)
         g.set_state(state)
         if name == 'limited':
             g.set_limiter()
@@ -846,7 +862,7 @@ def limiting_grid_measure(E, Timer, args, order=3, n=729, steps=20):
         t.stop(stream)
         ms = t.elapsed_ms() / steps
         E.device.synchronize()
-        res[name] = {'ms_per_step': ms, 'cell_updates_per_s': n * n / (ms * 1e-3),
+        res[name] = {'ms_per_step': ms, 'cell_updates_per_s': n ** dim / (ms * 1e-3),
                      'gpu_launches_per_step': (E.launch_count() - l0) / steps}
         if name == 'limited':
             _, counts = g.limiter_status()
@@ -854,6 +870,37 @@ def limiting_grid_measure(E, Timer, args, order=3, n=729, steps=20):
                               'troubled_cells': int(counts[2])})
         del g
     res['limiting_overhead'] = res['limited']['ms_per_step'] / res['unlimited']['ms_per_step'] - 1
+    return res
+
+
+def fv3d_measure(E, Timer, args, patch=9, npatches=32768):
+    """3D Godunov / MUSCL-Hancock on batches of 9^3 patches (the subcell
+    patches of N=4 cells), inputs larger than L2"""
+    from exahype_b200 import DeviceBuffer
+    from exahype_b200.fv import FVPatches
+    res = {'workload': '%d patches of %d^3 cells' % (npatches, patch)}
+    rng = np.random.default_rng(args.seed)
+    for name, scheme, g in (('godunov', 0, 1), ('musclhancock', 1, 2)):
+        S = patch + 2 * g
+        u = np.zeros((npatches, S ** 3, 5))
+        u[..., 0] = 1.0 + 0.1 * rng.random((npatches, S ** 3))
+        u[..., 4] = 2.5
+        d_old, d_new = DeviceBuffer.from_array(u.reshape(-1)), DeviceBuffer.from_array(u.reshape(-1))
+        fv = FVPatches(patch, g, [1.0, 1.0, 1.0], dim=3)
+        f = fv.godunov_update if scheme == 0 else fv.musclhancock_update
+        for _ in range(3):
+            f(npatches, d_new, d_old, 1e-4)
+        E.device.synchronize()
+        t = Timer()
+        t.start(None)
+        for _ in range(args.steps):
+            f(npatches, d_new, d_old, 1e-4)
+        t.stop(None)
+        ms = t.elapsed_ms() / args.steps
+        cells = npatches * patch ** 3
+        res[name] = {'ms_per_call': ms, 'cell_updates_per_s': cells / (ms * 1e-3),
+                     'hbm_gbs_at_80B': cells * 80 / (ms * 1e-3) / 1e9}
+        del d_old, d_new
     return res
 
 
@@ -905,6 +952,8 @@ def run_limiter(args, rank, world, dist):
     # limiting ADER-DG grid: 2D N=3 cylindrical explosion (discontinuous
     # density and pressure), with and without the limiter, graph-replayed
     lg = limiting_grid_measure(E, Timer, args)
+    lg3 = limiting_grid_measure(E, Timer, args, order=4, n=48, steps=10, dim=3)
+    fv3 = fv3d_measure(E, Timer, args)
     # CPU baseline: the reference's own Limiter.cpp (oracle/_ref) on a sample
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -934,7 +983,7 @@ def run_limiter(args, rank, world, dist):
                 'roofline': {'bound': 'hbm', 'achieved': out['project_on_fv']['hbm_gbs'],
                              'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s',
                              'frac': out['project_on_fv']['hbm_frac'], 'peak_source': peak_src},
-                'cpu_baseline': cpu, 'kernels': out, 'limiting_grid': lg}
+                'cpu_baseline': cpu, 'kernels': out, 'limiting_grid': lg, 'limiting_grid_3d': lg3, 'fv3d': fv3}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
