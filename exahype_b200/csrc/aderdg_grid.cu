@@ -107,7 +107,6 @@ struct exa_aderdg_grid {
   double* lim_bmin = nullptr;   // [cell][4 faces][nobs]
   double* lim_bmax = nullptr;
   double* lim_loc = nullptr;    // [cell][min | max][nobs]
-  double* lim_dt = nullptr;     // stable dt per cell
   int* lim_ok = nullptr;        // DMP and admissibility verdict per cell
   int* lim_status = nullptr;
   int* lim_status_tmp = nullptr;
@@ -227,15 +226,11 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
   const int dim = g->cfg.dim, order = g->cfg.order, nobs = L.nobs;
   const int S = 2 * order + 1, npc = dim == 3 ? (order + 1) * (order + 1) * (order + 1) : (order + 1) * (order + 1);
   const int planar = g->cfg.pde == EXA_PDE_EULER_PLANAR;
-  // the DMP pass also checks admissibility and takes every cell's stable dt
-  // of the candidate (the final state for all but the FV-updated cells)
-  const bool dt_on = g->cfg.dt_policy != 2;
   if (exa_status_t s = limiter_launch(kLimDmp, dim, order, kV, nobs, 0, g->ncells, g->luh, nullptr, g->lim_bmin,
                                       g->lim_bmax, g->lim_ok, L.relaxation, L.difference_scaling, g->st, nullptr,
-                                      nullptr, L.check_admissibility ? 0 : -1, dt_on ? g->lim_dt : nullptr,
-                                      g->dt_factor, g->desc.dx, planar))
+                                      nullptr))
     return s;
-  if (exa_status_t s = limiting_status(dim, g->cfg.n, npc, planar, 0,
+  if (exa_status_t s = limiting_status(dim, g->cfg.n, npc, planar, L.check_admissibility,
                                        L.steps_till_cured, g->luh, g->lim_ok, g->lim_status, g->lim_status_tmp,
                                        g->lim_cure, g->lim_list_patch, g->lim_list_fv, g->lim_counts, g->st))
     return s;
@@ -265,9 +260,8 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
     return s;
   if (exa_status_t s = limiting_check_finite(npc, g->luh, g->lim_list_fv, g->lim_counts + 1, &g->gd->nan_flag, g->st))
     return s;
-  if (dt_on)
-    return limiting_next_dt(dim, npc, planar, g->luh, g->lim_list_fv, g->lim_counts + 1, g->ncells, g->lim_dt,
-                            g->dt_factor, g->desc.dx, &g->gd->dt_next, g->st);
+  if (g->cfg.dt_policy != 2)
+    return launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr, &g->gd->dt_next, g->st);
   return EXA_OK;
 }
 
@@ -609,7 +603,7 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
   const size_t spc = g->cfg.dim == 3 ? (size_t)SG * SG * SG : (size_t)SG * SG;
   const size_t d_prev = (size_t)n * npc * kV, d_patch = (size_t)n * spc * kV;
   const size_t d_b = (size_t)n * 2 * g->cfg.dim * cfg->nobs, d_loc = (size_t)n * 2 * cfg->nobs;
-  const size_t doubles = d_prev + d_patch + 2 * d_b + d_loc + (size_t)n;
+  const size_t doubles = d_prev + d_patch + 2 * d_b + d_loc;
   const size_t ints = 6 * (size_t)n + 4;
   cudaError_t e = cudaMalloc(&g->lim_block, doubles * sizeof(double) + ints * sizeof(int));
   if (e != cudaSuccess) return cuda_status(e, "limiter allocation");
@@ -624,8 +618,6 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
   p += d_b;
   g->lim_loc = p;
   p += d_loc;
-  g->lim_dt = p;
-  p += n;
   int* q = reinterpret_cast<int*>(p);
   g->lim_ok = q;
   g->lim_status = q + n;

@@ -154,24 +154,15 @@ exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int
                              int* list_fv, int* counts, cudaStream_t st);
 exa_status_t limiting_merge_bounds(int dim, const int* ncell, int nobs, double* bmin, double* bmax, double* loc,
                                    cudaStream_t st);
-exa_status_t limiting_next_dt(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
-                              long ncells, double* dt_cell, double factor, const double* dx,
-                              unsigned long long* dt_min, cudaStream_t st);
 exa_status_t limiting_check_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag,
                                    cudaStream_t st);
 
 // limiter kernels (limiter.cu) on all cells, or on cells list[0 .. *count)
 // when list / count (device) are given
 enum LimiterOp { kLimToFv = 0, kLimToDg = 1, kLimMinMax = 2, kLimDmp = 3, kLimFvMinMax = 4 };
-// with op kLimDmp: admissibility >= 0 also requires positive density and
-// pressure at every node; dt_cell (nullable) receives each cell's stable dt
-// (dt_factor / sum_d |lambda_d| / dx_d over its nodes); planar selects the
-// planar Euler pressure for both
 exa_status_t limiter_launch(int op, int dim, int order, int nvar, int nobs, int ghost, long ncells, const double* in,
                             double* out, double* mn, double* mx, int* ok, double relax, double scaling,
-                            cudaStream_t st, const int* list, const int* count, int admissibility = -1,
-                            double* dt_cell = nullptr, double dt_factor = 0.0, const double* dx = nullptr,
-                            int planar = 0);
+                            cudaStream_t st, const int* list, const int* count);
 // host copy of the derived tables (same bytes as the device constants)
 const void* host_dg_tables(size_t* bytes);
 const void* host_dg_tables_f(size_t* bytes);  // FP32 copies (DGConstF)

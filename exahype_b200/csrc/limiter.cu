@@ -195,26 +195,12 @@ struct LimOcc {
   static constexpr int value = B <= 4 ? 4 : (B == 5 ? 3 : 1);
 };
 
-// Extra per-node work of the limiting grid's DMP pass (5 Euler variables):
-// physical admissibility (admissibility != -1) folded
-// into the verdict, and the stable dt of the candidate per cell (dt_cell
-// non-null; the reference's stableTimeStepSize rule factor / sum_d
-// |lambda_d| / dx_d, minimum over the nodes).
-struct LimGridExtras {
-  int admissibility = -1;
-  int planar = 0;  // planar Euler pressure (2D kernel-test form)
-  double* dt_cell = nullptr;
-  double dt_factor = 0.0;
-  double dx[3] = {1.0, 1.0, 1.0};
-};
-
 // Optional cell selection: the kernels run on cells list[0 .. *count) (at
 // most ncells) instead of cells 0 .. ncells; a device-resident count lets a
 // fixed launch sequence serve a selection that changes from step to step.
 struct LimSel {
   const int* list = nullptr;
   const int* count = nullptr;
-  LimGridExtras ex;  // DMP pass of the limiting grid only
   __device__ __forceinline__ long cells(long ncells) const {
     return count ? min(ncells, (long)*count) : ncells;
   }
@@ -362,28 +348,6 @@ __global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
 }
 
 // ------------------------------------------------ min/max and the DMP
-template <int DIM>
-__device__ __forceinline__ void lim_grid_node_checks(const double* A, int nvar, int npc, int nc, long c0,
-                                                     const LimGridExtras& ex, int* dmp_ok,
-                                                     unsigned long long* s_dt) {
-  const bool planar = ex.planar != 0;
-  for (int i = threadIdx.x; i < nc * npc; i += kLimNT) {
-    const double* q = A + i * nvar;
-    const int c = i / npc;
-    if (ex.admissibility >= 0) {
-      const double j2 = planar ? q[1] * q[1] + q[2] * q[2] : q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
-      const double p = (kGamma - 1.0) * (q[4] - 0.5 * j2 / q[0]);
-      if (!(q[0] > 0.0 && p > 0.0 && isfinite(p))) atomicAnd(dmp_ok + c0 + c, 0);
-    }
-    if (ex.dt_cell) {
-      double den = 0.0;
-      for (int d = 0; d < DIM; d++) den += (planar ? euler_max_eig<true>(q, d) : euler_max_eig<false>(q, d)) / ex.dx[d];
-      const double dt = ex.dt_factor / den;
-      if (dt >= 0.0) atomicMin(s_dt + c, (unsigned long long)__double_as_longlong(dt));
-    }
-  }
-}
-
 // The Gauss-Lobatto (B -> B) and subcell (B -> S) evaluations run side by
 // side, pass by pass; the first pass also takes the extrema of the nodes
 // (its input lines).  Per cell and observable, shared memory holds: the
@@ -410,17 +374,10 @@ struct LimMM {
 // mode 0: findCellLocalMinAndMax, result copied to all faces;
 // mode 1: discreteMaximumPrincipleAndMinAndMaxSearch (obs_min/max in/out,
 //         dmp_ok[cell] = 1 if the DMP holds).
-template <int B, bool EXTRAS>
-struct LimOccMM {
-  // the limiting grid's variant (per-node admissibility and dt) needs more
-  // registers than the plain search
-  static constexpr int value = EXTRAS ? (B <= 4 ? 3 : (B == 5 ? 2 : 1)) : LimOcc<B>::value;
-};
-
-template <int DIM, int B, int NVT, bool EXTRAS>
-__global__ void __launch_bounds__(kLimNT, LimOccMM<B, EXTRAS>::value)
+template <int DIM, int B, int NVT>
+__global__ void __launch_bounds__(kLimNT, LimOcc<B>::value)
     k_lim_min_max(int mode, int nvar_rt, int nobs_rt, long ncells, int cpb, const double* luh, double relaxation,
-                  double scaling, double* obs_min, double* obs_max, int* dmp_ok, LimGridExtras ex) {
+                  double scaling, double* obs_min, double* obs_max, int* dmp_ok) {
   using M = LimMM<DIM, B>;
   constexpr int S = M::S, NPC = M::NPC, NF = 2 * DIM;
   const int nvar = NVT ? NVT : nvar_rt;
@@ -440,15 +397,10 @@ __global__ void __launch_bounds__(kLimNT, LimOccMM<B, EXTRAS>::value)
   double* pn_mx = pmx;
   double* pl_mx = pmx + cpb * M::NODE_LINES * nobs;
   double* ps_mx = pl_mx + cpb * M::LOB_LINES * nobs;
-  __shared__ unsigned long long s_dt[EXTRAS ? 64 : 1];
   if (mode == 1)
-    for (int c = threadIdx.x; c < nc; c += kLimNT) {
-      dmp_ok[c0 + c] = 1;
-      if (EXTRAS) s_dt[c] = 0x7FF0000000000000ULL;  // +inf
-    }
+    for (int c = threadIdx.x; c < nc; c += kLimNT) dmp_ok[c0 + c] = 1;
   lim_copy_in(A, luh + c0 * NPC * nvar, (long)nc * NPC * nvar);
   __syncthreads();
-  if (EXTRAS && mode == 1) lim_grid_node_checks<DIM>(A, nvar, NPC, nc, c0, ex, dmp_ok, s_dt);
   const int ix = nc * M::NODE_LINES * nobs;  // items of one pass-x
   if (DIM == 2) {
     SmemOutInputMinMax ol{{XL, nobs, B * B * nobs, B, B}, pn_mn, pn_mx};
@@ -538,10 +490,6 @@ __global__ void __launch_bounds__(kLimNT, LimOccMM<B, EXTRAS>::value)
       }
       if (lane == 0) finish(pair, mn, mx);
     }
-  }
-  if (EXTRAS && mode == 1 && ex.dt_cell) {
-    __syncthreads();
-    for (int c = threadIdx.x; c < nc; c += kLimNT) ex.dt_cell[c0 + c] = __longlong_as_double((long long)s_dt[c]);
   }
 }
 
@@ -653,12 +601,11 @@ static exa_status_t lim_run(int op, int nvar, int nobs, int ghost, long ncells, 
       k_lim_fv_min_max<DIM, B><<<(unsigned)nblk, kLimNT, smem, st>>>(nvar, nobs, ghost, ncells, cpb, in, mn, mx,
                                                                        sel);
   } else {
-    const bool extras = sel.ex.admissibility >= 0 || sel.ex.dt_cell;
-    auto kern = extras ? k_lim_min_max<DIM, B, NVT, true> : k_lim_min_max<DIM, B, NVT, false>;
+    auto kern = k_lim_min_max<DIM, B, NVT>;
     e = lim_prepare(kern, smem);
     if (e == cudaSuccess)
       kern<<<(unsigned)nblk, kLimNT, smem, st>>>(op == kLimDmp ? 1 : 0, nvar, nobs, ncells, cpb, in, relax, scaling, mn,
-                                                  mx, ok, sel.ex);
+                                                  mx, ok);
   }
   if (e != cudaSuccess) return cuda_status(e, "limiter: shared-memory attribute");
   count_launch();
@@ -717,21 +664,10 @@ static exa_status_t lim_entry(int op, int dim, int order, int nvar, int nobs, in
 
 exa_status_t limiter_launch(int op, int dim, int order, int nvar, int nobs, int ghost, long ncells, const double* in,
                             double* out, double* mn, double* mx, int* ok, double relax, double scaling,
-                            cudaStream_t st, const int* list, const int* count, int admissibility,
-                            double* dt_cell, double dt_factor, const double* dx, int planar) {
+                            cudaStream_t st, const int* list, const int* count) {
   LimSel sel;
   sel.list = list;
   sel.count = count;
-  if (op == kLimDmp) {
-    if ((admissibility >= 0 || dt_cell) && nvar != 5)
-      return set_error(EXA_EINVAL, "limiter: admissibility / dt need the 5 Euler variables");
-    sel.ex.admissibility = admissibility < 0 ? -1 : 1;
-    sel.ex.planar = planar;
-    sel.ex.dt_cell = dt_cell;
-    sel.ex.dt_factor = dt_factor;
-    if (dx)
-      for (int d = 0; d < dim; d++) sel.ex.dx[d] = dx[d];
-  }
   return lim_entry(op, dim, order, nvar, nobs, ghost, ncells, in, out, mn, mx, ok, relax, scaling,
                    reinterpret_cast<void*>(st), sel);
 }

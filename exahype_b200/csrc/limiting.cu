@@ -129,59 +129,7 @@ __global__ void k_lim_finite(int npc, const double* luh, const int* list, const 
   }
 }
 
-// stable dt of the FV-updated cells' final state (one warp per listed cell,
-// the rule of k_stable_dt), over their candidate values in dt_cell
-__global__ void k_lim_dt_listed(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
-                                double* dt_cell, double factor, double dx0, double dx1, double dx2) {
-  const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  const long n = *count;
-  for (long e = w; e < n; e += ((long)gridDim.x * blockDim.x) >> 5) {
-    const long cell = list[e];
-    double dt = DBL_MAX;
-    for (int s = lane; s < npc; s += 32) {
-      const double* q = luh + (cell * npc + s) * kV;
-      double den = 0.0;
-      den += (planar ? euler_max_eig<true>(q, 0) : euler_max_eig<false>(q, 0)) / dx0;
-      den += (planar ? euler_max_eig<true>(q, 1) : euler_max_eig<false>(q, 1)) / dx1;
-      if (dim == 3) den += euler_max_eig<false>(q, 2) / dx2;
-      dt = fmin(dt, factor / den);
-    }
-    for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
-    if (lane == 0) dt_cell[cell] = dt;
-  }
-}
-
-// minimum of the per-cell dt, one atomic per CTA
-__global__ void k_lim_dt_reduce(long n, const double* dt_cell, unsigned long long* dt_min) {
-  __shared__ double wmin[8];
-  double dt = DBL_MAX;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    dt = fmin(dt, dt_cell[i]);
-  for (int o = 16; o > 0; o >>= 1) dt = fmin(dt, __shfl_xor_sync(0xffffffffu, dt, o));
-  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = dt;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int w = 1; w < (int)(blockDim.x >> 5); w++) dt = fmin(dt, wmin[w]);
-    atomic_min_pos_double(dt_min, dt);
-  }
-}
-
 static unsigned blocks(long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
-
-exa_status_t limiting_next_dt(int dim, int npc, int planar, const double* luh, const int* list, const int* count,
-                              long ncells, double* dt_cell, double factor, const double* dx,
-                              unsigned long long* dt_min, cudaStream_t st) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_lim_dt_listed<<<(unsigned)(4 * sms), 256, 0, st>>>(dim, npc, planar, luh, list, count, dt_cell, factor, dx[0],
-                                                       dx[1], dim == 3 ? dx[2] : 1.0);
-  const long nb = blocks(ncells, 256);
-  k_lim_dt_reduce<<<(unsigned)(nb < 2L * sms ? nb : 2L * sms), 256, 0, st>>>(ncells, dt_cell, dt_min);
-  count_launch(2);
-  return cuda_status(cudaGetLastError(), "limiter next dt");
-}
 
 static LimGrid lim_grid(int dim, const int* n) {
   LimGrid G;
