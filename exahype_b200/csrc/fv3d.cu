@@ -17,7 +17,12 @@
 
 namespace exa {
 
-constexpr int FV3_NT = 256;
+// threads per CTA: MUSCL-Hancock's staging (117 KB for 9^3 patches) leaves
+// one CTA per SM, so it runs 512 threads; Godunov fits several 256-thread CTAs
+template <int SCHEME>
+struct FV3Threads {
+  static constexpr int value = SCHEME == 1 ? 512 : 256;
+};
 
 struct FV3Args {
   int P, g, S, D;
@@ -70,8 +75,9 @@ __device__ __forceinline__ void fv3_face_value(const double* su, const double* q
 }
 
 template <int SCHEME>
-__global__ void __launch_bounds__(FV3_NT) k_fv3_patch(FV3Args a) {
+__global__ void __launch_bounds__(FV3Threads<SCHEME>::value) k_fv3_patch(FV3Args a) {
   constexpr int V = kV;
+  constexpr int FV3_NT = FV3Threads<SCHEME>::value;
   extern __shared__ double sm[];
   __shared__ double sred[FV3_NT / 32];
   const int P = a.P, g = a.g, S = a.S, D = a.D;
@@ -261,7 +267,7 @@ exa_status_t fv3_update(int scheme, int P, int g, int D, const double* h, long n
     grid = npatches < 4L * sms ? npatches : 4L * sms;  // CTAs loop over the listed patches
   }
   if (grid > 0x7fffffffL) return set_error(EXA_EINVAL, "3D FV: too many patches");
-  kern<<<(unsigned)grid, FV3_NT, smem, st>>>(a);
+  kern<<<(unsigned)grid, scheme == 0 ? FV3Threads<0>::value : FV3Threads<1>::value, smem, st>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_fv3_patch");
 }
