@@ -211,7 +211,7 @@ class ADERDGGrid:
     # -- a-posteriori subcell limiter (exa_aderdg_grid_set_limiter) --
     def set_limiter(self, scheme=0, nobs=5, relaxation=1e-4, difference_scaling=1e-3, steps_till_cured=0,
                     check_admissibility=True, enable=True):
-        """Limiting ADER-DG (periodic 2D or 3D): DMP + admissibility check of every
+        """Limiting ADER-DG (2D or 3D, any boundary rules): DMP + admissibility check of every
         step's DG candidate, subcell FV recomputation (scheme 0 Godunov, 1
         MUSCL-Hancock) of troubled cells and their neighbours."""
         if not enable:

@@ -230,7 +230,7 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
                                       g->lim_bmax, g->lim_ok, L.relaxation, L.difference_scaling, g->st, nullptr,
                                       nullptr))
     return s;
-  if (exa_status_t s = limiting_status(dim, g->cfg.n, npc, planar, L.check_admissibility,
+  if (exa_status_t s = limiting_status(dim, g->cfg.n, g->bc, npc, planar, L.check_admissibility,
                                        L.steps_till_cured, g->luh, g->lim_ok, g->lim_status, g->lim_status_tmp,
                                        g->lim_cure, g->lim_list_patch, g->lim_list_fv, g->lim_counts, g->st))
     return s;
@@ -241,12 +241,12 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
   if (dim == 2) {
     if (exa_status_t s = fv_subcell_step(L.scheme, planar, S, g->lim_ghost, g->cfg.n[0], g->cfg.n[1],
                                          g->desc.dx[0] / S, g->desc.dx[1] / S, g->lim_patch, g->lim_list_fv,
-                                         g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
+                                         g->lim_counts + 1, g->ncells, &g->gd->dt, g->st, g->bc))
       return s;
   } else {
     const double h[3] = {g->desc.dx[0] / S, g->desc.dx[1] / S, g->desc.dx[2] / S};
     if (exa_status_t s = fv3_subcell_step(L.scheme, S, g->lim_ghost, g->cfg.n, h, g->lim_patch, g->lim_list_fv,
-                                          g->lim_counts + 1, g->ncells, &g->gd->dt, g->st))
+                                          g->lim_counts + 1, g->ncells, &g->gd->dt, g->st, g->bc))
       return s;
   }
   if (exa_status_t s = limiter_launch(kLimToDg, dim, order, kV, 0, g->lim_ghost, g->ncells, g->lim_patch, g->luh,
@@ -256,7 +256,7 @@ static exa_status_t grid_limit(exa_aderdg_grid* g) {
                                       nullptr, g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, g->lim_list_fv,
                                       g->lim_counts + 1))
     return s;
-  if (exa_status_t s = limiting_merge_bounds(dim, g->cfg.n, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
+  if (exa_status_t s = limiting_merge_bounds(dim, g->cfg.n, g->bc, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
     return s;
   if (exa_status_t s = limiting_check_finite(npc, g->luh, g->lim_list_fv, g->lim_counts + 1, &g->gd->nan_flag, g->st))
     return s;
@@ -275,7 +275,7 @@ static exa_status_t grid_limiter_reset(exa_aderdg_grid* g) {
   if (exa_status_t s = limiter_launch(kLimMinMax, g->cfg.dim, g->cfg.order, kV, nobs, 0, g->ncells, g->luh, nullptr,
                                       g->lim_bmin, g->lim_bmax, nullptr, 0, 0, g->st, nullptr, nullptr))
     return s;
-  if (exa_status_t s = limiting_merge_bounds(g->cfg.dim, g->cfg.n, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
+  if (exa_status_t s = limiting_merge_bounds(g->cfg.dim, g->cfg.n, g->bc, nobs, g->lim_bmin, g->lim_bmax, g->lim_loc, g->st))
     return s;
   return cuda_status(cudaStreamSynchronize(g->st), "limiter reset");
 }
@@ -553,9 +553,6 @@ exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc) {
     if (bc[i] < EXA_BC_PERIODIC || bc[i] > EXA_BC_REFLECT) return set_error(EXA_EINVAL, "unknown boundary rule");
   if (g->halo && bc[g->cfg.dim - 1] != EXA_BC_PERIODIC)
     return set_error(EXA_EINVAL, "slab halos need a periodic last dimension");
-  if (g->lim_on)
-    for (int i = 0; i < g->cfg.dim; i++)
-      if (bc[i] != EXA_BC_PERIODIC) return set_error(EXA_EINVAL, "the limiter needs periodic boundaries");
   for (int i = 0; i < 3; i++) g->bc[i] = i < g->cfg.dim ? bc[i] : 0;
   if (g->graph) {  // the captured step holds the old arguments
     cudaGraphExecDestroy(g->graph);
@@ -578,8 +575,6 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
     return EXA_OK;
   }
   if (g->halo) return set_error(EXA_EINVAL, "limiter: not with slab halos");
-  for (int i = 0; i < g->cfg.dim; i++)
-    if (g->bc[i] != EXA_BC_PERIODIC) return set_error(EXA_EINVAL, "limiter: periodic boundaries only");
   if (g->cfg.dim == 3) {
     // one CTA stages a subcell patch with its ghosts (fv3d.cu)
     const int S = 2 * g->cfg.order + 1, gw = cfg->scheme == 0 ? 1 : 2;

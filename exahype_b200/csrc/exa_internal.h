@@ -129,11 +129,16 @@ exa_status_t upload_tables_limiter();
 // cells list[0 .. *count) of a periodic npx x npy grid: face ghosts from the
 // neighbour cells' patches, then the update in place with *dt_dev (fv.cu);
 // the 3D counterpart on an n[0] x n[1] x n[2] grid (fv3d.cu)
+// bc[d] (nullable: periodic) = EXA_BC_*: at a domain boundary the ghosts
+// come from the patch's own boundary layers (the reference's
+// boundaryLayerExtraction / ghostLayerFillingAtBoundary, commons.cpph:
+// 100-340), with the normal momentum negated for reflecting walls
 exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int npy, double hx, double hy,
                              double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
-                             cudaStream_t st);
+                             cudaStream_t st, const int* bc = nullptr);
 exa_status_t fv3_subcell_step(int scheme, int P, int g, const int* n, const double* h, double* lim, const int* list,
-                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st);
+                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st,
+                              const int* bc = nullptr);
 
 // 3D finite volumes (fv3d.cu): one CTA per patch of P^3 cells + g ghost
 // layers, [z][y][x][D]; h = cell sizes; dt read from dt_dev when non-null;
@@ -149,11 +154,11 @@ size_t fv3_smem(int P, int g, int scheme);
 // limiting-grid bookkeeping (limiting.cu): status from the DMP /
 // admissibility verdicts with spreading and the cell lists; the merge of
 // the per-cell extrema over faces; a finiteness check of listed cells
-exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int admissibility, int steps_till_cured,
-                             const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
-                             int* list_fv, int* counts, cudaStream_t st);
-exa_status_t limiting_merge_bounds(int dim, const int* ncell, int nobs, double* bmin, double* bmax, double* loc,
-                                   cudaStream_t st);
+exa_status_t limiting_status(int dim, const int* ncell, const int* bc, int npc, int planar, int admissibility,
+                             int steps_till_cured, const double* luh, int* ok, int* status, int* status_tmp,
+                             int* cure, int* list_patch, int* list_fv, int* counts, cudaStream_t st);
+exa_status_t limiting_merge_bounds(int dim, const int* ncell, const int* bc, int nobs, double* bmin, double* bmax,
+                                   double* loc, cudaStream_t st);
 exa_status_t limiting_check_finite(int npc, const double* luh, const int* list, const int* count, int* nan_flag,
                                    cudaStream_t st);
 

@@ -1168,8 +1168,12 @@ inline size_t fv_small_smem(int P, int g, int scheme) {
 // Subcell patches of the limiting ADER-DG grid: patch `cell` of a periodic
 // npx x npy grid of cells.  Face ghosts of the listed patches from the face
 // neighbours' boundary layers (grid-stride over list entries x ghosts).
-__global__ void k_fv_subcell_exchange(int P, int g, int npx, int npy, double* lim, const int* list,
-                                      const int* count) {
+// at a domain-boundary face (bcx / bcy != 0) the ghosts mirror the patch's
+// own boundary layers, ghost k <- interior g - 1 - k counted from the face
+// (FiniteVolumesSolver::mergeWithBoundaryData with commons.cpph:175-340),
+// the normal momentum negated for a reflecting wall
+__global__ void k_fv_subcell_exchange(int P, int g, int npx, int npy, int bcx, int bcy, double* lim,
+                                      const int* list, const int* count) {
   const int S = P + 2 * g;
   const long per = 4L * g * P;
   const long total = (long)*count * per;
@@ -1178,33 +1182,42 @@ __global__ void k_fv_subcell_exchange(int P, int g, int npx, int npy, double* li
     const int r = (int)(gid % per);
     const int side = r / (g * P), i = (r / g) % P, k = r % g;
     const int px = (int)(patch % npx), py = (int)(patch / npx);
-    int j, x, nj, nx, qx = px, qy = py;
+    int j, x, nj, nx, qx = px, qy = py, flip = -1;
     if (side == 0) {
-      j = g + i; x = k; qx = (px + npx - 1) % npx; nj = j; nx = P + k;
+      j = g + i; x = k; nj = j;
+      if (bcx && px == 0) { nx = 2 * g - 1 - k; flip = bcx == EXA_BC_REFLECT ? 1 : -1; }
+      else { qx = (px + npx - 1) % npx; nx = P + k; }
     } else if (side == 1) {
-      j = g + i; x = g + P + k; qx = (px + 1) % npx; nj = j; nx = g + k;
+      j = g + i; x = g + P + k; nj = j;
+      if (bcx && px == npx - 1) { nx = g + P - 1 - k; flip = bcx == EXA_BC_REFLECT ? 1 : -1; }
+      else { qx = (px + 1) % npx; nx = g + k; }
     } else if (side == 2) {
-      j = k; x = g + i; qy = (py + npy - 1) % npy; nj = P + k; nx = x;
+      j = k; x = g + i; nx = x;
+      if (bcy && py == 0) { nj = 2 * g - 1 - k; flip = bcy == EXA_BC_REFLECT ? 2 : -1; }
+      else { qy = (py + npy - 1) % npy; nj = P + k; }
     } else {
-      j = g + P + k; x = g + i; qy = (py + 1) % npy; nj = g + k; nx = x;
+      j = g + P + k; x = g + i; nx = x;
+      if (bcy && py == npy - 1) { nj = g + P - 1 - k; flip = bcy == EXA_BC_REFLECT ? 2 : -1; }
+      else { qy = (py + 1) % npy; nj = g + k; }
     }
     const long src_patch = (long)qy * npx + qx;
     double* dst = lim + (patch * S * S + (long)j * S + x) * kV;
     const double* src = lim + (src_patch * S * S + (long)nj * S + nx) * kV;
 #pragma unroll
-    for (int m = 0; m < kV; m++) dst[m] = src[m];
+    for (int m = 0; m < kV; m++) dst[m] = m == flip ? -src[m] : src[m];
   }
 }
 
 exa_status_t fv_subcell_step(int scheme, int planar, int P, int g, int npx, int npy, double hx, double hy,
                              double* lim, const int* list, const int* count, long maxcells, const double* dt_dev,
-                             cudaStream_t st) {
+                             cudaStream_t st, const int* bc) {
   if (P > kFvSmallMax || (scheme == 0 && g < 1) || (scheme == 1 && g < 2))
     return set_error(EXA_EINVAL, "subcell FV: patch too large or ghost layer too thin");
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_fv_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, npx, npy, lim, list, count);
+  k_fv_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, npx, npy, bc ? bc[0] : 0, bc ? bc[1] : 0, lim,
+                                                              list, count);
   count_launch();
   if (exa_status_t s = cuda_status(cudaGetLastError(), "k_fv_subcell_exchange")) return s;
   FVArgs a{};

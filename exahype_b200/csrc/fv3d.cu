@@ -273,9 +273,15 @@ exa_status_t fv3_update(int scheme, int P, int g, int D, const double* h, long n
 }
 
 // face ghosts of the listed 3D subcell patches from the face neighbours'
-// boundary layers (periodic grid of n[0] x n[1] x n[2] cells, x fastest);
-// grid-stride over list entries x face ghosts
-__global__ void k_fv3_subcell_exchange(int P, int g, int nx, int ny, int nz, double* lim, const int* list,
+// boundary layers (grid of n[0] x n[1] x n[2] cells, x fastest).  At a
+// domain-boundary face (bc[d] != 0) the ghosts mirror the patch's own
+// boundary layers, ghost layer k <- interior layer k counted from the face
+// (FiniteVolumesSolver::mergeWithBoundaryData: boundaryLayerExtraction,
+// boundaryConditions with its mirrored index K = g - 1 - k, and
+// ghostLayerFillingAtBoundary, commons.cpph:502-875), the normal momentum
+// negated for a reflecting wall.  Grid-stride over list entries x face
+// ghosts.
+__global__ void k_fv3_subcell_exchange(int P, int g, int nx, int ny, int nz, int3 bc, double* lim, const int* list,
                                        const int* count) {
   const int S = P + 2 * g;
   const long S3 = (long)S * S * S;
@@ -300,24 +306,36 @@ __global__ void k_fv3_subcell_exchange(int P, int g, int nx, int ny, int nz, dou
     si[ax] = src;
     di[o1] = si[o1] = g + a;
     di[o2] = si[o2] = g + b;
-    if (d == 0) x = up ? (x + 1 == nx ? 0 : x + 1) : (x == 0 ? nx - 1 : x - 1);
-    else if (d == 1) y = up ? (y + 1 == ny ? 0 : y + 1) : (y == 0 ? ny - 1 : y - 1);
-    else z = up ? (z + 1 == nz ? 0 : z + 1) : (z == 0 ? nz - 1 : z - 1);
-    const long nbp = ((long)z * ny + y) * nx + x;
+    int* p = d == 0 ? &x : (d == 1 ? &y : &z);
+    const int n = d == 0 ? nx : (d == 1 ? ny : nz);
+    const int rule = d == 0 ? bc.x : (d == 1 ? bc.y : bc.z);
+    long nbp;
+    if (rule != 0 && (up ? *p + 1 == n : *p == 0)) {
+      nbp = patch;
+      // lower y and z faces: every ghost layer repeats the layer next to the
+      // face (the reference's 3D extraction reads patchBegin for every
+      // layer there, commons.cpph:561 and 591)
+      si[ax] = up ? g + P - 1 - layer : (d > 0 ? g : 2 * g - 1 - layer);
+    } else {
+      *p = up ? (*p + 1 == n ? 0 : *p + 1) : (*p == 0 ? n - 1 : *p - 1);
+      nbp = ((long)z * ny + y) * nx + x;
+    }
+    const int flip = nbp == patch && rule == EXA_BC_REFLECT ? 1 + d : -1;
     double* dst = lim + patch * S3 * kV + (((long)di[0] * S + di[1]) * S + di[2]) * kV;
     const double* s = lim + nbp * S3 * kV + (((long)si[0] * S + si[1]) * S + si[2]) * kV;
 #pragma unroll
-    for (int m = 0; m < kV; m++) dst[m] = s[m];
+    for (int m = 0; m < kV; m++) dst[m] = m == flip ? -s[m] : s[m];
   }
 }
 
 exa_status_t fv3_subcell_step(int scheme, int P, int g, const int* n, const double* h, double* lim, const int* list,
-                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st) {
+                              const int* count, long maxcells, const double* dt_dev, cudaStream_t st, const int* bc) {
   if ((scheme == 0 && g < 1) || (scheme == 1 && g < 2)) return set_error(EXA_EINVAL, "subcell FV: ghost layer too thin");
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_fv3_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, n[0], n[1], n[2], lim, list, count);
+  const int3 rules = bc ? make_int3(bc[0], bc[1], bc[2]) : make_int3(0, 0, 0);
+  k_fv3_subcell_exchange<<<(unsigned)(8 * sms), 256, 0, st>>>(P, g, n[0], n[1], n[2], rules, lim, list, count);
   count_launch();
   if (exa_status_t s = cuda_status(cudaGetLastError(), "k_fv3_subcell_exchange")) return s;
   // in place: each CTA stages its patch before it writes

@@ -1,6 +1,6 @@
 // Cell-status and bookkeeping kernels of the limiting ADER-DG grid (the
 // a-posteriori subcell limiter of exahype/solvers/LimitingADERDGSolver.cpp on
-// a uniform periodic 2D or 3D grid).  Per step, after the unlimited DG candidate:
+// a uniform 2D or 3D grid, periodic or with outflow / reflecting walls).  Per step, after the unlimited DG candidate:
 //   k_lim_admissible   physical admissibility of the candidate (positive
 //                      density and pressure at every node), folded into the
 //                      DMP verdict (LimitingADERDGSolver.cpp:839-876,
@@ -58,18 +58,25 @@ __global__ void k_lim_base_status(long ncells, const int* ok, int* status, int* 
   status[c] = base;
 }
 
-// grid of n.x x n.y x n.z cells (n.z = 1 in 2D), x fastest, periodic
+// grid of n.x x n.y x n.z cells (n.z = 1 in 2D), x fastest; bc[d] = 0
+// periodic, else the domain ends in direction d
 struct LimGrid {
   int nx, ny, nz, dim;
+  int bc[3];
   __host__ __device__ __forceinline__ long cells() const { return (long)nx * ny * nz; }
-  // the neighbour across face f = 2 d + (0 lower, 1 upper)
+  // the neighbour across face f = 2 d + (0 lower, 1 upper), -1 outside
   __device__ __forceinline__ long nb(long c, int f) const {
     int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((long)nx * ny));
     const int d = f >> 1;
     const bool up = f & 1;
-    if (d == 0) x = up ? (x + 1 == nx ? 0 : x + 1) : (x == 0 ? nx - 1 : x - 1);
-    else if (d == 1) y = up ? (y + 1 == ny ? 0 : y + 1) : (y == 0 ? ny - 1 : y - 1);
-    else z = up ? (z + 1 == nz ? 0 : z + 1) : (z == 0 ? nz - 1 : z - 1);
+    int* p = d == 0 ? &x : (d == 1 ? &y : &z);
+    const int n = d == 0 ? nx : (d == 1 ? ny : nz);
+    if (up ? *p + 1 == n : *p == 0) {
+      if (bc[d] != 0) return -1;
+      *p = up ? 0 : n - 1;
+    } else {
+      *p += up ? 1 : -1;
+    }
     return ((long)z * ny + y) * nx + x;
   }
 };
@@ -78,7 +85,10 @@ __global__ void k_lim_spread(LimGrid G, const int* in, int* out) {
   const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= G.cells()) return;
   int nb = 0;
-  for (int f = 0; f < 2 * G.dim; f++) nb = max(nb, in[G.nb(c, f)]);
+  for (int f = 0; f < 2 * G.dim; f++) {
+    const long o = G.nb(c, f);
+    if (o >= 0) nb = max(nb, in[o]);
+  }
   out[c] = max(in[c], nb - 1);
 }
 
@@ -113,7 +123,8 @@ __global__ void k_lim_merge(LimGrid G, int nobs, const double* loc, double* bmin
   const int nf = 2 * G.dim;
   const double mo = loc[(c * 2) * nobs + v], xo = loc[(c * 2 + 1) * nobs + v];
   for (int f = 0; f < nf; f++) {
-    const long nb = G.nb(c, f);
+    const long nb0 = G.nb(c, f);
+    const long nb = nb0 >= 0 ? nb0 : c;  // a domain-boundary face keeps the cell's own extrema
     const double mn = loc[(nb * 2) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
     bmin[(c * nf + f) * nobs + v] = mn < mo ? mn : mo;
     bmax[(c * nf + f) * nobs + v] = xo < xn ? xn : xo;
@@ -131,19 +142,20 @@ __global__ void k_lim_finite(int npc, const double* luh, const int* list, const 
 
 static unsigned blocks(long n, int nt) { return (unsigned)((n + nt - 1) / nt); }
 
-static LimGrid lim_grid(int dim, const int* n) {
+static LimGrid lim_grid(int dim, const int* n, const int* bc) {
   LimGrid G;
   G.nx = n[0];
   G.ny = n[1];
   G.nz = dim == 3 ? n[2] : 1;
   G.dim = dim;
+  for (int d = 0; d < 3; d++) G.bc[d] = bc && d < dim ? bc[d] : 0;
   return G;
 }
 
-exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int admissibility, int steps_till_cured,
-                             const double* luh, int* ok, int* status, int* status_tmp, int* cure, int* list_patch,
-                             int* list_fv, int* counts, cudaStream_t st) {
-  const LimGrid G = lim_grid(dim, ncell);
+exa_status_t limiting_status(int dim, const int* ncell, const int* bc, int npc, int planar, int admissibility,
+                             int steps_till_cured, const double* luh, int* ok, int* status, int* status_tmp,
+                             int* cure, int* list_patch, int* list_fv, int* counts, cudaStream_t st) {
+  const LimGrid G = lim_grid(dim, ncell, bc);
   const long n = (long)G.nx * G.ny * G.nz;
   if (admissibility) k_lim_admissible<<<blocks(n * npc, 256), 256, 0, st>>>(npc, n, planar, luh, ok);
   k_lim_base_status<<<blocks(n, 256), 256, 0, st>>>(n, ok, status, cure, steps_till_cured);
@@ -158,9 +170,9 @@ exa_status_t limiting_status(int dim, const int* ncell, int npc, int planar, int
   return cuda_status(cudaGetLastError(), "limiter status kernels");
 }
 
-exa_status_t limiting_merge_bounds(int dim, const int* ncell, int nobs, double* bmin, double* bmax, double* loc,
-                                   cudaStream_t st) {
-  const LimGrid G = lim_grid(dim, ncell);
+exa_status_t limiting_merge_bounds(int dim, const int* ncell, const int* bc, int nobs, double* bmin, double* bmax,
+                                   double* loc, cudaStream_t st) {
+  const LimGrid G = lim_grid(dim, ncell, bc);
   const long n = (long)G.nx * G.ny * G.nz;
   k_lim_local<<<blocks(n * nobs, 256), 256, 0, st>>>(n, 2 * dim, nobs, bmin, bmax, loc);
   k_lim_merge<<<blocks(n * nobs, 256), 256, 0, st>>>(G, nobs, loc, bmin, bmax);

@@ -385,7 +385,7 @@ exa_status_t exa_limiter_dmp(int dim, int order, int nvar, int nobs, long ncells
 
 /* ---- Limiting ADER-DG on the uniform grid ----
  * exahype::solvers::LimitingADERDGSolver (exahype/solvers/
- * LimitingADERDGSolver.cpp) on a periodic exa_aderdg_grid (2D or 3D): each step the
+ * LimitingADERDGSolver.cpp) on an exa_aderdg_grid (2D or 3D): each step the
  * unlimited DG candidate is checked by the DMP (bounds: the cell's and its
  * face neighbours' extrema of the previous step) and, if enabled, by
  * physical admissibility (positive density and pressure at every node);
@@ -396,6 +396,13 @@ exa_status_t exa_limiter_dmp(int dim, int order, int nvar, int nobs, long ncells
  * cells' projected previous solutions, NeighbourOfTroubled3 included) and
  * project the result back (LimitingADERDGSolver::recomputeSolution,
  * :1378-1441); the next bounds and the next dt come from the final state.
+ * With exa_aderdg_grid_set_boundary's rules, a domain-boundary face adds no
+ * neighbour status (mergeWithBoundaryOrEmptyCellMetadata sets the facewise
+ * status 0) and keeps the cell's own extrema, and a subcell patch's ghost
+ * layers there mirror its boundary layers, ghost k <- interior g - 1 - k
+ * from the face, the normal momentum negated for EXA_BC_REFLECT
+ * (FiniteVolumesSolver::mergeWithBoundaryData, finitevolumes/commons/c/
+ * commons.cpph:175-340).
  * Parameters as in the reference's solver specification. */
 typedef struct {
   int scheme;                /* subcell FV scheme: 0 Godunov, 1 MUSCL-Hancock */
@@ -406,8 +413,8 @@ typedef struct {
   int check_admissibility;   /* 1: density and pressure > 0 at every node */
 } exa_limiter_config_t;
 
-/* Enables (cfg != NULL) or disables the limiter of a grid.  Needs periodic
- * boundaries and no slab halos (3D MUSCL-Hancock subcells: order <= 5);
+/* Enables (cfg != NULL) or disables the limiter of a grid.  Needs no slab
+ * halos (3D MUSCL-Hancock subcells: order <= 5);
  * allocates the limiter state (previous solution, one subcell patch per
  * cell, bounds, statuses) and sets every cell Ok with bounds from the
  * current state (also after init/set_state). */

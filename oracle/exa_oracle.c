@@ -1383,25 +1383,32 @@ int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, d
 }
 
 /* ------------------------------------------------------------------ */
-/* Limiting ADER-DG on a periodic 2D or 3D grid: LimitingADERDGSolver
+/* Limiting ADER-DG on a uniform 2D or 3D grid: LimitingADERDGSolver
  * (exahype/solvers/LimitingADERDGSolver.cpp) restated for a uniform mesh
  * with global time stepping, on top of the restated kernels above.  Cells
- * x fastest; n[2] is ignored in 2D. */
-static long lim_nb(int dim, const int* n, long c, int f) {
-  int x = (int)(c % n[0]), y = (int)((c / n[0]) % n[1]);
-  int z = dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0;
+ * x fastest; n[2] is ignored in 2D.  bc (nullable: all periodic) holds the
+ * boundary rule per dimension, 0 periodic, 1 outflow, 2 reflecting wall. */
+static long lim_nb(int dim, const int* n, const int* bc, long c, int f) {
+  int co[3];
   const int d = f >> 1, up = f & 1;
-  if (d == 0) x = up ? (x + 1 == n[0] ? 0 : x + 1) : (x == 0 ? n[0] - 1 : x - 1);
-  else if (d == 1) y = up ? (y + 1 == n[1] ? 0 : y + 1) : (y == 0 ? n[1] - 1 : y - 1);
-  else z = up ? (z + 1 == n[2] ? 0 : z + 1) : (z == 0 ? n[2] - 1 : z - 1);
-  return ((long)z * n[1] + y) * n[0] + x;
+  co[0] = (int)(c % n[0]);
+  co[1] = (int)((c / n[0]) % n[1]);
+  co[2] = dim == 3 ? (int)(c / ((long)n[0] * n[1])) : 0;
+  if (up ? co[d] == n[d] - 1 : co[d] == 0) {
+    if (bc && bc[d]) return -1; /* the domain boundary */
+    co[d] = up ? 0 : n[d] - 1;
+  } else {
+    co[d] += up ? 1 : -1;
+  }
+  return ((long)co[2] * n[1] + co[1]) * n[0] + co[0];
 }
 
 static long lim_ncells(int dim, const int* n) { return (long)n[0] * n[1] * (dim == 3 ? n[2] : 1); }
 
 /* mergeSolutionMinMaxOnFace (:1792-1853): face f keeps the extrema of the
- * cell (face block 0) and of its neighbour across f */
-static void lim_merge_bounds(int dim, const int* n, int nobs, double* bmin, double* bmax) {
+ * cell (face block 0) and of its neighbour across f; a domain-boundary face
+ * is never merged and keeps the cell's own */
+static void lim_merge_bounds(int dim, const int* n, const int* bc, int nobs, double* bmin, double* bmax) {
   const long nc = lim_ncells(dim, n);
   const int nf = 2 * dim;
   double* loc = (double*)malloc(sizeof(double) * nc * 2 * nobs);
@@ -1414,7 +1421,7 @@ static void lim_merge_bounds(int dim, const int* n, int nobs, double* bmin, doub
     }
   for (c = 0; c < nc; c++)
     for (f = 0; f < nf; f++) {
-      const long nb = lim_nb(dim, n, c, f);
+      const long nb0 = lim_nb(dim, n, bc, c, f), nb = nb0 < 0 ? c : nb0;
       for (v = 0; v < nobs; v++) {
         const double mo = loc[(c * 2) * nobs + v], mn = loc[(nb * 2) * nobs + v];
         const double xo = loc[(c * 2 + 1) * nobs + v], xn = loc[(nb * 2 + 1) * nobs + v];
@@ -1426,14 +1433,49 @@ static void lim_merge_bounds(int dim, const int* n, int nobs, double* bmin, doub
 }
 
 void orc_limiting_initial_bounds(int dim, int order, const int* n, const double* luh, int nobs, double* bmin,
-                                 double* bmax) {
+                                 double* bmax, const int* bc) {
   const long nc = lim_ncells(dim, n);
   const int B = order + 1, npc = dim == 3 ? B * B * B : B * B;
   long c;
   for (c = 0; c < nc; c++)
     orc_limiter_local_min_max(dim, order, 5, nobs, luh + c * npc * 5, bmin + c * 2 * dim * nobs,
                               bmax + c * 2 * dim * nobs);
-  lim_merge_bounds(dim, n, nobs, bmin, bmax);
+  lim_merge_bounds(dim, n, bc, nobs, bmin, bmax);
+}
+
+/* point (z, y, x) of a [S]^dim patch */
+static long lim_pt(int dim, int SG, int z, int y, int x) {
+  return dim == 3 ? ((long)z * SG + y) * SG + x : (long)y * SG + x;
+}
+
+void orc_fv_boundary_ghosts(int dim, int P, int g, double* luh, int face, int rule) {
+  const int SG = P + 2 * g, d = face >> 1, up = face & 1, amax = dim == 3 ? P : 1;
+  int a, b, k, m;
+  for (a = 0; a < amax; a++)
+    for (b = 0; b < P; b++)
+      for (k = 0; k < g; k++) {
+        /* ghost layer k and the interior layer it mirrors, along d; (a, b)
+         * run over the other axes */
+        const int gh = up ? g + P + k : k;
+        /* 3D lower y and z faces: the reference's boundaryLayerExtraction
+         * copies the first interior layer into every extracted layer
+         * (commons.cpph:561 and 591 index patchBegin without + k),
+         * so all those ghost layers repeat the layer next to the face */
+        const int src = up ? g + P - 1 - k : (dim == 3 && d > 0 ? g : 2 * g - 1 - k);
+        int dz, dy, dxx, sz, sy, sx;
+        if (d == 0) {
+          dz = sz = dim == 3 ? g + a : 0; dy = sy = g + b; dxx = gh; sx = src;
+        } else if (d == 1) {
+          dz = sz = dim == 3 ? g + a : 0; dxx = sx = g + b; dy = gh; sy = src;
+        } else {
+          dy = sy = g + a; dxx = sx = g + b; dz = gh; sz = src;
+        }
+        {
+          double* o = luh + lim_pt(dim, SG, dz, dy, dxx) * 5;
+          const double* q = luh + lim_pt(dim, SG, sz, sy, sx) * 5;
+          for (m = 0; m < 5; m++) o[m] = rule == 2 && m == d + 1 ? -q[m] : q[m];
+        }
+      }
 }
 
 /* positive density and pressure at every node */
@@ -1447,15 +1489,10 @@ static int lim_admissible(int npc, int planar, const double* q) {
   return 1;
 }
 
-/* point (z, y, x) of a [S]^dim patch */
-static long lim_pt(int dim, int SG, int z, int y, int x) {
-  return dim == 3 ? ((long)z * SG + y) * SG + x : (long)y * SG + x;
-}
-
 double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx, int planar, double* luh,
                               int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
                               double relaxation, double difference_scaling, int steps_till_cured, int admissibility,
-                              double dt, int dt_policy, double cfl, int* counts) {
+                              double dt, int dt_policy, double cfl, int* counts, const int* bc) {
   const int B = order + 1, npc = dim == 3 ? B * B * B : B * B, V = 5, S = 2 * order + 1;
   const int g = scheme == 0 ? 1 : 2, SG = S + 2 * g, nf = 2 * dim;
   const long nc = lim_ncells(dim, n), cell_d = (long)npc * V;
@@ -1469,7 +1506,7 @@ double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx
   int h, f, a, b, k, m;
   memcpy(prev, luh, sizeof(double) * nc * cell_d);
   /* 1. unlimited DG candidate */
-  orc_aderdg_grid_step(dim, order, planar, n, dx, luh, 2, cfl, dt, NULL, 0);
+  orc_aderdg_grid_step_bc(dim, order, planar, n, dx, luh, 2, cfl, dt, NULL, 0, bc);
   /* 2. DMP + admissibility -> status (determineLimiterStatusAfterSolutionUpdate) */
   for (c = 0; c < nc; c++) {
     int ok = orc_limiter_dmp(dim, order, V, nobs, luh + c * cell_d, relaxation, difference_scaling,
@@ -1490,12 +1527,15 @@ double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx
       tmp[c] = 0;
     }
   }
-  /* spreading: four face-neighbour hops, status = max(own, neighbour - 1) */
+  /* spreading: four face-neighbour hops, status = max(own, neighbour - 1);
+   * a domain-boundary face contributes status 0
+   * (ADERDGSolver::mergeWithBoundaryOrEmptyCellMetadata :2933-2947) */
   for (h = 0; h < 4; h++) {
     for (c = 0; c < nc; c++) {
       int s = tmp[c];
       for (f = 0; f < nf; f++) {
-        const int t = tmp[lim_nb(dim, n, c, f)] - 1;
+        const long o = lim_nb(dim, n, bc, c, f);
+        const int t = (o < 0 ? 0 : tmp[o]) - 1;
         if (t > s) s = t;
       }
       status[c] = s;
@@ -1512,13 +1552,19 @@ double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx
     if (status[c] == 5) cnt[2]++;
   }
   /* 4. face ghosts of the FV cells' patches from the neighbours' patches
-   * (FiniteVolumesSolver::mergeNeighbours / ghostLayerFilling) */
+   * (FiniteVolumesSolver::mergeNeighbours / ghostLayerFilling), at a domain
+   * boundary from the patch itself (orc_fv_boundary_ghosts) */
   for (c = 0; c < nc; c++) {
     if (status[c] < 3) continue;
     double* P = patch + c * patch_d;
     for (f = 0; f < nf; f++) {
       const int d = f >> 1, up = f & 1;
-      const double* N = patch + lim_nb(dim, n, c, f) * patch_d;
+      const long o = lim_nb(dim, n, bc, c, f);
+      const double* N = patch + o * patch_d;
+      if (o < 0) {
+        orc_fv_boundary_ghosts(dim, S, g, P, f, bc[d]);
+        continue;
+      }
       const int zmax = dim == 3 ? S : 1;
       for (a = 0; a < zmax; a++)
         for (b = 0; b < S; b++)
@@ -1555,7 +1601,7 @@ double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx
     orc_limiter_fv_min_max(dim, order, V, nobs, g, P, bmin + c * nf * nobs, bmax + c * nf * nobs);
   }
   /* 6. next bounds */
-  lim_merge_bounds(dim, n, nobs, bmin, bmax);
+  lim_merge_bounds(dim, n, bc, nobs, bmin, bmax);
   if (counts) memcpy(counts, cnt, sizeof(cnt));
   free(prev);
   free(patch);

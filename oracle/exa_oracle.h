@@ -174,7 +174,7 @@ void orc_limiter_fv_min_max(int dim, int order, int nvar, int nobs, int ghost,
 int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, double relaxation,
                     double difference_scaling, double* obs_min, double* obs_max);
 
-/* One step of the limiting ADER-DG grid (periodic 2D or 3D, n[0] x n[1]
+/* One step of the limiting ADER-DG grid (2D or 3D, n[0] x n[1]
  * (x n[2]) cells, order N, 5 variables), a restatement of
  * LimitingADERDGSolver's step on a uniform mesh: DG candidate with dt; DMP
  * against bmin/bmax ([cell][2 dim][nobs], updated in place to the next
@@ -184,15 +184,30 @@ int orc_limiter_dmp(int dim, int order, int nvar, int nobs, const double* luh, d
  * 1 MUSCL-Hancock) from the previous solution for status >= 3, ghost
  * subcells from the neighbours' projected previous solutions (status >= 2);
  * counts (nullable) = {cells with a patch, FV cells, Troubled cells}.
+ * bc (nullable: periodic) = boundary rule per dimension (0 periodic,
+ * 1 outflow, 2 reflecting wall) for the DG faces, the status spreading, the
+ * bounds merge and the subcell ghost layers.
  * Returns the next dt (orc_aderdg_grid_dt with dt_policy / cfl on the final
  * state). */
 double orc_limiting_grid_step(int dim, int order, const int* n, const double* dx, int planar, double* luh,
                               int* status, int* cure, double* bmin, double* bmax, int scheme, int nobs,
                               double relaxation, double difference_scaling, int steps_till_cured, int admissibility,
-                              double dt, int dt_policy, double cfl, int* counts);
+                              double dt, int dt_policy, double cfl, int* counts, const int* bc);
+/* Ghost layers of one FV patch ([S]^dim x 5 values, S = P + 2 g, (z) y x
+ * order) at a domain-boundary face 2 d + side: FiniteVolumesSolver::
+ * mergeWithBoundaryData (FiniteVolumesSolver.cpp:689-727) extracts the g
+ * layers next to the face (boundaryLayerExtraction), maps ghost k to the
+ * extracted layer K = g - 1 - k through boundaryValues (boundaryConditions,
+ * finitevolumes/commons/c/commons.cpph:175-265 and 726-875) and stores them
+ * (ghostLayerFillingAtBoundary), so the ghost k layers from the face mirror
+ * the interior k layers from the face (3D lower y and z faces: every ghost
+ * layer repeats the layer next to the face, as the reference's extraction
+ * there reads the first interior layer for every k).  rule 1 copies
+ * (outflow), rule 2 negates the normal momentum (reflecting wall). */
+void orc_fv_boundary_ghosts(int dim, int P, int g, double* luh, int face, int rule);
 /* bounds of the first DMP check: local extrema merged over faces */
 void orc_limiting_initial_bounds(int dim, int order, const int* n, const double* luh, int nobs, double* bmin,
-                                 double* bmax);
+                                 double* bmax, const int* bc);
 
 /* counter-based noise shared with the device IC kernel */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx);

@@ -101,6 +101,15 @@ struct Euler {
   void pointSource(const double* const, const double* const, const double, const double, double*, int) {}
   void boundaryValues(const double* const, const double, const double, const int, const int,
                       const double* const, const double* const, double*, double*) {}
+  /* FV boundary hook (FiniteVolumesSolver::boundaryValues): rule 1 copies
+   * the inside state (EulerFV's outflow), rule 2 also negates the normal
+   * momentum (slip wall) */
+  int rule = 1;
+  void boundaryValues(const double* const, const double, const double, const int, const int normalNonZero,
+                      const double* const stateIn, double* stateOut) {
+    for (int m = 0; m < 5; m++) stateOut[m] = stateIn[m];
+    if (rule == 2) stateOut[normalNonZero + 1] = -stateOut[normalNonZero + 1];
+  }
   double riemannSolver(double* fL, double* fR, const double* qL, const double* qR, int d) {
     return kernels::finitevolumes::riemannsolvers::c::rusanov<false, true>(*this, fL, fR, qL, qR, d);
   }
@@ -326,7 +335,43 @@ static double fv_step3_t(int scheme, double* luh, const double* dx, double dt_fi
 }
 #endif
 
+/* The reference's ghost filling of one FV patch at a domain-boundary face
+ * (FiniteVolumesSolver::mergeWithBoundaryData, FiniteVolumesSolver.cpp:
+ * 689-727): boundaryLayerExtraction, boundaryConditions and
+ * ghostLayerFillingAtBoundary of finitevolumes/commons/c/commons.cpph for
+ * face 2 d + side, with the boundary rule of Euler::boundaryValues. */
+template <int PS, int G>
+static void fv_boundary_t(double* luh, int face, int rule) {
+  typedef Euler<0, 0, PS, G> S;
+  namespace FC = kernels::finitevolumes::commons::c;
+  S s;
+  s.rule = rule;
+  const int d = face >> 1;
+  tarch::la::Vector<DIMENSIONS, int> pos(0);
+  pos[d] = (face & 1) ? 1 : -1;
+  long bnd = G * 5;
+  for (int i = 1; i < DIMENSIONS; i++) bnd *= PS;
+  std::vector<double> in(bnd), out(bnd);
+  FC::boundaryLayerExtraction<S>(s, in.data(), luh, pos);
+  FC::boundaryConditions<S>(s, out.data(), in.data(), Vec(0.5), Vec(1.0), 0.0, 0.0, face, d);
+  FC::ghostLayerFillingAtBoundary<S>(s, luh, out.data(), pos);
+}
+
 extern "C" {
+
+/* patch 3, 5, 7, 9 or 11 subcells (limiter patches of orders 1..5) with
+ * ghost 1 or 2; returns -1 for other sizes */
+int ref_fv_boundary(int patch, int ghost, double* luh, int face, int rule) {
+#define BCASE(P)                                                   \
+  case P:                                                          \
+    if (ghost == 1) fv_boundary_t<P, 1>(luh, face, rule);          \
+    else fv_boundary_t<P, 2>(luh, face, rule);                     \
+    return 0;
+  if (ghost != 1 && ghost != 2) return -1;
+  switch (patch) { BCASE(3) BCASE(5) BCASE(7) BCASE(9) BCASE(11) }
+#undef BCASE
+  return -1;
+}
 
 int ref_stp(int order, int npar, const double* luh, double* lQi, double* lQhi, double* lFhi,
             double* qb, double* fb, const double* dx, double dt) {

@@ -1,5 +1,5 @@
 """Initial states with discontinuities for the limiting ADER-DG tests: nodal
-values on the Gauss-Legendre nodes of a periodic 2D grid (cells x fastest,
+values on the Gauss-Legendre nodes of a 2D grid (cells x fastest,
 per cell [y][x][variable]), 5 Euler variables, gamma = 1.4."""
 import numpy as np
 
@@ -48,9 +48,9 @@ def smooth(order, n, length=(1.0, 1.0), amp=0.1):
     return q.reshape(-1)
 
 
-def explosion3d(order, n, radius=0.25, inner=(1.0, 1.0), outer=(0.125, 0.1)):
-    """Spherical explosion in the periodic unit cube (cells x fastest, per
-    cell [z][y][x][variable])."""
+def explosion3d(order, n, radius=0.25, inner=(1.0, 1.0), outer=(0.125, 0.1), center=(0.5, 0.5, 0.5)):
+    """Spherical explosion in the unit cube (cells x fastest, per cell
+    [z][y][x][variable])."""
     xi = nodes(order)
     nx, ny, nz = n
     B = order + 1
@@ -58,7 +58,7 @@ def explosion3d(order, n, radius=0.25, inner=(1.0, 1.0), outer=(0.125, 0.1)):
     Y = (np.arange(ny)[None, :, None, None, None, None] + xi[None, None, None, None, :, None]) / ny
     Z = (np.arange(nz)[:, None, None, None, None, None] + xi[None, None, None, :, None, None]) / nz
     X, Y, Z = np.broadcast_arrays(X, Y, Z)  # [cz][cy][cx][iz][iy][ix]
-    inside = (X - 0.5) ** 2 + (Y - 0.5) ** 2 + (Z - 0.5) ** 2 < radius ** 2
+    inside = (X - center[0]) ** 2 + (Y - center[1]) ** 2 + (Z - center[2]) ** 2 < radius ** 2
     q = np.zeros(X.shape + (5,))
     q[..., 0] = np.where(inside, inner[0], outer[0])
     q[..., 4] = np.where(inside, inner[1], outer[1]) / (GAMMA - 1)

@@ -85,8 +85,9 @@ def lib():
     L.orc_fv_periodic_ghosts_3d.argtypes = [i, i, i, _dp]
     L.orc_limiting_grid_step.restype = d
     L.orc_limiting_grid_step.argtypes = [i, i, _ip, _dp, i, _dp, _ip, _ip, _dp, _dp, i, i, d, d, i, i, d, i, d,
-                                         C.c_void_p]
-    L.orc_limiting_initial_bounds.argtypes = [i, i, _ip, _dp, i, _dp, _dp]
+                                         C.c_void_p, C.c_void_p]
+    L.orc_limiting_initial_bounds.argtypes = [i, i, _ip, _dp, i, _dp, _dp, C.c_void_p]
+    L.orc_fv_boundary_ghosts.argtypes = [i, i, i, _dp, i, i]
     _lib = L
     return L
 
@@ -209,14 +210,16 @@ def limiter_dmp(dim, order, luh, bmin, bmax, relax, scaling, nvar=5, nobs=5):
 
 
 class LimitingGrid:
-    """Oracle state of the limiting ADER-DG grid (periodic 2D or 3D): the
-    restated step of orc_limiting_grid_step with the same parameters as
-    ADERDGGrid.set_limiter."""
+    """Oracle state of the limiting ADER-DG grid (2D or 3D): the restated
+    step of orc_limiting_grid_step with the same parameters as
+    ADERDGGrid.set_limiter; bc = boundary rule per dimension (0 periodic,
+    1 outflow, 2 reflecting wall) as in ADERDGGrid.set_boundary."""
 
     def __init__(self, order, n, luh, length=None, scheme=0, nobs=5, relaxation=1e-4,
                  difference_scaling=1e-3, steps_till_cured=0, check_admissibility=True, dt_policy=0, cfl=0.9,
-                 planar=0):
+                 planar=0, bc=None):
         self.dim = len(n)
+        self.bc = np.asarray(list(bc or [0] * self.dim) + [0] * (3 - self.dim), dtype=np.int32)
         length = length or (1.0,) * self.dim
         self.order = order
         self.n = np.asarray(list(n) + [1] * (3 - self.dim), dtype=np.int32)
@@ -230,7 +233,8 @@ class LimitingGrid:
         self.bmax = np.zeros(nc * nf * nobs)
         self.p = (scheme, nobs, relaxation, difference_scaling, steps_till_cured, int(check_admissibility))
         self.dt_policy, self.cfl, self.planar = dt_policy, cfl, planar
-        lib().orc_limiting_initial_bounds(self.dim, order, self.n, self.luh, nobs, self.bmin, self.bmax)
+        lib().orc_limiting_initial_bounds(self.dim, order, self.n, self.luh, nobs, self.bmin, self.bmax,
+                                          self.bc.ctypes.data)
         self.dt = lib().orc_aderdg_grid_dt(self.dim, order, planar, self.n, self.dx, self.luh, dt_policy, cfl)
         self.counts = np.zeros(3, dtype=np.int32)
 
@@ -240,7 +244,8 @@ class LimitingGrid:
         s, nobs, rel, sc, cured, adm = self.p
         self.dt = lib().orc_limiting_grid_step(self.dim, self.order, self.n, self.dx, self.planar, self.luh,
                                                self.status, self.cure, self.bmin, self.bmax, s, nobs, rel, sc,
-                                               cured, adm, dt, self.dt_policy, self.cfl, self.counts.ctypes.data)
+                                               cured, adm, dt, self.dt_policy, self.cfl, self.counts.ctypes.data,
+                                               self.bc.ctypes.data)
         return dt
 
 
@@ -285,5 +290,8 @@ def ref_lib(dim):
         if hasattr(L, 'ref_fv_step'):
             L.ref_fv_step.restype = d
             L.ref_fv_step.argtypes = [i, i, _dp, _dp, d, C.c_void_p]
+        if hasattr(L, 'ref_fv_boundary'):
+            L.ref_fv_boundary.restype = i
+            L.ref_fv_boundary.argtypes = [i, i, _dp, i, i]
     _ref[dim] = L
     return L
