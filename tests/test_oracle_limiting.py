@@ -1,4 +1,4 @@
-"""The oracle's limiting ADER-DG step (orc_limiting_grid_step_2d, a
+"""The oracle's limiting ADER-DG step (orc_limiting_grid_step, a
 restatement of LimitingADERDGSolver on a uniform periodic grid) on its own:
 it leaves a smooth state to the unlimited DG scheme, and on an explosion it
 marks the cells along the discontinuity, spreads their status by face hops
