@@ -89,8 +89,14 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
 #pragma unroll
       for (int m = 0; m < V; m++) fa[d][m] = 0.0;
 
+    // The first iterate is luh in every time slice (the reference's trivial
+    // initial guess): iteration 0 evaluates slice 0 once and applies its
+    // flux and derivative for every slice n2 in order, the same operations
+    // on the same values as B separate evaluations.
 #pragma unroll
     for (int n = 0; n < B; n++) {
+      if (iter == 0 && n > 0) continue;
+      const int nend = iter == 0 ? B : n + 1;
       // alternate the two slice buffers: a thread writing slice n+1 has
       // passed the barrier of slice n, which every thread reaches only after
       // it finished reading slice n-1 (the buffer being overwritten)
@@ -105,12 +111,12 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
 #pragma unroll
           for (int m = 0; m < V; m++) F[d][m] = 0.0;
       }
-      if (!conv) {
+      if (!conv)
+        for (int n2 = n; n2 < nend; n2++)
 #pragma unroll
-        for (int d = 0; d < DIM; d++)
+          for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) fa[d][m] += T.w[n] * F[d][m];
-      }
+            for (int m = 0; m < V; m++) fa[d][m] += T.w[n2] * F[d][m];
       if (active) {
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
@@ -125,12 +131,14 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
         }
         if (FULL && !conv) {
           double* lFi = a.lFi + cell * (long)NPC * B * (DIM + 1) * V;
+          for (int n2 = n; n2 < nend; n2++) {
 #pragma unroll
-          for (int d = 0; d < DIM; d++)
+            for (int d = 0; d < DIM; d++)
 #pragma unroll
-            for (int m = 0; m < V; m++) lFi[((n * NPC + s) * (DIM + 1) + d) * V + m] = F[d][m];
+              for (int m = 0; m < V; m++) lFi[((n2 * NPC + s) * (DIM + 1) + d) * V + m] = F[d][m];
 #pragma unroll
-          for (int m = 0; m < V; m++) lFi[((n * NPC + s) * (DIM + 1) + DIM) * V + m] = 0.0;
+            for (int m = 0; m < V; m++) lFi[((n2 * NPC + s) * (DIM + 1) + DIM) * V + m] = 0.0;
+          }
         }
       }
       __syncthreads();
@@ -156,10 +164,11 @@ __device__ __forceinline__ void predictor_block(const PredArgs& a, long block, d
             Gm[4] += c * p4[p * stride[d]];
           }
         }
+        for (int n2 = n; n2 < nend; n2++)
 #pragma unroll
-        for (int t = 0; t < B; t++)
+          for (int t = 0; t < B; t++)
 #pragma unroll
-          for (int m = 0; m < V; m++) acc[t][m] += T.tA[t][n] * Gm[m];
+            for (int m = 0; m < V; m++) acc[t][m] += T.tA[t][n2] * Gm[m];
       }
     }
 

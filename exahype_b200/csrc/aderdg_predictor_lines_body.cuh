@@ -214,8 +214,13 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
 #pragma unroll
       for (int m = 0; m < V; m++) fa[d][m] = 0.f;
 
+    // the first iterate is the same in every time slice (deviation 0, the
+    // reference's trivial initial guess): iteration 0 evaluates slice 0 only
+    // and every later read of a slice's line sums takes slice 0, the values
+    // the B identical evaluations would give
 #pragma unroll
     for (int n = 0; n < B; n++) {
+      if (iter == 0 && n > 0) continue;
       // node threads: flux deviation of slice n into buffer buf (whose
       // previous contents, slice n-2, every thread read before the last
       // barrier)
@@ -234,6 +239,13 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
           for (int d = 0; d < DIM; d++)
 #pragma unroll
             for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dF[d][m], fa[d][m]);
+          if (iter == 0)  // slices 1..B-1 carry the same deviation
+#pragma unroll
+            for (int n2 = 1; n2 < B; n2++)
+#pragma unroll
+              for (int d = 0; d < DIM; d++)
+#pragma unroll
+                for (int m = 0; m < V; m++) fa[d][m] = fmaf(TF.w[n2], dF[d][m], fa[d][m]);
         }
       }
       __syncthreads();
@@ -289,12 +301,13 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
       for (int t = 0; t < B; t++) acc[t] = f5_zero();
 #pragma unroll
       for (int n = 0; n < B; n++) {
+        const int ns = iter == 0 ? 0 : n;
         float g[V];
 #pragma unroll
         for (int m = 0; m < V; m++) {
           g[m] = 0.f;
 #pragma unroll
-          for (int d = 0; d < DIM; d++) g[m] = fmaf(idxf[d], sX[S::x_addr(d, n, m, s)], g[m]);
+          for (int d = 0; d < DIM; d++) g[m] = fmaf(idxf[d], sX[S::x_addr(d, ns, m, s)], g[m]);
         }
         const F5 gn{make_float2(g[0], g[1]), make_float2(g[2], g[3]), g[4]};
 #pragma unroll

@@ -436,11 +436,26 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
         const float wn = TF.w[0];
 #pragma unroll
         for (int d = 0; d < DIM; d++) f5_fma(wn, dF[d], fa[d]);
+        // the first iterate is the same in every slice (deviation 0, the
+        // reference's trivial initial guess): iteration 0 evaluates slice 0
+        // only and applies it for every slice, in slice order
+        if (iter == 0)
+#pragma unroll
+          for (int n2 = 1; n2 < B; n2++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) f5_fma(TF.w[n2], dF[d], fa[d]);
       }
       __syncthreads();
     }
+    F5 Gm0 = f5_zero();
 #pragma unroll
     for (int n = 0; n < B; n++) {
+      if (iter == 0 && n > 0) {
+        if (active)
+#pragma unroll
+          for (int t = 0; t < B; t++) f5_fma(TF.tA[t][n], Gm0, acc[t]);
+        continue;
+      }
       // derivative of slice n (buffer buf), then the flux of slice n+1 into
       // the other buffer, whose slice n-1 every thread finished reading
       // before the previous barrier; one barrier per slice
@@ -457,7 +472,9 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
         }
 #pragma unroll
         for (int t = 0; t < B; t++) f5_fma(TF.tA[t][n], Gm, acc[t]);
+        Gm0 = Gm;
       }
+      if (iter == 0) continue;
       if (n + 1 < B) {
         F5 dFn[DIM];
         if (active) slice_flux(n + 1, dFn);
