@@ -129,11 +129,15 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
   __syncthreads();
   if (a.bc_any) {
     // outside states of domain-boundary faces, one thread per face node
+    // faces unrolled so that d indexes cc, a.bc and a.n at compile time
+    // (a runtime index would move them to local memory)
     if (valid)
-      for (int k = s; k < NFACE * NF; k += G) {
-        const int f = k / NF, j = k % NF, d = f >> 1;
+#pragma unroll
+      for (int f = 0; f < NFACE; f++) {
+        const int d = f >> 1;
         const bool up = f & 1;
         if (a.bc[d] == 0 || !(up ? cc[d] + 1 == a.n[d] : cc[d] == 0)) continue;
+        for (int j = s; j < NF; j += G) {
         const int o = (f * NF + j) * V;
         if (a.bc[d] == EXA_BC_OUTFLOW) {
 #pragma unroll
@@ -153,6 +157,7 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
             sQn[o + m] = qo_[m];
             sFn[o + m] = F[d][m];
           }
+        }
         }
       }
     __syncthreads();
