@@ -214,6 +214,9 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
   const int k0 = pb + blockIdx.x * FV_TX, j0 = pb + blockIdx.y * FV_TY;
   const int tid = threadIdx.x;
   const double hx = a.hx, hy = a.hy, dt = a.dt_dev ? *a.dt_dev : a.dt;
+  // reciprocal cell sizes: multiplications instead of the reference's
+  // divisions (an FP64 division is a long dependent chain)
+  const double ihx = 1.0 / hx, ihy = 1.0 / hy;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
     int j = j0 - 2 + r, k = k0 - 2 + c;
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
     if (has_x) {
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
         lx[m] = U[m] - 0.5 * hx * sl;
         rx[m] = U[m] + 0.5 * hx * sl;
       }
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
     if (has_y) {
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) / hy;
+        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
         ly[m] = U[m] - 0.5 * hy * sl;
         ry[m] = U[m] + 0.5 * hy * sl;
       }
@@ -263,16 +266,16 @@ __global__ void __launch_bounds__(FV_NT) k_fv_muscl(FVArgs a) {
       for (int m = 0; m < V; m++) Qt[m] = 0.0;
       euler_flux<2, PLANAR>(lx, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+      for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
       euler_flux<2, PLANAR>(rx, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
       euler_flux<2, PLANAR>(ly, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+      for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
       euler_flux<2, PLANAR>(ry, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
 #pragma unroll
       for (int m = 0; m < V; m++) {
         lx[m] += 0.5 * dt * Qt[m];
@@ -456,6 +459,9 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_muscl_periodic(FVArgs a) {
   const int k0 = pb + blockIdx.x * FVP_TX, j0 = pb + blockIdx.y * FVP_TY;
   const int tid = threadIdx.x;
   const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
+  // reciprocal cell sizes: multiplications instead of the reference's
+  // divisions (an FP64 division is a long dependent chain)
+  const double ihx = 1.0 / hx, ihy = 1.0 / hy;
   for (int i = tid; i < LY * LX; i += FVP_NT) {
     const int r = i / LX, c = i % LX;
     const int j = fv_wrap(j0 - 2 + r, pb, a.P), k = fv_wrap(k0 - 2 + c, pb, a.P);
@@ -478,7 +484,7 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_muscl_periodic(FVArgs a) {
     if (has_x) {
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
         lx[m] = U[m] - 0.5 * hx * sl;
         rx[m] = U[m] + 0.5 * hx * sl;
       }
@@ -486,7 +492,7 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_muscl_periodic(FVArgs a) {
     if (has_y) {
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) / hy;
+        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
         ly[m] = U[m] - 0.5 * hy * sl;
         ry[m] = U[m] + 0.5 * hy * sl;
       }
@@ -498,16 +504,16 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_muscl_periodic(FVArgs a) {
       for (int m = 0; m < V; m++) Qt[m] = 0.0;
       euler_flux<2, PLANAR>(lx, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+      for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
       euler_flux<2, PLANAR>(rx, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
       euler_flux<2, PLANAR>(ly, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+      for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
       euler_flux<2, PLANAR>(ry, F);
 #pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
 #pragma unroll
       for (int m = 0; m < V; m++) {
         lx[m] += 0.5 * dt * Qt[m];
@@ -1071,6 +1077,9 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
     double* out = a.out + patch * (long)S * S * D;
     const int tid = threadIdx.x;
     const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
+    // reciprocal cell sizes: multiplications instead of the reference's
+    // divisions (an FP64 division is a long dependent chain)
+    const double ihx = 1.0 / hx, ihy = 1.0 / hy;
     for (int i = tid; i < S * S * V; i += FVS_NT) su[i] = luh[i];  // D == V: no parameters here
     __syncthreads();
     if (SCHEME == 1) {
@@ -1086,7 +1095,7 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
         if (has_x) {
   #pragma unroll
           for (int m = 0; m < V; m++) {
-            const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) / hx;
+            const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
             lx[m] = U[m] - 0.5 * hx * sl;
             rx[m] = U[m] + 0.5 * hx * sl;
           }
@@ -1094,7 +1103,7 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
         if (has_y) {
   #pragma unroll
           for (int m = 0; m < V; m++) {
-            const double sl = minmod(U[S * V + m] - U[m], U[m] - U[-S * V + m]) / hy;
+            const double sl = minmod(U[S * V + m] - U[m], U[m] - U[-S * V + m]) * ihy;
             ly[m] = U[m] - 0.5 * hy * sl;
             ry[m] = U[m] + 0.5 * hy * sl;
           }
@@ -1106,16 +1115,16 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
           for (int m = 0; m < V; m++) Qt[m] = 0.0;
           euler_flux<2, PLANAR>(lx, F);
   #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] += F[0][m] / hx;
+          for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
           euler_flux<2, PLANAR>(rx, F);
   #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] -= F[0][m] / hx;
+          for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
           euler_flux<2, PLANAR>(ly, F);
   #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] += F[1][m] / hy;
+          for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
           euler_flux<2, PLANAR>(ry, F);
   #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] -= F[1][m] / hy;
+          for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
   #pragma unroll
           for (int m = 0; m < V; m++) {
             lx[m] += 0.5 * dt * Qt[m];

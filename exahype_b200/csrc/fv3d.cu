@@ -61,13 +61,14 @@ __device__ __forceinline__ double fv3_rusanov(const double* qL, const double* qR
 // wL) or +1 (upper, wR): u -/+ h/2 slope, plus the half step for interior
 // cells
 __device__ __forceinline__ void fv3_face_value(const double* su, const double* qt, int S, int P, int g, const double* h,
-                                               double dt, int i, int j, int k, int d, int side, double* w) {
+                                               const double* ih, double dt, int i, int j, int k, int d, int side,
+                                               double* w) {
   const int st = d == 0 ? 1 : (d == 1 ? S : S * S);
   const double* u = su + (((long)i * S + j) * S + k) * kV;
   const bool interior = i >= g && i < g + P && j >= g && j < g + P && k >= g && k < g + P;
 #pragma unroll
   for (int m = 0; m < kV; m++) {
-    const double sl = fv3_minmod(u[st * kV + m] - u[m], u[m] - u[-st * kV + m]) / h[d];
+    const double sl = fv3_minmod(u[st * kV + m] - u[m], u[m] - u[-st * kV + m]) * ih[d];
     double v = side < 0 ? u[m] - 0.5 * h[d] * sl : u[m] + 0.5 * h[d] * sl;
     if (interior) v += 0.5 * dt * qt[(((long)(i - g) * P + (j - g)) * P + (k - g)) * kV + m];
     w[m] = v;
@@ -87,6 +88,9 @@ __global__ void __launch_bounds__(FV3Threads<SCHEME>::value) k_fv3_patch(FV3Args
   const int tid = threadIdx.x;
   const double dt = a.dt_dev ? *a.dt_dev : a.dt;
   const double cfl = SCHEME == 0 ? 0.9 : 0.99;
+  // reciprocal cell sizes: multiplications instead of the reference's
+  // divisions in the slopes and half-step increments
+  const double ihs[3] = {1.0 / a.h[0], 1.0 / a.h[1], 1.0 / a.h[2]};
   const long npatch = a.count ? (long)*a.count : (long)gridDim.x;
   for (long e = blockIdx.x; e < npatch; e += gridDim.x) {
     const long patch = a.list ? (long)a.list[e] : e;
@@ -108,16 +112,16 @@ __global__ void __launch_bounds__(FV3Threads<SCHEME>::value) k_fv3_patch(FV3Args
           double wl[V], wr[V], F[3][V];
 #pragma unroll
           for (int m = 0; m < V; m++) {
-            const double sl = fv3_minmod(u[st * V + m] - u[m], u[m] - u[-st * V + m]) / a.h[d];
+            const double sl = fv3_minmod(u[st * V + m] - u[m], u[m] - u[-st * V + m]) * ihs[d];
             wl[m] = u[m] - 0.5 * a.h[d] * sl;
             wr[m] = u[m] + 0.5 * a.h[d] * sl;
           }
           euler_flux<3, false>(wl, F);
 #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] += F[d][m] / a.h[d];
+          for (int m = 0; m < V; m++) Qt[m] += F[d][m] * ihs[d];
           euler_flux<3, false>(wr, F);
 #pragma unroll
-          for (int m = 0; m < V; m++) Qt[m] -= F[d][m] / a.h[d];
+          for (int m = 0; m < V; m++) Qt[m] -= F[d][m] * ihs[d];
         }
 #pragma unroll
         for (int m = 0; m < V; m++) qt[(long)c * V + m] = Qt[m];
@@ -142,12 +146,12 @@ __global__ void __launch_bounds__(FV3Threads<SCHEME>::value) k_fv3_patch(FV3Args
           dtl = fmin(dtl, cfl / 3 * a.h[d] / s);
         } else {
           double wa[V], wb[V];
-          fv3_face_value(su, qt, S, P, g, a.h, dt, i - di, j - dj, k - dk, d, +1, wa);
-          fv3_face_value(su, qt, S, P, g, a.h, dt, i, j, k, d, -1, wb);
+          fv3_face_value(su, qt, S, P, g, a.h, ihs, dt, i - di, j - dj, k - dk, d, +1, wa);
+          fv3_face_value(su, qt, S, P, g, a.h, ihs, dt, i, j, k, d, -1, wb);
           s = fv3_rusanov(wa, wb, d, fl[d]);
           dtl = fmin(dtl, cfl / 3 * a.h[d] / s);
-          fv3_face_value(su, qt, S, P, g, a.h, dt, i, j, k, d, +1, wa);
-          fv3_face_value(su, qt, S, P, g, a.h, dt, i + di, j + dj, k + dk, d, -1, wb);
+          fv3_face_value(su, qt, S, P, g, a.h, ihs, dt, i, j, k, d, +1, wa);
+          fv3_face_value(su, qt, S, P, g, a.h, ihs, dt, i + di, j + dj, k + dk, d, -1, wb);
           s = fv3_rusanov(wa, wb, d, fr[d]);
           dtl = fmin(dtl, cfl / 3 * a.h[d] / s);
         }
