@@ -72,13 +72,41 @@ __device__ __forceinline__ double rusanov(const double* qL, const double* qR, in
 }
 
 // ------------------------------------------------------------- Godunov
+// The Rusanov flux of a face needs F_d and the largest |eigenvalue| of the
+// two cells beside it; both are evaluated once per cell and direction (the
+// reference's face loop evaluates them once per face side, i.e. twice per
+// cell and direction) and combined per face with the reference's formula,
+// so every face flux is the same value.
+template <bool PLANAR>
+__device__ __forceinline__ void fv_cell_flux(const double* q, int d, double* out) {
+  double F[2][kV];
+  euler_flux<2, PLANAR>(q, F);
+#pragma unroll
+  for (int m = 0; m < kV; m++) out[m] = F[d][m];
+  out[kV] = euler_max_eig<PLANAR>(q, d);
+}
+
+// rusanov() from per-cell fluxes: cl/cr = [F_d(q), lambda] of the left and
+// right cell
+__device__ __forceinline__ double fv_face_flux(const double* qL, const double* qR, const double* cl,
+                                               const double* cr, double* f) {
+  const double smax = fmax(cl[kV], cr[kV]);
+#pragma unroll
+  for (int i = 0; i < kV; i++) {
+    double v = 0.5 * smax * (qL[i] - qR[i]);
+    v += 0.5 * (cl[i] + cr[i]);
+    f[i] = v;
+  }
+  return smax;
+}
+
 template <bool PLANAR, bool FUSED>
 __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
-  constexpr int V = kV;
+  constexpr int V = kV, C = kV + 1;
   constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
   __shared__ double su[LY * LX * V];
-  __shared__ double sfx[FV_TY * (FV_TX + 1) * V];
-  __shared__ double sfy[(FV_TY + 1) * FV_TX * V];
+  __shared__ double scx[FV_TY * LX * C];  // x: staged rows 1..TY, all columns
+  __shared__ double scy[LY * FV_TX * C];  // y: all rows, staged columns 1..TX
   __shared__ double sred[FV_NT / 32];
   const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
   const long patch = blockIdx.z;
@@ -98,45 +126,49 @@ __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
       for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
   }
   __syncthreads();
-  double dtl = DBL_MAX;
-  // x faces: between (j, k-1) and (j, k), k in [k0, k0+TX], valid for k in [pb, pe]
-  for (int i = tid; i < FV_TY * (FV_TX + 1); i += FV_NT) {
-    const int r = i / (FV_TX + 1), c = i % (FV_TX + 1);
-    const int j = j0 + r, k = k0 + c;
-    if (j < pe && k <= pe) {
-      const double s = rusanov<PLANAR>(&su[((r + 1) * LX + c) * V], &su[((r + 1) * LX + c + 1) * V], 0,
-                                       &sfx[i * V]);
-      dtl = fmin(dtl, 0.9 / 2 * a.hx / s);
-    }
-  }
-  // y faces: between (j-1, k) and (j, k), j in [j0, j0+TY], valid for j in [pb, pe]
-  for (int i = tid; i < (FV_TY + 1) * FV_TX; i += FV_NT) {
-    const int r = i / FV_TX, c = i % FV_TX;
-    const int j = j0 + r, k = k0 + c;
-    if (j <= pe && k < pe) {
-      const double s = rusanov<PLANAR>(&su[(r * LX + c + 1) * V], &su[((r + 1) * LX + c + 1) * V], 1,
-                                       &sfy[i * V]);
-      dtl = fmin(dtl, 0.9 / 2 * a.hy / s);
+  // per-cell x fluxes of the cells beside the tile's x faces (rows j < pe,
+  // columns pb-1..pe) and y fluxes of the cells beside its y faces
+  for (int i = tid; i < FV_TY * LX + LY * FV_TX; i += FV_NT) {
+    if (i < FV_TY * LX) {
+      const int r = i / LX, c = i % LX;
+      const int j = j0 + r, k = k0 - 1 + c;
+      if (FUSED || (j < pe && k <= pe)) fv_cell_flux<PLANAR>(&su[((r + 1) * LX + c) * V], 0, &scx[i * C]);
+    } else {
+      const int i2 = i - FV_TY * LX;
+      const int r = i2 / FV_TX, c = i2 % FV_TX;
+      const int j = j0 - 1 + r, k = k0 + c;
+      if (FUSED || (j <= pe && k < pe)) fv_cell_flux<PLANAR>(&su[(r * LX + c + 1) * V], 1, &scy[i2 * C]);
     }
   }
   __syncthreads();
   const double dtv = a.dt_dev ? *a.dt_dev : a.dt;
   const double cx = dtv / a.hx, cy = dtv / a.hy;
-  double dtn = DBL_MAX;
+  double dtl = DBL_MAX, dtn = DBL_MAX;
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
-    if (j < pe && k < pe) {
+    const bool valid = j < pe && k < pe;
+    double fxl[V], fxr[V], fyb[V], fyt[V];
+    if (valid) {
+      const double* q = &su[((r + 1) * LX + c + 1) * V];
+      const double sxl = fv_face_flux(q - V, q, &scx[(r * LX + c) * C], &scx[(r * LX + c + 1) * C], fxl);
+      const double sxr = fv_face_flux(q, q + V, &scx[(r * LX + c + 1) * C], &scx[(r * LX + c + 2) * C], fxr);
+      const double syb = fv_face_flux(q - LX * V, q, &scy[(r * FV_TX + c) * C], &scy[((r + 1) * FV_TX + c) * C], fyb);
+      const double syt = fv_face_flux(q, q + LX * V, &scy[((r + 1) * FV_TX + c) * C], &scy[((r + 2) * FV_TX + c) * C], fyt);
+      if (!FUSED && a.max_dt) {
+        // min over faces of 0.45 h / s = 0.45 h / (max over faces of s):
+        // the division is monotone, so the same value as per face
+        dtl = fmin(0.9 / 2 * a.hx / fmax(sxl, sxr), 0.9 / 2 * a.hy / fmax(syb, syt));
+      }
       double* o = out + ((long)j * S + k) * D;
-      const double* uc = &su[((r + 1) * LX + c + 1) * V];
       double un[V];
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        double u = FUSED ? uc[m] : o[m];
-        u += cx * sfx[(r * (FV_TX + 1) + c) * V + m];
-        u -= cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
-        u += cy * sfy[(r * FV_TX + c) * V + m];
-        u -= cy * sfy[((r + 1) * FV_TX + c) * V + m];
+        double u = FUSED ? q[m] : o[m];
+        u += cx * fxl[m];
+        u -= cx * fxr[m];
+        u += cy * fyb[m];
+        u -= cy * fyt[m];
         o[m] = u;
         un[m] = u;
       }
@@ -151,25 +183,25 @@ __global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
       return;
     }
     // first ghost layer, as the reference's face loops touch it
-    if (j < pe && k0 == pb && c == 0) {
+    if (valid && k0 == pb && c == 0) {
       double* o = out + ((long)j * S + (pb - 1)) * D;
 #pragma unroll
-      for (int m = 0; m < V; m++) o[m] -= cx * sfx[(r * (FV_TX + 1)) * V + m];
+      for (int m = 0; m < V; m++) o[m] -= cx * fxl[m];
     }
-    if (j < pe && k == pe - 1) {
+    if (valid && k == pe - 1) {
       double* o = out + ((long)j * S + pe) * D;
 #pragma unroll
-      for (int m = 0; m < V; m++) o[m] += cx * sfx[(r * (FV_TX + 1) + c + 1) * V + m];
+      for (int m = 0; m < V; m++) o[m] += cx * fxr[m];
     }
-    if (k < pe && j0 == pb && r == 0) {
+    if (valid && j0 == pb && r == 0) {
       double* o = out + ((long)(pb - 1) * S + k) * D;
 #pragma unroll
-      for (int m = 0; m < V; m++) o[m] -= cy * sfy[c * V + m];
+      for (int m = 0; m < V; m++) o[m] -= cy * fyb[m];
     }
-    if (k < pe && j == pe - 1) {
+    if (valid && j == pe - 1) {
       double* o = out + ((long)pe * S + k) * D;
 #pragma unroll
-      for (int m = 0; m < V; m++) o[m] += cy * sfy[((r + 1) * FV_TX + c) * V + m];
+      for (int m = 0; m < V; m++) o[m] += cy * fyt[m];
     }
   }
   if (a.max_dt) {
@@ -1063,11 +1095,19 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
   extern __shared__ double sm[];
   const int P = a.P, g = a.g, S = a.S, D = V + a.npar, pb = g, pe = g + P;
   const int R = P + 2;  // ring side (MUSCL)
+  constexpr int C = kV + 1;
   double* su = sm;       // [S][S][V]
   double* wLx = su + S * S * V;
   double* wRx = wLx + R * R * V;
   double* wLy = wRx + R * R * V;
   double* wRy = wLy + R * R * V;
+  // Godunov: per-cell [F_d, lambda_d] (x: rows pb..pe-1, columns pb-1..pe;
+  // y: rows pb-1..pe, columns pb..pe-1); MUSCL-Hancock: one Rusanov flux
+  // per face (x: [P][P+1], y: [P+1][P])
+  double* scx = su + S * S * V;
+  double* scy = scx + P * R * C;
+  double* sfx = wRy + R * R * V;
+  double* sfy = sfx + P * (P + 1) * V;
   // one patch per iteration: patch blockIdx.x, or with a selection the
   // entries blockIdx.x, blockIdx.x + gridDim.x, ... of the list
   const long npatch = a.count ? (long)*a.count : (long)gridDim.x;
@@ -1142,24 +1182,56 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
         }
       }
       __syncthreads();
+      // each face's Rusanov flux once (the reference solves every face once)
+      for (int i = tid; i < 2 * P * (P + 1); i += FVS_NT) {
+        if (i < P * (P + 1)) {
+          const int r = i / (P + 1), c = i % (P + 1);  // face left of column pb + c, row pb + r
+          const int ic = (r + 1) * R + c + 1;
+          rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, &sfx[i * V]);
+        } else {
+          const int i2 = i - P * (P + 1);
+          const int r = i2 / P, c = i2 % P;  // face below row pb + r, column pb + c
+          const int ic = (r + 1) * R + c + 1;
+          rusanov<PLANAR>(&wRy[(ic - R) * V], &wLy[ic * V], 1, &sfy[i2 * V]);
+        }
+      }
+      __syncthreads();
+    } else {
+      // per-cell flux and eigenvalue bound, once per cell and direction
+      for (int i = tid; i < 2 * P * R; i += FVS_NT) {
+        if (i < P * R) {
+          const int j = pb + i / R, k = pb - 1 + i % R;
+          fv_cell_flux<PLANAR>(&su[(j * S + k) * V], 0, &scx[i * C]);
+        } else {
+          const int i2 = i - P * R;
+          const int j = pb - 1 + i2 / P, k = pb + i2 % P;
+          fv_cell_flux<PLANAR>(&su[(j * S + k) * V], 1, &scy[i2 * C]);
+        }
+      }
+      __syncthreads();
     }
     const double cx = dt / hx, cy = dt / hy;
     double dtn = DBL_MAX;
     for (int i = tid; i < P * P; i += FVS_NT) {
       const int j = pb + i / P, k = pb + i % P;
+      const int r = i / P, c = i % P;
       const double* U = &su[(j * S + k) * V];
       double fxl[V], fxr[V], fyb[V], fyt[V];
       if (SCHEME == 0) {
-        rusanov<PLANAR>(U - V, U, 0, fxl);
-        rusanov<PLANAR>(U, U + V, 0, fxr);
-        rusanov<PLANAR>(U - S * V, U, 1, fyb);
-        rusanov<PLANAR>(U, U + S * V, 1, fyt);
+        const double* xl = &scx[(r * R + c) * C];  // cells k-1, k, k+1 of row j
+        fv_face_flux(U - V, U, xl, xl + C, fxl);
+        fv_face_flux(U, U + V, xl + C, xl + 2 * C, fxr);
+        const double* yb = &scy[(r * P + c) * C];  // cells j-1, j, j+1 of column k
+        fv_face_flux(U - S * V, U, yb, yb + P * C, fyb);
+        fv_face_flux(U, U + S * V, yb + P * C, yb + 2 * P * C, fyt);
       } else {
-        const int ic = (j - pb + 1) * R + (k - pb + 1);
-        rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
-        rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
-        rusanov<PLANAR>(&wRy[(ic - R) * V], &wLy[ic * V], 1, fyb);
-        rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + R) * V], 1, fyt);
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          fxl[m] = sfx[(r * (P + 1) + c) * V + m];
+          fxr[m] = sfx[(r * (P + 1) + c + 1) * V + m];
+          fyb[m] = sfy[(r * P + c) * V + m];
+          fyt[m] = sfy[((r + 1) * P + c) * V + m];
+        }
       }
       fv_update_store_dt<PLANAR>(a, out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
     }
@@ -1171,7 +1243,8 @@ __global__ void __launch_bounds__(FVS_NT) k_fv_patch_small(FVArgs a) {
 
 inline size_t fv_small_smem(int P, int g, int scheme) {
   const size_t S = P + 2 * g, R = P + 2;
-  return sizeof(double) * (S * S * kV + (scheme == 1 ? 4 * R * R * kV : 0));
+  return sizeof(double) * (S * S * kV + (scheme == 1 ? 4 * R * R * kV + 2 * P * (P + 1) * kV
+                                                     : 2 * P * R * (kV + 1)));
 }
 
 // Subcell patches of the limiting ADER-DG grid: patch `cell` of a periodic
