@@ -380,7 +380,9 @@ __device__ __forceinline__ void predictor_mixed_block(const PredArgs& a, long bl
   }
   auto slice_flux = [&](int n, F5* dF) {
     const float dv[V] = {dq[n].a.x, dq[n].a.y, dq[n].b.x, dq[n].b.y, dq[n].c};
-    const float r1 = __frcp_rn(r0f + dv[0]);
+    // fast reciprocal (about 2 ulp): every use multiplies a deviation term,
+    // whose own FP32 rounding is of the same size
+    const float r1 = __fdividef(1.0f, r0f + dv[0]);
     float m1[3], w[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
