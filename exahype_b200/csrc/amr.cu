@@ -25,10 +25,13 @@ static __constant__ double c_fgp[kMaxOrder + 1][3][10][10];
 
 constexpr int kAmrNT = 128;
 
-template <int K, int B>
-__device__ __forceinline__ void amr_pass(double* out, const double* in, int nvar, int d, int sub, int order,
-                                         bool restrict_op, const double* w) {
-  // one direction: out[..m_d..][v] = sum_p op[p -> m_d] in[..p..][v]
+// one direction d: out[..m_d..][v] = sum_p op[m_d][p] in[..p..][v], op the
+// B x B operator of this level and direction staged in shared memory (a
+// per-thread constant-memory lookup with a thread-dependent index would be
+// serialised); NV > 0 fixes the variable count at compile time
+template <int K, int B, int NV>
+__device__ __forceinline__ void amr_pass(double* out, const double* in, int nvar_rt, int d, const double* op) {
+  const int nvar = NV > 0 ? NV : nvar_rt;
   int stride = nvar;
   for (int e = 0; e < d; e++) stride *= B;
   int total = nvar;
@@ -36,22 +39,21 @@ __device__ __forceinline__ void amr_pass(double* out, const double* in, int nvar
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const int md = (i / stride) % B;
     const int base = i - md * stride;
+    const double* row = op + md * B;
     double acc = 0.0;
 #pragma unroll
-    for (int p = 0; p < B; p++) {
-      const double c = restrict_op ? w[p] * c_fgp[order][sub][md][p] / (3.0 * w[md])
-                                   : c_fgp[order][sub][p][md];
-      acc += c * in[base + p * stride];
-    }
+    for (int p = 0; p < B; p++) acc += row[p] * in[base + p * stride];
     out[i] = acc;
   }
 }
 
-template <int K, int B>
-__global__ void __launch_bounds__(kAmrNT) k_amr(int order, int nvar, int restrict_op, double* dst,
+template <int K, int B, int NV>
+__global__ void __launch_bounds__(kAmrNT, 12) k_amr(int order, int nvar_rt, int restrict_op, double* dst,
                                                 const double* src, const long* src_item, int level_delta,
                                                 const int* index) {
   extern __shared__ double sm[];
+  __shared__ double sop[3][B * B];  // this level's operator per direction, [m][p]
+  const int nvar = NV > 0 ? NV : nvar_rt;
   int total = nvar;
   for (int e = 0; e < K; e++) total *= B;
   double* a = sm;
@@ -63,7 +65,6 @@ __global__ void __launch_bounds__(kAmrNT) k_amr(int order, int nvar, int restric
   int cur[3] = {0, 0, 0};
   for (int d = 0; d < K; d++) cur[d] = index[item * 3 + d];
   const double* w = c_dg[order].w;
-  __syncthreads();
   for (int l = 1; l <= level_delta; l++) {
     int sub[3];
     if (restrict_op) {
@@ -79,8 +80,16 @@ __global__ void __launch_bounds__(kAmrNT) k_amr(int order, int nvar, int restric
         cur[d] %= sig;
       }
     }
+    __syncthreads();  // the previous level's passes are done with sop
+    for (int t = threadIdx.x; t < K * B * B; t += blockDim.x) {
+      const int d = t / (B * B), md = (t / B) % B, p = t % B;
+      sop[d][md * B + p] = restrict_op ? w[p] * c_fgp[order][sub[d]][md][p] / (3.0 * w[md])
+                                       : c_fgp[order][sub[d]][p][md];
+    }
+    __syncthreads();
+#pragma unroll
     for (int d = 0; d < K; d++) {
-      amr_pass<K, B>(b, a, nvar, d, sub[d], order, restrict_op, w);
+      amr_pass<K, B, NV>(b, a, nvar, d, sop[d]);
       __syncthreads();
       double* t = a;
       a = b;
@@ -99,8 +108,12 @@ static exa_status_t launch_amr_k(int order, int nvar, int restrict_op, long coun
   const size_t smem = 2 * total * sizeof(double);
 #define EXA_AMR(BB)                                                                              \
   case BB - 1: {                                                                                 \
-    k_amr<K, BB><<<(unsigned)count, kAmrNT, smem, st>>>(order, nvar, restrict_op, dst, src,      \
-                                                        src_item, level_delta, index);           \
+    if (nvar == kV)                                                                              \
+      k_amr<K, BB, kV><<<(unsigned)count, kAmrNT, smem, st>>>(order, nvar, restrict_op, dst, src, \
+                                                              src_item, level_delta, index);     \
+    else                                                                                         \
+      k_amr<K, BB, 0><<<(unsigned)count, kAmrNT, smem, st>>>(order, nvar, restrict_op, dst, src,  \
+                                                             src_item, level_delta, index);      \
     break;                                                                                       \
   }
   switch (order) {
