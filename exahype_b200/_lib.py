@@ -28,6 +28,12 @@ PREC_MIXED = 1
 BC_PERIODIC = 0
 BC_OUTFLOW = 1
 BC_REFLECT = 2
+ADJUST_NONE = 0
+ADJUST_SINE_WAVE = 1
+ADJUST_ISENTROPIC_VORTEX = 2
+ADJUST_HEAT_SOURCE = 3
+ADJUST_AT_START = 0
+ADJUST_ALWAYS = 1
 
 
 class ExaError(RuntimeError):
@@ -52,6 +58,11 @@ class LimiterConfig(C.Structure):
     _fields_ = [('scheme', C.c_int), ('nobs', C.c_int), ('relaxation', C.c_double),
                 ('difference_scaling', C.c_double), ('steps_till_cured', C.c_int),
                 ('check_admissibility', C.c_int)]
+
+
+class AdjustHook(C.Structure):
+    """exa_adjust_t: a built-in adjustPointSolution form"""
+    _fields_ = [('kind', C.c_int), ('when', C.c_int), ('param', C.c_double * 6)]
 
 
 class FVDesc(C.Structure):
@@ -169,6 +180,9 @@ SIGNATURES = {
     'exa_aderdg_grid_limiter_bounds': (i32, [vp, vp, vp]),
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
+    'exa_aderdg_grid_set_adjustment': (i32, [vp, vp]),
+    'exa_aderdg_solution_adjustment': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, f64, f64, vp, vp]),
+    'exa_aderdg_solutionAdjustment': (i32, [i32, i32, dptr, dptr, dptr, f64, f64, vp]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
                                            C.POINTER(sz)]),
     'exa_aderdg_grid_dt_slot': (i32, [vp, C.POINTER(vp)]),

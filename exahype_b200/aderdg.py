@@ -121,9 +121,39 @@ class BatchedADERDG:
         call('exa_aderdg_riemann_faces', C.byref(self.desc), nfaces, left.ptr, right.ptr,
              direction.ptr, qb.ptr, fb.ptr, stream)
 
+    def solution_adjustment(self, ncells, luh, centers, t, dt, hook, stream=None):
+        """solutionAdjustment on ncells cells: centers = DeviceBuffer
+        [ncells][dim], hook = adjust_hook(...)"""
+        call('exa_aderdg_solution_adjustment', C.byref(self.desc), ncells, luh.ptr, centers.ptr, float(t),
+             float(dt), C.byref(hook), stream)
+
     def stable_dt(self, ncells, luh, dt_cell=None, dt_min=None, stream=None):
         call('exa_aderdg_stable_dt', C.byref(self.desc), ncells, luh.ptr,
              dt_cell.ptr if dt_cell else None, dt_min.ptr if dt_min else None, stream)
+
+
+def adjust_hook(kind, param=(), when=_lib.ADJUST_ALWAYS):
+    """exa_adjust_t: kind _lib.ADJUST_SINE_WAVE (param a), ADJUST_ISENTROPIC_VORTEX
+    (param eps) or ADJUST_HEAT_SOURCE (param A, width, frequency, centre x, y, z);
+    when ADJUST_AT_START (only at t == 0) or ADJUST_ALWAYS."""
+    h = _lib.AdjustHook()
+    h.kind, h.when = int(kind), int(when)
+    for i, v in enumerate(list(param)[:6]):
+        h.param[i] = float(v)
+    return h
+
+
+def solutionAdjustment(dim, order, luh, center, dx, t, dt, hook):
+    """kernels::aderdg::generic::c::solutionAdjustment for one cell (host
+    arrays; luh adjusted in place)."""
+    arr = np.ascontiguousarray(luh, dtype=np.float64)
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    d = np.ascontiguousarray(dx, dtype=np.float64)
+    call('exa_aderdg_solutionAdjustment', int(dim), int(order), _p(arr), _p(c), _p(d), float(t), float(dt),
+         C.byref(hook))
+    if arr is not luh:
+        luh[...] = arr.reshape(np.shape(luh))
+    return luh
 
 
 def grid_config(dim, order, n, length=None, pde=_lib.PDE_EULER, precision=_lib.PREC_FP64,
@@ -207,6 +237,11 @@ class ADERDGGrid:
         BC_REFLECT (see exa_aderdg_grid_set_boundary)."""
         arr = (C.c_int * 3)(*(list(bc) + [0] * (3 - len(bc))))
         call('exa_aderdg_grid_set_boundary', self.h, arr)
+
+    def set_adjustment(self, hook=None):
+        """Solution adjustment after every step's update (hook = adjust_hook(...),
+        None to turn it off; see exa_aderdg_grid_set_adjustment)."""
+        call('exa_aderdg_grid_set_adjustment', self.h, C.byref(hook) if hook is not None else None)
 
     # -- a-posteriori subcell limiter (exa_aderdg_grid_set_limiter) --
     def set_limiter(self, scheme=0, nobs=5, relaxation=1e-4, difference_scaling=1e-3, steps_till_cured=0,

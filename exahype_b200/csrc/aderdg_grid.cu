@@ -97,6 +97,9 @@ struct exa_aderdg_grid {
   double ms_pred = 0, ms_corr = 0;
   unsigned long long prof_steps = 0;
   uint64_t graph_launches = 3;  // kernels in one captured step
+  // solution adjustment after every update (exa_aderdg_grid_set_adjustment)
+  bool adj_on = false;
+  exa_adjust_t adj{};
   // a-posteriori subcell limiter (exa_aderdg_grid_set_limiter)
   bool lim_on = false;
   exa_limiter_config_t lim_cfg{};
@@ -197,7 +200,7 @@ static exa_status_t grid_correct(exa_aderdg_grid* g) {
   c.lFhbnd = g->fb;
   // with the limiter the candidate may be unusable in troubled cells: the
   // next dt and the NaN check come after the limiting
-  c.dt_next = (g->cfg.dt_policy == 2 || g->lim_on) ? nullptr : &g->gd->dt_next;
+  c.dt_next = (g->cfg.dt_policy == 2 || g->lim_on || g->adj_on) ? nullptr : &g->gd->dt_next;
   c.dt_factor = g->dt_factor;
   c.nan_flag = g->lim_on ? nullptr : &g->gd->nan_flag;
   if (g->halo) {
@@ -300,6 +303,16 @@ static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
   if (exa_status_t s = grid_correct(g)) return s;
   if (g->lim_on)
     if (exa_status_t s = grid_limit(g)) return s;
+  if (g->adj_on) {
+    // ADERDGSolver::updateSolution (:2158-2170): the hook after the update
+    // at t + dt; the next dt from the adjusted state
+    if (exa_status_t s = grid_adjust(g->cfg.dim, g->cfg.order, g->cfg.n, g->desc.dx, g->ncells, g->luh,
+                                     &g->gd->time, &g->gd->dt, g->adj, g->st))
+      return s;
+    if (g->cfg.dt_policy != 2)
+      if (exa_status_t s = launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr, &g->gd->dt_next, g->st))
+        return s;
+  }
   if (exa_status_t s = grid_commit(g)) return s;
   if (g->profile) {
     cudaEventRecord(g->ev[2], g->st);
@@ -561,6 +574,22 @@ exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc) {
   return EXA_OK;
 }
 
+exa_status_t exa_aderdg_grid_set_adjustment(exa_aderdg_grid* g, const exa_adjust_t* hook) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (hook)
+    if (exa_status_t s = check_adjust_hook(hook)) return s;
+  const bool on = hook && hook->kind != EXA_ADJUST_NONE && hook->when == EXA_ADJUST_ALWAYS;
+  if (on && g->lim_on) return set_error(EXA_EINVAL, "adjustment: not with the limiter");
+  if (on && g->halo) return set_error(EXA_EINVAL, "adjustment: not with slab halos");
+  if (g->graph) {  // the captured step changes
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  g->adj_on = on;
+  g->adj = on ? *hook : exa_adjust_t{};
+  return EXA_OK;
+}
+
 exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_config_t* cfg) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
   if (g->graph) {  // the captured step changes
@@ -575,6 +604,7 @@ exa_status_t exa_aderdg_grid_set_limiter(exa_aderdg_grid* g, const exa_limiter_c
     return EXA_OK;
   }
   if (g->halo) return set_error(EXA_EINVAL, "limiter: not with slab halos");
+  if (g->adj_on) return set_error(EXA_EINVAL, "limiter: not with a solution adjustment");
   if (g->cfg.dim == 3) {
     // one CTA stages a subcell patch with its ghosts (fv3d.cu)
     const int S = 2 * g->cfg.order + 1, gw = cfg->scheme == 0 ? 1 : 2;
@@ -652,6 +682,7 @@ exa_status_t exa_aderdg_grid_set_halo(exa_aderdg_grid* g, int enable) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
   if (enable && g->bc[g->cfg.dim - 1] != EXA_BC_PERIODIC)
     return set_error(EXA_EINVAL, "slab halos need a periodic last dimension");
+  if (enable && g->adj_on) return set_error(EXA_EINVAL, "slab halos: not with a solution adjustment");
   if (g->graph) {
     cudaGraphExecDestroy(g->graph);
     g->graph = nullptr;

@@ -58,6 +58,7 @@ exa_status_t ensure_tables() {
   if ((s = upload_tables_ensemble())) return s;
   if ((s = upload_tables_faces())) return s;
   if ((s = upload_tables_fv())) return s;
+  if ((s = upload_tables_adjust())) return s;
   g_tables_done[dev & 255] = true;
   return EXA_OK;
 }

@@ -123,6 +123,7 @@ exa_status_t upload_tables_faces();
 exa_status_t upload_tables_fv();
 exa_status_t upload_tables_amr();
 exa_status_t upload_tables_limiter();
+exa_status_t upload_tables_adjust();
 
 // FV step (scheme 0 Godunov, 1 MUSCL-Hancock) on the subcell patches
 // lim[cell] (P subcells + g ghost layers per direction, 5 variables) of the
@@ -154,6 +155,11 @@ size_t fv3_smem(int P, int g, int scheme);
 // limiting-grid bookkeeping (limiting.cu): status from the DMP /
 // admissibility verdicts with spreading and the cell lists; the merge of
 // the per-cell extrema over faces; a finiteness check of listed cells
+// solution adjustment on a uniform grid (adjust.cu): the hook at every node
+// of every cell, cell centers (i + 1/2) dx, t = *time_dev + *dt_dev
+exa_status_t grid_adjust(int dim, int order, const int* n, const double* dx, long ncells, double* luh,
+                         const double* time_dev, const double* dt_dev, const exa_adjust_t& hook, cudaStream_t st);
+exa_status_t check_adjust_hook(const exa_adjust_t* h);
 exa_status_t limiting_status(int dim, const int* ncell, const int* bc, int npc, int planar, int admissibility,
                              int steps_till_cured, const double* luh, int* ok, int* status, int* status_tmp,
                              int* cure, int* list_patch, int* list_fv, int* counts, cudaStream_t st);

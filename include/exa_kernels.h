@@ -308,6 +308,46 @@ exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable);
  *     normal flux of QOut (slip wall). */
 enum { EXA_BC_PERIODIC = 0, EXA_BC_OUTFLOW = 1, EXA_BC_REFLECT = 2 };
 exa_status_t exa_aderdg_grid_set_boundary(exa_aderdg_grid* g, const int* bc);
+/* Solution adjustment (kernels/aderdg/generic/c/{2d,3d}/solutionAdjustment.
+ * cpph: the solver's adjustPointSolution hook called at every Gauss-Legendre
+ * node x = center + dx (xi - 1/2) of a cell with the node's weight, t and
+ * dt; ADERDGSolver.cpp:2072-2092 applies it for the initial conditions at
+ * t = 0 and :2158-2170 after every solutionUpdate at t + dt, whenever the
+ * solver's useAdjustSolution says so).  PDE hooks cannot cross to the
+ * device, so the hook is one of these built-in forms:
+ *   EXA_ADJUST_SINE_WAVE: Q := (rho = 1 + a sin(2 pi (x0 + x1)), u = v = 1,
+ *     w = 0, p = 1), param[0] = a (the 2D sine-wave benchmark state);
+ *   EXA_ADJUST_ISENTROPIC_VORTEX: Q := the isentropic vortex of strength
+ *     eps = param[0] around (1/2, 1/2), radius 0.1, on the flow (1, 1)
+ *     (the 3D benchmark state, extruded in z);
+ *   EXA_ADJUST_HEAT_SOURCE: time-dependent forcing, E += dt A exp(-|x -
+ *     xc|^2 / s^2) (1 + sin(2 pi f t)), param = {A, s, f, xc0, xc1, xc2}.
+ * when = EXA_ADJUST_AT_START applies the hook only at t == 0 (the
+ * demonstrators' useAdjustSolution), EXA_ADJUST_ALWAYS at every call. */
+enum { EXA_ADJUST_NONE = 0, EXA_ADJUST_SINE_WAVE = 1, EXA_ADJUST_ISENTROPIC_VORTEX = 2,
+       EXA_ADJUST_HEAT_SOURCE = 3 };
+enum { EXA_ADJUST_AT_START = 0, EXA_ADJUST_ALWAYS = 1 };
+typedef struct {
+  int kind;        /* EXA_ADJUST_* */
+  int when;        /* EXA_ADJUST_AT_START or EXA_ADJUST_ALWAYS */
+  double param[6];
+} exa_adjust_t;
+/* kernels::aderdg::generic::c::solutionAdjustment (Kernels.h:129-131, 347)
+ * for one cell, HOST pointers: luh [B^dim][5], center[dim], dx[dim]. */
+exa_status_t exa_aderdg_solutionAdjustment(int dim, int order, double* luh, const double* center,
+                                           const double* dx, double t, double dt, const exa_adjust_t* hook);
+/* batched, device-resident: luh [ncells][B^dim][5], centers [ncells][dim]
+ * (device), cell size desc->dx */
+exa_status_t exa_aderdg_solution_adjustment(const exa_aderdg_desc_t* desc, long ncells, double* luh,
+                                            const double* centers, double t, double dt,
+                                            const exa_adjust_t* hook, void* stream);
+/* The grid applies the hook after every step's update at the new time
+ * t + dt with that dt (ADERDGSolver::updateSolution :2158-2170; cell centers
+ * (i + 1/2) dx), before the next dt is taken from the adjusted state; NULL
+ * (or kind EXA_ADJUST_NONE) turns it off.  EXA_ADJUST_AT_START hooks never
+ * fire during stepping (t > 0); exa_aderdg_grid_init sets the initial
+ * state. */
+exa_status_t exa_aderdg_grid_set_adjustment(exa_aderdg_grid* g, const exa_adjust_t* hook);
 exa_status_t exa_aderdg_grid_stream(exa_aderdg_grid* g, void** stream);
 /* per-phase CUDA-event timing of every step (disables graph replay):
  * predictor (k_predictor) and corrector (k_corrector + k_commit) */

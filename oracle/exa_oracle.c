@@ -1749,3 +1749,37 @@ void orc_fv_periodic_ghosts_3d(int P, int g, int D, double* luh) {
         memcpy(luh + I3(S, D, i, j, k, 0), luh + I3(S, D, si, sj, sk, 0), sizeof(double) * D);
       }
 }
+
+/* ------------------------------------------------------------------ */
+/* Solution adjustment (kernels/aderdg/generic/c/3d/solutionAdjustment.cpph:
+ * 17-52, 2D c/2d/solutionAdjustment.cpph): the adjustPointSolution hook at
+ * every Gauss-Legendre node x = center + dx (xi - 1/2), loops i (z), j (y),
+ * k (x) in 3D and i (y), j (x) in 2D; the hook is one of the built-in forms
+ * of the device library (kind 1 sine wave, 2 isentropic vortex, 3 heat
+ * source; when 0 = only at t == 0). */
+#include "adjust_hooks.h"
+
+void orc_solution_adjustment(int dim, int order, double* luh, const double* center, const double* dx, double t,
+                             double dt, int kind, int when, const double* param) {
+  const int B = order + 1;
+  int i, j, k;
+  double x[3];
+  if (kind == 0 || (when == 0 && t != 0.0)) return;
+  if (dim == 3) {
+    for (i = 0; i < B; i++)
+      for (j = 0; j < B; j++)
+        for (k = 0; k < B; k++) {
+          x[2] = center[2] + dx[2] * (exa_gl_nodes[order][i] - 0.5);
+          x[1] = center[1] + dx[1] * (exa_gl_nodes[order][j] - 0.5);
+          x[0] = center[0] + dx[0] * (exa_gl_nodes[order][k] - 0.5);
+          orc_adjust_point(kind, dim, param, x, t, dt, luh + ((i * B + j) * B + k) * 5);
+        }
+  } else {
+    for (i = 0; i < B; i++)
+      for (j = 0; j < B; j++) {
+        x[0] = center[0] + dx[0] * (exa_gl_nodes[order][j] - 0.5);
+        x[1] = center[1] + dx[1] * (exa_gl_nodes[order][i] - 0.5);
+        orc_adjust_point(kind, dim, param, x, t, dt, luh + (i * B + j) * 5);
+      }
+  }
+}

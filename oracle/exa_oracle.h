@@ -209,6 +209,12 @@ void orc_fv_boundary_ghosts(int dim, int P, int g, double* luh, int face, int ru
 void orc_limiting_initial_bounds(int dim, int order, const int* n, const double* luh, int nobs, double* bmin,
                                  double* bmax, const int* bc);
 
+/* solutionAdjustment of one cell with a built-in adjustPointSolution form
+ * (kind 1 sine wave, 2 isentropic vortex, 3 heat source; when 0: only at
+ * t == 0, 1: always), as exa_adjust_t of the device library. */
+void orc_solution_adjustment(int dim, int order, double* luh, const double* center, const double* dx, double t,
+                             double dt, int kind, int when, const double* param);
+
 /* counter-based noise shared with the device IC kernel */
 double orc_noise_u01(unsigned long long seed, unsigned long long idx);
 

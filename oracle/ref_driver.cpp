@@ -30,6 +30,7 @@
 #include "kernels/LimiterProjectionMatrices.h"
 #include "kernels/limiter/generic/Limiter.h"
 #include "exahype/solvers/ADERDGSolver.h"
+#include "adjust_hooks.h"
 
 namespace {
 
@@ -101,6 +102,12 @@ struct Euler {
   void pointSource(const double* const, const double* const, const double, const double, double*, int) {}
   void boundaryValues(const double* const, const double, const double, const int, const int,
                       const double* const, const double* const, double*, double*) {}
+  /* adjustPointSolution: one of the built-in forms of adjust_hooks.h */
+  int adj_kind = 0;
+  const double* adj_param = nullptr;
+  void adjustPointSolution(const double* const x, const double, const double t, const double dt, double* Q) {
+    orc_adjust_point(adj_kind, DIMENSIONS, adj_param, x, t, dt, Q);
+  }
   /* FV boundary hook (FiniteVolumesSolver::boundaryValues): rule 1 copies
    * the inside state (EulerFV's outflow), rule 2 also negates the normal
    * momentum (slip wall) */
@@ -358,6 +365,23 @@ static void fv_boundary_t(double* luh, int face, int rule) {
 }
 
 extern "C" {
+
+/* The reference's solutionAdjustment kernel (c/{2d,3d}/solutionAdjustment.
+ * cpph) on one cell of order 2..5 with a built-in hook of adjust_hooks.h */
+int ref_solution_adjustment(int order, double* luh, const double* center, const double* dx, double t, double dt,
+                            int kind, const double* param) {
+#define ACASE(N)                                                                  \
+  case N: {                                                                       \
+    Euler<N, 0> s;                                                                \
+    s.adj_kind = kind;                                                            \
+    s.adj_param = param;                                                          \
+    kernels::aderdg::generic::c::solutionAdjustment(s, luh, vec(center), vec(dx), t, dt); \
+    return 0;                                                                     \
+  }
+  switch (order) { ACASE(2) ACASE(3) ACASE(4) ACASE(5) }
+#undef ACASE
+  return -1;
+}
 
 /* patch 3, 5, 7, 9 or 11 subcells (limiter patches of orders 1..5) with
  * ghost 1 or 2; returns -1 for other sizes */

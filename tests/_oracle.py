@@ -88,6 +88,7 @@ def lib():
                                          C.c_void_p, C.c_void_p]
     L.orc_limiting_initial_bounds.argtypes = [i, i, _ip, _dp, i, _dp, _dp, C.c_void_p]
     L.orc_fv_boundary_ghosts.argtypes = [i, i, i, _dp, i, i]
+    L.orc_solution_adjustment.argtypes = [i, i, _dp, _dp, _dp, d, d, i, i, _dp]
     _lib = L
     return L
 
@@ -290,6 +291,9 @@ def ref_lib(dim):
         if hasattr(L, 'ref_fv_step'):
             L.ref_fv_step.restype = d
             L.ref_fv_step.argtypes = [i, i, _dp, _dp, d, C.c_void_p]
+        if hasattr(L, 'ref_solution_adjustment'):
+            L.ref_solution_adjustment.restype = i
+            L.ref_solution_adjustment.argtypes = [i, _dp, _dp, _dp, d, d, i, _dp]
         if hasattr(L, 'ref_fv_boundary'):
             L.ref_fv_boundary.restype = i
             L.ref_fv_boundary.argtypes = [i, i, _dp, i, i]
