@@ -181,6 +181,7 @@ SIGNATURES = {
     'exa_aderdg_grid_set_halo': (i32, [vp, i32]),
     'exa_aderdg_grid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_grid_set_adjustment': (i32, [vp, vp]),
+    'exa_fv_patchgrid_set_boundary': (i32, [vp, C.POINTER(i32)]),
     'exa_aderdg_solution_adjustment': (i32, [C.POINTER(AderdgDesc), i64, vp, vp, f64, f64, vp, vp]),
     'exa_aderdg_solutionAdjustment': (i32, [i32, i32, dptr, dptr, dptr, f64, f64, vp]),
     'exa_aderdg_grid_halo_buffers': (i32, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),

@@ -1026,8 +1026,12 @@ exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev) {
 // x fastest), which is the batched FV entry points' layout.
 namespace exa {
 
-// one thread per face-ghost cell of every patch
-__global__ void k_fv_patch_exchange(int P, int g, int D, int npx, int npy, double* luh) {
+// one thread per face-ghost cell of every patch; at a domain-boundary face
+// (bcx / bcy != 0) the ghosts mirror the patch's own boundary layers, ghost k
+// <- interior g - 1 - k counted from the face (FiniteVolumesSolver::
+// mergeWithBoundaryData, commons.cpph:99-340), the normal momentum negated
+// for a reflecting wall
+__global__ void k_fv_patch_exchange(int P, int g, int D, int npx, int npy, int bcx, int bcy, double* luh) {
   const int S = P + 2 * g;
   const long per = 4L * g * P;  // face ghosts per patch: left, right, bottom, top
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1036,20 +1040,29 @@ __global__ void k_fv_patch_exchange(int P, int g, int D, int npx, int npy, doubl
   const int r = (int)(gid % per);
   const int side = r / (g * P), i = (r / g) % P, k = r % g;  // i along the face, k across
   const int px = (int)(patch % npx), py = (int)(patch / npx);
-  int j, x, nj, nx, qx = px, qy = py;  // destination (j, x) and source (nj, nx) in patch (qx, qy)
+  // destination (j, x) and source (nj, nx) in patch (qx, qy)
+  int j, x, nj, nx, qx = px, qy = py, flip = -1;
   if (side == 0) {        // left ghosts <- left neighbour's right boundary layer
-    j = g + i; x = k; qx = (px + npx - 1) % npx; nj = j; nx = P + k;
+    j = g + i; x = k; nj = j;
+    if (bcx && px == 0) { nx = 2 * g - 1 - k; flip = bcx == EXA_BC_REFLECT ? 1 : -1; }
+    else { qx = (px + npx - 1) % npx; nx = P + k; }
   } else if (side == 1) { // right ghosts <- right neighbour's left boundary layer
-    j = g + i; x = g + P + k; qx = (px + 1) % npx; nj = j; nx = g + k;
+    j = g + i; x = g + P + k; nj = j;
+    if (bcx && px == npx - 1) { nx = g + P - 1 - k; flip = bcx == EXA_BC_REFLECT ? 1 : -1; }
+    else { qx = (px + 1) % npx; nx = g + k; }
   } else if (side == 2) { // bottom ghosts <- lower neighbour's top boundary layer
-    j = k; x = g + i; qy = (py + npy - 1) % npy; nj = P + k; nx = x;
+    j = k; x = g + i; nx = x;
+    if (bcy && py == 0) { nj = 2 * g - 1 - k; flip = bcy == EXA_BC_REFLECT ? 2 : -1; }
+    else { qy = (py + npy - 1) % npy; nj = P + k; }
   } else {                // top ghosts <- upper neighbour's bottom boundary layer
-    j = g + P + k; x = g + i; qy = (py + 1) % npy; nj = g + k; nx = x;
+    j = g + P + k; x = g + i; nx = x;
+    if (bcy && py == npy - 1) { nj = g + P - 1 - k; flip = bcy == EXA_BC_REFLECT ? 2 : -1; }
+    else { qy = (py + 1) % npy; nj = g + k; }
   }
   const long src_patch = (long)qy * npx + qx;
   double* dst = luh + (patch * S * S + (long)j * S + x) * D;
   const double* src = luh + (src_patch * S * S + (long)nj * S + nx) * D;
-  for (int m = 0; m < D; m++) dst[m] = src[m];
+  for (int m = 0; m < D; m++) dst[m] = m == flip ? -src[m] : src[m];
 }
 
 // density sine wave of the whole domain on every patch (global coordinates
@@ -1335,6 +1348,7 @@ struct exa_fv_patchgrid {
   size_t count = 0;
   long npatches = 0;
   bool primed = false;  // slot [0] holds the CFL dt of the current state (small-patch path)
+  int bc[2] = {0, 0};   // EXA_BC_* per dimension
 };
 
 namespace exa {
@@ -1359,7 +1373,8 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
   const exa_fv_desc_t& d = g->desc;
   const int S = d.patch + 2 * d.ghost;
   const long nex = 4L * d.ghost * d.patch * g->npatches;
-  k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy, g->luh);
+  k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy,
+                                                                       g->bc[0], g->bc[1], g->luh);
   count_launch();
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
   if (d.patch <= kFvSmallMax && d.npar == 0) {
@@ -1537,6 +1552,15 @@ exa_status_t exa_fv_patchgrid_status(exa_fv_patchgrid* g, double* time, double* 
   memcpy(&t, &h[1], 8);
   if (time) *time = t;
   if (last_dt) *last_dt = dt;
+  return EXA_OK;
+}
+
+exa_status_t exa_fv_patchgrid_set_boundary(exa_fv_patchgrid* g, const int* bc) {
+  if (!g || !bc) return set_error(EXA_EINVAL, "NULL argument");
+  for (int i = 0; i < 2; i++)
+    if (bc[i] < EXA_BC_PERIODIC || bc[i] > EXA_BC_REFLECT) return set_error(EXA_EINVAL, "unknown boundary rule");
+  g->bc[0] = bc[0];
+  g->bc[1] = bc[1];
   return EXA_OK;
 }
 

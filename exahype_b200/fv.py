@@ -149,6 +149,12 @@ class FVPatchGrid:
         g, P, S = self.ghost, self.patch, self.side
         return q.reshape(self.npy, self.npx, S, S, 5)[:, :, g:g + P, g:g + P]
 
+    def set_boundary(self, bc):
+        """Boundary rule per dimension: _lib.BC_PERIODIC / BC_OUTFLOW /
+        BC_REFLECT (see exa_fv_patchgrid_set_boundary)."""
+        arr = (C.c_int * 2)(*list(bc)[:2])
+        call('exa_fv_patchgrid_set_boundary', self.h, arr)
+
     def step(self, nsteps=1):
         call('exa_fv_patchgrid_step', self.h, int(nsteps))
 

@@ -663,7 +663,8 @@ exa_status_t exa_fv_grid_stream(exa_fv_grid* g, void** stream);
 exa_status_t exa_fv_grid_device_state(exa_fv_grid* g, double** luh_dev);
 
 /* ---- Device-resident grid of FV patches (the reference's FV layout) ----
- * npx x npy periodic patches of patch x patch subcells (+ ghost layers: 1
+ * npx x npy patches (periodic, or with exa_fv_patchgrid_set_boundary's
+ * rules) of patch x patch subcells (+ ghost layers: 1
  * Godunov, 2 MUSCL-Hancock) over [0,length)^2, stored back to back (x
  * fastest) like the batched FV entry points.  One step: face ghost layers
  * copied from the neighbouring patches' boundary layers (ghostLayerFilling,
@@ -688,6 +689,16 @@ exa_status_t exa_fv_patchgrid_step(exa_fv_patchgrid* g, int nsteps);
 /* simulated time and the dt of the last step */
 exa_status_t exa_fv_patchgrid_status(exa_fv_patchgrid* g, double* time, double* last_dt);
 exa_status_t exa_fv_patchgrid_stream(exa_fv_patchgrid* g, void** stream);
+/* Boundary rule per dimension (bc[2], EXA_BC_*) in place of the periodic
+ * wrap: a domain-boundary patch fills that face's ghost layers from its own
+ * boundary layers as FiniteVolumesSolver::mergeWithBoundaryData does
+ * (FiniteVolumesSolver.cpp:689-727: boundaryLayerExtraction,
+ * boundaryConditions with the mirrored index K = g - 1 - k through the
+ * boundaryValues hook, ghostLayerFillingAtBoundary; commons.cpph:99-340):
+ * ghost k from the face <- interior layer k from the face; EXA_BC_OUTFLOW
+ * copies (the EulerFV demonstrator's boundaryValues), EXA_BC_REFLECT also
+ * negates the normal momentum. */
+exa_status_t exa_fv_patchgrid_set_boundary(exa_fv_patchgrid* g, const int* bc);
 
 /* rusanov (riemannsolvers/c/rusanov.cpph:24-83), host drop-in, returns s_max */
 exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL,

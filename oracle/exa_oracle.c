@@ -815,8 +815,18 @@ void orc_aderdg_sample_step(int dim, int order, int planar, long ncells,
  * dt = min over patches of the CFL rule, then every patch's solutionUpdate
  * with luh_new = luh beforehand (FiniteVolumesSolver.cpp:529-531).
  * dx = the patch extent.  Returns the dt used. */
+void orc_fv_boundary_ghosts(int dim, int P, int g, double* luh, int face, int rule);
+
 double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
                                 double* luh, const double* dx) {
+  return orc_fv_patchgrid_step_2d_bc(scheme, P, npx, npy, planar, luh, dx, NULL);
+}
+
+/* bc (nullable: periodic) = boundary rule per dimension; a domain-boundary
+ * face of a patch takes its ghosts from the patch itself
+ * (orc_fv_boundary_ghosts, FiniteVolumesSolver::mergeWithBoundaryData) */
+double orc_fv_patchgrid_step_2d_bc(int scheme, int P, int npx, int npy, int planar,
+                                   double* luh, const double* dx, const int* bc) {
   const int g = scheme == 0 ? 1 : 2, V = 5, S = P + 2 * g;
   const long per = (long)S * S * V, np = (long)npx * npy;
   long p;
@@ -827,14 +837,20 @@ double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
     const double* R = luh + ((long)py * npx + (px + 1) % npx) * per;
     const double* Bm = luh + ((long)((py + npy - 1) % npy) * npx + px) * per;
     const double* T = luh + ((long)((py + 1) % npy) * npx + px) * per;
+    const int wl = bc && bc[0] && px == 0, wr = bc && bc[0] && px == npx - 1;
+    const int wb = bc && bc[1] && py == 0, wt = bc && bc[1] && py == npy - 1;
     int i, k;
     for (i = g; i < g + P; i++)
       for (k = 0; k < g; k++) {
-        memcpy(u + ((long)i * S + k) * V, L + ((long)i * S + P + k) * V, sizeof(double) * V);
-        memcpy(u + ((long)i * S + g + P + k) * V, R + ((long)i * S + g + k) * V, sizeof(double) * V);
-        memcpy(u + ((long)k * S + i) * V, Bm + ((long)(P + k) * S + i) * V, sizeof(double) * V);
-        memcpy(u + ((long)(g + P + k) * S + i) * V, T + ((long)(g + k) * S + i) * V, sizeof(double) * V);
+        if (!wl) memcpy(u + ((long)i * S + k) * V, L + ((long)i * S + P + k) * V, sizeof(double) * V);
+        if (!wr) memcpy(u + ((long)i * S + g + P + k) * V, R + ((long)i * S + g + k) * V, sizeof(double) * V);
+        if (!wb) memcpy(u + ((long)k * S + i) * V, Bm + ((long)(P + k) * S + i) * V, sizeof(double) * V);
+        if (!wt) memcpy(u + ((long)(g + P + k) * S + i) * V, T + ((long)(g + k) * S + i) * V, sizeof(double) * V);
       }
+    if (wl) orc_fv_boundary_ghosts(2, P, g, u, 0, bc[0]);
+    if (wr) orc_fv_boundary_ghosts(2, P, g, u, 1, bc[0]);
+    if (wb) orc_fv_boundary_ghosts(2, P, g, u, 2, bc[1]);
+    if (wt) orc_fv_boundary_ghosts(2, P, g, u, 3, bc[1]);
   }
   double dt = DBL_MAX;
   for (p = 0; p < np; p++) {

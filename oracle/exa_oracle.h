@@ -147,6 +147,10 @@ void orc_fv_periodic_ghosts_3d(int patch, int ghost, int ndata, double* luh);
 /* one step of a periodic npx x npy grid of FV patches (dx = patch extent) */
 double orc_fv_patchgrid_step_2d(int scheme, int P, int npx, int npy, int planar,
                                 double* luh, const double* dx);
+/* the same with a boundary rule per dimension (bc[2], nullable: periodic):
+ * domain-boundary faces filled by orc_fv_boundary_ghosts */
+double orc_fv_patchgrid_step_2d_bc(int scheme, int P, int npx, int npy, int planar, double* luh, const double* dx,
+                                   const int* bc);
 
 /* A-posteriori subcell limiter, kernels/limiter/generic/c/Limiter.cpp, for
  * one cell of order N (B = N+1 nodes, S = 2N+1 subcells per direction):

@@ -68,6 +68,8 @@ def lib():
     L.orc_amr_restriction.argtypes = [i, i, i, _dp, _dp, i, _ip]
     L.orc_fv_patchgrid_step_2d.restype = d
     L.orc_fv_patchgrid_step_2d.argtypes = [i, i, i, i, i, _dp, _dp]
+    L.orc_fv_patchgrid_step_2d_bc.restype = d
+    L.orc_fv_patchgrid_step_2d_bc.argtypes = [i, i, i, i, i, _dp, _dp, C.c_void_p]
     L.orc_noise_u01.restype = d
     L.orc_noise_u01.argtypes = [C.c_ulonglong, C.c_ulonglong]
     L.orc_limiter_project_on_fv.argtypes = [i, i, i, i, _dp, _dp]

@@ -184,3 +184,32 @@ def test_fv_patch_grid_vs_oracle(scheme, P, npx, npy):
         u = got.copy()  # next step from the GPU state
     assert abs(g.status()['time'] - t) <= 1e-12 * t
     g.destroy()
+
+
+@pytest.mark.parametrize('scheme', [0, 1])
+@pytest.mark.parametrize('P,npx,npy,bc', [(10, 3, 4, (1, 2)), (7, 2, 2, (2, 1)), (16, 1, 3, (2, 0)),
+                                          (20, 2, 1, (1, 1))])
+def test_fv_patch_grid_walls_vs_oracle(scheme, P, npx, npy, bc):
+    """Patch grid with outflow / reflecting walls: domain-boundary ghosts
+    from the patch's own boundary layers (orc_fv_boundary_ghosts, pinned to
+    the reference's FiniteVolumesSolver::mergeWithBoundaryData kernels)."""
+    g = E.FVPatchGrid(scheme, P, npx, npy)
+    g.init(amp=0.2, seed=5, noise=1e-3)
+    g.set_boundary(bc)
+    u = g.get_state()
+    dx = np.array([1.0 / npx, 1.0 / npy])
+    bcs = np.asarray(bc, dtype=np.int32)
+    for s in range(5):
+        g.step(1)
+        O.lib().orc_fv_patchgrid_step_2d_bc(scheme, P, npx, npy, 0, u, dx, bcs.ctypes.data)
+        got = g.get_state()
+        a, b = g.interiors(got), g.interiors(u)
+        assert rel(a, b) < 1e-13, (s, rel(a, b))
+        u = got.copy()
+    # the walls change the result against the periodic grid
+    p = E.FVPatchGrid(scheme, P, npx, npy)
+    p.init(amp=0.2, seed=5, noise=1e-3)
+    p.step(5)
+    assert rel(g.interiors(g.get_state()), p.interiors(p.get_state())) > 1e-8
+    g.destroy()
+    p.destroy()
