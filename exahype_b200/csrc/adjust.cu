@@ -163,31 +163,4 @@ exa_status_t exa_aderdg_solution_adjustment(const exa_aderdg_desc_t* desc, long 
   return launch_adjust(a, luh, as_stream(stream));
 }
 
-exa_status_t exa_aderdg_solutionAdjustment(int dim, int order, double* luh, const double* center,
-                                           const double* dx, double t, double dt, const exa_adjust_t* hook) {
-  if ((dim != 2 && dim != 3) || order < 1 || order > kMaxOrder || !luh || !center || !dx)
-    return set_error(EXA_EINVAL, "bad argument");
-  if (exa_status_t s = check_hook(hook)) return s;
-  if (exa_status_t s = ensure_tables()) return s;
-  const int nn = dim == 3 ? (order + 1) * (order + 1) * (order + 1) : (order + 1) * (order + 1);
-  double* d_buf = nullptr;
-  cudaError_t e = cudaMalloc(&d_buf, sizeof(double) * (nn * kV + 3));
-  if (e != cudaSuccess) return cuda_status(e, "adjustment buffer");
-  exa_aderdg_desc_t desc{};
-  desc.dim = dim;
-  desc.order = order;
-  desc.nvar = kV;
-  for (int d = 0; d < dim; d++) desc.dx[d] = dx[d];
-  e = cudaMemcpy(d_buf, luh, sizeof(double) * nn * kV, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_buf + nn * kV, center, sizeof(double) * dim, cudaMemcpyHostToDevice);
-  exa_status_t s = e == cudaSuccess ? exa_aderdg_solution_adjustment(&desc, 1, d_buf, d_buf + nn * kV, t, dt, hook, nullptr)
-                                    : cuda_status(e, "adjustment upload");
-  if (s == EXA_OK) {
-    e = cudaMemcpy(luh, d_buf, sizeof(double) * nn * kV, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) s = cuda_status(e, "adjustment download");
-  }
-  cudaFree(d_buf);
-  return s;
-}
-
 }  // extern "C"

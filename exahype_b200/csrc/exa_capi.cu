@@ -487,6 +487,26 @@ exa_status_t exa_aderdg_stable_dt(const exa_aderdg_desc_t* desc, long ncells, co
                           (unsigned long long*)dt_min, st);
 }
 
+// solutionAdjustment for one cell through the drop-in workspace (no
+// allocation per call): luh and the center in, luh out
+exa_status_t exa_aderdg_solutionAdjustment(int dim, int order, double* luh, const double* center,
+                                           const double* dx, double t, double dt, const exa_adjust_t* hook) {
+  if ((dim != 2 && dim != 3) || order < 1 || order > kMaxOrder || !luh || !center || !dx || !hook)
+    return set_error(EXA_EINVAL, "bad argument");
+  exa_aderdg_desc_t desc{};
+  desc.dim = dim;
+  desc.order = order;
+  desc.nvar = kV;
+  for (int d = 0; d < dim; d++) desc.dx[d] = dx[d];
+  const size_t nn = (size_t)ipow_h(order + 1, dim) * kV;
+  HostArr arr[2] = {{luh, luh, nn}, {center, nullptr, (size_t)dim}};
+  return run_one_cell(arr, 2, [&](double** p) {
+    exa_status_t s = exa_aderdg_solution_adjustment(&desc, 1, p[0], p[1], t, dt, hook, nullptr);
+    if (s == EXA_OK) s = cuda_status(cudaDeviceSynchronize(), "solutionAdjustment");
+    return s;
+  });
+}
+
 exa_status_t exa_fv_rusanov(int dim, int nvar, int npar, int pde, double* fL, double* fR,
                             const double* qL, const double* qR, int normalNonZero, double* s_max) {
   if ((dim != 2 && dim != 3) || nvar != kV || npar < 0 || npar > 8 || !fL || !fR || !qL || !qR)
