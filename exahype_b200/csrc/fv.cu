@@ -477,7 +477,7 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_godunov_periodic(FVArgs a) {
 }
 
 template <bool PLANAR>
-__global__ void __launch_bounds__(FVP_NT) k_fv_muscl_periodic(FVArgs a) {
+__global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
   constexpr int V = kV;
   constexpr int LX = FVP_TX + 4, LY = FVP_TY + 4;   // state: cells j0-2..j0+TY+1, k0-2..k0+TX+1
   constexpr int RX = FVP_TX + 2, RY = FVP_TY + 2;   // ring: j0-1..j0+TY, k0-1..k0+TX
@@ -741,8 +741,11 @@ exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const doubl
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      cudaError_t e = planar ? cudaFuncSetAttribute(k_fv_muscl_periodic<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem)
-                             : cudaFuncSetAttribute(k_fv_muscl_periodic<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
+      auto kern = planar ? k_fv_muscl_periodic<true> : k_fv_muscl_periodic<false>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
+      // three CTAs of ~72 KB per SM need the largest shared-memory carveout
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
