@@ -100,8 +100,10 @@ __device__ __forceinline__ double fv_face_flux(const double* qL, const double* q
   return smax;
 }
 
+// five 256-thread CTAs (42 KB each) per SM: 48 registers and the largest
+// shared-memory carveout
 template <bool PLANAR, bool FUSED>
-__global__ void __launch_bounds__(FV_NT) k_fv_godunov(FVArgs a) {
+__global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
   constexpr int V = kV, C = kV + 1;
   constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
   __shared__ double su[LY * LX * V];
@@ -736,6 +738,14 @@ exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const doubl
     // for first order than per-cell face fluxes (k_fv_godunov_periodic),
     // whose doubled Riemann work is not paid back by the saved barrier
     dim3 gt((d.patch + FV_TX - 1) / FV_TX, (d.patch + FV_TY - 1) / FV_TY, 1);
+    static bool gattr[2] = {false, false};
+    if (!gattr[planar]) {
+      cudaError_t e = cudaFuncSetAttribute(planar ? k_fv_godunov<true, true> : k_fv_godunov<false, true>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return cuda_status(e, "godunov attribute");
+      gattr[planar] = true;
+    }
     if (planar) k_fv_godunov<true, true><<<gt, FV_NT, 0, st>>>(a);
     else k_fv_godunov<false, true><<<gt, FV_NT, 0, st>>>(a);
   } else {
