@@ -1038,26 +1038,49 @@ void orc_aderdg_grid_ic(int dim, int order, const int* n, const double* dx,
 }
 
 /* ------------------------------------------------------------------ */
-/* FV Rusanov: kernels/finitevolumes/riemannsolvers/c/rusanov.cpph:24-83 */
-double orc_rusanov(int dim, int nvar, int npar, int planar, double* fL,
-                   double* fR, const double* qL, const double* qR, int d) {
-  (void)npar;
-  double sL[5], sR[5];
-  orc_euler_eigenvalues(planar, qL, d, sL);
-  orc_euler_eigenvalues(planar, qR, d, sR);
+/* FV Rusanov: kernels/finitevolumes/riemannsolvers/c/rusanov.cpph:24-83
+ * (2D) / :98-156 (3D), without the non-conservative product: s_max over
+ * the eigenvalues of both sides, fL = fR = 0.5 s_max (qL - qR) +
+ * 0.5 (FL_d + FR_d), flux arrays zero before the PDE fills them.  The PDE
+ * comes as callbacks (the reference's unit test drives the same kernel
+ * with a mock solver, RusanovTest.cpp:33-90); nvar <= 16. */
+double orc_rusanov_pde(int dim, int nvar, orc_flux_fn flux, orc_eig_fn eig, void* ctx,
+                       double* fL, double* fR, const double* qL, const double* qR, int d) {
+  double sL[16], sR[16];
+  eig(ctx, qL, d, sL);
+  eig(ctx, qR, d, sR);
   double smax = -1.0;
   for (int i = 0; i < nvar; i++) smax = fabs(sL[i]) > smax ? fabs(sL[i]) : smax;
   for (int i = 0; i < nvar; i++) smax = fabs(sR[i]) > smax ? fabs(sR[i]) : smax;
-  double FL[15], FR[15];
-  orc_euler_flux(dim, planar, qL, FL);
-  orc_euler_flux(dim, planar, qR, FR);
+  double FL[3 * 16], FR[3 * 16];
+  for (int i = 0; i < 3 * 16; i++) FL[i] = FR[i] = 0.0;
+  flux(ctx, qL, FL);
+  flux(ctx, qR, FR);
   for (int i = 0; i < nvar; i++) {
     double f = 0.5 * smax * (qL[i] - qR[i]);
-    f += 0.5 * (FL[5 * d + i] + FR[5 * d + i]);
+    f += 0.5 * (FL[nvar * d + i] + FR[nvar * d + i]);
     fL[i] = f;
     fR[i] = f;
   }
+  (void)dim;
   return smax;
+}
+
+struct euler_ctx { int dim, planar; };
+static void euler_flux_cb(void* c, const double* q, double* F) {
+  const struct euler_ctx* e = (const struct euler_ctx*)c;
+  orc_euler_flux(e->dim, e->planar, q, F);
+}
+static void euler_eig_cb(void* c, const double* q, int d, double* lam) {
+  orc_euler_eigenvalues(((const struct euler_ctx*)c)->planar, q, d, lam);
+}
+
+/* the Euler PDE's Rusanov flux (5 variables) */
+double orc_rusanov(int dim, int nvar, int npar, int planar, double* fL,
+                   double* fR, const double* qL, const double* qR, int d) {
+  struct euler_ctx e = {dim, planar};
+  (void)npar;
+  return orc_rusanov_pde(dim, nvar, euler_flux_cb, euler_eig_cb, &e, fL, fR, qL, qR, d);
 }
 
 /* FV Godunov 2D: kernels/finitevolumes/godunov/c/2d/godunov.cpph:33-120 */

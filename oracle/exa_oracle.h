@@ -104,6 +104,11 @@ void orc_aderdg_grid_ic(int dim, int order, const int* n, const double* dx,
                         unsigned long long seed, double noise_amp);
 
 /* ---- finite volumes, 2D patch (reference godunov / musclhancock) ---- */
+/* PDE callbacks of orc_rusanov_pde: F is [dim][nvar], lam is [nvar] */
+typedef void (*orc_flux_fn)(void* ctx, const double* q, double* F);
+typedef void (*orc_eig_fn)(void* ctx, const double* q, int d, double* lam);
+double orc_rusanov_pde(int dim, int nvar, orc_flux_fn flux, orc_eig_fn eig, void* ctx,
+                       double* fL, double* fR, const double* qL, const double* qR, int d);
 double orc_rusanov(int dim, int nvar, int npar, int planar, double* fL,
                    double* fR, const double* qL, const double* qR, int d);
 double orc_fv_godunov_2d(int patch, int ghost, int nvar, int npar, int planar,

@@ -14,6 +14,7 @@
 #include <vector>
 #include <set>
 #include <thread>
+#include <pthread.h>
 #include <float.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -100,8 +101,25 @@ struct Euler {
     for (int i = 0; i < 25; i++) Bn[i] = 0.0;
   }
   void pointSource(const double* const, const double* const, const double, const double, double*, int) {}
-  void boundaryValues(const double* const, const double, const double, const int, const int,
-                      const double* const, const double* const, double*, double*) {}
+  /* ADER-DG boundary hook (ADERDGSolver::boundaryValues, called per face
+   * node by boundaryConditions.cpph): rule 1 copies the inside state and
+   * flux (outflow), rule 2 negates the normal momentum and takes the normal
+   * flux of that reflected state (slip wall) */
+  void boundaryValues(const double* const, const double, const double, const int, const int normalNonZero,
+                      const double* const fluxIn, const double* const stateIn, double* fluxOut,
+                      double* stateOut) {
+    for (int m = 0; m < 5; m++) {
+      stateOut[m] = stateIn[m];
+      fluxOut[m] = fluxIn[m];
+    }
+    if (rule == 2) {
+      stateOut[normalNonZero + 1] = -stateOut[normalNonZero + 1];
+      double F2[3][5];
+      double* F[3] = {F2[0], F2[1], F2[2]};
+      flux(stateOut, F);
+      for (int m = 0; m < 5; m++) fluxOut[m] = F2[normalNonZero][m];
+    }
+  }
   /* adjustPointSolution: one of the built-in forms of adjust_hooks.h */
   int adj_kind = 0;
   const double* adj_param = nullptr;
@@ -182,9 +200,14 @@ struct DG {
     double lam[5];
     return kernels::aderdg::generic::c::stableTimeStepSize<S>(s, luh, lam, vec(dx));
   }
-  /* one step on a uniform periodic grid (reference non-fused order) */
+  /* one step on a uniform grid (reference non-fused order); periodic in
+   * every dimension d with bc == nullptr or bc[d] == 0, else the faces on
+   * the two domain ends of d go through the reference's boundaryConditions
+   * kernel with rule bc[d] and the Riemann solve of
+   * ADERDGSolver::applyBoundaryConditions (ADERDGSolver.cpp:2854-2925:
+   * outside state on the left for faces 2d, on the right for faces 2d+1) */
   static double grid_step(const int* n, const double* dx, double* luh, int policy,
-                          double dt_fixed, int nthreads) {
+                          double dt_fixed, int nthreads, const int* bc = nullptr) {
     static_assert(P == 0, "grid step without parameters");
     const long nc = DIMENSIONS == 3 ? (long)n[0] * n[1] * n[2] : (long)n[0] * n[1];
 #ifdef _OPENMP
@@ -216,10 +239,19 @@ struct DG {
       }
     }
     for (int d = 0; d < DIMENSIONS; d++) {
+      const int rule = bc ? bc[d] : 0;
 #pragma omp parallel for
       for (long c = 0; c < nc; c++) {
         int r[3] = {(int)(c % n[0]), (int)((c / n[0]) % n[1]),
                     DIMENSIONS == 3 ? (int)(c / ((long)n[0] * n[1])) : 0};
+        if (rule) {
+          const int j0 = r[d];
+          if (j0 == 0) boundary_face(c, 2 * d, d, rule, dx, dtv, qb.data(), fb.data());
+          if (j0 + 1 == n[d]) {
+            boundary_face(c, 2 * d + 1, d, rule, dx, dtv, qb.data(), fb.data());
+            continue;
+          }
+        }
         r[d] = (r[d] + 1) % n[d];
         long cr = DIMENSIONS == 3 ? ((long)r[2] * n[1] + r[1]) * n[0] + r[0]
                                   : (long)r[1] * n[0] + r[0];
@@ -235,6 +267,21 @@ struct DG {
       update(luh + c * NN * D, lduh.data() + c * NN * V, dtv);
     }
     return dtv;
+  }
+  /* the domain-boundary face `face` of cell c: outside state from the
+   * reference's boundaryConditions kernel, then the Riemann solve with the
+   * outside state on the side applyBoundaryConditions puts it */
+  static void boundary_face(long c, int face, int d, int rule, const double* dx, double dtv,
+                            const double* qb, double* fb) {
+    S s;
+    s.rule = rule;
+    double qo[NF * D], fo[NF * V];
+    double* FIn = fb + (c * 2 * DIMENSIONS + face) * NF * V;
+    const double* QIn = qb + (c * 2 * DIMENSIONS + face) * NF * D;
+    kernels::aderdg::generic::c::boundaryConditions<S>(s, fo, qo, FIn, QIn, Vec(0.5), vec(dx), 0.0, dtv,
+                                                       face, d);
+    if (face % 2 == 0) riemann(fo, FIn, qo, QIn, d);
+    else riemann(FIn, fo, QIn, qo, d);
   }
   /* per-cell work of one step on ncells independent cells (each its own
    * periodic neighbour): the CPU-baseline sample */
@@ -270,6 +317,38 @@ struct DG {
 #define EXA_ORDERS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7)
 
 }  // namespace
+
+/* Runs f() on a thread with a 1 GiB stack: the reference keeps its FV work
+ * arrays on the stack (musclhancock/c/2d/musclhancock.cpph:75,102-105), a
+ * 256^2 MUSCL-Hancock patch needs ~25 MB of them. */
+template <typename F>
+static void on_big_stack(F f) {
+  struct Run {
+    static void* go(void* p) {
+      (*static_cast<F*>(p))();
+      return nullptr;
+    }
+  };
+  pthread_attr_t a;
+  pthread_attr_init(&a);
+  pthread_attr_setstacksize(&a, (size_t)1 << 30);
+  pthread_t th;
+  if (pthread_create(&th, &a, &Run::go, &f) == 0) pthread_join(th, nullptr);
+  pthread_attr_destroy(&a);
+}
+
+/* The mock PDE of the reference's Rusanov unit test (exahype/tests/kernels/
+ * finitevolumes/riemannsolvers/c/RusanovTest.cpp:33-60, RusanovTest.h:37-38):
+ * 4 variables, 3 parameters, zero flux, every eigenvalue 1. */
+struct ZeroFluxZeroNCP {
+  static constexpr int NumberOfVariables = 4;
+  static constexpr int NumberOfParameters = 3;
+  void flux(const double* const, double**) {}
+  void eigenvalues(const double* const, const int, double* lambda) {
+    for (int i = 0; i < NumberOfVariables; i++) lambda[i] = 1.0;
+  }
+  void nonConservativeProduct(const double* const, const double* const, double*) {}
+};
 
 #if DIMENSIONS == 2
 /* One step of a single periodic FV patch with the reference's godunov
@@ -461,6 +540,24 @@ double ref_grid_step(int order, const int* n, const double* dx, double* luh, int
   return -1;
 }
 
+/* As ref_grid_step with a boundary rule per dimension (0 periodic, 1 outflow,
+ * 2 reflecting wall) */
+double ref_grid_step_bc(int order, const int* n, const double* dx, double* luh, int policy,
+                        double dt_fixed, int nthreads, const int* bc) {
+#define CASE(N) case N: return DG<N, 0>::grid_step(n, dx, luh, policy, dt_fixed, nthreads, bc);
+  switch (order) { EXA_ORDERS(CASE) }
+#undef CASE
+  return -1;
+}
+
+/* The reference's rusanov on the unit test's mock PDE (useNCP = false,
+ * useFlux = true, as RusanovTest.cpp:81-88 calls it); returns s_max */
+double ref_rusanov_mock(double* fL, double* fR, const double* qL, const double* qR, int d) {
+  ZeroFluxZeroNCP s;
+  return kernels::finitevolumes::riemannsolvers::c::rusanov<false, true, ZeroFluxZeroNCP>(s, fL, fR, qL, qR,
+                                                                                          d);
+}
+
 int ref_sample_step(int order, long ncells, const double* dx, double* luh, double dt,
                     int nthreads) {
 #define CASE(N) case N: DG<N, 0>::sample_step(ncells, dx, luh, dt, nthreads); return 0;
@@ -473,16 +570,15 @@ int ref_sample_step(int order, long ncells, const double* dx, double* luh, doubl
 double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double dt_fixed,
                    double* adm) {
   double r = -1;
-  std::thread th([&]() {
+  on_big_stack([&]() {
 #define PCASE(P)                                                        \
   case P:                                                               \
     r = scheme == 0 ? fv_step_t<P, 1>(0, luh, dx, dt_fixed, adm)        \
                     : fv_step_t<P, 2>(1, luh, dx, dt_fixed, adm);       \
     break;
-    switch (patch) { PCASE(8) PCASE(16) PCASE(32) PCASE(64) PCASE(128) }
+    switch (patch) { PCASE(4) PCASE(5) PCASE(8) PCASE(16) PCASE(32) PCASE(64) PCASE(128) PCASE(256) }
 #undef PCASE
   });
-  th.join();
   return r;
 }
 #endif
@@ -492,7 +588,7 @@ double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double 
  * 3D godunov (scheme 0, ghost 1) or musclhancock (scheme 1, ghost 2) */
 double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double dt_fixed, double* adm) {
   double r = -1;
-  std::thread th([&]() {
+  on_big_stack([&]() {
 #define PCASE(P)                                                          \
   case P:                                                                 \
     r = scheme == 0 ? fv_step3_t<P, 1>(0, luh, dx, dt_fixed, adm)         \
@@ -501,7 +597,6 @@ double ref_fv_step(int scheme, int patch, double* luh, const double* dx, double 
     switch (patch) { PCASE(4) PCASE(5) PCASE(7) PCASE(9) }
 #undef PCASE
   });
-  th.join();
   return r;
 }
 #endif

@@ -50,6 +50,8 @@ def lib():
     L.orc_aderdg_grid_step_bc.restype = d
     L.orc_aderdg_grid_step_bc.argtypes = [i, i, i, _ip, _dp, _dp, i, d, d, C.c_void_p, i, C.c_void_p]
     L.orc_aderdg_grid_ic.argtypes = [i, i, _ip, _dp, _dp, i, d, C.c_ulonglong, d]
+    L.orc_rusanov_pde.restype = d
+    L.orc_rusanov_pde.argtypes = [i, i, C.c_void_p, C.c_void_p, C.c_void_p, _dp, _dp, _dp, _dp, i]
     L.orc_rusanov.restype = d
     L.orc_rusanov.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, i]
     L.orc_fv_godunov_2d.restype = d
@@ -142,6 +144,18 @@ def grid_step(dim, order, n, luh, dt_policy=0, cfl=0.9, dt_fixed=0.0, planar=0,
                                        dt_policy, cfl, dt_fixed, iters.ctypes.data, nthreads,
                                        bcs.ctypes.data if bcs is not None else None)
     return dt, iters
+
+
+def ref_grid_step(dim, order, n, luh, dt_policy=0, dt_fixed=0.0, nthreads=0, dx=None, bc=None):
+    """One step of the reference's own kernels on the uniform grid (periodic,
+    or boundary rules per dimension through its boundaryConditions kernel)."""
+    R = ref_lib(dim)
+    n = np.asarray(n, dtype=np.int32)
+    if dx is None:
+        dx = 1.0 / n.astype(np.float64)
+    bcs = np.asarray(list(bc or []) + [0] * (3 - len(bc or [])), dtype=np.int32)
+    return R.ref_grid_step_bc(order, n, np.asarray(dx, dtype=np.float64), luh, dt_policy, dt_fixed,
+                              nthreads, bcs)
 
 
 def lim_sizes(dim, order, nvar=5, ghost=0):
@@ -296,6 +310,12 @@ def ref_lib(dim):
         if hasattr(L, 'ref_solution_adjustment'):
             L.ref_solution_adjustment.restype = i
             L.ref_solution_adjustment.argtypes = [i, _dp, _dp, _dp, d, d, i, _dp]
+        if hasattr(L, 'ref_grid_step_bc'):
+            L.ref_grid_step_bc.restype = d
+            L.ref_grid_step_bc.argtypes = [i, _ip, _dp, _dp, i, d, i, _ip]
+        if hasattr(L, 'ref_rusanov_mock'):
+            L.ref_rusanov_mock.restype = d
+            L.ref_rusanov_mock.argtypes = [_dp, _dp, _dp, _dp, i]
         if hasattr(L, 'ref_fv_boundary'):
             L.ref_fv_boundary.restype = i
             L.ref_fv_boundary.argtypes = [i, i, _dp, i, i]

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Extract the reference's known-answer data into small numpy fixtures.
 
-Run in a checkout that has the reference sources (the path is the first
-argument, default ``/root/reference``).  It writes, next to this script:
+Run in a checkout that has the reference sources: the path of the reference
+tree is the first argument (or the ``EXA_REFERENCE`` environment variable).  It writes, next to this script:
 
 * ``generic_euler_2d.npz`` / ``generic_euler_3d.npz`` -- every array of
   ``ExaHyPE/exahype/tests/kernels/testdata/generic_euler_testdata.cpp``
@@ -124,7 +124,9 @@ def extract_limiter(ref):
 
 
 if __name__ == '__main__':
-    ref = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('EXA_REFERENCE')
+    if not ref:
+        sys.exit('usage: make_golden.py <reference tree>  (or set EXA_REFERENCE)')
     ge = extract_generic_euler(ref)
     tabs = extract_dg_tables(ref)
     lim = extract_limiter(ref)
