@@ -11,13 +11,18 @@ Metric: cell-updates/s (one cell advanced one step = 1).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|mixed] [--n 81] [--order 4]
 
-N>1 runs one independent replica of the grid per GPU (weak scaling; the
-uniform grid has no cross-replica exchange), launched one process per GPU
-by torch.distributed.run; the timing is the max over ranks.
+N>1 cuts one periodic 81 x 81 x 81N grid into z-slabs, one per GPU (81^3
+cells per GPU, weak scaling): each step exchanges the two boundary face
+layers with the neighbouring slabs and reduces the dt minimum over all
+ranks; launched one process per GPU by torch.distributed.run; the timing is
+the max over ranks.
 
 --impl reference times the reference's own generic CPU kernels (compiled
-from its sources into oracle/_ref) on the host cores, each step a bounded
-sample of the same workload's cells.
+from its sources into oracle/_ref) on all host cores, each step one whole
+step of the grid in the reference's step order.  The default run's CPU
+baseline is one such step from the GPU's state after its timed steps, and
+the GPU's FP64 and mixed-precision steps from that state are compared with
+it over the whole grid (parity_81, mixed.accuracy_vs_oracle).
 """
 import argparse
 import json
@@ -131,6 +136,22 @@ class ClockSampler:
                 'samples': len(sm)}
 
 
+def fp64_fma_peak():
+    """FP64 FMA TFLOP/s of this GPU from the benchmark's own probe library
+    (exahype_b200/libexa_fp64_probe.so, built beside the product library but
+    not part of it): the FP64 roofline denominator."""
+    import ctypes as C
+    so = os.path.join(ROOT, 'exahype_b200', 'libexa_fp64_probe.so')
+    P = C.CDLL(so)
+    P.exa_probe_fp64_fma_tflops.restype = C.c_int
+    P.exa_probe_fp64_fma_tflops.argtypes = [C.POINTER(C.c_double)]
+    v = C.c_double()
+    rc = P.exa_probe_fp64_fma_tflops(C.byref(v))
+    if rc != 0:
+        raise RuntimeError('FP64 peak probe failed: cudaError %d' % rc)
+    return v.value
+
+
 def measured_peaks():
     p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.exists(p):
@@ -154,45 +175,48 @@ def ncu_traffic_per_cell():
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_sample(order, n, state, dt, budget_s, steps=None):
-    """Times the reference's generic kernels (oracle/_ref) -- or the C oracle
-    if the reference build is absent -- on a bounded sample of the grid's
-    cells with all host threads.  Returns (cells/s, kind, cores, sample)."""
+def reference_step_check(ctx, state):
+    """CPU baseline and parity at the benchmark configuration in one pass:
+    one whole-grid step of the reference's own kernels (oracle/_ref, all host
+    cores; the C oracle when that was not built) from the GPU's state after
+    the timed steps is timed, and the GPU's FP64 and mixed-precision steps
+    from the same state are compared with it (relative L2 / Linf over the
+    whole grid, and the dt)."""
     sys.path.insert(0, os.path.join(ROOT, 'tests'))
     import _oracle as O
+    E, args = ctx['E'], ctx['args']
+    n, order = args.n, args.order
     cores = os.cpu_count() or 1
-    B = order + 1
-    per = B ** 3 * 5
-    ncells = state.size // per
-    dx = np.full(3, 1.0 / n)
     R = O.ref_lib(3)
-    if R is not None:
-        kind = 'reference'
-
-        def run(u, m):
-            R.ref_sample_step(order, m, dx, u, dt, cores)
-    else:
-        kind = 'port'
-
-        def run(u, m):
-            O.lib().orc_aderdg_sample_step(3, order, 0, m, dx, u, dt, cores)
-    m0 = min(ncells, 64 * cores)
-    u = np.ascontiguousarray(state[:m0 * per]).copy()
+    kind = 'reference' if R is not None else 'port'
+    nn = np.array([n, n, n], dtype=np.int32)
+    dx = np.full(3, 1.0 / n)
+    ref = np.ascontiguousarray(state).copy()
     t0 = time.perf_counter()
-    run(u, m0)
-    t_cal = time.perf_counter() - t0
-    rate = m0 / max(t_cal, 1e-6)
-    nsteps = steps or 3
-    m = int(min(ncells, max(m0, rate * budget_s / nsteps)))
-    u = np.ascontiguousarray(state[:m * per]).copy()
-    times = []
-    for _ in range(nsteps):
-        t0 = time.perf_counter()
-        run(u, m)
-        times.append(time.perf_counter() - t0)
-    value = m * nsteps / sum(times)
-    sample = '%d of %d cells x %d steps (first cells of the %d^3 state, its dt)' % (m, ncells, nsteps, n)
-    return value, kind, cores, sample, times
+    if R is not None:
+        dt_ref = R.ref_grid_step(order, nn, dx, ref, 0, 0.0, cores)
+    else:
+        dt_ref = O.lib().orc_aderdg_grid_step(3, order, 0, nn, dx, ref, 0, 0.9, 0.0, None, cores)
+    t = time.perf_counter() - t0
+    cpu = {'value': n ** 3 / t, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind,
+           'sample': 'one whole %d^3 grid step (dt + predictor + volume integral + Riemann + surface integral + '
+                     'update) from the GPU state after the timed steps' % n}
+    parity = {'reference': kind, 'from': 'GPU state after warm-up + timed steps, one step on each side'}
+    nrm2, nrmi = float(np.linalg.norm(ref)), float(np.abs(ref).max())
+    for name, prec in (('fp64', E.PREC_FP64), ('mixed', E.PREC_MIXED)):
+        g = E.ADERDGGrid(3, order, (n, n, n), precision=prec)
+        g.set_state(state)
+        dt = float(g.step(1, want_dt=True)[0])
+        got = g.get_state()
+        g.destroy()
+        d = got - ref
+        parity[name] = {'rel_l2': float(np.linalg.norm(d)) / nrm2, 'rel_linf': float(np.abs(d).max()) / nrmi,
+                        'dt': dt, 'dt_reference': float(dt_ref), 'dt_rel_diff': abs(dt - dt_ref) / dt_ref,
+                        'cells': n ** 3}
+        del got, d
+    parity['fp64']['bar'] = 1e-12
+    parity['mixed']['bar'] = 1e-8
+    return cpu, parity
 
 
 # ---------------------------------------------------------------- reference
@@ -203,8 +227,6 @@ def run_reference(args, rank, world):
     import _oracle as O
     n, order = args.n, args.order
     state = O.grid_ic(3, order, (n, n, n), kind=0, param=5.0, seed=args.seed, noise=1e-3)
-    dt = O.lib().orc_aderdg_grid_dt(3, order, 0, np.array([n, n, n], dtype=np.int32), np.full(3, 1.0 / n),
-                                    state, 0, 0.9)
     cores = os.cpu_count() or 1
     R = O.ref_lib(3)
     kind = 'reference' if R is not None else 'port'
@@ -212,27 +234,26 @@ def run_reference(args, rank, world):
     ncells = state.size // per
     dx = np.full(3, 1.0 / n)
 
-    def run(u, m):
+    # one step = one whole-grid step of the reference's kernels in the
+    # reference's order (stableTimeStepSize + global min, predictor + volume
+    # integral, Riemann per face, surface integral + update), all host cores;
+    # about 4 s per step on 16 cores for 81^3 N=4
+    u = state.copy()
+    nn = np.array([n, n, n], dtype=np.int32)
+
+    def run():
         if R is not None:
-            R.ref_sample_step(order, m, dx, u, dt, cores)
+            R.ref_grid_step(order, nn, dx, u, 0, 0.0, cores)
         else:
-            O.lib().orc_aderdg_sample_step(3, order, 0, m, dx, u, dt, cores)
-    # size one step for ~2.5 s of work so K+W steps end within minutes
-    m0 = min(ncells, 64 * cores)
-    u = state[:m0 * per].copy()
-    t0 = time.perf_counter()
-    run(u, m0)
-    rate = m0 / max(time.perf_counter() - t0, 1e-6)
-    m = int(min(ncells, max(m0, rate * 2.5)))
-    u = state[:m * per].copy()
+            O.lib().orc_aderdg_grid_step(3, order, 0, nn, dx, u, 0, 0.9, 0.0, None, cores)
     for _ in range(args.warmup):
-        run(u, m)
+        run()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        run(u, m)
+        run()
     t = time.perf_counter() - t0
-    value = m * args.steps / t
-    sample = '%d of %d cells per step (first cells of the %d^3 vortex state, its dt)' % (m, ncells, n)
+    value = ncells * args.steps / t
+    sample = 'whole %d^3 grid, every step (dt + predictor + volume integral + Riemann + surface integral + update)' % n
     line = {
         'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'cell-updates/s', 'n_gpus': world,
         'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
@@ -344,8 +365,7 @@ def main():
     import exahype_b200 as E
     E.lib().exa_set_device(local)
     import ctypes as C
-    fp64_peak = C.c_double()
-    E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))
+    fp64_peak = C.c_double(fp64_fma_peak())
     peaks, peak_src = measured_peaks()
 
     def barrier():
@@ -369,10 +389,11 @@ def main():
         other = measure(ctx, 'mixed', with_e2e=False)
         other['accuracy'] = mixed_accuracy(ctx, steps=min(50, args.warmup + args.steps))
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, kind, cores, sample, _ = cpu_sample(args.order, args.n, res['state'], res['dt'], budget_s=15.0)
-        cpu = {'value': v, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind, 'sample': sample}
+        cpu, parity = reference_step_check(ctx, res['state'])
+        if other is not None and parity is not None:
+            other['accuracy_vs_oracle'] = parity.pop('mixed')
 
     if rank == 0:
         ncells = res['ncells']
@@ -389,6 +410,7 @@ def main():
                 'bytes_per_cell_update': bytes_per_cell_update(3, args.order)},
             'flop_per_cell_update': res['flop_per_cell_update'],
             'cpu_baseline': cpu,
+            'parity_81': parity,
             'e2e': res.get('e2e'),
             'gpu_launches': res['launches'],
             'clocks': res['clocks'],
@@ -397,7 +419,8 @@ def main():
             line['mixed'] = {
                 'value': other['value'], 'unit': 'cell-updates/s', 'ms_per_step': other['ms_per_step'],
                 'speedup_vs_fp64': other['value'] / res['value'], 'roofline': other['roofline'],
-                'accuracy_vs_fp64': other['accuracy'], 'gpu_launches': other['launches'],
+                'accuracy_vs_fp64': other['accuracy'], 'accuracy_vs_oracle': other.get('accuracy_vs_oracle'),
+                'gpu_launches': other['launches'],
                 'clocks': other['clocks'],
                 'form': 'Picard deviations dq = q - luh and dF = F(q) - F(luh) in FP32 (FP32 accumulate); '
                         'luh, F(luh) and its derivative, the update, Riemann fluxes, faces and dt in FP64'}
@@ -668,8 +691,7 @@ def run_fv(args, rank, world, dist):
     local = int(os.environ.get('LOCAL_RANK', '0'))
     E.lib().exa_set_device(local)
     import ctypes as C
-    fp64_peak = C.c_double()
-    E._lib.call('exa_measure_fp64_peak', C.byref(fp64_peak))
+    fp64_peak = C.c_double(fp64_fma_peak())
     peaks, peak_src = measured_peaks()
     P = args.fv_patch
     out = {}

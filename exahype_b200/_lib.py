@@ -106,11 +106,9 @@ SIGNATURES = {
     'exa_timer_stop': (i32, [vp, vp]),
     'exa_timer_elapsed_ms': (i32, [vp, C.POINTER(C.c_float)]),
     'exa_launch_count': (u64, []),
+    'exa_dropin_workspace_doubles': (i32, [i32, C.POINTER(sz)]),
     'exa_tune_set': (i32, [i32, i32]),
     'exa_tune_get': (i32, [i32]),
-    'exa_measure_fp64_peak': (i32, [C.POINTER(f64)]),
-    'exa_measure_fp64_tensor_peak': (i32, [C.POINTER(f64)]),
-    'exa_measure_copy_bandwidth': (i32, [sz, C.POINTER(f64)]),
     'exa_diff_norms': (i32, [vp, vp, sz, C.POINTER(f64), vp]),
     'exa_aderdg_spaceTimePredictor': (i32, [C.POINTER(AderdgDesc), dptr, dptr, dpp, dpp, dptr, dptr,
                                             dptr, dptr, dptr, f64, dptr, ipt]),

@@ -300,10 +300,10 @@ class ADERDGGrid:
     def status(self):
         t, it, nc, nan = C.c_double(), C.c_uint64(), C.c_uint64(), C.c_int()
         st = lib().exa_aderdg_grid_status(self.h, C.byref(t), C.byref(it), C.byref(nc), C.byref(nan))
-        if st not in (_lib.EXA_OK, _lib.EXA_ENAN):
+        if st not in (_lib.EXA_OK, _lib.EXA_ENAN, _lib.EXA_ENONCONV):
             _lib.check(st, 'exa_aderdg_grid_status')
         return dict(time=t.value, picard_iters=int(it.value), nonconverged=int(nc.value),
-                    nan=bool(nan.value))
+                    nan=bool(nan.value), code=int(st))
 
     def destroy(self):
         if self.h:

@@ -543,6 +543,7 @@ exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time, uint64_t* 
   if (nonconverged) *nonconverged = h.stats[1];
   if (nan_flag) *nan_flag = h.nan_flag;
   if (h.nan_flag) return EXA_ENAN;
+  if (h.stats[1]) return EXA_ENONCONV;
   return EXA_OK;
 }
 

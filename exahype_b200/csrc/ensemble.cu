@@ -195,6 +195,12 @@ __global__ void __launch_bounds__(kEnsNT) k_ensemble_step(EnsArgs a) {
   for (int s = gtid; s < a.nsolves; s += gridDim.x * blockDim.x) {
     SolveDev& sv = a.solves[s];
     if (!sv.active) continue;
+    if (sv.nan_flag) {
+      // this step produced a non-finite state: the solve stops here (not
+      // counted as a step) and is reported failed; the others go on
+      sv.active = 0;
+      continue;
+    }
     sv.time += sv.dt;
     sv.steps_done += 1;
     if (sv.dt_policy == 2) {

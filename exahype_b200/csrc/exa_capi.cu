@@ -63,7 +63,7 @@ exa_status_t ensure_tables() {
   return EXA_OK;
 }
 
-static exa_status_t check_aderdg(const exa_aderdg_desc_t* d) {
+exa_status_t check_aderdg_desc(const exa_aderdg_desc_t* d) {
   if (!d) return set_error(EXA_EINVAL, "NULL descriptor");
   if (d->dim != 2 && d->dim != 3) return set_error(EXA_EINVAL, "dim must be 2 or 3");
   if (d->order < 2 || d->order > 5) return set_error(EXA_EINVAL, "order must be in 2..5");
@@ -75,6 +75,11 @@ static exa_status_t check_aderdg(const exa_aderdg_desc_t* d) {
     return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
   for (int i = 0; i < d->dim; i++)
     if (!(d->dx[i] > 0.0)) return set_error(EXA_EINVAL, "dx must be positive");
+  return EXA_OK;
+}
+
+static exa_status_t check_aderdg(const exa_aderdg_desc_t* d) {
+  if (exa_status_t s = check_aderdg_desc(d)) return s;
   return ensure_tables();
 }
 
@@ -103,6 +108,12 @@ static exa_status_t ws_get(size_t doubles, double** out, std::unique_lock<std::m
   }
   *out = w.buf;
   return EXA_OK;
+}
+
+static size_t ws_capacity(int dev) {
+  Workspace& w = g_ws[dev & 255];
+  std::lock_guard<std::mutex> lk(w.mu);
+  return w.cap;
 }
 
 }  // namespace exa
@@ -169,6 +180,13 @@ int exa_device_count(void) {
 }
 
 exa_status_t exa_set_device(int device) { return cuda_status(cudaSetDevice(device), "cudaSetDevice"); }
+
+exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles) {
+  if (!doubles) return set_error(EXA_EINVAL, "NULL doubles");
+  if (device < 0 || device > 255) return set_error(EXA_EINVAL, "device out of range");
+  *doubles = ws_capacity(device);
+  return EXA_OK;
+}
 
 exa_status_t exa_device_alloc(size_t bytes, void** ptr) {
   if (!ptr) return set_error(EXA_EINVAL, "NULL ptr");

@@ -26,6 +26,9 @@ void count_launch(uint64_t n = 1);
 // Makes sure the constant-memory tables of every translation unit are
 // uploaded on the current device.
 exa_status_t ensure_tables();
+// Descriptor checks of the per-cell ADER-DG drop-ins (dim, order, nvar,
+// npar, pde, dx), without the table upload.
+exa_status_t check_aderdg_desc(const exa_aderdg_desc_t* d);
 
 // Arguments of the fused predictor kernel (one struct so the launch
 // wrappers stay small).

@@ -3,8 +3,6 @@
 // exa_aderdg_spaceTimePredictor stages the cell through a device workspace
 // that the library allocates with cudaMalloc on first use (and re-allocates
 // when a larger order arrives).  Some callers cannot let that happen:
-//  * code that runs while a CUDA graph is being captured: cudaMalloc is not
-//    permitted inside a capture;
 //  * many host threads calling the per-cell kernels concurrently, as
 //    ExaHyPE's TBB workers do (mappings/Prediction.cpp:152): cudaMalloc and
 //    cudaFree take a device-wide lock and cudaFree synchronises the device,
@@ -13,7 +11,8 @@
 //    allocator, where a late cudaMalloc fails with out-of-memory.
 // exa_aderdg_spaceTimePredictor_noalloc therefore stages through a
 // file-scope __device__ array of fixed size that every GPU holds from the
-// moment the library is loaded until the process exits.
+// moment the library is loaded until the process exits.  Its copies are
+// synchronous on the default stream, like the drop-in's.
 #include <mutex>
 
 #include "exa_device.cuh"
@@ -44,12 +43,10 @@ exa_status_t exa_aderdg_spaceTimePredictor_noalloc(
     double dt, double* pointForceSources, int* picardIterations) {
   (void)tempStateSizedVectors;
   (void)pointForceSources;
-  if (!desc) return set_error(EXA_EINVAL, "NULL descriptor");
+  // the drop-in's own descriptor checks (dim, order, nvar, npar, pde, dx)
+  if (exa_status_t s = check_aderdg_desc(desc)) return s;
   if (!lQhbnd || !lFhbnd || !luh || !tempUnknowns || !tempFluxUnknowns)
     return set_error(EXA_EINVAL, "NULL buffer");
-  if ((desc->dim != 2 && desc->dim != 3) || desc->order < 2 || desc->order > 5 || desc->nvar != kV ||
-      desc->npar < 0 || desc->npar > 1)
-    return set_error(EXA_EINVAL, "unsupported descriptor (dim 2|3, order 2..5, nvar 5, npar 0|1)");
   exa_aderdg_desc_t d = *desc;
   if (dx)
     for (int i = 0; i < d.dim; i++) d.dx[i] = dx[i];

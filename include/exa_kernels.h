@@ -100,6 +100,10 @@ exa_status_t exa_timer_stop(void* timer, void* stream);
 exa_status_t exa_timer_elapsed_ms(void* timer, float* ms);
 /* number of kernels this library has launched in this process */
 uint64_t exa_launch_count(void);
+/* Diagnostic: capacity in doubles of the device workspace that the per-cell
+ * drop-ins below allocate on first use on `device` (0 = not allocated).  No
+ * counterpart in the reference. */
+exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles);
 /* Tuning knobs chosen by the autotuner (exahype_b200/autotune.py) or the
  * user; process-wide.  Keys: 0 = register budget of the 3D order-4 mixed
  * predictor as minimum resident CTAs per SM (1: unconstrained; 3: 168
@@ -111,18 +115,10 @@ uint64_t exa_launch_count(void);
  * returns -1 for keys never set. */
 exa_status_t exa_tune_set(int key, int value);
 int exa_tune_get(int key);
-/* FP64 FMA throughput of the current device in TFLOP/s, measured with a
- * dependent-chain DFMA kernel over all SMs (a roofline denominator; the
- * device's peak files carry no FP64 figure) */
-exa_status_t exa_measure_fp64_peak(double* tflops);
-/* FP64 tensor-core (mma.sync m8n8k4 f64) throughput of this GPU, TFLOP/s */
-exa_status_t exa_measure_fp64_tensor_peak(double* tflops);
 /* Error norms of device array a against reference b (n doubles): out[0]
  * relative L2 ||a-b||/||b||, out[1] relative Linf max|a-b|/max|b|,
  * out[2] ||a-b||, out[3] max|a-b|.  Synchronous on stream. */
 exa_status_t exa_diff_norms(const double* a, const double* b, size_t n, double* out, void* stream);
-/* DRAM copy bandwidth (read + write bytes / time) in GB/s over `bytes` */
-exa_status_t exa_measure_copy_bandwidth(size_t bytes, double* gbs);
 
 /* ---------------------------------- ADER-DG: per-cell drop-ins (host) --
  * Same argument lists and semantics as the generated solver methods; the
@@ -147,20 +143,21 @@ exa_status_t exa_aderdg_spaceTimePredictor(
     double dt, double* pointForceSources, int* picardIterations);
 
 /* Allocation-free variant of exa_aderdg_spaceTimePredictor (same arguments,
- * same results).  It has no counterpart in the reference: it exists for
- * callers that must not trigger a device allocation -- code running while a
- * CUDA graph is captured (cudaMalloc is not permitted there), many host
- * threads calling per-cell kernels at once (cudaMalloc/cudaFree take a
- * device-wide lock and cudaFree synchronises the device), or processes whose
- * device memory is already handed out by a pool allocator.  The cell is
- * staged through a file-scope device array of 65536 doubles (512 KiB) that
- * every GPU holds from library load to process exit; every supported cell
- * (order 2..5, 2D/3D, nPar <= 1) fits, larger requests get EXA_EINVAL.
- * The first call on a device performs a one-time set-up (looks up the
- * array's device address, uploads the operator tables); make that first call
- * before any stream capture.  All calls on a device share the one array and
- * keep the last call's contents; calls of this process are serialised by a
- * lock, any other overlap on the GPU races.  Synchronous, like the drop-in. */
+ * same checks, same results).  It has no counterpart in the reference: it
+ * exists for callers that must not trigger a device allocation -- many host
+ * threads calling per-cell kernels at once, as the reference's TBB workers
+ * do (cudaMalloc/cudaFree take a device-wide lock and cudaFree synchronises
+ * the device, stalling every other worker), or processes whose device memory
+ * is already handed out by a pool allocator (a late cudaMalloc fails there).
+ * The cell is staged through a file-scope device array of 65536 doubles
+ * (512 KiB) that every GPU holds from library load to process exit; every
+ * supported cell (order 2..5, 2D/3D, nPar <= 1) fits, larger requests get
+ * EXA_EINVAL.  The first call on a device performs a one-time set-up (looks
+ * up the array's device address, uploads the operator tables); make that
+ * first call before any stream capture.  All calls on a device share the one
+ * array and keep the last call's contents; calls of this process are
+ * serialised by a lock, any other overlap on the GPU races.  Like the
+ * drop-in it copies synchronously on the default stream. */
 exa_status_t exa_aderdg_spaceTimePredictor_noalloc(
     const exa_aderdg_desc_t* desc, double* lQhbnd, double* lFhbnd,
     double** tempSpaceTimeUnknowns, double** tempSpaceTimeFluxUnknowns,
@@ -289,8 +286,8 @@ exa_status_t exa_aderdg_grid_init(exa_aderdg_grid* g, int kind, double param,
 exa_status_t exa_aderdg_grid_set_state(exa_aderdg_grid* g, const double* host_luh);
 exa_status_t exa_aderdg_grid_get_state(exa_aderdg_grid* g, double* host_luh);
 /* advance nsteps; dt_host (nullable) receives nsteps dt values (forces a
- * device->host read at the end).  Returns EXA_ENAN / EXA_ENONCONV
- * conditions through exa_aderdg_grid_status. */
+ * device->host read at the end).  NaN and Picard non-convergence are
+ * reported through exa_aderdg_grid_status (EXA_ENAN / EXA_ENONCONV). */
 exa_status_t exa_aderdg_grid_step(exa_aderdg_grid* g, int nsteps, double* dt_host);
 /* capture one step pair in a CUDA graph and replay it for later steps */
 exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable);
@@ -355,7 +352,13 @@ exa_status_t exa_aderdg_grid_profile(exa_aderdg_grid* g, int enable);
 exa_status_t exa_aderdg_grid_phase_times(exa_aderdg_grid* g, double* ms_predictor,
                                          double* ms_corrector, uint64_t* steps);
 exa_status_t exa_aderdg_grid_device_state(exa_aderdg_grid* g, double** luh_dev);
-/* time, accumulated Picard iterations, non-converged cell count, NaN flag */
+/* time, accumulated Picard iterations, non-converged cell count, NaN flag.
+ * Returns EXA_ENAN once a step produced a non-finite state (the reference's
+ * validateNoNansInADERDGSolver, ADERDGSolver.cpp:1746), else EXA_ENONCONV
+ * once any cell's Picard loop stopped at 2(N+1) iterations without meeting
+ * its tolerance (the reference only warns, spaceTimePredictorNonlinear.cpph:
+ * 308-315: the step's result is kept), else EXA_OK; the outputs are written
+ * in every case. */
 exa_status_t exa_aderdg_grid_status(exa_aderdg_grid* g, double* time,
                                     uint64_t* picard_iters_sum,
                                     uint64_t* nonconverged, int* nan_flag);

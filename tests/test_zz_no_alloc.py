@@ -1,12 +1,16 @@
 """The allocation-free predictor entry point, called through the C ABI,
 returns what the ordinary drop-in returns, on two calls in a row.
 
-It exists for callers that must not trigger a device allocation (code that
-runs inside a CUDA graph capture, many host threads calling per-cell
-kernels at once, or a device whose memory a pool allocator already owns);
-it stages the cell through a fixed device array instead of a workspace the
-library allocates.  This file is collected last on purpose."""
+It exists for callers that must not trigger a device allocation (many host
+threads calling per-cell kernels at once, where cudaMalloc/cudaFree would
+lock and synchronise the device, or a device whose memory a pool allocator
+already owns); it stages the cell through a fixed device array instead of a
+workspace the library allocates.  This file is collected last on purpose."""
 import ctypes as C
+import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -81,3 +85,79 @@ def test_noalloc_reproduces_golden(golden3d):
             return dict(lQi=r['lQi'], lFi=r['lFi'], lQhi=r['lQhi'], lFhi=r['lFhi'], lQhbnd=r['qb'],
                         lFhbnd=r['fb'])
     _cases.stp_3d(Impl(), golden3d)
+
+
+def _status(fn, desc, luh, dx, dt, dim, order, npar):
+    try:
+        _run(fn, desc, luh, dx, dt, dim, order, npar)
+    except _lib.ExaError as e:
+        return e.status
+    return _lib.EXA_OK
+
+
+def test_noalloc_rejects_what_the_dropin_rejects():
+    """Same descriptor checks as the drop-in: an unknown pde, planar Euler in
+    3D, nPar = 1 at an order other than 3, a bad order or a non-positive dx
+    all return EXA_EINVAL from both entry points."""
+    luh = np.ones(4 ** 3 * 6)
+    bad = []
+    d = E.make_desc(3, 3, [0.1] * 3)
+    d.pde = 7
+    bad.append((d, 3, 3, 0))
+    bad.append((E.make_desc(3, 3, [0.1] * 3, pde=E.PDE_EULER_PLANAR), 3, 3, 0))
+    bad.append((E.make_desc(3, 4, [0.1] * 3, npar=1), 3, 4, 1))
+    d = E.make_desc(3, 3, [0.1] * 3)
+    d.order = 6
+    bad.append((d, 3, 6, 0))
+    for desc, dim, order, npar in bad:
+        B = order + 1
+        u = np.ones(B ** dim * (5 + npar))
+        for fn in ('exa_aderdg_spaceTimePredictor', 'exa_aderdg_spaceTimePredictor_noalloc'):
+            assert _status(fn, desc, u, [0.1] * 3, 1e-4, dim, order, npar) == _lib.EXA_EINVAL, (fn, order)
+    desc = E.make_desc(3, 3, [0.1, -0.1, 0.1])
+    for fn in ('exa_aderdg_spaceTimePredictor', 'exa_aderdg_spaceTimePredictor_noalloc'):
+        assert _status(fn, desc, luh[:4 ** 3 * 5], [0.1, -0.1, 0.1], 1e-4, 3, 3, 0) == _lib.EXA_EINVAL
+
+
+_FRESH = textwrap.dedent('''
+    import ctypes as C, sys
+    import numpy as np
+    sys.path.insert(0, sys.argv[1])
+    import exahype_b200 as E
+    from exahype_b200 import _lib
+    L = E.lib()
+    _lib.check(L.exa_set_device(0), 'set device')
+    cap = C.c_size_t(123)
+    dp = C.POINTER(C.c_double)
+    def call(fn, order):
+        B = order + 1
+        nn = B ** 3
+        desc = E.make_desc(3, order, [0.1] * 3)
+        luh = np.zeros(nn * 5)
+        luh[0::5] = 1.0
+        luh[4::5] = 2.5
+        o = [np.zeros(n) for n in (6 * B * B * 5, 6 * B * B * 5, nn * 5, nn * 4 * 5)]
+        dx = np.full(3, 0.1)
+        _lib.check(getattr(L, fn)(C.byref(desc), *[a.ctypes.data_as(dp) for a in o[:2]], None, None,
+                                  *[a.ctypes.data_as(dp) for a in o[2:]], None, luh.ctypes.data_as(dp),
+                                  dx.ctypes.data_as(dp), 1e-4, None, None), fn)
+    for order in (2, 5, 3):
+        call('exa_aderdg_spaceTimePredictor_noalloc', order)
+        _lib.check(L.exa_dropin_workspace_doubles(0, C.byref(cap)), 'query')
+        assert cap.value == 0, cap.value
+    call('exa_aderdg_spaceTimePredictor', 3)
+    _lib.check(L.exa_dropin_workspace_doubles(0, C.byref(cap)), 'query')
+    assert cap.value > 0, cap.value
+    print('fresh ok', cap.value)
+''')
+
+
+def test_noalloc_allocates_nothing_in_a_fresh_process():
+    """In a process that never called the drop-in, calls of the allocation-
+    free entry point (orders 2, 5, 3) leave the drop-in workspace
+    unallocated; the drop-in's first call then allocates it (the query
+    sees an allocation when there is one)."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, '-c', _FRESH, root], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert 'fresh ok' in r.stdout
