@@ -226,8 +226,13 @@ struct DG {
       }
       dtv = m;
     }
-    std::vector<double> lduh(nc * NN * V), qb(nc * 2 * DIMENSIONS * NF * D),
-        fb(nc * 2 * DIMENSIONS * NF * V);
+    // the solver's per-cell arrays (lduh, lQhbnd, lFhbnd) persist between
+    // steps as the reference's cell descriptions do; every kernel writes
+    // its outputs in full (volumeIntegral and the extrapolation zero them)
+    static std::vector<double> lduh, qb, fb;
+    lduh.resize(nc * NN * V);
+    qb.resize(nc * 2 * DIMENSIONS * NF * D);
+    fb.resize(nc * 2 * DIMENSIONS * NF * V);
 #pragma omp parallel
     {
       Temps t;

@@ -111,7 +111,7 @@ def test_ensemble_nan_solve_fails_alone(graph):
     ptr = bad.device_state_ptr(sb[1]).value
     nan = np.array([np.nan])
     _lib.call('exa_memcpy_h2d', C.c_void_p(ptr + 8 * 123), nan.ctypes.data, 8, None)
-    E.synchronize()
+    E.device.synchronize()
     for _ in range(5):
         for ens in (clean, bad):
             ens.step(1)

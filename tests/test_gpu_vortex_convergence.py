@@ -11,8 +11,12 @@ cells rolled.  The GPU grid steps with a fixed dt (0.9 of the stable dt on
 the initial state, t_end divided into whole steps) so time and space are
 refined together; ADER-DG is of order N+1 in both, and the nodal L2 error
 must fall faster than h^(N+0.5).  3D: the vortex extruded along z on a grid
-two cells deep.  The coarsest 2D errors are also checked against the
-oracle's grid step on the same state and dt.
+two cells deep.  N=4 stops at 32^2: at 64^2 its error (~2e-7 after ~770
+steps) reaches the level of the Picard stopping rule (the iteration stops
+once the squared update falls below 1e-14, as the reference's does), so the
+rate there measures that tolerance, not the discretisation.  The coarsest 2D
+errors are also checked against the oracle's grid step on the same state and
+dt.
 """
 import numpy as np
 import pytest
@@ -84,7 +88,7 @@ def gpu_error(dim, order, n):
     return float(np.sqrt(np.mean(e ** 2))), u
 
 
-@pytest.mark.parametrize('dim,order,sizes', [(2, 2, (16, 32, 64)), (2, 3, (16, 32, 64)), (2, 4, (16, 32, 64)),
+@pytest.mark.parametrize('dim,order,sizes', [(2, 2, (16, 32, 64)), (2, 3, (16, 32, 64)), (2, 4, (16, 32)),
                                               (3, 3, (16, 32)), (3, 4, (16, 32))])
 def test_isentropic_vortex_convergence_order(dim, order, sizes):
     errs = [gpu_error(dim, order, n)[0] for n in sizes]
