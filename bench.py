@@ -300,6 +300,9 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-mixed', action='store_true')
+    ap.add_argument('--mixed-variant', type=int, default=0,
+                    help='contraction of the mixed predictor (tuning key 2): 0 default, 1 node-gather, '
+                         '2 line-owner FP32, 3 tensor cores (3D N=4)')
     ap.add_argument('--workload', default='grid3d',
                     choices=['grid3d', 'ensemble', 'serving', 'fv', 'amr', 'limiter'],
                     help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
@@ -380,6 +383,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX, group=cpu_group)
         return float(t.item())
 
+    if args.mixed_variant:
+        E._lib.call('exa_tune_set', 2, args.mixed_variant)
     ctx = dict(E=E, args=args, rank=rank, world=world, local=local, barrier=barrier, dist=dist,
                max_over_ranks=max_over_ranks, fp64_peak=fp64_peak.value)
     primary = 'mixed' if args.precision == 'mixed' else 'fp64'

@@ -22,6 +22,7 @@
 #include "exa_device.cuh"
 #include "aderdg_predictor_mixed_body.cuh"
 #include "aderdg_predictor_lines_body.cuh"
+#include "aderdg_predictor_tc_body.cuh"
 
 namespace exa {
 
@@ -77,6 +78,31 @@ static exa_status_t launch_lines_t(const PredArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_predictor_mixed_lines launch");
 }
 
+// tensor-core variant, 3D order 4 (aderdg_predictor_tc_body.cuh): 128
+// threads, 3 CTAs per SM
+template <bool PLANAR>
+__global__ void __launch_bounds__(TcShape::NT, 3) k_predictor_mixed_tc(PredArgs a) {
+  extern __shared__ double smem[];
+  predictor_mixed_tc_block<PLANAR>(a, blockIdx.x, smem);
+}
+
+static exa_status_t launch_predictor_mixed_tc(const PredArgs& a, cudaStream_t st) {
+  auto kern = k_predictor_mixed_tc<false>;
+  const size_t smem = sizeof(double) * TcShape::SM_DOUBLES;
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "mixed predictor (tensor cores) attribute");
+    attr_done[dev & 63] = true;
+  }
+  if (a.ncells <= 0) return EXA_OK;
+  kern<<<(unsigned)a.ncells, TcShape::NT, smem, st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_predictor_mixed_tc launch");
+}
+
 // line-owner variant (aderdg_predictor_lines_body.cuh)
 static exa_status_t launch_predictor_mixed_lines(const exa_aderdg_desc_t& d, const PredArgs& a,
                                                  cudaStream_t st) {
@@ -109,7 +135,9 @@ exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& 
   // default: line-owner for orders >= 4 (measured faster in 2D and 3D),
   // node-gather for orders 2-3
   const int variant = tune_get(kTuneMixedVariant, 0);
-  if (d.npar == 0 && (variant == 2 || (variant == 0 && d.order >= 4)))
+  if (d.npar == 0 && variant == 3 && d.dim == 3 && d.order == 4 && d.pde == EXA_PDE_EULER)
+    return launch_predictor_mixed_tc(a, st);
+  if (d.npar == 0 && (variant >= 2 || (variant == 0 && d.order >= 4)))
     return launch_predictor_mixed_lines(d, a, st);
   if (d.npar != 0) return set_error(EXA_EINVAL, "mixed precision: npar must be 0");
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;

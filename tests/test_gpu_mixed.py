@@ -20,9 +20,10 @@ pytestmark = pytest.mark.gpu
     (2, 5, (9, 9), 0, 20),
     (2, 2, (20, 20), 1, 30),
 ])
-@pytest.mark.parametrize('variant', [1, 2])
+@pytest.mark.parametrize('variant', [1, 2, 3])
 def test_mixed_vs_fp64_per_step(dim, order, n, kind, steps, variant):
-    # variant (tuning key 2): 1 = node-gather contraction, 2 = line-owner
+    # variant (tuning key 2): 1 = node-gather contraction, 2 = line-owner,
+    # 3 = tensor-core line derivatives (3D order 4; line-owner elsewhere)
     E._lib.call('exa_tune_set', 2, variant)
     try:
         _mixed_vs_fp64(dim, order, n, kind, steps)
