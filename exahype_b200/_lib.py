@@ -107,6 +107,11 @@ SIGNATURES = {
     'exa_timer_elapsed_ms': (i32, [vp, C.POINTER(C.c_float)]),
     'exa_launch_count': (u64, []),
     'exa_dropin_workspace_doubles': (i32, [i32, C.POINTER(sz)]),
+    'exa_nccl_unique_id': (i32, [vp]),
+    'exa_slab_comm_create': (i32, [vp, i32, i32, C.POINTER(vp)]),
+    'exa_slab_comm_destroy': (i32, [vp]),
+    'exa_aderdg_grid_slab_prime': (i32, [vp, vp, f64]),
+    'exa_aderdg_grid_slab_step': (i32, [vp, vp, i32, f64]),
     'exa_tune_set': (i32, [i32, i32]),
     'exa_tune_get': (i32, [i32]),
     'exa_diff_norms': (i32, [vp, vp, sz, C.POINTER(f64), vp]),
@@ -211,6 +216,8 @@ SIGNATURES = {
     'exa_server_result_size': (sz, [vp, u64]),
     'exa_server_result': (i32, [vp, u64, vp, C.POINTER(f64), C.POINTER(C.c_longlong)]),
     'exa_server_info': (i32, [vp, C.POINTER(i32), C.POINTER(C.c_long), C.POINTER(sz)]),
+    'exa_server_run': (i32, [vp, vp, vp, i32, f64, vp, C.POINTER(u64)]),
+    'exa_server_device_state': (i32, [vp, u64, C.POINTER(vp)]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_stable_dt': (i32, [C.POINTER(FVDesc), i64, vp, vp, vp]),

@@ -730,6 +730,14 @@ exa_status_t exa_aderdg_grid_dt_slot(exa_aderdg_grid* g, uint64_t** slot) {
   return EXA_OK;
 }
 
+}  // extern "C"
+
+namespace exa {
+bool grid_fixed_dt(const exa_aderdg_grid* g) { return g->cfg.dt_policy == 2; }
+}  // namespace exa
+
+extern "C" {
+
 exa_status_t exa_aderdg_grid_phase(exa_aderdg_grid* g, int phase) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
   switch (phase) {

@@ -26,6 +26,9 @@ void count_launch(uint64_t n = 1);
 // Makes sure the constant-memory tables of every translation unit are
 // uploaded on the current device.
 exa_status_t ensure_tables();
+// Whether a grid steps with a fixed dt (no dt reduction between slabs).
+bool grid_fixed_dt(const exa_aderdg_grid* g);
+
 // Descriptor checks of the per-cell ADER-DG drop-ins (dim, order, nvar,
 // npar, pde, dx), without the table upload.
 exa_status_t check_aderdg_desc(const exa_aderdg_desc_t* d);
@@ -182,5 +185,23 @@ const void* host_dg_tables(size_t* bytes);
 const void* host_dg_tables_f(size_t* bytes);  // FP32 copies (DGConstF)
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// One live periodic FV patch of the serving batch (fv.cu): the state
+// alternates between buf[0] and buf[1]; slots: [0] dt of the current step,
+// [1] simulated time, [2] next dt (atomic min), [3] index of the buffer that
+// holds the state.  Patches of one launch are listed by their first tile
+// (tile0, ascending); tiles_x tiles per tile row.
+struct FVServePatch {
+  double* buf[2];
+  unsigned long long* slots;
+  int P, g, tiles_x, tile0;
+  double hx, hy;
+};
+// tiles of a patch of `patch` cells per side for the scheme's tile kernel
+int fv_serve_tiles(int scheme, int patch, int* tiles_x);
+// one step of every listed patch (device table of np entries, ntiles tiles
+// in all) and the per-patch commit, on stream st
+exa_status_t fv_serve_step_async(int scheme, bool planar, const FVServePatch* table, int np, int ntiles,
+                                 cudaStream_t st);
 
 }  // namespace exa

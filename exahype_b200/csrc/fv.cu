@@ -102,8 +102,10 @@ __device__ __forceinline__ double fv_face_flux(const double* qL, const double* q
 
 // five 256-thread CTAs (42 KB each) per SM: 48 registers and the largest
 // shared-memory carveout
+// One FV_TX x FV_TY tile (tile column bx, row by) of patch `patch` of a.luh
+// / a.out (the body of k_fv_godunov; the serving batch calls it per entry).
 template <bool PLANAR, bool FUSED>
-__global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
+__device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by, long patch) {
   constexpr int V = kV, C = kV + 1;
   constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
   __shared__ double su[LY * LX * V];
@@ -111,10 +113,9 @@ __global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
   __shared__ double scy[LY * FV_TX * C];  // y: all rows, staged columns 1..TX
   __shared__ double sred[FV_NT / 32];
   const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
-  const long patch = blockIdx.z;
   const double* luh = a.luh + patch * (long)S * S * D;
   double* out = a.out + patch * (long)S * S * D;
-  const int k0 = pb + blockIdx.x * FV_TX, j0 = pb + blockIdx.y * FV_TY;
+  const int k0 = pb + bx * FV_TX, j0 = pb + by * FV_TY;
   const int tid = threadIdx.x;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
@@ -216,6 +217,11 @@ __global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
       atomic_min_pos_double(&a.max_dt[patch], m);
     }
   }
+}
+
+template <bool PLANAR, bool FUSED>
+__global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
+  fv_godunov_tile<PLANAR, FUSED>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // -------------------------------------------------------- MUSCL-Hancock
@@ -478,19 +484,21 @@ __global__ void __launch_bounds__(FVP_NT) k_fv_godunov_periodic(FVArgs a) {
   if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
 }
 
+// One FVP_TX x FVP_TY tile (tile column bx, row by) of one periodic patch
+// (the body of k_fv_muscl_periodic; the serving batch calls it per entry);
+// sm: kMusclPeriodicSmem bytes of dynamic shared memory
 template <bool PLANAR>
-__global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
+__device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, int by, double* sm) {
   constexpr int V = kV;
   constexpr int LX = FVP_TX + 4, LY = FVP_TY + 4;   // state: cells j0-2..j0+TY+1, k0-2..k0+TX+1
   constexpr int RX = FVP_TX + 2, RY = FVP_TY + 2;   // ring: j0-1..j0+TY, k0-1..k0+TX
-  extern __shared__ double sm[];
   double* su = sm;                 // LY*LX*V
   double* wLx = su + LY * LX * V;  // RY*RX*V each
   double* wRx = wLx + RY * RX * V;
   double* wLy = wRx + RY * RX * V;
   double* wRy = wLy + RY * RX * V;
   const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
-  const int k0 = pb + blockIdx.x * FVP_TX, j0 = pb + blockIdx.y * FVP_TY;
+  const int k0 = pb + bx * FVP_TX, j0 = pb + by * FVP_TY;
   const int tid = threadIdx.x;
   const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
   // reciprocal cell sizes: multiplications instead of the reference's
@@ -583,6 +591,12 @@ __global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
   if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
 }
 
+template <bool PLANAR>
+__global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
+  extern __shared__ double sm[];
+  fv_muscl_periodic_tile<PLANAR>(a, blockIdx.x, blockIdx.y, sm);
+}
+
 constexpr size_t kMusclPeriodicSmem =
     sizeof(double) * ((FVP_TY + 4) * (FVP_TX + 4) * kV + 4 * (FVP_TY + 2) * (FVP_TX + 2) * kV);
 
@@ -663,6 +677,104 @@ __global__ void k_fv_commit(unsigned long long* s) {
   *time += __longlong_as_double((long long)s[0]);
   s[0] = s[2];
   s[2] = 0x7FF0000000000000ULL;
+}
+
+// ----------------------------------------------------- serving batch
+// All live periodic patches of one scheme advanced by one launch: CTA t
+// takes global tile t, finds its patch by binary search over the patches'
+// first tiles, and runs the same tile body as the single-patch kernels.
+__device__ __forceinline__ int fv_serve_find(const FVServePatch* pt, int np, int tile) {
+  int lo = 0, hi = np - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pt[mid].tile0 <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ FVArgs fv_serve_args(const FVServePatch& p) {
+  FVArgs a{};
+  a.P = p.P;
+  a.g = p.g;
+  a.S = p.P + 2 * p.g;
+  a.npar = 0;
+  a.hx = p.hx;
+  a.hy = p.hy;
+  const int par = (int)(p.slots[3] & 1ULL);
+  a.luh = p.buf[par];
+  a.out = p.buf[par ^ 1];
+  a.dt_dev = (const double*)p.slots;
+  a.next_dt = p.slots + 2;
+  return a;
+}
+
+template <bool PLANAR>
+__global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_serve(const FVServePatch* __restrict__ pt, int np) {
+  extern __shared__ double sm[];
+  const FVServePatch& p = pt[fv_serve_find(pt, np, blockIdx.x)];
+  const FVArgs a = fv_serve_args(p);
+  const int t = blockIdx.x - p.tile0;
+  fv_muscl_periodic_tile<PLANAR>(a, t % p.tiles_x, t / p.tiles_x, sm);
+}
+
+template <bool PLANAR>
+__global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov_serve(const FVServePatch* __restrict__ pt, int np) {
+  const FVServePatch& p = pt[fv_serve_find(pt, np, blockIdx.x)];
+  const FVArgs a = fv_serve_args(p);
+  const int t = blockIdx.x - p.tile0;
+  fv_godunov_tile<PLANAR, true>(a, t % p.tiles_x, t / p.tiles_x, 0);
+}
+
+// per patch: time += dt, dt = next dt, next dt = +inf, state buffer flipped
+__global__ void k_fv_serve_commit(const FVServePatch* __restrict__ pt, int np) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  unsigned long long* s = pt[i].slots;
+  double* time = (double*)(s + 1);
+  *time += __longlong_as_double((long long)s[0]);
+  s[0] = s[2];
+  s[2] = 0x7FF0000000000000ULL;
+  s[3] ^= 1ULL;
+}
+
+int fv_serve_tiles(int scheme, int patch, int* tiles_x) {
+  const int tx = scheme == 0 ? FV_TX : FVP_TX, ty = scheme == 0 ? FV_TY : FVP_TY;
+  const int nx = (patch + tx - 1) / tx, ny = (patch + ty - 1) / ty;
+  if (tiles_x) *tiles_x = nx;
+  return nx * ny;
+}
+
+exa_status_t fv_serve_step_async(int scheme, bool planar, const FVServePatch* table, int np, int ntiles,
+                                 cudaStream_t st) {
+  if (np <= 0) return EXA_OK;
+  if (scheme == 0) {
+    static bool gattr[2] = {false, false};
+    if (!gattr[planar]) {
+      cudaError_t e = cudaFuncSetAttribute(planar ? k_fv_godunov_serve<true> : k_fv_godunov_serve<false>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return cuda_status(e, "godunov serve attribute");
+      gattr[planar] = true;
+    }
+    if (planar) k_fv_godunov_serve<true><<<ntiles, FV_NT, 0, st>>>(table, np);
+    else k_fv_godunov_serve<false><<<ntiles, FV_NT, 0, st>>>(table, np);
+  } else {
+    static bool attr[2] = {false, false};
+    if (!attr[planar]) {
+      auto kern = planar ? k_fv_muscl_serve<true> : k_fv_muscl_serve<false>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return cuda_status(e, "muscl serve attribute");
+      attr[planar] = true;
+    }
+    if (planar) k_fv_muscl_serve<true><<<ntiles, FVP_NT, kMusclPeriodicSmem, st>>>(table, np);
+    else k_fv_muscl_serve<false><<<ntiles, FVP_NT, kMusclPeriodicSmem, st>>>(table, np);
+  }
+  k_fv_serve_commit<<<(np + 127) / 128, 128, 0, st>>>(table, np);
+  count_launch(2);
+  return cuda_status(cudaGetLastError(), "fv serve step");
 }
 
 __device__ __forceinline__ double fv_noise_u01(unsigned long long seed, unsigned long long idx) {

@@ -8,13 +8,19 @@
 // is collected.  Every tick advances every active request by one step:
 //   * all ADER-DG requests together in the ensemble's single persistent
 //     launch (one launch regardless of how many requests are active);
-//   * each FV request as a device-resident patch step on a second stream,
-//     so FV work overlaps the ADER-DG launch.
+//   * all FV requests of one scheme together in one batched patch launch on
+//     a second stream (a device table of the live patches; each CTA finds
+//     its patch from its tile index), so FV work overlaps the ADER-DG
+//     launch and costs two launches per tick however many patches are
+//     live.
 // A request that arrives while others run joins at the next tick; its
 // arithmetic is independent of its neighbours (per-request dt and state),
 // so its result is the same alone or in any mix.
 #include <algorithm>
+#include <chrono>
+#include <deque>
 #include <map>
+#include <thread>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -33,7 +39,8 @@ struct Req {
   exa_fv_desc_t fv{};
   double* luh = nullptr;
   double* luh_new = nullptr;
-  unsigned long long* dt_slot = nullptr;  // scalars: [0] dt bits, [1] time, [2] next dt bits
+  unsigned long long* dt_slot = nullptr;  // scalars: [0] dt bits, [1] time, [2] next dt bits, [3] buffer
+  int par = 0;                            // buffer holding the state: 0 luh, 1 luh_new
   size_t off = 0, bytes = 0;
   long long steps_left = 0;
   long long steps_done = 0;
@@ -48,9 +55,19 @@ size_t fv_bytes(const exa_request_t* r) {
 }
 }  // namespace
 
+// the live FV patches of one (scheme, planar) group as a device table
+struct FVGroup {
+  std::vector<FVServePatch> host;
+  FVServePatch* dev = nullptr;
+  int cap = 0;
+  int ntiles = 0;
+};
+
 struct exa_server {
   exa_ensemble* ens = nullptr;
   cudaStream_t fv_st = nullptr;
+  FVGroup groups[4];  // scheme * 2 + planar
+  bool fv_dirty = true;
   int precision = 0;
   int max_requests = 0;
   uint64_t next_id = 1;
@@ -103,6 +120,7 @@ exa_status_t exa_server_destroy(exa_server* s) {
     cudaStreamDestroy(s->fv_st);
   }
   if (s->ens) exa_ensemble_destroy(s->ens);
+  for (FVGroup& gr : s->groups) cudaFree(gr.dev);
   delete s;
   return EXA_OK;
 }
@@ -135,7 +153,7 @@ exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* 
     q.luh = (double*)p;
     q.luh_new = (double*)(p + state);
     q.dt_slot = (unsigned long long*)(p + 2 * state);
-    cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 24, s->fv_st);
+    cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 32, s->fv_st);
     exa_status_t st = e == cudaSuccess ? launch_fv_ic(q.fv, q.luh, r->dg.ic_param, r->dg.seed, r->dg.noise, s->fv_st)
                                        : cuda_status(e, "fv scalars");
     if (!st) st = fv_patch_prime_async(q.fv, q.luh, q.dt_slot, s->fv_st);
@@ -149,8 +167,56 @@ exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* 
   s->next_id++;
   *id = q.id;
   s->live[q.id] = q;
+  if (r->kind == EXA_REQ_FV) s->fv_dirty = true;
   return EXA_OK;
 }
+
+namespace {
+// rebuilds the device tables of the live FV patches (after admissions and
+// completions); stream-ordered after the previous tick's launches
+exa_status_t rebuild_fv_groups(exa_server* s) {
+  for (FVGroup& gr : s->groups) {
+    gr.host.clear();
+    gr.ntiles = 0;
+  }
+  for (auto& kv : s->live) {
+    Req& q = kv.second;
+    if (q.done || q.r.kind != EXA_REQ_FV) continue;
+    FVGroup& gr = s->groups[q.r.fv_scheme * 2 + (q.fv.pde == EXA_PDE_EULER_PLANAR ? 1 : 0)];
+    FVServePatch p{};
+    p.buf[0] = q.luh;
+    p.buf[1] = q.luh_new;
+    p.slots = q.dt_slot;
+    p.P = q.fv.patch;
+    p.g = q.fv.ghost;
+    p.hx = q.fv.dx[0] / q.fv.patch;
+    p.hy = q.fv.dx[1] / q.fv.patch;
+    p.tile0 = gr.ntiles;
+    gr.ntiles += fv_serve_tiles(q.r.fv_scheme, q.fv.patch, &p.tiles_x);
+    gr.host.push_back(p);
+  }
+  for (FVGroup& gr : s->groups) {
+    const int np = (int)gr.host.size();
+    if (np == 0) continue;
+    if (np > gr.cap) {
+      // the old table may still be read by the last tick's launch
+      cudaError_t e = cudaStreamSynchronize(s->fv_st);
+      if (e == cudaSuccess) e = cudaFree(gr.dev);
+      gr.dev = nullptr;
+      gr.cap = 0;
+      const int cap = np > 64 ? 2 * np : 128;
+      if (e == cudaSuccess) e = cudaMalloc(&gr.dev, sizeof(FVServePatch) * cap);
+      if (e != cudaSuccess) return cuda_status(e, "fv serving table");
+      gr.cap = cap;
+    }
+    cudaError_t e = cudaMemcpyAsync(gr.dev, gr.host.data(), sizeof(FVServePatch) * np, cudaMemcpyHostToDevice,
+                                    s->fv_st);
+    if (e != cudaSuccess) return cuda_status(e, "fv serving table upload");
+  }
+  s->fv_dirty = false;
+  return EXA_OK;
+}
+}  // namespace
 
 exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
   if (!s) return set_error(EXA_EINVAL, "NULL server");
@@ -160,14 +226,22 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
     if (!kv.second.done && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
   if (any_dg)
     if (exa_status_t st = exa_ensemble_step(s->ens, 1)) return st;
+  if (s->fv_dirty)
+    if (exa_status_t st = rebuild_fv_groups(s)) return st;
+  for (int k = 0; k < 4; k++) {
+    FVGroup& gr = s->groups[k];
+    if (exa_status_t st = fv_serve_step_async(k / 2, k % 2 == 1, gr.dev, (int)gr.host.size(), gr.ntiles, s->fv_st))
+      return st;
+  }
   for (auto& kv : s->live) {
     Req& q = kv.second;
     if (q.done || q.r.kind != EXA_REQ_FV) continue;
-    if (exa_status_t st = fv_patch_step_async(q.r.fv_scheme, q.fv, q.luh, q.luh_new, q.dt_slot, s->fv_st))
-      return st;
-    std::swap(q.luh, q.luh_new);
+    q.par ^= 1;
     q.steps_done++;
-    if (--q.steps_left == 0) q.done = true;
+    if (--q.steps_left == 0) {
+      q.done = true;
+      s->fv_dirty = true;
+    }
   }
   exa_status_t st = EXA_OK;
   if (any_dg) {
@@ -230,12 +304,17 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
   if (!q.done) return set_error(EXA_EBUSY, "request still running");
   exa_status_t st = EXA_OK;
   if (q.r.kind == EXA_REQ_ADERDG) {
+    const bool failed = s->st_nan[q.slot] != 0;
     st = exa_ensemble_get_state(s->ens, q.slot, host_out);
     if (sim_time) *sim_time = s->st_time[q.slot];
     if (!st) st = exa_ensemble_remove(s->ens, q.slot);
+    // a solve that produced a non-finite state stopped there (the others
+    // went on): its result is returned and the request reported failed
+    if (!st && failed) st = set_error(EXA_ENAN, "the solve produced a non-finite state");
   } else {
     double scal[2];
-    cudaError_t e = cudaMemcpyAsync(host_out, q.luh, n * sizeof(double), cudaMemcpyDeviceToHost, s->fv_st);
+    cudaError_t e = cudaMemcpyAsync(host_out, q.par ? q.luh_new : q.luh, n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s->fv_st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(scal, q.dt_slot, 16, cudaMemcpyDeviceToHost, s->fv_st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->fv_st);
     if (e != cudaSuccess) return cuda_status(e, "fv result");
@@ -247,6 +326,17 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
   return st;
 }
 
+exa_status_t exa_server_device_state(exa_server* s, uint64_t id, double** luh_dev) {
+  if (!s || !luh_dev) return set_error(EXA_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  const Req& q = it->second;
+  if (q.r.kind == EXA_REQ_ADERDG) return exa_ensemble_device_state(s->ens, q.slot, luh_dev);
+  *luh_dev = q.par ? q.luh_new : q.luh;
+  return EXA_OK;
+}
+
 exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_cells,
                              size_t* arena_free_bytes) {
   if (!s) return set_error(EXA_EINVAL, "NULL server");
@@ -254,6 +344,97 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
   if (live_requests) *live_requests = (int)s->live.size();
   if (active_dg_cells) *active_dg_cells = exa_ensemble_active_cells(s->ens);
   return exa_ensemble_info(s->ens, nullptr, nullptr, arena_free_bytes);
+}
+
+exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_request_record_t* rec, int n,
+                            double time_limit_s, double* const* results, uint64_t* ticks) {
+  if (!s || (n > 0 && (!reqs || !rec)) || n < 0) return set_error(EXA_EINVAL, "bad argument");
+  using clock = std::chrono::steady_clock;
+  const auto t0 = clock::now();
+  auto now = [&]() { return std::chrono::duration<double>(clock::now() - t0).count(); };
+  for (int i = 0; i < n; i++) {
+    rec[i].admitted_s = -1.0;
+    rec[i].completed_s = -1.0;
+    rec[i].sim_time = 0.0;
+    rec[i].steps_done = 0;
+    rec[i].status = -1;
+  }
+  std::deque<int> queue;              // arrived, not yet admitted (arrival order)
+  std::map<uint64_t, int> live;       // request id -> index
+  std::vector<double> scratch;
+  std::vector<uint64_t> ids(256);
+  int next = 0, done = 0;
+  uint64_t nt = 0;
+  exa_status_t err = EXA_OK;
+  while (done < n) {
+    const double t = now();
+    if (time_limit_s > 0 && t > time_limit_s) break;
+    while (next < n && rec[next].arrival_s <= t) queue.push_back(next++);
+    // admission: first fit in arrival order (a request that does not fit
+    // now keeps its place; smaller later ones may go first)
+    for (auto it = queue.begin(); it != queue.end();) {
+      uint64_t id = 0;
+      const exa_status_t st = exa_server_submit(s, &reqs[*it], &id);
+      if (st == EXA_EBUSY) {
+        ++it;
+        continue;
+      }
+      if (st) {
+        err = st;
+        break;
+      }
+      rec[*it].admitted_s = now();
+      live[id] = *it;
+      it = queue.erase(it);
+    }
+    if (err) break;
+    if (live.empty()) {
+      if (next < n) {
+        const double wait = rec[next].arrival_s - now();
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait < 0.01 ? wait : 0.01));
+      } else if (!queue.empty()) {
+        err = set_error(EXA_EBUSY, "a request does not fit into the server's memory budget even alone");
+        break;
+      }
+      continue;
+    }
+    int nc = 0;
+    const exa_status_t st = exa_server_tick(s, &nc);
+    nt++;
+    if (st && st != EXA_ENAN) {
+      err = st;
+      break;
+    }
+    for (;;) {
+      int k = 0;
+      if ((err = exa_server_completed(s, ids.data(), (int)ids.size(), &k))) break;
+      for (int j = 0; j < k; j++) {
+        const int i = live[ids[j]];
+        live.erase(ids[j]);
+        double* out = results ? results[i] : nullptr;
+        if (!out) {
+          scratch.resize(exa_server_result_size(s, ids[j]));
+          out = scratch.data();
+        }
+        double simt = 0.0;
+        long long steps = 0;
+        const exa_status_t rs = exa_server_result(s, ids[j], out, &simt, &steps);
+        if (rs && rs != EXA_ENAN) {
+          err = rs;
+          break;
+        }
+        rec[i].completed_s = now();
+        rec[i].sim_time = simt;
+        rec[i].steps_done = steps;
+        rec[i].status = rs;
+        done++;
+      }
+      if (err || k < (int)ids.size()) break;
+    }
+    if (err) break;
+  }
+  if (ticks) *ticks = nt;
+  return err;
 }
 
 }  // extern "C"

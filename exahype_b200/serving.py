@@ -1,9 +1,10 @@
-"""Serving loop over the C++ engine (exa_server_* in include/exa_kernels.h):
-a seeded Poisson stream of solve requests, a host-side admission queue for
-requests that do not fit yet, continuous batching (every tick advances all
-admitted requests by one step), and time-to-solution accounting."""
+"""Serving over the C++ engine (exa_server_* in include/exa_kernels.h): a
+seeded Poisson stream of solve requests handed to the engine's own request
+loop (exa_server_run: admission queue for requests that do not fit yet,
+continuous batching -- every tick advances all admitted requests by one
+step -- and time-to-solution records, all in C++); this module builds the
+requests and the arrival times and summarises the records."""
 import ctypes as C
-import time
 
 import numpy as np
 
@@ -13,6 +14,11 @@ from .ensemble import SolveConfig, solve_config
 
 REQ_ADERDG = 0
 REQ_FV = 1
+
+
+class RequestRecord(C.Structure):
+    _fields_ = [('arrival_s', C.c_double), ('admitted_s', C.c_double), ('completed_s', C.c_double),
+                ('sim_time', C.c_double), ('steps_done', C.c_longlong), ('status', C.c_int)]
 
 
 class Request(C.Structure):
@@ -68,12 +74,24 @@ class Server:
         call('exa_server_completed', self.h, ids, cap, C.byref(n))
         return [ids[i] for i in range(n.value)]
 
-    def result(self, rid):
+    def result(self, rid, with_status=False):
+        """(final state, simulated time, steps done) of a finished request;
+        with_status also returns the status: EXA_ENAN for a solve that
+        produced a non-finite state (without with_status that raises)."""
         size = int(lib().exa_server_result_size(self.h, C.c_uint64(rid)))
         out = np.empty(size)
         t, steps = C.c_double(), C.c_longlong()
-        call('exa_server_result', self.h, C.c_uint64(rid), out.ctypes.data, C.byref(t), C.byref(steps))
+        st = lib().exa_server_result(self.h, C.c_uint64(rid), out.ctypes.data, C.byref(t), C.byref(steps))
+        if st != _lib.EXA_OK and not (with_status and st == _lib.EXA_ENAN):
+            _lib.check(st, 'exa_server_result')
+        if with_status:
+            return out, t.value, steps.value, st
         return out, t.value, steps.value
+
+    def device_state_ptr(self, rid):
+        p = C.c_void_p()
+        call('exa_server_device_state', self.h, C.c_uint64(rid), C.byref(p))
+        return p.value
 
     def info(self):
         live, cells, free = C.c_int(), C.c_long(), C.c_size_t()
@@ -111,47 +129,45 @@ def request_mix(n, seed, dg_fraction=0.25):
     return out
 
 
+def result_size(req):
+    if req.kind == REQ_ADERDG:
+        B = req.dg.order + 1
+        return req.dg.n[0] * req.dg.n[1] * B * B * 5
+    g = 1 if req.fv_scheme == 0 else 2
+    return (req.fv_patch + 2 * g) ** 2 * 5
+
+
 def run_poisson(server, requests, rate, seed, collect=False, time_limit=None):
-    """Releases `requests` at seeded Poisson arrival times (rate per second,
-    host wall clock), ticks the server continuously, and returns per-request
-    time-to-solution (completion - arrival) plus throughput numbers."""
+    """Runs `requests` ((name, Request) pairs) arriving at seeded Poisson
+    times (rate per second) through the engine's C++ request loop; returns
+    per-request time-to-solution (completion - arrival), throughput and the
+    records."""
     rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(requests)))
-    t0 = time.perf_counter()
-    queue = []          # indices waiting for admission
-    live = {}           # id -> index
-    done = {}           # index -> (completion time, sim time, steps, state or None)
-    nxt = 0
-    cell_updates = 0
-    ticks = 0
-    while len(done) < len(requests):
-        now = time.perf_counter() - t0
-        if time_limit and now > time_limit:
-            break
-        while nxt < len(requests) and arrivals[nxt] <= now:
-            queue.append(nxt)
-            nxt += 1
-        still = []
-        for i in queue:
-            rid = server.submit(requests[i][1])
-            if rid is None:
-                still.append(i)
-            else:
-                live[rid] = i
-        queue = still
-        if not live:
-            if nxt < len(requests):
-                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.01)))
+    n = len(requests)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    reqs = (Request * n)(*[r for _, r in requests])
+    rec = (RequestRecord * n)()
+    for i in range(n):
+        rec[i].arrival_s = float(arrivals[i])
+    outs = ptrs = None
+    if collect:
+        outs = [np.empty(result_size(r)) for _, r in requests]
+        ptrs = (C.POINTER(C.c_double) * n)(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
+    ticks = C.c_uint64()
+    _lib.check(lib().exa_server_run(server.h, reqs, rec, n, float(time_limit or 0.0), ptrs, C.byref(ticks)),
+               'exa_server_run')
+    done, cell_updates, failed = {}, 0, []
+    for i in range(n):
+        if rec[i].completed_s < 0:
             continue
-        server.tick()
-        ticks += 1
-        for rid in server.completed():
-            i = live.pop(rid)
-            state, sim_t, steps = server.result(rid)
-            r = requests[i][1]
-            cells = r.dg.n[0] * r.dg.n[1] if r.kind == REQ_ADERDG else r.fv_patch * r.fv_patch
-            cell_updates += cells * steps
-            done[i] = (time.perf_counter() - t0, sim_t, steps, state if collect else None)
-    wall = time.perf_counter() - t0
+        r = requests[i][1]
+        cells = r.dg.n[0] * r.dg.n[1] if r.kind == REQ_ADERDG else r.fv_patch * r.fv_patch
+        cell_updates += cells * rec[i].steps_done
+        done[i] = (rec[i].completed_s, rec[i].sim_time, rec[i].steps_done, outs[i] if collect else None)
+        if rec[i].status != _lib.EXA_OK:
+            failed.append(i)
+    wall = max([rec[i].completed_s for i in done] + [0.0])
     lat = np.array([done[i][0] - arrivals[i] for i in sorted(done)])
-    return dict(latency=lat, done=done, arrivals=arrivals, wall=wall, ticks=ticks, cell_updates=cell_updates)
+    return dict(latency=lat, done=done, arrivals=arrivals, wall=wall, ticks=int(ticks.value),
+                cell_updates=cell_updates, failed=failed,
+                admitted=np.array([rec[i].admitted_s for i in range(n)]))

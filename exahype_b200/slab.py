@@ -22,11 +22,18 @@ The exchange is two face layers per step (a 81x81 layer of N=4 faces is
 13 MB) and the reduction is 8 bytes, against a ~60 ms step: NCCL send/recv
 on the grid's stream is enough; nothing here waits on the host.
 
-Transports: `DistRing` (torch.distributed; NCCL on GPUs, gloo for the CPU
-tests of this driver) and `LocalRing` (all slabs in one process, e.g.
-several slabs on one GPU).  Both drive any object with the slab interface
-(`phase`, `halo_tensors`, `dt_slot_tensor`, `stream_ctx`, `fixed_dt`).
+Transports:
+
+* `NcclRing` -- the GPU transport: exchange and reduction run inside the
+  library (exa_aderdg_grid_slab_step, C++ over NCCL on the grid's stream);
+  Python only passes the communicator's id between processes at start-up.
+* `DistRing` (torch.distributed, gloo) and `LocalRing` (all slabs in one
+  process) drive the same phases from Python for the CPU tests of this
+  driver with oracle slabs (any object with `phase`, `halo_tensors`,
+  `dt_slot_tensor`, `stream_ctx`, `fixed_dt`).
 """
+import ctypes as C
+
 import numpy as np
 
 from . import _lib
@@ -191,6 +198,45 @@ class LocalRing:
         return self.all
 
 
+class NcclRing:
+    """Slab transport inside the library (C++ over NCCL): one communicator
+    per process, rank `rank` of `nranks`; `uid` is the 128-byte id made by
+    rank 0 with NcclRing.make_id() and handed to every rank (e.g. over a
+    host-side process group).  prime / step run whole steps through
+    exa_aderdg_grid_slab_prime / _step, which wait with a deadline and abort
+    the communicator if a peer stops answering (EXA_ETIMEDOUT)."""
+
+    native = True
+
+    def __init__(self, rank, nranks, uid, timeout_s=60.0):
+        h = C.c_void_p()
+        buf = C.create_string_buffer(bytes(uid), 128)
+        _lib.call('exa_slab_comm_create', buf, int(nranks), int(rank), C.byref(h))
+        self.h = h
+        self.rank, self.world = rank, nranks
+        self.timeout_s = float(timeout_s)
+
+    @staticmethod
+    def make_id():
+        buf = C.create_string_buffer(128)
+        _lib.call('exa_nccl_unique_id', buf)
+        return buf.raw
+
+    def prime(self, slab):
+        _lib.call('exa_aderdg_grid_slab_prime', slab.grid.h, self.h, self.timeout_s)
+
+    def step(self, slab, nsteps):
+        _lib.call('exa_aderdg_grid_slab_step', slab.grid.h, self.h, int(nsteps), self.timeout_s)
+
+    def slabs(self, slab):
+        return [slab]
+
+    def destroy(self):
+        if self.h:
+            _lib.call('exa_slab_comm_destroy', self.h)
+            self.h = None
+
+
 def _each(ring, slab, fn):
     for s in ring.slabs(slab):
         fn(s)
@@ -198,6 +244,9 @@ def _each(ring, slab, fn):
 
 def prime(ring, slab=None):
     """Initial dt: local minimum per slab, MIN over slabs, commit."""
+    if getattr(ring, 'native', False):
+        ring.prime(slab)
+        return
     first = ring.slabs(slab)[0]
     if first.fixed_dt:
         _each(ring, slab, lambda s: s.phase(PHASE_PRIME_COMMIT))
@@ -209,6 +258,9 @@ def prime(ring, slab=None):
 
 def step(ring, slab=None, nsteps=1):
     """Advance every slab of the ring by nsteps time steps."""
+    if getattr(ring, 'native', False):
+        ring.step(slab, nsteps)
+        return
     fixed = ring.slabs(slab)[0].fixed_dt
     for _ in range(nsteps):
         _each(ring, slab, lambda s: s.phase(PHASE_PREDICT))

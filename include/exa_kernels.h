@@ -526,6 +526,27 @@ exa_status_t exa_aderdg_grid_phase(exa_aderdg_grid* g, int phase);
 exa_status_t exa_aderdg_grid_init_slab(exa_aderdg_grid* g, int kind, double param, uint64_t seed,
                                        double noise_amp, int rank, int nranks);
 
+/* Slab transport over NCCL inside the library (replaces the reference's MPI
+ * face exchange, ADERDGSolver::sendDataToNeighbour / mergeWithNeighbourData,
+ * ADERDGSolver.cpp:3379 and :3451, and the global dt minimum of
+ * TimeStepSizeComputation.cpp:83-109).  One communicator per process (rank
+ * r holds slab r of nranks along the last dimension, on the current device):
+ * rank 0 makes the 128-byte id with exa_nccl_unique_id, every rank passes
+ * it to exa_slab_comm_create.  exa_aderdg_grid_slab_step enqueues nsteps
+ * whole steps on the grid's stream (predict, NCCL send/recv of the two
+ * boundary face layers, correct, NCCL MIN all-reduce of the dt slot,
+ * commit) and waits for them; if they have not finished after timeout_s
+ * seconds per step (<= 0: 60 s) the communicator is aborted and
+ * EXA_ETIMEDOUT returned.  With nranks == 1 the face layers are copied on
+ * the stream.  NCCL is opened at run time (libnccl.so.2); without it these
+ * calls return EXA_ECUDA with the reason. */
+typedef struct exa_slab_comm exa_slab_comm;
+exa_status_t exa_nccl_unique_id(void* id128);
+exa_status_t exa_slab_comm_create(const void* id128, int nranks, int rank, exa_slab_comm** out);
+exa_status_t exa_slab_comm_destroy(exa_slab_comm* c);
+exa_status_t exa_aderdg_grid_slab_prime(exa_aderdg_grid* g, exa_slab_comm* c, double timeout_s);
+exa_status_t exa_aderdg_grid_slab_step(exa_aderdg_grid* g, exa_slab_comm* c, int nsteps, double timeout_s);
+
 /* ------------------------------------ ADER-DG: ensemble of 2D solves --
  * Many independent uniform periodic 2D grids (each its own order 2..5, size,
  * dt and step budget -- the per-solver state of ADERDGSolver.cpp:557-585)
@@ -606,6 +627,34 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
                                long long* steps_done);
 exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_cells,
                              size_t* arena_free_bytes);
+/* device pointer of a live request's current state (ADER-DG: the solve's
+ * luh; FV: the patch buffer that holds the state), for zero-copy inspection
+ * between ticks */
+exa_status_t exa_server_device_state(exa_server* s, uint64_t id, double** luh_dev);
+
+/* One request of a stream run by exa_server_run (times in seconds after the
+ * start of the run). */
+typedef struct {
+  double arrival_s;      /* in: when the request arrives */
+  double admitted_s;     /* out: when it was admitted (-1: never) */
+  double completed_s;    /* out: when its result was on the host (-1: not completed) */
+  double sim_time;       /* out: simulated time reached */
+  long long steps_done;  /* out */
+  int status;            /* out: EXA_OK; EXA_ENAN for a solve that produced a non-finite state
+                            (stopped there, its state returned, the others unaffected); -1 not completed */
+} exa_request_record_t;
+
+/* The serving loop, from this host thread: requests arrive at their
+ * arrival_s; arrived requests are admitted first-fit in arrival order as
+ * memory and slots free up; every tick advances every admitted request one
+ * step (continuous batching, exa_server_tick); finished results are copied
+ * out (into results[i] when results and results[i] are non-NULL) and their
+ * memory freed.  Returns when every request has completed or after
+ * time_limit_s seconds (<= 0: no limit); ticks (nullable) receives the tick
+ * count.  No counterpart in the reference (its requests are whole runs of
+ * the executable); the solves are the reference's step as in the ensemble. */
+exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_request_record_t* rec, int n,
+                            double time_limit_s, double* const* results, uint64_t* ticks);
 
 /* ------------------------------------------------ finite volumes (2D) --
  * One patch of patch x patch cells with `ghost` ghost layers, layout

@@ -122,3 +122,58 @@ def test_poisson_stream_small():
     assert len(res['done']) == 12
     assert (res['latency'] > 0).all()
     assert res['cell_updates'] > 0
+
+
+def test_failed_request_reported_and_others_unchanged():
+    """A NaN planted in one live ADER-DG request's state (between ticks, on
+    the host side of the call) makes that request finish as failed
+    (EXA_ENAN, stopped at the step that produced it) while the other
+    requests in the mix complete bit for bit as they do without it."""
+    import ctypes as C
+    from exahype_b200 import _lib
+    mix = [S.dg_request(3, 15, 8, seed=31), S.dg_request(4, 12, 8, seed=32), S.fv_request(80, 8, seed=33),
+           S.dg_request(2, 20, 8, seed=34)]
+    clean = run_to_completion(S.Server(1 << 28), mix)
+    srv = S.Server(1 << 28)
+    ids = [srv.submit(r) for r in mix]
+    for _ in range(2):
+        srv.tick()
+    ptr = srv.device_state_ptr(ids[1])
+    nan = np.array([np.nan])
+    _lib.call('exa_memcpy_h2d', C.c_void_p(ptr + 8 * 77), nan.ctypes.data, 8, None)
+    E.device.synchronize()
+    got, status = {}, {}
+    for _ in range(20):
+        srv.tick()
+        for rid in srv.completed():
+            i = ids.index(rid)
+            out, t, steps, st = srv.result(rid, with_status=True)
+            got[i] = (out, t, steps)
+            status[i] = st
+        if len(got) == len(mix):
+            break
+    srv.destroy()
+    assert status[1] == _lib.EXA_ENAN and got[1][2] == 2
+    for i in (0, 2, 3):
+        assert status[i] == _lib.EXA_OK
+        assert np.array_equal(got[i][0], clean[i][0]) and got[i][2] == clean[i][2] == 8
+
+
+def test_fv_batch_equals_single_patches():
+    """FV requests of several sizes and both schemes stepped together in the
+    batched serving launch equal each patch stepped alone by the
+    single-patch kernels (FVGrid), bit for bit, with requests joining and
+    leaving mid-stream."""
+    sizes, steps = [64, 100, 37, 256, 90], [6, 9, 4, 7, 5]
+    reqs = [S.fv_request(P, k, scheme=1 if i % 2 == 0 else 0, seed=40 + i, noise=1e-3)
+            for i, (P, k) in enumerate(zip(sizes, steps))]
+    srv = S.Server(1 << 28)
+    got = run_to_completion(srv, reqs, submit_at=[0, 1, 0, 3, 2])
+    srv.destroy()
+    for i, (r, P, k) in enumerate(zip(reqs, sizes, steps)):
+        g = E.FVGrid(r.fv_scheme, P)
+        g.init(amp=0.2, seed=40 + i, noise=1e-3)
+        g.step(k)
+        ref, t = g.get_state(), g.status()['time']
+        g.destroy()
+        assert np.array_equal(got[i][0], ref) and got[i][1] == t and got[i][2] == k, i

@@ -1,12 +1,18 @@
 """Slab decomposition on the GPU: slabs of one grid (several on this GPU,
-exchanged by a local ring; or one slab per rank through torch.distributed
-with NCCL) reproduce the undivided periodic grid bit for bit."""
+exchanged by a local ring; or one slab per process through the library's
+own NCCL transport, exa_aderdg_grid_slab_step) reproduce the undivided
+periodic grid bit for bit.  Every GPU run here has one GPU, so the NCCL
+transport is exercised with a one-rank communicator (its face layers are
+copied on the stream, its dt minimum is NCCL's one-rank all-reduce); the
+multi-rank exchange order is covered by the CPU tests of the same driver
+(tests/test_slab_host.py)."""
 import os
-import socket
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
-import torch.multiprocessing as mp
 
 import exahype_b200 as E
 from exahype_b200 import slab as SL
@@ -57,31 +63,49 @@ def test_halo_grid_refuses_plain_step():
     g.destroy()
 
 
-def _nccl_rank(rank, port, outdir):
-    import datetime
-    import torch
-    import torch.distributed as dist
-    os.environ['MASTER_ADDR'] = '127.0.0.1'
-    os.environ['MASTER_PORT'] = str(port)
-    torch.cuda.set_device(0)
-    dist.init_process_group('nccl', rank=rank, world_size=1, timeout=datetime.timedelta(seconds=60),
-                            device_id=torch.device('cuda', 0))
-    try:
-        s = SL.SlabGrid(3, 3, (4, 5, 3), rank, 1)
-        s.init(**IC)
-        ring = SL.DistRing(dist)
-        SL.prime(ring, s)
-        SL.step(ring, s, 3)
-        np.save(os.path.join(outdir, 'state.npy'), s.get_state())
-        s.destroy()
-    finally:
-        dist.destroy_process_group()
+@pytest.mark.parametrize('dt_policy', [0, 2])
+def test_nccl_ring_single_rank(dt_policy):
+    kw = dict(dt_policy=dt_policy, dt_fixed=2e-3) if dt_policy == 2 else {}
+    s = SL.SlabGrid(3, 3, (4, 5, 3), 0, 1, **kw)
+    s.init(**IC)
+    ring = SL.NcclRing(0, 1, SL.NcclRing.make_id())
+    SL.prime(ring, s)
+    SL.step(ring, s, 3)
+    got, t = s.get_state(), s.status()['time']
+    s.destroy()
+    ring.destroy()
+    g = E.ADERDGGrid(3, 3, (4, 5, 3), **kw)
+    g.init(**IC)
+    g.step(3)
+    assert np.array_equal(got, g.get_state())
+    assert t == g.status()['time']
+    g.destroy()
 
 
-def test_dist_ring_nccl_single_rank(tmp_path):
-    with socket.socket() as so:
-        so.bind(('127.0.0.1', 0))
-        port = so.getsockname()[1]
-    mp.spawn(_nccl_rank, args=(port, str(tmp_path)), nprocs=1, join=True)
-    ref, _, _ = undivided(3, 3, (4, 5, 3), 3, **IC)
-    assert np.array_equal(np.load(tmp_path / 'state.npy'), ref)
+_NO_TORCH = textwrap.dedent('''
+    import sys
+    sys.path.insert(0, sys.argv[1])
+    import numpy as np
+    import exahype_b200 as E
+    from exahype_b200 import slab as SL
+    E.lib().exa_set_device(0)
+    s = SL.SlabGrid(3, 2, (3, 3, 4), 0, 1)
+    s.init(kind=0, param=5.0, seed=3, noise=1e-3)
+    ring = SL.NcclRing(0, 1, SL.NcclRing.make_id())
+    SL.prime(ring, s)
+    SL.step(ring, s, 2)
+    st = s.status()
+    assert st['time'] > 0 and not st['nan']
+    ring.destroy()
+    s.destroy()
+    assert 'torch' not in sys.modules, 'torch was imported on the slab path'
+    print('no torch ok')
+''')
+
+
+def test_nccl_ring_needs_no_torch():
+    """The slab transport runs in a process that never imports torch."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, '-c', _NO_TORCH, root], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert 'no torch ok' in r.stdout
