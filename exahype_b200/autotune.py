@@ -2,8 +2,9 @@
 workload with CUDA events (the measure-then-pick idea of the reference's
 shared-memory oracles, Peano/sharedmemoryoracles/, applied to GPU knobs).
 
-tune_ensemble: persistent CTAs per SM x work items per grab x work order
-for an Ensemble; tune_predictor: register budget of the predictor kernels
+tune_ensemble: the contraction per order, then persistent CTAs per SM x
+work items per grab (cells per CTA) x work order, for an Ensemble;
+tune_predictor: register budget of the predictor kernels
 (exa_tune_set keys) for a grid.  Results can be cached in a JSON file keyed
 by the workload signature."""
 import itertools
@@ -24,24 +25,52 @@ def _time_ensemble(ens, steps):
     return t.elapsed_ms() / steps
 
 
-def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 4), orders=(0, 1), cache=None, key=None):
-    """Times every (ctas_per_sm, grab, order_policy) combination on `ens`
-    (which advances while being measured), applies the fastest and returns
-    (best, table)."""
+def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), contraction=True, cache=None,
+                  key=None):
+    """Picks the ensemble's knobs by timing `ens` itself (which advances
+    while being measured):
+
+    1. the contraction of each order present (line-owner or node-gather;
+       exa_ensemble_tune_contraction): coordinate descent from the default,
+       flipping one order at a time and keeping the faster;
+    2. the persistent schedule: CTAs per SM x work items per atomic grab
+       (the cells-per-CTA schedule: a grab takes that many consecutive
+       blocks of cells) x work order (costly orders first / solve order),
+       every combination timed.
+
+    Applies the fastest and returns (best, table), best =
+    (ctas_per_sm, grab, order_policy, lines_mask)."""
     if cache and key and os.path.exists(cache):
         with open(cache) as f:
             got = json.load(f).get(key)
         if got:
-            ens.tune(*got['best'])
+            c, g, o, m = got['best']
+            ens.tune_contraction(m)
+            ens.tune(c, g, o)
             return tuple(got['best']), got['table']
     table = []
+    mask = 0x30  # orders 4 and 5 line-owner: the library's default
+    present = sorted({c.order for c in ens.cfgs.values()})
+    if contraction and present:
+        ens.tune_contraction(mask)
+        ens.tune(ctas[0], grabs[0], orders[0])
+        base = _time_ensemble(ens, steps)
+        table.append({'stage': 'contraction', 'lines_mask': mask, 'ms_per_step': base})
+        for n in present:
+            trial = mask ^ (1 << n)
+            ens.tune_contraction(trial)
+            ms = _time_ensemble(ens, steps)
+            table.append({'stage': 'contraction', 'lines_mask': trial, 'ms_per_step': ms})
+            if ms < base:
+                mask, base = trial, ms
+        ens.tune_contraction(mask)
     for c, g, o in itertools.product(ctas, grabs, orders):
         ens.tune(c, g, o)
         ms = _time_ensemble(ens, steps)
-        table.append({'ctas_per_sm': c, 'grab': g, 'order_policy': o, 'ms_per_step': ms})
-    best = min(table, key=lambda r: r['ms_per_step'])
-    b = (best['ctas_per_sm'], best['grab'], best['order_policy'])
-    ens.tune(*b)
+        table.append({'stage': 'schedule', 'ctas_per_sm': c, 'grab': g, 'order_policy': o, 'ms_per_step': ms})
+    best = min((r for r in table if r['stage'] == 'schedule'), key=lambda r: r['ms_per_step'])
+    b = (best['ctas_per_sm'], best['grab'], best['order_policy'], mask)
+    ens.tune(*b[:3])
     if cache and key:
         data = {}
         if os.path.exists(cache):

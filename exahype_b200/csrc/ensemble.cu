@@ -68,20 +68,22 @@ struct EnsArgs {
   int grab;            // work items taken per atomic
   unsigned int* ctr;   // [2] phase counters, reset by phase 3
   int precision;
+  int lines_mask;      // bit N set: order N's predictor uses the line-owner contraction
 };
 
 constexpr int kEnsNT = 128;
 
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
-// orders whose predictor runs the line-owner contraction (as the stand-alone
-// kernels do by default: measured faster from order 4 on)
-template <int N>
-constexpr bool ens_lines() { return N >= 4; }
-// shared memory (doubles) the largest 2D order needs in either phase
+// default: orders whose predictor runs the line-owner contraction (as the
+// stand-alone kernels do by default: measured faster from order 4 on); the
+// autotuner may choose per order (exa_ensemble_tune_contraction)
+constexpr int kEnsLinesDefault = (1 << 4) | (1 << 5);
+// shared memory (doubles) the largest 2D order needs in either phase and
+// either contraction
 template <int N>
 constexpr int ens_smem_n() {
-  return cmax(cmax(ens_lines<N>() ? Fp64LineShape<2, N>::SM_DOUBLES : PredShape<2, N, 0>::SM_DOUBLES,
-                   ens_lines<N>() ? LineShape<2, N>::SM_DOUBLES : MixShape<2, N>::SM_DOUBLES),
+  return cmax(cmax(cmax(Fp64LineShape<2, N>::SM_DOUBLES, PredShape<2, N, 0>::SM_DOUBLES),
+                   cmax(LineShape<2, N>::SM_DOUBLES, MixShape<2, N>::SM_DOUBLES)),
               CorrShapeSmem<2, N>::value);
 }
 constexpr int kEnsSmemDoubles = cmax(cmax(ens_smem_n<2>(), ens_smem_n<3>()), cmax(ens_smem_n<4>(), ens_smem_n<5>()));
@@ -127,10 +129,10 @@ __device__ __forceinline__ CorrArgs corr_args(SolveDev& sv) {
 // One non-inlined function per (phase, order, precision, pde form): each
 // keeps the register allocation of the stand-alone kernel instead of
 // sharing one allocation across every path of the persistent kernel.
-template <int N, bool PLANAR, int PREC>
+template <int N, bool PLANAR, int PREC, bool LINES>
 __device__ __noinline__ void ens_pred(const SolveDev* sv, int block, double* smem, int precision) {
   const PredArgs a = pred_args(*sv, precision);
-  if constexpr (ens_lines<N>()) {
+  if constexpr (LINES) {
     if (PREC) predictor_mixed_lines_block<2, N, PLANAR>(a, block, smem);
     else predictor_fp64_lines_block<2, N, PLANAR>(a, block, smem);
   } else {
@@ -145,14 +147,27 @@ __device__ __noinline__ void ens_corr(SolveDev* sv, int block, double* smem) {
   corrector_block<2, N, PLANAR>(c, block, smem);
 }
 
-template <int PREC>
-__device__ __forceinline__ void run_pred(const SolveDev& sv, int block, double* smem, int precision) {
+template <int N, int PREC>
+__device__ __forceinline__ void run_pred_n(const SolveDev& sv, int block, double* smem, int precision, bool lines) {
   const bool planar = sv.pde == EXA_PDE_EULER_PLANAR;
+  if (lines) {
+    if (planar) ens_pred<N, true, PREC, true>(&sv, block, smem, precision);
+    else ens_pred<N, false, PREC, true>(&sv, block, smem, precision);
+  } else {
+    if (planar) ens_pred<N, true, PREC, false>(&sv, block, smem, precision);
+    else ens_pred<N, false, PREC, false>(&sv, block, smem, precision);
+  }
+}
+
+template <int PREC>
+__device__ __forceinline__ void run_pred(const SolveDev& sv, int block, double* smem, int precision,
+                                         int lines_mask) {
+  const bool lines = (lines_mask >> sv.order) & 1;
   switch (sv.order) {
-    case 2: planar ? ens_pred<2, true, PREC>(&sv, block, smem, precision) : ens_pred<2, false, PREC>(&sv, block, smem, precision); break;
-    case 3: planar ? ens_pred<3, true, PREC>(&sv, block, smem, precision) : ens_pred<3, false, PREC>(&sv, block, smem, precision); break;
-    case 4: planar ? ens_pred<4, true, PREC>(&sv, block, smem, precision) : ens_pred<4, false, PREC>(&sv, block, smem, precision); break;
-    case 5: planar ? ens_pred<5, true, PREC>(&sv, block, smem, precision) : ens_pred<5, false, PREC>(&sv, block, smem, precision); break;
+    case 2: run_pred_n<2, PREC>(sv, block, smem, precision, lines); break;
+    case 3: run_pred_n<3, PREC>(sv, block, smem, precision, lines); break;
+    case 4: run_pred_n<4, PREC>(sv, block, smem, precision, lines); break;
+    case 5: run_pred_n<5, PREC>(sv, block, smem, precision, lines); break;
   }
 }
 
@@ -183,7 +198,7 @@ __global__ void __launch_bounds__(kEnsNT) k_ensemble_step(EnsArgs a) {
         const WorkItem it = a.items[w];
         SolveDev& sv = a.solves[it.solve];
         if (!sv.active) continue;  // uniform across the CTA
-        if (phase == 0) run_pred<PREC>(sv, it.block, smem, a.precision);
+        if (phase == 0) run_pred<PREC>(sv, it.block, smem, a.precision, a.lines_mask);
         else run_corr(sv, it.block, smem);
         __syncthreads();  // smem reuse by the next item
       }
@@ -266,6 +281,7 @@ struct exa_ensemble {
   cudaGraphExec_t graph = nullptr;
   // tuning (exa_ensemble_tune): CTAs per SM, items per grab, order policy
   int ctas_per_sm = 0, grab = 1, order_policy = 0;
+  int lines_mask = kEnsLinesDefault;  // per order: line-owner (bit set) or node-gather contraction
   int grid = 0;
   std::mutex mu;
 };
@@ -383,6 +399,7 @@ static exa_status_t launch_step(exa_ensemble* e) {
   a.grab = e->grab;
   a.ctr = e->d_ctr;
   a.precision = e->precision;
+  a.lines_mask = e->lines_mask;
   void* args[] = {&a};
   const size_t smem = sizeof(double) * kEnsSmemDoubles;
   cudaError_t err;
@@ -607,6 +624,15 @@ exa_status_t exa_ensemble_tune(exa_ensemble* e, int ctas_per_sm, int grab, int o
   e->order_policy = order_policy;
   e->dirty = true;
   return configure_grid(e);
+}
+
+exa_status_t exa_ensemble_tune_contraction(exa_ensemble* e, int lines_mask) {
+  if (!e || (lines_mask & ~0x3C)) return set_error(EXA_EINVAL, "contraction mask: bits 2..5 (orders) only");
+  std::lock_guard<std::mutex> lk(e->mu);
+  cudaStreamSynchronize(e->st);
+  e->lines_mask = lines_mask;
+  e->dirty = true;  // the step graph holds the kernel arguments
+  return EXA_OK;
 }
 
 exa_status_t exa_ensemble_synchronize(exa_ensemble* e) {

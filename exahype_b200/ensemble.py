@@ -60,6 +60,10 @@ class Ensemble:
     def tune(self, ctas_per_sm=0, grab=1, order_policy=0):
         call('exa_ensemble_tune', self.h, int(ctas_per_sm), int(grab), int(order_policy))
 
+    def tune_contraction(self, lines_mask):
+        """Per order N: bit N set = line-owner contraction, clear = node-gather."""
+        call('exa_ensemble_tune_contraction', self.h, int(lines_mask))
+
     def synchronize(self):
         call('exa_ensemble_synchronize', self.h)
 

@@ -584,6 +584,10 @@ exa_status_t exa_ensemble_use_graph(exa_ensemble* e, int enable);
 /* schedule knobs: persistent CTAs per SM (0 = max resident), work items per
  * atomic grab, work order (0 = costly orders first, 1 = solve order) */
 exa_status_t exa_ensemble_tune(exa_ensemble* e, int ctas_per_sm, int grab, int order_policy);
+/* contraction of each order's predictor inside the persistent launch: bit N
+ * of lines_mask set = line-owner contraction, clear = node-gather (default:
+ * orders 4 and 5 line-owner); results agree to rounding */
+exa_status_t exa_ensemble_tune_contraction(exa_ensemble* e, int lines_mask);
 exa_status_t exa_ensemble_synchronize(exa_ensemble* e);
 exa_status_t exa_ensemble_stream(exa_ensemble* e, void** stream);
 exa_status_t exa_ensemble_get_state(exa_ensemble* e, int slot, double* host_luh);

@@ -114,3 +114,32 @@ def test_mixed_ensemble_vs_fp64(seed):
         assert e['rel_l2'] <= 1e-8, e
     a.destroy()
     b.destroy()
+
+
+def test_contraction_choice_agrees_and_autotuner_applies_it():
+    """Every order's predictor gives the same solves with either contraction
+    inside the persistent launch (to rounding), and the autotuner's
+    contraction stage and schedule stage produce a applied 4-tuple."""
+    from exahype_b200.autotune import tune_ensemble
+    mix = MIX[:4]
+    a = E.Ensemble(8, 1 << 27)
+    b = E.Ensemble(8, 1 << 27)
+    sa = [a.add(cfg(*m), steps=5) for m in mix]
+    sb = [b.add(cfg(*m), steps=5) for m in mix]
+    b.tune_contraction(0x0C)  # orders 2 and 3 line-owner, 4 and 5 node-gather: the opposite of the default
+    for ens in (a, b):
+        ens.step(5)
+        ens.status()
+    for x, y in zip(sa, sb):
+        assert rel(b.get_state(y), a.get_state(x)) < 1e-12
+    a.destroy()
+    b.destroy()
+    c = E.Ensemble(8, 1 << 27)
+    for m in mix:
+        c.add(cfg(*m))
+    best, table = tune_ensemble(c, steps=1, ctas=(1,), grabs=(1, 2), orders=(0,))
+    assert len(best) == 4 and best[3] & ~0x3C == 0
+    assert sum(1 for r in table if r['stage'] == 'contraction') == 1 + len({m[0] for m in mix})
+    c.step(2)
+    assert not c.status()['nan'].any()
+    c.destroy()
