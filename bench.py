@@ -776,13 +776,25 @@ def run_fv(args, rank, world, dist):
         flop = fv_flop_per_cell(scheme) * cells
         hbm = bytes_alg / (per * 1e-3) / 1e9
         tf = flop / (per * 1e-3) / 1e12
+        # the bound follows the arithmetic intensity: FLOP per algorithmic
+        # byte against the ridge of the measured FP64 and HBM peaks
+        intensity = fv_flop_per_cell(scheme) / 80.0
+        ridge = fp64_peak.value * 1e12 / (peaks['hbm_gbs'] * 1e9) if peaks.get('hbm_gbs') else None
+        fp64_bound = ridge is not None and intensity > ridge
         r = {'value': ups, 'ms_per_step': per, 'gpu_launches': launches, 'clocks': clk,
-             'roofline': {'kernel': 'k_fv_muscl<fused>' if scheme else 'k_fv_godunov<fused>',
-                          'bound': 'hbm', 'achieved': hbm, 'peak': peaks.get('hbm_gbs'), 'unit': 'GB/s',
-                          'frac': hbm / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None,
-                          'peak_source': peak_src, 'bytes_per_cell_update': 80,
+             'roofline': {'kernel': 'k_fv_muscl_periodic' if scheme else 'k_fv_godunov<fused>',
+                          'bound': 'fp64' if fp64_bound else 'hbm',
+                          'achieved': tf if fp64_bound else hbm,
+                          'peak': fp64_peak.value if fp64_bound else peaks.get('hbm_gbs'),
+                          'unit': 'TFLOP/s' if fp64_bound else 'GB/s',
+                          'frac': (tf / fp64_peak.value) if fp64_bound else
+                                  (hbm / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None),
+                          'intensity_flop_per_byte': intensity, 'ridge_flop_per_byte': ridge,
+                          'hbm_achieved_gbs': hbm, 'hbm_peak_gbs': peaks.get('hbm_gbs'),
+                          'hbm_frac': hbm / peaks['hbm_gbs'] if peaks.get('hbm_gbs') else None,
                           'fp64_achieved_tflops': tf, 'fp64_peak_tflops': fp64_peak.value,
                           'fp64_frac': tf / fp64_peak.value, 'flop_per_cell_update': fv_flop_per_cell(scheme),
+                          'bytes_per_cell_update': 80, 'peak_source': peak_src + ' (HBM); DFMA probe (FP64)',
                           'note': 'step time includes the one-thread commit launch'}}
         if scheme == 1:
             pin = PinnedBuffer(g.state_size)
