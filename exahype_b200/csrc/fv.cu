@@ -573,63 +573,17 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
     }
   }
   __syncthreads();
-  // every face's Rusanov flux once (the reference's loops, and a per-cell
-  // form, solve each interior face from both sides: the same value twice).
-  // x face (r, cf), r < TY, cf <= TX: between ring columns cf and cf + 1 of
-  // ring row r + 1; y face (r, c), r <= TY, c < TX: between ring rows r and
-  // r + 1 of ring column c + 1.  The x-face fluxes are solved into
-  // registers, then (after every thread has read the x-face states) stored
-  // over wLx while the y faces are solved, then stored over wLy.
-  constexpr int NFX = FVP_TY * (FVP_TX + 1), NFY = (FVP_TY + 1) * FVP_TX;
-  constexpr int PX = (NFX + FVP_NT - 1) / FVP_NT, PY = (NFY + FVP_NT - 1) / FVP_NT;
-  {
-    double fx[PX][V];
-#pragma unroll
-    for (int q = 0; q < PX; q++) {
-      const int f = tid + q * FVP_NT;
-      if (f < NFX) {
-        const int il = (f / (FVP_TX + 1) + 1) * RX + f % (FVP_TX + 1);
-        rusanov<PLANAR>(&wRx[il * V], &wLx[(il + 1) * V], 0, fx[q]);
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PX; q++) {
-      const int f = tid + q * FVP_NT;
-      if (f < NFX)
-#pragma unroll
-        for (int m = 0; m < V; m++) wLx[f * V + m] = fx[q][m];
-    }
-  }
-  {
-    double fy[PY][V];
-#pragma unroll
-    for (int q = 0; q < PY; q++) {
-      const int f = tid + q * FVP_NT;
-      if (f < NFY) {
-        const int ib = (f / FVP_TX) * RX + f % FVP_TX + 1;
-        rusanov<PLANAR>(&wRy[ib * V], &wLy[(ib + RX) * V], 1, fy[q]);
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < PY; q++) {
-      const int f = tid + q * FVP_NT;
-      if (f < NFY)
-#pragma unroll
-        for (int m = 0; m < V; m++) wLy[f * V + m] = fy[q][m];
-    }
-  }
-  __syncthreads();
   const double cx = dt / hx, cy = dt / hy;
   double dtn = DBL_MAX;
   const int r = tid / FVP_TX, c = tid % FVP_TX;
   const int j = j0 + r, k = k0 + c;
   if (j < pe && k < pe) {
-    const double* fxl = &wLx[(r * (FVP_TX + 1) + c) * V];
-    const double* fxr = fxl + V;
-    const double* fyb = &wLy[(r * FVP_TX + c) * V];
-    const double* fyt = fyb + FVP_TX * V;
+    const int ic = (r + 1) * RX + c + 1;  // this cell in the ring arrays
+    double fxl[V], fxr[V], fyb[V], fyt[V];
+    rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
+    rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
+    rusanov<PLANAR>(&wRy[(ic - RX) * V], &wLy[ic * V], 1, fyb);
+    rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + RX) * V], 1, fyt);
     fv_update_store_dt<PLANAR>(a, a.out + ((long)j * S + k) * D, &su[((r + 2) * LX + c + 2) * V], fxl, fxr,
                                fyb, fyt, cx, cy, dtn);
   }
