@@ -724,7 +724,8 @@ def ensemble_measure(args, rank, dist):
         out[prec_name] = {'value': updates / (ms * 1e-3), 'ms_per_step': ms / args.steps, 'cells': cells,
                           'launches_per_step': launches / args.steps, 'tuned': {'ctas_per_sm': best[0],
                           'grab': best[1], 'order_policy': best[2], 'line_owner_orders':
-                          [n for n in range(2, 6) if (best[3] >> n) & 1]}, 'tuning_table': table}
+                          [n for n in range(2, 6) if (best[3] >> n) & 1],
+                          'launch_mode': 'per order' if best[4] else 'persistent'}, 'tuning_table': table}
         if prec_name == 'fp64':
             ref_states = {sl: ens.get_state(sl) for sl in list(ens.cfgs)[:16]}
         else:

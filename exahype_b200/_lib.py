@@ -201,6 +201,7 @@ SIGNATURES = {
     'exa_ensemble_use_graph': (i32, [vp, i32]),
     'exa_ensemble_tune': (i32, [vp, i32, i32, i32]),
     'exa_ensemble_tune_contraction': (i32, [vp, i32]),
+    'exa_ensemble_set_launch_mode': (i32, [vp, i32]),
     'exa_ensemble_synchronize': (i32, [vp]),
     'exa_ensemble_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_ensemble_get_state': (i32, [vp, i32, vp]),

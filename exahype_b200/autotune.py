@@ -38,15 +38,19 @@ def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), 
        blocks of cells) x work order (costly orders first / solve order),
        every combination timed.
 
+    3. the launch form: the best persistent schedule against one launch per
+       order and phase (exa_ensemble_set_launch_mode).
+
     Applies the fastest and returns (best, table), best =
-    (ctas_per_sm, grab, order_policy, lines_mask)."""
+    (ctas_per_sm, grab, order_policy, lines_mask, launch_mode)."""
     if cache and key and os.path.exists(cache):
         with open(cache) as f:
             got = json.load(f).get(key)
         if got:
-            c, g, o, m = got['best']
+            c, g, o, m, lm = got['best']
             ens.tune_contraction(m)
             ens.tune(c, g, o)
+            ens.set_launch_mode(lm)
             return tuple(got['best']), got['table']
     table = []
     mask = 0x30  # orders 4 and 5 line-owner: the library's default
@@ -69,8 +73,13 @@ def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), 
         ms = _time_ensemble(ens, steps)
         table.append({'stage': 'schedule', 'ctas_per_sm': c, 'grab': g, 'order_policy': o, 'ms_per_step': ms})
     best = min((r for r in table if r['stage'] == 'schedule'), key=lambda r: r['ms_per_step'])
-    b = (best['ctas_per_sm'], best['grab'], best['order_policy'], mask)
-    ens.tune(*b[:3])
+    ens.tune(best['ctas_per_sm'], best['grab'], best['order_policy'])
+    ens.set_launch_mode(1)
+    ms = _time_ensemble(ens, steps)
+    table.append({'stage': 'launch_mode', 'launch_mode': 1, 'ms_per_step': ms})
+    mode = 1 if ms < best['ms_per_step'] else 0
+    ens.set_launch_mode(mode)
+    b = (best['ctas_per_sm'], best['grab'], best['order_policy'], mask, mode)
     if cache and key:
         data = {}
         if os.path.exists(cache):

@@ -181,6 +181,63 @@ __device__ __forceinline__ void run_corr(SolveDev& sv, int block, double* smem) 
   }
 }
 
+// end of a step for one solve: time, step count, next dt, step budget
+__device__ __forceinline__ void ens_commit(SolveDev& sv) {
+  if (!sv.active) return;
+  if (sv.nan_flag) {
+    // this step produced a non-finite state: the solve stops here (not
+    // counted as a step) and is reported failed; the others go on
+    sv.active = 0;
+    return;
+  }
+  sv.time += sv.dt;
+  sv.steps_done += 1;
+  if (sv.dt_policy == 2) {
+    sv.dt = sv.dt_fixed;
+  } else {
+    sv.dt = __longlong_as_double((long long)sv.dt_next);
+    sv.dt_next = 0x7FF0000000000000ULL;
+  }
+  if (sv.steps_left > 0) {
+    sv.steps_left -= 1;
+    if (sv.steps_left == 0) sv.active = 0;
+  }
+}
+
+// Per-order launch mode: one CTA per work item of one order (the items of
+// an order are contiguous from `first`), each launch with that order's own
+// shared memory and occupancy; then a commit launch over the solves.
+template <int N, int PREC, bool LINES>
+__global__ void __launch_bounds__(kEnsNT) k_ens_pred_order(EnsArgs a, int first) {
+  extern __shared__ double smem[];
+  const WorkItem it = a.items[first + blockIdx.x];
+  const SolveDev& sv = a.solves[it.solve];
+  if (!sv.active) return;  // uniform across the CTA
+  if (sv.pde == EXA_PDE_EULER_PLANAR) ens_pred<N, true, PREC, LINES>(&sv, it.block, smem, a.precision);
+  else ens_pred<N, false, PREC, LINES>(&sv, it.block, smem, a.precision);
+}
+
+template <int N>
+__global__ void __launch_bounds__(kEnsNT) k_ens_corr_order(EnsArgs a, int first) {
+  extern __shared__ double smem[];
+  const WorkItem it = a.items[first + blockIdx.x];
+  SolveDev& sv = a.solves[it.solve];
+  if (!sv.active) return;
+  if (sv.pde == EXA_PDE_EULER_PLANAR) ens_corr<N, true>(&sv, it.block, smem);
+  else ens_corr<N, false>(&sv, it.block, smem);
+}
+
+__global__ void k_ens_commit(EnsArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.nsolves) ens_commit(a.solves[s]);
+}
+
+template <int N, int PREC, bool LINES>
+constexpr int ens_pred_smem() {
+  return LINES ? (PREC ? LineShape<2, N>::SM_DOUBLES : Fp64LineShape<2, N>::SM_DOUBLES)
+               : (PREC ? MixShape<2, N>::SM_DOUBLES : PredShape<2, N, 0>::SM_DOUBLES);
+}
+
 template <int PREC>
 __global__ void __launch_bounds__(kEnsNT) k_ensemble_step(EnsArgs a) {
   cg::grid_group grid = cg::this_grid();
@@ -207,28 +264,7 @@ __global__ void __launch_bounds__(kEnsNT) k_ensemble_step(EnsArgs a) {
   }
   // phase 3: commit every active solve
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int s = gtid; s < a.nsolves; s += gridDim.x * blockDim.x) {
-    SolveDev& sv = a.solves[s];
-    if (!sv.active) continue;
-    if (sv.nan_flag) {
-      // this step produced a non-finite state: the solve stops here (not
-      // counted as a step) and is reported failed; the others go on
-      sv.active = 0;
-      continue;
-    }
-    sv.time += sv.dt;
-    sv.steps_done += 1;
-    if (sv.dt_policy == 2) {
-      sv.dt = sv.dt_fixed;
-    } else {
-      sv.dt = __longlong_as_double((long long)sv.dt_next);
-      sv.dt_next = 0x7FF0000000000000ULL;
-    }
-    if (sv.steps_left > 0) {
-      sv.steps_left -= 1;
-      if (sv.steps_left == 0) sv.active = 0;
-    }
-  }
+  for (int s = gtid; s < a.nsolves; s += gridDim.x * blockDim.x) ens_commit(a.solves[s]);
   if (gtid == 0) {
     a.ctr[0] = 0;
     a.ctr[1] = 0;
@@ -282,6 +318,11 @@ struct exa_ensemble {
   // tuning (exa_ensemble_tune): CTAs per SM, items per grab, order policy
   int ctas_per_sm = 0, grab = 1, order_policy = 0;
   int lines_mask = kEnsLinesDefault;  // per order: line-owner (bit set) or node-gather contraction
+  // launch mode (exa_ensemble_set_launch_mode): 0 one persistent cooperative
+  // launch per step; 1 per-order launches (items of an order contiguous)
+  int mode = 0;
+  int order_first[6] = {0, 0, 0, 0, 0, 0}, order_count[6] = {0, 0, 0, 0, 0, 0};
+  bool order_attrs = false;
   int grid = 0;
   std::mutex mu;
 };
@@ -360,10 +401,16 @@ static exa_status_t rebuild_items(exa_ensemble* e) {
     const long nb = (e->host[s].ncells + cells_per_block(e->host[s].order) - 1) / cells_per_block(e->host[s].order);
     for (long b = 0; b < nb; b++) items.push_back(WorkItem{s, (int)b});
   }
-  if (e->order_policy == 0) {
+  if (e->order_policy == 0 || e->mode == 1) {
     std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
       return e->host[a.solve].order > e->host[b.solve].order;
     });
+  }
+  for (int n = 0; n < 6; n++) e->order_first[n] = e->order_count[n] = 0;
+  for (int i = 0; i < (int)items.size(); i++) {
+    const int n = e->host[items[i].solve].order;
+    if (e->order_count[n] == 0) e->order_first[n] = i;
+    e->order_count[n]++;
   }
   if ((int)items.size() > e->items_cap) {
     if (e->d_items) cudaFree(e->d_items);
@@ -390,6 +437,64 @@ static exa_status_t rebuild_items(exa_ensemble* e) {
   return EXA_OK;
 }
 
+template <int N, int PREC>
+static cudaError_t set_order_attrs() {
+  cudaError_t e = cudaFuncSetAttribute(k_ens_pred_order<N, PREC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(double) * ens_pred_smem<N, PREC, true>()));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ens_pred_order<N, PREC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * ens_pred_smem<N, PREC, false>()));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_ens_corr_order<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(sizeof(double) * CorrShapeSmem<2, N>::value));
+  return e;
+}
+
+template <int N, int PREC>
+static void launch_pred_order(const EnsArgs& a, const exa_ensemble* e, cudaStream_t st) {
+  const int cnt = e->order_count[N];
+  if (cnt == 0) return;
+  if ((e->lines_mask >> N) & 1)
+    k_ens_pred_order<N, PREC, true><<<cnt, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, true>(), st>>>(
+        a, e->order_first[N]);
+  else
+    k_ens_pred_order<N, PREC, false><<<cnt, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, false>(), st>>>(
+        a, e->order_first[N]);
+  count_launch();
+}
+
+template <int N>
+static void launch_corr_order(const EnsArgs& a, const exa_ensemble* e, cudaStream_t st) {
+  const int cnt = e->order_count[N];
+  if (cnt == 0) return;
+  k_ens_corr_order<N><<<cnt, kEnsNT, sizeof(double) * CorrShapeSmem<2, N>::value, st>>>(a, e->order_first[N]);
+  count_launch();
+}
+
+template <int PREC>
+static exa_status_t launch_step_orders(exa_ensemble* e, const EnsArgs& a) {
+  if (!e->order_attrs) {
+    cudaError_t err = set_order_attrs<2, PREC>();
+    if (err == cudaSuccess) err = set_order_attrs<3, PREC>();
+    if (err == cudaSuccess) err = set_order_attrs<4, PREC>();
+    if (err == cudaSuccess) err = set_order_attrs<5, PREC>();
+    if (err != cudaSuccess) return cuda_status(err, "ensemble per-order attributes");
+    e->order_attrs = true;
+  }
+  // costly orders first, as the persistent schedule's default
+  launch_pred_order<5, PREC>(a, e, e->st);
+  launch_pred_order<4, PREC>(a, e, e->st);
+  launch_pred_order<3, PREC>(a, e, e->st);
+  launch_pred_order<2, PREC>(a, e, e->st);
+  launch_corr_order<5>(a, e, e->st);
+  launch_corr_order<4>(a, e, e->st);
+  launch_corr_order<3>(a, e, e->st);
+  launch_corr_order<2>(a, e, e->st);
+  k_ens_commit<<<(a.nsolves + 127) / 128, 128, 0, e->st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "ensemble per-order launches");
+}
+
 static exa_status_t launch_step(exa_ensemble* e) {
   EnsArgs a;
   a.solves = e->d_solves;
@@ -400,6 +505,8 @@ static exa_status_t launch_step(exa_ensemble* e) {
   a.ctr = e->d_ctr;
   a.precision = e->precision;
   a.lines_mask = e->lines_mask;
+  if (e->mode == 1)
+    return e->precision == EXA_PREC_MIXED ? launch_step_orders<1>(e, a) : launch_step_orders<0>(e, a);
   void* args[] = {&a};
   const size_t smem = sizeof(double) * kEnsSmemDoubles;
   cudaError_t err;
@@ -632,6 +739,15 @@ exa_status_t exa_ensemble_tune_contraction(exa_ensemble* e, int lines_mask) {
   cudaStreamSynchronize(e->st);
   e->lines_mask = lines_mask;
   e->dirty = true;  // the step graph holds the kernel arguments
+  return EXA_OK;
+}
+
+exa_status_t exa_ensemble_set_launch_mode(exa_ensemble* e, int mode) {
+  if (!e || mode < 0 || mode > 1) return set_error(EXA_EINVAL, "launch mode: 0 persistent, 1 per order");
+  std::lock_guard<std::mutex> lk(e->mu);
+  cudaStreamSynchronize(e->st);
+  e->mode = mode;
+  e->dirty = true;  // item order and the step graph
   return EXA_OK;
 }
 

@@ -64,6 +64,10 @@ class Ensemble:
         """Per order N: bit N set = line-owner contraction, clear = node-gather."""
         call('exa_ensemble_tune_contraction', self.h, int(lines_mask))
 
+    def set_launch_mode(self, mode):
+        """0: one persistent launch per step; 1: one launch per order and phase."""
+        call('exa_ensemble_set_launch_mode', self.h, int(mode))
+
     def synchronize(self):
         call('exa_ensemble_synchronize', self.h)
 

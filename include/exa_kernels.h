@@ -588,6 +588,11 @@ exa_status_t exa_ensemble_tune(exa_ensemble* e, int ctas_per_sm, int grab, int o
  * of lines_mask set = line-owner contraction, clear = node-gather (default:
  * orders 4 and 5 line-owner); results agree to rounding */
 exa_status_t exa_ensemble_tune_contraction(exa_ensemble* e, int lines_mask);
+/* launch form of a step: 0 (default) one persistent cooperative launch
+ * (work items taken from an atomic counter, grid barriers between the
+ * phases); 1 one launch per order and phase (each with that order's own
+ * shared memory and occupancy) and a commit launch, the same arithmetic */
+exa_status_t exa_ensemble_set_launch_mode(exa_ensemble* e, int mode);
 exa_status_t exa_ensemble_synchronize(exa_ensemble* e);
 exa_status_t exa_ensemble_stream(exa_ensemble* e, void** stream);
 exa_status_t exa_ensemble_get_state(exa_ensemble* e, int slot, double* host_luh);

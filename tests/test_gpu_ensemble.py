@@ -138,8 +138,35 @@ def test_contraction_choice_agrees_and_autotuner_applies_it():
     for m in mix:
         c.add(cfg(*m))
     best, table = tune_ensemble(c, steps=1, ctas=(1,), grabs=(1, 2), orders=(0,))
-    assert len(best) == 4 and best[3] & ~0x3C == 0
+    assert len(best) == 5 and best[3] & ~0x3C == 0 and best[4] in (0, 1)
     assert sum(1 for r in table if r['stage'] == 'contraction') == 1 + len({m[0] for m in mix})
     c.step(2)
     assert not c.status()['nan'].any()
     c.destroy()
+
+
+@pytest.mark.parametrize('precision', [E.PREC_FP64, E.PREC_MIXED])
+def test_per_order_launches_equal_persistent(precision):
+    """One launch per order and phase gives the solves of the persistent
+    launch bit for bit (the same block functions on the same data), with
+    step budgets, graph replay and a solve added mid-run."""
+    a = E.Ensemble(16, 1 << 28, precision=precision)
+    b = E.Ensemble(16, 1 << 28, precision=precision)
+    b.set_launch_mode(1)
+    for ens in (a, b):
+        ens.use_graph(True)
+        for m, k in zip(MIX, [6, 3, -1, 5, 4, 6]):
+            ens.add(cfg(*m), steps=k)
+    for k in range(6):
+        for ens in (a, b):
+            ens.step(1)
+            ens.status()
+        if k == 2:
+            for ens in (a, b):
+                ens.add(cfg(3, (10, 12), 0, 5.0, E.PDE_EULER, 77), steps=3)
+    sa, sb = a.status(), b.status()
+    assert np.array_equal(sa['steps'], sb['steps']) and np.array_equal(sa['time'], sb['time'])
+    for sl in a.cfgs:
+        assert np.array_equal(a.get_state(sl), b.get_state(sl)), sl
+    a.destroy()
+    b.destroy()
