@@ -191,16 +191,21 @@ def reference_step_check(ctx, state):
     kind = 'reference' if R is not None else 'port'
     nn = np.array([n, n, n], dtype=np.int32)
     dx = np.full(3, 1.0 / n)
+    def ref_step(u):
+        if R is not None:
+            return R.ref_grid_step(order, nn, dx, u, 0, 0.0, cores)
+        return O.lib().orc_aderdg_grid_step(3, order, 0, nn, dx, u, 0, 0.9, 0.0, None, cores)
     ref = np.ascontiguousarray(state).copy()
+    dt_ref = ref_step(ref)  # the step the GPU is compared with (also the warm-up)
+    warm = ref.copy()
     t0 = time.perf_counter()
-    if R is not None:
-        dt_ref = R.ref_grid_step(order, nn, dx, ref, 0, 0.0, cores)
-    else:
-        dt_ref = O.lib().orc_aderdg_grid_step(3, order, 0, nn, dx, ref, 0, 0.9, 0.0, None, cores)
+    ref_step(warm)
     t = time.perf_counter() - t0
+    del warm
     cpu = {'value': n ** 3 / t, 'unit': 'cell-updates/s', 'cores': cores, 'kind': kind,
            'sample': 'one whole %d^3 grid step (dt + predictor + volume integral + Riemann + surface integral + '
-                     'update) from the GPU state after the timed steps' % n}
+                     'update), the second from the GPU state after the timed steps (the first, untimed, is the '
+                     'step the GPU steps are compared with)' % n}
     parity = {'reference': kind, 'from': 'GPU state after warm-up + timed steps, one step on each side'}
     nrm2, nrmi = float(np.linalg.norm(ref)), float(np.abs(ref).max())
     for name, prec in (('fp64', E.PREC_FP64), ('mixed', E.PREC_MIXED)):
@@ -316,6 +321,8 @@ def main():
     ap.add_argument('--no-extras', action='store_true', help='grid workload: skip the ensemble and serving summaries')
     ap.add_argument('--rates', default='', help='serving: comma-separated offered rates (req/s)')
     ap.add_argument('--serving-seconds', type=float, default=20.0, help='serving: seconds of arrivals per rate')
+    ap.add_argument('--serving-mode', type=int, default=0, help='serving: ADER-DG launch form (0 persistent, 1 per order)')
+    ap.add_argument('--serving-no-graph', action='store_true', help='serving: direct launches instead of graph replay')
     ap.add_argument('--mixed-variant', type=int, default=0,
                     help='contraction of the mixed predictor (tuning key 2): 0 default, 1 node-gather, '
                          '2 line-owner FP32, 3 tensor cores (3D N=4)')
@@ -634,7 +641,7 @@ def ensemble_summary(args, rank):
     a = _ap.Namespace(**vars(args))
     a.steps, a.warmup = 10, 3
     out = ensemble_measure(a, rank, None)
-    keep = ('value', 'ms_per_step', 'cells', 'launches_per_step', 'tuned')
+    keep = ('value', 'ms_per_step', 'cells', 'launches_per_step', 'tuned', 'form', 'per_order_launches')
     res = {k: {kk: out[k][kk] for kk in keep if kk in out[k]} for k in ('fp64', 'mixed')}
     res['mixed']['max_rel_l2_vs_fp64_first16'] = out['mixed'].get('max_rel_l2_vs_fp64_first16')
     res['mixed_speedup'] = out['mixed']['value'] / out['fp64']['value']
@@ -702,30 +709,43 @@ def ensemble_measure(args, rank, dist):
         ens = E.Ensemble(len(cfgs), arena, precision=prec)
         for c in cfgs:
             assert ens.add(c) is not None
-        best, table = tune_ensemble(ens, steps=3)
+        # the specified form first: one persistent launch per step, its
+        # contraction per order and schedule autotuned
+        best, table = tune_ensemble(ens, steps=3, modes=(0,))
         ens.use_graph(True)
-        ens.step(args.warmup)
-        ens.synchronize()
-        st0 = ens.status()
-        if dist:
-            dist.barrier()
-        t = Timer()
-        s = ens.stream()
-        l0 = E.launch_count()
-        t.start(s)
-        ens.step(args.steps)
-        t.stop(s)
-        ms = t.elapsed_ms()
-        launches = E.launch_count() - l0
-        st1 = ens.status()
+
+        def timed():
+            ens.step(args.warmup)
+            ens.synchronize()
+            st0 = ens.status()
+            if dist:
+                dist.barrier()
+            t = Timer()
+            s = ens.stream()
+            l0 = E.launch_count()
+            t.start(s)
+            ens.step(args.steps)
+            t.stop(s)
+            ms = t.elapsed_ms()
+            launches = E.launch_count() - l0
+            st1 = ens.status()
+            steps_done = (st1['steps'] - st0['steps']).astype(np.int64)
+            updates = sum(int(steps_done[sl]) * c.n[0] * c.n[1] for sl, c in ens.cfgs.items())
+            return updates / (ms * 1e-3), ms / args.steps, launches / args.steps
+        value, ms_step, lps = timed()
         cells = ens.active_cells()
-        steps_done = (st1['steps'] - st0['steps']).astype(np.int64)
-        updates = sum(int(steps_done[sl]) * c.n[0] * c.n[1] for sl, c in ens.cfgs.items())
-        out[prec_name] = {'value': updates / (ms * 1e-3), 'ms_per_step': ms / args.steps, 'cells': cells,
-                          'launches_per_step': launches / args.steps, 'tuned': {'ctas_per_sm': best[0],
-                          'grab': best[1], 'order_policy': best[2], 'line_owner_orders':
-                          [n for n in range(2, 6) if (best[3] >> n) & 1],
-                          'launch_mode': 'per order' if best[4] else 'persistent'}, 'tuning_table': table}
+        # the same step as one launch per order and phase (replayed as one graph)
+        ens.set_launch_mode(1)
+        v1, ms1, lps1 = timed()
+        ens.set_launch_mode(0)
+        out[prec_name] = {'value': value, 'ms_per_step': ms_step, 'cells': cells, 'launches_per_step': lps,
+                          'form': 'one persistent cooperative launch per step, CUDA-graph replay',
+                          'tuned': {'ctas_per_sm': best[0], 'grab': best[1], 'order_policy': best[2],
+                                    'line_owner_orders': [n for n in range(2, 6) if (best[3] >> n) & 1]},
+                          'tuning_table': table,
+                          'per_order_launches': {'value': v1, 'ms_per_step': ms1, 'graph_launches_per_step': lps1,
+                                                 'speedup_vs_persistent': v1 / value,
+                                                 'form': 'one launch per order and phase + commit, one graph'}}
         if prec_name == 'fp64':
             ref_states = {sl: ens.get_state(sl) for sl in list(ens.cfgs)[:16]}
         else:
@@ -1153,6 +1173,7 @@ def run_serving(args, rank, world, dist):
     E.lib().exa_set_device(int(os.environ.get('LOCAL_RANK', '0')))
     budget = 64 << 30
     srv = S.Server(budget, max_requests=4096)
+    srv.tune(args.serving_mode, not args.serving_no_graph)
     # warm-up: a few small requests through every code path
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
@@ -1174,6 +1195,8 @@ def run_serving(args, rank, world, dist):
                            'dg': 'order U{2..5}, side log-U[9,243], steps U{20..200}',
                            'fv': 'MUSCL-Hancock, side log-U[64,1024], steps U{20..200}',
                            'loop': 'exa_server_run (C++), FV patches batched per tick',
+                           'dg_launch': ('per order' if args.serving_mode else 'persistent') +
+                                        (', direct' if args.serving_no_graph else ', graph'),
                            'hbm_budget_gb': budget / 2 ** 30}}
         print(json.dumps(line), flush=True)
     if dist:

@@ -219,6 +219,7 @@ SIGNATURES = {
     'exa_server_result': (i32, [vp, u64, vp, C.POINTER(f64), C.POINTER(C.c_longlong)]),
     'exa_server_info': (i32, [vp, C.POINTER(i32), C.POINTER(C.c_long), C.POINTER(sz)]),
     'exa_server_run': (i32, [vp, vp, vp, i32, f64, vp, C.POINTER(u64)]),
+    'exa_server_tune': (i32, [vp, i32, i32]),
     'exa_server_device_state': (i32, [vp, u64, C.POINTER(vp)]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),

@@ -25,8 +25,8 @@ def _time_ensemble(ens, steps):
     return t.elapsed_ms() / steps
 
 
-def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), contraction=True, cache=None,
-                  key=None):
+def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), contraction=True, modes=(0, 1),
+                  cache=None, key=None):
     """Picks the ensemble's knobs by timing `ens` itself (which advances
     while being measured):
 
@@ -38,8 +38,8 @@ def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), 
        blocks of cells) x work order (costly orders first / solve order),
        every combination timed.
 
-    3. the launch form: the best persistent schedule against one launch per
-       order and phase (exa_ensemble_set_launch_mode).
+    3. the launch form (among `modes`): the best persistent schedule against
+       one launch per order and phase (exa_ensemble_set_launch_mode).
 
     Applies the fastest and returns (best, table), best =
     (ctas_per_sm, grab, order_policy, lines_mask, launch_mode)."""
@@ -74,10 +74,12 @@ def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), 
         table.append({'stage': 'schedule', 'ctas_per_sm': c, 'grab': g, 'order_policy': o, 'ms_per_step': ms})
     best = min((r for r in table if r['stage'] == 'schedule'), key=lambda r: r['ms_per_step'])
     ens.tune(best['ctas_per_sm'], best['grab'], best['order_policy'])
-    ens.set_launch_mode(1)
-    ms = _time_ensemble(ens, steps)
-    table.append({'stage': 'launch_mode', 'launch_mode': 1, 'ms_per_step': ms})
-    mode = 1 if ms < best['ms_per_step'] else 0
+    mode = 0
+    if 1 in modes:
+        ens.set_launch_mode(1)
+        ms = _time_ensemble(ens, steps)
+        table.append({'stage': 'launch_mode', 'launch_mode': 1, 'ms_per_step': ms})
+        mode = 1 if (ms < best['ms_per_step'] or 0 not in modes) else 0
     ens.set_launch_mode(mode)
     b = (best['ctas_per_sm'], best['grab'], best['order_policy'], mask, mode)
     if cache and key:

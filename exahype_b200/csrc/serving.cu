@@ -326,6 +326,13 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
   return st;
 }
 
+exa_status_t exa_server_tune(exa_server* s, int launch_mode, int use_graph) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (exa_status_t st = exa_ensemble_set_launch_mode(s->ens, launch_mode)) return st;
+  return exa_ensemble_use_graph(s->ens, use_graph);
+}
+
 exa_status_t exa_server_device_state(exa_server* s, uint64_t id, double** luh_dev) {
   if (!s || !luh_dev) return set_error(EXA_EINVAL, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);

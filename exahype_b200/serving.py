@@ -88,6 +88,10 @@ class Server:
             return out, t.value, steps.value, st
         return out, t.value, steps.value
 
+    def tune(self, launch_mode=0, use_graph=True):
+        """ADER-DG launch form of a tick (0 persistent, 1 per order) and graph replay."""
+        call('exa_server_tune', self.h, int(launch_mode), int(bool(use_graph)))
+
     def device_state_ptr(self, rid):
         p = C.c_void_p()
         call('exa_server_device_state', self.h, C.c_uint64(rid), C.byref(p))
