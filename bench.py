@@ -321,7 +321,7 @@ def main():
     ap.add_argument('--no-extras', action='store_true', help='grid workload: skip the ensemble and serving summaries')
     ap.add_argument('--rates', default='', help='serving: comma-separated offered rates (req/s)')
     ap.add_argument('--serving-seconds', type=float, default=20.0, help='serving: seconds of arrivals per rate')
-    ap.add_argument('--serving-mode', type=int, default=0, help='serving: ADER-DG launch form (0 persistent, 1 per order)')
+    ap.add_argument('--serving-mode', type=int, default=1, help='serving: ADER-DG launch form (0 persistent, 1 per order: the default)')
     ap.add_argument('--serving-no-graph', action='store_true', help='serving: direct launches instead of graph replay')
     ap.add_argument('--mixed-variant', type=int, default=0,
                     help='contraction of the mixed predictor (tuning key 2): 0 default, 1 node-gather, '
@@ -651,13 +651,13 @@ def ensemble_summary(args, rank):
 
 
 def serving_summary(args):
-    """One steady-state serving stream (150 req/s, 10 s of arrivals, the
+    """One steady-state serving stream (175 req/s, 10 s of arrivals, the
     highest rate measured to be sustained) for the default run's line."""
     from exahype_b200 import serving as S
     srv = S.Server(64 << 30, max_requests=4096)
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
-    r = serving_stream(S, srv, 150.0, 10.0, args.seed + 500, args.dg_fraction)
+    r = serving_stream(S, srv, 175.0, 10.0, args.seed + 500, args.dg_fraction)
     srv.destroy()
     r['workload'] = ('Poisson stream, 25 % ADER-DG 2D (N 2..5, 9^2..243^2) and 75 % FV MUSCL-Hancock '
                      '(64^2..1024^2), 20..200 steps each, C++ request loop')

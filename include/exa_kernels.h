@@ -639,7 +639,7 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
 /* how the ADER-DG requests of a tick are launched: the ensemble's launch
  * form (exa_ensemble_set_launch_mode) and whether a tick's launches replay
  * a CUDA graph (re-captured whenever the set of requests changes; default
- * 0 and 1) */
+ * 1 and 1: one launch per order and phase, graph replay) */
 exa_status_t exa_server_tune(exa_server* s, int launch_mode, int use_graph);
 /* device pointer of a live request's current state (ADER-DG: the solve's
  * luh; FV: the patch buffer that holds the state), for zero-copy inspection
