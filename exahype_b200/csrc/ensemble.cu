@@ -207,10 +207,25 @@ __device__ __forceinline__ void ens_commit(SolveDev& sv) {
 // Per-order launch mode: one CTA per work item of one order (the items of
 // an order are contiguous from `first`), each launch with that order's own
 // shared memory and occupancy; then a commit launch over the solves.
+// CTA blockIdx.x of an order's launch -> (solve, block of that solve): the
+// order's segments a.items[first .. first + nseg) hold each solve's first
+// block in the order's block numbering (ascending)
+__device__ __forceinline__ WorkItem ens_segment_item(const EnsArgs& a, int first, int nseg) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (a.items[first + mid].block <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  const WorkItem seg = a.items[first + lo];
+  return WorkItem{seg.solve, b - seg.block};
+}
+
 template <int N, int PREC, bool LINES>
-__global__ void __launch_bounds__(kEnsNT) k_ens_pred_order(EnsArgs a, int first) {
+__global__ void __launch_bounds__(kEnsNT) k_ens_pred_order(EnsArgs a, int first, int nseg) {
   extern __shared__ double smem[];
-  const WorkItem it = a.items[first + blockIdx.x];
+  const WorkItem it = ens_segment_item(a, first, nseg);
   const SolveDev& sv = a.solves[it.solve];
   if (!sv.active) return;  // uniform across the CTA
   if (sv.pde == EXA_PDE_EULER_PLANAR) ens_pred<N, true, PREC, LINES>(&sv, it.block, smem, a.precision);
@@ -218,9 +233,9 @@ __global__ void __launch_bounds__(kEnsNT) k_ens_pred_order(EnsArgs a, int first)
 }
 
 template <int N>
-__global__ void __launch_bounds__(kEnsNT) k_ens_corr_order(EnsArgs a, int first) {
+__global__ void __launch_bounds__(kEnsNT) k_ens_corr_order(EnsArgs a, int first, int nseg) {
   extern __shared__ double smem[];
-  const WorkItem it = a.items[first + blockIdx.x];
+  const WorkItem it = ens_segment_item(a, first, nseg);
   SolveDev& sv = a.solves[it.solve];
   if (!sv.active) return;
   if (sv.pde == EXA_PDE_EULER_PLANAR) ens_corr<N, true>(&sv, it.block, smem);
@@ -321,7 +336,8 @@ struct exa_ensemble {
   // launch mode (exa_ensemble_set_launch_mode): 0 one persistent cooperative
   // launch per step; 1 per-order launches (items of an order contiguous)
   int mode = 0;
-  int order_first[6] = {0, 0, 0, 0, 0, 0}, order_count[6] = {0, 0, 0, 0, 0, 0};
+  int order_first[6] = {0, 0, 0, 0, 0, 0}, order_count[6] = {0, 0, 0, 0, 0, 0};  // segments per order
+  long order_blocks[6] = {0, 0, 0, 0, 0, 0};  // blocks of cells per order (per-order launches)
   bool order_attrs = false;
   int grid = 0;
   std::mutex mu;
@@ -391,27 +407,7 @@ static int cells_per_block(int order) {
   return kEnsNT / g > 0 ? kEnsNT / g : 1;
 }
 
-static exa_status_t rebuild_items(exa_ensemble* e) {
-  // one work item per block of cells of each active solve; costly orders
-  // first (longest-processing-time order) unless the policy interleaves
-  std::vector<WorkItem> items;
-  std::vector<int> order_of;
-  for (int s = 0; s < e->max_solves; s++) {
-    if (!e->used[s] || !e->host[s].active) continue;
-    const long nb = (e->host[s].ncells + cells_per_block(e->host[s].order) - 1) / cells_per_block(e->host[s].order);
-    for (long b = 0; b < nb; b++) items.push_back(WorkItem{s, (int)b});
-  }
-  if (e->order_policy == 0 || e->mode == 1) {
-    std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
-      return e->host[a.solve].order > e->host[b.solve].order;
-    });
-  }
-  for (int n = 0; n < 6; n++) e->order_first[n] = e->order_count[n] = 0;
-  for (int i = 0; i < (int)items.size(); i++) {
-    const int n = e->host[items[i].solve].order;
-    if (e->order_count[n] == 0) e->order_first[n] = i;
-    e->order_count[n]++;
-  }
+static exa_status_t upload_items(exa_ensemble* e, const std::vector<WorkItem>& items) {
   if ((int)items.size() > e->items_cap) {
     if (e->d_items) cudaFree(e->d_items);
     e->d_items = nullptr;
@@ -424,11 +420,52 @@ static exa_status_t rebuild_items(exa_ensemble* e) {
   }
   e->nitems = (int)items.size();
   if (e->nitems) {
+    // stream-ordered after the launches that read the previous list; a copy
+    // from pageable memory is staged before the call returns
     cudaError_t err = cudaMemcpyAsync(e->d_items, items.data(), sizeof(WorkItem) * e->nitems,
                                       cudaMemcpyHostToDevice, e->st);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(e->st);
     if (err != cudaSuccess) return cuda_status(err, "upload work items");
   }
+  return EXA_OK;
+}
+
+static exa_status_t rebuild_items(exa_ensemble* e) {
+  std::vector<WorkItem> items;
+  for (int n = 0; n < 6; n++) e->order_first[n] = e->order_count[n] = e->order_blocks[n] = 0;
+  if (e->mode == 1) {
+    // per-order launches: per order, one segment per active solve holding
+    // the order's running block count at its first block (block field);
+    // CTA b of the order's launch finds its segment by binary search.  Work
+    // on the host is per solve, not per block.
+    std::vector<WorkItem> per[6];
+    for (int s = 0; s < e->max_solves; s++) {
+      if (!e->used[s] || !e->host[s].active) continue;
+      const int n = e->host[s].order;
+      const long nb = (e->host[s].ncells + cells_per_block(n) - 1) / cells_per_block(n);
+      per[n].push_back(WorkItem{s, (int)e->order_blocks[n]});
+      e->order_blocks[n] += nb;
+    }
+    for (int n = 5; n >= 2; n--) {
+      e->order_first[n] = (int)items.size();
+      e->order_count[n] = (int)per[n].size();
+      items.insert(items.end(), per[n].begin(), per[n].end());
+    }
+  } else {
+    // persistent launch: one work item per block of cells of each active
+    // solve; costly orders first (longest-processing-time order) unless the
+    // policy interleaves
+    for (int s = 0; s < e->max_solves; s++) {
+      if (!e->used[s] || !e->host[s].active) continue;
+      const long nb = (e->host[s].ncells + cells_per_block(e->host[s].order) - 1) / cells_per_block(e->host[s].order);
+      for (long b = 0; b < nb; b++) items.push_back(WorkItem{s, (int)b});
+    }
+    if (e->order_policy == 0) {
+      std::stable_sort(items.begin(), items.end(), [&](const WorkItem& a, const WorkItem& b) {
+        return e->host[a.solve].order > e->host[b.solve].order;
+      });
+    }
+  }
+  if (exa_status_t st = upload_items(e, items)) return st;
   if (e->graph) {
     cudaGraphExecDestroy(e->graph);
     e->graph = nullptr;
@@ -452,22 +489,23 @@ static cudaError_t set_order_attrs() {
 
 template <int N, int PREC>
 static void launch_pred_order(const EnsArgs& a, const exa_ensemble* e, cudaStream_t st) {
-  const int cnt = e->order_count[N];
-  if (cnt == 0) return;
+  const long blocks = e->order_blocks[N];
+  if (blocks == 0) return;
   if ((e->lines_mask >> N) & 1)
-    k_ens_pred_order<N, PREC, true><<<cnt, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, true>(), st>>>(
-        a, e->order_first[N]);
+    k_ens_pred_order<N, PREC, true><<<(unsigned)blocks, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, true>(), st>>>(
+        a, e->order_first[N], e->order_count[N]);
   else
-    k_ens_pred_order<N, PREC, false><<<cnt, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, false>(), st>>>(
-        a, e->order_first[N]);
+    k_ens_pred_order<N, PREC, false><<<(unsigned)blocks, kEnsNT, sizeof(double) * ens_pred_smem<N, PREC, false>(),
+                                       st>>>(a, e->order_first[N], e->order_count[N]);
   count_launch();
 }
 
 template <int N>
 static void launch_corr_order(const EnsArgs& a, const exa_ensemble* e, cudaStream_t st) {
-  const int cnt = e->order_count[N];
-  if (cnt == 0) return;
-  k_ens_corr_order<N><<<cnt, kEnsNT, sizeof(double) * CorrShapeSmem<2, N>::value, st>>>(a, e->order_first[N]);
+  const long blocks = e->order_blocks[N];
+  if (blocks == 0) return;
+  k_ens_corr_order<N><<<(unsigned)blocks, kEnsNT, sizeof(double) * CorrShapeSmem<2, N>::value, st>>>(
+      a, e->order_first[N], e->order_count[N]);
   count_launch();
 }
 
