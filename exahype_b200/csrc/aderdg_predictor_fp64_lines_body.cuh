@@ -48,7 +48,7 @@ struct Fp64LineShape {
   static constexpr int X_SIZE = DIM * B * V * NPC;
   static constexpr int LOOP_D = 2 * F_SLICE + X_SIZE;
   static constexpr int CELL_D = ((LOOP_D > M::STAGE_D ? LOOP_D : M::STAGE_D) + 1) & ~1;
-  static constexpr int SM_DOUBLES = CPB * CELL_D + NT / 32 + 1;
+  static constexpr int SM_DOUBLES = CPB * CELL_D + 2 * (NT / 32) + 1;
 };
 
 template <int DIM, int N, bool PLANAR>
@@ -208,12 +208,18 @@ __device__ __forceinline__ void predictor_fp64_lines_block(const PredArgs& a, lo
 #pragma unroll
           for (int m = 0; m < V; m++) fkeep[d][m] = fa[d][m];
     }
-    const double res = group_sum<G>(r2, sred);
+    // one barrier per iteration for the residual; with one cell per CTA
+    // every thread holds the same sum, so the exit needs no vote
+    const double res = group_sum_1b<G, S::NT>(r2, sred, iter);
     if (!conv) {
       it = iter + 1;
       if (res < 1e-7 * 1e-7) conv = true;
     }
-    if (__syncthreads_and(conv || !valid)) break;
+    if constexpr (S::CPB == 1) {
+      if (conv || !valid) break;
+    } else {
+      if (__syncthreads_and(conv || !valid)) break;
+    }
   }
 
   // time averages -> staging, then faces and volume integral

@@ -69,7 +69,7 @@ struct LineShape {
   static constexpr int LOOP_F = 2 * F_SLICE + X_SIZE + BASE_SIZE;
   static constexpr int STAGE_F = 2 * M::STAGE_D;  // FP64 staging (mixed_outputs), in floats
   static constexpr int CELL_F = ((LOOP_F > STAGE_F ? LOOP_F : STAGE_F) + 1) & ~1;  // keep doubles aligned
-  static constexpr int SM_DOUBLES = CPB * CELL_F / 2 + NT / 32 + 1;
+  static constexpr int SM_DOUBLES = CPB * CELL_F / 2 + 2 * (NT / 32) + 1;
 };
 
 template <int DIM, int N, bool PLANAR>
@@ -160,11 +160,18 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
     const float dH = dv[4] + dp;
     const float H1 = H0f + dH;
     const float e = fmaf(-h0f, dv[0], dH);
+    // components 1 and 2 of each direction on the packed FP32 pipe: the
+    // same multiply, fma, multiply as the scalar lines, two lanes at once
+    const float2 m1p = make_float2(m1[0], m1[1]), wp = make_float2(w[0], w[1]), r1p = make_float2(r1, r1);
 #pragma unroll
     for (int j = 0; j < DIM; j++) {
       dF[j][0] = dv[j + 1];
-#pragma unroll
-      for (int k = 0; k < 3; k++) dF[j][k + 1] = fmaf(m0f[j], w[k], dv[j + 1] * m1[k]) * r1;
+      const float2 t = __fmul2_rn(__ffma2_rn(make_float2(m0f[j], m0f[j]), wp,
+                                             __fmul2_rn(make_float2(dv[j + 1], dv[j + 1]), m1p)),
+                                  r1p);
+      dF[j][1] = t.x;
+      dF[j][2] = t.y;
+      dF[j][3] = fmaf(m0f[j], w[2], dv[j + 1] * m1[2]) * r1;
       dF[j][j + 1] += dp;
       dF[j][4] = fmaf(m0f[j], e, dv[j + 1] * H1) * r1;
     }
@@ -237,10 +244,18 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
             for (int m = 0; m < V; m++) sFn[S::flux_addr(d, s, m)] = dF[d][m];
         if (active) {
           const float wn = TF.w[n];
+          const float2 wn2 = make_float2(wn, wn);
 #pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int m = 0; m < V; m++) fa[d][m] = fmaf(wn, dF[d][m], fa[d][m]);
+          for (int d = 0; d < DIM; d++) {
+            // (0,1) and (2,3) on the packed FP32 pipe, bitwise the scalar fmaf
+            const float2 a01 = __ffma2_rn(wn2, make_float2(dF[d][0], dF[d][1]), make_float2(fa[d][0], fa[d][1]));
+            const float2 a23 = __ffma2_rn(wn2, make_float2(dF[d][2], dF[d][3]), make_float2(fa[d][2], fa[d][3]));
+            fa[d][0] = a01.x;
+            fa[d][1] = a01.y;
+            fa[d][2] = a23.x;
+            fa[d][3] = a23.y;
+            fa[d][4] = fmaf(wn, dF[d][4], fa[d][4]);
+          }
           if (iter == 0)  // slices 1..B-1 carry the same deviation
 #pragma unroll
             for (int n2 = 1; n2 < B; n2++)
@@ -330,12 +345,18 @@ __device__ __forceinline__ void predictor_mixed_lines_block(const PredArgs& a, l
 #pragma unroll
           for (int m = 0; m < V; m++) fkeep[d][m] = fa[d][m];
     }
-    const double res = group_sum<G>((double)r2, sred);
+    // one barrier per iteration for the residual; with one cell per CTA
+    // every thread holds the same sum, so the exit needs no vote
+    const double res = group_sum_1b<G, S::NT>((double)r2, sred, iter);
     if (!conv) {
       it = iter + 1;
       if (res < 1e-7 * 1e-7) conv = true;
     }
-    if (__syncthreads_and(conv || !valid)) break;
+    if constexpr (S::CPB == 1) {
+      if (conv || !valid) break;
+    } else {
+      if (__syncthreads_and(conv || !valid)) break;
+    }
   }
 
   // fa holds the weighted flux-deviation sum of the last iteration (the

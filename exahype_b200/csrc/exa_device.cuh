@@ -117,6 +117,32 @@ __device__ __forceinline__ double group_sum(double v, double* sred) {
   }
 }
 
+// group_sum with one barrier, for a loop that calls it once per iteration:
+// the warp partials go to one of two slot sets chosen by the iteration's
+// parity, so the next iteration's writes never meet this iteration's reads
+// (every thread passes this barrier before any thread writes again).  sred
+// needs 2 NT/32 doubles.  Same summation order, so the same bits as
+// group_sum.
+template <int G, int NT>
+__device__ __forceinline__ double group_sum_1b(double v, double* sred, int parity) {
+  constexpr int L = G < 32 ? G : 32;
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if constexpr (G <= 32) {
+    return v;
+  } else {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* slot = sred + (parity & 1) * (NT / 32);
+    if (lane == 0) slot[warp] = v;
+    __syncthreads();
+    const int g0 = (threadIdx.x / G) * (G / 32);
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < G / 32; k++) s += slot[g0 + k];
+    return s;
+  }
+}
+
 template <int G>
 __device__ __forceinline__ double group_min(double v, double* sred) {
   constexpr int L = G < 32 ? G : 32;
