@@ -1153,11 +1153,11 @@ def serving_stream(S, srv, rate, seconds, seed, dg_fraction):
            'latency_growth_last_quarter': growth, 'ticks': res['ticks'], 'wall_s': res['wall'],
            'aggregate_cell_updates_per_s': res['cell_updates'] / res['wall'] if res['wall'] > 0 else 0.0}
     out['drain_after_last_arrival_s'] = last - T
-    # sustained: everything completed, finished within a short drain after
-    # the last arrival, and the latency of the last quarter of the arrivals
-    # did not grow against the third quarter
+    # sustained: everything completed at >= 95 % of the offered rate,
+    # finished within a short drain after the last arrival, and the latency
+    # of the last quarter of the arrivals did not grow against the third
     out['sustained'] = bool(len(comp) == n and last - T <= max(5.0, 0.1 * T) and growth is not None
-                            and growth < 1.5)
+                            and growth < 1.5 and achieved >= 0.95 * rate)
     return out
 
 
