@@ -27,6 +27,7 @@
 #include "exa_device.cuh"
 #include "aderdg_predictor_body.cuh"
 #include "aderdg_predictor_fp64_lines_body.cuh"
+#include "aderdg_predictor_fp64_prog_body.cuh"
 
 namespace exa {
 
@@ -85,6 +86,37 @@ static exa_status_t launch_lines_fp64(const PredArgs& a, cudaStream_t st) {
   return cuda_status(cudaGetLastError(), "k_predictor_lines launch");
 }
 
+// progressive line-owner variant (aderdg_predictor_fp64_prog_body.cuh): 3D,
+// one cell per CTA, 60 KB of shared memory, bounded for 3 CTAs per SM
+template <int DIM, int N, bool PLANAR>
+__global__ void __launch_bounds__(Fp64ProgShape<DIM, N>::NT, 3) k_predictor_prog(PredArgs a) {
+  extern __shared__ double smem[];
+  predictor_fp64_prog_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
+}
+
+template <int DIM, int N>
+static exa_status_t launch_prog_fp64(const PredArgs& a, cudaStream_t st) {
+  using S = Fp64ProgShape<DIM, N>;
+  auto kern = k_predictor_prog<DIM, N, false>;
+  const size_t smem = sizeof(double) * S::SM_DOUBLES;
+  static bool attr_done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_done[dev & 63]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
+    if (e != cudaSuccess) return cuda_status(e, "predictor (progressive) attribute");
+    attr_done[dev & 63] = true;
+  }
+  if (a.ncells <= 0) return EXA_OK;
+  if (a.ncells > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
+  kern<<<(unsigned)a.ncells, S::NT, smem, st>>>(a);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_predictor_prog launch");
+}
+
 template <int DIM, int N>
 static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
                               cudaStream_t st) {
@@ -94,7 +126,10 @@ static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int
   // it measured faster in 2D and 3D (for orders 2-3 the cell has more
   // line tasks than threads and node-gather wins)
   const int variant = tune_get(kTuneFp64Variant, 0);
-  if (d.npar == 0 && !full && (variant == 2 || (variant == 0 && N >= 4))) {
+  // knob 3 = 3: the progressive line-owner form (3D order 4, Euler)
+  if constexpr (DIM == 3 && N == 4)
+    if (d.npar == 0 && !full && variant == 3 && !planar) return launch_prog_fp64<DIM, N>(a, st);
+  if (d.npar == 0 && !full && (variant >= 2 || (variant == 0 && N >= 4))) {
     if (DIM == 3 && planar) return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
     return planar ? launch_lines_fp64<DIM, N, true>(a, st) : launch_lines_fp64<DIM, N, false>(a, st);
   }

@@ -168,12 +168,13 @@ def test_grid_ic_matches_oracle():
     (2, 4, (6, 9), 0, 1, 1, 10),
     (2, 5, (5, 5), 1, 0, 0, 10),
 ])
-@pytest.mark.parametrize('variant', [1, 2])
+@pytest.mark.parametrize('variant', [1, 2, 3])
 def test_grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps, variant):
     """Every step is compared with the oracle stepping the identical input
     state (per-step parity, relative L2 <= 1e-12); a second oracle copy runs
     free for all steps to bound the accumulated drift.  variant (tuning key
-    3): FP64 predictor contraction, 1 = node-gather, 2 = line-owner."""
+    3): FP64 predictor contraction, 1 = node-gather, 2 = line-owner, 3 = the
+    progressive line-owner form (3D order 4; line-owner elsewhere)."""
     E._lib.call('exa_tune_set', 3, variant)
     try:
         _grid_steps_vs_oracle(dim, order, n, kind, planar, policy, steps)
@@ -251,3 +252,32 @@ def test_grid_boundary_rejects_bad_rule():
     with pytest.raises(E.ExaError):
         g.set_boundary((1, 1))  # slab halos need a periodic last dimension
     g.destroy()
+
+
+def test_progressive_fp64_equals_line_owner_bitwise():
+    """The progressive FP64 predictor performs the line-owner kernel's
+    operations in the same order: the same grid, stepped with either, is
+    identical bit for bit (3D order 4, also with a dt four times the stable
+    one, where cells stop at the iteration cap)."""
+    out = []
+    for variant in (2, 3):
+        E._lib.call('exa_tune_set', 3, variant)
+        try:
+            g = E.ADERDGGrid(3, 4, (5, 4, 3))
+            g.init(kind=0, param=5.0, seed=21, noise=1e-3)
+            g.step(4)
+            u0 = O.grid_ic(3, 4, (3, 3, 3), kind=0, param=5.0, seed=22, noise=1e-3)
+            nn = np.full(3, 3, dtype=np.int32)
+            dt4 = 4.0 * O.lib().orc_aderdg_grid_dt(3, 4, 0, nn, np.full(3, 1.0 / 3), u0, 0, 0.9)
+            h = E.ADERDGGrid(3, 4, (3, 3, 3), dt_policy=2, dt_fixed=dt4)
+            h.set_state(u0)
+            h.step(1)
+            out.append((g.get_state(), h.get_state(), g.status()['picard_iters'], h.status()['nonconverged']))
+            g.destroy()
+            h.destroy()
+        finally:
+            E._lib.call('exa_tune_set', 3, 0)
+    a, b = out
+    assert np.isfinite(a[1]).all()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert a[2] == b[2] and a[3] == b[3]
