@@ -121,14 +121,17 @@ template <int DIM, int N>
 static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int full,
                               cudaStream_t st) {
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
-  // knob 3: 1 = node-gather, 2 = line-owner contraction (FP64, not for the
-  // reference-temporaries mode); default: line-owner for orders >= 4, where
-  // it measured faster in 2D and 3D (for orders 2-3 the cell has more
-  // line tasks than threads and node-gather wins)
+  // knob 3: 1 = node-gather, 2 = line-owner contraction, 3 = the
+  // progressive line-owner form (FP64, not for the reference-temporaries
+  // mode); default: progressive for 3D order 4 (Euler; 3 CTAs per SM, it
+  // measured 6.5 % faster than the line-owner kernel at 81^3), line-owner
+  // for the other orders >= 4, where it measured faster in 2D and 3D (for
+  // orders 2-3 the cell has more line tasks than threads and node-gather
+  // wins)
   const int variant = tune_get(kTuneFp64Variant, 0);
-  // knob 3 = 3: the progressive line-owner form (3D order 4, Euler)
   if constexpr (DIM == 3 && N == 4)
-    if (d.npar == 0 && !full && variant == 3 && !planar) return launch_prog_fp64<DIM, N>(a, st);
+    if (d.npar == 0 && !full && (variant == 3 || variant == 0) && !planar)
+      return launch_prog_fp64<DIM, N>(a, st);
   if (d.npar == 0 && !full && (variant >= 2 || (variant == 0 && N >= 4))) {
     if (DIM == 3 && planar) return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
     return planar ? launch_lines_fp64<DIM, N, true>(a, st) : launch_lines_fp64<DIM, N, false>(a, st);

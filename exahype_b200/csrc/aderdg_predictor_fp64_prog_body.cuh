@@ -194,7 +194,9 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
       for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) {
-          const double qn = T.c0[t] * lu[m] - dt * acc[t][m];
+          // luh re-read (read-only path, L1): ten fewer registers across
+          // the slice loop
+          const double qn = T.c0[t] * __ldg(a.luh + cell * (long)NPC * V + s * V + m) - dt * acc[t][m];
           const double dq = q[t][m] - qn;
           r2 += dq * dq;
           acc[t][m] = qn;
