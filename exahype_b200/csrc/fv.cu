@@ -39,11 +39,48 @@ struct FVArgs {
   // optional patch selection of k_fv_patch_small: patches list[0 .. *count)
   const int* list;
   const int* count;
+  // fused steps: a grid of npx x npy patches (one patch: 1 x 1) and its
+  // boundary rule per dimension (EXA_BC_*)
+  int npx, npy, bcx, bcy;
 };
 
 // Periodic index of a cell coordinate of a single patch with ghost width g:
 // ghost coordinates map to the interior cell a ghost fill would copy.
 __device__ __forceinline__ int fv_wrap(int j, int g, int P) { return g + ((j - g) % P + P) % P; }
+
+// Fused steps address the state as one global grid of cells: cell (X, Y),
+// 0 <= X < npx P, 0 <= Y < npy P, is interior cell (X mod P, Y mod P) of
+// patch (X / P, Y / P) (patch-major, x fastest, P^2 interior cells and g
+// ghost layers per patch).  A stencil coordinate outside the domain folds
+// back to the cell that a ghost fill would have copied there: the periodic
+// image, or at a wall the mirror image (ghost k from the face <- interior
+// layer k from the face; FiniteVolumesSolver::mergeWithBoundaryData,
+// kernels/finitevolumes/commons/c/commons.cpph:99-340), and inside the
+// domain a neighbour patch's ghost cell is that neighbour's interior cell
+// (ghostLayerFilling, commons.cpph:337-405).  So a fused step reads no ghost
+// cell and needs no exchange pass.
+__device__ __forceinline__ int fv_fold(int X, int NX, int bc, bool& mirrored) {
+  if (X >= 0 && X < NX) return X;
+  if (bc == 0) return (X % NX + NX) % NX;
+  mirrored = true;
+  return X < 0 ? -1 - X : 2 * NX - 1 - X;
+}
+
+// element offset of in-domain cell (X, Y)
+__device__ __forceinline__ long fv_cell_offset(const FVArgs& a, int X, int Y) {
+  const int px = a.npx == 1 ? 0 : X / a.P, py = a.npy == 1 ? 0 : Y / a.P;
+  const long patch = (long)py * a.npx + px;
+  return (patch * a.S * a.S + (long)(a.g + Y - py * a.P) * a.S + (a.g + X - px * a.P)) * (kV + a.npar);
+}
+
+// element offset of the cell read at stencil coordinate (X, Y); *flip =
+// the momentum component a reflecting wall negates there, else -1
+__device__ __forceinline__ long fv_stencil_offset(const FVArgs& a, int X, int Y, int* flip) {
+  bool mx = false, my = false;
+  const int Xf = fv_fold(X, a.P * a.npx, a.bcx, mx), Yf = fv_fold(Y, a.P * a.npy, a.bcy, my);
+  *flip = (mx && a.bcx == EXA_BC_REFLECT) ? 1 : ((my && a.bcy == EXA_BC_REFLECT) ? 2 : -1);
+  return fv_cell_offset(a, Xf, Yf);
+}
 
 // Fused steps (FUSED = true) of a single periodic patch: the tile is loaded
 // straight from the periodic interior (no ghost fill, no luh_new copy), the
@@ -115,18 +152,21 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
   const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
   const double* luh = a.luh + patch * (long)S * S * D;
   double* out = a.out + patch * (long)S * S * D;
-  const int k0 = pb + bx * FV_TX, j0 = pb + by * FV_TY;
+  // FUSED: global cell coordinates of the patch grid (fv_cell_offset)
+  const int k0 = (FUSED ? 0 : pb) + bx * FV_TX, j0 = (FUSED ? 0 : pb) + by * FV_TY;
   const int tid = threadIdx.x;
   for (int i = tid; i < LY * LX; i += FV_NT) {
     const int r = i / LX, c = i % LX;
-    int j = j0 - 1 + r, k = k0 - 1 + c;
+    const int j = j0 - 1 + r, k = k0 - 1 + c;
     if (FUSED) {
-      j = fv_wrap(j, pb, a.P);
-      k = fv_wrap(k, pb, a.P);
-    }
-    if (j >= 0 && j < S && k >= 0 && k < S)
+      int flip;
+      const double* q = luh + fv_stencil_offset(a, k, j, &flip);
+#pragma unroll
+      for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
+    } else if (j >= 0 && j < S && k >= 0 && k < S) {
 #pragma unroll
       for (int m = 0; m < V; m++) su[i * V + m] = luh[((long)j * S + k) * D + m];
+    }
   }
   __syncthreads();
   // per-cell x fluxes of the cells beside the tile's x faces (rows j < pe,
@@ -150,8 +190,10 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
-    const bool valid = j < pe && k < pe;
+    const bool valid = FUSED ? (j < a.P * a.npy && k < a.P * a.npx) : (j < pe && k < pe);
     double fxl[V], fxr[V], fyb[V], fyt[V];
+    // output cell, addressed before the face fluxes hold their registers
+    double* o = FUSED ? a.out + (valid ? fv_cell_offset(a, k, j) : 0) : out + ((long)j * S + k) * D;
     if (valid) {
       const double* q = &su[((r + 1) * LX + c + 1) * V];
       const double sxl = fv_face_flux(q - V, q, &scx[(r * LX + c) * C], &scx[(r * LX + c + 1) * C], fxl);
@@ -163,7 +205,6 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
         // the division is monotone, so the same value as per face
         dtl = fmin(0.9 / 2 * a.hx / fmax(sxl, sxr), 0.9 / 2 * a.hy / fmax(syb, syt));
       }
-      double* o = out + ((long)j * S + k) * D;
       double un[V];
 #pragma unroll
       for (int m = 0; m < V; m++) {
@@ -187,7 +228,7 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
     }
     // first ghost layer, as the reference's face loops touch it
     if (valid && k0 == pb && c == 0) {
-      double* o = out + ((long)j * S + (pb - 1)) * D;
+      o = out + ((long)j * S + (pb - 1)) * D;
 #pragma unroll
       for (int m = 0; m < V; m++) o[m] -= cx * fxl[m];
     }
@@ -420,16 +461,16 @@ constexpr size_t kMusclSmem =
     sizeof(double) * ((FV_TY + 4) * (FV_TX + 4) * kV + 4 * (FV_TY + 2) * (FV_TX + 2) * kV +
                       FV_TY * (FV_TX + 1) * kV + (FV_TY + 1) * FV_TX * kV + FV_NT / 32);
 
-// --------------------------------------------- periodic single-patch steps
-// Device-resident stepping of one periodic patch (exa_fv_grid, serving):
-// the tile and its halo are loaded straight from the periodic interior,
-// every interior cell evaluates its own four face fluxes (each face is
-// computed by the two cells that share it, from identical inputs, so the
-// result is the same as a shared face flux) -- no flux arrays and one
-// barrier fewer than the tile kernels above, which lets more CTAs share an
-// SM -- and the new state's CFL dt is reduced in the same pass.  The
-// update applies the face contributions in the reference's order (x faces,
-// then y faces).  Ghost cells of the output are not written.
+// ------------------------------------- fused steps of patches and grids
+// Device-resident stepping of one periodic patch (exa_fv_grid, serving) or
+// of a grid of patches (exa_fv_patchgrid): the tile and its halo are loaded
+// through the global cell view (fv_stencil_offset), the MUSCL-Hancock tile
+// lets every interior cell evaluate its own four face fluxes (no flux
+// arrays and one barrier fewer than the tile kernels above, which lets more
+// CTAs share an SM), and the new state's CFL dt is reduced in the same
+// pass.  The update applies the face contributions in the reference's
+// order (x faces, then y faces).  Ghost cells of the output are not
+// written.
 constexpr int FVP_TX = 32, FVP_TY = 8, FVP_NT = FVP_TX * FVP_TY;
 
 template <bool PLANAR>
@@ -451,42 +492,19 @@ __device__ __forceinline__ void fv_update_store_dt(const FVArgs& a, double* out,
   dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(un, 1));
 }
 
-template <bool PLANAR>
-__global__ void __launch_bounds__(FVP_NT) k_fv_godunov_periodic(FVArgs a) {
-  constexpr int V = kV;
-  constexpr int LX = FVP_TX + 2, LY = FVP_TY + 2;
-  __shared__ double su[LY * LX * V];
-  const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
-  const int k0 = pb + blockIdx.x * FVP_TX, j0 = pb + blockIdx.y * FVP_TY;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < LY * LX; i += FVP_NT) {
-    const int r = i / LX, c = i % LX;
-    const int j = fv_wrap(j0 - 1 + r, pb, a.P), k = fv_wrap(k0 - 1 + c, pb, a.P);
-#pragma unroll
-    for (int m = 0; m < V; m++) su[i * V + m] = a.luh[((long)j * S + k) * D + m];
-  }
-  __syncthreads();
-  const double dtv = *a.dt_dev;
-  const double cx = dtv / a.hx, cy = dtv / a.hy;
-  double dtn = DBL_MAX;
-  const int r = tid / FVP_TX, c = tid % FVP_TX;
-  const int j = j0 + r, k = k0 + c;
-  if (j < pe && k < pe) {
-    const double* U = &su[((r + 1) * LX + c + 1) * V];
-    double fxl[V], fxr[V], fyb[V], fyt[V];
-    rusanov<PLANAR>(U - V, U, 0, fxl);
-    rusanov<PLANAR>(U, U + V, 0, fxr);
-    rusanov<PLANAR>(U - LX * V, U, 1, fyb);
-    rusanov<PLANAR>(U, U + LX * V, 1, fyt);
-    fv_update_store_dt<PLANAR>(a, a.out + ((long)j * S + k) * D, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
-  }
-  for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
-  if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
-}
-
-// One FVP_TX x FVP_TY tile (tile column bx, row by) of one periodic patch
-// (the body of k_fv_muscl_periodic; the serving batch calls it per entry);
-// sm: kMusclPeriodicSmem bytes of dynamic shared memory
+// One FVP_TX x FVP_TY tile (tile column bx, row by) of a fused MUSCL-Hancock
+// step over a grid of patches (one periodic patch: npx = npy = 1; the
+// serving batch calls it per entry); sm: kMusclPeriodicSmem bytes of dynamic
+// shared memory.
+//
+// The reference evolves (half step, musclhancock.cpph:79-170) only a
+// patch's interior cells: the extrapolations of its ghost cells enter its
+// boundary faces without the half step.  So the face between two patches
+// has two different fluxes, one per side.  Here every cell of the tile's
+// ring is evolved (in the global view each is interior to its own patch),
+// and a cell on its patch's boundary recomputes the neighbour's plain
+// extrapolation (the ghost cell's value) for that face from the staged
+// state: the same values as a per-patch step after a ghost exchange.
 template <bool PLANAR>
 __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, int by, double* sm) {
   constexpr int V = kV;
@@ -497,8 +515,8 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   double* wRx = wLx + RY * RX * V;
   double* wLy = wRx + RY * RX * V;
   double* wRy = wLy + RY * RX * V;
-  const int D = V + a.npar, S = a.S, pb = a.g, pe = a.g + a.P;
-  const int k0 = pb + bx * FVP_TX, j0 = pb + by * FVP_TY;
+  const int P = a.P, NX = P * a.npx, NY = P * a.npy;
+  const int k0 = bx * FVP_TX, j0 = by * FVP_TY;  // global cell coordinates
   const int tid = threadIdx.x;
   const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
   // reciprocal cell sizes: multiplications instead of the reference's
@@ -506,70 +524,50 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   const double ihx = 1.0 / hx, ihy = 1.0 / hy;
   for (int i = tid; i < LY * LX; i += FVP_NT) {
     const int r = i / LX, c = i % LX;
-    const int j = fv_wrap(j0 - 2 + r, pb, a.P), k = fv_wrap(k0 - 2 + c, pb, a.P);
+    int flip;
+    const double* q = a.luh + fv_stencil_offset(a, k0 - 2 + c, j0 - 2 + r, &flip);
 #pragma unroll
-    for (int m = 0; m < V; m++) su[i * V + m] = a.luh[((long)j * S + k) * D + m];
+    for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
   }
   __syncthreads();
-  // ring cells: slopes, extrapolations, half step of the interior cells
-  // (musclhancock.cpph:79-170; ghost cells are not evolved, as there)
+  // ring cells: slopes, extrapolations and the half step
   for (int i = tid; i < RY * RX; i += FVP_NT) {
-    const int rr = i / RX, rc = i % RX;
-    const int j = j0 - 1 + rr, k = k0 - 1 + rc;
-    const double* U = &su[((rr + 1) * LX + rc + 1) * V];
-    const bool has_x = j >= pb && j < pe && k >= pb - 1 && k < pe + 1;
-    const bool has_y = j >= pb - 1 && j < pe + 1 && k >= pb && k < pe;
-    const bool interior = j >= pb && j < pe && k >= pb && k < pe;
+    const double* U = &su[((i / RX + 1) * LX + i % RX + 1) * V];
     double lx[V], rx[V], ly[V], ry[V];
 #pragma unroll
-    for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
-    if (has_x) {
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
-        lx[m] = U[m] - 0.5 * hx * sl;
-        rx[m] = U[m] + 0.5 * hx * sl;
-      }
-    }
-    if (has_y) {
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
-        ly[m] = U[m] - 0.5 * hy * sl;
-        ry[m] = U[m] + 0.5 * hy * sl;
-      }
-    }
-    if (interior) {
-      double Qt[V];
-      double F[2][V];
-#pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] = 0.0;
-      euler_flux<2, PLANAR>(lx, F);
-#pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
-      euler_flux<2, PLANAR>(rx, F);
-#pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
-      euler_flux<2, PLANAR>(ly, F);
-#pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
-      euler_flux<2, PLANAR>(ry, F);
-#pragma unroll
-      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        lx[m] += 0.5 * dt * Qt[m];
-        rx[m] += 0.5 * dt * Qt[m];
-        ly[m] += 0.5 * dt * Qt[m];
-        ry[m] += 0.5 * dt * Qt[m];
-      }
+    for (int m = 0; m < V; m++) {
+      const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
+      lx[m] = U[m] - 0.5 * hx * sl;
+      rx[m] = U[m] + 0.5 * hx * sl;
     }
 #pragma unroll
     for (int m = 0; m < V; m++) {
-      wLx[i * V + m] = lx[m];
-      wRx[i * V + m] = rx[m];
-      wLy[i * V + m] = ly[m];
-      wRy[i * V + m] = ry[m];
+      const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
+      ly[m] = U[m] - 0.5 * hy * sl;
+      ry[m] = U[m] + 0.5 * hy * sl;
+    }
+    double Qt[V];
+    double F[2][V];
+#pragma unroll
+    for (int m = 0; m < V; m++) Qt[m] = 0.0;
+    euler_flux<2, PLANAR>(lx, F);
+#pragma unroll
+    for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
+    euler_flux<2, PLANAR>(rx, F);
+#pragma unroll
+    for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
+    euler_flux<2, PLANAR>(ly, F);
+#pragma unroll
+    for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
+    euler_flux<2, PLANAR>(ry, F);
+#pragma unroll
+    for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      wLx[i * V + m] = lx[m] + 0.5 * dt * Qt[m];
+      wRx[i * V + m] = rx[m] + 0.5 * dt * Qt[m];
+      wLy[i * V + m] = ly[m] + 0.5 * dt * Qt[m];
+      wRy[i * V + m] = ry[m] + 0.5 * dt * Qt[m];
     }
   }
   __syncthreads();
@@ -577,15 +575,63 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   double dtn = DBL_MAX;
   const int r = tid / FVP_TX, c = tid % FVP_TX;
   const int j = j0 + r, k = k0 + c;
-  if (j < pe && k < pe) {
+  if (j < NY && k < NX) {
     const int ic = (r + 1) * RX + c + 1;  // this cell in the ring arrays
+    const double* U = &su[((r + 2) * LX + c + 2) * V];
+    const int kx = a.npx == 1 ? k : k % P, ky = a.npy == 1 ? j : j % P;  // position in the patch
+    double* o = a.out + fv_cell_offset(a, k, j);
     double fxl[V], fxr[V], fyb[V], fyt[V];
-    rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
-    rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
-    rusanov<PLANAR>(&wRy[(ic - RX) * V], &wLy[ic * V], 1, fyb);
-    rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + RX) * V], 1, fyt);
-    fv_update_store_dt<PLANAR>(a, a.out + ((long)j * S + k) * D, &su[((r + 2) * LX + c + 2) * V], fxl, fxr,
-                               fyb, fyt, cx, cy, dtn);
+    double qa[V], qb[V];
+    // x faces; across a patch boundary the outer side is the plain
+    // extrapolation of the neighbour cell (its ghost image in this patch)
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      qa[m] = wRx[(ic - 1) * V + m];
+      qb[m] = wLx[ic * V + m];
+    }
+    if (kx == 0) {
+      const double* W = U - V;
+#pragma unroll
+      for (int m = 0; m < V; m++) qa[m] = W[m] + 0.5 * hx * (minmod(W[V + m] - W[m], W[m] - W[-V + m]) * ihx);
+    }
+    rusanov<PLANAR>(qa, qb, 0, fxl);
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      qa[m] = wRx[ic * V + m];
+      qb[m] = wLx[(ic + 1) * V + m];
+    }
+    if (kx == P - 1) {
+      const double* W = U + V;
+#pragma unroll
+      for (int m = 0; m < V; m++) qb[m] = W[m] - 0.5 * hx * (minmod(W[V + m] - W[m], W[m] - W[-V + m]) * ihx);
+    }
+    rusanov<PLANAR>(qa, qb, 0, fxr);
+    // y faces
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      qa[m] = wRy[(ic - RX) * V + m];
+      qb[m] = wLy[ic * V + m];
+    }
+    if (ky == 0) {
+      const double* W = U - LX * V;
+#pragma unroll
+      for (int m = 0; m < V; m++)
+        qa[m] = W[m] + 0.5 * hy * (minmod(W[LX * V + m] - W[m], W[m] - W[-LX * V + m]) * ihy);
+    }
+    rusanov<PLANAR>(qa, qb, 1, fyb);
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      qa[m] = wRy[ic * V + m];
+      qb[m] = wLy[(ic + RX) * V + m];
+    }
+    if (ky == P - 1) {
+      const double* W = U + LX * V;
+#pragma unroll
+      for (int m = 0; m < V; m++)
+        qb[m] = W[m] - 0.5 * hy * (minmod(W[LX * V + m] - W[m], W[m] - W[-LX * V + m]) * ihy);
+    }
+    rusanov<PLANAR>(qa, qb, 1, fyt);
+    fv_update_store_dt<PLANAR>(a, o, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
   }
   for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
   if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
@@ -654,6 +700,7 @@ static exa_status_t check_fv(const exa_fv_desc_t* d, int want_ghost) {
 
 static FVArgs fv_args(const exa_fv_desc_t* d) {
   FVArgs a{};
+  a.npx = a.npy = 1;
   a.P = d->patch;
   a.g = d->ghost;
   a.S = d->patch + 2 * d->ghost;
@@ -695,6 +742,7 @@ __device__ __forceinline__ int fv_serve_find(const FVServePatch* pt, int np, int
 
 __device__ __forceinline__ FVArgs fv_serve_args(const FVServePatch& p) {
   FVArgs a{};
+  a.npx = a.npy = 1;
   a.P = p.P;
   a.g = p.g;
   a.S = p.P + 2 * p.g;
@@ -1217,8 +1265,9 @@ __global__ void k_fv_patch_ic(int P, int g, int D, int npx, int npy, double hx, 
 }  // namespace exa
 
 namespace exa {
-// Small patches (patch <= 16, the reference's per-cell FV patches): one CTA
-// of 128 threads per patch.  The whole patch with its ghosts (contiguous in
+// Small patches (patch <= 16, the subcell patches of the limiting ADER-DG
+// grid, stepped for a list of troubled cells): one CTA of 128 threads per
+// patch.  The whole patch with its ghosts (contiguous in
 // memory) is staged in shared memory, MUSCL-Hancock's ring cells compute
 // their evolved face extrapolations, and every interior cell evaluates its
 // own four face fluxes, applies them in the reference's order and writes
@@ -1472,18 +1521,12 @@ struct exa_fv_patchgrid {
   unsigned long long* slots = nullptr;  // [0] dt, [1] time, [2] next dt, [3] last dt
   size_t count = 0;
   long npatches = 0;
-  bool primed = false;  // slot [0] holds the CFL dt of the current state (small-patch path)
+  bool primed = false;  // slot [0] holds the CFL dt of the current state
   int bc[2] = {0, 0};   // EXA_BC_* per dimension
 };
 
 namespace exa {
-__global__ void k_fv_slot_reset(unsigned long long* s) { s[0] = 0x7FF0000000000000ULL; }
-__global__ void k_fv_time_add(unsigned long long* s) {
-  double* time = (double*)(s + 1);
-  *time += __longlong_as_double((long long)s[0]);
-  s[3] = s[0];
-}
-// fused small-patch steps: time += dt, last <- dt, dt <- next, next <- +inf
+// fused patch-grid steps: time += dt, last <- dt, dt <- next, next <- +inf
 __global__ void k_fv_patch_commit(unsigned long long* s) {
   double* time = (double*)(s + 1);
   *time += __longlong_as_double((long long)s[0]);
@@ -1493,90 +1536,71 @@ __global__ void k_fv_patch_commit(unsigned long long* s) {
 }
 }  // namespace exa
 
+// One step of the patch grid: one fused tile launch over the global cell
+// view (a ghost cell is read as the neighbour cell it would hold after the
+// exchange, so no exchange pass), the next dt reduced in the same pass, and
+// the commit rotating the dt slots.  The CFL dt of a state that was set or
+// initialised is reduced once first.
 static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
   using namespace exa;
   const exa_fv_desc_t& d = g->desc;
-  const int S = d.patch + 2 * d.ghost;
-  const long nex = 4L * d.ghost * d.patch * g->npatches;
-  k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy,
-                                                                       g->bc[0], g->bc[1], g->luh);
-  count_launch();
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
-  if (d.patch <= kFvSmallMax && d.npar == 0) {
-    // small patches: one fused launch per step (dt of this state from the
-    // previous update, or primed once), the commit rotates the dt slots
-    FVArgs a = fv_args(&d);
-    if (!g->primed) {
-      k_fv_slots_init<<<1, 1, 0, g->st>>>(g->slots);
-      a.luh = g->luh;
-      const long per0 = (long)S * S * kV;
-      for (long p0 = 0; p0 < g->npatches; p0 += 65535) {
-        const unsigned np = (unsigned)(g->npatches - p0 < 65535 ? g->npatches - p0 : 65535);
-        a.luh = g->luh + p0 * per0;
-        if (planar) k_fv_stable_dt<true><<<dim3(1, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
-        else k_fv_stable_dt<false><<<dim3(1, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
-        count_launch();
-      }
-      g->primed = true;
-    }
-    a.luh = g->luh;
-    a.out = g->luh_new;
-    a.dt_dev = (const double*)g->slots;
-    a.next_dt = g->slots + 2;
-    const size_t smem = fv_small_smem(d.patch, d.ghost, g->scheme);
-    auto kern = g->scheme == 0 ? (planar ? k_fv_patch_small<true, 0> : k_fv_patch_small<false, 0>)
-                               : (planar ? k_fv_patch_small<true, 1> : k_fv_patch_small<false, 1>);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "small patch attribute");
-    kern<<<(unsigned)g->npatches, FVS_NT, smem, g->st>>>(a);
-    k_fv_patch_commit<<<1, 1, 0, g->st>>>(g->slots);
-    count_launch(2);
-    std::swap(g->luh, g->luh_new);
-    return cuda_status(cudaGetLastError(), "fv patch grid step");
-  }
-  // dt: the CFL rule (commons::stableTimeStepSize) minimised over every patch
-  k_fv_slot_reset<<<1, 1, 0, g->st>>>(g->slots);
+  const int S = d.patch + 2 * d.ghost;
   FVArgs a = fv_args(&d);
-  const long cells = (long)d.patch * d.patch;
-  unsigned bx = (unsigned)((cells + 255) / 256);
-  if (bx > 64) bx = 64;
-  const long per = (long)S * S * kV;
-  constexpr long kChunk = 65535;  // grid y / z limit: patches per launch
-  for (long p0 = 0; p0 < g->npatches; p0 += kChunk) {
-    const unsigned np = (unsigned)(g->npatches - p0 < kChunk ? g->npatches - p0 : kChunk);
-    a.luh = g->luh + p0 * per;
-    if (planar) k_fv_stable_dt<true><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
-    else k_fv_stable_dt<false><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+  a.npx = g->npx;
+  a.npy = g->npy;
+  a.bcx = g->bc[0];
+  a.bcy = g->bc[1];
+  if (!g->primed) {
+    k_fv_slots_init<<<1, 1, 0, g->st>>>(g->slots);
     count_launch();
+    const long per0 = (long)S * S * kV;
+    const long cells = (long)d.patch * d.patch;
+    unsigned bx = (unsigned)((cells + 255) / 256);
+    if (bx > 64) bx = 64;
+    for (long p0 = 0; p0 < g->npatches; p0 += 65535) {
+      const unsigned np = (unsigned)(g->npatches - p0 < 65535 ? g->npatches - p0 : 65535);
+      a.luh = g->luh + p0 * per0;
+      if (planar) k_fv_stable_dt<true><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+      else k_fv_stable_dt<false><<<dim3(bx, np), 256, 0, g->st>>>(a, (double*)g->slots, 1);
+      count_launch();
+    }
+    if (exa_status_t s = cuda_status(cudaGetLastError(), "fv patch grid dt")) return s;
+    g->primed = true;
   }
-  cudaError_t e = cudaMemcpyAsync(g->luh_new, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToDevice, g->st);
-  if (e != cudaSuccess) return cuda_status(e, "fv patch copy");
+  a.luh = g->luh;
+  a.out = g->luh_new;
   a.dt_dev = (const double*)g->slots;
+  a.next_dt = g->slots + 2;
   a.max_dt = nullptr;
-  if (g->scheme == 1) {
+  const long NX = (long)d.patch * g->npx, NY = (long)d.patch * g->npy;
+  if (g->scheme == 0) {
+    static bool gattr[2] = {false, false};
+    if (!gattr[planar]) {
+      cudaError_t e = cudaFuncSetAttribute(planar ? k_fv_godunov<true, true> : k_fv_godunov<false, true>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout,
+                                           (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return cuda_status(e, "godunov attribute");
+      gattr[planar] = true;
+    }
+    const dim3 grid((unsigned)((NX + FV_TX - 1) / FV_TX), (unsigned)((NY + FV_TY - 1) / FV_TY), 1);
+    if (planar) k_fv_godunov<true, true><<<grid, FV_NT, 0, g->st>>>(a);
+    else k_fv_godunov<false, true><<<grid, FV_NT, 0, g->st>>>(a);
+  } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      e = planar ? cudaFuncSetAttribute(k_fv_muscl<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem)
-                 : cudaFuncSetAttribute(k_fv_muscl<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclSmem);
+      auto kern = planar ? k_fv_muscl_periodic<true> : k_fv_muscl_periodic<false>;
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
+    const dim3 grid((unsigned)((NX + FVP_TX - 1) / FVP_TX), (unsigned)((NY + FVP_TY - 1) / FVP_TY), 1);
+    if (planar) k_fv_muscl_periodic<true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
+    else k_fv_muscl_periodic<false><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
   }
-  for (long p0 = 0; p0 < g->npatches; p0 += kChunk) {
-    const unsigned np = (unsigned)(g->npatches - p0 < kChunk ? g->npatches - p0 : kChunk);
-    a.luh = g->luh + p0 * per;
-    a.out = g->luh_new + p0 * per;
-    dim3 grid((d.patch + FV_TX - 1) / FV_TX, (d.patch + FV_TY - 1) / FV_TY, np);
-    if (g->scheme == 0) {
-      if (planar) k_fv_godunov<true, false><<<grid, FV_NT, 0, g->st>>>(a);
-      else k_fv_godunov<false, false><<<grid, FV_NT, 0, g->st>>>(a);
-    } else {
-      if (planar) k_fv_muscl<true, false><<<grid, FV_NT, kMusclSmem, g->st>>>(a);
-      else k_fv_muscl<false, false><<<grid, FV_NT, kMusclSmem, g->st>>>(a);
-    }
-    count_launch();
-  }
-  k_fv_time_add<<<1, 1, 0, g->st>>>(g->slots);
+  k_fv_patch_commit<<<1, 1, 0, g->st>>>(g->slots);
   count_launch(2);
   std::swap(g->luh, g->luh_new);
   return cuda_status(cudaGetLastError(), "fv patch grid step");
@@ -1654,7 +1678,17 @@ exa_status_t exa_fv_patchgrid_set_state(exa_fv_patchgrid* g, const double* host)
 
 exa_status_t exa_fv_patchgrid_get_state(exa_fv_patchgrid* g, double* host) {
   if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
-  cudaError_t e = cudaMemcpyAsync(host, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToHost, g->st);
+  // the steps read no ghost cell and write none: fill the face ghosts here
+  // so the returned state is the one the reference holds after its
+  // neighbour merge (corner ghosts are not filled, as there)
+  const exa_fv_desc_t& d = g->desc;
+  const long nex = 4L * d.ghost * d.patch * g->npatches;
+  k_fv_patch_exchange<<<(unsigned)((nex + 255) / 256), 256, 0, g->st>>>(d.patch, d.ghost, kV, g->npx, g->npy,
+                                                                       g->bc[0], g->bc[1], g->luh);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(host, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToHost, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   return cuda_status(e, "fv patch grid get_state");
 }

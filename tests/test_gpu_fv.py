@@ -166,7 +166,7 @@ def test_fv_grid_noise_and_restart():
 
 
 @pytest.mark.parametrize('scheme', [0, 1])
-@pytest.mark.parametrize('P,npx,npy', [(10, 3, 4), (7, 2, 2), (16, 1, 3), (20, 2, 1)])
+@pytest.mark.parametrize('P,npx,npy', [(10, 3, 4), (7, 2, 2), (16, 1, 3), (20, 2, 1), (2, 1, 1), (3, 5, 1)])
 def test_fv_patch_grid_vs_oracle(scheme, P, npx, npy):
     """Grid of patches with ghost exchange (the EulerFV layout, patch 10)
     against the oracle's per-patch ghostLayerFilling + step, per step."""
@@ -187,8 +187,36 @@ def test_fv_patch_grid_vs_oracle(scheme, P, npx, npy):
 
 
 @pytest.mark.parametrize('scheme', [0, 1])
+def test_fv_patch_grid_state_ghosts(scheme):
+    """The steps read neighbour cells in place of ghost cells and write no
+    ghost cell; the state handed out has its face ghosts filled from the
+    neighbours' boundary layers (the state after the reference's neighbour
+    merge), with a reflecting wall in y."""
+    P, npx, npy = 6, 3, 2
+    g = E.FVPatchGrid(scheme, P, npx, npy)
+    g.init(amp=0.2, seed=9, noise=1e-3)
+    g.set_boundary((0, 2))
+    g.step(3)
+    G, S = g.ghost, g.side
+    q = g.get_state().reshape(npy, npx, S, S, 5)
+    for py in range(npy):
+        for px in range(npx):
+            left = q[py, (px - 1) % npx]
+            assert np.array_equal(q[py, px, G:G + P, :G], left[G:G + P, P:P + G])
+            right = q[py, (px + 1) % npx]
+            assert np.array_equal(q[py, px, G:G + P, G + P:], right[G:G + P, G:2 * G])
+            if py > 0:
+                assert np.array_equal(q[py, px, :G, G:G + P], q[py - 1, px, P:P + G, G:G + P])
+            else:  # wall: mirror of the own boundary layers, v negated
+                mir = q[py, px, 2 * G - 1:G - 1:-1, G:G + P].copy()
+                mir[..., 2] *= -1
+                assert np.array_equal(q[py, px, :G, G:G + P], mir)
+    g.destroy()
+
+
+@pytest.mark.parametrize('scheme', [0, 1])
 @pytest.mark.parametrize('P,npx,npy,bc', [(10, 3, 4, (1, 2)), (7, 2, 2, (2, 1)), (16, 1, 3, (2, 0)),
-                                          (20, 2, 1, (1, 1))])
+                                          (20, 2, 1, (1, 1)), (2, 1, 2, (2, 2)), (3, 2, 3, (0, 2))])
 def test_fv_patch_grid_walls_vs_oracle(scheme, P, npx, npy, bc):
     """Patch grid with outflow / reflecting walls: domain-boundary ghosts
     from the patch's own boundary layers (orc_fv_boundary_ghosts, pinned to
