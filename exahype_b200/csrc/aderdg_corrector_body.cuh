@@ -59,7 +59,6 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
   double* sFn = sFo + FV;
   double* sAv = sFn + FV;            // [NFACE][2 (own, neighbour)][V]
   double* sSm = sAv + NFACE * 2 * V;  // [NFACE]
-  double* sred = smem + S::CPB * (4 * FV + NFACE * 2 * V + NFACE);
 
   int cc[3] = {0, 0, 0};
   if (valid) {
@@ -162,43 +161,58 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
       }
     __syncthreads();
   }
-  // face-averaged states (riemannSolverNonlinear.cpph:52-69)
-  if (valid) {
-    for (int k = s; k < NFACE * 2 * V; k += G) {
-      const int f = k / (2 * V), side = (k / V) & 1, m = k % V;
-      const double* Q = (side ? sQn : sQo) + f * NF * V;
-      double acc = 0.0;
+  // face-averaged states (riemannSolverNonlinear.cpph:52-69) and smax per
+  // face (:71-81)
+  if constexpr (G >= 32) {
+    // one warp per face: the averages, a warp barrier, then the face's smax
+    constexpr int NWC = G / 32;  // warps of this cell
+    const int wc = s >> 5, lane = s & 31;
+    if (valid)
+      for (int f = wc; f < NFACE; f += NWC) {
+        if (lane < 2 * V) {
+          const int side = lane / V, m = lane % V;
+          const double* Q = (side ? sQn : sQo) + f * NF * V;
+          double acc = 0.0;
 #pragma unroll
-      for (int j = 0; j < NF; j++) acc += face_weight<DIM, B>(T, j) * Q[j * V + m];
-      sAv[k] = acc;
-    }
-  }
-  __syncthreads();
-  // smax per face (:71-81)
-  if (valid && s < NFACE) {
-    const int f = s, d = f >> 1;
-    double qa[5], qb[5];
+          for (int j = 0; j < NF; j++) acc += face_weight<DIM, B>(T, j) * Q[j * V + m];
+          sAv[f * 2 * V + lane] = acc;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          double qa[5], qb[5];
 #pragma unroll
-    for (int m = 0; m < V; m++) {
-      qa[m] = sAv[(f * 2 + 0) * V + m];
-      qb[m] = sAv[(f * 2 + 1) * V + m];
+          for (int m = 0; m < V; m++) {
+            qa[m] = sAv[(f * 2 + 0) * V + m];
+            qb[m] = sAv[(f * 2 + 1) * V + m];
+          }
+          sSm[f] = fmax(euler_max_eig<PLANAR>(qa, f >> 1), euler_max_eig<PLANAR>(qb, f >> 1));
+        }
+      }
+    __syncthreads();
+  } else {
+    if (valid) {
+      for (int k = s; k < NFACE * 2 * V; k += G) {
+        const int f = k / (2 * V), side = (k / V) & 1, m = k % V;
+        const double* Q = (side ? sQn : sQo) + f * NF * V;
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < NF; j++) acc += face_weight<DIM, B>(T, j) * Q[j * V + m];
+        sAv[k] = acc;
+      }
     }
-    sSm[f] = fmax(euler_max_eig<PLANAR>(qa, d), euler_max_eig<PLANAR>(qb, d));
-  }
-  __syncthreads();
-  // Rusanov flux (:83-115): F = (FL+FR)/2 - smax/2 (QR-QL); left = lower cell
-  if (valid) {
-    for (int k = s; k < FV; k += G) {
-      const int f = k / (NF * V);
-      const bool own_left = f & 1;  // face 2d+1: this cell is the left one
-      const double ql = own_left ? sQo[k] : sQn[k];
-      const double qr = own_left ? sQn[k] : sQo[k];
-      const double fl = own_left ? sFo[k] : sFn[k];
-      const double fr = own_left ? sFn[k] : sFo[k];
-      sFo[k] = 0.5 * (fr + fl) - 0.5 * sSm[f] * (qr - ql);
+    __syncthreads();
+    if (valid && s < NFACE) {
+      const int f = s, d = f >> 1;
+      double qa[5], qb[5];
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        qa[m] = sAv[(f * 2 + 0) * V + m];
+        qb[m] = sAv[(f * 2 + 1) * V + m];
+      }
+      sSm[f] = fmax(euler_max_eig<PLANAR>(qa, d), euler_max_eig<PLANAR>(qb, d));
     }
+    __syncthreads();
   }
-  __syncthreads();
   double dtc = DBL_MAX;
   if (valid && s < NPC) {
     int sd[3];
@@ -209,21 +223,28 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     double v[V];
 #pragma unroll
     for (int m = 0; m < V; m++) v[m] = v_lduh[m];
-    // surface integral (surfaceIntegralNonlinear.cpph:21-85)
+    // surface integral (surfaceIntegralNonlinear.cpph:21-85) of the Rusanov
+    // fluxes at this node's face nodes (riemannSolverNonlinear.cpph:83-115:
+    // F = (FL+FR)/2 - smax/2 (QR-QL), left = lower cell), formed here by
+    // each node that applies them instead of being stored first
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      double us = 1.0 / a.dx[d];
       double wprod = 1.0;
 #pragma unroll
       for (int e = DIM - 1; e >= 0; e--)
         if (e != d) wprod *= T.w[sd[e]];
-      us = wprod / a.dx[d];
+      const double us = wprod / a.dx[d];
       const int j = face_node<DIM, B>(sd, d);
       const double cr = T.fr[sd[d]], cl = T.fl[sd[d]];
-      const double* FR_ = sFo + ((2 * d + 1) * NF + j) * V;
-      const double* FL_ = sFo + ((2 * d) * NF + j) * V;
+      const int kr = ((2 * d + 1) * NF + j) * V, kl = ((2 * d) * NF + j) * V;
+      const double smr = sSm[2 * d + 1], sml = sSm[2 * d];
 #pragma unroll
-      for (int m = 0; m < V; m++) v[m] -= (FR_[m] * cr - FL_[m] * cl) * us;
+      for (int m = 0; m < V; m++) {
+        // face 2d+1: this cell is the left one; face 2d: the right one
+        const double FR_ = 0.5 * (sFn[kr + m] + sFo[kr + m]) - 0.5 * smr * (sQn[kr + m] - sQo[kr + m]);
+        const double FL_ = 0.5 * (sFo[kl + m] + sFn[kl + m]) - 0.5 * sml * (sQo[kl + m] - sQn[kl + m]);
+        v[m] -= (FR_ * cr - FL_ * cl) * us;
+      }
     }
     // solution update (solutionUpdate.cpph:23-47)
     double W = 1.0;
@@ -249,9 +270,17 @@ __device__ __forceinline__ void corrector_block(const CorrArgs& a, long block, d
     }
   }
   if (a.dt_next) {
-    const double cm = group_min<G>(dtc, sred);
-    if (valid && s == 0) atomic_min_pos_double(a.dt_next, cm);
+    // minimum over the warp's lanes of this cell, then one atomic per warp
+    // (per cell for cells narrower than a warp), skipped when the slot
+    // already holds a smaller value (read at L2, where the atomics land;
+    // the slot only decreases within a step)
+    constexpr int L = G < 32 ? G : 32;
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+    if (valid && (s % L) == 0 && dtc < __longlong_as_double((long long)__ldcg(a.dt_next)))
+      atomic_min_pos_double(a.dt_next, dtc);
   }
 }
 
 }  // namespace exa
+
