@@ -66,8 +66,11 @@ __device__ __forceinline__ int fv_fold(int X, int NX, int bc, bool& mirrored) {
   return X < 0 ? -1 - X : 2 * NX - 1 - X;
 }
 
-// element offset of in-domain cell (X, Y)
+// element offset of in-domain cell (X, Y); GRID = false: one periodic
+// patch (npx = npy = 1, no walls), known at compile time
+template <bool GRID>
 __device__ __forceinline__ long fv_cell_offset(const FVArgs& a, int X, int Y) {
+  if (!GRID) return ((long)(a.g + Y) * a.S + (a.g + X)) * (kV + a.npar);
   const int px = a.npx == 1 ? 0 : X / a.P, py = a.npy == 1 ? 0 : Y / a.P;
   const long patch = (long)py * a.npx + px;
   return (patch * a.S * a.S + (long)(a.g + Y - py * a.P) * a.S + (a.g + X - px * a.P)) * (kV + a.npar);
@@ -75,11 +78,13 @@ __device__ __forceinline__ long fv_cell_offset(const FVArgs& a, int X, int Y) {
 
 // element offset of the cell read at stencil coordinate (X, Y); *flip =
 // the momentum component a reflecting wall negates there, else -1
+template <bool GRID>
 __device__ __forceinline__ long fv_stencil_offset(const FVArgs& a, int X, int Y, int* flip) {
   bool mx = false, my = false;
-  const int Xf = fv_fold(X, a.P * a.npx, a.bcx, mx), Yf = fv_fold(Y, a.P * a.npy, a.bcy, my);
-  *flip = (mx && a.bcx == EXA_BC_REFLECT) ? 1 : ((my && a.bcy == EXA_BC_REFLECT) ? 2 : -1);
-  return fv_cell_offset(a, Xf, Yf);
+  const int Xf = fv_fold(X, a.P * (GRID ? a.npx : 1), GRID ? a.bcx : 0, mx);
+  const int Yf = fv_fold(Y, a.P * (GRID ? a.npy : 1), GRID ? a.bcy : 0, my);
+  *flip = !GRID ? -1 : ((mx && a.bcx == EXA_BC_REFLECT) ? 1 : ((my && a.bcy == EXA_BC_REFLECT) ? 2 : -1));
+  return fv_cell_offset<GRID>(a, Xf, Yf);
 }
 
 // Fused steps (FUSED = true) of a single periodic patch: the tile is loaded
@@ -141,7 +146,7 @@ __device__ __forceinline__ double fv_face_flux(const double* qL, const double* q
 // shared-memory carveout
 // One FV_TX x FV_TY tile (tile column bx, row by) of patch `patch` of a.luh
 // / a.out (the body of k_fv_godunov; the serving batch calls it per entry).
-template <bool PLANAR, bool FUSED>
+template <bool PLANAR, bool FUSED, bool GRID = false>
 __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by, long patch) {
   constexpr int V = kV, C = kV + 1;
   constexpr int LX = FV_TX + 2, LY = FV_TY + 2;
@@ -160,7 +165,7 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
     const int j = j0 - 1 + r, k = k0 - 1 + c;
     if (FUSED) {
       int flip;
-      const double* q = luh + fv_stencil_offset(a, k, j, &flip);
+      const double* q = luh + fv_stencil_offset<GRID>(a, k, j, &flip);
 #pragma unroll
       for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
     } else if (j >= 0 && j < S && k >= 0 && k < S) {
@@ -193,7 +198,7 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
     const bool valid = FUSED ? (j < a.P * a.npy && k < a.P * a.npx) : (j < pe && k < pe);
     double fxl[V], fxr[V], fyb[V], fyt[V];
     // output cell, addressed before the face fluxes hold their registers
-    double* o = FUSED ? a.out + (valid ? fv_cell_offset(a, k, j) : 0) : out + ((long)j * S + k) * D;
+    double* o = FUSED ? a.out + (valid ? fv_cell_offset<GRID>(a, k, j) : 0) : out + ((long)j * S + k) * D;
     if (valid) {
       const double* q = &su[((r + 1) * LX + c + 1) * V];
       const double sxl = fv_face_flux(q - V, q, &scx[(r * LX + c) * C], &scx[(r * LX + c + 1) * C], fxl);
@@ -260,9 +265,9 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
   }
 }
 
-template <bool PLANAR, bool FUSED>
+template <bool PLANAR, bool FUSED, bool GRID = false>
 __global__ void __launch_bounds__(FV_NT, 5) k_fv_godunov(FVArgs a) {
-  fv_godunov_tile<PLANAR, FUSED>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  fv_godunov_tile<PLANAR, FUSED, GRID>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // -------------------------------------------------------- MUSCL-Hancock
@@ -505,7 +510,7 @@ __device__ __forceinline__ void fv_update_store_dt(const FVArgs& a, double* out,
 // and a cell on its patch's boundary recomputes the neighbour's plain
 // extrapolation (the ghost cell's value) for that face from the staged
 // state: the same values as a per-patch step after a ghost exchange.
-template <bool PLANAR>
+template <bool PLANAR, bool GRID>
 __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, int by, double* sm) {
   constexpr int V = kV;
   constexpr int LX = FVP_TX + 4, LY = FVP_TY + 4;   // state: cells j0-2..j0+TY+1, k0-2..k0+TX+1
@@ -515,7 +520,7 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   double* wRx = wLx + RY * RX * V;
   double* wLy = wRx + RY * RX * V;
   double* wRy = wLy + RY * RX * V;
-  const int P = a.P, NX = P * a.npx, NY = P * a.npy;
+  const int P = a.P, NX = GRID ? P * a.npx : P, NY = GRID ? P * a.npy : P;
   const int k0 = bx * FVP_TX, j0 = by * FVP_TY;  // global cell coordinates
   const int tid = threadIdx.x;
   const double hx = a.hx, hy = a.hy, dt = *a.dt_dev;
@@ -525,49 +530,76 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   for (int i = tid; i < LY * LX; i += FVP_NT) {
     const int r = i / LX, c = i % LX;
     int flip;
-    const double* q = a.luh + fv_stencil_offset(a, k0 - 2 + c, j0 - 2 + r, &flip);
+    const double* q = a.luh + fv_stencil_offset<GRID>(a, k0 - 2 + c, j0 - 2 + r, &flip);
 #pragma unroll
     for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
   }
   __syncthreads();
-  // ring cells: slopes, extrapolations and the half step
+  // ring cells: slopes, extrapolations and the half step.  One patch: a
+  // ring cell outside the patch is its ghost (x or y extrapolation only, no
+  // half step), as the reference's per-patch loops have it.  Patch grid:
+  // every ring cell is evolved as the interior cell of its own patch, and
+  // the face phase recomputes the ghost form on patch faces.
   for (int i = tid; i < RY * RX; i += FVP_NT) {
-    const double* U = &su[((i / RX + 1) * LX + i % RX + 1) * V];
+    const int rr = i / RX, rc = i % RX;
+    const double* U = &su[((rr + 1) * LX + rc + 1) * V];
+    bool has_x = true, has_y = true, interior = true;
+    if (!GRID) {
+      const int j = j0 - 1 + rr, k = k0 - 1 + rc;
+      has_x = j >= 0 && j < P && k >= -1 && k < P + 1;
+      has_y = j >= -1 && j < P + 1 && k >= 0 && k < P;
+      interior = j >= 0 && j < P && k >= 0 && k < P;
+    }
     double lx[V], rx[V], ly[V], ry[V];
 #pragma unroll
-    for (int m = 0; m < V; m++) {
-      const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
-      lx[m] = U[m] - 0.5 * hx * sl;
-      rx[m] = U[m] + 0.5 * hx * sl;
+    for (int m = 0; m < V; m++) { lx[m] = rx[m] = ly[m] = ry[m] = 0.0; }
+    if (has_x) {
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        const double sl = minmod(U[V + m] - U[m], U[m] - U[-V + m]) * ihx;
+        lx[m] = U[m] - 0.5 * hx * sl;
+        rx[m] = U[m] + 0.5 * hx * sl;
+      }
+    }
+    if (has_y) {
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
+        ly[m] = U[m] - 0.5 * hy * sl;
+        ry[m] = U[m] + 0.5 * hy * sl;
+      }
+    }
+    if (interior) {
+      double Qt[V];
+      double F[2][V];
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] = 0.0;
+      euler_flux<2, PLANAR>(lx, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
+      euler_flux<2, PLANAR>(rx, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
+      euler_flux<2, PLANAR>(ly, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
+      euler_flux<2, PLANAR>(ry, F);
+#pragma unroll
+      for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        lx[m] += 0.5 * dt * Qt[m];
+        rx[m] += 0.5 * dt * Qt[m];
+        ly[m] += 0.5 * dt * Qt[m];
+        ry[m] += 0.5 * dt * Qt[m];
+      }
     }
 #pragma unroll
     for (int m = 0; m < V; m++) {
-      const double sl = minmod(U[LX * V + m] - U[m], U[m] - U[-LX * V + m]) * ihy;
-      ly[m] = U[m] - 0.5 * hy * sl;
-      ry[m] = U[m] + 0.5 * hy * sl;
-    }
-    double Qt[V];
-    double F[2][V];
-#pragma unroll
-    for (int m = 0; m < V; m++) Qt[m] = 0.0;
-    euler_flux<2, PLANAR>(lx, F);
-#pragma unroll
-    for (int m = 0; m < V; m++) Qt[m] += F[0][m] * ihx;
-    euler_flux<2, PLANAR>(rx, F);
-#pragma unroll
-    for (int m = 0; m < V; m++) Qt[m] -= F[0][m] * ihx;
-    euler_flux<2, PLANAR>(ly, F);
-#pragma unroll
-    for (int m = 0; m < V; m++) Qt[m] += F[1][m] * ihy;
-    euler_flux<2, PLANAR>(ry, F);
-#pragma unroll
-    for (int m = 0; m < V; m++) Qt[m] -= F[1][m] * ihy;
-#pragma unroll
-    for (int m = 0; m < V; m++) {
-      wLx[i * V + m] = lx[m] + 0.5 * dt * Qt[m];
-      wRx[i * V + m] = rx[m] + 0.5 * dt * Qt[m];
-      wLy[i * V + m] = ly[m] + 0.5 * dt * Qt[m];
-      wRy[i * V + m] = ry[m] + 0.5 * dt * Qt[m];
+      wLx[i * V + m] = lx[m];
+      wRx[i * V + m] = rx[m];
+      wLy[i * V + m] = ly[m];
+      wRy[i * V + m] = ry[m];
     }
   }
   __syncthreads();
@@ -578,9 +610,16 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   if (j < NY && k < NX) {
     const int ic = (r + 1) * RX + c + 1;  // this cell in the ring arrays
     const double* U = &su[((r + 2) * LX + c + 2) * V];
-    const int kx = a.npx == 1 ? k : k % P, ky = a.npy == 1 ? j : j % P;  // position in the patch
-    double* o = a.out + fv_cell_offset(a, k, j);
+    const int kx = (!GRID || a.npx == 1) ? k : k % P, ky = (!GRID || a.npy == 1) ? j : j % P;  // in the patch
+    double* o = a.out + fv_cell_offset<GRID>(a, k, j);
     double fxl[V], fxr[V], fyb[V], fyt[V];
+    if constexpr (!GRID) {
+      rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
+      rusanov<PLANAR>(&wRx[ic * V], &wLx[(ic + 1) * V], 0, fxr);
+      rusanov<PLANAR>(&wRy[(ic - RX) * V], &wLy[ic * V], 1, fyb);
+      rusanov<PLANAR>(&wRy[ic * V], &wLy[(ic + RX) * V], 1, fyt);
+      fv_update_store_dt<PLANAR>(a, o, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
+    } else {
     double qa[V], qb[V];
     // x faces; across a patch boundary the outer side is the plain
     // extrapolation of the neighbour cell (its ghost image in this patch)
@@ -632,15 +671,16 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
     }
     rusanov<PLANAR>(qa, qb, 1, fyt);
     fv_update_store_dt<PLANAR>(a, o, U, fxl, fxr, fyb, fyt, cx, cy, dtn);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
   if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
 }
 
-template <bool PLANAR>
+template <bool PLANAR, bool GRID>
 __global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
   extern __shared__ double sm[];
-  fv_muscl_periodic_tile<PLANAR>(a, blockIdx.x, blockIdx.y, sm);
+  fv_muscl_periodic_tile<PLANAR, GRID>(a, blockIdx.x, blockIdx.y, sm);
 }
 
 constexpr size_t kMusclPeriodicSmem =
@@ -763,7 +803,7 @@ __global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_serve(const FVServePatch
   const FVServePatch& p = pt[fv_serve_find(pt, np, blockIdx.x)];
   const FVArgs a = fv_serve_args(p);
   const int t = blockIdx.x - p.tile0;
-  fv_muscl_periodic_tile<PLANAR>(a, t % p.tiles_x, t / p.tiles_x, sm);
+  fv_muscl_periodic_tile<PLANAR, false>(a, t % p.tiles_x, t / p.tiles_x, sm);
 }
 
 template <bool PLANAR>
@@ -911,7 +951,7 @@ exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const doubl
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      auto kern = planar ? k_fv_muscl_periodic<true> : k_fv_muscl_periodic<false>;
+      auto kern = planar ? k_fv_muscl_periodic<true, false> : k_fv_muscl_periodic<false, false>;
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
       // three CTAs of ~72 KB per SM need the largest shared-memory carveout
       if (e == cudaSuccess)
@@ -919,8 +959,8 @@ exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const doubl
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
-    if (planar) k_fv_muscl_periodic<true><<<grid, FVP_NT, kMusclPeriodicSmem, st>>>(a);
-    else k_fv_muscl_periodic<false><<<grid, FVP_NT, kMusclPeriodicSmem, st>>>(a);
+    if (planar) k_fv_muscl_periodic<true, false><<<grid, FVP_NT, kMusclPeriodicSmem, st>>>(a);
+    else k_fv_muscl_periodic<false, false><<<grid, FVP_NT, kMusclPeriodicSmem, st>>>(a);
   }
   k_fv_commit<<<1, 1, 0, st>>>(slots);
   count_launch(2);
@@ -1577,19 +1617,19 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
   if (g->scheme == 0) {
     static bool gattr[2] = {false, false};
     if (!gattr[planar]) {
-      cudaError_t e = cudaFuncSetAttribute(planar ? k_fv_godunov<true, true> : k_fv_godunov<false, true>,
+      cudaError_t e = cudaFuncSetAttribute(planar ? k_fv_godunov<true, true, true> : k_fv_godunov<false, true, true>,
                                            cudaFuncAttributePreferredSharedMemoryCarveout,
                                            (int)cudaSharedmemCarveoutMaxShared);
       if (e != cudaSuccess) return cuda_status(e, "godunov attribute");
       gattr[planar] = true;
     }
     const dim3 grid((unsigned)((NX + FV_TX - 1) / FV_TX), (unsigned)((NY + FV_TY - 1) / FV_TY), 1);
-    if (planar) k_fv_godunov<true, true><<<grid, FV_NT, 0, g->st>>>(a);
-    else k_fv_godunov<false, true><<<grid, FV_NT, 0, g->st>>>(a);
+    if (planar) k_fv_godunov<true, true, true><<<grid, FV_NT, 0, g->st>>>(a);
+    else k_fv_godunov<false, true, true><<<grid, FV_NT, 0, g->st>>>(a);
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
-      auto kern = planar ? k_fv_muscl_periodic<true> : k_fv_muscl_periodic<false>;
+      auto kern = planar ? k_fv_muscl_periodic<true, true> : k_fv_muscl_periodic<false, true>;
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
       if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
@@ -1597,8 +1637,8 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
       attr[planar] = true;
     }
     const dim3 grid((unsigned)((NX + FVP_TX - 1) / FVP_TX), (unsigned)((NY + FVP_TY - 1) / FVP_TY), 1);
-    if (planar) k_fv_muscl_periodic<true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
-    else k_fv_muscl_periodic<false><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
+    if (planar) k_fv_muscl_periodic<true, true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
+    else k_fv_muscl_periodic<false, true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
   }
   k_fv_patch_commit<<<1, 1, 0, g->st>>>(g->slots);
   count_launch(2);
