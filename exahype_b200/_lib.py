@@ -206,6 +206,8 @@ SIGNATURES = {
     'exa_ensemble_stream': (i32, [vp, C.POINTER(vp)]),
     'exa_ensemble_get_state': (i32, [vp, i32, vp]),
     'exa_ensemble_device_state': (i32, [vp, i32, C.POINTER(vp)]),
+    'exa_ensemble_checkpoint': (i32, [vp, i32, vp, vp]),
+    'exa_ensemble_restore': (i32, [vp, vp, vp, vp, C.POINTER(i32)]),
     'exa_ensemble_status': (i32, [vp, vp, vp, vp, vp, vp]),
     'exa_ensemble_active_cells': (i64, [vp]),
     'exa_ensemble_info': (i32, [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(sz)]),
@@ -221,6 +223,10 @@ SIGNATURES = {
     'exa_server_run': (i32, [vp, vp, vp, i32, f64, vp, C.POINTER(u64)]),
     'exa_server_tune': (i32, [vp, i32, i32]),
     'exa_server_device_state': (i32, [vp, u64, C.POINTER(vp)]),
+    'exa_server_evict': (i32, [vp, u64]),
+    'exa_server_restore': (i32, [vp, u64]),
+    'exa_server_evicted': (i32, [vp, u64, C.POINTER(i32)]),
+    'exa_server_set_eviction': (i32, [vp, f64]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_stable_dt': (i32, [C.POINTER(FVDesc), i64, vp, vp, vp]),

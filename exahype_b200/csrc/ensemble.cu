@@ -811,6 +811,92 @@ exa_status_t exa_ensemble_get_state(exa_ensemble* e, int slot, double* host_luh)
   return cuda_status(err, "ensemble get_state");
 }
 
+exa_status_t exa_ensemble_checkpoint(exa_ensemble* e, int slot, double* host_luh, exa_solve_checkpoint_t* ck) {
+  if (!e || !host_luh || !ck || slot < 0 || slot >= e->max_solves) return set_error(EXA_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  if (!e->used[slot]) return set_error(EXA_ENOTFOUND, "slot not in use");
+  const SolveDev& hs = e->host[slot];
+  const int B = hs.order + 1;
+  SolveDev d{};
+  cudaError_t err = cudaMemcpyAsync(host_luh, hs.luh, sizeof(double) * hs.ncells * B * B * kV,
+                                    cudaMemcpyDeviceToHost, e->st);
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(&d, e->d_solves + slot, sizeof(SolveDev), cudaMemcpyDeviceToHost, e->st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->st);
+  if (err != cudaSuccess) return cuda_status(err, "ensemble checkpoint");
+  *ck = exa_solve_checkpoint_t{};
+  ck->time = d.time;
+  ck->dt = d.dt;
+  ck->dt_next_bits = d.dt_next;
+  ck->steps_done = d.steps_done;
+  ck->steps_left = d.steps_left;
+  ck->picard = d.stats[0];
+  ck->nonconverged = d.stats[1];
+  ck->active = d.active;
+  ck->nan_flag = d.nan_flag;
+  return EXA_OK;
+}
+
+exa_status_t exa_ensemble_restore(exa_ensemble* e, const exa_solve_config_t* c, const double* host_luh,
+                                  const exa_solve_checkpoint_t* ck, int* slot) {
+  if (!e || !c || !host_luh || !ck || !slot) return set_error(EXA_EINVAL, "NULL argument");
+  long nc;
+  size_t n_luh, n_face;
+  if (exa_status_t s = solve_sizes(c, &nc, &n_luh, &n_face)) return s;
+  std::lock_guard<std::mutex> lk(e->mu);
+  int sl = -1;
+  for (int i = 0; i < e->max_solves; i++)
+    if (!e->used[i]) { sl = i; break; }
+  if (sl < 0) return set_error(EXA_EBUSY, "no free solve slot");
+  const size_t bytes = solve_footprint(nc, n_luh, n_face);
+  size_t off = 0;
+  if (!arena_alloc(e, bytes, &off)) return set_error(EXA_EBUSY, "not enough free device memory in the arena");
+  SolveDev& sv = e->host[sl];
+  sv = SolveDev{};
+  sv.order = c->order;
+  sv.pde = c->pde;
+  sv.dt_policy = c->dt_policy;
+  sv.n[0] = c->n[0];
+  sv.n[1] = c->n[1];
+  sv.dx[0] = c->length[0] / c->n[0];
+  sv.dx[1] = c->length[1] / c->n[1];
+  sv.ncells = nc;
+  char* base = e->arena + off;
+  sv.luh = (double*)base;
+  sv.lduh = (double*)(base + align256(n_luh * 8));
+  sv.qb = (double*)(base + 2 * align256(n_luh * 8));
+  sv.fb = (double*)(base + 2 * align256(n_luh * 8) + align256(n_face * 8));
+  sv.dt_factor = c->dt_policy == 0 ? c->cfl * host_pnpm(c->order) : c->cfl / (2 * c->order + 1);
+  sv.dt_fixed = c->dt_fixed;
+  // the time-step state exactly as checkpointed: the solve continues with
+  // the dt its last corrector reduced, bit for bit as if never removed
+  sv.active = ck->active;
+  sv.dt = ck->dt;
+  sv.dt_next = ck->dt_next_bits;
+  sv.time = ck->time;
+  sv.steps_done = ck->steps_done;
+  sv.steps_left = ck->steps_left;
+  sv.stats[0] = ck->picard;
+  sv.stats[1] = ck->nonconverged;
+  sv.nan_flag = ck->nan_flag;
+  e->used[sl] = 1;
+  e->alloc_off[sl] = off;
+  e->alloc_size[sl] = bytes;
+  cudaError_t err = cudaMemcpyAsync(sv.luh, host_luh, n_luh * 8, cudaMemcpyHostToDevice, e->st);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(e->d_solves + sl, &sv, sizeof(SolveDev), cudaMemcpyHostToDevice, e->st);
+  // the host copy must not be reused before the upload has read it
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->st);
+  if (err != cudaSuccess) {
+    e->used[sl] = 0;
+    arena_free(e, off, bytes);
+    sv = SolveDev{};
+    return cuda_status(err, "ensemble restore");
+  }
+  e->dirty = true;
+  *slot = sl;
+  return EXA_OK;
+}
+
 exa_status_t exa_ensemble_device_state(exa_ensemble* e, int slot, double** luh_dev) {
   if (!e || !luh_dev || slot < 0 || slot >= e->max_solves) return set_error(EXA_EINVAL, "bad argument");
   if (!e->used[slot]) return set_error(EXA_ENOTFOUND, "slot not in use");

@@ -1166,12 +1166,18 @@ exa_status_t exa_fv_grid_init(exa_fv_grid* g, double amp, uint64_t seed, double 
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
   if (exa_status_t s = launch_fv_ic(g->desc, g->luh, amp, seed, noise, g->st)) return s;
   g->primed = false;
-  return cuda_status(cudaStreamSynchronize(g->st), "fv grid init");
+  // both buffers hold the state: the steps write interiors only, so the
+  // ghost cells of a stepped state are the initial ones in either buffer
+  cudaError_t e = cudaMemcpyAsync(g->luh_new, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToDevice, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  return cuda_status(e, "fv grid init");
 }
 
 exa_status_t exa_fv_grid_set_state(exa_fv_grid* g, const double* host) {
   if (!g || !host) return set_error(EXA_EINVAL, "NULL argument");
   cudaError_t e = cudaMemcpyAsync(g->luh, host, g->count * sizeof(double), cudaMemcpyHostToDevice, g->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(g->luh_new, g->luh, g->count * sizeof(double), cudaMemcpyDeviceToDevice, g->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
   g->primed = false;
   return cuda_status(e, "fv grid set_state");

@@ -45,6 +45,11 @@ struct Req {
   long long steps_left = 0;
   long long steps_done = 0;
   bool done = false;
+  // eviction: the state and time-step scalars on the host, no device memory
+  bool evicted = false;
+  std::vector<double> saved;
+  exa_solve_checkpoint_t ck{};         // ADER-DG
+  unsigned long long fv_scal[4] = {};  // FV: dt bits, time, next dt bits, buffer
 };
 
 size_t fv_bytes(const exa_request_t* r) {
@@ -77,6 +82,7 @@ struct exa_server {
   std::vector<double> st_time;
   std::vector<uint64_t> st_steps, st_picard;
   std::vector<int> st_active, st_nan;
+  double evict_after_s = 0.0;  // exa_server_run preemption (<= 0: off)
 };
 
 extern "C" {
@@ -161,6 +167,12 @@ exa_status_t exa_server_submit(exa_server* s, const exa_request_t* r, uint64_t* 
     cudaError_t e = cudaMemsetAsync(q.dt_slot, 0, 32, s->fv_st);
     exa_status_t st = e == cudaSuccess ? launch_fv_ic(q.fv, q.luh, r->dg.ic_param, r->dg.seed, r->dg.noise, s->fv_st)
                                        : cuda_status(e, "fv scalars");
+    // both state buffers start as the initial state: the steps write
+    // interiors only, so the ghost cells of a result are the initial ones
+    // whichever buffer holds it
+    if (!st)
+      st = cuda_status(cudaMemcpyAsync(q.luh_new, q.luh, S * S * kV * 8, cudaMemcpyDeviceToDevice, s->fv_st),
+                       "fv second buffer");
     if (!st) st = fv_patch_prime_async(q.fv, q.luh, q.dt_slot, s->fv_st);
     if (st) {
       ens_arena_free(s->ens, q.off, q.bytes);
@@ -186,7 +198,7 @@ exa_status_t rebuild_fv_groups(exa_server* s) {
   }
   for (auto& kv : s->live) {
     Req& q = kv.second;
-    if (q.done || q.r.kind != EXA_REQ_FV) continue;
+    if (q.done || q.evicted || q.r.kind != EXA_REQ_FV) continue;
     FVGroup& gr = s->groups[q.r.fv_scheme * 2 + (q.fv.pde == EXA_PDE_EULER_PLANAR ? 1 : 0)];
     FVServePatch p{};
     p.buf[0] = q.luh;
@@ -228,7 +240,7 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
   std::lock_guard<std::mutex> lk(s->mu);
   bool any_dg = false;
   for (auto& kv : s->live)
-    if (!kv.second.done && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
+    if (!kv.second.done && !kv.second.evicted && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
   if (any_dg)
     if (exa_status_t st = exa_ensemble_step(s->ens, 1)) return st;
   if (s->fv_dirty)
@@ -240,7 +252,7 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
   }
   for (auto& kv : s->live) {
     Req& q = kv.second;
-    if (q.done || q.r.kind != EXA_REQ_FV) continue;
+    if (q.done || q.evicted || q.r.kind != EXA_REQ_FV) continue;
     q.par ^= 1;
     q.steps_done++;
     if (--q.steps_left == 0) {
@@ -259,7 +271,7 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
   int n = 0;
   for (auto& kv : s->live) {
     Req& q = kv.second;
-    if (q.r.kind == EXA_REQ_ADERDG && !q.done && any_dg && !s->st_active[q.slot]) {
+    if (q.r.kind == EXA_REQ_ADERDG && !q.done && !q.evicted && any_dg && !s->st_active[q.slot]) {
       q.done = true;
       q.steps_done = (long long)s->st_steps[q.slot];
     }
@@ -331,6 +343,104 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
   return st;
 }
 
+// Eviction (SURVEY-style dump/restore of a solve's device state): the
+// request's state and time-step scalars move to host memory and its device
+// memory returns to the arena; restore re-admits it from there.
+static exa_status_t server_evict_locked(exa_server* s, Req& q) {
+  if (q.done) return set_error(EXA_EINVAL, "request already finished");
+  if (q.evicted) return EXA_OK;
+  if (q.r.kind == EXA_REQ_ADERDG) {
+    const int B = q.r.dg.order + 1;
+    q.saved.resize((size_t)q.r.dg.n[0] * q.r.dg.n[1] * B * B * kV);
+    if (exa_status_t st = exa_ensemble_checkpoint(s->ens, q.slot, q.saved.data(), &q.ck)) return st;
+    if (exa_status_t st = exa_ensemble_remove(s->ens, q.slot)) return st;
+    q.slot = -1;
+  } else {
+    const size_t S = (size_t)q.fv.patch + 2 * q.fv.ghost;
+    q.saved.resize(S * S * kV);
+    // the last tick's launches on the FV stream wrote this state
+    cudaError_t e = cudaMemcpyAsync(q.saved.data(), q.par ? q.luh_new : q.luh, q.saved.size() * 8,
+                                    cudaMemcpyDeviceToHost, s->fv_st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.fv_scal, q.dt_slot, 32, cudaMemcpyDeviceToHost, s->fv_st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->fv_st);
+    if (e != cudaSuccess) return cuda_status(e, "fv evict");
+    ens_arena_free(s->ens, q.off, q.bytes);
+    q.luh = q.luh_new = nullptr;
+    q.dt_slot = nullptr;
+    s->fv_dirty = true;
+  }
+  q.evicted = true;
+  return EXA_OK;
+}
+
+static exa_status_t server_restore_locked(exa_server* s, Req& q) {
+  if (!q.evicted) return EXA_OK;
+  if (q.r.kind == EXA_REQ_ADERDG) {
+    int slot = -1;
+    if (exa_status_t st = exa_ensemble_restore(s->ens, &q.r.dg, q.saved.data(), &q.ck, &slot)) return st;
+    q.slot = slot;
+  } else {
+    char* p = nullptr;
+    if (!ens_arena_alloc(s->ens, q.bytes, &p, &q.off))
+      return set_error(EXA_EBUSY, "not enough free device memory in the arena");
+    const size_t S = (size_t)q.fv.patch + 2 * q.fv.ghost;
+    const size_t state = ((S * S * kV * 8) + 255) & ~size_t(255);
+    q.luh = (double*)p;
+    q.luh_new = (double*)(p + state);
+    q.dt_slot = (unsigned long long*)(p + 2 * state);
+    q.par = 0;  // the state goes to buffer 0
+    unsigned long long scal[4] = {q.fv_scal[0], q.fv_scal[1], q.fv_scal[2], 0ULL};
+    // the saved state into both buffers (as at submission, both hold the
+    // same ghost cells; the next step overwrites the other's interior)
+    cudaError_t e = cudaMemcpyAsync(q.luh, q.saved.data(), q.saved.size() * 8, cudaMemcpyHostToDevice, s->fv_st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(q.luh_new, q.luh, q.saved.size() * 8, cudaMemcpyDeviceToDevice, s->fv_st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.dt_slot, scal, 32, cudaMemcpyHostToDevice, s->fv_st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->fv_st);
+    if (e != cudaSuccess) {
+      ens_arena_free(s->ens, q.off, q.bytes);
+      return cuda_status(e, "fv restore");
+    }
+    s->fv_dirty = true;
+  }
+  q.evicted = false;
+  q.saved.clear();
+  q.saved.shrink_to_fit();
+  return EXA_OK;
+}
+
+exa_status_t exa_server_evict(exa_server* s, uint64_t id) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  return server_evict_locked(s, it->second);
+}
+
+exa_status_t exa_server_restore(exa_server* s, uint64_t id) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  return server_restore_locked(s, it->second);
+}
+
+exa_status_t exa_server_evicted(exa_server* s, uint64_t id, int* evicted) {
+  if (!s || !evicted) return set_error(EXA_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  *evicted = it->second.evicted ? 1 : 0;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_set_eviction(exa_server* s, double wait_s) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->evict_after_s = wait_s > 0 ? wait_s : 0.0;
+  return EXA_OK;
+}
+
 exa_status_t exa_server_tune(exa_server* s, int launch_mode, int use_graph) {
   if (!s) return set_error(EXA_EINVAL, "NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
@@ -344,6 +454,7 @@ exa_status_t exa_server_device_state(exa_server* s, uint64_t id, double** luh_de
   auto it = s->live.find(id);
   if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
   const Req& q = it->second;
+  if (q.evicted) return set_error(EXA_EBUSY, "request evicted to host memory");
   if (q.r.kind == EXA_REQ_ADERDG) return exa_ensemble_device_state(s->ens, q.slot, luh_dev);
   *luh_dev = q.par ? q.luh_new : q.luh;
   return EXA_OK;
@@ -370,9 +481,17 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
     rec[i].sim_time = 0.0;
     rec[i].steps_done = 0;
     rec[i].status = -1;
+    rec[i].evictions = 0;
+  }
+  double evict_after = 0.0;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    evict_after = s->evict_after_s;
   }
   std::deque<int> queue;              // arrived, not yet admitted (arrival order)
   std::map<uint64_t, int> live;       // request id -> index
+  std::deque<uint64_t> evicted;       // evicted ids, in eviction order
+  std::map<uint64_t, double> resident_since;
   std::vector<double> scratch;
   std::vector<uint64_t> ids(256);
   int next = 0, done = 0;
@@ -382,9 +501,25 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
     const double t = now();
     if (time_limit_s > 0 && t > time_limit_s) break;
     while (next < n && rec[next].arrival_s <= t) queue.push_back(next++);
+    // evicted requests come back first, as soon as they fit
+    for (auto it = evicted.begin(); it != evicted.end();) {
+      const exa_status_t st = exa_server_restore(s, *it);
+      if (st == EXA_EBUSY) {
+        ++it;
+        continue;
+      }
+      if (st) {
+        err = st;
+        break;
+      }
+      resident_since[*it] = now();
+      it = evicted.erase(it);
+    }
+    if (err) break;
     // admission: first fit in arrival order (a request that does not fit
-    // now keeps its place; smaller later ones may go first)
-    for (auto it = queue.begin(); it != queue.end();) {
+    // now keeps its place; smaller later ones may go first); none while an
+    // evicted request waits to come back, so it cannot starve
+    for (auto it = queue.begin(); evicted.empty() && it != queue.end();) {
       uint64_t id = 0;
       const exa_status_t st = exa_server_submit(s, &reqs[*it], &id);
       if (st == EXA_EBUSY) {
@@ -397,9 +532,46 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
       }
       rec[*it].admitted_s = now();
       live[id] = *it;
+      resident_since[id] = rec[*it].admitted_s;
       it = queue.erase(it);
     }
     if (err) break;
+    // preemption: the oldest waiting request has waited too long: evict
+    // running requests resident for at least as long, largest footprint
+    // first, until it is admitted
+    if (evict_after > 0 && !queue.empty() && evicted.empty() && now() - rec[queue.front()].arrival_s > evict_after) {
+      std::vector<std::pair<size_t, uint64_t>> cand;
+      for (auto& kv : live) {
+        if (now() - resident_since[kv.first] < evict_after) continue;
+        cand.push_back({exa_server_footprint(&reqs[kv.second]), kv.first});
+      }
+      std::sort(cand.begin(), cand.end(), [](const std::pair<size_t, uint64_t>& a,
+                                             const std::pair<size_t, uint64_t>& b) { return a.first > b.first; });
+      const int head = queue.front();
+      for (const auto& c : cand) {
+        const exa_status_t ev = exa_server_evict(s, c.second);
+        if (ev == EXA_EINVAL) continue;  // finished in the last tick: its result is collected below
+        if (ev) {
+          err = ev;
+          break;
+        }
+        evicted.push_back(c.second);
+        rec[live[c.second]].evictions++;
+        uint64_t id = 0;
+        const exa_status_t st = exa_server_submit(s, &reqs[head], &id);
+        if (st == EXA_EBUSY) continue;
+        if (st) {
+          err = st;
+          break;
+        }
+        rec[head].admitted_s = now();
+        live[id] = head;
+        resident_since[id] = rec[head].admitted_s;
+        queue.pop_front();
+        break;
+      }
+      if (err) break;
+    }
     if (live.empty()) {
       if (next < n) {
         const double wait = rec[next].arrival_s - now();
@@ -423,6 +595,7 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
       for (int j = 0; j < k; j++) {
         const int i = live[ids[j]];
         live.erase(ids[j]);
+        resident_since.erase(ids[j]);
         double* out = results ? results[i] : nullptr;
         if (!out) {
           scratch.resize(exa_server_result_size(s, ids[j]));

@@ -29,6 +29,12 @@ def footprint(cfg):
     return int(lib().exa_ensemble_footprint(C.byref(cfg)))
 
 
+class SolveCheckpoint(C.Structure):
+    _fields_ = [('time', C.c_double), ('dt', C.c_double), ('dt_next_bits', C.c_uint64),
+                ('steps_done', C.c_uint64), ('steps_left', C.c_int64), ('picard', C.c_uint64),
+                ('nonconverged', C.c_uint64), ('active', C.c_int), ('nan_flag', C.c_int)]
+
+
 class Ensemble:
     def __init__(self, max_solves, arena_bytes, precision=_lib.PREC_FP64):
         h = C.c_void_p()
@@ -84,6 +90,26 @@ class Ensemble:
         out = np.empty(self.state_size(slot))
         call('exa_ensemble_get_state', self.h, int(slot), out.ctypes.data)
         return out
+
+    def checkpoint(self, slot):
+        """(state, SolveCheckpoint) of a solve: what restore() needs to
+        continue it bit for bit."""
+        out = np.empty(self.state_size(slot))
+        ck = SolveCheckpoint()
+        call('exa_ensemble_checkpoint', self.h, int(slot), out.ctypes.data, C.byref(ck))
+        return out, ck
+
+    def restore(self, cfg, state, ck):
+        """Adds a solve from a checkpoint; returns its slot, or None when it
+        does not fit now."""
+        state = np.ascontiguousarray(state, dtype=np.float64)
+        slot = C.c_int(-1)
+        st = lib().exa_ensemble_restore(self.h, C.byref(cfg), state.ctypes.data, C.byref(ck), C.byref(slot))
+        if st == _lib.EXA_EBUSY:
+            return None
+        _lib.check(st, 'exa_ensemble_restore')
+        self.cfgs[slot.value] = cfg
+        return slot.value
 
     def device_state_ptr(self, slot):
         p = C.c_void_p()

@@ -18,7 +18,8 @@ REQ_FV = 1
 
 class RequestRecord(C.Structure):
     _fields_ = [('arrival_s', C.c_double), ('admitted_s', C.c_double), ('completed_s', C.c_double),
-                ('sim_time', C.c_double), ('steps_done', C.c_longlong), ('status', C.c_int)]
+                ('sim_time', C.c_double), ('steps_done', C.c_longlong), ('status', C.c_int),
+                ('evictions', C.c_int)]
 
 
 class Request(C.Structure):
@@ -87,6 +88,29 @@ class Server:
         if with_status:
             return out, t.value, steps.value, st
         return out, t.value, steps.value
+
+    def evict(self, rid):
+        """Moves a running request's state to host memory and frees its
+        device memory (exa_server_evict)."""
+        call('exa_server_evict', self.h, C.c_uint64(rid))
+
+    def restore(self, rid):
+        """Re-admits an evicted request; False when it does not fit now."""
+        st = lib().exa_server_restore(self.h, C.c_uint64(rid))
+        if st == _lib.EXA_EBUSY:
+            return False
+        _lib.check(st, 'exa_server_restore')
+        return True
+
+    def evicted(self, rid):
+        v = C.c_int()
+        call('exa_server_evicted', self.h, C.c_uint64(rid), C.byref(v))
+        return bool(v.value)
+
+    def set_eviction(self, wait_s):
+        """Preemption in run_poisson / exa_server_run after wait_s seconds of
+        waiting (0: off)."""
+        call('exa_server_set_eviction', self.h, float(wait_s))
 
     def tune(self, launch_mode=0, use_graph=True):
         """ADER-DG launch form of a tick (0 persistent, 1 per order) and graph replay."""
@@ -174,4 +198,5 @@ def run_poisson(server, requests, rate, seed, collect=False, time_limit=None):
     lat = np.array([done[i][0] - arrivals[i] for i in sorted(done)])
     return dict(latency=lat, done=done, arrivals=arrivals, wall=wall, ticks=int(ticks.value),
                 cell_updates=cell_updates, failed=failed,
-                admitted=np.array([rec[i].admitted_s for i in range(n)]))
+                admitted=np.array([rec[i].admitted_s for i in range(n)]),
+                evictions=np.array([rec[i].evictions for i in range(n)]))

@@ -599,6 +599,22 @@ exa_status_t exa_ensemble_set_launch_mode(exa_ensemble* e, int mode);
 exa_status_t exa_ensemble_synchronize(exa_ensemble* e);
 exa_status_t exa_ensemble_stream(exa_ensemble* e, void** stream);
 exa_status_t exa_ensemble_get_state(exa_ensemble* e, int slot, double* host_luh);
+/* Checkpoint of one solve: its state (host_luh, as exa_ensemble_get_state)
+ * and its time-step scalars.  exa_ensemble_restore adds a solve of the same
+ * configuration from a checkpoint (EXA_EBUSY when it does not fit now); it
+ * then continues bit for bit as the checkpointed solve would have. */
+typedef struct {
+  double time;            /* simulated time */
+  double dt;              /* dt of the next step */
+  uint64_t dt_next_bits;  /* the next-dt reduction slot (bit pattern) */
+  uint64_t steps_done;
+  int64_t steps_left;     /* < 0: unlimited */
+  uint64_t picard, nonconverged;
+  int active, nan_flag;
+} exa_solve_checkpoint_t;
+exa_status_t exa_ensemble_checkpoint(exa_ensemble* e, int slot, double* host_luh, exa_solve_checkpoint_t* ck);
+exa_status_t exa_ensemble_restore(exa_ensemble* e, const exa_solve_config_t* cfg, const double* host_luh,
+                                  const exa_solve_checkpoint_t* ck, int* slot);
 exa_status_t exa_ensemble_device_state(exa_ensemble* e, int slot, double** luh_dev);
 exa_status_t exa_ensemble_status(exa_ensemble* e, double* time, uint64_t* steps_done, int* active,
                                  uint64_t* picard, int* nan_flag);
@@ -648,6 +664,20 @@ exa_status_t exa_server_tune(exa_server* s, int launch_mode, int use_graph);
  * luh; FV: the patch buffer that holds the state), for zero-copy inspection
  * between ticks */
 exa_status_t exa_server_device_state(exa_server* s, uint64_t id, double** luh_dev);
+/* Eviction: a running request's state and time-step scalars move to host
+ * memory and its device memory returns to the arena; ticks skip it until
+ * exa_server_restore re-admits it (EXA_EBUSY while it does not fit), after
+ * which it continues bit for bit as if never evicted.  exa_server_evicted
+ * reports the state. */
+exa_status_t exa_server_evict(exa_server* s, uint64_t id);
+exa_status_t exa_server_restore(exa_server* s, uint64_t id);
+exa_status_t exa_server_evicted(exa_server* s, uint64_t id, int* evicted);
+/* Preemption in exa_server_run: when the oldest waiting request has waited
+ * longer than wait_s and does not fit, running requests that have been
+ * resident for at least wait_s are evicted, largest footprint first, until
+ * it fits; evicted requests are restored, before new admissions, as soon as
+ * they fit.  wait_s <= 0 (the default): no preemption. */
+exa_status_t exa_server_set_eviction(exa_server* s, double wait_s);
 
 /* One request of a stream run by exa_server_run (times in seconds after the
  * start of the run). */
@@ -659,6 +689,7 @@ typedef struct {
   long long steps_done;  /* out */
   int status;            /* out: EXA_OK; EXA_ENAN for a solve that produced a non-finite state
                             (stopped there, its state returned, the others unaffected); -1 not completed */
+  int evictions;         /* out: how often it was evicted to host memory (exa_server_set_eviction) */
 } exa_request_record_t;
 
 /* The serving loop, from this host thread: requests arrive at their

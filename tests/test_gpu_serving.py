@@ -177,3 +177,67 @@ def test_fv_batch_equals_single_patches():
         ref, t = g.get_state(), g.status()['time']
         g.destroy()
         assert np.array_equal(got[i][0], ref) and got[i][1] == t and got[i][2] == k, i
+
+
+def test_evict_restore_continues_bitwise():
+    """Evicted requests (state and time-step scalars to host memory, device
+    memory back to the arena) restored a few ticks later finish with the
+    result of an uninterrupted run, bit for bit, while the other requests
+    keep stepping meanwhile; ADER-DG (orders 2 and 4) and both FV schemes."""
+    reqs = [S.dg_request(4, 15, 12, ic_param=0.25, seed=3, noise=1e-3),
+            S.fv_request(48, 11, scheme=1, ic_param=0.2, seed=4, noise=1e-3),
+            S.dg_request(2, 20, 9, seed=5),
+            S.fv_request(40, 10, scheme=0, seed=6, noise=1e-3)]
+    srv = S.Server(1 << 29)
+    ref = run_to_completion(srv, reqs)
+    srv.destroy()
+
+    srv = S.Server(1 << 29)
+    ids = [srv.submit(r) for r in reqs]
+    free0 = None
+    out, tick = {}, 0
+    while len(out) < len(reqs):
+        if tick == 3:
+            free0 = srv.info()['arena_free']
+            for rid in ids[:2] + ids[3:]:
+                srv.evict(rid)
+                assert srv.evicted(rid)
+            assert srv.info()['arena_free'] > free0
+        if tick == 6:
+            for rid in ids[:2] + ids[3:]:
+                assert srv.restore(rid)
+                assert not srv.evicted(rid)
+        srv.tick()
+        tick += 1
+        for rid in srv.completed():
+            out[ids.index(rid)] = srv.result(rid)
+        assert tick < 1000
+    srv.destroy()
+    for i in range(len(reqs)):
+        assert np.array_equal(ref[i][0], out[i][0]), i
+        assert ref[i][1] == out[i][1] and ref[i][2] == out[i][2], i
+
+
+def test_preemption_admits_a_waiting_request():
+    """exa_server_run with eviction after 0.05 s: a small request that does
+    not fit beside a long-running large one is admitted by evicting the
+    large one, which is restored when memory frees and still ends with its
+    uninterrupted result."""
+    big = S.dg_request(5, 60, 3000, seed=21)  # runs for about a second
+    small = S.fv_request(64, 5, scheme=1, seed=22)
+    budget = S.footprint(big) + S.footprint(small) // 2
+    assert S.footprint(small) <= budget and S.footprint(big) <= budget
+    srv = S.Server(1 << 30)
+    alone = run_to_completion(srv, [big])[0]
+    srv.destroy()
+
+    srv = S.Server(budget)
+    srv.set_eviction(0.05)
+    res = S.run_poisson(srv, [('dg', big), ('fv', small)], rate=20.0, seed=1, collect=True, time_limit=120.0)
+    srv.destroy()
+    assert sorted(res['done']) == [0, 1]
+    assert res['evictions'][0] >= 1 and res['evictions'][1] == 0
+    # the small request finished before the large one
+    assert res['done'][1][0] < res['done'][0][0]
+    st, t, steps, state = res['done'][0]
+    assert np.array_equal(state, alone[0]) and t == alone[1] and steps == alone[2]
