@@ -142,6 +142,8 @@ SIGNATURES = {
     'exa_aderdg_grid_step': (i32, [vp, i32, vp]),
     'exa_aderdg_grid_use_graph': (i32, [vp, i32]),
     'exa_aderdg_grid_stream': (i32, [vp, C.POINTER(vp)]),
+    'exa_aderdg_grid_set_debug': (i32, [vp, i32]),
+    'exa_aderdg_grid_debug_status': (i32, [vp, C.POINTER(i32), C.POINTER(u64), C.POINTER(u64)]),
     'exa_aderdg_grid_profile': (i32, [vp, i32]),
     'exa_aderdg_grid_phase_times': (i32, [vp, C.POINTER(f64), C.POINTER(f64), C.POINTER(u64)]),
     'exa_aderdg_grid_device_state': (i32, [vp, C.POINTER(vp)]),

@@ -214,6 +214,17 @@ class ADERDGGrid:
     def use_graph(self, enable=True):
         call('exa_aderdg_grid_use_graph', self.h, int(enable))
 
+    def set_debug(self, enable=True):
+        """Scan each phase's outputs for non-finite values every step."""
+        call('exa_aderdg_grid_set_debug', self.h, int(enable))
+
+    def debug_status(self):
+        """(where, step, index) of the first non-finite value seen by the
+        debug scan: where 0 none, 1 lduh, 2 lQhbnd, 3 lFhbnd, 4 luh."""
+        w, st, ix = C.c_int(), C.c_uint64(), C.c_uint64()
+        call('exa_aderdg_grid_debug_status', self.h, C.byref(w), C.byref(st), C.byref(ix))
+        return w.value, st.value, ix.value
+
     def profile(self, enable=True):
         call('exa_aderdg_grid_profile', self.h, int(enable))
 

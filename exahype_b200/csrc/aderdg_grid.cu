@@ -25,8 +25,39 @@ struct GridDev {
   unsigned long long step;
   unsigned long long stats[2];   // sum of Picard iterations, non-converged cells
   int nan_flag;
-  int pad;
+  // debug scan (exa_aderdg_grid_set_debug): the first array seen holding a
+  // non-finite value (1 lduh, 2 lQhbnd, 3 lFhbnd after the predictor; 4 luh
+  // after the update), the step and the element index
+  int nan_where;
+  unsigned long long nan_step;
+  unsigned long long nan_index;
 };
+
+__global__ void k_debug_reset(GridDev* g) {
+  g->nan_where = 0;
+  g->nan_step = ~0ULL;  // not yet recorded
+  g->nan_index = ~0ULL;
+}
+
+// Debug scan of one array for non-finite values; the first array of the
+// first step to hold one is recorded (later scans leave it), with the
+// smallest such element index of that array.
+__global__ void k_scan_nonfinite(const double* a, long n, int where, GridDev* g) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    if (isfinite(a[i])) continue;
+    const int prev = atomicCAS(&g->nan_where, 0, where);
+    if (prev == 0) {
+      atomicExch(&g->nan_step, g->step);
+      g->nan_flag = 1;
+    }
+    // the index only from the recording scan (the step's other threads may
+    // still see the step unrecorded; a later step sees it recorded)
+    const unsigned long long ns = atomicAdd(&g->nan_step, 0ULL);
+    if (prev == 0 || (prev == where && (ns == ~0ULL || ns == g->step)))
+      atomicMin(&g->nan_index, (unsigned long long)i);
+  }
+}
 
 __global__ void k_commit(GridDev* g, double* dt_log, int log_cap, int fixed, double dt_fixed) {
   const double dt = g->dt;
@@ -90,6 +121,7 @@ struct exa_aderdg_grid {
   double dt_factor = 0;
   bool primed = false;
   bool use_graph = false;
+  bool debug = false;  // scan each phase's outputs for non-finite values
   cudaGraphExec_t graph = nullptr;
   // optional per-phase CUDA-event timing (predictor / corrector+commit)
   bool profile = false;
@@ -283,6 +315,28 @@ static exa_status_t grid_limiter_reset(exa_aderdg_grid* g) {
   return cuda_status(cudaStreamSynchronize(g->st), "limiter reset");
 }
 
+// debug scans: after the predictor (after = 0) its three output arrays,
+// after the update (after = 1) the state
+static exa_status_t grid_scan(exa_aderdg_grid* g, int after) {
+  long nc;
+  size_t n_luh, n_face;
+  grid_sizes(&g->cfg, &nc, &n_luh, &n_face);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)(4 * sms);
+  if (after == 0) {
+    k_scan_nonfinite<<<grid, 256, 0, g->st>>>(g->lduh, (long)n_luh, 1, g->gd);
+    k_scan_nonfinite<<<grid, 256, 0, g->st>>>(g->qb, (long)n_face, 2, g->gd);
+    k_scan_nonfinite<<<grid, 256, 0, g->st>>>(g->fb, (long)n_face, 3, g->gd);
+    count_launch(3);
+  } else {
+    k_scan_nonfinite<<<grid, 256, 0, g->st>>>(g->luh, (long)n_luh, 4, g->gd);
+    count_launch();
+  }
+  return cuda_status(cudaGetLastError(), "k_scan_nonfinite");
+}
+
 static exa_status_t grid_commit(exa_aderdg_grid* g) {
   k_commit<<<1, 1, 0, g->st>>>(g->gd, g->dt_log, g->log_cap, g->cfg.dt_policy == 2, g->cfg.dt_fixed);
   count_launch();
@@ -299,6 +353,8 @@ static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
     if (e != cudaSuccess) return cuda_status(e, "limiter: keep previous solution");
   }
   if (exa_status_t s = grid_predict(g)) return s;
+  if (g->debug)
+    if (exa_status_t s = grid_scan(g, 0)) return s;
   if (g->profile) cudaEventRecord(g->ev[1], g->st);
   if (exa_status_t s = grid_correct(g)) return s;
   if (g->lim_on)
@@ -313,6 +369,8 @@ static exa_status_t grid_launch_step(exa_aderdg_grid* g) {
       if (exa_status_t s = launch_stable_dt(g->desc, g->ncells, g->luh, g->dt_factor, nullptr, &g->gd->dt_next, g->st))
         return s;
   }
+  if (g->debug)
+    if (exa_status_t s = grid_scan(g, 1)) return s;
   if (exa_status_t s = grid_commit(g)) return s;
   if (g->profile) {
     cudaEventRecord(g->ev[2], g->st);
@@ -444,6 +502,31 @@ exa_status_t exa_aderdg_grid_get_state(exa_aderdg_grid* g, double* host_luh) {
 exa_status_t exa_aderdg_grid_use_graph(exa_aderdg_grid* g, int enable) {
   if (!g) return set_error(EXA_EINVAL, "NULL grid");
   g->use_graph = enable != 0;
+  return EXA_OK;
+}
+
+exa_status_t exa_aderdg_grid_set_debug(exa_aderdg_grid* g, int enable) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  if (g->graph) {  // the captured step has no scans (or has them)
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  g->debug = enable != 0;
+  // a fresh record
+  k_debug_reset<<<1, 1, 0, g->st>>>(g->gd);
+  count_launch();
+  return cuda_status(cudaGetLastError(), "k_debug_reset");
+}
+
+exa_status_t exa_aderdg_grid_debug_status(exa_aderdg_grid* g, int* where, uint64_t* step, uint64_t* index) {
+  if (!g) return set_error(EXA_EINVAL, "NULL grid");
+  GridDev h{};
+  cudaError_t e = cudaMemcpyAsync(&h, g->gd, sizeof(GridDev), cudaMemcpyDeviceToHost, g->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->st);
+  if (e != cudaSuccess) return cuda_status(e, "grid debug status");
+  if (where) *where = h.nan_where;
+  if (step) *step = h.nan_where ? h.nan_step : 0;
+  if (index) *index = h.nan_where ? h.nan_index : 0;
   return EXA_OK;
 }
 

@@ -349,6 +349,15 @@ exa_status_t exa_aderdg_solution_adjustment(const exa_aderdg_desc_t* desc, long 
  * state. */
 exa_status_t exa_aderdg_grid_set_adjustment(exa_aderdg_grid* g, const exa_adjust_t* hook);
 exa_status_t exa_aderdg_grid_stream(exa_aderdg_grid* g, void** stream);
+/* Debug scan: with enable, every step scans the predictor's outputs (lduh,
+ * lQhbnd, lFhbnd) and, after the update, the state for non-finite values
+ * (one extra pass over each array).  exa_aderdg_grid_debug_status reports
+ * where the first one was seen since the scan was enabled: where = 0 none,
+ * 1 lduh, 2 lQhbnd, 3 lFhbnd, 4 luh; the step (counted from grid creation)
+ * and the smallest element index of that array.  A NaN seeded into the
+ * state shows up in the predictor's outputs of its cell (where = 1). */
+exa_status_t exa_aderdg_grid_set_debug(exa_aderdg_grid* g, int enable);
+exa_status_t exa_aderdg_grid_debug_status(exa_aderdg_grid* g, int* where, uint64_t* step, uint64_t* index);
 /* per-phase CUDA-event timing of every step (disables graph replay):
  * predictor (k_predictor) and corrector (k_corrector + k_commit) */
 exa_status_t exa_aderdg_grid_profile(exa_aderdg_grid* g, int enable);

@@ -47,6 +47,31 @@ def test_grid_nan_reported(graph):
     g.destroy()
 
 
+@pytest.mark.parametrize('graph', [False, True])
+def test_grid_debug_scan_locates_first_nonfinite(graph):
+    """Debug scan of each phase's outputs: a clean run records nothing; a
+    NaN seeded into one node of cell 7 is first seen in the predictor's lduh
+    of that cell (the cell whose Picard loop read it), in the step after it
+    was seeded."""
+    g = E.ADERDGGrid(3, 3, (4, 3, 3))
+    g.init(kind=0, param=5.0, seed=5, noise=1e-3)
+    if graph:
+        g.use_graph(True)
+    g.set_debug(True)
+    g.step(2)
+    assert g.debug_status() == (0, 0, 0)
+    u = g.get_state()
+    u[(7 * 64 + 10) * 5 + 0] = np.nan
+    g.set_state(u)
+    g.step(2)
+    where, step, index = g.debug_status()
+    assert where == 1 and step == 2
+    assert 7 * 64 * 5 <= index < 8 * 64 * 5  # lduh of cell 7
+    assert g.status()['nan']
+    g.set_debug(False)
+    g.destroy()
+
+
 @pytest.mark.parametrize('dim,n', [(2, (6, 6)), (3, (3, 3, 3))])
 def test_grid_picard_nonconvergence_reported(dim, n):
     order = 3
