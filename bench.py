@@ -168,6 +168,18 @@ def fp64_predictor_kernel(order):
     return 'k_predictor_lines' if order >= 4 else 'k_predictor'
 
 
+def mixed_predictor_kernel(order, variant=0):
+    """The mixed-precision predictor kernel for 3D Euler at this order and
+    tuning key 2 value."""
+    if order == 4 and variant in (0, 4):
+        return 'k_predictor_mixed_prog'
+    if order == 4 and variant == 3:
+        return 'k_predictor_mixed_tc'
+    if variant == 1 or (variant == 0 and order < 4):
+        return 'k_predictor_mixed'
+    return 'k_predictor_mixed_lines'
+
+
 def ncu_traffic_per_cell(kernel, order):
     """DRAM bytes per cell of the FP64 predictor from the committed ncu summary."""
     p = os.path.join(ROOT, 'profiles', '%s_3d_N%d.md' % (kernel, order))
@@ -333,7 +345,7 @@ def main():
     ap.add_argument('--serving-no-graph', action='store_true', help='serving: direct launches instead of graph replay')
     ap.add_argument('--mixed-variant', type=int, default=0,
                     help='contraction of the mixed predictor (tuning key 2): 0 default, 1 node-gather, '
-                         '2 line-owner FP32, 3 tensor cores (3D N=4)')
+                         '2 line-owner FP32, 3 tensor cores, 4 progressive line-owner (3 and 4: 3D N=4)')
     ap.add_argument('--workload', default='grid3d',
                     choices=['grid3d', 'ensemble', 'serving', 'fv', 'amr', 'limiter'],
                     help='grid3d: the 81^3 N=4 grid (default); ensemble: 512 independent 2D solves; '
@@ -588,7 +600,8 @@ def measure(ctx, precision, with_e2e):
             'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}
     else:
         out['roofline'] = {
-            'kernel': 'k_predictor_mixed_lines', 'bound': 'fp64+fp32', 'achieved_equiv_fp64_flop': achieved,
+            'kernel': mixed_predictor_kernel(order, args.mixed_variant), 'bound': 'fp64+fp32',
+            'achieved_equiv_fp64_flop': achieved,
             'unit': 'TFLOP/s', 'flop_per_cell': pred_flop, 'picard_mean_iterations': kbar,
             'ms_per_launch': pred_ms, 'frac_of_fp64_peak': achieved / ctx['fp64_peak'],
             'share_of_step': phases['predictor_ms'] / max(1e-9, phases['predictor_ms'] + phases['corrector_ms'])}

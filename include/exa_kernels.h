@@ -110,8 +110,9 @@ exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles);
  * registers, the default; 4: 128 registers), 1 = the FP64 predictor's
  * (0: unconstrained; non-zero: cap for 3 CTAs/SM), 2 = contraction of the
  * mixed predictor (1: node-gather, 2: line-owner, 3: line-owner on tensor
- * cores (3xTF32, 3D order 4); 0: line-owner for orders >= 4, node-gather
- * otherwise), 3 = the same for the FP64 predictor (1: node-gather,
+ * cores (3xTF32, 3D order 4), 4: progressive line-owner (3D order 4 Euler);
+ * 0: progressive for 3D order 4 Euler, line-owner for the other orders
+ * >= 4, node-gather otherwise), 3 = the same for the FP64 predictor (1: node-gather,
  * 2: line-owner, 3: progressive line-owner, 3D order 4 Euler; 0: progressive
  * for 3D order 4 Euler, line-owner for the other orders >= 4, node-gather
  * otherwise), 4 = cells per CTA of the limiter kernels (0: automatic).  exa_tune_get

@@ -20,10 +20,11 @@ pytestmark = pytest.mark.gpu
     (2, 5, (9, 9), 0, 20),
     (2, 2, (20, 20), 1, 30),
 ])
-@pytest.mark.parametrize('variant', [1, 2, 3])
+@pytest.mark.parametrize('variant', [1, 2, 3, 4])
 def test_mixed_vs_fp64_per_step(dim, order, n, kind, steps, variant):
     # variant (tuning key 2): 1 = node-gather contraction, 2 = line-owner,
-    # 3 = tensor-core line derivatives (3D order 4; line-owner elsewhere)
+    # 3 = tensor-core line derivatives, 4 = progressive line-owner (both 3D
+    # order 4; line-owner elsewhere)
     E._lib.call('exa_tune_set', 2, variant)
     try:
         _mixed_vs_fp64(dim, order, n, kind, steps)
@@ -52,6 +53,25 @@ def _mixed_vs_fp64(dim, order, n, kind, steps):
     assert abs(sa['picard_iters'] - sb['picard_iters']) <= 0.01 * sa['picard_iters']
     a.destroy()
     b.destroy()
+
+
+def test_progressive_mixed_equals_line_owner_bitwise():
+    """The progressive mixed predictor (tuning key 2 = 4) performs the
+    line-owner kernel's FP32 operations in the same order: the same grid
+    stepped with either is identical bit for bit (3D order 4), Picard counts
+    included."""
+    out = []
+    for variant in (2, 4):
+        E._lib.call('exa_tune_set', 2, variant)
+        try:
+            g = E.ADERDGGrid(3, 4, (5, 4, 3), precision=E.PREC_MIXED)
+            g.init(kind=0, param=5.0, seed=23, noise=1e-3)
+            g.step(5)
+            out.append((g.get_state(), g.status()['picard_iters']))
+            g.destroy()
+        finally:
+            E._lib.call('exa_tune_set', 2, 0)
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
 
 
 def test_diff_norms_utility():
