@@ -81,16 +81,16 @@ static exa_status_t launch_lines_t(const PredArgs& a, cudaStream_t st) {
 
 // progressive line-owner variant, 3D (aderdg_predictor_mixed_prog_body.cuh):
 // 44 KB of shared memory, bounded for 4 CTAs per SM
-template <int DIM, int N, bool PLANAR>
-__global__ void __launch_bounds__(MixProgShape<DIM, N>::NT, 4) k_predictor_mixed_prog(PredArgs a) {
+template <int DIM, int N, bool PLANAR, int MINB>
+__global__ void __launch_bounds__(MixProgShape<DIM, N>::NT, MINB) k_predictor_mixed_prog(PredArgs a) {
   extern __shared__ double smem[];
   predictor_mixed_prog_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
 }
 
-template <int DIM, int N>
+template <int DIM, int N, int MINB>
 static exa_status_t launch_mixed_prog(const PredArgs& a, cudaStream_t st) {
   using S = MixProgShape<DIM, N>;
-  auto kern = k_predictor_mixed_prog<DIM, N, false>;
+  auto kern = k_predictor_mixed_prog<DIM, N, false, MINB>;
   const size_t smem = sizeof(double) * S::SM_DOUBLES;
   static bool attr_done[64] = {false};
   int dev = 0;
@@ -172,8 +172,11 @@ exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& 
   // knob 2 = 4, and the default for 3D order 4 Euler: the progressive
   // line-owner form (4 CTAs per SM; measured 9 % faster per step than the
   // line-owner kernel at 81^3, bit-identical results)
-  if (d.npar == 0 && (variant == 4 || variant == 0) && d.dim == 3 && d.order == 4 && d.pde == EXA_PDE_EULER)
-    return launch_mixed_prog<3, 4>(a, st);
+  if (d.npar == 0 && (variant == 4 || variant == 0) && d.dim == 3 && d.order == 4 && d.pde == EXA_PDE_EULER) {
+    // knob 0 for this form: 5 = 96 registers (5 CTAs/SM), else 128 (4 CTAs/SM)
+    if (tune_get(kTuneMixedOccupancy, 0) == 5) return launch_mixed_prog<3, 4, 5>(a, st);
+    return launch_mixed_prog<3, 4, 4>(a, st);
+  }
   if (d.npar == 0 && (variant >= 2 || (variant == 0 && d.order >= 4)))
     return launch_predictor_mixed_lines(d, a, st);
   if (d.npar != 0) return set_error(EXA_EINVAL, "mixed precision: npar must be 0");

@@ -106,8 +106,9 @@ uint64_t exa_launch_count(void);
 exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles);
 /* Tuning knobs chosen by the autotuner (exahype_b200/autotune.py) or the
  * user; process-wide.  Keys: 0 = register budget of the 3D order-4 mixed
- * predictor as minimum resident CTAs per SM (1: unconstrained; 3: 168
- * registers, the default; 4: 128 registers), 1 = the FP64 predictor's
+ * predictor as minimum resident CTAs per SM (node-gather and line-owner
+ * forms: 1 unconstrained, 3 168 registers (the default), 4 128 registers;
+ * progressive form: 5 96 registers, otherwise 128), 1 = the FP64 predictor's
  * (0: unconstrained; non-zero: cap for 3 CTAs/SM), 2 = contraction of the
  * mixed predictor (1: node-gather, 2: line-owner, 3: line-owner on tensor
  * cores (3xTF32, 3D order 4), 4: progressive line-owner (3D order 4 Euler);
