@@ -343,6 +343,8 @@ def main():
     ap.add_argument('--serving-seconds', type=float, default=20.0, help='serving: seconds of arrivals per rate')
     ap.add_argument('--serving-mode', type=int, default=1, help='serving: ADER-DG launch form (0 persistent, 1 per order: the default)')
     ap.add_argument('--serving-no-graph', action='store_true', help='serving: direct launches instead of graph replay')
+    ap.add_argument('--serving-fv-steps', type=int, default=3,
+                    help='serving: FV steps per tick (exa_server_set_fv_steps)')
     ap.add_argument('--mixed-variant', type=int, default=0,
                     help='contraction of the mixed predictor (tuning key 2): 0 default, 1 node-gather, '
                          '2 line-owner FP32, 3 tensor cores, 4 progressive line-owner (3 and 4: 3D N=4)')
@@ -677,6 +679,7 @@ def serving_summary(args):
     arrivals) for the default run's line."""
     from exahype_b200 import serving as S
     srv = S.Server(64 << 30, max_requests=4096)
+    srv.set_fv_steps(args.serving_fv_steps)
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
     r = serving_stream(S, srv, 200.0, 30.0, args.seed + 500, args.dg_fraction)
@@ -1199,6 +1202,7 @@ def run_serving(args, rank, world, dist):
     budget = 64 << 30
     srv = S.Server(budget, max_requests=4096)
     srv.tune(args.serving_mode, not args.serving_no_graph)
+    srv.set_fv_steps(args.serving_fv_steps)
     # warm-up: a few small requests through every code path
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
@@ -1220,6 +1224,7 @@ def run_serving(args, rank, world, dist):
                            'dg': 'order U{2..5}, side log-U[9,243], steps U{20..200}',
                            'fv': 'MUSCL-Hancock, side log-U[64,1024], steps U{20..200}',
                            'loop': 'exa_server_run (C++), FV patches batched per tick',
+                           'fv_steps_per_tick': args.serving_fv_steps,
                            'dg_launch': ('per order' if args.serving_mode else 'persistent') +
                                         (', direct' if args.serving_no_graph else ', graph'),
                            'hbm_budget_gb': budget / 2 ** 30}}

@@ -224,6 +224,7 @@ SIGNATURES = {
     'exa_server_info': (i32, [vp, C.POINTER(i32), C.POINTER(C.c_long), C.POINTER(sz)]),
     'exa_server_run': (i32, [vp, vp, vp, i32, f64, vp, C.POINTER(u64)]),
     'exa_server_tune': (i32, [vp, i32, i32]),
+    'exa_server_set_fv_steps': (i32, [vp, i32]),
     'exa_server_device_state': (i32, [vp, u64, C.POINTER(vp)]),
     'exa_server_evict': (i32, [vp, u64]),
     'exa_server_restore': (i32, [vp, u64]),

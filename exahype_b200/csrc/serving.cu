@@ -5,7 +5,8 @@
 // memory footprint out of one arena (the ensemble's): a request that does
 // not fit is refused with EXA_EBUSY and the caller retries after others
 // finish.  Admitted requests stay resident on the device until their result
-// is collected.  Every tick advances every active request by one step:
+// is collected.  Every tick advances every active request (ADER-DG requests
+// by one step, FV requests by up to exa_server_set_fv_steps steps):
 //   * all ADER-DG requests together in the ensemble's single persistent
 //     launch (one launch regardless of how many requests are active);
 //   * all FV requests of one scheme together in one batched patch launch on
@@ -83,6 +84,11 @@ struct exa_server {
   std::vector<uint64_t> st_steps, st_picard;
   std::vector<int> st_active, st_nan;
   double evict_after_s = 0.0;  // exa_server_run preemption (<= 0: off)
+  // FV steps per tick (exa_server_set_fv_steps); measured on the benchmark
+  // mix at 200 req/s: 1 step p50 / p99 1.43 / 3.95 s, 2 steps 0.67 / 3.53 s,
+  // 3 steps 0.44-0.49 / 3.5-3.6 s, and choosing per tick from event timings
+  // (DG step time over one FV step's, 1..4) 0.59 / 4.43 s
+  int fv_steps = 3;
 };
 
 extern "C" {
@@ -115,6 +121,7 @@ exa_status_t exa_server_create(size_t hbm_budget, int max_requests, int precisio
   // shared memory)
   exa_ensemble_set_launch_mode(s->ens, 1);
   exa_ensemble_use_graph(s->ens, 1);
+
   s->st_time.resize(max_requests);
   s->st_steps.resize(max_requests);
   s->st_picard.resize(max_requests);
@@ -243,21 +250,29 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
     if (!kv.second.done && !kv.second.evicted && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
   if (any_dg)
     if (exa_status_t st = exa_ensemble_step(s->ens, 1)) return st;
-  if (s->fv_dirty)
-    if (exa_status_t st = rebuild_fv_groups(s)) return st;
-  for (int k = 0; k < 4; k++) {
-    FVGroup& gr = s->groups[k];
-    if (exa_status_t st = fv_serve_step_async(k / 2, k % 2 == 1, gr.dev, (int)gr.host.size(), gr.ntiles, s->fv_st))
-      return st;
-  }
-  for (auto& kv : s->live) {
-    Req& q = kv.second;
-    if (q.done || q.evicted || q.r.kind != EXA_REQ_FV) continue;
-    q.par ^= 1;
-    q.steps_done++;
-    if (--q.steps_left == 0) {
-      q.done = true;
-      s->fv_dirty = true;
+  // FV patches: several steps per tick on their own stream (they overlap
+  // the ADER-DG launch, whose step is the longer one); a patch whose budget
+  // runs out mid-tick leaves the table before the next of them
+  for (int sub = 0; sub < s->fv_steps; sub++) {
+    if (s->fv_dirty)
+      if (exa_status_t st = rebuild_fv_groups(s)) return st;
+    bool any_fv = false;
+    for (int k = 0; k < 4; k++) {
+      FVGroup& gr = s->groups[k];
+      any_fv = any_fv || !gr.host.empty();
+      if (exa_status_t st = fv_serve_step_async(k / 2, k % 2 == 1, gr.dev, (int)gr.host.size(), gr.ntiles, s->fv_st))
+        return st;
+    }
+    if (!any_fv) break;
+    for (auto& kv : s->live) {
+      Req& q = kv.second;
+      if (q.done || q.evicted || q.r.kind != EXA_REQ_FV) continue;
+      q.par ^= 1;
+      q.steps_done++;
+      if (--q.steps_left == 0) {
+        q.done = true;
+        s->fv_dirty = true;
+      }
     }
   }
   exa_status_t st = EXA_OK;
@@ -431,6 +446,13 @@ exa_status_t exa_server_evicted(exa_server* s, uint64_t id, int* evicted) {
   auto it = s->live.find(id);
   if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
   *evicted = it->second.evicted ? 1 : 0;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_set_fv_steps(exa_server* s, int steps) {
+  if (!s || steps < 1) return set_error(EXA_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->fv_steps = steps;
   return EXA_OK;
 }
 

@@ -1,8 +1,9 @@
 """Serving over the C++ engine (exa_server_* in include/exa_kernels.h): a
 seeded Poisson stream of solve requests handed to the engine's own request
 loop (exa_server_run: admission queue for requests that do not fit yet,
-continuous batching -- every tick advances all admitted requests by one
-step -- and time-to-solution records, all in C++); this module builds the
+continuous batching -- every tick advances all admitted requests, ADER-DG
+ones by one step and FV ones by up to set_fv_steps steps -- and
+time-to-solution records, all in C++); this module builds the
 requests and the arrival times and summarises the records."""
 import ctypes as C
 
@@ -115,6 +116,10 @@ class Server:
     def tune(self, launch_mode=0, use_graph=True):
         """ADER-DG launch form of a tick (0 persistent, 1 per order) and graph replay."""
         call('exa_server_tune', self.h, int(launch_mode), int(bool(use_graph)))
+
+    def set_fv_steps(self, steps):
+        """FV steps per tick (exa_server_set_fv_steps)."""
+        call('exa_server_set_fv_steps', self.h, int(steps))
 
     def device_state_ptr(self, rid):
         p = C.c_void_p()

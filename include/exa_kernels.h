@@ -637,8 +637,9 @@ exa_status_t exa_ensemble_info(exa_ensemble* e, int* grid_ctas, int* nitems,
  * Continuous batching of solve requests: admission by device-memory
  * footprint (EXA_EBUSY when a request does not fit now), state resident on
  * the device until the result is collected, every tick advances every
- * active request one step (all ADER-DG requests in one persistent launch,
- * FV patches on a second stream that overlaps it). */
+ * active request (ADER-DG requests one step, in the ensemble's launches; FV
+ * patches up to exa_server_set_fv_steps steps, on a second stream that
+ * overlaps them). */
 typedef struct exa_server exa_server;
 
 #define EXA_REQ_ADERDG 0
@@ -671,6 +672,11 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
  * a CUDA graph (re-captured whenever the set of requests changes; default
  * 1 and 1: one launch per order and phase, graph replay) */
 exa_status_t exa_server_tune(exa_server* s, int launch_mode, int use_graph);
+/* FV requests advance `steps` steps per tick (default 3), on the FV
+ * stream that overlaps the ADER-DG launch, whose step is the longer one.  A
+ * request never takes more steps than its budget, and its result is the
+ * same whatever the setting. */
+exa_status_t exa_server_set_fv_steps(exa_server* s, int steps);
 /* device pointer of a live request's current state (ADER-DG: the solve's
  * luh; FV: the patch buffer that holds the state), for zero-copy inspection
  * between ticks */
@@ -705,8 +711,8 @@ typedef struct {
 
 /* The serving loop, from this host thread: requests arrive at their
  * arrival_s; arrived requests are admitted first-fit in arrival order as
- * memory and slots free up; every tick advances every admitted request one
- * step (continuous batching, exa_server_tick); finished results are copied
+ * memory and slots free up; every tick advances every admitted request
+ * (continuous batching, exa_server_tick); finished results are copied
  * out (into results[i] when results and results[i] are non-NULL) and their
  * memory freed.  Returns when every request has completed or after
  * time_limit_s seconds (<= 0: no limit); ticks (nullable) receives the tick

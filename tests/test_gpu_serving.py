@@ -241,3 +241,21 @@ def test_preemption_admits_a_waiting_request():
     assert res['done'][1][0] < res['done'][0][0]
     st, t, steps, state = res['done'][0]
     assert np.array_equal(state, alone[0]) and t == alone[1] and steps == alone[2]
+
+
+def test_fv_steps_per_tick_same_results():
+    """FV requests advancing two or three steps per tick
+    (exa_server_set_fv_steps) end with the results of one step per tick,
+    bit for bit, including budgets that run out in the middle of a tick."""
+    reqs = [S.fv_request(48, 10, scheme=1, seed=31, noise=1e-3), S.dg_request(3, 12, 6, seed=32),
+            S.fv_request(33, 7, scheme=0, seed=33, noise=1e-3), S.fv_request(64, 8, scheme=1, seed=34)]
+    out = []
+    for k in (1, 3, 2):
+        srv = S.Server(1 << 29)
+        srv.set_fv_steps(k)
+        out.append(run_to_completion(srv, reqs, submit_at=[0, 0, 1, 2]))
+        srv.destroy()
+    for j in (1, 2):
+        for i in range(len(reqs)):
+            assert np.array_equal(out[0][i][0], out[j][i][0]), (j, i)
+            assert out[0][i][1] == out[j][i][1] and out[0][i][2] == out[j][i][2], (j, i)
