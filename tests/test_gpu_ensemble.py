@@ -170,3 +170,29 @@ def test_per_order_launches_equal_persistent(precision):
         assert np.array_equal(a.get_state(sl), b.get_state(sl)), sl
     a.destroy()
     b.destroy()
+
+
+@pytest.mark.parametrize('precision,bar', [(E.PREC_FP64, 1e-12), (E.PREC_MIXED, 1e-8)])
+def test_ensemble_vs_reference_kernels(precision, bar):
+    """Every solve of a small ensemble (orders 2..5) against the reference's
+    own kernels compiled from source stepping the same initial state the
+    same number of steps (each with its own CFL dt): relative L2 <= 1e-12
+    for FP64 and <= 1e-8 for the mixed-precision form."""
+    import _oracle as O
+    R = O.ref_lib(2)
+    if R is None or not hasattr(R, 'ref_grid_step_bc'):
+        pytest.skip('reference kernels not built')
+    mix = [(2, (10, 9), 1, 0.2, 11), (3, (9, 12), 1, 0.25, 12), (4, (8, 8), 0, 5.0, 13), (5, (7, 9), 1, 0.15, 14)]
+    ens = E.Ensemble(8, 1 << 27, precision=precision)
+    slots = [ens.add(cfg(o, n, kind, param, E.PDE_EULER, seed)) for o, n, kind, param, seed in mix]
+    init = {sl: ens.get_state(sl) for sl in slots}
+    steps = 5
+    ens.step(steps)
+    ens.synchronize()
+    for sl, (order, n, _, _, _) in zip(slots, mix):
+        ref = init[sl].copy()
+        for _ in range(steps):
+            O.ref_grid_step(2, order, n, ref, dt_policy=0)
+        got = ens.get_state(sl)
+        assert rel(got, ref) <= bar, (order, rel(got, ref))
+    ens.destroy()
