@@ -14,6 +14,7 @@ enum TuneKey {
   kTuneMixedVariant = 2,
   kTuneFp64Variant = 3,
   kTuneLimiterCellsPerCta = 4,
+  kTuneFvGodunov = 5,
   kTuneCount = 8
 };
 int tune_get(int key, int dflt);

@@ -146,6 +146,99 @@ __device__ __forceinline__ double fv_face_flux(const double* qL, const double* q
 // shared-memory carveout
 // One FV_TX x FV_TY tile (tile column bx, row by) of patch `patch` of a.luh
 // / a.out (the body of k_fv_godunov; the serving batch calls it per entry).
+// Godunov step as a sweep in y (one periodic patch, or the global view of a
+// patch grid): each warp owns a strip of FVS_W output columns (lane l =
+// column k0 - 1 + l; lanes 0 and 31 are halo columns) and walks up FVS_H
+// rows.  A lane loads its cell of the next row into registers, evaluates F_x,
+// F_y and their eigenvalue bounds once, takes the left neighbour's x values
+// by a warp shuffle and the row below's y values from its own registers, so
+// the kernel has no shared memory and no barrier.  A cell's update is the
+// tile kernel's, in the same order (x faces, bottom, then the top face once
+// the row above is known), bit for bit.
+constexpr int FVS_W = 30, FVS_WARPS = 4, FVS_H = 32;
+
+template <bool PLANAR, bool GRID>
+__global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
+  constexpr int V = kV, C = kV + 1;
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int NX = GRID ? a.P * a.npx : a.P, NY = GRID ? a.P * a.npy : a.P;
+  const int c = (blockIdx.x * FVS_WARPS + w) * FVS_W - 1 + l;  // this lane's column
+  const int j0 = blockIdx.y * FVS_H;
+  const bool out_col = l >= 1 && l <= FVS_W && c < NX;
+  const double dtv = *a.dt_dev;
+  const double cx = dtv / a.hx, cy = dtv / a.hy;
+  double dtn = DBL_MAX;
+
+  auto load = [&](int r, double* q) {
+    int flip;
+    const double* p = a.luh + fv_stencil_offset<GRID>(a, c, r, &flip);
+#pragma unroll
+    for (int m = 0; m < V; m++) q[m] = m == flip ? -p[m] : p[m];
+  };
+  // the row below the strip: its state and y flux record
+  double up[V], cyp[C];
+  load(j0 - 1, up);
+  fv_cell_flux<PLANAR>(up, 1, cyp);
+  double part[V];  // the row below's update without its top face
+#pragma unroll
+  for (int m = 0; m < V; m++) part[m] = 0.0;
+  double un[V];
+  load(j0, un);
+  for (int i = 0; i <= FVS_H; i++) {
+    const int r = j0 + i;
+    double u[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) u[m] = un[m];
+    if (i < FVS_H) load(r + 1, un);  // prefetch the next row
+    double cyr[C];
+    fv_cell_flux<PLANAR>(u, 1, cyr);
+    // the face below row r: bottom face of row r, top face of row r - 1
+    double fy[V];
+    fv_face_flux(up, u, cyp, cyr, fy);
+    if (i > 0 && out_col && r - 1 < NY) {
+      double v[V];
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        v[m] = part[m];
+        v[m] -= cy * fy[m];
+      }
+      double* o = a.out + fv_cell_offset<GRID>(a, c, r - 1);
+#pragma unroll
+      for (int m = 0; m < V; m++) o[m] = v[m];
+      dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(v, 0));
+      dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(v, 1));
+    }
+    if (i == FVS_H) break;
+    // x faces of row r: the left one from this lane and its left neighbour,
+    // the right one from the right neighbour lane
+    double cxr[C];
+    fv_cell_flux<PLANAR>(u, 0, cxr);
+    double ul[V], cxl[C];
+#pragma unroll
+    for (int m = 0; m < V; m++) ul[m] = __shfl_up_sync(0xffffffffu, u[m], 1);
+#pragma unroll
+    for (int m = 0; m < C; m++) cxl[m] = __shfl_up_sync(0xffffffffu, cxr[m], 1);
+    double fxl[V], fxr[V];
+    fv_face_flux(ul, u, cxl, cxr, fxl);
+#pragma unroll
+    for (int m = 0; m < V; m++) fxr[m] = __shfl_down_sync(0xffffffffu, fxl[m], 1);
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      double v = u[m];
+      v += cx * fxl[m];
+      v -= cx * fxr[m];
+      v += cy * fy[m];
+      part[m] = v;
+    }
+#pragma unroll
+    for (int m = 0; m < V; m++) up[m] = u[m];
+#pragma unroll
+    for (int m = 0; m < C; m++) cyp[m] = cyr[m];
+  }
+  for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
+  if (l == 0) atomic_min_pos_double(a.next_dt, dtn);
+}
+
 template <bool PLANAR, bool FUSED, bool GRID = false>
 __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by, long patch) {
   constexpr int V = kV, C = kV + 1;
@@ -946,8 +1039,16 @@ exa_status_t fv_patch_step_async(int scheme, const exa_fv_desc_t& d, const doubl
       if (e != cudaSuccess) return cuda_status(e, "godunov attribute");
       gattr[planar] = true;
     }
-    if (planar) k_fv_godunov<true, true><<<gt, FV_NT, 0, st>>>(a);
-    else k_fv_godunov<false, true><<<gt, FV_NT, 0, st>>>(a);
+    if (tune_get(kTuneFvGodunov, 0) != 1) {
+      const dim3 gs((unsigned)((d.patch + FVS_WARPS * FVS_W - 1) / (FVS_WARPS * FVS_W)),
+                    (unsigned)((d.patch + FVS_H - 1) / FVS_H), 1);
+      if (planar) k_fv_godunov_sweep<true, false><<<gs, 32 * FVS_WARPS, 0, st>>>(a);
+      else k_fv_godunov_sweep<false, false><<<gs, 32 * FVS_WARPS, 0, st>>>(a);
+    } else if (planar) {
+      k_fv_godunov<true, true><<<gt, FV_NT, 0, st>>>(a);
+    } else {
+      k_fv_godunov<false, true><<<gt, FV_NT, 0, st>>>(a);
+    }
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
@@ -1629,9 +1730,16 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
       if (e != cudaSuccess) return cuda_status(e, "godunov attribute");
       gattr[planar] = true;
     }
-    const dim3 grid((unsigned)((NX + FV_TX - 1) / FV_TX), (unsigned)((NY + FV_TY - 1) / FV_TY), 1);
-    if (planar) k_fv_godunov<true, true, true><<<grid, FV_NT, 0, g->st>>>(a);
-    else k_fv_godunov<false, true, true><<<grid, FV_NT, 0, g->st>>>(a);
+    if (tune_get(kTuneFvGodunov, 0) != 1) {
+      const dim3 gs((unsigned)((NX + FVS_WARPS * FVS_W - 1) / (FVS_WARPS * FVS_W)),
+                    (unsigned)((NY + FVS_H - 1) / FVS_H), 1);
+      if (planar) k_fv_godunov_sweep<true, true><<<gs, 32 * FVS_WARPS, 0, g->st>>>(a);
+      else k_fv_godunov_sweep<false, true><<<gs, 32 * FVS_WARPS, 0, g->st>>>(a);
+    } else {
+      const dim3 grid((unsigned)((NX + FV_TX - 1) / FV_TX), (unsigned)((NY + FV_TY - 1) / FV_TY), 1);
+      if (planar) k_fv_godunov<true, true, true><<<grid, FV_NT, 0, g->st>>>(a);
+      else k_fv_godunov<false, true, true><<<grid, FV_NT, 0, g->st>>>(a);
+    }
   } else {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {

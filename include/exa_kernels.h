@@ -116,7 +116,9 @@ exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles);
  * >= 4, node-gather otherwise), 3 = the same for the FP64 predictor (1: node-gather,
  * 2: line-owner, 3: progressive line-owner, 3D order 4 Euler; 0: progressive
  * for 3D order 4 Euler, line-owner for the other orders >= 4, node-gather
- * otherwise), 4 = cells per CTA of the limiter kernels (0: automatic).  exa_tune_get
+ * otherwise), 4 = cells per CTA of the limiter kernels (0: automatic),
+ * 5 = the fused 2D Godunov step (one patch, the patch grid; 1: 32 x 8 tile
+ * kernel; otherwise the sweep kernel, warps walking up strips of rows).  exa_tune_get
  * returns -1 for keys never set. */
 exa_status_t exa_tune_set(int key, int value);
 int exa_tune_get(int key);
