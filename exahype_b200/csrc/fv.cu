@@ -169,27 +169,62 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
   const double cx = dtv / a.hx, cy = dtv / a.hy;
   double dtn = DBL_MAX;
 
-  auto load = [&](int r, double* q) {
-    int flip;
-    const double* p = a.luh + fv_stencil_offset<GRID>(a, c, r, &flip);
+  // cell offsets split into a column part, fixed for the lane, and a row
+  // part that follows the rows as the strip walks up them (no division per
+  // row inside the domain; rows beyond it fold as fv_stencil_offset does)
+  const int D = kV + a.npar, S = a.S;
+  int fx;
+  long colc;
+  {
+    bool mx = false;
+    const int Xf = fv_fold(c, NX, GRID ? a.bcx : 0, mx);
+    fx = (GRID && mx && a.bcx == EXA_BC_REFLECT) ? 1 : -1;
+    const int px = (GRID && a.npx != 1) ? Xf / a.P : 0;
+    colc = (long)px * S * S + (a.g + Xf - px * a.P);
+  }
+  const int r0 = j0 > 0 ? j0 - 1 : 0;  // first in-domain row the strip loads
+  int py = (GRID && a.npy != 1) ? r0 / a.P : 0, ky = r0 - py * a.P;
+  auto row_part = [&](int r, int* fy) -> long {
+    if (r >= 0 && r < NY) {  // rows load in order: r is the tracked row
+      const long rc = (long)py * a.npx * S * S + (long)(a.g + ky) * S;
+      if (++ky == a.P) {
+        ky = 0;
+        ++py;
+      }
+      *fy = -1;
+      return rc;
+    }
+    bool my = false;
+    const int Yf = fv_fold(r, NY, GRID ? a.bcy : 0, my);
+    *fy = (GRID && my && a.bcy == EXA_BC_REFLECT) ? 2 : -1;
+    const int pr = (GRID && a.npy != 1) ? Yf / a.P : 0;
+    return (long)pr * a.npx * S * S + (long)(a.g + Yf - pr * a.P) * S;
+  };
+  auto load = [&](int r, double* q, long* rc) {
+    int fy;
+    *rc = row_part(r, &fy);
+    const int flip = fx >= 0 ? fx : fy;
+    const double* p = a.luh + (*rc + colc) * D;
 #pragma unroll
     for (int m = 0; m < V; m++) q[m] = m == flip ? -p[m] : p[m];
   };
   // the row below the strip: its state and y flux record
   double up[V], cyp[C];
-  load(j0 - 1, up);
+  long rc_up, rc_u, rc_n;
+  load(j0 - 1, up, &rc_up);
   fv_cell_flux<PLANAR>(up, 1, cyp);
   double part[V];  // the row below's update without its top face
 #pragma unroll
   for (int m = 0; m < V; m++) part[m] = 0.0;
   double un[V];
-  load(j0, un);
+  load(j0, un, &rc_n);
   for (int i = 0; i <= FVS_H; i++) {
     const int r = j0 + i;
     double u[V];
 #pragma unroll
     for (int m = 0; m < V; m++) u[m] = un[m];
-    if (i < FVS_H) load(r + 1, un);  // prefetch the next row
+    rc_u = rc_n;
+    if (i < FVS_H) load(r + 1, un, &rc_n);  // prefetch the next row
     double cyr[C];
     fv_cell_flux<PLANAR>(u, 1, cyr);
     // the face below row r: bottom face of row r, top face of row r - 1
@@ -202,7 +237,7 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
         v[m] = part[m];
         v[m] -= cy * fy[m];
       }
-      double* o = a.out + fv_cell_offset<GRID>(a, c, r - 1);
+      double* o = a.out + (rc_up + colc) * D;  // row r - 1, in the domain
 #pragma unroll
       for (int m = 0; m < V; m++) o[m] = v[m];
       dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(v, 0));
@@ -234,6 +269,7 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
     for (int m = 0; m < V; m++) up[m] = u[m];
 #pragma unroll
     for (int m = 0; m < C; m++) cyp[m] = cyr[m];
+    rc_up = rc_u;
   }
   for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
   if (l == 0) atomic_min_pos_double(a.next_dt, dtn);

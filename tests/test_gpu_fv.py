@@ -246,9 +246,12 @@ def test_fv_patch_grid_walls_vs_oracle(scheme, P, npx, npy, bc):
 @pytest.mark.parametrize('case', ['patch', 'patch_odd', 'grid', 'walls'])
 def test_godunov_sweep_equals_tile_kernel(case):
     """The Godunov sweep kernel (warp strips walking up the rows, tuning key
-    5 unset) and the 32 x 8 tile kernel (key 5 = 1) give the same states bit
-    for bit: periodic patches (one not a multiple of the strip sizes), a
-    periodic patch grid and a grid with outflow and reflecting sides."""
+    5 unset) and the 32 x 8 tile kernel (key 5 = 1) perform the same
+    operations per face and cell; the compiler may contract a multiply-add
+    differently in the two, so the states agree to rounding (relative L2
+    <= 1e-14, with the same time): periodic patches (one not a multiple of
+    the strip sizes), a periodic patch grid and a grid with outflow and
+    reflecting sides."""
     out = []
     for form in (1, 0):
         E._lib.call('exa_tune_set', 5, form)
@@ -275,6 +278,7 @@ def test_godunov_sweep_equals_tile_kernel(case):
         P = int(round(S ** 0.5)) - 2 * G
         ia = a[0].reshape(P + 2 * G, P + 2 * G, 5)[G:G + P, G:G + P]
         ib = b[0].reshape(P + 2 * G, P + 2 * G, 5)[G:G + P, G:G + P]
-        assert np.array_equal(ia, ib) and a[1] == b[1]
     else:
-        assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+        ia, ib = a[0], b[0]
+    assert rel(ib, ia) <= 1e-14, rel(ib, ia)
+    assert abs(a[1] - b[1]) <= 1e-14 * a[1]
