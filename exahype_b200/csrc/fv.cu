@@ -63,7 +63,11 @@ __device__ __forceinline__ int fv_fold(int X, int NX, int bc, bool& mirrored) {
   if (X >= 0 && X < NX) return X;
   if (bc == 0) return (X % NX + NX) % NX;
   mirrored = true;
-  return X < 0 ? -1 - X : 2 * NX - 1 - X;
+  // the mirror image of a ghost layer; a coordinate further out than the
+  // domain is wide (a tile or strip that overhangs a small grid) feeds only
+  // cells that are not written, and is clamped so that it reads inside
+  const int Y = X < 0 ? -1 - X : 2 * NX - 1 - X;
+  return Y < 0 ? 0 : (Y >= NX ? NX - 1 : Y);
 }
 
 // element offset of in-domain cell (X, Y); GRID = false: one periodic
