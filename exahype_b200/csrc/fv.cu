@@ -660,12 +660,43 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   // reciprocal cell sizes: multiplications instead of the reference's
   // divisions (an FP64 division is a long dependent chain)
   const double ihx = 1.0 / hx, ihy = 1.0 / hy;
-  for (int i = tid; i < LY * LX; i += FVP_NT) {
-    const int r = i / LX, c = i % LX;
-    int flip;
-    const double* q = a.luh + fv_stencil_offset<GRID>(a, k0 - 2 + c, j0 - 2 + r, &flip);
+  if constexpr (GRID) {
+    // the staged block's cell offsets as a column part per staged column
+    // and a row part per staged row (48 folds instead of one per cell),
+    // kept in the ring buffer until the ring phase
+    long* offs = reinterpret_cast<long*>(wLx);  // [LX] columns, then [LY] rows
+    int* flips = reinterpret_cast<int*>(offs + LX + LY);
+    const int S = a.S;
+    if (tid < LX) {
+      bool mx = false;
+      const int Xf = fv_fold(k0 - 2 + tid, NX, a.bcx, mx);
+      const int px = a.npx == 1 ? 0 : Xf / P;
+      offs[tid] = (long)px * S * S + (a.g + Xf - px * P);
+      flips[tid] = (mx && a.bcx == EXA_BC_REFLECT) ? 1 : -1;
+    } else if (tid < LX + LY) {
+      bool my = false;
+      const int Yf = fv_fold(j0 - 2 + (tid - LX), NY, a.bcy, my);
+      const int py = a.npy == 1 ? 0 : Yf / P;
+      offs[tid] = (long)py * a.npx * S * S + (long)(a.g + Yf - py * P) * S;
+      flips[tid] = (my && a.bcy == EXA_BC_REFLECT) ? 2 : -1;
+    }
+    __syncthreads();
+    const int D = kV + a.npar;
+    for (int i = tid; i < LY * LX; i += FVP_NT) {
+      const int r = i / LX, c = i % LX;
+      const int flip = flips[c] >= 0 ? flips[c] : flips[LX + r];
+      const double* q = a.luh + (offs[c] + offs[LX + r]) * D;
 #pragma unroll
-    for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
+      for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
+    }
+  } else {
+    for (int i = tid; i < LY * LX; i += FVP_NT) {
+      const int r = i / LX, c = i % LX;
+      int flip;
+      const double* q = a.luh + fv_stencil_offset<GRID>(a, k0 - 2 + c, j0 - 2 + r, &flip);
+#pragma unroll
+      for (int m = 0; m < V; m++) su[i * V + m] = m == flip ? -q[m] : q[m];
+    }
   }
   __syncthreads();
   // ring cells: slopes, extrapolations and the half step.  One patch: a
