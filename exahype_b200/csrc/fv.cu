@@ -664,8 +664,9 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
     // the staged block's cell offsets as a column part per staged column
     // and a row part per staged row (48 folds instead of one per cell),
     // kept in the ring buffer until the ring phase
-    long* offs = reinterpret_cast<long*>(wLx);  // [LX] columns, then [LY] rows
+    long* offs = reinterpret_cast<long*>(wRy + RY * RX * V);  // [LX] columns, then [LY] rows
     int* flips = reinterpret_cast<int*>(offs + LX + LY);
+    int* kpos = flips + LX + LY;  // position in the patch (for in-domain columns and rows)
     const int S = a.S;
     if (tid < LX) {
       bool mx = false;
@@ -673,12 +674,14 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
       const int px = a.npx == 1 ? 0 : Xf / P;
       offs[tid] = (long)px * S * S + (a.g + Xf - px * P);
       flips[tid] = (mx && a.bcx == EXA_BC_REFLECT) ? 1 : -1;
+      kpos[tid] = Xf - px * P;
     } else if (tid < LX + LY) {
       bool my = false;
       const int Yf = fv_fold(j0 - 2 + (tid - LX), NY, a.bcy, my);
       const int py = a.npy == 1 ? 0 : Yf / P;
       offs[tid] = (long)py * a.npx * S * S + (long)(a.g + Yf - py * P) * S;
       flips[tid] = (my && a.bcy == EXA_BC_REFLECT) ? 2 : -1;
+      kpos[tid] = Yf - py * P;
     }
     __syncthreads();
     const int D = kV + a.npar;
@@ -774,8 +777,18 @@ __device__ __forceinline__ void fv_muscl_periodic_tile(const FVArgs& a, int bx, 
   if (j < NY && k < NX) {
     const int ic = (r + 1) * RX + c + 1;  // this cell in the ring arrays
     const double* U = &su[((r + 2) * LX + c + 2) * V];
-    const int kx = (!GRID || a.npx == 1) ? k : k % P, ky = (!GRID || a.npy == 1) ? j : j % P;  // in the patch
-    double* o = a.out + fv_cell_offset<GRID>(a, k, j);
+    int kx = k, ky = j;  // position in the patch
+    double* o;
+    if constexpr (GRID) {
+      // the staged column c + 2 and row r + 2 are this cell's (in the domain)
+      const long* offs = reinterpret_cast<const long*>(wRy + RY * RX * V);
+      const int* kpos = reinterpret_cast<const int*>(offs + LX + LY) + LX + LY;
+      kx = kpos[c + 2];
+      ky = kpos[LX + r + 2];
+      o = a.out + (offs[c + 2] + offs[LX + r + 2]) * (kV + a.npar);
+    } else {
+      o = a.out + fv_cell_offset<GRID>(a, k, j);
+    }
     double fxl[V], fxr[V], fyb[V], fyt[V];
     if constexpr (!GRID) {
       rusanov<PLANAR>(&wRx[(ic - 1) * V], &wLx[ic * V], 0, fxl);
@@ -849,6 +862,8 @@ __global__ void __launch_bounds__(FVP_NT, 3) k_fv_muscl_periodic(FVArgs a) {
 
 constexpr size_t kMusclPeriodicSmem =
     sizeof(double) * ((FVP_TY + 4) * (FVP_TX + 4) * kV + 4 * (FVP_TY + 2) * (FVP_TX + 2) * kV);
+// the patch grid adds the staged block's offsets, flips and patch positions
+constexpr size_t kMusclGridSmem = kMusclPeriodicSmem + ((FVP_TX + 4) + (FVP_TY + 4)) * (8 + 4 + 4);
 
 // --------------------------------------------------------- stable dt
 template <bool PLANAR>
@@ -1815,15 +1830,15 @@ static exa_status_t fv_patchgrid_step_one(exa_fv_patchgrid* g) {
     static bool attr[2] = {false, false};
     if (!attr[planar]) {
       auto kern = planar ? k_fv_muscl_periodic<true, true> : k_fv_muscl_periodic<false, true>;
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclPeriodicSmem);
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMusclGridSmem);
       if (e == cudaSuccess)
         e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
       if (e != cudaSuccess) return cuda_status(e, "muscl attribute");
       attr[planar] = true;
     }
     const dim3 grid((unsigned)((NX + FVP_TX - 1) / FVP_TX), (unsigned)((NY + FVP_TY - 1) / FVP_TY), 1);
-    if (planar) k_fv_muscl_periodic<true, true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
-    else k_fv_muscl_periodic<false, true><<<grid, FVP_NT, kMusclPeriodicSmem, g->st>>>(a);
+    if (planar) k_fv_muscl_periodic<true, true><<<grid, FVP_NT, kMusclGridSmem, g->st>>>(a);
+    else k_fv_muscl_periodic<false, true><<<grid, FVP_NT, kMusclGridSmem, g->st>>>(a);
   }
   k_fv_patch_commit<<<1, 1, 0, g->st>>>(g->slots);
   count_launch(2);
