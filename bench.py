@@ -343,6 +343,8 @@ def main():
     ap.add_argument('--serving-seconds', type=float, default=20.0, help='serving: seconds of arrivals per rate')
     ap.add_argument('--serving-mode', type=int, default=1, help='serving: ADER-DG launch form (0 persistent, 1 per order: the default)')
     ap.add_argument('--serving-no-graph', action='store_true', help='serving: direct launches instead of graph replay')
+    ap.add_argument('--serving-result-mode', type=int, default=1,
+                    help='serving: result hand-out (1 overlapped with the next tick: the default, 0 synchronous)')
     ap.add_argument('--serving-fv-steps', type=int, default=3,
                     help='serving: FV steps per tick (exa_server_set_fv_steps)')
     ap.add_argument('--mixed-variant', type=int, default=0,
@@ -680,6 +682,7 @@ def serving_summary(args):
     from exahype_b200 import serving as S
     srv = S.Server(64 << 30, max_requests=4096)
     srv.set_fv_steps(args.serving_fv_steps)
+    srv.set_result_mode(args.serving_result_mode)
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
     r = serving_stream(S, srv, 200.0, 30.0, args.seed + 500, args.dg_fraction)
@@ -1153,6 +1156,7 @@ def serving_stream(S, srv, rate, seconds, seed, dg_fraction):
     n = max(8, int(round(rate * seconds)))
     reqs = S.request_mix(n, seed=seed, dg_fraction=dg_fraction)
     res = S.run_poisson(srv, reqs, rate=rate, seed=seed + 17, time_limit=seconds * 2.0 + 30.0)
+    loop = srv.loop_times()
     arr = res['arrivals']
     T = float(arr[-1])
     comp = {i: res['done'][i][0] for i in res['done']}
@@ -1180,6 +1184,9 @@ def serving_stream(S, srv, rate, seconds, seed, dg_fraction):
            'latency_growth_last_quarter': growth, 'ticks': res['ticks'], 'wall_s': res['wall'],
            'aggregate_cell_updates_per_s': res['cell_updates'] / res['wall'] if res['wall'] > 0 else 0.0}
     out['drain_after_last_arrival_s'] = last - T
+    # host seconds of the loop: launching ticks, waiting for them, handing
+    # out results (overlapped with the next tick), admission
+    out['loop_s'] = {k: round(v, 3) for k, v in loop.items()}
     # sustained: everything completed, at >= 95 % of the offered rate in
     # the steady half, within a short drain after the last arrival, and the
     # latency of the last quarter of the arrivals did not grow against the
@@ -1203,6 +1210,7 @@ def run_serving(args, rank, world, dist):
     srv = S.Server(budget, max_requests=4096)
     srv.tune(args.serving_mode, not args.serving_no_graph)
     srv.set_fv_steps(args.serving_fv_steps)
+    srv.set_result_mode(args.serving_result_mode)
     # warm-up: a few small requests through every code path
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
@@ -1225,6 +1233,7 @@ def run_serving(args, rank, world, dist):
                            'fv': 'MUSCL-Hancock, side log-U[64,1024], steps U{20..200}',
                            'loop': 'exa_server_run (C++), FV patches batched per tick',
                            'fv_steps_per_tick': args.serving_fv_steps,
+                           'result_hand_out': 'overlapped' if args.serving_result_mode else 'synchronous',
                            'dg_launch': ('per order' if args.serving_mode else 'persistent') +
                                         (', direct' if args.serving_no_graph else ', graph'),
                            'hbm_budget_gb': budget / 2 ** 30}}

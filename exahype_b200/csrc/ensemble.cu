@@ -336,6 +336,12 @@ struct exa_ensemble {
   // launch mode (exa_ensemble_set_launch_mode): 0 one persistent cooperative
   // launch per step; 1 per-order launches (items of an order contiguous)
   int mode = 0;
+  // per-order launches: the orders' predictor + corrector pairs run on one
+  // stream each (forked from st, joined before the commit), so one order's
+  // launch tail overlaps the others' work
+  cudaStream_t ost[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int order_first[6] = {0, 0, 0, 0, 0, 0}, order_count[6] = {0, 0, 0, 0, 0, 0};  // segments per order
   long order_blocks[6] = {0, 0, 0, 0, 0, 0};  // blocks of cells per order (per-order launches)
   bool order_attrs = false;
@@ -519,15 +525,24 @@ static exa_status_t launch_step_orders(exa_ensemble* e, const EnsArgs& a) {
     if (err != cudaSuccess) return cuda_status(err, "ensemble per-order attributes");
     e->order_attrs = true;
   }
-  // costly orders first, as the persistent schedule's default
-  launch_pred_order<5, PREC>(a, e, e->st);
-  launch_pred_order<4, PREC>(a, e, e->st);
-  launch_pred_order<3, PREC>(a, e, e->st);
-  launch_pred_order<2, PREC>(a, e, e->st);
-  launch_corr_order<5>(a, e, e->st);
-  launch_corr_order<4>(a, e, e->st);
-  launch_corr_order<3>(a, e, e->st);
-  launch_corr_order<2>(a, e, e->st);
+  // one branch per order present (the solves of different orders share
+  // nothing until the commit), costly orders issued first
+  cudaError_t err = cudaEventRecord(e->fork_ev, e->st);
+  for (int n = 5; n >= 2 && err == cudaSuccess; n--) {
+    if (e->order_blocks[n] == 0) continue;
+    cudaStream_t os = e->ost[n - 2];
+    err = cudaStreamWaitEvent(os, e->fork_ev, 0);
+    if (err != cudaSuccess) break;
+    switch (n) {
+      case 5: launch_pred_order<5, PREC>(a, e, os); launch_corr_order<5>(a, e, os); break;
+      case 4: launch_pred_order<4, PREC>(a, e, os); launch_corr_order<4>(a, e, os); break;
+      case 3: launch_pred_order<3, PREC>(a, e, os); launch_corr_order<3>(a, e, os); break;
+      default: launch_pred_order<2, PREC>(a, e, os); launch_corr_order<2>(a, e, os); break;
+    }
+    err = cudaEventRecord(e->join_ev[n - 2], os);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(e->st, e->join_ev[n - 2], 0);
+  }
+  if (err != cudaSuccess) return cuda_status(err, "ensemble per-order branches");
   k_ens_commit<<<(a.nsolves + 127) / 128, 128, 0, e->st>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "ensemble per-order launches");
@@ -587,6 +602,20 @@ void ens_arena_free(exa_ensemble* e, size_t off, size_t bytes) {
   arena_free(e, off, align256(bytes));
 }
 cudaStream_t ens_stream(exa_ensemble* e) { return e->st; }
+// The kernels skip an inactive solve without touching its state, faces or
+// arena range, so a finished solve's memory can go back to the arena while
+// a step is in flight; its record is zeroed after that step, in stream order.
+exa_status_t ens_remove_finished(exa_ensemble* e, int slot) {
+  std::lock_guard<std::mutex> lk(e->mu);
+  if (slot < 0 || slot >= e->max_solves || !e->used[slot]) return set_error(EXA_ENOTFOUND, "slot not in use");
+  const cudaError_t err = cudaMemsetAsync(e->d_solves + slot, 0, sizeof(SolveDev), e->st);
+  if (err != cudaSuccess) return cuda_status(err, "ensemble remove");
+  arena_free(e, e->alloc_off[slot], e->alloc_size[slot]);
+  e->used[slot] = 0;
+  e->host[slot] = SolveDev{};
+  e->dirty = true;
+  return EXA_OK;
+}
 }  // namespace exa
 
 extern "C" {
@@ -615,6 +644,11 @@ exa_status_t exa_ensemble_create(int precision, int max_solves, size_t arena_byt
   exa_status_t s = ensure_tables();
   cudaError_t err = cudaSuccess;
   if (!s) err = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+  for (int k = 0; k < 4 && !s && err == cudaSuccess; k++) {
+    err = cudaStreamCreateWithFlags(&e->ost[k], cudaStreamNonBlocking);
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->join_ev[k], cudaEventDisableTiming);
+  }
+  if (!s && err == cudaSuccess) err = cudaEventCreateWithFlags(&e->fork_ev, cudaEventDisableTiming);
   if (!s && err == cudaSuccess) err = cudaMalloc(&e->arena, arena_bytes);
   if (!s && err == cudaSuccess) err = cudaMalloc(&e->d_solves, sizeof(SolveDev) * max_solves);
   if (!s && err == cudaSuccess) err = cudaMalloc(&e->d_ctr, 2 * sizeof(unsigned int));
@@ -641,6 +675,11 @@ exa_status_t exa_ensemble_destroy(exa_ensemble* e) {
   cudaFree(e->d_items);
   cudaFree(e->d_ctr);
   if (e->st) cudaStreamDestroy(e->st);
+  for (int k = 0; k < 4; k++) {
+    if (e->ost[k]) cudaStreamDestroy(e->ost[k]);
+    if (e->join_ev[k]) cudaEventDestroy(e->join_ev[k]);
+  }
+  if (e->fork_ev) cudaEventDestroy(e->fork_ev);
   delete e;
   return EXA_OK;
 }

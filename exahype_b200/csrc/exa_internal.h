@@ -119,6 +119,9 @@ exa_status_t launch_fv_ic(const exa_fv_desc_t& d, double* luh, double amp, uint6
 bool ens_arena_alloc(exa_ensemble* e, size_t bytes, char** ptr, size_t* off);
 void ens_arena_free(exa_ensemble* e, size_t off, size_t bytes);
 cudaStream_t ens_stream(exa_ensemble* e);
+// exa_ensemble_remove of a finished solve (inactive on the device): the slot
+// is cleared in stream order and its memory returned without a host wait
+exa_status_t ens_remove_finished(exa_ensemble* e, int slot);
 
 exa_status_t launch_rusanov_one(int pde, int d, const double* qL, const double* qR, double* out);
 

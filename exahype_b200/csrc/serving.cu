@@ -19,6 +19,7 @@
 // so its result is the same alone or in any mix.
 #include <algorithm>
 #include <chrono>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <thread>
@@ -46,6 +47,7 @@ struct Req {
   long long steps_left = 0;
   long long steps_done = 0;
   bool done = false;
+  bool reported = false;  // listed for exa_server_completed once
   // eviction: the state and time-step scalars on the host, no device memory
   bool evicted = false;
   std::vector<double> saved;
@@ -89,6 +91,19 @@ struct exa_server {
   // 3 steps 0.44-0.49 / 3.5-3.6 s, and choosing per tick from event timings
   // (DG step time over one FV step's, 1..4) 0.59 / 4.43 s
   int fv_steps = 3;
+  bool tick_dg = false;  // the launched tick has ADER-DG work (tick_launch -> tick_finish)
+  // exa_server_run's result hand-out (exa_server_set_result_mode): 1 the
+  // finished states are copied into a pinned staging ring on their own
+  // stream while the next tick runs; 0 each is copied synchronously after
+  // its tick (the GPU idles meanwhile)
+  int result_mode = 1;
+  cudaStream_t res_st = nullptr;
+  char* stage = nullptr;  // pinned host memory
+  size_t stage_cap = 0;
+  std::vector<cudaEvent_t> free_events;
+  // host seconds of the last exa_server_run: launching ticks, waiting for
+  // them, handing out results, admission and eviction
+  double loop_s[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
 extern "C" {
@@ -137,6 +152,12 @@ exa_status_t exa_server_destroy(exa_server* s) {
     cudaStreamSynchronize(s->fv_st);
     cudaStreamDestroy(s->fv_st);
   }
+  if (s->res_st) {
+    cudaStreamSynchronize(s->res_st);
+    cudaStreamDestroy(s->res_st);
+  }
+  for (cudaEvent_t ev : s->free_events) cudaEventDestroy(ev);
+  if (s->stage) cudaFreeHost(s->stage);
   if (s->ens) exa_ensemble_destroy(s->ens);
   for (FVGroup& gr : s->groups) cudaFree(gr.dev);
   delete s;
@@ -242,12 +263,15 @@ exa_status_t rebuild_fv_groups(exa_server* s) {
 }
 }  // namespace
 
-exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
-  if (!s) return set_error(EXA_EINVAL, "NULL server");
-  std::lock_guard<std::mutex> lk(s->mu);
+namespace {
+// A tick in two halves: tick_launch enqueues the work (the host returns
+// while the GPU runs it), tick_finish waits for it and records the
+// completions.  Both with s->mu held.
+exa_status_t tick_launch(exa_server* s) {
   bool any_dg = false;
   for (auto& kv : s->live)
     if (!kv.second.done && !kv.second.evicted && kv.second.r.kind == EXA_REQ_ADERDG) any_dg = true;
+  s->tick_dg = any_dg;
   if (any_dg)
     if (exa_status_t st = exa_ensemble_step(s->ens, 1)) return st;
   // FV patches: several steps per tick on their own stream (they overlap
@@ -275,6 +299,11 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
       }
     }
   }
+  return EXA_OK;
+}
+
+exa_status_t tick_finish(exa_server* s, int* ncompleted) {
+  const bool any_dg = s->tick_dg;
   exa_status_t st = EXA_OK;
   if (any_dg) {
     st = exa_ensemble_status(s->ens, s->st_time.data(), s->st_steps.data(), s->st_active.data(),
@@ -290,13 +319,22 @@ exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
       q.done = true;
       q.steps_done = (long long)s->st_steps[q.slot];
     }
-    if (q.done && std::find(s->completed.begin(), s->completed.end(), q.id) == s->completed.end()) {
+    if (q.done && !q.reported) {
+      q.reported = true;
       s->completed.push_back(q.id);
       n++;
     }
   }
   if (ncompleted) *ncompleted = n;
   return st;
+}
+}  // namespace
+
+exa_status_t exa_server_tick(exa_server* s, int* ncompleted) {
+  if (!s) return set_error(EXA_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (exa_status_t st = tick_launch(s)) return st;
+  return tick_finish(s, ncompleted);
 }
 
 exa_status_t exa_server_completed(exa_server* s, uint64_t* ids, int cap, int* n) {
@@ -358,7 +396,7 @@ exa_status_t exa_server_result(exa_server* s, uint64_t id, double* host_out, dou
   return st;
 }
 
-// Eviction (SURVEY-style dump/restore of a solve's device state): the
+// Eviction (dump and restore of a solve's device state): the
 // request's state and time-step scalars move to host memory and its device
 // memory returns to the arena; restore re-admits it from there.
 static exa_status_t server_evict_locked(exa_server* s, Req& q) {
@@ -491,6 +529,86 @@ exa_status_t exa_server_info(exa_server* s, int* live_requests, long* active_dg_
   return exa_ensemble_info(s->ens, nullptr, nullptr, arena_free_bytes);
 }
 
+namespace {
+// A finished request whose state exa_server_run is copying into the pinned
+// staging ring (stage + off: the state, then for FV the 16 bytes of dt and
+// time) on the result stream
+struct PendingResult {
+  uint64_t id = 0;
+  int index = 0;
+  size_t off = 0;
+  size_t n = 0;  // doubles of the state
+  bool fv = false;
+  cudaEvent_t ev = nullptr;
+  double sim_time = 0.0;
+  long long steps = 0;
+  exa_status_t status = EXA_OK;
+};
+
+// enqueues the copy of finished request p.id's state; the tick that
+// finished it has completed, and no later tick writes it (ADER-DG: the
+// solve is inactive; FV: the patch has left the table)
+exa_status_t result_copy_begin(exa_server* s, PendingResult& p) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(p.id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  const Req& q = it->second;
+  const double* src = nullptr;
+  if (q.r.kind == EXA_REQ_ADERDG) {
+    double* d = nullptr;
+    if (exa_status_t st = exa_ensemble_device_state(s->ens, q.slot, &d)) return st;
+    src = d;
+    p.sim_time = s->st_time[q.slot];
+    p.status = s->st_nan[q.slot] ? EXA_ENAN : EXA_OK;
+  } else {
+    src = q.par ? q.luh_new : q.luh;
+  }
+  p.steps = q.steps_done;
+  char* dst = s->stage + p.off;
+  cudaError_t e = cudaMemcpyAsync(dst, src, p.n * sizeof(double), cudaMemcpyDeviceToHost, s->res_st);
+  if (e == cudaSuccess && p.fv)
+    e = cudaMemcpyAsync(dst + p.n * sizeof(double), q.dt_slot, 16, cudaMemcpyDeviceToHost, s->res_st);
+  if (e == cudaSuccess) e = cudaEventRecord(p.ev, s->res_st);
+  return cuda_status(e, "result copy");
+}
+
+// the copy of p has completed: the state goes to out (nullable), the
+// request's device memory back to the arena
+exa_status_t result_hand_out(exa_server* s, PendingResult& p, double* out) {
+  if (out) std::memcpy(out, s->stage + p.off, p.n * sizeof(double));
+  if (p.fv) {
+    double scal[2];
+    std::memcpy(scal, s->stage + p.off + p.n * sizeof(double), sizeof(scal));
+    p.sim_time = scal[1];
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->free_events.push_back(p.ev);
+  p.ev = nullptr;
+  auto it = s->live.find(p.id);
+  if (it == s->live.end()) return set_error(EXA_ENOTFOUND, "unknown request id");
+  Req& q = it->second;
+  exa_status_t st = EXA_OK;
+  if (q.r.kind == EXA_REQ_ADERDG) st = ens_remove_finished(s->ens, q.slot);
+  else ens_arena_free(s->ens, q.off, q.bytes);
+  s->live.erase(it);
+  return st;
+}
+}  // namespace
+
+exa_status_t exa_server_set_result_mode(exa_server* s, int mode) {
+  if (!s || mode < 0 || mode > 1) return set_error(EXA_EINVAL, "result mode: 0 synchronous, 1 overlapped");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->result_mode = mode;
+  return EXA_OK;
+}
+
+exa_status_t exa_server_loop_times(exa_server* s, double* seconds4) {
+  if (!s || !seconds4) return set_error(EXA_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (int k = 0; k < 4; k++) seconds4[k] = s->loop_s[k];
+  return EXA_OK;
+}
+
 exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_request_record_t* rec, int n,
                             double time_limit_s, double* const* results, uint64_t* ticks) {
   if (!s || (n > 0 && (!reqs || !rec)) || n < 0) return set_error(EXA_EINVAL, "bad argument");
@@ -506,19 +624,100 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
     rec[i].evictions = 0;
   }
   double evict_after = 0.0;
+  bool overlap = true;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     evict_after = s->evict_after_s;
+    overlap = s->result_mode == 1;
+    if (overlap && !s->res_st) {
+      const cudaError_t e = cudaStreamCreateWithFlags(&s->res_st, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_status(e, "result stream");
+    }
   }
+  double loop_s[4] = {0.0, 0.0, 0.0, 0.0};  // launch, wait, results, admission
   std::deque<int> queue;              // arrived, not yet admitted (arrival order)
-  std::map<uint64_t, int> live;       // request id -> index
+  std::map<uint64_t, int> live;       // request id -> index (running)
   std::deque<uint64_t> evicted;       // evicted ids, in eviction order
   std::map<uint64_t, double> resident_since;
   std::vector<double> scratch;
   std::vector<uint64_t> ids(256);
+  // overlapped results: copies in flight, in issue order; they occupy the
+  // staging ring from pend.front().off up to head (wrapping at stage_cap)
+  std::deque<PendingResult> pend;
+  size_t head = 0;
   int next = 0, done = 0;
   uint64_t nt = 0;
   exa_status_t err = EXA_OK;
+
+  // hands out the oldest copy in flight once it has completed (wait: block
+  // until then)
+  auto finish_front = [&](bool wait, bool* finished) -> exa_status_t {
+    *finished = false;
+    PendingResult& p = pend.front();
+    const cudaError_t e = wait ? cudaEventSynchronize(p.ev) : cudaEventQuery(p.ev);
+    if (e == cudaErrorNotReady) return EXA_OK;
+    if (e != cudaSuccess) return cuda_status(e, "result copy");
+    const exa_status_t rs = result_hand_out(s, p, results ? results[p.index] : nullptr);
+    exa_request_record_t& r = rec[p.index];
+    r.completed_s = now();
+    r.sim_time = p.sim_time;
+    r.steps_done = p.steps;
+    r.status = rs ? rs : p.status;
+    done++;
+    pend.pop_front();
+    *finished = true;
+    return rs;
+  };
+  auto finish_ready = [&](bool wait) -> exa_status_t {
+    while (!pend.empty()) {
+      bool fin = false;
+      if (exa_status_t st = finish_front(wait, &fin)) return st;
+      if (!fin) break;
+    }
+    return EXA_OK;
+  };
+  // a staging range of `bytes` for the next copy, waiting for older copies
+  // while the ring has no room
+  auto stage_alloc = [&](size_t bytes, size_t* off) -> exa_status_t {
+    bytes = (bytes + 255) & ~size_t(255);
+    for (;;) {
+      if (pend.empty()) {
+        if (bytes > s->stage_cap) {
+          std::lock_guard<std::mutex> lk(s->mu);
+          if (s->stage) cudaFreeHost(s->stage);
+          s->stage = nullptr;
+          s->stage_cap = 0;
+          const size_t cap = std::max(bytes, size_t(256) << 20);
+          const cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&s->stage), cap, cudaHostAllocDefault);
+          if (e != cudaSuccess) return cuda_status(e, "result staging memory");
+          s->stage_cap = cap;
+        }
+        *off = 0;
+        head = bytes;
+        return EXA_OK;
+      }
+      const size_t tail = pend.front().off;
+      if (head > tail) {  // [tail, head) in use
+        if (s->stage_cap - head >= bytes) {
+          *off = head;
+          head += bytes;
+          return EXA_OK;
+        }
+        if (bytes < tail) {
+          *off = 0;
+          head = bytes;
+          return EXA_OK;
+        }
+      } else if (head + bytes < tail) {  // wrapped: [tail, cap) and [0, head) in use
+        *off = head;
+        head += bytes;
+        return EXA_OK;
+      }
+      bool fin = false;
+      if (exa_status_t st = finish_front(true, &fin)) return st;
+    }
+  };
+
   while (done < n) {
     const double t = now();
     if (time_limit_s > 0 && t > time_limit_s) break;
@@ -569,7 +768,7 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
       }
       std::sort(cand.begin(), cand.end(), [](const std::pair<size_t, uint64_t>& a,
                                              const std::pair<size_t, uint64_t>& b) { return a.first > b.first; });
-      const int head = queue.front();
+      const int head_req = queue.front();
       for (const auto& c : cand) {
         const exa_status_t ev = exa_server_evict(s, c.second);
         if (ev == EXA_EINVAL) continue;  // finished in the last tick: its result is collected below
@@ -580,21 +779,29 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
         evicted.push_back(c.second);
         rec[live[c.second]].evictions++;
         uint64_t id = 0;
-        const exa_status_t st = exa_server_submit(s, &reqs[head], &id);
+        const exa_status_t st = exa_server_submit(s, &reqs[head_req], &id);
         if (st == EXA_EBUSY) continue;
         if (st) {
           err = st;
           break;
         }
-        rec[head].admitted_s = now();
-        live[id] = head;
-        resident_since[id] = rec[head].admitted_s;
+        rec[head_req].admitted_s = now();
+        live[id] = head_req;
+        resident_since[id] = rec[head_req].admitted_s;
         queue.pop_front();
         break;
       }
       if (err) break;
     }
+    loop_s[3] += now() - t;
     if (live.empty()) {
+      if (!pend.empty()) {
+        const double t1 = now();
+        err = finish_ready(true);
+        loop_s[2] += now() - t1;
+        if (err) break;
+        continue;
+      }
       if (next < n) {
         const double wait = rec[next].arrival_s - now();
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait < 0.01 ? wait : 0.01));
@@ -605,8 +812,29 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
       continue;
     }
     int nc = 0;
-    const exa_status_t st = exa_server_tick(s, &nc);
+    const double t1 = now();
+    exa_status_t st;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      st = tick_launch(s);
+    }
     nt++;
+    if (st) {
+      err = st;
+      break;
+    }
+    const double t2 = now();
+    // while the GPU runs the tick: hand out the results whose copies are done
+    if ((err = finish_ready(false))) break;
+    const double t3 = now();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      st = tick_finish(s, &nc);
+    }
+    const double t4 = now();
+    loop_s[0] += t2 - t1;
+    loop_s[2] += t3 - t2;
+    loop_s[1] += t4 - t3;
     if (st && st != EXA_ENAN) {
       err = st;
       break;
@@ -618,6 +846,36 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
         const int i = live[ids[j]];
         live.erase(ids[j]);
         resident_since.erase(ids[j]);
+        if (overlap) {
+          PendingResult p;
+          p.id = ids[j];
+          p.index = i;
+          p.n = exa_server_result_size(s, ids[j]);
+          p.fv = reqs[i].kind == EXA_REQ_FV;
+          if ((err = stage_alloc(p.n * sizeof(double) + (p.fv ? 16 : 0), &p.off))) break;
+          {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (!s->free_events.empty()) {
+              p.ev = s->free_events.back();
+              s->free_events.pop_back();
+            }
+          }
+          if (!p.ev) {
+            const cudaError_t e = cudaEventCreateWithFlags(&p.ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) {
+              err = cuda_status(e, "result event");
+              break;
+            }
+          }
+          pend.push_back(p);
+          if ((err = result_copy_begin(s, pend.back()))) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->free_events.push_back(pend.back().ev);
+            pend.pop_back();
+            break;
+          }
+          continue;
+        }
         double* out = results ? results[i] : nullptr;
         if (!out) {
           scratch.resize(exa_server_result_size(s, ids[j]));
@@ -638,7 +896,19 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
       }
       if (err || k < (int)ids.size()) break;
     }
+    loop_s[2] += now() - t4;
     if (err) break;
+  }
+  // copies still in flight (time limit, error): wait for them and hand
+  // them out, so that no request is left half collected
+  if (!pend.empty()) {
+    if (s->res_st) cudaStreamSynchronize(s->res_st);
+    const exa_status_t st = finish_ready(true);
+    if (!err) err = st;
+  }
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int k = 0; k < 4; k++) s->loop_s[k] = loop_s[k];
   }
   if (ticks) *ticks = nt;
   return err;

@@ -121,6 +121,18 @@ class Server:
         """FV steps per tick (exa_server_set_fv_steps)."""
         call('exa_server_set_fv_steps', self.h, int(steps))
 
+    def set_result_mode(self, mode):
+        """exa_server_run's result hand-out (exa_server_set_result_mode):
+        1 overlapped with the next tick (the default), 0 synchronous."""
+        call('exa_server_set_result_mode', self.h, int(mode))
+
+    def loop_times(self):
+        """Host seconds of the last exa_server_run: launching ticks, waiting
+        for them, handing out results, admission and eviction."""
+        out = (C.c_double * 4)()
+        call('exa_server_loop_times', self.h, out)
+        return dict(zip(('launch_s', 'wait_s', 'results_s', 'admission_s'), list(out)))
+
     def device_state_ptr(self, rid):
         p = C.c_void_p()
         call('exa_server_device_state', self.h, C.c_uint64(rid), C.byref(p))

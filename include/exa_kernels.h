@@ -697,6 +697,16 @@ exa_status_t exa_server_evicted(exa_server* s, uint64_t id, int* evicted);
  * it fits; evicted requests are restored, before new admissions, as soon as
  * they fit.  wait_s <= 0 (the default): no preemption. */
 exa_status_t exa_server_set_eviction(exa_server* s, double wait_s);
+/* How exa_server_run hands out finished results: 1 (the default) each
+ * finished state is copied into pinned staging memory on its own stream
+ * while the next tick runs, and handed out (copied into results[i], device
+ * memory released) once that copy has completed; 0 each is copied
+ * synchronously right after its tick, the GPU idle meanwhile.  Results are
+ * the same either way. */
+exa_status_t exa_server_set_result_mode(exa_server* s, int mode);
+/* host seconds of the last exa_server_run: [0] launching ticks, [1] waiting
+ * for them, [2] handing out results, [3] arrivals, admission and eviction */
+exa_status_t exa_server_loop_times(exa_server* s, double* seconds4);
 
 /* One request of a stream run by exa_server_run (times in seconds after the
  * start of the run). */

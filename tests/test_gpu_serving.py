@@ -259,3 +259,30 @@ def test_fv_steps_per_tick_same_results():
         for i in range(len(reqs)):
             assert np.array_equal(out[0][i][0], out[j][i][0]), (j, i)
             assert out[0][i][1] == out[j][i][1] and out[0][i][2] == out[j][i][2], (j, i)
+
+
+def test_overlapped_result_hand_out_same_results():
+    """exa_server_run hands out results while the next tick runs (result
+    mode 1, pinned staging on its own stream) with the same states, times
+    and step counts as the synchronous hand-out (mode 0)."""
+    reqs = S.request_mix(24, seed=41)
+    for _, r in reqs:  # keep the stream small
+        if r.kind == S.REQ_ADERDG:
+            r.dg.n[0] = r.dg.n[1] = min(r.dg.n[0], 40)
+        else:
+            r.fv_patch = min(r.fv_patch, 200)
+        r.steps = min(r.steps, 30)
+    got = []
+    for mode in (0, 1):
+        srv = S.Server(1 << 30)
+        srv.set_result_mode(mode)
+        res = S.run_poisson(srv, reqs, rate=400.0, seed=5, collect=True, time_limit=120.0)
+        times = srv.loop_times()
+        srv.destroy()
+        assert len(res['done']) == len(reqs) and not res['failed']
+        assert all(v >= 0.0 for v in times.values()) and times['wait_s'] > 0.0
+        got.append(res['done'])
+    for i in range(len(reqs)):
+        a, b = got[0][i], got[1][i]
+        assert a[1] == b[1] and a[2] == b[2], i
+        assert np.array_equal(a[3], b[3]), i
