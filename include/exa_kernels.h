@@ -160,8 +160,8 @@ exa_status_t exa_aderdg_spaceTimePredictor(
  * (512 KiB) that every GPU holds from library load to process exit; every
  * supported cell (order 2..5, 2D/3D, nPar <= 1) fits, larger requests get
  * EXA_EINVAL.  The first call on a device performs a one-time set-up (looks
- * up the array's device address, uploads the operator tables); make that
- * first call before any stream capture.  All calls on a device share the one
+ * up the array's device address, uploads the operator tables).  All calls
+ * on a device share the one
  * array and keep the last call's contents; calls of this process are
  * serialised by a lock, any other overlap on the GPU races.  Like the
  * drop-in it copies synchronously on the default stream. */
