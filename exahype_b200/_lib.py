@@ -231,6 +231,7 @@ SIGNATURES = {
     'exa_server_evicted': (i32, [vp, u64, C.POINTER(i32)]),
     'exa_server_set_eviction': (i32, [vp, f64]),
     'exa_server_set_result_mode': (i32, [vp, i32]),
+    'exa_server_set_staging': (i32, [vp, sz]),
     'exa_server_loop_times': (i32, [vp, dptr]),
     'exa_fv_godunov_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),
     'exa_fv_musclhancock_update': (i32, [C.POINTER(FVDesc), i64, vp, vp, f64, vp, vp]),

@@ -100,6 +100,7 @@ struct exa_server {
   cudaStream_t res_st = nullptr;
   char* stage = nullptr;  // pinned host memory
   size_t stage_cap = 0;
+  size_t stage_min = size_t(256) << 20;  // exa_server_set_staging
   std::vector<cudaEvent_t> free_events;
   // host seconds of the last exa_server_run: launching ticks, waiting for
   // them, handing out results, admission and eviction
@@ -602,6 +603,20 @@ exa_status_t exa_server_set_result_mode(exa_server* s, int mode) {
   return EXA_OK;
 }
 
+exa_status_t exa_server_set_staging(exa_server* s, size_t bytes) {
+  if (!s || bytes < 4096) return set_error(EXA_EINVAL, "staging capacity: at least 4096 bytes");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->res_st) {
+    const cudaError_t e = cudaStreamSynchronize(s->res_st);
+    if (e != cudaSuccess) return cuda_status(e, "result stream");
+  }
+  if (s->stage) cudaFreeHost(s->stage);
+  s->stage = nullptr;
+  s->stage_cap = 0;
+  s->stage_min = bytes;
+  return EXA_OK;
+}
+
 exa_status_t exa_server_loop_times(exa_server* s, double* seconds4) {
   if (!s || !seconds4) return set_error(EXA_EINVAL, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
@@ -687,7 +702,7 @@ exa_status_t exa_server_run(exa_server* s, const exa_request_t* reqs, exa_reques
           if (s->stage) cudaFreeHost(s->stage);
           s->stage = nullptr;
           s->stage_cap = 0;
-          const size_t cap = std::max(bytes, size_t(256) << 20);
+          const size_t cap = std::max(bytes, s->stage_min);
           const cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&s->stage), cap, cudaHostAllocDefault);
           if (e != cudaSuccess) return cuda_status(e, "result staging memory");
           s->stage_cap = cap;

@@ -126,6 +126,11 @@ class Server:
         1 overlapped with the next tick (the default), 0 synchronous."""
         call('exa_server_set_result_mode', self.h, int(mode))
 
+    def set_staging(self, nbytes):
+        """Capacity of the pinned staging ring of the overlapped hand-out
+        (exa_server_set_staging; default 256 MiB)."""
+        call('exa_server_set_staging', self.h, int(nbytes))
+
     def loop_times(self):
         """Host seconds of the last exa_server_run: launching ticks, waiting
         for them, handing out results, admission and eviction."""

@@ -704,6 +704,11 @@ exa_status_t exa_server_set_eviction(exa_server* s, double wait_s);
  * synchronously right after its tick, the GPU idle meanwhile.  Results are
  * the same either way. */
 exa_status_t exa_server_set_result_mode(exa_server* s, int mode);
+/* capacity of that pinned staging ring in bytes (default 256 MiB, at least
+ * 4096; allocated at the first run that needs it and grown to the largest
+ * single result); results wait for older ones to be handed out while the
+ * ring is full.  Call between runs. */
+exa_status_t exa_server_set_staging(exa_server* s, size_t bytes);
 /* host seconds of the last exa_server_run: [0] launching ticks, [1] waiting
  * for them, [2] handing out results, [3] arrivals, admission and eviction */
 exa_status_t exa_server_loop_times(exa_server* s, double* seconds4);

@@ -273,16 +273,21 @@ def test_overlapped_result_hand_out_same_results():
             r.fv_patch = min(r.fv_patch, 200)
         r.steps = min(r.steps, 30)
     got = []
-    for mode in (0, 1):
+    # mode 1 twice: the default ring, and a 1 MiB ring that the larger
+    # results outgrow and the others wrap around, waiting for older copies
+    for mode, staging in ((0, None), (1, None), (1, 1 << 20)):
         srv = S.Server(1 << 30)
         srv.set_result_mode(mode)
+        if staging:
+            srv.set_staging(staging)
         res = S.run_poisson(srv, reqs, rate=400.0, seed=5, collect=True, time_limit=120.0)
         times = srv.loop_times()
         srv.destroy()
         assert len(res['done']) == len(reqs) and not res['failed']
         assert all(v >= 0.0 for v in times.values()) and times['wait_s'] > 0.0
         got.append(res['done'])
-    for i in range(len(reqs)):
-        a, b = got[0][i], got[1][i]
-        assert a[1] == b[1] and a[2] == b[2], i
-        assert np.array_equal(a[3], b[3]), i
+    for j in (1, 2):
+        for i in range(len(reqs)):
+            a, b = got[0][i], got[j][i]
+            assert a[1] == b[1] and a[2] == b[2], (j, i)
+            assert np.array_equal(a[3], b[3]), (j, i)
