@@ -844,7 +844,8 @@ def run_fv(args, rank, world, dist):
         ridge = fp64_peak.value * 1e12 / (peaks['hbm_gbs'] * 1e9) if peaks.get('hbm_gbs') else None
         fp64_bound = ridge is not None and intensity > ridge
         r = {'value': ups, 'ms_per_step': per, 'gpu_launches': launches, 'clocks': clk,
-             'roofline': {'kernel': 'k_fv_muscl_periodic' if scheme else 'k_fv_godunov<fused>',
+             'roofline': {'kernel': 'k_fv_muscl_periodic' if scheme else
+                          ('k_fv_godunov<fused>' if '5=1' in args.tune else 'k_fv_godunov_sweep'),
                           'bound': 'fp64' if fp64_bound else 'hbm',
                           'achieved': tf if fp64_bound else hbm,
                           'peak': fp64_peak.value if fp64_bound else peaks.get('hbm_gbs'),

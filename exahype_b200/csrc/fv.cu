@@ -99,6 +99,31 @@ __device__ __forceinline__ long fv_stencil_offset(const FVArgs& a, int X, int Y,
 // Per cell-update HBM traffic: one state read, one state write.
 
 
+// The next step's CFL dt over the cells a warp updated: the minimum over
+// its cells and both directions of 0.45 h_d / s_d (s_d the cell's largest
+// |eigenvalue| in direction d, commons::stableTimeStepSize), taken as
+// 0.45 h_d / (max over its cells of s_d).  The division is monotone, so
+// this is the same value with two divisions per warp instead of two per
+// cell; a warp without cells contributes DBL_MAX as before.  Used by the
+// Godunov kernels; the MUSCL-Hancock kernels keep the per-cell form, which
+// measured faster there (their registers are capped for occupancy).
+struct FVNextDt {
+  double sx = 0.0, sy = 0.0;
+  template <bool PLANAR>
+  __device__ __forceinline__ void add(const double* u) {
+    sx = fmax(sx, euler_max_eig<PLANAR>(u, 0));
+    sy = fmax(sy, euler_max_eig<PLANAR>(u, 1));
+  }
+  // every lane of the warp calls it; lane 0 reduces into slot
+  __device__ __forceinline__ void commit(const FVArgs& a, unsigned long long* slot, bool lane0) {
+    for (int o = 16; o > 0; o >>= 1) {
+      sx = fmax(sx, __shfl_xor_sync(0xffffffffu, sx, o));
+      sy = fmax(sy, __shfl_xor_sync(0xffffffffu, sy, o));
+    }
+    if (lane0) atomic_min_pos_double(slot, fmin(DBL_MAX, fmin(0.9 / 2 * a.hx / sx, 0.9 / 2 * a.hy / sy)));
+  }
+};
+
 // Rusanov flux of the face between qL and qR in direction d
 // (riemannsolvers/c/rusanov.cpph:24-83); returns s_max.
 template <bool PLANAR>
@@ -171,7 +196,7 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
   const bool out_col = l >= 1 && l <= FVS_W && c < NX;
   const double dtv = *a.dt_dev;
   const double cx = dtv / a.hx, cy = dtv / a.hy;
-  double dtn = DBL_MAX;
+  FVNextDt ndt;
 
   // cell offsets split into a column part, fixed for the lane, and a row
   // part that follows the rows as the strip walks up them (no division per
@@ -244,8 +269,7 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
       double* o = a.out + (rc_up + colc) * D;  // row r - 1, in the domain
 #pragma unroll
       for (int m = 0; m < V; m++) o[m] = v[m];
-      dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(v, 0));
-      dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(v, 1));
+      ndt.add<PLANAR>(v);
     }
     if (i == FVS_H) break;
     // x faces of row r: the left one from this lane and its left neighbour,
@@ -275,8 +299,7 @@ __global__ void __launch_bounds__(32 * FVS_WARPS) k_fv_godunov_sweep(FVArgs a) {
     for (int m = 0; m < C; m++) cyp[m] = cyr[m];
     rc_up = rc_u;
   }
-  for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
-  if (l == 0) atomic_min_pos_double(a.next_dt, dtn);
+  ndt.commit(a, a.next_dt, l == 0);
 }
 
 template <bool PLANAR, bool FUSED, bool GRID = false>
@@ -324,7 +347,8 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
   __syncthreads();
   const double dtv = a.dt_dev ? *a.dt_dev : a.dt;
   const double cx = dtv / a.hx, cy = dtv / a.hy;
-  double dtl = DBL_MAX, dtn = DBL_MAX;
+  double dtl = DBL_MAX;
+  FVNextDt ndt;
   {
     const int r = tid / FV_TX, c = tid % FV_TX;
     const int j = j0 + r, k = k0 + c;
@@ -355,13 +379,11 @@ __device__ __forceinline__ void fv_godunov_tile(const FVArgs& a, int bx, int by,
         un[m] = u;
       }
       if (FUSED) {
-        dtn = fmin(dtn, 0.9 / 2 * a.hx / euler_max_eig<PLANAR>(un, 0));
-        dtn = fmin(dtn, 0.9 / 2 * a.hy / euler_max_eig<PLANAR>(un, 1));
+        ndt.add<PLANAR>(un);
       }
     }
     if (FUSED) {
-      for (int o = 16; o > 0; o >>= 1) dtn = fmin(dtn, __shfl_xor_sync(0xffffffffu, dtn, o));
-      if ((tid & 31) == 0) atomic_min_pos_double(a.next_dt, dtn);
+      ndt.commit(a, a.next_dt, (tid & 31) == 0);
       return;
     }
     // first ghost layer, as the reference's face loops touch it
