@@ -677,7 +677,7 @@ def ensemble_summary(args, rank):
 
 
 def serving_summary(args):
-    """One steady-state serving stream at the stated 200 req/s (30 s of
+    """One steady-state serving stream at the stated 200 req/s (60 s of
     arrivals) for the default run's line."""
     from exahype_b200 import serving as S
     srv = S.Server(64 << 30, max_requests=4096)
@@ -685,7 +685,7 @@ def serving_summary(args):
     srv.set_result_mode(args.serving_result_mode)
     S.run_poisson(srv, [('dg', S.dg_request(o, 9, 3)) for o in (2, 3, 4, 5)] + [('fv', S.fv_request(64, 3))],
                   rate=1e4, seed=1)
-    r = serving_stream(S, srv, 200.0, 30.0, args.seed + 500, args.dg_fraction)
+    r = serving_stream(S, srv, 200.0, 60.0, args.seed + 500, args.dg_fraction)
     srv.destroy()
     r['workload'] = ('Poisson stream, 25 % ADER-DG 2D (N 2..5, 9^2..243^2) and 75 % FV MUSCL-Hancock '
                      '(64^2..1024^2), 20..200 steps each, C++ request loop')
