@@ -359,6 +359,8 @@ def main():
     ap.add_argument('--rate', type=float, default=200.0)
     ap.add_argument('--dg-fraction', type=float, default=0.25)
     ap.add_argument('--nsolves', type=int, default=512)
+    ap.add_argument('--ens-orders', default='2,3,4,5', help='ensemble: orders drawn from (comma-separated)')
+    ap.add_argument('--ens-sides', default='9,81', help='ensemble: grid sides drawn uniformly from lo,hi')
     ap.add_argument('--limiter-cells', type=int, default=131072)
     ap.add_argument('--tune', action='append', default=[],
                     help='key=value tuning knob passed to exa_tune_set (see include/exa_kernels.h)')
@@ -693,12 +695,13 @@ def serving_summary(args):
 
 
 # ---------------------------------------------------------------- ensemble
-def ensemble_mix(nsolves, seed):
+def ensemble_mix(nsolves, seed, orders=(2, 3, 4, 5), sides=(9, 81)):
     """Seeded ensemble: grid side ~U{9..81}, order ~U{2..5}, sine-wave
-    density amplitude ~U(0.05, 0.3)."""
+    density amplitude ~U(0.05, 0.3) (the default mix; other orders and
+    sides for per-order measurements)."""
     rng = np.random.default_rng(seed)
-    return [(int(rng.integers(2, 6)), int(rng.integers(9, 82)), float(rng.uniform(0.05, 0.3)), int(1000 + i))
-            for i in range(nsolves)]
+    return [(int(orders[rng.integers(0, len(orders))]), int(rng.integers(sides[0], sides[1] + 1)),
+             float(rng.uniform(0.05, 0.3)), int(1000 + i)) for i in range(nsolves)]
 
 
 def run_ensemble(args, rank, world, dist):
@@ -729,7 +732,8 @@ def ensemble_measure(args, rank, dist):
     import exahype_b200 as E
     from exahype_b200 import Timer
     from exahype_b200.autotune import tune_ensemble
-    mix = ensemble_mix(args.nsolves, args.seed + rank)
+    mix = ensemble_mix(args.nsolves, args.seed + rank, tuple(int(x) for x in args.ens_orders.split(',')),
+                       tuple(int(x) for x in args.ens_sides.split(',')))
     out = {}
     for prec_name, prec in (('fp64', E.PREC_FP64), ('mixed', E.PREC_MIXED)):
         cfgs = [E.solve_config(o, (n, n), ic_kind=1, ic_param=amp, seed=sd, noise=0.0) for o, n, amp, sd in mix]
