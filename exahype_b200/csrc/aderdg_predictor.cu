@@ -94,10 +94,10 @@ __global__ void __launch_bounds__(Fp64ProgShape<DIM, N>::NT, 3) k_predictor_prog
   predictor_fp64_prog_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
 }
 
-template <int DIM, int N>
+template <int DIM, int N, bool PLANAR>
 static exa_status_t launch_prog_fp64(const PredArgs& a, cudaStream_t st) {
   using S = Fp64ProgShape<DIM, N>;
-  auto kern = k_predictor_prog<DIM, N, false>;
+  auto kern = k_predictor_prog<DIM, N, PLANAR>;
   const size_t smem = sizeof(double) * S::SM_DOUBLES;
   static bool attr_done[64] = {false};
   int dev = 0;
@@ -111,8 +111,9 @@ static exa_status_t launch_prog_fp64(const PredArgs& a, cudaStream_t st) {
     attr_done[dev & 63] = true;
   }
   if (a.ncells <= 0) return EXA_OK;
-  if (a.ncells > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
-  kern<<<(unsigned)a.ncells, S::NT, smem, st>>>(a);
+  const long blocks = (a.ncells + S::CPB - 1) / S::CPB;
+  if (blocks > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
+  kern<<<(unsigned)blocks, S::NT, smem, st>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_predictor_prog launch");
 }
@@ -123,15 +124,18 @@ static exa_status_t launch_dn(const exa_aderdg_desc_t& d, const PredArgs& a, int
   const bool planar = d.pde == EXA_PDE_EULER_PLANAR;
   // knob 3: 1 = node-gather, 2 = line-owner contraction, 3 = the
   // progressive line-owner form (FP64, not for the reference-temporaries
-  // mode); default: progressive for 3D order 4 (Euler; 3 CTAs per SM, it
-  // measured 6.5 % faster than the line-owner kernel at 81^3), line-owner
-  // for the other orders >= 4, where it measured faster in 2D and 3D (for
-  // orders 2-3 the cell has more line tasks than threads and node-gather
-  // wins)
+  // mode); default: progressive for order 4 (3D Euler: 3 CTAs per SM, it
+  // measured 6.5 % faster than the line-owner kernel at 81^3; 2D: 7 % in
+  // the ensemble's order-4 launches), line-owner for the other orders >= 4,
+  // where it measured faster in 2D and 3D (for orders 2-3 the cell has more
+  // line tasks than threads and node-gather wins)
   const int variant = tune_get(kTuneFp64Variant, 0);
-  if constexpr (DIM == 3 && N == 4)
-    if (d.npar == 0 && !full && (variant == 3 || variant == 0) && !planar)
-      return launch_prog_fp64<DIM, N>(a, st);
+  if constexpr (N == 4)
+    if (d.npar == 0 && !full && (variant == 3 || variant == 0) && !(DIM == 3 && planar)) {
+      if constexpr (DIM == 2)
+        if (planar) return launch_prog_fp64<DIM, N, true>(a, st);
+      return launch_prog_fp64<DIM, N, false>(a, st);
+    }
   if (d.npar == 0 && !full && (variant >= 2 || (variant == 0 && N >= 4))) {
     if (DIM == 3 && planar) return set_error(EXA_EINVAL, "planar Euler is a 2D PDE");
     return planar ? launch_lines_fp64<DIM, N, true>(a, st) : launch_lines_fp64<DIM, N, false>(a, st);

@@ -1,6 +1,6 @@
 // FP64 predictor + volume integral, line-owner contraction with the time
-// contraction folded in slice by slice ("progressive"), for one cell per
-// CTA (3D).
+// contraction folded in slice by slice ("progressive"): one cell per CTA
+// (3D) or several cells per CTA (2D), as the line-owner block.
 //
 // Same operator, same operations in the same order and so the same bits as
 // predictor_fp64_lines_block (aderdg_predictor_fp64_lines_body.cuh); what
@@ -51,19 +51,19 @@ struct Fp64ProgShape {
 template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, long block, double* smem) {
   using S = Fp64ProgShape<DIM, N>;
-  static_assert(S::CPB == 1, "one cell per CTA (the loop exit needs no vote)");
   constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, L = S::L, TPD = S::TPD, TPT = S::TPT;
   constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
 
-  const int s = threadIdx.x;
-  const long cell = block;
+  const int lc = threadIdx.x / G;  // cell of the CTA
+  const int s = threadIdx.x % G;
+  const long cell = block * S::CPB + lc;
   const bool valid = cell < a.ncells;
   const bool active = valid && s < NPC;
-  double* sD = smem;
+  double* sD = smem + lc * S::CELL_D;
   double* sF = sD;                    // [2][F_SLICE]
   double* sX = sD + 2 * S::F_SLICE;  // [2][X_SLICE]
-  double* sred = smem + S::CELL_D;
+  double* sred = smem + S::CPB * S::CELL_D;
 
   double lu[V];
   {
@@ -111,6 +111,7 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
   double fa[DIM][V];
   int it = 0;
   bool conv = false;
+  bool done = false;  // this cell's outputs are final (several cells per CTA)
   int buf = 0;
   for (int iter = 0; iter < MAXIT; iter++) {
     double acc[B][V];
@@ -208,7 +209,7 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
       if (res < 1e-7 * 1e-7) conv = true;
     }
     const bool last = conv || iter == MAXIT - 1;
-    if (last && active) {
+    if (last && active && !done) {
       // the outputs' flux time average: the fluxes of this iteration's
       // input iterate q, weighted and summed slice by slice in order
 #pragma unroll
@@ -228,12 +229,19 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
           for (int m = 0; m < V; m++) fa[d][m] += T.w[n] * F[d][m];
       }
     }
-    if (active)
+    if (active && !done)
 #pragma unroll
       for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) q[t][m] = acc[t][m];
-    if (last || !valid) break;
+    done = done || last;
+    // one cell per CTA: every thread holds its cell's sum, so the exit needs
+    // no vote; several cells run until the last of them is done
+    if constexpr (S::CPB == 1) {
+      if (last || !valid) break;
+    } else {
+      if (__syncthreads_and(done || !valid)) break;
+    }
   }
 
   // time averages -> staging, then faces and volume integral

@@ -254,22 +254,27 @@ def test_grid_boundary_rejects_bad_rule():
     g.destroy()
 
 
-def test_progressive_fp64_equals_line_owner_bitwise():
+@pytest.mark.parametrize('dim,pde', [(3, E.PDE_EULER), (2, E.PDE_EULER), (2, E.PDE_EULER_PLANAR)])
+def test_progressive_fp64_equals_line_owner_bitwise(dim, pde):
     """The progressive FP64 predictor performs the line-owner kernel's
     operations in the same order: the same grid, stepped with either, is
-    identical bit for bit (3D order 4, also with a dt four times the stable
+    identical bit for bit (order 4; 3D one cell per CTA, 2D four cells per
+    CTA with a partial last block; also with a dt four times the stable
     one, where cells stop at the iteration cap)."""
+    planar = int(pde == E.PDE_EULER_PLANAR)
+    n1 = (5, 4, 3) if dim == 3 else (7, 5)
+    n2 = (3,) * dim
     out = []
     for variant in (2, 3):
         E._lib.call('exa_tune_set', 3, variant)
         try:
-            g = E.ADERDGGrid(3, 4, (5, 4, 3))
+            g = E.ADERDGGrid(dim, 4, n1, pde=pde)
             g.init(kind=0, param=5.0, seed=21, noise=1e-3)
             g.step(4)
-            u0 = O.grid_ic(3, 4, (3, 3, 3), kind=0, param=5.0, seed=22, noise=1e-3)
-            nn = np.full(3, 3, dtype=np.int32)
-            dt4 = 4.0 * O.lib().orc_aderdg_grid_dt(3, 4, 0, nn, np.full(3, 1.0 / 3), u0, 0, 0.9)
-            h = E.ADERDGGrid(3, 4, (3, 3, 3), dt_policy=2, dt_fixed=dt4)
+            u0 = O.grid_ic(dim, 4, n2, kind=0, param=5.0, seed=22, noise=1e-3)
+            nn = np.full(dim, 3, dtype=np.int32)
+            dt4 = 4.0 * O.lib().orc_aderdg_grid_dt(dim, 4, planar, nn, np.full(dim, 1.0 / 3), u0, 0, 0.9)
+            h = E.ADERDGGrid(dim, 4, n2, pde=pde, dt_policy=2, dt_fixed=dt4)
             h.set_state(u0)
             h.step(1)
             out.append((g.get_state(), h.get_state(), g.status()['picard_iters'], h.status()['nonconverged']))
