@@ -55,8 +55,9 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
   constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
 
-  const int lc = threadIdx.x / G;  // cell of the CTA
-  const int s = threadIdx.x % G;
+  constexpr bool kMulti = S::CPB > 1;  // several cells per CTA
+  const int lc = kMulti ? threadIdx.x / G : 0;  // cell of the CTA
+  const int s = kMulti ? threadIdx.x % G : threadIdx.x;
   const long cell = block * S::CPB + lc;
   const bool valid = cell < a.ncells;
   const bool active = valid && s < NPC;
@@ -209,7 +210,7 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
       if (res < 1e-7 * 1e-7) conv = true;
     }
     const bool last = conv || iter == MAXIT - 1;
-    if (last && active && !done) {
+    if (last && active && (!kMulti || !done)) {
       // the outputs' flux time average: the fluxes of this iteration's
       // input iterate q, weighted and summed slice by slice in order
 #pragma unroll
@@ -229,17 +230,17 @@ __device__ __forceinline__ void predictor_fp64_prog_block(const PredArgs& a, lon
           for (int m = 0; m < V; m++) fa[d][m] += T.w[n] * F[d][m];
       }
     }
-    if (active && !done)
+    if (active && (!kMulti || !done))
 #pragma unroll
       for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) q[t][m] = acc[t][m];
-    done = done || last;
     // one cell per CTA: every thread holds its cell's sum, so the exit needs
     // no vote; several cells run until the last of them is done
-    if constexpr (S::CPB == 1) {
+    if constexpr (!kMulti) {
       if (last || !valid) break;
     } else {
+      done = done || last;
       if (__syncthreads_and(done || !valid)) break;
     }
   }
