@@ -134,7 +134,9 @@ template <int N, bool PLANAR, int PREC, bool LINES>
 __device__ __noinline__ void ens_pred(const SolveDev* sv, int block, double* smem, int precision) {
   const PredArgs a = pred_args(*sv, precision);
   if constexpr (LINES) {
-    if (PREC) predictor_mixed_lines_block<2, N, PLANAR>(a, block, smem);
+    // (compile-time branches: a dead FP64 body in the mixed instantiation
+    // raised its registers from 127 to 131, one CTA per SM fewer at order 4)
+    if constexpr (PREC != 0) predictor_mixed_lines_block<2, N, PLANAR>(a, block, smem);
     // FP64 order 4: the progressive form (three CTAs per SM in the
     // per-order launch, 7 % faster); order 5 keeps the line-owner form,
     // which its registers suit better (measured 10.9 ms per step of a
@@ -228,12 +230,13 @@ __device__ __forceinline__ WorkItem ens_segment_item(const EnsArgs& a, int first
   return WorkItem{seg.solve, b - seg.block};
 }
 
-// order 4 in FP64 (the progressive form) is bounded to three CTAs per SM
-template <int N, int PREC>
-constexpr int ens_pred_minb() { return (N == 4 && PREC == 0) ? 3 : 1; }
+// order 4 in FP64 with the line-owner contraction (the progressive form)
+// is bounded to three CTAs per SM; 0 leaves the others unconstrained
+template <int N, int PREC, bool LINES>
+constexpr int ens_pred_minb() { return (N == 4 && PREC == 0 && LINES) ? 3 : 0; }
 
 template <int N, int PREC, bool LINES>
-__global__ void __launch_bounds__(kEnsNT, ens_pred_minb<N, PREC>()) k_ens_pred_order(EnsArgs a, int first, int nseg) {
+__global__ void __launch_bounds__(kEnsNT, ens_pred_minb<N, PREC, LINES>()) k_ens_pred_order(EnsArgs a, int first, int nseg) {
   extern __shared__ double smem[];
   const WorkItem it = ens_segment_item(a, first, nseg);
   const SolveDev& sv = a.solves[it.solve];
