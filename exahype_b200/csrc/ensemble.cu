@@ -134,8 +134,7 @@ template <int N, bool PLANAR, int PREC, bool LINES>
 __device__ __noinline__ void ens_pred(const SolveDev* sv, int block, double* smem, int precision) {
   const PredArgs a = pred_args(*sv, precision);
   if constexpr (LINES) {
-    // (compile-time branches: a dead FP64 body in the mixed instantiation
-    // raised its registers from 127 to 131, one CTA per SM fewer at order 4)
+    // (compile-time branches: each instantiation holds only its own body)
     if constexpr (PREC != 0) predictor_mixed_lines_block<2, N, PLANAR>(a, block, smem);
     // FP64 order 4: the progressive form (three CTAs per SM in the
     // per-order launch, 7 % faster); order 5 keeps the line-owner form,
