@@ -87,10 +87,10 @@ __global__ void __launch_bounds__(MixProgShape<DIM, N>::NT, MINB) k_predictor_mi
   predictor_mixed_prog_block<DIM, N, PLANAR>(a, blockIdx.x, smem);
 }
 
-template <int DIM, int N, int MINB>
+template <int DIM, int N, int MINB, bool PLANAR = false>
 static exa_status_t launch_mixed_prog(const PredArgs& a, cudaStream_t st) {
   using S = MixProgShape<DIM, N>;
-  auto kern = k_predictor_mixed_prog<DIM, N, false, MINB>;
+  auto kern = k_predictor_mixed_prog<DIM, N, PLANAR, MINB>;
   const size_t smem = sizeof(double) * S::SM_DOUBLES;
   static bool attr_done[64] = {false};
   int dev = 0;
@@ -103,8 +103,9 @@ static exa_status_t launch_mixed_prog(const PredArgs& a, cudaStream_t st) {
     attr_done[dev & 63] = true;
   }
   if (a.ncells <= 0) return EXA_OK;
-  if (a.ncells > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
-  kern<<<(unsigned)a.ncells, S::NT, smem, st>>>(a);
+  const long blocks = (a.ncells + S::CPB - 1) / S::CPB;
+  if (blocks > 0x7fffffffL) return set_error(EXA_EINVAL, "too many cells");
+  kern<<<(unsigned)blocks, S::NT, smem, st>>>(a);
   count_launch();
   return cuda_status(cudaGetLastError(), "k_predictor_mixed_prog launch");
 }
@@ -164,7 +165,8 @@ static exa_status_t launch_predictor_mixed_lines(const exa_aderdg_desc_t& d, con
 exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& a, cudaStream_t st) {
   // knob 2: 1 = node-gather contraction, 2 = line-owner contraction,
   // 3 = line-owner on tensor cores, 4 = progressive line-owner; default:
-  // progressive for 3D order 4 Euler, line-owner for the other orders >= 4
+  // progressive for 3D order 4 Euler and 2D order 5, line-owner for the
+  // other orders >= 4
   // (measured faster in 2D and 3D), node-gather for orders 2-3
   const int variant = tune_get(kTuneMixedVariant, 0);
   if (d.npar == 0 && variant == 3 && d.dim == 3 && d.order == 4 && d.pde == EXA_PDE_EULER)
@@ -176,6 +178,12 @@ exa_status_t launch_predictor_mixed(const exa_aderdg_desc_t& d, const PredArgs& 
     // knob 0 for this form: 5 = 96 registers (5 CTAs/SM), else 128 (4 CTAs/SM)
     if (tune_get(kTuneMixedOccupancy, 0) == 5) return launch_mixed_prog<3, 4, 5>(a, st);
     return launch_mixed_prog<3, 4, 4>(a, st);
+  }
+  // and for 2D order 5 (two cells per CTA, 128 registers: 4 CTAs per SM
+  // instead of 3; 8 % faster in the ensemble's order-5 launches)
+  if (d.npar == 0 && (variant == 4 || variant == 0) && d.dim == 2 && d.order == 5) {
+    if (d.pde == EXA_PDE_EULER_PLANAR) return launch_mixed_prog<2, 5, 4, true>(a, st);
+    return launch_mixed_prog<2, 5, 4, false>(a, st);
   }
   if (d.npar == 0 && (variant >= 2 || (variant == 0 && d.order >= 4)))
     return launch_predictor_mixed_lines(d, a, st);

@@ -1,6 +1,6 @@
 // Mixed-precision predictor, line-owner contraction with the time
-// contraction folded in slice by slice ("progressive"), one cell per CTA
-// (3D).
+// contraction folded in slice by slice ("progressive"): one cell per CTA
+// (3D) or several cells per CTA (2D), as the line-owner block.
 //
 // Same operator, same FP32 operations in the same order and so the same
 // bits as predictor_mixed_lines_block (aderdg_predictor_lines_body.cuh);
@@ -51,22 +51,23 @@ template <int DIM, int N, bool PLANAR>
 __device__ __forceinline__ void predictor_mixed_prog_block(const PredArgs& a, long block, double* smem) {
   using S = MixProgShape<DIM, N>;
   using LS = LineShape<DIM, N>;
-  static_assert(S::CPB == 1, "one cell per CTA (the loop exit needs no vote)");
+  constexpr bool kMulti = S::CPB > 1;  // several cells per CTA (2D)
   constexpr int B = S::B, V = S::V, NPC = S::NPC, G = S::G, L = LS::L, TPD = LS::TPD, TPT = LS::TPT;
   constexpr int MAXIT = 2 * (N + 1);
   const DGConst& T = c_dg[N];
   const DGConstF& TF = c_dgf[N];
 
-  const int s = threadIdx.x;
-  const long cell = block;
+  const int lc = kMulti ? threadIdx.x / G : 0;  // cell of the CTA
+  const int s = kMulti ? threadIdx.x % G : threadIdx.x;
+  const long cell = block * S::CPB + lc;
   const bool valid = cell < a.ncells;
   const bool active = valid && s < NPC;
-  float* cf = reinterpret_cast<float*>(smem);
-  double* sD = smem;                    // FP64 staging (before / after the loop)
+  float* cf = reinterpret_cast<float*>(smem) + lc * S::CELL_F;
+  double* sD = reinterpret_cast<double*>(cf);  // FP64 staging (before / after the loop)
   float* sF = cf;                       // [2][F_SLICE]
   float* sX = cf + 2 * LS::F_SLICE;     // [2][X_SLICE]
   float* sB = sX + 2 * S::X_SLICE;      // [B][V][NPC]
-  double* sred = smem + S::CELL_F / 2;
+  double* sred = smem + S::CPB * S::CELL_F / 2;
 
   double lu[V];
   {
@@ -182,6 +183,7 @@ __device__ __forceinline__ void predictor_mixed_prog_block(const PredArgs& a, lo
     for (int m = 0; m < V; m++) fa[d][m] = 0.f;
   int it = 0;
   bool conv = false;
+  bool done = false;  // this cell's outputs are final (several cells per CTA)
   int buf = 0;
   for (int iter = 0; iter < MAXIT; iter++) {
     F5 acc[B];
@@ -286,7 +288,7 @@ __device__ __forceinline__ void predictor_mixed_prog_block(const PredArgs& a, lo
       if (res < 1e-7 * 1e-7) conv = true;
     }
     const bool last = conv || iter == MAXIT - 1;
-    if (last && active) {
+    if (last && active && (!kMulti || !done)) {
       // the outputs' time-weighted flux deviations: those of this
       // iteration's input deviations, weighted and summed slice by slice
       // (the first iterate's slices are all deviation 0)
@@ -302,13 +304,19 @@ __device__ __forceinline__ void predictor_mixed_prog_block(const PredArgs& a, lo
       }
     }
     // (with one cell per CTA an iteration never starts converged: the loop
-    // ends in the iteration that converges)
-    if (active)
+    // ends in the iteration that converges; several cells run until the
+    // last of them is done, the others' outputs fixed)
+    if (active && (!kMulti || !done))
 #pragma unroll
       for (int t = 0; t < B; t++)
 #pragma unroll
         for (int m = 0; m < V; m++) dq[t][m] = f5_get(acc[t], m);
-    if (last || !valid) break;
+    if constexpr (!kMulti) {
+      if (last || !valid) break;
+    } else {
+      done = done || last;
+      if (__syncthreads_and(done || !valid)) break;
+    }
   }
 
   mixed_outputs<DIM, N, PLANAR>(a, cell, s, valid, active, dq, fa, sD, it, conv);

@@ -55,16 +55,19 @@ def _mixed_vs_fp64(dim, order, n, kind, steps):
     b.destroy()
 
 
-def test_progressive_mixed_equals_line_owner_bitwise():
+@pytest.mark.parametrize('dim,order,n,pde', [(3, 4, (5, 4, 3), E.PDE_EULER), (2, 5, (7, 5), E.PDE_EULER),
+                                             (2, 5, (7, 5), E.PDE_EULER_PLANAR)])
+def test_progressive_mixed_equals_line_owner_bitwise(dim, order, n, pde):
     """The progressive mixed predictor (tuning key 2 = 4) performs the
     line-owner kernel's FP32 operations in the same order: the same grid
-    stepped with either is identical bit for bit (3D order 4), Picard counts
-    included."""
+    stepped with either is identical bit for bit (3D order 4, one cell per
+    CTA; 2D order 5, two cells per CTA with a partial last block), Picard
+    counts included."""
     out = []
     for variant in (2, 4):
         E._lib.call('exa_tune_set', 2, variant)
         try:
-            g = E.ADERDGGrid(3, 4, (5, 4, 3), precision=E.PREC_MIXED)
+            g = E.ADERDGGrid(dim, order, n, pde=pde, precision=E.PREC_MIXED)
             g.init(kind=0, param=5.0, seed=23, noise=1e-3)
             g.step(5)
             out.append((g.get_state(), g.status()['picard_iters']))
