@@ -111,12 +111,12 @@ exa_status_t exa_dropin_workspace_doubles(int device, size_t* doubles);
  * progressive form: 5 96 registers, otherwise 128), 1 = the FP64 predictor's
  * (0: unconstrained; non-zero: cap for 3 CTAs/SM), 2 = contraction of the
  * mixed predictor (1: node-gather, 2: line-owner, 3: line-owner on tensor
- * cores (3xTF32, 3D order 4), 4: progressive line-owner (3D order 4 Euler);
- * 0: progressive for 3D order 4 Euler, line-owner for the other orders
- * >= 4, node-gather otherwise), 3 = the same for the FP64 predictor (1: node-gather,
- * 2: line-owner, 3: progressive line-owner, 3D order 4 Euler; 0: progressive
- * for 3D order 4 Euler, line-owner for the other orders >= 4, node-gather
- * otherwise), 4 = cells per CTA of the limiter kernels (0: automatic),
+ * cores (3xTF32, 3D order 4), 4: progressive line-owner (3D order 4 Euler,
+ * 2D order 5); 0: progressive for 3D order 4 Euler and 2D order 5,
+ * line-owner for the other orders >= 4, node-gather otherwise), 3 = the same
+ * for the FP64 predictor (1: node-gather, 2: line-owner, 3: progressive
+ * line-owner, order 4 (3D: Euler); 0: progressive for order 4 (3D: Euler),
+ * line-owner for the other orders >= 4, node-gather otherwise), 4 = cells per CTA of the limiter kernels (0: automatic),
  * 5 = the fused 2D Godunov step (one patch, the patch grid; 1: 32 x 8 tile
  * kernel; otherwise the sweep kernel, warps walking up strips of rows).  exa_tune_get
  * returns -1 for keys never set. */
