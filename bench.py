@@ -731,7 +731,7 @@ def ensemble_measure(args, rank, dist):
     schedule, graph-replayed steps); returns their figures."""
     import exahype_b200 as E
     from exahype_b200 import Timer
-    from exahype_b200.autotune import tune_ensemble
+    from exahype_b200.autotune import tune_contraction, tune_ensemble
     mix = ensemble_mix(args.nsolves, args.seed + rank, tuple(int(x) for x in args.ens_orders.split(',')),
                        tuple(int(x) for x in args.ens_sides.split(',')))
     out = {}
@@ -766,10 +766,14 @@ def ensemble_measure(args, rank, dist):
             return updates / (ms * 1e-3), ms / args.steps, launches / args.steps
         value, ms_step, lps = timed()
         cells = ens.active_cells()
-        # the same step as one launch per order and phase (replayed as one graph)
+        # the same step as one launch per order and phase (replayed as one
+        # graph), its contraction per order tuned again in that form (each
+        # order's kernel has its own occupancy there)
         ens.set_launch_mode(1)
+        mask1, _ = tune_contraction(ens, steps=3, mask=best[3])
         v1, ms1, lps1 = timed()
         ens.set_launch_mode(0)
+        ens.tune_contraction(best[3])
         out[prec_name] = {'value': value, 'ms_per_step': ms_step, 'cells': cells, 'launches_per_step': lps,
                           'form': 'one persistent cooperative launch per step, CUDA-graph replay',
                           'tuned': {'ctas_per_sm': best[0], 'grab': best[1], 'order_policy': best[2],
@@ -777,6 +781,7 @@ def ensemble_measure(args, rank, dist):
                           'tuning_table': table,
                           'per_order_launches': {'value': v1, 'ms_per_step': ms1, 'graph_launches_per_step': lps1,
                                                  'speedup_vs_persistent': v1 / value,
+                                                 'line_owner_orders': [n for n in range(2, 6) if (mask1 >> n) & 1],
                                                  'form': 'one launch per order and phase + commit, one graph'}}
         if prec_name == 'fp64':
             ref_states = {sl: ens.get_state(sl) for sl in list(ens.cfgs)[:16]}

@@ -4,6 +4,7 @@ shared-memory oracles, Peano/sharedmemoryoracles/, applied to GPU knobs).
 
 tune_ensemble: the contraction per order, then persistent CTAs per SM x
 work items per grab (cells per CTA) x work order, for an Ensemble;
+tune_contraction: the contraction per order alone, in the current launch form;
 tune_predictor: register budget of the predictor kernels
 (exa_tune_set keys) for a grid.  Results can be cached in a JSON file keyed
 by the workload signature."""
@@ -23,6 +24,30 @@ def _time_ensemble(ens, steps):
     ens.step(steps)
     t.stop(s)
     return t.elapsed_ms() / steps
+
+
+def tune_contraction(ens, steps=3, mask=0x30):
+    """Coordinate descent over the contraction of each order present
+    (line-owner or node-gather; exa_ensemble_tune_contraction) in the
+    ensemble's current launch form and schedule, from `mask` (default: the
+    library's, orders 4 and 5 line-owner), flipping one order at a time and
+    keeping the faster.  Applies the result and returns (mask, table)."""
+    table = []
+    present = sorted({c.order for c in ens.cfgs.values()})
+    if not present:
+        return mask, table
+    ens.tune_contraction(mask)
+    base = _time_ensemble(ens, steps)
+    table.append({'stage': 'contraction', 'lines_mask': mask, 'ms_per_step': base})
+    for n in present:
+        trial = mask ^ (1 << n)
+        ens.tune_contraction(trial)
+        ms = _time_ensemble(ens, steps)
+        table.append({'stage': 'contraction', 'lines_mask': trial, 'ms_per_step': ms})
+        if ms < base:
+            mask, base = trial, ms
+    ens.tune_contraction(mask)
+    return mask, table
 
 
 def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), contraction=True, modes=(0, 1),
@@ -54,20 +79,9 @@ def tune_ensemble(ens, steps=3, ctas=(1, 2), grabs=(1, 2, 4, 8), orders=(0, 1), 
             return tuple(got['best']), got['table']
     table = []
     mask = 0x30  # orders 4 and 5 line-owner: the library's default
-    present = sorted({c.order for c in ens.cfgs.values()})
-    if contraction and present:
-        ens.tune_contraction(mask)
+    if contraction and ens.cfgs:
         ens.tune(ctas[0], grabs[0], orders[0])
-        base = _time_ensemble(ens, steps)
-        table.append({'stage': 'contraction', 'lines_mask': mask, 'ms_per_step': base})
-        for n in present:
-            trial = mask ^ (1 << n)
-            ens.tune_contraction(trial)
-            ms = _time_ensemble(ens, steps)
-            table.append({'stage': 'contraction', 'lines_mask': trial, 'ms_per_step': ms})
-            if ms < base:
-                mask, base = trial, ms
-        ens.tune_contraction(mask)
+        mask, table = tune_contraction(ens, steps, mask)
     for c, g, o in itertools.product(ctas, grabs, orders):
         ens.tune(c, g, o)
         ms = _time_ensemble(ens, steps)
